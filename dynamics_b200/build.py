@@ -1,0 +1,62 @@
+"""Build libdynb200.so (all CUDA sources, sm_100a) in-tree.
+
+    python -m dynamics_b200.build          # build if sources are newer
+    python -m dynamics_b200.build --force  # always rebuild
+
+The library is a plain shared object with a C ABI (include/dynb200.h); the
+CUDA runtime is linked statically and cuFFT dynamically (rpath to the CUDA
+toolkit's lib64), so the same .so loads from ctypes, C++ or a Rust FFI.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libdynb200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+SOURCES = ["errors.cu", "nb_compat.cu", "nblist.cu", "pair.cu", "pme.cu", "integrate.cu",
+           "bonded.cu", "system.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def cuda_home():
+    return os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+
+def nvcc():
+    return os.path.join(cuda_home(), "bin", "nvcc")
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "dynb200.h")]
+    return any(os.path.getmtime(p) > t for p in deps)
+
+
+def build(force=False, verbose=False):
+    """Compile every source into dynamics_b200/libdynb200.so."""
+    if not force and not _stale():
+        return LIB
+    lib64 = os.path.join(cuda_home(), "lib64")
+    cmd = [nvcc(), "-shared", "-std=c++17", "-O3", "-lineinfo", *ARCH,
+           "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=default",
+           "-cudart", "static",
+           "-I" + INCLUDE,
+           *[os.path.join(CSRC, s) for s in SOURCES],
+           "-L" + lib64, "-lcufft",
+           "-Xlinker", "-rpath=" + lib64,
+           "-o", LIB + ".tmp"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True, cwd=CSRC)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    path = build(force="--force" in sys.argv, verbose=True)
+    print(path)

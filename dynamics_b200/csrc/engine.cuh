@@ -1,0 +1,174 @@
+// Internal layout of the device-resident engine (layer 2 of the C ABI).
+//
+// HBM layout of one system
+// ------------------------
+// Waters are stored in cluster order: the rebuild sorts molecules into
+// columns of an xy grid, by z inside a column, and pads every column to a
+// multiple of 8 so that each aligned group of 8 slots is a spatially
+// compact cluster.  Per slot:
+//   wpos  float4[4]  O, H0, H1, M positions (.w = site charge)
+//   wvel  float4[3]  O, H0, H1 velocities
+//   wacc  float4[3]  accelerations from the last kick
+//   wid   uint32     original molecule index (INVALID_ID for padding)
+// Forces are int64 fixed point (2^-32 kcal/mol/A): wforce[slot*12 + site*3].
+// Non-water atoms stay in home order (their topology indexes them) and a
+// cluster-ordered copy (spos/slj/sidx) is gathered for the pair kernels.
+// Reciprocal-space forces are cached by original index (wid / atom index)
+// so that they survive re-sorting between SPME evaluations.
+#pragma once
+
+#include <cufft.h>
+
+#include "common.cuh"
+
+#define WCL 8             // waters per cluster
+#define ACL 8             // atoms per cluster
+#define INVALID_ID 0xFFFFFFFFu
+#define NACC 16           // accumulator slots
+
+enum Acc {
+    ACC_E_LJ_WW = 0, ACC_E_COUL_WW, ACC_E_LJ_S, ACC_E_COUL_S, ACC_VIR_SHORT,
+    ACC_E_BONDED, ACC_VIR_BONDED, ACC_KE, ACC_KE_TRANS, ACC_VIR_CONSTR,
+    ACC_E_14, ACC_VIR_14, ACC_E_CORR, ACC_VIR_CORR, ACC_E_RECIP, ACC_VIR_RECIP
+};
+
+// Device-resident scalars of one system.
+struct Scalars {
+    unsigned long long step;      // completed steps
+    unsigned long long rebuilds;
+    unsigned int need_rebuild;    // set by the displacement check
+    unsigned int n_wclus;         // current water cluster count
+    unsigned int n_aclus;         // current atom cluster count
+    unsigned int overflow;        // largest list length that did not fit (0 = ok)
+    unsigned int nonfinite;       // set when a kernel saw NaN/Inf
+    unsigned int max_disp2_bits;  // float bits, atomicMax over non-negative floats
+    unsigned int pad0, pad1;
+    double acc[NACC];             // finalised accumulators of the last step
+    double recip_cache[4];        // e_recip, vir_recip, e_corr, vir_corr of last SPME step
+    double csvr_lambda;
+    double baro_mu;
+    double pressure, temperature;
+    double pe;                    // potential energy of the last energy step
+    double ke_rigid;              // rigid-body KE of the waters + atomic KE of atoms
+    double pressure_atomic;       // the reference's site-virial pressure
+    unsigned long long list_pairs;
+};
+
+// Partial-sum regions (each kernel family writes 4 doubles per block).
+enum Region {
+    REG_WW = 0, REG_WS, REG_SW, REG_SS, REG_14, REG_BOND, REG_KICK_W, REG_KICK_A,
+    REG_CONS, REG_PME, REG_CORR, REG_CORR_A, REG_COM, NREGION
+};
+
+// Pointers and sizes passed by value to every kernel.
+struct SysView {
+    // waters (cluster order)
+    uint32_t nw, nw_cap, nwclus_cap;
+    float4* wpos; float4* wvel; float4* wacc; uint32_t* wid;
+    long long* wforce;            // [nw_cap*12] O,H0,H1,M
+    float4* wref;                 // O position at the last rebuild [nw_cap]
+    float4* wtmp;                 // scratch for permutation [nw_cap*10]
+    uint32_t* wtmp_id;
+    long long* wrecip;            // [nw*9] recip + corrections on M, H0, H1 by original id (M,H0,H1)
+    // atoms (home order)
+    uint32_t na, na_cap, naclus_cap;
+    float4* apos;                 // x, y, z, q
+    float4* avel;                 // x, y, z, unused
+    float4* aacc;
+    float* amass;                 // 0 for static atoms' integration purposes handled by astatic
+    float2* alj;                  // sigma, eps
+    uint8_t* astatic;
+    long long* aforce;            // [na*3]
+    long long* arecip;            // [na*3]
+    float4* aref;                 // position at the last rebuild
+    // atom cluster copy
+    float4* spos; float2* slj; uint32_t* sidx;   // [na_cap]
+    uint32_t* aslot;              // home index -> cluster slot [na]
+    // exclusion CSR over home indices (1-2, 1-3 and 1-4 partners)
+    uint32_t* ex_off; uint32_t* ex_idx;
+    // columns
+    uint32_t ncx, ncy, ncol;
+    uint32_t* col_count; uint32_t* col_off; uint32_t* col_fill;   // [ncol(+1)]
+    uint32_t* col_boff;                         // unpadded bucket offsets [ncol+1]
+    uint32_t* acol_count; uint32_t* acol_off; uint32_t* acol_fill; uint32_t* acol_boff;
+    uint32_t* wnew;                             // new slot of each old water slot
+    float* wkey; float* akey;                   // z sort keys (fraction of the box)
+    uint32_t* bucket; uint32_t* abucket;        // unsorted column members
+    uint32_t* wcol; uint32_t* acol;             // column of each water / atom
+    // cluster bounding boxes (center xyz, half extent xyz)
+    float4* wbb_c; float4* wbb_h; float4* abb_c; float4* abb_h;
+    // cluster lists (fixed capacity per i cluster)
+    uint32_t cap_ww, cap_ws, cap_sw, cap_ss;
+    uint32_t* ww_n; uint32_t* ww_j;
+    uint32_t* ws_n; uint32_t* ws_j;
+    uint32_t* sw_n; uint32_t* sw_j;
+    uint32_t* ss_n; uint32_t* ss_j; unsigned long long* ss_mask;
+    // 1-4 pairs, exclusions (pairs), bonded terms, constraints
+    uint32_t n14; uint2* p14; float4* p14_par;     // sigma, eps, qq, unused
+    uint32_t nexcl; uint2* excl; float* excl_qq;
+    uint32_t nbond; uint2* bond; float2* bond_par;
+    uint32_t nangle; uint4* angle; float2* angle_par;
+    uint32_t ndih; uint4* dih; float4* dih_par;      // k, n, phase
+    uint32_t ncons; uint2* cons; float* cons_r0;
+    // PME
+    uint32_t K[3];
+    long long* qgrid_fix;   // [K0*K1*K2]
+    float* qgrid;           // real grid (cuFFT in/out)
+    float2* cgrid;          // complex grid [K0*K1*(K2/2+1)]
+    float* bmod[3];         // |b(m)|^2 per dimension
+    // box and scalars
+    BoxDev* box;
+    Scalars* sc;
+    double* partials;       // [NREGION][max_blocks][4]
+    uint32_t max_blocks;
+    // parameters
+    float rc, rc2, ljc2, alpha, buffer;
+    float r_ww, r_ws, r_ss;     // list radii
+    uint32_t flags;
+    uint64_t seed;
+    float temperature, gamma, tau_t, p_target, tau_p, kappa;
+    uint32_t thermo_dof;
+    uint32_t integrator, thermostat, barostat;
+    uint32_t spme_interval, com_interval, recenter_interval;
+    double e_self;          // Ewald self energy -alpha/sqrt(pi) sum q^2
+    uint32_t nb[NREGION];   // blocks each region's kernel is launched with
+};
+
+// ---------------------------------------------------------------------------
+// launch wrappers (defined in the .cu files)
+// ---------------------------------------------------------------------------
+namespace dyn {
+
+// nblist.cu
+void launch_displacement_check(const SysView& v, cudaStream_t st);
+void launch_rebuild(const SysView& v, cudaStream_t st, bool force);
+void launch_gather_atoms(const SysView& v, cudaStream_t st);
+
+// pair.cu
+void launch_pairs(const SysView& v, cudaStream_t st, bool energy);
+void launch_pair14(const SysView& v, cudaStream_t st, bool energy);
+int pair_blocks_ww(const SysView& v);
+int pair_blocks_ss(const SysView& v);
+int pair14_blocks(const SysView& v);
+
+// pme.cu
+int pme_init(SysView& v, cufftHandle* plan_f, cufftHandle* plan_b, cudaStream_t st);
+void pme_free(SysView& v, cufftHandle plan_f, cufftHandle plan_b);
+void launch_pme(const SysView& v, cudaStream_t st, cufftHandle plan_f, cufftHandle plan_b);
+void launch_corrections(const SysView& v, cudaStream_t st);
+int pme_blocks(const SysView& v);
+int gather_blocks(const SysView& v);
+int corr_blocks(const SysView& v);
+
+// integrate.cu
+void launch_first_half(const SysView& v, cudaStream_t st, float dt);
+void launch_second_half(const SysView& v, cudaStream_t st, float dt);
+void launch_finalize(const SysView& v, cudaStream_t st, float dt, bool energy, bool thermo);
+void launch_periodic(const SysView& v, cudaStream_t st);
+void launch_bonded(const SysView& v, cudaStream_t st, bool energy);
+void launch_step_end(const SysView& v, cudaStream_t st);
+int kick_blocks_w(const SysView& v);
+int kick_blocks_a(const SysView& v);
+int bond_blocks(const SysView& v);
+
+}  // namespace dyn

@@ -1,0 +1,603 @@
+// Integrator kernels of the resident engine: rigid OPC water, solute atoms,
+// Langevin OU noise, CSVR, C-rescale, COM removal, recentering, and the
+// deterministic float64 reductions that feed the thermostat and barostat.
+//
+// The rigid-water update restates integrate_rigid_water
+// (src/solvent/opc_settle.rs:107-198): COM translation plus a Rodrigues
+// rotation with omega = I^-1 L, wrap of O, minimum-image H, M on the
+// bisector.  Step orders follow MdState::step (src/integrate.rs:100-317):
+//   Langevin-middle: kick dt/2, drift dt/2, OU(dt), drift dt/2, forces,
+//                    kick dt/2;
+//   velocity Verlet: kick dt/2, drift dt, forces, kick dt/2, CSVR.
+// Every kernel processes one water slot or one atom per thread.
+#include "engine.cuh"
+
+namespace {
+
+constexpr int IT = 256;
+
+__device__ __forceinline__ float3 wrap_pos(float3 p, const BoxDev& b) {
+    p.x -= floorf((p.x - b.lo[0]) * b.inv_ext[0]) * b.ext[0];
+    p.y -= floorf((p.y - b.lo[1]) * b.inv_ext[1]) * b.ext[1];
+    p.z -= floorf((p.z - b.lo[2]) * b.inv_ext[2]) * b.ext[2];
+    return p;
+}
+
+__device__ __forceinline__ float3 rodrigues(float3 r, float3 w, float dt) {
+    const float3 od = w * dt;
+    const float th = sqrtf(dot3(od, od));
+    if (th < 1e-12f) {
+        const float3 wxr = cross3(od, r);
+        return r + wxr + cross3(od, wxr) * 0.5f;
+    }
+    const float3 n = od * (1.0f / th);
+    float s, c, sh, ch;
+    sincosf(th, &s, &c);
+    sincosf(0.5f * th, &sh, &ch);
+    const float omc = 2.0f * sh * sh;  // 1 - cos(th) without cancellation
+    return r * c + cross3(n, r) * s + n * (dot3(n, r) * omc);
+}
+
+// COM, COM-frame vectors and angular velocity omega = I^-1 L of one water
+// (src/solvent/opc_settle.rs:108-153).
+struct RigidFrame {
+    float3 rcom, vcom, rO, rH0, rH1, uO, uH0, uH1, L, w;
+};
+
+__device__ __forceinline__ RigidFrame rigid_frame(float3 o, float3 h0, float3 h1, float3 vo, float3 vh0,
+                                                  float3 vh1, const BoxDev& b) {
+    const float mo = OPC_O_MASS, mh = OPC_H_MASS, mt = OPC_MASS_MOL;
+    RigidFrame f;
+    const float3 h0l = o + min_image_rint(h0 - o, b);
+    const float3 h1l = o + min_image_rint(h1 - o, b);
+    f.rcom = (o * mo + h0l * mh + h1l * mh) * (1.0f / mt);
+    f.vcom = (vo * mo + vh0 * mh + vh1 * mh) * (1.0f / mt);
+    f.rO = o - f.rcom; f.rH0 = h0l - f.rcom; f.rH1 = h1l - f.rcom;
+    f.uO = vo - f.vcom; f.uH0 = vh0 - f.vcom; f.uH1 = vh1 - f.vcom;
+    f.L = cross3(f.rO, f.uO) * mo + cross3(f.rH0, f.uH0) * mh + cross3(f.rH1, f.uH1) * mh;
+    float ixx = 0.f, iyy = 0.f, izz = 0.f, ixy = 0.f, ixz = 0.f, iyz = 0.f;
+    const float3 rs[3] = {f.rO, f.rH0, f.rH1};
+    const float ms[3] = {mo, mh, mh};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float3 r = rs[k];
+        const float m = ms[k];
+        const float r2 = dot3(r, r);
+        ixx += m * (r2 - r.x * r.x); iyy += m * (r2 - r.y * r.y); izz += m * (r2 - r.z * r.z);
+        ixy += -m * r.x * r.y; ixz += -m * r.x * r.z; iyz += -m * r.y * r.z;
+    }
+    // solve_symmetric3 (src/solvent/opc_settle.rs:69-95)
+    const float det = ixx * (iyy * izz - iyz * iyz) - ixy * (ixy * izz - iyz * ixz) +
+                      ixz * (ixy * iyz - iyy * ixz);
+    f.w = f3(0.f, 0.f, 0.f);
+    if (fabsf(det) >= 1e-12f) {
+        const float id = 1.0f / det;
+        const float i00 = (iyy * izz - iyz * iyz) * id, i01 = (ixz * iyz - ixy * izz) * id;
+        const float i02 = (ixy * iyz - ixz * iyy) * id, i11 = (ixx * izz - ixz * ixz) * id;
+        const float i12 = (ixz * ixy - ixx * iyz) * id, i22 = (ixx * iyy - ixy * ixy) * id;
+        const float3 L = f.L;
+        f.w = f3(i00 * L.x + i01 * L.y + i02 * L.z, i01 * L.x + i11 * L.y + i12 * L.z,
+                 i02 * L.x + i12 * L.y + i22 * L.z);
+    }
+    return f;
+}
+
+// Rigid drift of one water (src/solvent/opc_settle.rs:107-198).
+__device__ void rigid_drift(float3& o, float3& h0, float3& h1, float3& vo, float3& vh0, float3& vh1,
+                            float dt, const BoxDev& b) {
+    const RigidFrame fr = rigid_frame(o, h0, h1, vo, vh0, vh1, b);
+    const float3 rcom = fr.rcom, vcom = fr.vcom, rO = fr.rO, rH0 = fr.rH0, rH1 = fr.rH1, w = fr.w;
+    const float3 delta = vcom * dt;
+    const float3 rO2 = rodrigues(rO, w, dt), rH02 = rodrigues(rH0, w, dt), rH12 = rodrigues(rH1, w, dt);
+    const float3 no = wrap_pos(rcom + delta + rO2, b);
+    h0 = no + min_image_rint(rcom + delta + rH02 - no, b);
+    h1 = no + min_image_rint(rcom + delta + rH12 - no, b);
+    o = no;
+    vo = vcom + cross3(w, rO2);
+    vh0 = vcom + cross3(w, rH02);
+    vh1 = vcom + cross3(w, rH12);
+}
+
+__device__ __forceinline__ float3 m_site(float3 o, float3 h0, float3 h1) {
+    const float3 bis = (h0 - o) + (h1 - o);
+    return o + bis * (OPC_O_EP_R * rsqrtf(dot3(bis, bis)));
+}
+
+__device__ __forceinline__ bool finite3(float3 a) {
+    return isfinite(a.x) && isfinite(a.y) && isfinite(a.z);
+}
+
+// ---------------------------------------------------------------------------
+// first half of the step
+// ---------------------------------------------------------------------------
+__global__ void k_water_first(SysView v, float dt) {
+    const BoxDev b = *v.box;
+    const uint64_t step = v.sc->step;
+    const bool lm = v.integrator == DYN_INTEGRATOR_LANGEVIN_MIDDLE;
+    const float c = expf(-v.gamma * dt);
+    const float num = KB_NATIVE * v.temperature * fmaxf(1.0f - c * c, 0.f);
+    const float sg_o = sqrtf(num / OPC_O_MASS), sg_h = sqrtf(num / OPC_H_MASS);
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+        const uint32_t id = v.wid[s];
+        if (id == INVALID_ID) continue;
+        float3 o = xyz(v.wpos[4 * s]), h0 = xyz(v.wpos[4 * s + 1]), h1 = xyz(v.wpos[4 * s + 2]);
+        float3 vo = xyz(v.wvel[3 * s]), vh0 = xyz(v.wvel[3 * s + 1]), vh1 = xyz(v.wvel[3 * s + 2]);
+        const float hk = 0.5f * dt;
+        vo = vo + xyz(v.wacc[3 * s]) * hk;
+        vh0 = vh0 + xyz(v.wacc[3 * s + 1]) * hk;
+        vh1 = vh1 + xyz(v.wacc[3 * s + 2]) * hk;
+        if (lm) {
+            rigid_drift(o, h0, h1, vo, vh0, vh1, hk, b);
+            const uint32_t pid = v.na + 3 * id;
+            vo = vo * c + ou_normals(pid, step, v.seed) * sg_o;
+            vh0 = vh0 * c + ou_normals(pid + 1, step, v.seed) * sg_h;
+            vh1 = vh1 * c + ou_normals(pid + 2, step, v.seed) * sg_h;
+            rigid_drift(o, h0, h1, vo, vh0, vh1, hk, b);
+        } else {
+            rigid_drift(o, h0, h1, vo, vh0, vh1, dt, b);
+        }
+        const float3 m = m_site(o, h0, h1);
+        v.wpos[4 * s + 0] = make_float4(o.x, o.y, o.z, 0.f);
+        v.wpos[4 * s + 1] = make_float4(h0.x, h0.y, h0.z, OPC_Q_H);
+        v.wpos[4 * s + 2] = make_float4(h1.x, h1.y, h1.z, OPC_Q_H);
+        v.wpos[4 * s + 3] = make_float4(m.x, m.y, m.z, OPC_Q_EP);
+        v.wvel[3 * s + 0] = make_float4(vo.x, vo.y, vo.z, 0.f);
+        v.wvel[3 * s + 1] = make_float4(vh0.x, vh0.y, vh0.z, 0.f);
+        v.wvel[3 * s + 2] = make_float4(vh1.x, vh1.y, vh1.z, 0.f);
+        if (!finite3(o)) v.sc->nonfinite = 1u;
+    }
+}
+
+__global__ void k_atom_first(SysView v, float dt) {
+    const uint64_t step = v.sc->step;
+    const bool lm = v.integrator == DYN_INTEGRATOR_LANGEVIN_MIDDLE;
+    const float c = expf(-v.gamma * dt);
+    const float num = KB_NATIVE * v.temperature * fmaxf(1.0f - c * c, 0.f);
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+        if (v.astatic && v.astatic[a]) continue;
+        float4 p = v.apos[a];
+        float3 x = xyz(p), vel = xyz(v.avel[a]);
+        const float hk = 0.5f * dt;
+        vel = vel + xyz(v.aacc[a]) * hk;
+        if (lm) {
+            x = x + vel * hk;
+            const float sg = sqrtf(num / v.amass[a]);
+            vel = vel * c + ou_normals(a, step, v.seed) * sg;
+            x = x + vel * hk;
+        } else {
+            x = x + vel * dt;
+        }
+        v.apos[a] = make_float4(x.x, x.y, x.z, p.w);
+        v.avel[a] = make_float4(vel.x, vel.y, vel.z, 0.f);
+        if (!finite3(x)) v.sc->nonfinite = 1u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// second half: forces -> accelerations -> kick, KE partials
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float3 ldfix3(const long long* p) {
+    return f3((float)((double)p[0] * DYN_FIX_INV), (float)((double)p[1] * DYN_FIX_INV),
+              (float)((double)p[2] * DYN_FIX_INV));
+}
+__device__ __forceinline__ float3 ldfix3sum(const long long* p, const long long* q) {
+    return f3((float)((double)(p[0] + q[0]) * DYN_FIX_INV), (float)((double)(p[1] + q[1]) * DYN_FIX_INV),
+              (float)((double)(p[2] + q[2]) * DYN_FIX_INV));
+}
+
+// Besides the reference's KE (every site velocity after the kick,
+// src/integrate.rs:561) this accumulates the rigid-body KE the next drift
+// keeps (M v_com^2 + omega . L), and the intramolecular virial
+// sum_s (r_s - R_com) . F_s, which turns the site virial into the molecular
+// virial a rigid-water pressure needs.
+__global__ void k_water_kick(SysView v, float dt) {
+    const BoxDev b = *v.box;
+    double ke = 0.0, ket = 0.0, ker = 0.0, wi = 0.0;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+        const uint32_t id = v.wid[s];
+        if (id == INVALID_ID) continue;
+        const long long* f = v.wforce + (size_t)s * 12;
+        const long long* r = v.wrecip + (size_t)id * 9;
+        const float3 fo = ldfix3(f);
+        const float3 fh0 = ldfix3sum(f + 3, r + 0);
+        const float3 fh1 = ldfix3sum(f + 6, r + 3);
+        const float3 fm = ldfix3sum(f + 9, r + 6);
+        // project_ep_force (src/solvent/mod.rs:397-406)
+        const float3 ao = (fo + fm * OPC_C_O) * (KCAL_TO_NATIVE / OPC_O_MASS);
+        const float3 ah0 = (fh0 + fm * OPC_C_H) * (KCAL_TO_NATIVE / OPC_H_MASS);
+        const float3 ah1 = (fh1 + fm * OPC_C_H) * (KCAL_TO_NATIVE / OPC_H_MASS);
+        const float hk = 0.5f * dt;
+        const float3 vo = xyz(v.wvel[3 * s]) + ao * hk;
+        const float3 vh0 = xyz(v.wvel[3 * s + 1]) + ah0 * hk;
+        const float3 vh1 = xyz(v.wvel[3 * s + 2]) + ah1 * hk;
+        v.wacc[3 * s + 0] = make_float4(ao.x, ao.y, ao.z, 0.f);
+        v.wacc[3 * s + 1] = make_float4(ah0.x, ah0.y, ah0.z, 0.f);
+        v.wacc[3 * s + 2] = make_float4(ah1.x, ah1.y, ah1.z, 0.f);
+        v.wvel[3 * s + 0] = make_float4(vo.x, vo.y, vo.z, 0.f);
+        v.wvel[3 * s + 1] = make_float4(vh0.x, vh0.y, vh0.z, 0.f);
+        v.wvel[3 * s + 2] = make_float4(vh1.x, vh1.y, vh1.z, 0.f);
+        ke += (double)(OPC_O_MASS * dot3(vo, vo)) + (double)(OPC_H_MASS * dot3(vh0, vh0)) +
+              (double)(OPC_H_MASS * dot3(vh1, vh1));
+        const float3 po = xyz(v.wpos[4 * s]);
+        const RigidFrame fr = rigid_frame(po, xyz(v.wpos[4 * s + 1]), xyz(v.wpos[4 * s + 2]), vo, vh0, vh1, b);
+        ket += (double)(OPC_MASS_MOL * dot3(fr.vcom, fr.vcom));
+        ker += (double)(OPC_MASS_MOL * dot3(fr.vcom, fr.vcom)) + (double)dot3(fr.w, fr.L);
+        const float3 rm = po + min_image_rint(xyz(v.wpos[4 * s + 3]) - po, b) - fr.rcom;
+        wi += (double)dot3(fr.rO, fo) + (double)dot3(fr.rH0, fh0) + (double)dot3(fr.rH1, fh1) +
+              (double)dot3(rm, fm);
+        if (!finite3(ao) || !finite3(ah0) || !finite3(ah1)) v.sc->nonfinite = 1u;
+    }
+    double x[4] = {ke, ket, ker, wi};
+    block_sum_d<4>(x);
+    if (threadIdx.x == 0) {
+        double* p = v.partials + ((size_t)REG_KICK_W * v.max_blocks + blockIdx.x) * 4;
+        p[0] = x[0]; p[1] = x[1]; p[2] = x[2]; p[3] = x[3];
+    }
+}
+
+__global__ void k_atom_kick(SysView v, float dt) {
+    double ke = 0.0;
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+        if (v.astatic && v.astatic[a]) continue;
+        const float3 f = ldfix3sum(v.aforce + 3 * (size_t)a, v.arecip + 3 * (size_t)a);
+        // kick_and_calc_accel with the MAX_ACCEL clamp (src/integrate.rs:521-535)
+        float3 acc = f * (KCAL_TO_NATIVE / v.amass[a]);
+        const float a2 = dot3(acc, acc);
+        if (a2 > MAX_ACCEL * MAX_ACCEL) acc = acc * (MAX_ACCEL * rsqrtf(a2));
+        const float3 vel = xyz(v.avel[a]) + acc * (0.5f * dt);
+        v.aacc[a] = make_float4(acc.x, acc.y, acc.z, 0.f);
+        v.avel[a] = make_float4(vel.x, vel.y, vel.z, 0.f);
+        ke += (double)(v.amass[a] * dot3(vel, vel));
+        if (!finite3(acc)) v.sc->nonfinite = 1u;
+    }
+    double x[2] = {ke, ke};
+    block_sum_d<2>(x);
+    if (threadIdx.x == 0) {
+        double* p = v.partials + ((size_t)REG_KICK_A * v.max_blocks + blockIdx.x) * 4;
+        p[0] = x[0]; p[1] = x[1]; p[2] = x[0]; p[3] = 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// finalize: fixed-order sums of all partials, pressure, temperature, CSVR
+// and C-rescale scalars (single block)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void region_sum(const SysView& v, int reg, double* out) {
+    for (uint32_t i = threadIdx.x; i < v.nb[reg]; i += blockDim.x) {
+        const double* p = v.partials + ((size_t)reg * v.max_blocks + i) * 4;
+        out[0] += p[0]; out[1] += p[1]; out[2] += p[2]; out[3] += p[3];
+    }
+}
+
+__device__ double gamma_mt(double shape, uint64_t step, uint64_t seed) {
+    // Marsaglia & Tsang (ACM TOMS 26, 2000); bounded attempts.
+    const double d = shape - 1.0 / 3.0;
+    const double c = 1.0 / sqrt(9.0 * d);
+    for (uint32_t a = 0; a < 64; ++a) {
+        const Philox4 r = philox4x32(a + 1, (uint32_t)step, DYN_STREAM_CSVR, (uint32_t)(step >> 32),
+                                     (uint32_t)seed, (uint32_t)(seed >> 32));
+        const double u1 = uniform24d(r.x[0]), u2 = uniform24d(r.x[1]);
+        const double x = sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2);
+        const double vv = (1.0 + c * x) * (1.0 + c * x) * (1.0 + c * x);
+        if (vv <= 0.0) continue;
+        const double u = uniform24d(r.x[2]);
+        if (log(u) < 0.5 * x * x + d - d * vv + d * log(vv)) return d * vv;
+    }
+    return d;
+}
+
+template <bool ENERGY>
+__global__ void k_finalize(SysView v, float dt, bool thermo) {
+    double ww[4] = {0, 0, 0, 0}, ws[4] = {0, 0, 0, 0}, sw[4] = {0, 0, 0, 0}, ss[4] = {0, 0, 0, 0};
+    double p14[4] = {0, 0, 0, 0}, bo[4] = {0, 0, 0, 0}, kw[4] = {0, 0, 0, 0}, ka[4] = {0, 0, 0, 0};
+    double co[4] = {0, 0, 0, 0};
+    region_sum(v, REG_WW, ww);
+    if (v.na) {
+        region_sum(v, REG_SS, ss);
+        if (v.nw) { region_sum(v, REG_WS, ws); region_sum(v, REG_SW, sw); }
+        region_sum(v, REG_14, p14);
+        region_sum(v, REG_BOND, bo);
+        region_sum(v, REG_KICK_A, ka);
+        region_sum(v, REG_CONS, co);
+    }
+    region_sum(v, REG_KICK_W, kw);
+    double x[16] = {ww[0], ww[1], ww[2], ws[0] + sw[0] + ss[0], ws[1] + sw[1] + ss[1],
+                    ws[2] + sw[2] + ss[2], p14[0], p14[2], bo[0], bo[2], kw[0] + ka[0],
+                    kw[1] + ka[1], co[0], kw[2] + ka[2], kw[3], 0};
+    block_sum_d<16>(x);
+    if (threadIdx.x != 0) return;
+    Scalars* sc = v.sc;
+    // full lists count every pair from both sides
+    if (ENERGY) {
+        sc->acc[ACC_E_LJ_WW] = 0.5 * x[0];
+        sc->acc[ACC_E_COUL_WW] = 0.5 * x[1];
+        sc->acc[ACC_E_LJ_S] = 0.5 * x[3];
+        sc->acc[ACC_E_COUL_S] = 0.5 * x[4];
+        sc->acc[ACC_E_14] = x[6];
+        sc->acc[ACC_E_BONDED] = x[8];
+    }
+    sc->acc[ACC_VIR_SHORT] = 0.5 * (x[2] + x[5]) + x[7];
+    sc->acc[ACC_VIR_14] = x[7];
+    sc->acc[ACC_VIR_BONDED] = x[9];
+    sc->acc[ACC_VIR_CONSTR] = x[12];
+    sc->acc[ACC_E_RECIP] = sc->recip_cache[0];
+    sc->acc[ACC_VIR_RECIP] = sc->recip_cache[1];
+    sc->acc[ACC_E_CORR] = sc->recip_cache[2];
+    sc->acc[ACC_VIR_CORR] = sc->recip_cache[3];
+    const double to_kcal = 0.5 / (double)KCAL_TO_NATIVE;
+    double ke = x[10] * to_kcal, ket = x[11] * to_kcal, ker = x[13] * to_kcal;
+    const double w_intra = x[14];
+    // CSVR (src/thermostat.rs:258-304) after the final kick of velocity Verlet
+    sc->csvr_lambda = 1.0;
+    if (thermo && v.integrator == DYN_INTEGRATOR_VERLET_VELOCITY && v.thermostat == DYN_THERMO_CSVR &&
+        v.tau_t > 0.f && ker > 1e-20) {
+        const double dof = (double)(v.thermo_dof > 2 ? v.thermo_dof : 2);
+        const double cc = exp(-(double)dt / (double)v.tau_t);
+        const uint64_t step = sc->step;
+        const Philox4 r = philox4x32(0u, (uint32_t)step, DYN_STREAM_CSVR, (uint32_t)(step >> 32),
+                                     (uint32_t)v.seed, (uint32_t)(v.seed >> 32));
+        const double rn = sqrt(-2.0 * log(uniform24d(r.x[0]))) * cos(2.0 * M_PI * uniform24d(r.x[1]));
+        const double chi = 2.0 * gamma_mt(0.5 * (dof - 1.0), step, v.seed);
+        const double ket_target = 0.5 * dof * GAS_CONST_R * (double)v.temperature;
+        // the thermostat acts on the rigid-body KE (the degrees of freedom
+        // that survive the next rigid drift), not the kicked site velocities
+        double kp = ker * cc + ket_target * (1.0 - cc) * ((chi + rn * rn) / dof) +
+                    2.0 * rn * sqrt(cc * (1.0 - cc) * ker * ket_target / dof);
+        kp = kp > 1e-20 ? kp : 1e-20;
+        const double lam = sqrt(kp / ker);
+        sc->csvr_lambda = lam;
+        ke *= lam * lam;
+        ket *= lam * lam;
+        ker *= lam * lam;
+    }
+    sc->acc[ACC_KE] = ke;
+    sc->acc[ACC_KE_TRANS] = ket;
+    sc->ke_rigid = ker;
+    const BoxDev b = *v.box;
+    const double vol = (double)b.ext[0] * b.ext[1] * b.ext[2];
+    const double vir = sc->acc[ACC_VIR_SHORT] + sc->acc[ACC_VIR_RECIP] + sc->acc[ACC_VIR_CORR] +
+                       sc->acc[ACC_VIR_BONDED] + sc->acc[ACC_VIR_CONSTR] / (double)KCAL_TO_NATIVE;
+    // reference formula (src/barostat.rs:419-431): COM KE with the site virial
+    sc->pressure_atomic = (2.0 * ket + vir) / (3.0 * vol) * BAR_PER_KCAL_MOL_A3;
+    // molecular virial for the rigid waters: the barostat's pressure
+    sc->pressure = (2.0 * ket + vir - w_intra) / (3.0 * vol) * BAR_PER_KCAL_MOL_A3;
+    sc->temperature = v.thermo_dof ? 2.0 * ker / ((double)v.thermo_dof * GAS_CONST_R) : 0.0;
+    // C-rescale (Bernetti & Bussi, J. Chem. Phys. 153, 114107 (2020))
+    sc->baro_mu = 1.0;
+    if (thermo && v.barostat == DYN_BARO_CRESCALE && v.tau_p > 0.f) {
+        const uint64_t step = sc->step;
+        const Philox4 r = philox4x32(0u, (uint32_t)step, DYN_STREAM_BARO, (uint32_t)(step >> 32),
+                                     (uint32_t)v.seed, (uint32_t)(v.seed >> 32));
+        const double xi = sqrt(-2.0 * log(uniform24d(r.x[0]))) * cos(2.0 * M_PI * uniform24d(r.x[1]));
+        const double kap = v.kappa, tau = v.tau_p;
+        const double det = kap / tau * (sc->pressure - (double)v.p_target) * dt;
+        const double sig = sqrt(2.0 * kap * KB_BAR_A3 * (double)v.temperature * dt / (tau * vol));
+        double dl = det + sig * xi;
+        dl = dl > 0.1 ? 0.1 : (dl < -0.1 ? -0.1 : dl);
+        sc->baro_mu = exp(dl / 3.0);
+    }
+    if (ENERGY) {
+        double pe;
+        if (v.flags & DYN_FLAG_FULL_ENERGY)
+            pe = sc->acc[ACC_E_LJ_WW] + sc->acc[ACC_E_COUL_WW] + sc->acc[ACC_E_LJ_S] +
+                 sc->acc[ACC_E_COUL_S] + sc->acc[ACC_E_14] + sc->acc[ACC_E_RECIP] +
+                 sc->acc[ACC_E_CORR] + sc->acc[ACC_E_BONDED];
+        else
+            pe = sc->acc[ACC_E_LJ_S] + sc->acc[ACC_E_COUL_S] + sc->acc[ACC_E_14] +
+                 sc->acc[ACC_E_RECIP] + sc->acc[ACC_E_CORR] + sc->acc[ACC_E_BONDED];
+        sc->pe = pe;
+    }
+}
+
+// velocity scaling (CSVR) and C-rescale of positions / box
+__global__ void k_scale(SysView v) {
+    const double lam_d = v.sc->csvr_lambda, mu_d = v.sc->baro_mu;
+    if (lam_d == 1.0 && mu_d == 1.0) return;
+    const float lam = (float)lam_d, mu = (float)mu_d;
+    const BoxDev b = *v.box;
+    const float3 cen = f3(b.lo[0] + 0.5f * b.ext[0], b.lo[1] + 0.5f * b.ext[1], b.lo[2] + 0.5f * b.ext[2]);
+    const float vs = lam / mu;  // C-rescale scales momenta by 1/mu
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        if (v.wid[s] == INVALID_ID) continue;
+        for (int k = 0; k < 3; ++k) {
+            float4 q = v.wvel[3 * s + k];
+            q.x *= vs; q.y *= vs; q.z *= vs;
+            v.wvel[3 * s + k] = q;
+        }
+        if (mu != 1.0f) {
+            // rigid molecules: move the COM, keep the geometry
+            const float3 o = xyz(v.wpos[4 * s]);
+            const float3 h0 = o + min_image_rint(xyz(v.wpos[4 * s + 1]) - o, b);
+            const float3 h1 = o + min_image_rint(xyz(v.wpos[4 * s + 2]) - o, b);
+            const float3 com = (o * OPC_O_MASS + h0 * OPC_H_MASS + h1 * OPC_H_MASS) * (1.0f / OPC_MASS_MOL);
+            const float3 sh = (com - cen) * (mu - 1.0f);
+            for (int k = 0; k < 4; ++k) {
+                float4 q = v.wpos[4 * s + k];
+                q.x += sh.x; q.y += sh.y; q.z += sh.z;
+                v.wpos[4 * s + k] = q;
+            }
+        }
+    }
+    for (uint32_t a = tid; a < v.na; a += stride) {
+        if (v.astatic && v.astatic[a]) continue;
+        float4 q = v.avel[a];
+        q.x *= vs; q.y *= vs; q.z *= vs;
+        v.avel[a] = q;
+        if (mu != 1.0f) {
+            float4 p = v.apos[a];
+            p.x = cen.x + (p.x - cen.x) * mu; p.y = cen.y + (p.y - cen.y) * mu; p.z = cen.z + (p.z - cen.z) * mu;
+            v.apos[a] = p;
+        }
+    }
+}
+
+__global__ void k_scale_box(SysView v) {
+    const double mu = v.sc->baro_mu;
+    if (mu == 1.0) return;
+    BoxDev b = *v.box;
+    for (int k = 0; k < 3; ++k) {
+        const double c = (double)b.lo[k] + 0.5 * (double)b.ext[k];
+        const double e = (double)b.ext[k] * mu;
+        b.lo[k] = (float)(c - 0.5 * e);
+        b.ext[k] = (float)e;
+        b.inv_ext[k] = (float)(1.0 / e);
+    }
+    *v.box = b;
+}
+
+// COM motion removal (src/com_zero.rs:57-81) every com_interval steps
+__global__ void k_com_reduce(SysView v) {
+    const uint64_t next = v.sc->step + 1;
+    const bool on = (v.flags & DYN_FLAG_COM_REMOVAL) && v.com_interval && (next % v.com_interval == 0);
+    double x[4] = {0, 0, 0, 0};
+    if (on) {
+        for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+            if (v.wid[s] == INVALID_ID) continue;
+            const float3 p = xyz(v.wvel[3 * s]) * OPC_O_MASS + xyz(v.wvel[3 * s + 1]) * OPC_H_MASS +
+                             xyz(v.wvel[3 * s + 2]) * OPC_H_MASS;
+            x[0] += p.x; x[1] += p.y; x[2] += p.z; x[3] += OPC_MASS_MOL;
+        }
+        for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+            if (v.astatic && v.astatic[a]) continue;
+            const float3 p = xyz(v.avel[a]) * v.amass[a];
+            x[0] += p.x; x[1] += p.y; x[2] += p.z; x[3] += v.amass[a];
+        }
+    }
+    block_sum_d<4>(x);
+    if (threadIdx.x == 0) {
+        double* p = v.partials + ((size_t)REG_COM * v.max_blocks + blockIdx.x) * 4;
+        p[0] = x[0]; p[1] = x[1]; p[2] = x[2]; p[3] = x[3];
+    }
+}
+
+__global__ void k_com_apply(SysView v) {
+    const uint64_t next = v.sc->step + 1;
+    const bool on = (v.flags & DYN_FLAG_COM_REMOVAL) && v.com_interval && (next % v.com_interval == 0);
+    if (!on) return;
+    __shared__ float3 vc;
+    if (threadIdx.x < 32) {
+        double x[4] = {0, 0, 0, 0};
+        for (uint32_t i = threadIdx.x; i < v.nb[REG_COM]; i += 32) {
+            const double* p = v.partials + ((size_t)REG_COM * v.max_blocks + i) * 4;
+            x[0] += p[0]; x[1] += p[1]; x[2] += p[2]; x[3] += p[3];
+        }
+        for (int k = 0; k < 4; ++k) x[k] = warp_sum_d(x[k]);
+        if (threadIdx.x == 0) {
+            vc = x[3] > 1e-6 ? f3((float)(x[0] / x[3]), (float)(x[1] / x[3]), (float)(x[2] / x[3]))
+                             : f3(0.f, 0.f, 0.f);
+        }
+    }
+    __syncthreads();
+    const float3 c = vc;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+        if (v.wid[s] == INVALID_ID) continue;
+        for (int k = 0; k < 3; ++k) {
+            float4 q = v.wvel[3 * s + k];
+            q.x -= c.x; q.y -= c.y; q.z -= c.z;
+            v.wvel[3 * s + k] = q;
+        }
+    }
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+        if (v.astatic && v.astatic[a]) continue;
+        float4 q = v.avel[a];
+        q.x -= c.x; q.y -= c.y; q.z -= c.z;
+        v.avel[a] = q;
+    }
+}
+
+// SimBox::recenter (src/barostat.rs:111-137) every recenter_interval steps
+__global__ void k_recenter(SysView v) {
+    const uint64_t next = v.sc->step + 1;
+    const bool on = (v.flags & DYN_FLAG_RECENTER) && v.recenter_interval && v.na &&
+                    (next % v.recenter_interval == 0);
+    if (!on) return;
+    double x[4] = {0, 0, 0, 0};
+    for (uint32_t a = threadIdx.x; a < v.na; a += blockDim.x) {
+        if (v.astatic && v.astatic[a]) continue;
+        const float4 p = v.apos[a];
+        x[0] += p.x; x[1] += p.y; x[2] += p.z; x[3] += 1.0;
+    }
+    block_sum_d<4>(x);
+    if (threadIdx.x == 0 && x[3] > 0.0) {
+        BoxDev b = *v.box;
+        for (int k = 0; k < 3; ++k) b.lo[k] = (float)(x[k] / x[3]) - 0.5f * b.ext[k];
+        *v.box = b;
+    }
+}
+
+// reset_angle (src/solvent/opc_settle.rs:202-219) every 1000 steps
+__global__ void k_reset_angle(SysView v) {
+    const uint64_t next = v.sc->step + 1;
+    if (!(v.flags & DYN_FLAG_RESET_ANGLE) || next % 1000 != 0) return;
+    const BoxDev b = *v.box;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+        if (v.wid[s] == INVALID_ID) continue;
+        const float3 o = xyz(v.wpos[4 * s]);
+        const float3 h0 = o + min_image_rint(xyz(v.wpos[4 * s + 1]) - o, b);
+        const float3 h1 = o + min_image_rint(xyz(v.wpos[4 * s + 2]) - o, b);
+        float3 u = h0 + h1 - o * 2.0f;
+        u = u * rsqrtf(dot3(u, u));
+        float3 w = h0 - h1;
+        w = w * rsqrtf(dot3(w, w));
+        w = w - u * dot3(u, w);
+        w = w * rsqrtf(dot3(w, w));
+        float sh, ch;
+        sincosf(0.5f * OPC_HOH_THETA, &sh, &ch);
+        const float3 n0 = o + (u * ch + w * sh) * OPC_O_H_R;
+        const float3 n1 = o + (u * ch - w * sh) * OPC_O_H_R;
+        const float3 m = m_site(o, n0, n1);
+        v.wpos[4 * s + 1] = make_float4(n0.x, n0.y, n0.z, OPC_Q_H);
+        v.wpos[4 * s + 2] = make_float4(n1.x, n1.y, n1.z, OPC_Q_H);
+        v.wpos[4 * s + 3] = make_float4(m.x, m.y, m.z, OPC_Q_EP);
+    }
+}
+
+__global__ void k_step_end(SysView v) { v.sc->step += 1ull; }
+
+inline int iblocks(const SysView& v, uint64_t n) {
+    uint64_t bl = (n + IT - 1) / IT;
+    if (bl < 1) bl = 1;
+    return (int)(bl < v.max_blocks ? bl : v.max_blocks);
+}
+
+}  // namespace
+
+namespace dyn {
+
+int kick_blocks_w(const SysView& v) { return iblocks(v, v.nw_cap); }
+int kick_blocks_a(const SysView& v) { return iblocks(v, v.na); }
+
+void launch_first_half(const SysView& v, cudaStream_t st, float dt) {
+    if (v.nw) k_water_first<<<iblocks(v, v.nw_cap), IT, 0, st>>>(v, dt);
+    if (v.na) k_atom_first<<<iblocks(v, v.na), IT, 0, st>>>(v, dt);
+}
+
+void launch_second_half(const SysView& v, cudaStream_t st, float dt) {
+    if (v.nw) k_water_kick<<<v.nb[REG_KICK_W], IT, 0, st>>>(v, dt);
+    if (v.na) k_atom_kick<<<v.nb[REG_KICK_A], IT, 0, st>>>(v, dt);
+}
+
+void launch_finalize(const SysView& v, cudaStream_t st, float dt, bool energy, bool thermo) {
+    if (energy) k_finalize<true><<<1, 256, 0, st>>>(v, dt, thermo);
+    else k_finalize<false><<<1, 256, 0, st>>>(v, dt, thermo);
+    if (!thermo) return;
+    const bool scales = (v.integrator == DYN_INTEGRATOR_VERLET_VELOCITY && v.thermostat == DYN_THERMO_CSVR) ||
+                        v.barostat == DYN_BARO_CRESCALE;
+    if (!scales) return;
+    k_scale<<<iblocks(v, (uint64_t)v.nw_cap + v.na), IT, 0, st>>>(v);
+    if (v.barostat == DYN_BARO_CRESCALE) k_scale_box<<<1, 1, 0, st>>>(v);
+}
+
+void launch_periodic(const SysView& v, cudaStream_t st) {
+    if (v.flags & DYN_FLAG_COM_REMOVAL) {
+        k_com_reduce<<<v.nb[REG_COM], IT, 0, st>>>(v);
+        k_com_apply<<<v.nb[REG_COM], IT, 0, st>>>(v);
+    }
+    if ((v.flags & DYN_FLAG_RECENTER) && v.na) k_recenter<<<1, 256, 0, st>>>(v);
+    if ((v.flags & DYN_FLAG_RESET_ANGLE) && v.nw) k_reset_angle<<<iblocks(v, v.nw_cap), IT, 0, st>>>(v);
+}
+
+void launch_step_end(const SysView& v, cudaStream_t st) { k_step_end<<<1, 1, 0, st>>>(v); }
+
+}  // namespace dyn

@@ -1,0 +1,400 @@
+// Cluster neighbour lists of the resident engine.
+//
+// The reference rebuilds O(N^2) Verlet lists with a 4 A skin on the host and
+// re-uploads 33 B per pair (src/neighbors.rs:102-281,
+// src/gpu_interface.rs:243-410).  Here the rebuild runs on the device:
+//   1. molecules / atoms are binned into columns of an xy grid and ranked by
+//      z inside each column (deterministic: ties broken by index);
+//   2. waters are physically permuted into that order, columns padded to a
+//      multiple of 8, so every aligned 8-slot group is a compact cluster;
+//   3. cluster bounding boxes are tested against each other (all pairs,
+//      min-image on centres) and each i-cluster's hits are compacted with
+//      warp ballots into a fixed-capacity list, ascending in j.
+// Every kernel of the rebuild returns immediately unless the displacement
+// check raised Scalars::need_rebuild, so the whole step is one static CUDA
+// graph.  The rebuild criterion is the reference's: max displacement since
+// the last rebuild >= buffer / 2 (src/neighbors.rs:159-169), tracking water
+// O only (src/neighbors.rs:71-82); water list radii add twice the O-H reach.
+#include "engine.cuh"
+
+namespace {
+
+__device__ __forceinline__ bool rebuild_on(const SysView& v, bool force) {
+    return force || v.sc->need_rebuild;
+}
+
+__device__ __forceinline__ float frac_box(float x, float lo, float inv_ext) {
+    float f = (x - lo) * inv_ext;
+    f -= floorf(f);
+    return f >= 1.0f ? 0.0f : f;
+}
+
+__device__ __forceinline__ uint32_t column_of(float3 p, const BoxDev& b, uint32_t ncx, uint32_t ncy,
+                                              float* zf) {
+    const float fx = frac_box(p.x, b.lo[0], b.inv_ext[0]);
+    const float fy = frac_box(p.y, b.lo[1], b.inv_ext[1]);
+    *zf = frac_box(p.z, b.lo[2], b.inv_ext[2]);
+    uint32_t cx = min((uint32_t)(fx * ncx), ncx - 1);
+    uint32_t cy = min((uint32_t)(fy * ncy), ncy - 1);
+    return cy * ncx + cx;
+}
+
+// ---------------------------------------------------------------------------
+// displacement check
+// ---------------------------------------------------------------------------
+__global__ void k_disp_check(SysView v) {
+    const BoxDev b = *v.box;
+    float m = 0.f;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        if (v.wid[s] == INVALID_ID) continue;
+        const float3 d = min_image_rint(xyz(v.wpos[4 * s]) - xyz(v.wref[s]), b);
+        const float d2 = dot3(d, d);
+        m = fmaxf(m, isfinite(d2) ? d2 : 1e30f);
+    }
+    for (uint32_t a = tid; a < v.na; a += stride) {
+        const float3 d = xyz(v.apos[a]) - xyz(v.aref[a]);
+        const float d2 = dot3(d, d);
+        m = fmaxf(m, isfinite(d2) ? d2 : 1e30f);
+    }
+    m = warp_max_f(m);
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(&v.sc->max_disp2_bits, __float_as_uint(m));
+}
+
+__global__ void k_disp_decide(SysView v) {
+    const float m = __uint_as_float(v.sc->max_disp2_bits);
+    const float h = 0.5f * v.buffer;
+    if (m >= h * h) v.sc->need_rebuild = 1u;
+    if (m >= 1e29f) v.sc->nonfinite = 1u;
+    v.sc->max_disp2_bits = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// column binning
+// ---------------------------------------------------------------------------
+__global__ void k_col_clear(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= v.ncol; c += gridDim.x * blockDim.x) {
+        if (c < v.ncol) {
+            v.col_count[c] = 0; v.col_fill[c] = 0;
+            v.acol_count[c] = 0; v.acol_fill[c] = 0;
+        }
+    }
+}
+
+__global__ void k_col_assign(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const BoxDev b = *v.box;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        if (v.wid[s] == INVALID_ID) continue;
+        float zf;
+        const uint32_t c = column_of(xyz(v.wpos[4 * s]), b, v.ncx, v.ncy, &zf);
+        v.wcol[s] = c;
+        v.wkey[s] = zf;
+        atomicAdd(&v.col_count[c], 1u);
+    }
+    for (uint32_t a = tid; a < v.na; a += stride) {
+        float zf;
+        const uint32_t c = column_of(xyz(v.apos[a]), b, v.ncx, v.ncy, &zf);
+        v.acol[a] = c;
+        v.akey[a] = zf;
+        atomicAdd(&v.acol_count[c], 1u);
+    }
+}
+
+// Serial scan over columns (only at rebuilds; columns number a few hundred).
+__global__ void k_col_scan(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    if (threadIdx.x == 0) {
+        uint32_t p = 0, q = 0;
+        for (uint32_t c = 0; c < v.ncol; ++c) {
+            v.col_off[c] = p; v.col_boff[c] = q;
+            const uint32_t n = v.col_count[c];
+            p += (n + WCL - 1) / WCL * WCL; q += n;
+        }
+        v.col_off[v.ncol] = p; v.col_boff[v.ncol] = q;
+        v.sc->n_wclus = p / WCL;
+    } else if (threadIdx.x == 32) {
+        uint32_t p = 0, q = 0;
+        for (uint32_t c = 0; c < v.ncol; ++c) {
+            v.acol_off[c] = p; v.acol_boff[c] = q;
+            const uint32_t n = v.acol_count[c];
+            p += (n + ACL - 1) / ACL * ACL; q += n;
+        }
+        v.acol_off[v.ncol] = p; v.acol_boff[v.ncol] = q;
+        v.sc->n_aclus = p / ACL;
+    }
+}
+
+__global__ void k_col_bucket(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        if (v.wid[s] == INVALID_ID) continue;
+        const uint32_t c = v.wcol[s];
+        v.bucket[v.col_boff[c] + atomicAdd(&v.col_fill[c], 1u)] = s;
+    }
+    for (uint32_t a = tid; a < v.na; a += stride) {
+        const uint32_t c = v.acol[a];
+        v.abucket[v.acol_boff[c] + atomicAdd(&v.acol_fill[c], 1u)] = a;
+    }
+}
+
+// Rank inside the column by (z, original index): deterministic order.
+__global__ void k_col_rank(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        if (v.wid[s] == INVALID_ID) continue;
+        const uint32_t c = v.wcol[s];
+        const float z = v.wkey[s];
+        const uint32_t id = v.wid[s];
+        uint32_t r = 0;
+        for (uint32_t k = v.col_boff[c]; k < v.col_boff[c + 1]; ++k) {
+            const uint32_t m = v.bucket[k];
+            const float zm = v.wkey[m];
+            r += (zm < z) || (zm == z && v.wid[m] < id);
+        }
+        v.wnew[s] = v.col_off[c] + r;
+    }
+    for (uint32_t a = tid; a < v.na; a += stride) {
+        const uint32_t c = v.acol[a];
+        const float z = v.akey[a];
+        uint32_t r = 0;
+        for (uint32_t k = v.acol_boff[c]; k < v.acol_boff[c + 1]; ++k) {
+            const uint32_t m = v.abucket[k];
+            const float zm = v.akey[m];
+            r += (zm < z) || (zm == z && m < a);
+        }
+        v.aslot[a] = v.acol_off[c] + r;
+    }
+}
+
+__global__ void k_perm_init(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        v.wtmp_id[s] = INVALID_ID;
+        for (int k = 0; k < 10; ++k) v.wtmp[10 * s + k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (uint32_t s = tid; s < v.na_cap; s += stride) {
+        v.sidx[s] = INVALID_ID;
+        v.slj[s] = make_float2(0.f, 0.f);
+        v.spos[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+__global__ void k_perm_scatter(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        if (v.wid[s] == INVALID_ID) continue;
+        const uint32_t n = v.wnew[s];
+        for (int k = 0; k < 4; ++k) v.wtmp[10 * n + k] = v.wpos[4 * s + k];
+        for (int k = 0; k < 3; ++k) v.wtmp[10 * n + 4 + k] = v.wvel[3 * s + k];
+        for (int k = 0; k < 3; ++k) v.wtmp[10 * n + 7 + k] = v.wacc[3 * s + k];
+        v.wtmp_id[n] = v.wid[s];
+    }
+    for (uint32_t a = tid; a < v.na; a += stride) {
+        const uint32_t s = v.aslot[a];
+        v.sidx[s] = a;
+        v.slj[s] = v.alj[a];
+        v.spos[s] = v.apos[a];
+        v.aref[a] = v.apos[a];
+    }
+}
+
+__global__ void k_perm_copyback(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        for (int k = 0; k < 4; ++k) v.wpos[4 * s + k] = v.wtmp[10 * s + k];
+        for (int k = 0; k < 3; ++k) v.wvel[3 * s + k] = v.wtmp[10 * s + 4 + k];
+        for (int k = 0; k < 3; ++k) v.wacc[3 * s + k] = v.wtmp[10 * s + 7 + k];
+        v.wid[s] = v.wtmp_id[s];
+        v.wref[s] = v.wtmp[10 * s];
+    }
+}
+
+// Bounding boxes of water clusters (O positions) and atom clusters.
+__global__ void k_bbox(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const BoxDev b = *v.box;
+    const uint32_t nwc = v.sc->n_wclus, nac = v.sc->n_aclus;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t c = tid; c < nwc + nac; c += stride) {
+        float3 lo = f3(1e30f, 1e30f, 1e30f), hi = f3(-1e30f, -1e30f, -1e30f);
+        const bool is_w = c < nwc;
+        const uint32_t cl = is_w ? c : c - nwc;
+        // reference point: first valid member; others are min-imaged to it so
+        // a cluster straddling a periodic face still gets a compact box
+        bool have = false;
+        float3 ref = f3(0.f, 0.f, 0.f);
+        for (int k = 0; k < 8; ++k) {
+            float3 p;
+            if (is_w) {
+                const uint32_t s = cl * WCL + k;
+                if (v.wid[s] == INVALID_ID) continue;
+                p = xyz(v.wpos[4 * s]);
+            } else {
+                const uint32_t s = cl * ACL + k;
+                if (v.sidx[s] == INVALID_ID) continue;
+                p = xyz(v.spos[s]);
+            }
+            if (!have) { ref = p; have = true; }
+            p = ref + min_image_rint(p - ref, b);
+            lo = f3(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z));
+            hi = f3(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z));
+        }
+        if (!have) { lo = f3(0.f, 0.f, 0.f); hi = lo; }
+        const float4 cen = make_float4(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z), 0.f);
+        const float4 half = make_float4(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z), 0.f);
+        if (is_w) { v.wbb_c[cl] = cen; v.wbb_h[cl] = half; }
+        else { v.abb_c[cl] = cen; v.abb_h[cl] = half; }
+    }
+}
+
+__device__ __forceinline__ float bb_dist2(float4 ci, float4 hi, float4 cj, float4 hj, const BoxDev& b) {
+    float3 d = f3(ci.x - cj.x, ci.y - cj.y, ci.z - cj.z);
+    d = min_image_rint(d, b);
+    const float gx = fmaxf(0.f, fabsf(d.x) - hi.x - hj.x);
+    const float gy = fmaxf(0.f, fabsf(d.y) - hi.y - hj.y);
+    const float gz = fmaxf(0.f, fabsf(d.z) - hi.z - hj.z);
+    return gx * gx + gy * gy + gz * gz;
+}
+
+__device__ __forceinline__ bool excluded(const SysView& v, uint32_t a, uint32_t b) {
+    uint32_t lo = v.ex_off[a], hi = v.ex_off[a + 1];
+    while (lo < hi) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (v.ex_idx[m] < b) lo = m + 1; else hi = m;
+    }
+    return lo < v.ex_off[a + 1] && v.ex_idx[lo] == b;
+}
+
+// MODE: 0 water-water, 1 water(i)-atom(j), 2 atom(i)-water(j), 3 atom-atom
+template <int MODE>
+__global__ void k_list(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const BoxDev b = *v.box;
+    const int lane = threadIdx.x & 31;
+    const uint32_t ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t ni = (MODE < 2) ? v.sc->n_wclus : v.sc->n_aclus;
+    const uint32_t nj = (MODE == 0 || MODE == 2) ? v.sc->n_wclus : v.sc->n_aclus;
+    if (ci >= ni) return;
+    const float4* bci = (MODE < 2) ? v.wbb_c : v.abb_c;
+    const float4* bhi = (MODE < 2) ? v.wbb_h : v.abb_h;
+    const float4* bcj = (MODE == 0 || MODE == 2) ? v.wbb_c : v.abb_c;
+    const float4* bhj = (MODE == 0 || MODE == 2) ? v.wbb_h : v.abb_h;
+    const float r = MODE == 0 ? v.r_ww : (MODE == 3 ? v.r_ss : v.r_ws);
+    const float r2 = r * r;
+    const uint32_t cap = MODE == 0 ? v.cap_ww : MODE == 1 ? v.cap_ws : MODE == 2 ? v.cap_sw : v.cap_ss;
+    uint32_t* out = MODE == 0 ? v.ww_j : MODE == 1 ? v.ws_j : MODE == 2 ? v.sw_j : v.ss_j;
+    uint32_t* outn = MODE == 0 ? v.ww_n : MODE == 1 ? v.ws_n : MODE == 2 ? v.sw_n : v.ss_n;
+    const float4 c0 = bci[ci], h0 = bhi[ci];
+    uint32_t cnt = 0;
+    for (uint32_t jb = 0; jb < nj; jb += 32) {
+        const uint32_t cj = jb + lane;
+        bool hit = false;
+        if (cj < nj) hit = bb_dist2(c0, h0, bcj[cj], bhj[cj], b) < r2;
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const uint32_t k = cnt + __popc(m & ((1u << lane) - 1u));
+            if (k < cap) {
+                out[(size_t)ci * cap + k] = cj;
+                if (MODE == 3) {
+                    unsigned long long mask = 0ull;
+                    for (int ii = 0; ii < ACL; ++ii) {
+                        const uint32_t a = v.sidx[ci * ACL + ii];
+                        if (a == INVALID_ID) continue;
+                        for (int jj = 0; jj < ACL; ++jj) {
+                            const uint32_t c = v.sidx[cj * ACL + jj];
+                            if (c == INVALID_ID || c == a) continue;
+                            if (v.astatic && v.astatic[a] && v.astatic[c]) continue;
+                            if (v.ex_off && excluded(v, a, c)) continue;
+                            mask |= 1ull << (ii * ACL + jj);
+                        }
+                    }
+                    v.ss_mask[(size_t)ci * cap + k] = mask;
+                }
+            }
+        }
+        cnt += __popc(m);
+    }
+    if (lane == 0) {
+        outn[ci] = min(cnt, cap);
+        if (cnt > cap) atomicMax(&v.sc->overflow, cnt);
+        atomicAdd(&v.sc->list_pairs, (unsigned long long)min(cnt, cap));
+    }
+}
+
+__global__ void k_rebuild_done(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    v.sc->need_rebuild = 0u;
+    v.sc->rebuilds += 1ull;
+}
+
+__global__ void k_list_pairs_reset(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    v.sc->list_pairs = 0ull;
+}
+
+__global__ void k_gather_atoms(SysView v) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.na_cap; s += gridDim.x * blockDim.x) {
+        const uint32_t a = v.sidx[s];
+        if (a != INVALID_ID) v.spos[s] = v.apos[a];
+    }
+}
+
+inline int nblocks(uint64_t n, int threads, int cap = 148 * 8) {
+    uint64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    return (int)(b < (uint64_t)cap ? b : cap);
+}
+
+}  // namespace
+
+namespace dyn {
+
+void launch_displacement_check(const SysView& v, cudaStream_t st) {
+    k_disp_check<<<nblocks(v.nw_cap + v.na, 256), 256, 0, st>>>(v);
+    k_disp_decide<<<1, 1, 0, st>>>(v);
+}
+
+void launch_rebuild(const SysView& v, cudaStream_t st, bool force) {
+    const int T = 256;
+    const uint32_t nmax = v.nw_cap > v.na_cap ? v.nw_cap : v.na_cap;
+    k_col_clear<<<nblocks(v.ncol + 1, T), T, 0, st>>>(v, force);
+    k_col_assign<<<nblocks(nmax, T), T, 0, st>>>(v, force);
+    k_col_scan<<<1, 64, 0, st>>>(v, force);
+    k_col_bucket<<<nblocks(nmax, T), T, 0, st>>>(v, force);
+    k_col_rank<<<nblocks(nmax, T), T, 0, st>>>(v, force);
+    k_perm_init<<<nblocks(nmax, T), T, 0, st>>>(v, force);
+    k_perm_scatter<<<nblocks(nmax, T), T, 0, st>>>(v, force);
+    k_perm_copyback<<<nblocks(v.nw_cap, T), T, 0, st>>>(v, force);
+    k_bbox<<<nblocks(v.nwclus_cap + v.naclus_cap, T), T, 0, st>>>(v, force);
+    k_list_pairs_reset<<<1, 1, 0, st>>>(v, force);
+    const int LT = 128;  // 4 warps per block, one i-cluster per warp
+    if (v.nw) k_list<0><<<nblocks((uint64_t)v.nwclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
+    if (v.nw && v.na) {
+        k_list<1><<<nblocks((uint64_t)v.nwclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
+        k_list<2><<<nblocks((uint64_t)v.naclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
+    }
+    if (v.na) k_list<3><<<nblocks((uint64_t)v.naclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
+    k_rebuild_done<<<1, 1, 0, st>>>(v, force);
+}
+
+void launch_gather_atoms(const SysView& v, cudaStream_t st) {
+    if (v.na) k_gather_atoms<<<nblocks(v.na_cap, 256), 256, 0, st>>>(v);
+}
+
+}  // namespace dyn

@@ -1,0 +1,394 @@
+// Smooth PME on the device: spread -> cuFFT R2C -> fused convolution (energy
+// and virial in float64) -> cuFFT C2R -> gather.
+//
+// The reference hands wrapped positions and charges to the external crate
+// ``ewald`` (src/non_bonded.rs:681-846); this is the published method
+// (Essmann et al. 1995, order-4 cardinal B-splines) on the same grid.
+// Determinism: charges are spread as 64-bit fixed point (2^-32 e-units), so
+// the grid, and everything downstream, is bit-identical run to run.
+// Reciprocal forces (plus the exclusion corrections) are written to a cache
+// indexed by original particle id and added by the kick kernels on every
+// step, which implements the reference's SPME-every-n-steps reuse
+// (src/lib.rs:1282-1341).
+#include <cmath>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace {
+
+constexpr int GT = 256;
+
+__device__ __forceinline__ void bspline4(float w, float* th, float* dth) {
+    const float w2 = w * w, w3 = w2 * w, om = 1.0f - w;
+    th[0] = om * om * om * (1.0f / 6.0f);
+    th[1] = (3.0f * w3 - 6.0f * w2 + 4.0f) * (1.0f / 6.0f);
+    th[2] = (-3.0f * w3 + 3.0f * w2 + 3.0f * w + 1.0f) * (1.0f / 6.0f);
+    th[3] = w3 * (1.0f / 6.0f);
+    if (dth) {
+        dth[0] = -0.5f * om * om;
+        dth[1] = 1.5f * w2 - 2.0f * w;
+        dth[2] = -1.5f * w2 + w + 0.5f;
+        dth[3] = 0.5f * w2;
+    }
+}
+
+// grid coordinate of a position: u = K * frac((x - lo) / L)
+__device__ __forceinline__ void grid_coord(float3 p, const BoxDev& b, const uint32_t* K, int* base,
+                                           float* w) {
+    const float c[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float f = (c[a] - b.lo[a]) * b.inv_ext[a];
+        f -= floorf(f);
+        float u = f * (float)K[a];
+        int i = (int)floorf(u);
+        float ww = u - (float)i;
+        if (i >= (int)K[a]) { i -= K[a]; }
+        if (i < 0) { i += K[a]; }
+        base[a] = i;
+        w[a] = ww;
+    }
+}
+
+__device__ __forceinline__ void spread_one(const SysView& v, float3 p, float q, const BoxDev& b) {
+    int base[3];
+    float w[3];
+    grid_coord(p, b, v.K, base, w);
+    float tx[4], ty[4], tz[4];
+    bspline4(w[0], tx, nullptr);
+    bspline4(w[1], ty, nullptr);
+    bspline4(w[2], tz, nullptr);
+    const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
+    int iz[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) { int z = base[2] - 3 + c; iz[c] = z < 0 ? z + K2 : z; }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        int x = base[0] - 3 + a; x = x < 0 ? x + K0 : x;
+        const float qa = q * tx[a];
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            int y = base[1] - 3 + bb; y = y < 0 ? y + K1 : y;
+            const float qab = qa * ty[bb];
+            long long* row = v.qgrid_fix + ((size_t)x * K1 + y) * K2;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) fix_atomic_add(row + iz[c], fix_from_float(qab * tz[c]));
+        }
+    }
+}
+
+// one thread per charged site: atoms (q != 0), then water H0, H1, M
+__global__ void k_spread(SysView v) {
+    const BoxDev b = *v.box;
+    const uint32_t total = v.na + 3 * v.nw_cap;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        if (t < v.na) {
+            const float4 p = v.apos[t];
+            if (p.w != 0.f) spread_one(v, xyz(p), p.w, b);
+        } else {
+            const uint32_t k = t - v.na;
+            const uint32_t s = k / 3, site = 1 + k % 3;
+            if (v.wid[s] == INVALID_ID) continue;
+            const float4 p = v.wpos[4 * s + site];
+            spread_one(v, xyz(p), p.w, b);
+        }
+    }
+}
+
+__global__ void k_fix2real(SysView v, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        v.qgrid[i] = (float)((double)v.qgrid_fix[i] * DYN_FIX_INV);
+        v.qgrid_fix[i] = 0;
+    }
+}
+
+// Influence function B(m) C(m) applied in place; energy and virial of the
+// reciprocal sum (Essmann eq. 2.10 and the trace of the k-space virial).
+__global__ void k_convolve(SysView v) {
+    const BoxDev b = *v.box;
+    const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
+    const int K2h = K2 / 2 + 1;
+    const uint32_t n = (uint32_t)K0 * K1 * K2h;
+    const float inv_vol = b.inv_ext[0] * b.inv_ext[1] * b.inv_ext[2];
+    const float pa2 = (float)(M_PI * M_PI) / (v.alpha * v.alpha);
+    const float pref = inv_vol * (float)(1.0 / M_PI);
+    double e = 0.0, w = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int kz = i % K2h;
+        const int ky = (i / K2h) % K1;
+        const int kx = i / (K2h * K1);
+        const int mx = kx <= K0 / 2 ? kx : kx - K0;
+        const int my = ky <= K1 / 2 ? ky : ky - K1;
+        const float fx = mx * b.inv_ext[0], fy = my * b.inv_ext[1], fz = kz * b.inv_ext[2];
+        const float m2 = fx * fx + fy * fy + fz * fz;
+        float2 c = v.cgrid[i];
+        float g = 0.f;
+        if (m2 > 0.f) {
+            g = v.bmod[0][kx] * v.bmod[1][ky] * v.bmod[2][kz] * pref * __expf(-pa2 * m2) / m2;
+            const double mult = (kz == 0 || (K2 % 2 == 0 && kz == K2 / 2)) ? 1.0 : 2.0;
+            const double em = 0.5 * mult * (double)g * ((double)c.x * c.x + (double)c.y * c.y);
+            e += em;
+            w += em * (1.0 - 2.0 * (double)pa2 * m2);
+        }
+        c.x *= g; c.y *= g;
+        v.cgrid[i] = c;
+    }
+    double x[2] = {e, w};
+    block_sum_d<2>(x);
+    if (threadIdx.x == 0) {
+        double* p = v.partials + ((size_t)REG_PME * v.max_blocks + blockIdx.x) * 4;
+        p[0] = x[0]; p[1] = x[1]; p[2] = 0.0; p[3] = 0.0;
+    }
+}
+
+__device__ __forceinline__ float3 gather_one(const SysView& v, float3 p, float q, const BoxDev& b) {
+    int base[3];
+    float w[3];
+    grid_coord(p, b, v.K, base, w);
+    float tx[4], ty[4], tz[4], dx[4], dy[4], dz[4];
+    bspline4(w[0], tx, dx);
+    bspline4(w[1], ty, dy);
+    bspline4(w[2], tz, dz);
+    const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
+    int iz[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) { int z = base[2] - 3 + c; iz[c] = z < 0 ? z + K2 : z; }
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        int x = base[0] - 3 + a; x = x < 0 ? x + K0 : x;
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            int y = base[1] - 3 + bb; y = y < 0 ? y + K1 : y;
+            const float* row = v.qgrid + ((size_t)x * K1 + y) * K2;
+            float sz = 0.f, sdz = 0.f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float ph = __ldg(row + iz[c]);
+                sz = fmaf(tz[c], ph, sz);
+                sdz = fmaf(dz[c], ph, sdz);
+            }
+            gx = fmaf(dx[a] * ty[bb], sz, gx);
+            gy = fmaf(tx[a] * dy[bb], sz, gy);
+            gz = fmaf(tx[a] * ty[bb], sdz, gz);
+        }
+    }
+    return f3(-q * K0 * b.inv_ext[0] * gx, -q * K1 * b.inv_ext[1] * gy, -q * K2 * b.inv_ext[2] * gz);
+}
+
+// -q q erf(alpha r)/r between two sites, float64; returns force on the first
+__device__ __forceinline__ double excl_corr(float3 d, double qq, double alpha, double3* f) {
+    const double dx = d.x, dy = d.y, dz = d.z;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double r = sqrt(r2);
+    const double ar = alpha * r;
+    const double er = erf(ar);
+    const double du = qq * (er / r2 - 2.0 * alpha * 0.5641895835477563 * exp(-ar * ar) / r);
+    const double s = -du / r;
+    f->x = s * dx; f->y = s * dy; f->z = s * dz;
+    return -qq * er / r;
+}
+
+// Gather: one thread per atom, or per water (its H0, H1, M), writing the
+// reciprocal cache.  With Ewald corrections on, the intra-water exclusion
+// corrections (H0-H1, H0-M, H1-M) are added here in float64.
+__global__ void k_gather(SysView v) {
+    const BoxDev b = *v.box;
+    const bool corr = v.flags & DYN_FLAG_EWALD_CORRECTIONS;
+    double e_c = 0.0, w_c = 0.0;
+    const uint32_t total = v.na + v.nw_cap;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        if (t < v.na) {
+            const float4 p = v.apos[t];
+            float3 f = f3(0.f, 0.f, 0.f);
+            if (p.w != 0.f) f = gather_one(v, xyz(p), p.w, b);
+            long long* c = v.arecip + 3 * (size_t)t;
+            c[0] = fix_from_float(f.x); c[1] = fix_from_float(f.y); c[2] = fix_from_float(f.z);
+        } else {
+            const uint32_t s = t - v.na;
+            const uint32_t id = v.wid[s];
+            if (id == INVALID_ID) continue;
+            double3 fs[3];
+            float3 ps[3];
+            for (int k = 0; k < 3; ++k) {
+                const float4 p = v.wpos[4 * s + 1 + k];
+                ps[k] = xyz(p);
+                const float3 f = gather_one(v, ps[k], p.w, b);
+                fs[k] = make_double3(f.x, f.y, f.z);
+            }
+            if (corr) {
+                const double q[3] = {OPC_Q_H, OPC_Q_H, OPC_Q_EP};
+                const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
+                for (int k = 0; k < 3; ++k) {
+                    double3 f;
+                    const float3 d = ps[pa[k]] - ps[pb[k]];
+                    e_c += excl_corr(d, q[pa[k]] * q[pb[k]], (double)v.alpha, &f);
+                    w_c += f.x * d.x + f.y * d.y + f.z * d.z;
+                    fs[pa[k]].x += f.x; fs[pa[k]].y += f.y; fs[pa[k]].z += f.z;
+                    fs[pb[k]].x -= f.x; fs[pb[k]].y -= f.y; fs[pb[k]].z -= f.z;
+                }
+            }
+            long long* c = v.wrecip + 9 * (size_t)id;
+            for (int k = 0; k < 3; ++k) {
+                c[3 * k + 0] = fix_from_double(fs[k].x);
+                c[3 * k + 1] = fix_from_double(fs[k].y);
+                c[3 * k + 2] = fix_from_double(fs[k].z);
+            }
+        }
+    }
+    double x[2] = {e_c, w_c};
+    block_sum_d<2>(x);
+    if (threadIdx.x == 0) {
+        double* p = v.partials + ((size_t)REG_CORR * v.max_blocks + blockIdx.x) * 4;
+        p[0] = x[0]; p[1] = x[1]; p[2] = 0.0; p[3] = 0.0;
+    }
+}
+
+// Atom corrections on SPME steps.  Reference bookkeeping: the 1-4 vacuum
+// force correction (src/non_bonded.rs:763-790), applied to the step's forces
+// only, its virial kept with the reciprocal virial.  Corrected mode: float64
+// exclusion corrections for 1-2/1-3 pairs (full) and 1-4 pairs (1 - 1/1.2),
+// into the reciprocal cache.
+__global__ void k_corr_atoms(SysView v) {
+    const BoxDev b = *v.box;
+    const bool corr = v.flags & DYN_FLAG_EWALD_CORRECTIONS;
+    double e_c = 0.0, w_c = 0.0;
+    const uint32_t total = v.n14 + (corr ? v.nexcl : 0u);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        uint2 p;
+        double qq;
+        double scale = 1.0;
+        if (k < v.n14) { p = v.p14[k]; qq = v.p14_par[k].z; scale = 1.0 - 1.0 / 1.2; }
+        else { p = v.excl[k - v.n14]; qq = v.excl_qq[k - v.n14]; }
+        const float3 d = min_image_rint(xyz(v.apos[p.x]) - xyz(v.apos[p.y]), b);
+        if (!corr) {
+            // float32, as the reference: f_vac = dir qq / r^2, df = f_vac (1/1.2 - 1)
+            const float r = sqrtf(dot3(d, d));
+            if (fabsf(r) < 1e-6f) continue;
+            const float3 dir = d * (1.0f / r);
+            const float ir = 1.0f / r;
+            const float3 df = dir * ((float)qq * ir * ir) * (0.833333333f - 1.0f);
+            long long* fa = v.aforce + 3 * (size_t)p.x;
+            long long* fb = v.aforce + 3 * (size_t)p.y;
+            fix_atomic_add(fa + 0, fix_from_float(df.x)); fix_atomic_add(fa + 1, fix_from_float(df.y));
+            fix_atomic_add(fa + 2, fix_from_float(df.z));
+            fix_atomic_add(fb + 0, -fix_from_float(df.x)); fix_atomic_add(fb + 1, -fix_from_float(df.y));
+            fix_atomic_add(fb + 2, -fix_from_float(df.z));
+            w_c += (double)dot3(dir * r, df);
+        } else {
+            double3 f;
+            e_c += excl_corr(d, qq * scale, (double)v.alpha, &f);
+            w_c += f.x * d.x + f.y * d.y + f.z * d.z;
+            long long* fa = v.arecip + 3 * (size_t)p.x;
+            long long* fb = v.arecip + 3 * (size_t)p.y;
+            fix_atomic_add(fa + 0, fix_from_double(f.x)); fix_atomic_add(fa + 1, fix_from_double(f.y));
+            fix_atomic_add(fa + 2, fix_from_double(f.z));
+            fix_atomic_add(fb + 0, -fix_from_double(f.x)); fix_atomic_add(fb + 1, -fix_from_double(f.y));
+            fix_atomic_add(fb + 2, -fix_from_double(f.z));
+        }
+    }
+    double x[2] = {e_c, w_c};
+    block_sum_d<2>(x);
+    if (threadIdx.x == 0) {
+        double* pp = v.partials + ((size_t)REG_CORR_A * v.max_blocks + blockIdx.x) * 4;
+        pp[0] = x[0]; pp[1] = x[1]; pp[2] = 0.0; pp[3] = 0.0;
+    }
+}
+
+// Sums the reciprocal-step partials (fixed order) into the cache.
+__global__ void k_recip_finalize(SysView v) {
+    double x[4] = {0.0, 0.0, 0.0, 0.0};
+    for (uint32_t i = threadIdx.x; i < v.nb[REG_PME]; i += blockDim.x) {
+        const double* p = v.partials + ((size_t)REG_PME * v.max_blocks + i) * 4;
+        x[0] += p[0]; x[1] += p[1];
+    }
+    for (uint32_t i = threadIdx.x; i < v.nb[REG_CORR]; i += blockDim.x) {
+        const double* p = v.partials + ((size_t)REG_CORR * v.max_blocks + i) * 4;
+        x[2] += p[0]; x[3] += p[1];
+    }
+    for (uint32_t i = threadIdx.x; i < v.nb[REG_CORR_A]; i += blockDim.x) {
+        const double* p = v.partials + ((size_t)REG_CORR_A * v.max_blocks + i) * 4;
+        x[2] += p[0]; x[3] += p[1];
+    }
+    block_sum_d<4>(x);
+    if (threadIdx.x == 0) {
+        v.sc->recip_cache[0] = x[0] + v.e_self;
+        v.sc->recip_cache[1] = x[1];
+        v.sc->recip_cache[2] = x[2];
+        v.sc->recip_cache[3] = x[3];
+    }
+}
+
+inline int gblocks(const SysView& v, uint64_t n) {
+    uint64_t bl = (n + GT - 1) / GT;
+    if (bl < 1) bl = 1;
+    return (int)(bl < v.max_blocks ? bl : v.max_blocks);
+}
+
+}  // namespace
+
+namespace dyn {
+
+int pme_blocks(const SysView& v) {
+    return gblocks(v, (uint64_t)v.K[0] * v.K[1] * (v.K[2] / 2 + 1));
+}
+int gather_blocks(const SysView& v) { return gblocks(v, (uint64_t)v.na + v.nw_cap); }
+int corr_blocks(const SysView& v) { return gblocks(v, (uint64_t)v.n14 + v.nexcl); }
+
+int pme_init(SysView& v, cufftHandle* plan_f, cufftHandle* plan_b, cudaStream_t st) {
+    const size_t n = (size_t)v.K[0] * v.K[1] * v.K[2];
+    const size_t nc = (size_t)v.K[0] * v.K[1] * (v.K[2] / 2 + 1);
+    DYN_CUDA(cudaMalloc(&v.qgrid_fix, n * sizeof(long long)));
+    DYN_CUDA(cudaMemsetAsync(v.qgrid_fix, 0, n * sizeof(long long), st));
+    DYN_CUDA(cudaMalloc(&v.qgrid, n * sizeof(float)));
+    DYN_CUDA(cudaMalloc(&v.cgrid, nc * sizeof(float2)));
+    for (int a = 0; a < 3; ++a) {
+        // |b(m)|^2 = 1 / |sum_{k=0}^{2} M4(k+1) exp(2 pi i m k / K)|^2 (Essmann eq. 4.4)
+        const int K = (int)v.K[a];
+        std::vector<float> bm(K);
+        const double mv[3] = {1.0 / 6.0, 4.0 / 6.0, 1.0 / 6.0};
+        for (int m = 0; m < K; ++m) {
+            double re = 0.0, im = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                re += mv[k] * std::cos(2.0 * M_PI * m * k / K);
+                im += mv[k] * std::sin(2.0 * M_PI * m * k / K);
+            }
+            bm[m] = (float)(1.0 / (re * re + im * im));
+        }
+        DYN_CUDA(cudaMalloc(&v.bmod[a], K * sizeof(float)));
+        DYN_CUDA(cudaMemcpyAsync(v.bmod[a], bm.data(), K * sizeof(float), cudaMemcpyHostToDevice, st));
+    }
+    DYN_CUDA(cudaStreamSynchronize(st));
+    if (cufftPlan3d(plan_f, v.K[0], v.K[1], v.K[2], CUFFT_R2C) != CUFFT_SUCCESS)
+        return dyn::fail(DYN_ERR_CUDA, "cufftPlan3d R2C failed");
+    if (cufftPlan3d(plan_b, v.K[0], v.K[1], v.K[2], CUFFT_C2R) != CUFFT_SUCCESS)
+        return dyn::fail(DYN_ERR_CUDA, "cufftPlan3d C2R failed");
+    if (cufftSetStream(*plan_f, st) != CUFFT_SUCCESS || cufftSetStream(*plan_b, st) != CUFFT_SUCCESS)
+        return dyn::fail(DYN_ERR_CUDA, "cufftSetStream failed");
+    return DYN_OK;
+}
+
+void pme_free(SysView& v, cufftHandle plan_f, cufftHandle plan_b) {
+    if (plan_f) cufftDestroy(plan_f);
+    if (plan_b) cufftDestroy(plan_b);
+    cudaFree(v.qgrid_fix); cudaFree(v.qgrid); cudaFree(v.cgrid);
+    for (int a = 0; a < 3; ++a) cudaFree(v.bmod[a]);
+}
+
+void launch_pme(const SysView& v, cudaStream_t st, cufftHandle plan_f, cufftHandle plan_b) {
+    const uint32_t n = v.K[0] * v.K[1] * v.K[2];
+    k_spread<<<gblocks(v, (uint64_t)v.na + 3ull * v.nw_cap), GT, 0, st>>>(v);
+    k_fix2real<<<gblocks(v, n), GT, 0, st>>>(v, n);
+    cufftExecR2C(plan_f, v.qgrid, (cufftComplex*)v.cgrid);
+    k_convolve<<<v.nb[REG_PME], GT, 0, st>>>(v);
+    cufftExecC2R(plan_b, (cufftComplex*)v.cgrid, v.qgrid);
+    k_gather<<<v.nb[REG_CORR], GT, 0, st>>>(v);
+}
+
+void launch_corrections(const SysView& v, cudaStream_t st) {
+    k_corr_atoms<<<v.nb[REG_CORR_A], GT, 0, st>>>(v);
+    k_recip_finalize<<<1, 256, 0, st>>>(v);
+}
+
+}  // namespace dyn

@@ -1,0 +1,864 @@
+// Layer 2 of the C ABI: the device-resident engine behind MdState::step
+// (src/integrate.rs:72-473).  One handle owns one system's HBM state, its
+// CUDA stream, two cuFFT plans and up to four captured CUDA graphs (step
+// with/without SPME, with/without energies).  A step is entirely on the
+// device; the host only picks which graph to launch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.cuh"
+
+struct dyn_sys_s {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;       // created here because the caller passed NULL
+    SysView v{};
+    dyn_config_t cfg{};
+    cufftHandle plan_f = 0, plan_b = 0;
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    float graph_dt[4] = {0, 0, 0, 0};
+    uint64_t host_step = 0;        // steps enqueued so far
+    std::vector<void*> allocs;     // every device allocation, freed on destroy
+    Scalars* h_sc = nullptr;       // pinned mirror of the scalars
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(dyn_sys_s* h, T** p, size_t n, bool zero = true) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaMalloc");
+    h->allocs.push_back((void*)*p);
+    if (zero) {
+        e = cudaMemsetAsync(*p, 0, n * sizeof(T), h->stream);
+        if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaMemsetAsync");
+    }
+    return DYN_OK;
+}
+
+template <typename T>
+int upload(dyn_sys_s* h, T* d, const T* src, size_t n) {
+    if (n == 0 || src == nullptr) return DYN_OK;
+    cudaError_t e = cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaMemcpyAsync H2D");
+    return DYN_OK;
+}
+
+inline uint32_t round8(uint32_t x) { return (x + 7u) / 8u * 8u; }
+
+// Water M site from O, H0, H1 on the host (src/solvent/mod.rs:411-422).
+void host_m_site(const float* o, const float* h0, const float* h1, float* m) {
+    double b[3];
+    for (int k = 0; k < 3; ++k) b[k] = ((double)h0[k] - o[k]) + ((double)h1[k] - o[k]);
+    const double n = std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+    for (int k = 0; k < 3; ++k) m[k] = (float)(o[k] + b[k] / n * (double)OPC_O_EP_R);
+}
+
+void set_block_counts(SysView& v) {
+    for (int r = 0; r < NREGION; ++r) v.nb[r] = 0;
+    v.nb[REG_WW] = v.nw ? dyn::pair_blocks_ww(v) : 0;
+    v.nb[REG_WS] = (v.nw && v.na) ? dyn::pair_blocks_ww(v) : 0;
+    v.nb[REG_SW] = (v.nw && v.na) ? dyn::pair_blocks_ss(v) : 0;
+    v.nb[REG_SS] = v.na ? dyn::pair_blocks_ss(v) : 0;
+    v.nb[REG_14] = v.n14 ? dyn::pair14_blocks(v) : 0;
+    v.nb[REG_BOND] = (v.nbond + v.nangle + v.ndih) ? dyn::bond_blocks(v) : 0;
+    v.nb[REG_KICK_W] = v.nw ? dyn::kick_blocks_w(v) : 0;
+    v.nb[REG_KICK_A] = v.na ? dyn::kick_blocks_a(v) : 0;
+    v.nb[REG_CONS] = 0;
+    v.nb[REG_PME] = dyn::pme_blocks(v);
+    v.nb[REG_CORR] = dyn::gather_blocks(v);
+    v.nb[REG_CORR_A] = dyn::corr_blocks(v);
+    v.nb[REG_COM] = dyn::kick_blocks_w(v) > dyn::kick_blocks_a(v) ? dyn::kick_blocks_w(v)
+                                                                   : dyn::kick_blocks_a(v);
+}
+
+// Everything one step enqueues (MdState::step, src/integrate.rs:100-473).
+void enqueue_step(dyn_sys_s* h, float dt, bool spme, bool energy) {
+    const SysView& v = h->v;
+    cudaStream_t st = h->stream;
+    dyn::launch_first_half(v, st, dt);
+    dyn::launch_displacement_check(v, st);
+    dyn::launch_rebuild(v, st, false);
+    dyn::launch_gather_atoms(v, st);
+    dyn::launch_pairs(v, st, energy);
+    dyn::launch_pair14(v, st, energy);
+    dyn::launch_bonded(v, st, energy);
+    if (spme) {
+        dyn::launch_pme(v, st, h->plan_f, h->plan_b);
+        dyn::launch_corrections(v, st);
+    }
+    dyn::launch_second_half(v, st, dt);
+    dyn::launch_finalize(v, st, dt, energy, true);
+    dyn::launch_periodic(v, st);
+    dyn::launch_step_end(v, st);
+}
+
+// Forces at the current coordinates (no integration); dt = 0 kicks set the
+// accelerations without changing velocities.
+void enqueue_forces(dyn_sys_s* h, bool force_rebuild) {
+    const SysView& v = h->v;
+    cudaStream_t st = h->stream;
+    if (!force_rebuild) dyn::launch_displacement_check(v, st);
+    dyn::launch_rebuild(v, st, force_rebuild);
+    dyn::launch_gather_atoms(v, st);
+    dyn::launch_pairs(v, st, true);
+    dyn::launch_pair14(v, st, true);
+    dyn::launch_bonded(v, st, true);
+    dyn::launch_pme(v, st, h->plan_f, h->plan_b);
+    dyn::launch_corrections(v, st);
+    dyn::launch_second_half(v, st, 0.0f);
+    dyn::launch_finalize(v, st, 0.0f, true, false);
+}
+
+int read_scalars(dyn_sys_s* h) {
+    DYN_CUDA(cudaMemcpyAsync(h->h_sc, h->v.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->h_sc->overflow)
+        return dyn::fail(DYN_ERR_UNSUPPORTED, "cluster list capacity exceeded (list length " +
+                                                  std::to_string(h->h_sc->overflow) + ")");
+    if (h->h_sc->nonfinite) return dyn::fail(DYN_ERR_NONFINITE, "non-finite coordinates or forces");
+    return DYN_OK;
+}
+
+void fill_energies(dyn_sys_s* h, dyn_energies_t* e) {
+    const Scalars& s = *h->h_sc;
+    std::memset(e, 0, sizeof(*e));
+    e->kinetic = s.acc[ACC_KE];
+    e->kinetic_trans = s.acc[ACC_KE_TRANS];
+    e->potential = s.pe;
+    e->e_lj = s.acc[ACC_E_LJ_WW] + s.acc[ACC_E_LJ_S];
+    e->e_coul_short = s.acc[ACC_E_COUL_WW] + s.acc[ACC_E_COUL_S];
+    e->e_water_water_short = s.acc[ACC_E_LJ_WW] + s.acc[ACC_E_COUL_WW];
+    e->e_recip = s.acc[ACC_E_RECIP];
+    e->e_corrections = s.acc[ACC_E_CORR];
+    e->e_bonded = s.acc[ACC_E_BONDED] + s.acc[ACC_E_14];
+    e->virial_short = s.acc[ACC_VIR_SHORT];
+    e->virial_recip = s.acc[ACC_VIR_RECIP] + s.acc[ACC_VIR_CORR];
+    e->virial_bonded = s.acc[ACC_VIR_BONDED];
+    e->virial_constraints = s.acc[ACC_VIR_CONSTR] / (double)KCAL_TO_NATIVE;
+    e->virial = e->virial_short + e->virial_recip + e->virial_bonded + e->virial_constraints;
+    e->pressure_bar = s.pressure;
+    e->temperature = s.temperature;
+    e->step = s.step;
+    e->list_rebuilds = s.rebuilds;
+    e->pairs_in_list = s.list_pairs;
+    e->kinetic_rigid = s.ke_rigid;
+    e->pressure_atomic_bar = s.pressure_atomic;
+}
+
+}  // namespace
+
+extern "C" int dyn_sys_destroy(dyn_sys_t h) {
+    if (!h) return DYN_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream); else cudaDeviceSynchronize();
+    for (int g = 0; g < 4; ++g)
+        if (h->graph[g]) cudaGraphExecDestroy(h->graph[g]);
+    if (h->plan_f) cufftDestroy(h->plan_f);
+    if (h->plan_b) cufftDestroy(h->plan_b);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->h_sc) cudaFreeHost(h->h_sc);
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return DYN_OK;
+}
+
+extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_system_desc_t* d,
+                              dyn_sys_t* out) {
+    DYN_CHECK(cfg && d && out, DYN_ERR_INVALID, "dyn_sys_create: NULL argument");
+    *out = nullptr;
+    DYN_CHECK(d->n_atoms + d->n_water > 0, DYN_ERR_INVALID, "dyn_sys_create: empty system");
+    DYN_CHECK(d->n_water == 0 || (d->water_pos && d->water_vel), DYN_ERR_INVALID,
+              "dyn_sys_create: water arrays required");
+    DYN_CHECK(d->n_atoms == 0 || (d->atom_pos && d->atom_vel && d->atom_mass && d->atom_q &&
+                                  d->atom_sigma && d->atom_eps),
+              DYN_ERR_INVALID, "dyn_sys_create: atom arrays required");
+    float ext[3];
+    for (int k = 0; k < 3; ++k) {
+        ext[k] = cfg->box_hi[k] - cfg->box_lo[k];
+        DYN_CHECK(ext[k] > 0.f, DYN_ERR_INVALID, "dyn_sys_create: box extent must be > 0");
+    }
+    const float rc = cfg->coulomb_cutoff, ljc = cfg->lj_cutoff > 0.f ? cfg->lj_cutoff : rc;
+    DYN_CHECK(rc > 0.f && cfg->ewald_alpha > 0.f && cfg->list_buffer >= 0.f, DYN_ERR_INVALID,
+              "dyn_sys_create: cutoff and alpha must be > 0, buffer >= 0");
+    const float lmin = std::min(ext[0], std::min(ext[1], ext[2]));
+    DYN_CHECK(std::max(rc, ljc) + 2.0f * OPC_SITE_REACH < 0.5f * lmin, DYN_ERR_INVALID,
+              "dyn_sys_create: cutoff + 2 * 0.8725 A must be below half the smallest box edge");
+    for (int k = 0; k < 3; ++k)
+        DYN_CHECK(cfg->grid[k] >= 8 && cfg->grid[k] <= 1024, DYN_ERR_INVALID,
+                  "dyn_sys_create: grid dimensions must be in [8, 1024]");
+    DYN_CHECK(cfg->integrator <= 1 && cfg->thermostat <= 1 && cfg->barostat <= 1, DYN_ERR_INVALID,
+              "dyn_sys_create: unknown integrator/thermostat/barostat");
+    for (uint32_t i = 0; i < d->n_excl * 2; ++i)
+        DYN_CHECK(d->excl[i] < d->n_atoms, DYN_ERR_INVALID, "dyn_sys_create: exclusion index out of range");
+    for (uint32_t i = 0; i < d->n_pair14 * 2; ++i)
+        DYN_CHECK(d->pair14[i] < d->n_atoms, DYN_ERR_INVALID, "dyn_sys_create: 1-4 index out of range");
+    for (uint32_t i = 0; i < d->n_bonds * 2; ++i)
+        DYN_CHECK(d->bonds[i] < d->n_atoms, DYN_ERR_INVALID, "dyn_sys_create: bond index out of range");
+    for (uint32_t i = 0; i < d->n_angles * 3; ++i)
+        DYN_CHECK(d->angles[i] < d->n_atoms, DYN_ERR_INVALID, "dyn_sys_create: angle index out of range");
+    for (uint32_t i = 0; i < d->n_dihedrals * 4; ++i)
+        DYN_CHECK(d->dihedrals[i] < d->n_atoms, DYN_ERR_INVALID, "dyn_sys_create: dihedral index out of range");
+    for (uint32_t i = 0; i < d->n_atoms; ++i)
+        DYN_CHECK(d->atom_mass[i] > 0.f || (d->atom_static && d->atom_static[i]), DYN_ERR_INVALID,
+                  "dyn_sys_create: non-static atoms need mass > 0");
+
+    dyn_sys_s* h = new dyn_sys_s();
+    h->stream = (cudaStream_t)stream;
+    if (!h->stream) {
+        // graphs cannot be captured on the legacy default stream
+        cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete h; return dyn::cuda_fail(e, "cudaStreamCreateWithFlags"); }
+        h->own_stream = true;
+    }
+    h->cfg = *cfg;
+    SysView& v = h->v;
+    int rc_ = DYN_OK;
+#define TRY(x) do { if ((rc_ = (x)) != DYN_OK) { dyn_sys_destroy(h); return rc_; } } while (0)
+#define TRYC(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { rc_ = dyn::cuda_fail(_e, #x); dyn_sys_destroy(h); return rc_; } } while (0)
+    TRYC(cudaMallocHost((void**)&h->h_sc, sizeof(Scalars)));
+    std::memset(h->h_sc, 0, sizeof(Scalars));
+
+    v.nw = d->n_water;
+    v.na = d->n_atoms;
+    // parameters
+    v.rc = rc; v.rc2 = rc * rc; v.ljc2 = ljc * ljc; v.alpha = cfg->ewald_alpha;
+    v.buffer = cfg->list_buffer;
+    v.r_ww = std::max(ljc, rc + 2.0f * OPC_SITE_REACH) + v.buffer;
+    v.r_ws = std::max(ljc, rc + OPC_SITE_REACH) + v.buffer;
+    v.r_ss = std::max(ljc, rc) + v.buffer;
+    v.flags = cfg->flags; v.seed = cfg->seed;
+    v.temperature = cfg->temperature; v.gamma = cfg->langevin_gamma; v.tau_t = cfg->tau_temp;
+    v.p_target = cfg->pressure_bar; v.tau_p = cfg->tau_pressure; v.kappa = cfg->compressibility;
+    v.thermo_dof = cfg->thermo_dof;
+    v.integrator = cfg->integrator; v.thermostat = cfg->thermostat; v.barostat = cfg->barostat;
+    v.spme_interval = std::max(1u, cfg->spme_interval);
+    v.com_interval = cfg->com_interval; v.recenter_interval = cfg->recenter_interval;
+    for (int k = 0; k < 3; ++k) v.K[k] = cfg->grid[k];
+
+    // column grid: edge close to that of a cube holding 8 waters
+    const double vol = (double)ext[0] * ext[1] * ext[2];
+    const double dens = (double)std::max<uint32_t>(1u, v.nw + v.na / 3) / vol;
+    const double edge = std::cbrt(8.0 / dens);
+    v.ncx = std::max(1u, (uint32_t)std::floor(ext[0] / edge));
+    v.ncy = std::max(1u, (uint32_t)std::floor(ext[1] / edge));
+    v.ncol = v.ncx * v.ncy;
+    v.nw_cap = v.nw ? round8(v.nw + 7 * v.ncol + 8) : 8;
+    v.nwclus_cap = v.nw_cap / WCL;
+    v.na_cap = v.na ? round8(v.na + 7 * v.ncol + 8) : 8;
+    v.naclus_cap = v.na_cap / ACL;
+    v.max_blocks = 148 * 16;
+
+    // list capacities from the cluster density, generous margin
+    auto est = [&](double r, double cl_vol, uint32_t ncl) -> uint32_t {
+        const double rad = r + 2.0 * 0.9 * std::cbrt(cl_vol);
+        const double n = 4.0 / 3.0 * M_PI * rad * rad * rad / cl_vol;
+        const uint32_t e = (uint32_t)(2.0 * n) + 32;
+        return std::max(1u, std::min(e, ncl));
+    };
+    const double wcl_vol = v.nw ? vol / std::max(1.0, v.nw / 8.0) : vol;
+    const double acl_vol = std::max(8.0 / 0.12, v.na ? 8.0 * vol / std::max(1u, v.nw * 4 + v.na) * 4.0 : vol);
+    v.cap_ww = v.nw ? est(v.r_ww, wcl_vol, v.nwclus_cap) : 1;
+    v.cap_ws = (v.nw && v.na) ? est(v.r_ws, acl_vol, v.naclus_cap) : 1;
+    v.cap_sw = (v.nw && v.na) ? est(v.r_ws, wcl_vol, v.nwclus_cap) : 1;
+    v.cap_ss = v.na ? est(v.r_ss, acl_vol, v.naclus_cap) : 1;
+
+    // ---- allocations ----
+    TRY(dev_alloc(h, &v.wpos, 4 * (size_t)v.nw_cap));
+    TRY(dev_alloc(h, &v.wvel, 3 * (size_t)v.nw_cap));
+    TRY(dev_alloc(h, &v.wacc, 3 * (size_t)v.nw_cap));
+    TRY(dev_alloc(h, &v.wid, v.nw_cap, false));
+    TRYC(cudaMemsetAsync(v.wid, 0xFF, v.nw_cap * sizeof(uint32_t), h->stream));
+    TRY(dev_alloc(h, &v.wforce, 12 * (size_t)v.nw_cap));
+    TRY(dev_alloc(h, &v.wref, v.nw_cap));
+    TRY(dev_alloc(h, &v.wtmp, 10 * (size_t)v.nw_cap));
+    TRY(dev_alloc(h, &v.wtmp_id, v.nw_cap));
+    TRY(dev_alloc(h, &v.wrecip, 9 * (size_t)std::max(1u, v.nw)));
+    TRY(dev_alloc(h, &v.wnew, v.nw_cap));
+    TRY(dev_alloc(h, &v.wkey, v.nw_cap));
+    TRY(dev_alloc(h, &v.wcol, v.nw_cap));
+    TRY(dev_alloc(h, &v.bucket, v.nw_cap));
+    TRY(dev_alloc(h, &v.apos, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.avel, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.aacc, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.amass, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.alj, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.aforce, 3 * (size_t)std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.arecip, 3 * (size_t)std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.aref, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.spos, v.na_cap));
+    TRY(dev_alloc(h, &v.slj, v.na_cap));
+    TRY(dev_alloc(h, &v.sidx, v.na_cap, false));
+    TRYC(cudaMemsetAsync(v.sidx, 0xFF, v.na_cap * sizeof(uint32_t), h->stream));
+    TRY(dev_alloc(h, &v.aslot, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.akey, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.acol, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.abucket, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.col_count, v.ncol + 1));
+    TRY(dev_alloc(h, &v.col_off, v.ncol + 1));
+    TRY(dev_alloc(h, &v.col_fill, v.ncol + 1));
+    TRY(dev_alloc(h, &v.col_boff, v.ncol + 1));
+    TRY(dev_alloc(h, &v.acol_count, v.ncol + 1));
+    TRY(dev_alloc(h, &v.acol_off, v.ncol + 1));
+    TRY(dev_alloc(h, &v.acol_fill, v.ncol + 1));
+    TRY(dev_alloc(h, &v.acol_boff, v.ncol + 1));
+    TRY(dev_alloc(h, &v.wbb_c, v.nwclus_cap));
+    TRY(dev_alloc(h, &v.wbb_h, v.nwclus_cap));
+    TRY(dev_alloc(h, &v.abb_c, v.naclus_cap));
+    TRY(dev_alloc(h, &v.abb_h, v.naclus_cap));
+    TRY(dev_alloc(h, &v.ww_n, v.nwclus_cap));
+    TRY(dev_alloc(h, &v.ww_j, (size_t)v.nwclus_cap * v.cap_ww));
+    TRY(dev_alloc(h, &v.ws_n, v.nwclus_cap));
+    TRY(dev_alloc(h, &v.ws_j, (size_t)v.nwclus_cap * v.cap_ws));
+    TRY(dev_alloc(h, &v.sw_n, v.naclus_cap));
+    TRY(dev_alloc(h, &v.sw_j, (size_t)v.naclus_cap * v.cap_sw));
+    TRY(dev_alloc(h, &v.ss_n, v.naclus_cap));
+    TRY(dev_alloc(h, &v.ss_j, (size_t)v.naclus_cap * v.cap_ss));
+    TRY(dev_alloc(h, &v.ss_mask, (size_t)v.naclus_cap * v.cap_ss));
+    TRY(dev_alloc(h, &v.box, 1));
+    TRY(dev_alloc(h, &v.sc, 1));
+    TRY(dev_alloc(h, &v.partials, (size_t)NREGION * v.max_blocks * 4));
+
+    // ---- state upload ----
+    if (v.nw) {
+        std::vector<float4> wp(4 * (size_t)v.nw_cap, make_float4(0, 0, 0, 0));
+        std::vector<float4> wv(3 * (size_t)v.nw_cap, make_float4(0, 0, 0, 0));
+        std::vector<uint32_t> wid(v.nw_cap, INVALID_ID);
+        const float q[4] = {0.f, OPC_Q_H, OPC_Q_H, OPC_Q_EP};
+        for (uint32_t i = 0; i < v.nw; ++i) {
+            const float* p = d->water_pos + 9 * (size_t)i;
+            float m[3];
+            host_m_site(p, p + 3, p + 6, m);
+            for (int s = 0; s < 3; ++s) wp[4 * i + s] = make_float4(p[3 * s], p[3 * s + 1], p[3 * s + 2], q[s]);
+            wp[4 * i + 3] = make_float4(m[0], m[1], m[2], q[3]);
+            const float* w = d->water_vel + 9 * (size_t)i;
+            for (int s = 0; s < 3; ++s) wv[3 * i + s] = make_float4(w[3 * s], w[3 * s + 1], w[3 * s + 2], 0.f);
+            wid[i] = i;
+        }
+        TRY(upload(h, v.wpos, wp.data(), wp.size()));
+        TRY(upload(h, v.wvel, wv.data(), wv.size()));
+        TRY(upload(h, v.wid, wid.data(), wid.size()));
+        TRYC(cudaStreamSynchronize(h->stream));
+    }
+    double qsum2 = (double)v.nw * (2.0 * (double)OPC_Q_H * OPC_Q_H + (double)OPC_Q_EP * OPC_Q_EP);
+    if (v.na) {
+        std::vector<float4> ap(v.na), av(v.na);
+        std::vector<float2> lj(v.na);
+        for (uint32_t i = 0; i < v.na; ++i) {
+            ap[i] = make_float4(d->atom_pos[3 * i], d->atom_pos[3 * i + 1], d->atom_pos[3 * i + 2], d->atom_q[i]);
+            av[i] = make_float4(d->atom_vel[3 * i], d->atom_vel[3 * i + 1], d->atom_vel[3 * i + 2], 0.f);
+            lj[i] = make_float2(d->atom_sigma[i], d->atom_eps[i]);
+            qsum2 += (double)d->atom_q[i] * d->atom_q[i];
+        }
+        TRY(upload(h, v.apos, ap.data(), v.na));
+        TRY(upload(h, v.avel, av.data(), v.na));
+        TRY(upload(h, v.amass, d->atom_mass, v.na));
+        TRY(upload(h, v.alj, lj.data(), v.na));
+        if (d->atom_static) {
+            TRY(dev_alloc(h, &v.astatic, v.na));
+            TRY(upload(h, v.astatic, d->atom_static, v.na));
+        }
+        // exclusion CSR (1-2, 1-3 and 1-4 partners; 1-4 pairs are evaluated
+        // separately, scaled)
+        std::vector<std::vector<uint32_t>> rows(v.na);
+        for (uint32_t k = 0; k < d->n_excl; ++k) {
+            rows[d->excl[2 * k]].push_back(d->excl[2 * k + 1]);
+            rows[d->excl[2 * k + 1]].push_back(d->excl[2 * k]);
+        }
+        for (uint32_t k = 0; k < d->n_pair14; ++k) {
+            rows[d->pair14[2 * k]].push_back(d->pair14[2 * k + 1]);
+            rows[d->pair14[2 * k + 1]].push_back(d->pair14[2 * k]);
+        }
+        std::vector<uint32_t> off(v.na + 1, 0), idx;
+        for (uint32_t i = 0; i < v.na; ++i) {
+            std::sort(rows[i].begin(), rows[i].end());
+            rows[i].erase(std::unique(rows[i].begin(), rows[i].end()), rows[i].end());
+            off[i + 1] = off[i] + (uint32_t)rows[i].size();
+            idx.insert(idx.end(), rows[i].begin(), rows[i].end());
+        }
+        TRY(dev_alloc(h, &v.ex_off, v.na + 1));
+        TRY(dev_alloc(h, &v.ex_idx, std::max<size_t>(1, idx.size())));
+        TRY(upload(h, v.ex_off, off.data(), off.size()));
+        TRY(upload(h, v.ex_idx, idx.data(), idx.size()));
+        // 1-4 and exclusion lists
+        v.n14 = d->n_pair14;
+        if (v.n14) {
+            std::vector<uint2> p(v.n14);
+            std::vector<float4> par(v.n14);
+            for (uint32_t k = 0; k < v.n14; ++k) {
+                const uint32_t i = d->pair14[2 * k], j = d->pair14[2 * k + 1];
+                p[k] = make_uint2(i, j);
+                par[k] = make_float4(0.5f * (d->atom_sigma[i] + d->atom_sigma[j]),
+                                     std::sqrt(d->atom_eps[i] * d->atom_eps[j]), d->atom_q[i] * d->atom_q[j], 0.f);
+            }
+            TRY(dev_alloc(h, &v.p14, v.n14));
+            TRY(dev_alloc(h, &v.p14_par, v.n14));
+            TRY(upload(h, v.p14, p.data(), v.n14));
+            TRY(upload(h, v.p14_par, par.data(), v.n14));
+        }
+        v.nexcl = d->n_excl;
+        if (v.nexcl) {
+            std::vector<uint2> p(v.nexcl);
+            std::vector<float> qq(v.nexcl);
+            for (uint32_t k = 0; k < v.nexcl; ++k) {
+                p[k] = make_uint2(d->excl[2 * k], d->excl[2 * k + 1]);
+                qq[k] = d->atom_q[d->excl[2 * k]] * d->atom_q[d->excl[2 * k + 1]];
+            }
+            TRY(dev_alloc(h, &v.excl, v.nexcl));
+            TRY(dev_alloc(h, &v.excl_qq, v.nexcl));
+            TRY(upload(h, v.excl, p.data(), v.nexcl));
+            TRY(upload(h, v.excl_qq, qq.data(), v.nexcl));
+        }
+        // bonded terms
+        v.nbond = d->n_bonds;
+        if (v.nbond) {
+            std::vector<uint2> p(v.nbond);
+            std::vector<float2> par(v.nbond);
+            for (uint32_t k = 0; k < v.nbond; ++k) {
+                p[k] = make_uint2(d->bonds[2 * k], d->bonds[2 * k + 1]);
+                par[k] = make_float2(d->bond_k[k], d->bond_r0[k]);
+            }
+            TRY(dev_alloc(h, &v.bond, v.nbond));
+            TRY(dev_alloc(h, &v.bond_par, v.nbond));
+            TRY(upload(h, v.bond, p.data(), v.nbond));
+            TRY(upload(h, v.bond_par, par.data(), v.nbond));
+        }
+        v.nangle = d->n_angles;
+        if (v.nangle) {
+            std::vector<uint4> p(v.nangle);
+            std::vector<float2> par(v.nangle);
+            for (uint32_t k = 0; k < v.nangle; ++k) {
+                p[k] = make_uint4(d->angles[3 * k], d->angles[3 * k + 1], d->angles[3 * k + 2], 0);
+                par[k] = make_float2(d->angle_k[k], d->angle_theta0[k]);
+            }
+            TRY(dev_alloc(h, &v.angle, v.nangle));
+            TRY(dev_alloc(h, &v.angle_par, v.nangle));
+            TRY(upload(h, v.angle, p.data(), v.nangle));
+            TRY(upload(h, v.angle_par, par.data(), v.nangle));
+        }
+        v.ndih = d->n_dihedrals;
+        if (v.ndih) {
+            std::vector<uint4> p(v.ndih);
+            std::vector<float4> par(v.ndih);
+            for (uint32_t k = 0; k < v.ndih; ++k) {
+                p[k] = make_uint4(d->dihedrals[4 * k], d->dihedrals[4 * k + 1], d->dihedrals[4 * k + 2],
+                                  d->dihedrals[4 * k + 3]);
+                par[k] = make_float4(d->dihedral_k[k], d->dihedral_n[k], d->dihedral_phase[k], 0.f);
+            }
+            TRY(dev_alloc(h, &v.dih, v.ndih));
+            TRY(dev_alloc(h, &v.dih_par, v.ndih));
+            TRY(upload(h, v.dih, p.data(), v.ndih));
+            TRY(upload(h, v.dih_par, par.data(), v.ndih));
+        }
+    }
+    v.e_self = -(double)v.alpha / std::sqrt(M_PI) * qsum2;
+    BoxDev bx{};
+    for (int k = 0; k < 3; ++k) {
+        bx.lo[k] = cfg->box_lo[k];
+        bx.ext[k] = ext[k];
+        bx.inv_ext[k] = (float)(1.0 / (double)ext[k]);
+    }
+    TRY(upload(h, v.box, &bx, 1));
+    TRY(dyn::pme_init(v, &h->plan_f, &h->plan_b, h->stream));
+    h->allocs.push_back(v.qgrid_fix); h->allocs.push_back(v.qgrid); h->allocs.push_back(v.cgrid);
+    for (int a = 0; a < 3; ++a) h->allocs.push_back(v.bmod[a]);
+    set_block_counts(v);
+    TRYC(cudaStreamSynchronize(h->stream));
+    // prime: first list build and forces -> accelerations
+    enqueue_forces(h, true);
+    TRYC(cudaGetLastError());
+    TRY(read_scalars(h));
+#undef TRY
+#undef TRYC
+    *out = h;
+    return DYN_OK;
+}
+
+extern "C" int dyn_sys_step(dyn_sys_t h, uint32_t n_steps, float dt) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_step: NULL handle");
+    DYN_CHECK(dt > 0.f && std::isfinite(dt), DYN_ERR_INVALID, "dyn_sys_step: dt must be > 0");
+    const uint32_t e_int = std::max(1u, h->cfg.energy_interval);
+    for (uint32_t i = 0; i < n_steps; ++i) {
+        const uint64_t s = h->host_step;
+        const bool spme = (s % h->v.spme_interval) == 0;
+        const bool energy = ((s + 1) % e_int) == 0;
+        const int g = (spme ? 1 : 0) | (energy ? 2 : 0);
+        if (!h->graph[g] || h->graph_dt[g] != dt) {
+            if (h->graph[g]) { cudaGraphExecDestroy(h->graph[g]); h->graph[g] = nullptr; }
+            cudaGraph_t graph;
+            DYN_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_step(h, dt, spme, energy);
+            DYN_CUDA(cudaStreamEndCapture(h->stream, &graph));
+            cudaError_t e = cudaGraphInstantiate(&h->graph[g], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaGraphInstantiate");
+            h->graph_dt[g] = dt;
+        }
+        DYN_CUDA(cudaGraphLaunch(h->graph[g], h->stream));
+        h->host_step += 1;
+    }
+    return DYN_OK;
+}
+
+extern "C" int dyn_sys_sync(dyn_sys_t h) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_sync: NULL handle");
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    return read_scalars(h);
+}
+
+extern "C" int dyn_sys_get_energies(dyn_sys_t h, dyn_energies_t* out) {
+    DYN_CHECK(h && out, DYN_ERR_INVALID, "dyn_sys_get_energies: NULL argument");
+    int rc = read_scalars(h);
+    BoxDev bx;
+    DYN_CUDA(cudaMemcpy(&bx, h->v.box, sizeof(BoxDev), cudaMemcpyDeviceToHost));
+    fill_energies(h, out);
+    for (int k = 0; k < 3; ++k) out->box[k] = bx.ext[k];
+    return rc;
+}
+
+extern "C" int dyn_sys_forces(dyn_sys_t h, double* f_atoms, double* f_water, dyn_energies_t* energies) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_forces: NULL handle");
+    const SysView& v = h->v;
+    enqueue_forces(h, false);
+    DYN_CUDA(cudaGetLastError());
+    int rc = read_scalars(h);
+    if (rc) return rc;
+    if (f_atoms && v.na) {
+        std::vector<long long> a(3 * (size_t)v.na), r(3 * (size_t)v.na);
+        DYN_CUDA(cudaMemcpy(a.data(), v.aforce, a.size() * 8, cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(r.data(), v.arecip, r.size() * 8, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < a.size(); ++k) f_atoms[k] = (double)(a[k] + r[k]) * DYN_FIX_INV;
+    }
+    if (f_water && v.nw) {
+        std::vector<long long> f(12 * (size_t)v.nw_cap), r(9 * (size_t)v.nw);
+        std::vector<uint32_t> wid(v.nw_cap);
+        DYN_CUDA(cudaMemcpy(f.data(), v.wforce, f.size() * 8, cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(r.data(), v.wrecip, r.size() * 8, cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(wid.data(), v.wid, wid.size() * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t s = 0; s < v.nw_cap; ++s) {
+            const uint32_t id = wid[s];
+            if (id == INVALID_ID) continue;
+            // sites O, H0, H1, M; the cache holds H0, H1, M
+            for (int c = 0; c < 12; ++c) {
+                long long x = f[12 * (size_t)s + c];
+                if (c >= 3) x += r[9 * (size_t)id + (c - 3)];
+                f_water[12 * (size_t)id + c] = (double)x * DYN_FIX_INV;
+            }
+        }
+    }
+    if (energies) {
+        BoxDev bx;
+        DYN_CUDA(cudaMemcpy(&bx, v.box, sizeof(BoxDev), cudaMemcpyDeviceToHost));
+        fill_energies(h, energies);
+        for (int k = 0; k < 3; ++k) energies->box[k] = bx.ext[k];
+    }
+    return DYN_OK;
+}
+
+extern "C" int dyn_sys_get_state(dyn_sys_t h, float* atom_pos, float* atom_vel, float* water_pos,
+                                 float* water_vel, float* water_m) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_get_state: NULL handle");
+    const SysView& v = h->v;
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    if (v.na && (atom_pos || atom_vel)) {
+        std::vector<float4> p(v.na), w(v.na);
+        DYN_CUDA(cudaMemcpy(p.data(), v.apos, v.na * sizeof(float4), cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(w.data(), v.avel, v.na * sizeof(float4), cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < v.na; ++i) {
+            if (atom_pos) { atom_pos[3 * i] = p[i].x; atom_pos[3 * i + 1] = p[i].y; atom_pos[3 * i + 2] = p[i].z; }
+            if (atom_vel) { atom_vel[3 * i] = w[i].x; atom_vel[3 * i + 1] = w[i].y; atom_vel[3 * i + 2] = w[i].z; }
+        }
+    }
+    if (v.nw && (water_pos || water_vel || water_m)) {
+        std::vector<float4> p(4 * (size_t)v.nw_cap), w(3 * (size_t)v.nw_cap);
+        std::vector<uint32_t> wid(v.nw_cap);
+        DYN_CUDA(cudaMemcpy(p.data(), v.wpos, p.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(w.data(), v.wvel, w.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(wid.data(), v.wid, wid.size() * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t s = 0; s < v.nw_cap; ++s) {
+            const uint32_t id = wid[s];
+            if (id == INVALID_ID) continue;
+            for (int k = 0; k < 3; ++k) {
+                const float4 a = p[4 * (size_t)s + k], b = w[3 * (size_t)s + k];
+                if (water_pos) { water_pos[9 * (size_t)id + 3 * k] = a.x; water_pos[9 * (size_t)id + 3 * k + 1] = a.y; water_pos[9 * (size_t)id + 3 * k + 2] = a.z; }
+                if (water_vel) { water_vel[9 * (size_t)id + 3 * k] = b.x; water_vel[9 * (size_t)id + 3 * k + 1] = b.y; water_vel[9 * (size_t)id + 3 * k + 2] = b.z; }
+            }
+            if (water_m) {
+                const float4 m = p[4 * (size_t)s + 3];
+                water_m[3 * (size_t)id] = m.x; water_m[3 * (size_t)id + 1] = m.y; water_m[3 * (size_t)id + 2] = m.z;
+            }
+        }
+    }
+    return DYN_OK;
+}
+
+extern "C" int dyn_sys_set_state(dyn_sys_t h, const float* atom_pos, const float* atom_vel,
+                                 const float* water_pos, const float* water_vel) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_set_state: NULL handle");
+    SysView& v = h->v;
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    if (v.na && (atom_pos || atom_vel)) {
+        std::vector<float4> p(v.na), w(v.na);
+        DYN_CUDA(cudaMemcpy(p.data(), v.apos, v.na * sizeof(float4), cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(w.data(), v.avel, v.na * sizeof(float4), cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < v.na; ++i) {
+            if (atom_pos) { p[i].x = atom_pos[3 * i]; p[i].y = atom_pos[3 * i + 1]; p[i].z = atom_pos[3 * i + 2]; }
+            if (atom_vel) { w[i].x = atom_vel[3 * i]; w[i].y = atom_vel[3 * i + 1]; w[i].z = atom_vel[3 * i + 2]; }
+        }
+        DYN_CUDA(cudaMemcpy(v.apos, p.data(), v.na * sizeof(float4), cudaMemcpyHostToDevice));
+        DYN_CUDA(cudaMemcpy(v.avel, w.data(), v.na * sizeof(float4), cudaMemcpyHostToDevice));
+    }
+    if (v.nw && (water_pos || water_vel)) {
+        std::vector<float4> p(4 * (size_t)v.nw_cap), w(3 * (size_t)v.nw_cap);
+        std::vector<uint32_t> wid(v.nw_cap);
+        DYN_CUDA(cudaMemcpy(p.data(), v.wpos, p.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(w.data(), v.wvel, w.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+        DYN_CUDA(cudaMemcpy(wid.data(), v.wid, wid.size() * 4, cudaMemcpyDeviceToHost));
+        const float q[4] = {0.f, OPC_Q_H, OPC_Q_H, OPC_Q_EP};
+        for (uint32_t s = 0; s < v.nw_cap; ++s) {
+            const uint32_t id = wid[s];
+            if (id == INVALID_ID) continue;
+            if (water_pos) {
+                const float* x = water_pos + 9 * (size_t)id;
+                float m[3];
+                host_m_site(x, x + 3, x + 6, m);
+                for (int k = 0; k < 3; ++k) p[4 * (size_t)s + k] = make_float4(x[3 * k], x[3 * k + 1], x[3 * k + 2], q[k]);
+                p[4 * (size_t)s + 3] = make_float4(m[0], m[1], m[2], q[3]);
+            }
+            if (water_vel) {
+                const float* x = water_vel + 9 * (size_t)id;
+                for (int k = 0; k < 3; ++k) w[3 * (size_t)s + k] = make_float4(x[3 * k], x[3 * k + 1], x[3 * k + 2], 0.f);
+            }
+        }
+        DYN_CUDA(cudaMemcpy(v.wpos, p.data(), p.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        DYN_CUDA(cudaMemcpy(v.wvel, w.data(), w.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    }
+    // new coordinates: rebuild lists and re-prime forces/accelerations
+    enqueue_forces(h, true);
+    DYN_CUDA(cudaGetLastError());
+    return read_scalars(h);
+}
+
+// Home-order staging for the host-step path: water (pos, vel) as [nw*9]
+// floats each; kernels scatter into / gather from the cluster-ordered slots.
+__global__ void k_stage_in(SysView v, const float* __restrict__ wp, const float* __restrict__ wv) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+        const uint32_t id = v.wid[s];
+        if (id == INVALID_ID) continue;
+        if (wp) {
+            const float* x = wp + 9 * (size_t)id;
+            const float3 o = f3(x[0], x[1], x[2]), h0 = f3(x[3], x[4], x[5]), h1 = f3(x[6], x[7], x[8]);
+            const float3 bis = (h0 - o) + (h1 - o);
+            const float3 m = o + bis * (OPC_O_EP_R * rsqrtf(dot3(bis, bis)));
+            v.wpos[4 * s + 0] = make_float4(o.x, o.y, o.z, 0.f);
+            v.wpos[4 * s + 1] = make_float4(h0.x, h0.y, h0.z, OPC_Q_H);
+            v.wpos[4 * s + 2] = make_float4(h1.x, h1.y, h1.z, OPC_Q_H);
+            v.wpos[4 * s + 3] = make_float4(m.x, m.y, m.z, OPC_Q_EP);
+        }
+        if (wv) {
+            const float* x = wv + 9 * (size_t)id;
+            for (int k = 0; k < 3; ++k) v.wvel[3 * s + k] = make_float4(x[3 * k], x[3 * k + 1], x[3 * k + 2], 0.f);
+        }
+    }
+}
+
+__global__ void k_stage_out(SysView v, float* __restrict__ wp, float* __restrict__ wv) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+        const uint32_t id = v.wid[s];
+        if (id == INVALID_ID) continue;
+        for (int k = 0; k < 3; ++k) {
+            if (wp) {
+                const float4 a = v.wpos[4 * s + k];
+                wp[9 * (size_t)id + 3 * k] = a.x; wp[9 * (size_t)id + 3 * k + 1] = a.y; wp[9 * (size_t)id + 3 * k + 2] = a.z;
+            }
+            if (wv) {
+                const float4 b = v.wvel[3 * s + k];
+                wv[9 * (size_t)id + 3 * k] = b.x; wv[9 * (size_t)id + 3 * k + 1] = b.y; wv[9 * (size_t)id + 3 * k + 2] = b.z;
+            }
+        }
+    }
+}
+
+__global__ void k_atoms_in(SysView v, const float* __restrict__ ap, const float* __restrict__ av) {
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+        if (ap) { float4 p = v.apos[a]; p.x = ap[3 * a]; p.y = ap[3 * a + 1]; p.z = ap[3 * a + 2]; v.apos[a] = p; }
+        if (av) v.avel[a] = make_float4(av[3 * a], av[3 * a + 1], av[3 * a + 2], 0.f);
+    }
+}
+
+__global__ void k_atoms_out(SysView v, float* __restrict__ ap, float* __restrict__ av) {
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+        const float4 p = v.apos[a], w = v.avel[a];
+        if (ap) { ap[3 * a] = p.x; ap[3 * a + 1] = p.y; ap[3 * a + 2] = p.z; }
+        if (av) { av[3 * a] = w.x; av[3 * a + 1] = w.y; av[3 * a + 2] = w.z; }
+    }
+}
+
+namespace {
+
+struct HostStage {
+    float* d = nullptr;   // [4 * (na*3 + nw*9)] device staging
+    size_t n = 0;
+};
+
+int ensure_stage(dyn_sys_s* h, HostStage& hs) {
+    const size_t need = 2 * (3 * (size_t)h->v.na) + 2 * (9 * (size_t)h->v.nw);
+    if (hs.d && hs.n >= need) return DYN_OK;
+    if (hs.d) cudaFree(hs.d);
+    DYN_CUDA(cudaMalloc(&hs.d, std::max<size_t>(need, 1) * sizeof(float)));
+    h->allocs.push_back(hs.d);
+    hs.n = need;
+    return DYN_OK;
+}
+
+HostStage& stage_of(dyn_sys_s* h) {
+    static thread_local std::vector<std::pair<dyn_sys_s*, HostStage>> tbl;
+    for (auto& e : tbl)
+        if (e.first == h) return e.second;
+    tbl.push_back({h, HostStage{}});
+    return tbl.back().second;
+}
+
+int count_graph_kernels(cudaGraph_t g, uint32_t* n) {
+    size_t cnt = 0;
+    DYN_CUDA(cudaGraphGetNodes(g, nullptr, &cnt));
+    std::vector<cudaGraphNode_t> nodes(cnt);
+    DYN_CUDA(cudaGraphGetNodes(g, nodes.data(), &cnt));
+    uint32_t k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        DYN_CUDA(cudaGraphNodeGetType(nd, &t));
+        if (t == cudaGraphNodeTypeKernel) ++k;
+    }
+    *n = k;
+    return DYN_OK;
+}
+
+}  // namespace
+
+extern "C" int dyn_sys_step_host(dyn_sys_t h, uint32_t n_steps, float dt, const float* atom_pos_in,
+                                 const float* atom_vel_in, const float* water_pos_in,
+                                 const float* water_vel_in, float* atom_pos_out, float* atom_vel_out,
+                                 float* water_pos_out, float* water_vel_out, dyn_energies_t* energies) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_step_host: NULL handle");
+    SysView& v = h->v;
+    HostStage& hs = stage_of(h);
+    int rc = ensure_stage(h, hs);
+    if (rc) return rc;
+    float* d_ap = hs.d;
+    float* d_av = d_ap + 3 * (size_t)v.na;
+    float* d_wp = d_av + 3 * (size_t)v.na;
+    float* d_wv = d_wp + 9 * (size_t)v.nw;
+    cudaStream_t st = h->stream;
+    const int nbw = std::max(1u, std::min(v.max_blocks, (v.nw_cap + 255) / 256));
+    const int nba = std::max(1u, std::min(v.max_blocks, (v.na + 255) / 256));
+    if (v.na && (atom_pos_in || atom_vel_in)) {
+        if (atom_pos_in) DYN_CUDA(cudaMemcpyAsync(d_ap, atom_pos_in, 12 * (size_t)v.na, cudaMemcpyHostToDevice, st));
+        if (atom_vel_in) DYN_CUDA(cudaMemcpyAsync(d_av, atom_vel_in, 12 * (size_t)v.na, cudaMemcpyHostToDevice, st));
+        k_atoms_in<<<nba, 256, 0, st>>>(v, atom_pos_in ? d_ap : nullptr, atom_vel_in ? d_av : nullptr);
+    }
+    if (v.nw && (water_pos_in || water_vel_in)) {
+        if (water_pos_in) DYN_CUDA(cudaMemcpyAsync(d_wp, water_pos_in, 36 * (size_t)v.nw, cudaMemcpyHostToDevice, st));
+        if (water_vel_in) DYN_CUDA(cudaMemcpyAsync(d_wv, water_vel_in, 36 * (size_t)v.nw, cudaMemcpyHostToDevice, st));
+        k_stage_in<<<nbw, 256, 0, st>>>(v, water_pos_in ? d_wp : nullptr, water_vel_in ? d_wv : nullptr);
+    }
+    DYN_CUDA(cudaGetLastError());
+    rc = dyn_sys_step(h, n_steps, dt);
+    if (rc) return rc;
+    if (v.na && (atom_pos_out || atom_vel_out)) {
+        k_atoms_out<<<nba, 256, 0, st>>>(v, d_ap, d_av);
+        if (atom_pos_out) DYN_CUDA(cudaMemcpyAsync(atom_pos_out, d_ap, 12 * (size_t)v.na, cudaMemcpyDeviceToHost, st));
+        if (atom_vel_out) DYN_CUDA(cudaMemcpyAsync(atom_vel_out, d_av, 12 * (size_t)v.na, cudaMemcpyDeviceToHost, st));
+    }
+    if (v.nw && (water_pos_out || water_vel_out)) {
+        k_stage_out<<<nbw, 256, 0, st>>>(v, d_wp, d_wv);
+        if (water_pos_out) DYN_CUDA(cudaMemcpyAsync(water_pos_out, d_wp, 36 * (size_t)v.nw, cudaMemcpyDeviceToHost, st));
+        if (water_vel_out) DYN_CUDA(cudaMemcpyAsync(water_vel_out, d_wv, 36 * (size_t)v.nw, cudaMemcpyDeviceToHost, st));
+    }
+    DYN_CUDA(cudaGetLastError());
+    DYN_CUDA(cudaMemcpyAsync(h->h_sc, v.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+    DYN_CUDA(cudaStreamSynchronize(st));
+    if (energies) {
+        fill_energies(h, energies);
+    }
+    if (h->h_sc->nonfinite) return dyn::fail(DYN_ERR_NONFINITE, "non-finite coordinates or forces");
+    if (h->h_sc->overflow) return dyn::fail(DYN_ERR_UNSUPPORTED, "cluster list capacity exceeded");
+    return DYN_OK;
+}
+
+extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, double* ms) {
+    DYN_CHECK(h && ms, DYN_ERR_INVALID, "dyn_sys_stage_times: NULL argument");
+    DYN_CHECK(dt > 0.f, DYN_ERR_INVALID, "dyn_sys_stage_times: dt must be > 0");
+    const SysView& v = h->v;
+    cudaStream_t st = h->stream;
+    cudaEvent_t ev[7];
+    for (int i = 0; i < 7; ++i) DYN_CUDA(cudaEventCreate(&ev[i]));
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t n_spme = 0;
+    const uint32_t e_int = std::max(1u, h->cfg.energy_interval);
+    for (uint32_t i = 0; i < n_steps; ++i) {
+        const uint64_t s = h->host_step;
+        const bool spme = (s % v.spme_interval) == 0;
+        const bool energy = ((s + 1) % e_int) == 0;
+        cudaEventRecord(ev[0], st);
+        dyn::launch_first_half(v, st, dt);
+        cudaEventRecord(ev[1], st);
+        dyn::launch_displacement_check(v, st);
+        dyn::launch_rebuild(v, st, false);
+        cudaEventRecord(ev[2], st);
+        dyn::launch_gather_atoms(v, st);
+        dyn::launch_pairs(v, st, energy);
+        cudaEventRecord(ev[3], st);
+        dyn::launch_pair14(v, st, energy);
+        dyn::launch_bonded(v, st, energy);
+        cudaEventRecord(ev[4], st);
+        if (spme) {
+            dyn::launch_pme(v, st, h->plan_f, h->plan_b);
+            dyn::launch_corrections(v, st);
+        }
+        cudaEventRecord(ev[5], st);
+        dyn::launch_second_half(v, st, dt);
+        dyn::launch_finalize(v, st, dt, energy, true);
+        dyn::launch_periodic(v, st);
+        dyn::launch_step_end(v, st);
+        cudaEventRecord(ev[6], st);
+        DYN_CUDA(cudaGetLastError());
+        DYN_CUDA(cudaEventSynchronize(ev[6]));
+        for (int k = 0; k < 6; ++k) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            acc[k] += t;
+        }
+        n_spme += spme ? 1u : 0u;
+        h->host_step += 1;
+    }
+    for (int i = 0; i < 7; ++i) cudaEventDestroy(ev[i]);
+    for (int k = 0; k < 6; ++k) ms[k] = n_steps ? acc[k] / n_steps : 0.0;
+    ms[4] = n_spme ? acc[4] / n_spme : 0.0;
+    return read_scalars(h);
+}
+
+extern "C" int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out) {
+    DYN_CHECK(h && out, DYN_ERR_INVALID, "dyn_sys_launches_per_step: NULL argument");
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    cudaGraph_t g = nullptr, gf = nullptr;
+    DYN_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(h, 0.002f, spme != 0, true);
+    DYN_CUDA(cudaStreamEndCapture(h->stream, &g));
+    uint32_t total = 0, fft = 0;
+    int rc = count_graph_kernels(g, &total);
+    cudaGraphDestroy(g);
+    if (rc) return rc;
+    if (spme) {
+        DYN_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        cufftExecR2C(h->plan_f, h->v.qgrid, (cufftComplex*)h->v.cgrid);
+        cufftExecC2R(h->plan_b, (cufftComplex*)h->v.cgrid, h->v.qgrid);
+        DYN_CUDA(cudaStreamEndCapture(h->stream, &gf));
+        rc = count_graph_kernels(gf, &fft);
+        cudaGraphDestroy(gf);
+        if (rc) return rc;
+    }
+    *out = total - fft;
+    return DYN_OK;
+}

@@ -1,0 +1,308 @@
+"""Python mirror of the reference's public simulation API (MdState, MdConfig).
+
+The reference drives a simulation with ``MdState::new(dev, &MdConfig, ..)``
+and ``MdState::step(dev, dt, external_force)`` (src/lib.rs:711,
+src/integrate.rs:72).  Here ``MdState(system, MdConfig)`` uploads a system
+once and ``step(dt, n)`` advances it on the device through the C ABI
+(dyn_sys_*); coordinates, velocities, lists and PME grids stay in HBM.
+
+``system`` is a dict of numpy arrays (see dynamics_b200.synth):
+  box_lo, box_hi (3,); water_pos, water_vel (n_water, 3, 3) [O, H0, H1];
+  atom_pos, atom_vel (n, 3); atom_mass, atom_q, atom_sigma, atom_eps (n,);
+  atom_static (n,) optional; excl, pair14 (m, 2); bonds (m, 2) + bond_k,
+  bond_r0; angles (m, 3) + angle_k, angle_theta0; dihedrals (m, 4) +
+  dihedral_k, dihedral_n, dihedral_phase.
+"""
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, f32, lib, ptr, u8, u32
+
+
+@dataclass
+class LangevinMiddle:
+    """Integrator::LangevinMiddle { gamma } (src/integrate.rs:43)."""
+    gamma: float = 0.5  # LANGEVIN_GAMMA_DEFAULT, src/thermostat.rs:32
+
+
+@dataclass
+class VerletVelocity:
+    """Integrator::VerletVelocity { thermostat } (src/integrate.rs:39);
+    ``thermostat`` is the CSVR time constant in ps, or None."""
+    thermostat: Optional[float] = 0.1  # TAU_TEMP_DEFAULT, src/thermostat.rs:27
+
+
+@dataclass
+class BarostatCfg:
+    """BarostatCfg (src/barostat.rs:32-50): C-rescale."""
+    pressure_target: float = 1.0
+    tau: float = 5.0
+    solvent_compressibility: float = 4.5e-5
+
+
+@dataclass
+class MdConfig:
+    """The fields of MdConfig (src/config.rs:43-107) this engine uses.
+
+    ``neighbor_skin`` is the Verlet buffer of the cluster lists (the
+    reference's default of 4 A sizes its flat lists; the cluster lists need
+    far less, and results do not depend on it).  ``spme_grid`` replaces
+    ``spme_mesh_spacing``: the grid is given explicitly.
+    """
+    integrator: object = field(default_factory=LangevinMiddle)
+    temp_target: float = 300.0
+    coulomb_cutoff: float = 10.0
+    lj_cutoff: float = 10.0
+    neighbor_skin: float = 1.5
+    spme_alpha: float = 0.26
+    spme_grid: tuple = (32, 32, 32)
+    barostat_cfg: Optional[BarostatCfg] = None
+    zero_com_drift: bool = True
+    com_removal_interval: int = 100
+    recenter_sim_box: bool = True
+    spme_interval: int = 2          # SPME_RATIO, src/lib.rs:208
+    energy_interval: int = 1
+    ewald_corrections: bool = False
+    full_energy: bool = False
+    reset_angle: bool = True
+    seed: int = 0
+
+
+def thermo_dof(system, cfg):
+    """dof_for_thermo (src/thermostat.rs:220-251)."""
+    nw = len(np.asarray(system.get("water_pos", np.zeros((0, 3, 3)))).reshape(-1, 3, 3))
+    na = len(np.asarray(system.get("atom_pos", np.zeros((0, 3)))).reshape(-1, 3))
+    st = np.asarray(system.get("atom_static", np.zeros(na, bool)), dtype=bool)
+    dof = 6 * nw + 3 * int(np.count_nonzero(~st))
+    dof -= len(np.asarray(system.get("constraints", np.zeros((0, 2)))).reshape(-1, 2))
+    if cfg.zero_com_drift:
+        dof -= 3
+    return max(dof, 0)
+
+
+def _config_struct(system, cfg):
+    c = _lib.Config()
+    lo = f32(system["box_lo"], 3)
+    hi = f32(system["box_hi"], 3)
+    for k in range(3):
+        c.box_lo[k] = lo[k]
+        c.box_hi[k] = hi[k]
+        c.grid[k] = int(cfg.spme_grid[k])
+    c.coulomb_cutoff = cfg.coulomb_cutoff
+    c.lj_cutoff = cfg.lj_cutoff
+    c.list_buffer = cfg.neighbor_skin
+    c.ewald_alpha = cfg.spme_alpha
+    integ = cfg.integrator
+    if isinstance(integ, LangevinMiddle):
+        c.integrator = _lib.DYN_INTEGRATOR_LANGEVIN_MIDDLE
+        c.langevin_gamma = integ.gamma
+    elif isinstance(integ, VerletVelocity):
+        c.integrator = _lib.DYN_INTEGRATOR_VERLET_VELOCITY
+        c.thermostat = _lib.DYN_THERMO_CSVR if integ.thermostat else _lib.DYN_THERMO_NONE
+        c.tau_temp = float(integ.thermostat or 0.0)
+    else:
+        raise _lib.DynError(_lib.DYN_ERR_INVALID, f"unsupported integrator {integ!r}")
+    if cfg.barostat_cfg is not None:
+        c.barostat = _lib.DYN_BARO_CRESCALE
+        c.pressure_bar = cfg.barostat_cfg.pressure_target
+        c.tau_pressure = cfg.barostat_cfg.tau
+        c.compressibility = cfg.barostat_cfg.solvent_compressibility
+    c.temperature = cfg.temp_target
+    c.spme_interval = max(1, int(cfg.spme_interval))
+    c.com_interval = int(cfg.com_removal_interval)
+    c.recenter_interval = 30  # CENTER_SIMBOX_RATIO, src/lib.rs:204
+    c.energy_interval = max(1, int(cfg.energy_interval))
+    flags = 0
+    if cfg.ewald_corrections:
+        flags |= _lib.DYN_FLAG_EWALD_CORRECTIONS
+    if cfg.full_energy:
+        flags |= _lib.DYN_FLAG_FULL_ENERGY
+    if cfg.zero_com_drift:
+        flags |= _lib.DYN_FLAG_COM_REMOVAL
+    if cfg.recenter_sim_box:
+        flags |= _lib.DYN_FLAG_RECENTER
+    if cfg.reset_angle:
+        flags |= _lib.DYN_FLAG_RESET_ANGLE
+    c.flags = flags
+    c.thermo_dof = thermo_dof(system, cfg)
+    c.seed = int(cfg.seed) & 0xFFFFFFFFFFFFFFFF
+    return c
+
+
+class MdState:
+    """A device-resident simulation (MdState, src/lib.rs:610-705)."""
+
+    def __init__(self, system, cfg=None, stream=None):
+        self.cfg = cfg or MdConfig()
+        self.system = system
+        wp = f32(system.get("water_pos", np.zeros((0, 3, 3)))).reshape(-1, 9)
+        wv = f32(system.get("water_vel", np.zeros_like(wp))).reshape(-1, 9)
+        ap = f32(system.get("atom_pos", np.zeros((0, 3)))).reshape(-1, 3)
+        na = len(ap)
+        self.n_water = len(wp)
+        self.n_atoms = na
+        keep = {}
+
+        def arr(name, conv, shape=None, default=None):
+            if name not in system or system[name] is None or len(system[name]) == 0:
+                return None
+            a = conv(system[name])
+            if shape is not None:
+                a = a.reshape(shape)
+            keep[name] = a
+            return a
+
+        d = _lib.SystemDesc()
+        d.n_atoms = na
+        d.atom_pos = ptr(arr("atom_pos", f32, -1))
+        d.atom_vel = ptr(arr("atom_vel", f32, -1))
+        d.atom_mass = ptr(arr("atom_mass", f32))
+        d.atom_q = ptr(arr("atom_q", f32))
+        d.atom_sigma = ptr(arr("atom_sigma", f32))
+        d.atom_eps = ptr(arr("atom_eps", f32))
+        d.atom_static = ptr(arr("atom_static", u8))
+        d.n_water = self.n_water
+        keep["wp"] = np.ascontiguousarray(wp)
+        keep["wv"] = np.ascontiguousarray(wv)
+        d.water_pos = ptr(keep["wp"]) if self.n_water else None
+        d.water_vel = ptr(keep["wv"]) if self.n_water else None
+        for name, width, pfx in (("excl", 2, None), ("pair14", 2, None)):
+            a = arr(name, u32, -1)
+            setattr(d, "n_" + name, 0 if a is None else len(a) // width)
+            setattr(d, name, ptr(a))
+        b = arr("bonds", u32, -1)
+        d.n_bonds = 0 if b is None else len(b) // 2
+        d.bonds = ptr(b)
+        d.bond_k = ptr(arr("bond_k", f32))
+        d.bond_r0 = ptr(arr("bond_r0", f32))
+        a = arr("angles", u32, -1)
+        d.n_angles = 0 if a is None else len(a) // 3
+        d.angles = ptr(a)
+        d.angle_k = ptr(arr("angle_k", f32))
+        d.angle_theta0 = ptr(arr("angle_theta0", f32))
+        dh = arr("dihedrals", u32, -1)
+        d.n_dihedrals = 0 if dh is None else len(dh) // 4
+        d.dihedrals = ptr(dh)
+        d.dihedral_k = ptr(arr("dihedral_k", f32))
+        d.dihedral_n = ptr(arr("dihedral_n", f32))
+        d.dihedral_phase = ptr(arr("dihedral_phase", f32))
+        cn = arr("constraints", u32, -1)
+        d.n_constraints = 0 if cn is None else len(cn) // 2
+        d.constraints = ptr(cn)
+        d.constraint_r0 = ptr(arr("constraint_r0", f32))
+        c = _config_struct(system, self.cfg)
+        h = C.c_void_p()
+        check(lib().dyn_sys_create(stream, C.byref(c), C.byref(d), C.byref(h)))
+        self._h = h
+        self._cstruct = c
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise _lib.DynError(_lib.DYN_ERR_INVALID, "MdState already closed")
+        return self._h
+
+    def step(self, dt, n_steps=1):
+        """Advance n_steps of dt ps (asynchronous; see sync())."""
+        check(lib().dyn_sys_step(self.handle, int(n_steps), float(dt)))
+
+    def sync(self):
+        check(lib().dyn_sys_sync(self.handle))
+
+    def energies(self):
+        e = _lib.Energies()
+        check(lib().dyn_sys_get_energies(self.handle, C.byref(e)))
+        return e.as_dict()
+
+    def forces(self):
+        """One force evaluation (reset_f_acc_pe_virial + apply_all_forces,
+        src/lib.rs:1220-1348): dict with f_atoms (n,3), f_water (nw,4,3)
+        sites O, H0, H1, M, and the energies."""
+        fa = np.zeros((max(self.n_atoms, 1), 3))
+        fw = np.zeros((max(self.n_water, 1), 4, 3))
+        e = _lib.Energies()
+        check(lib().dyn_sys_forces(self.handle, ptr(fa), ptr(fw), C.byref(e)))
+        out = e.as_dict()
+        out["f_atoms"] = fa[:self.n_atoms]
+        out["f_water"] = fw[:self.n_water]
+        return out
+
+    def state(self):
+        na, nw = self.n_atoms, self.n_water
+        ap = np.zeros((max(na, 1), 3), np.float32)
+        av = np.zeros((max(na, 1), 3), np.float32)
+        wp = np.zeros((max(nw, 1), 3, 3), np.float32)
+        wv = np.zeros((max(nw, 1), 3, 3), np.float32)
+        wm = np.zeros((max(nw, 1), 3), np.float32)
+        check(lib().dyn_sys_get_state(self.handle, ptr(ap), ptr(av), ptr(wp), ptr(wv), ptr(wm)))
+        return {"atom_pos": ap[:na], "atom_vel": av[:na], "water_pos": wp[:nw],
+                "water_vel": wv[:nw], "water_m": wm[:nw]}
+
+    def step_host(self, dt, n_steps, inputs, outputs):
+        """dyn_sys_step_host: host buffers in, n steps, host buffers out.
+
+        ``inputs`` / ``outputs``: dicts with optional atom_pos, atom_vel,
+        water_pos, water_vel float32 arrays (home order; page-locked for full
+        bandwidth).  Returns the energies dict."""
+        keys = ("atom_pos", "atom_vel", "water_pos", "water_vel")
+        e = _lib.Energies()
+        check(lib().dyn_sys_step_host(self.handle, int(n_steps), float(dt),
+                                      *[ptr(inputs.get(k)) for k in keys],
+                                      *[ptr(outputs.get(k)) for k in keys], C.byref(e)))
+        return e.as_dict()
+
+    STAGES = ("first_half", "list", "pairs", "bonded", "spme", "kick_finalize")
+
+    def stage_times(self, dt, n_steps):
+        """Mean ms per step of each stage, timed with CUDA events."""
+        ms = np.zeros(6)
+        check(lib().dyn_sys_stage_times(self.handle, int(n_steps), float(dt), ptr(ms)))
+        return dict(zip(self.STAGES, ms.tolist()))
+
+    def launches_per_step(self, spme=True):
+        n = C.c_uint32()
+        check(lib().dyn_sys_launches_per_step(self.handle, 1 if spme else 0, C.byref(n)))
+        return n.value
+
+    def set_state(self, atom_pos=None, atom_vel=None, water_pos=None, water_vel=None):
+        conv = [None if x is None else f32(x).reshape(-1) for x in (atom_pos, atom_vel, water_pos, water_vel)]
+        check(lib().dyn_sys_set_state(self.handle, *[ptr(x) for x in conv]))
+
+    def close(self):
+        if self._h is not None:
+            lib().dyn_sys_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def equilibrate(system, cfg, n_steps=1000, dt=0.001, gamma=50.0):
+    """Relax a freshly generated system with strongly damped Langevin
+    dynamics on the device and return a copy with the new positions and
+    velocities.  Plays the role of the reference's start-up relaxation
+    (minimize_energy and the solvent-only MD of MdState::new,
+    src/lib.rs:1106-1112) for synthetic inputs."""
+    import copy
+    c = copy.deepcopy(cfg)
+    c.integrator = LangevinMiddle(gamma=gamma)
+    c.spme_interval = 1
+    c.energy_interval = max(1, n_steps)
+    st = MdState(system, c)
+    st.step(dt, n_steps)
+    s = st.state()
+    st.close()
+    out = dict(system)
+    out["water_pos"] = s["water_pos"]
+    out["water_vel"] = s["water_vel"]
+    if len(s["atom_pos"]):
+        out["atom_pos"] = s["atom_pos"]
+        out["atom_vel"] = s["atom_vel"]
+    return out

@@ -1,0 +1,333 @@
+/*
+ * dynb200 -- B200-native (sm_100a) nonbonded force and integration engine
+ * for the molecular-dynamics library David-OConnor/dynamics (crate
+ * `dynamics` 0.2.2).  This header is the whole drop-in boundary: a plain
+ * C ABI (opaque handles, pointers and sizes, int status codes) that a Rust
+ * `extern "C"` block, ctypes or C++ can bind.
+ *
+ * Two layers:
+ *
+ *  1. dyn_nb_*  -- one-to-one replacement of src/gpu_interface.rs.  The
+ *     caller keeps the simulation state on the host, exactly like the
+ *     reference's MdState, and asks the GPU for the short-range forces of a
+ *     flat pair list each step.  dyn_nb_build_pairs additionally replaces
+ *     build_all_neighbors + setup_pairs (src/neighbors.rs:102-156,
+ *     src/non_bonded.rs:541-677) with a GPU cell-list build whose pair set is
+ *     bit-identical to the reference's brute-force lists.
+ *
+ *  2. dyn_sys_*  -- the native, device-resident engine behind
+ *     MdState::step (src/integrate.rs:72): positions, velocities, neighbour
+ *     cluster lists and PME grids stay in HBM; one call advances n steps.
+ *
+ * Conventions (both layers):
+ *  - Every call returns DYN_OK (0) or a negative DYN_ERR_* code and never
+ *    aborts the process.  dyn_last_error() returns a message for the last
+ *    failure on the calling thread.
+ *  - Handles are opaque.  One handle = one CUDA stream; a handle is not
+ *    thread-safe, distinct handles may be used from distinct threads.
+ *  - Caller-owned host buffers are only read/written during the call.
+ *    Device memory is owned by the library and released by *_destroy.
+ *  - Units: Angstrom, ps, amu, kcal/mol.  Charges are pre-scaled by
+ *    18.2223 = sqrt(332.0522) as in the reference (src/non_bonded.rs:58-63).
+ *  - Streams are passed as `void*` holding a cudaStream_t (NULL = legacy
+ *    default stream).
+ */
+#ifndef DYNB200_H
+#define DYNB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DYN_OK 0
+#define DYN_ERR_INVALID (-1)    /* bad argument, size or call order        */
+#define DYN_ERR_CUDA (-2)       /* a CUDA runtime / cuFFT call failed      */
+#define DYN_ERR_OOM (-3)        /* device or pinned allocation failed      */
+#define DYN_ERR_NONFINITE (-5)  /* NaN/Inf detected in coordinates/forces  */
+#define DYN_ERR_TIMEOUT (-6)    /* a bounded device wait gave up           */
+#define DYN_ERR_UNSUPPORTED (-7)/* feature not available for this system  */
+
+/* ------------------------------------------------------------------ */
+/* errors / version                                                    */
+/* ------------------------------------------------------------------ */
+
+/* Message describing the last failed call on this thread ("" if none). */
+const char* dyn_last_error(void);
+/* Library version, e.g. 1 */
+int dyn_version(void);
+/* Number of CUDA devices visible; 0 without a GPU (never fails). */
+int dyn_device_count(void);
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (best of 5
+ * launches of an FMA-chain kernel over all SMs); the roofline denominator
+ * for the FP32 pair kernels. */
+int dyn_probe_fp32_peak(void* stream, double* tflops);
+
+/* ------------------------------------------------------------------ */
+/* Layer 1: gpu_interface.rs replacement                              */
+/* ------------------------------------------------------------------ */
+
+typedef struct dyn_nb_s* dyn_nb_t;
+
+/* Override bits, mirroring MdOverrides (src/lib.rs:590-607) as the pair
+ * kernel honours them (src/cuda/cuda.cu:229-230). */
+#define DYN_OVR_COULOMB_DISABLED 1u
+#define DYN_OVR_LJ_DISABLED 2u
+
+/* Pair flag bits for dyn_nb_set_pairs' packed flags array; one byte per
+ * pair replaces the reference's four bool arrays (scale_14s, calc_ljs,
+ * calc_coulombs, symmetric; src/gpu_interface.rs:233-237). */
+#define DYN_PAIR_SCALE14 1u
+#define DYN_PAIR_LJ 2u
+#define DYN_PAIR_COULOMB 4u
+#define DYN_PAIR_SYMMETRIC 8u
+
+/* Body codes, one byte per pair end: 0 = non-water atom, 1..4 = water site
+ * O, M, H0, H1 (the reference's atom_types_* + water_types_* arrays,
+ * src/gpu_interface.rs:269-279, WaterSite src/solvent/mod.rs:256-261). */
+#define DYN_BODY_ATOM 0u
+#define DYN_BODY_W_O 1u
+#define DYN_BODY_W_M 2u
+#define DYN_BODY_W_H0 3u
+#define DYN_BODY_W_H1 4u
+
+/* Replaces ForcesPositsGpu::new (src/gpu_interface.rs:123-214): device and
+ * pinned buffers for n_dyn atoms and n_water 4-site waters.
+ * lj_cutoff <= 0 reproduces the reference CUDA kernel (no LJ cutoff,
+ * src/cuda/cuda.cu:277-279); lj_cutoff > 0 reproduces the CPU path
+ * (LJ only for r <= lj_cutoff, src/non_bonded.rs:1001). */
+int dyn_nb_create(void* stream, uint32_t n_dyn, uint32_t n_water, float cutoff_ewald,
+                  float alpha_ewald, float lj_cutoff, dyn_nb_t* out);
+
+/* Replaces PerNeighborGpu::new (src/gpu_interface.rs:243-410): uploads the
+ * flat pair list.  tgt/src index the atom array (body 0) or the water
+ * molecule (bodies 1..4).  body_tgt/body_src: DYN_BODY_* per pair.
+ * flags: DYN_PAIR_* per pair.  The library re-packs these into its own
+ * 16-byte-per-pair layout. */
+int dyn_nb_set_pairs(dyn_nb_t h, uint64_t n_pairs, const uint32_t* tgt, const uint32_t* src,
+                     const float* sigma, const float* eps, const float* q_tgt,
+                     const float* q_src, const uint8_t* body_tgt, const uint8_t* body_src,
+                     const uint8_t* flags);
+
+/* Replaces build_all_neighbors + setup_pairs + PerNeighborGpu::new
+ * (src/neighbors.rs:102-156, src/non_bonded.rs:541-677,
+ * src/gpu_interface.rs:243-410) on the GPU.  Builds the three Verlet lists
+ * with |min_image(d)|^2 < (cutoff+skin)^2 in the reference's float32
+ * arithmetic (bit-identical pair set; water uses wrapped O positions), then
+ * the flat pair list in the reference's canonical order, and installs it as
+ * if by dyn_nb_set_pairs.
+ *   atom_*: n_dyn entries (positions [n_dyn*3]); is_static/bonded_only may be
+ *           NULL (all false).
+ *   excl / pair14: (i, j) index pairs, i < j, for 1-2/1-3 exclusions and
+ *           1-4 scaled pairs (src/prep.rs:114-143).
+ *   box_lo/box_hi: SimBox bounds (src/barostat.rs:56-61).
+ * n_pairs_out receives the flat pair count. */
+int dyn_nb_build_pairs(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o,
+                       const float* atom_q, const float* atom_sigma, const float* atom_eps,
+                       const uint8_t* is_static, const uint8_t* bonded_only,
+                       uint64_t n_excl, const uint32_t* excl, uint64_t n_pair14,
+                       const uint32_t* pair14, const float box_lo[3], const float box_hi[3],
+                       float skin, uint64_t* n_pairs_out);
+
+/* Copies the installed flat pair list back to the host (arrays of n_pairs
+ * entries, any of them may be NULL).  Used to check the pair set. */
+int dyn_nb_get_pairs(dyn_nb_t h, uint64_t n_pairs, uint32_t* tgt, uint32_t* src, float* sigma,
+                     float* eps, float* q_tgt, float* q_src, uint8_t* body_tgt,
+                     uint8_t* body_src, uint8_t* flags);
+
+/* Replaces force_nonbonded_gpu (src/gpu_interface.rs:463-632): uploads the
+ * positions (float [3*n] per array, as the reference's five position
+ * arrays), evaluates the installed pair list and returns forces on the
+ * target/source of every pair (float64 [3*n] arrays), the virial sum and
+ * the potential energy with the reference's conventions (energy only for
+ * pairs whose target is a non-water atom).  Forces are accumulated as
+ * 64-bit fixed point on the device, so repeated calls are bit-identical.
+ * cell_extent: SimBox extent (bounds_high - bounds_low). */
+int dyn_nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o, const float* pos_w_m,
+                  const float* pos_w_h0, const float* pos_w_h1, const float cell_extent[3],
+                  uint32_t override_bits, double* f_dyn, double* f_w_o, double* f_w_m,
+                  double* f_w_h0, double* f_w_h1, double* virial, double* energy);
+
+/* Releases everything dyn_nb_create allocated. */
+int dyn_nb_destroy(dyn_nb_t h);
+
+/* ------------------------------------------------------------------ */
+/* Layer 2: device-resident engine (MdState::step)                    */
+/* ------------------------------------------------------------------ */
+
+typedef struct dyn_sys_s* dyn_sys_t;
+
+/* Integrator (src/integrate.rs:32-44). */
+#define DYN_INTEGRATOR_LANGEVIN_MIDDLE 0u
+#define DYN_INTEGRATOR_VERLET_VELOCITY 1u
+
+/* Thermostat for the velocity-Verlet integrator (src/thermostat.rs:258). */
+#define DYN_THERMO_NONE 0u
+#define DYN_THERMO_CSVR 1u
+
+/* Barostat (src/barostat.rs:300-413). */
+#define DYN_BARO_NONE 0u
+#define DYN_BARO_CRESCALE 1u
+
+/* dyn_config_t.flags */
+/* Add the Ewald exclusion corrections (intra-water, 1-2/1-3 and 1-4 pairs)
+ * in float64.  Off = the reference's bookkeeping (no correction, plus its
+ * 1-4 vacuum force correction, src/non_bonded.rs:763-790). */
+#define DYN_FLAG_EWALD_CORRECTIONS 1u
+/* Count water-water short-range energy in the potential energy (the
+ * reference omits it, src/non_bonded.rs:335-342). */
+#define DYN_FLAG_FULL_ENERGY 2u
+/* Remove linear COM motion every com_interval steps (src/com_zero.rs:57). */
+#define DYN_FLAG_COM_REMOVAL 4u
+/* Recenter the box on the solute every recenter_interval steps
+ * (src/barostat.rs:111-137, src/integrate.rs:439-443). */
+#define DYN_FLAG_RECENTER 8u
+/* Re-establish the water geometry every 1000 steps
+ * (src/solvent/opc_settle.rs:202-219, src/integrate.rs:445-449). */
+#define DYN_FLAG_RESET_ANGLE 16u
+
+typedef struct {
+    float box_lo[3];
+    float box_hi[3];
+    float coulomb_cutoff;   /* MdConfig.coulomb_cutoff (src/config.rs:100)  */
+    float lj_cutoff;        /* MdConfig.lj_cutoff                           */
+    float list_buffer;      /* Verlet buffer of the cluster lists (A)       */
+    float ewald_alpha;      /* MdConfig.spme_alpha                          */
+    uint32_t grid[3];       /* SPME grid; spline order is 4                 */
+    uint32_t integrator;    /* DYN_INTEGRATOR_*                             */
+    uint32_t thermostat;    /* DYN_THERMO_* (velocity Verlet only)          */
+    uint32_t barostat;      /* DYN_BARO_*                                   */
+    float temperature;      /* K                                            */
+    float langevin_gamma;   /* 1/ps                                         */
+    float tau_temp;         /* ps (CSVR)                                    */
+    float pressure_bar;     /* C-rescale target                             */
+    float tau_pressure;     /* ps                                           */
+    float compressibility;  /* 1/bar                                        */
+    uint32_t spme_interval; /* recompute SPME every n steps (reference: 2)  */
+    uint32_t com_interval;  /* reference: 100                               */
+    uint32_t recenter_interval; /* reference: 30                            */
+    uint32_t energy_interval;   /* energies every n steps (1 = every step)  */
+    uint32_t flags;         /* DYN_FLAG_*                                   */
+    uint32_t thermo_dof;    /* degrees of freedom (src/thermostat.rs:220)   */
+    uint64_t seed;          /* Philox key for all stochastic terms          */
+} dyn_config_t;
+
+typedef struct {
+    /* non-water atoms (solute + ions), home order */
+    uint32_t n_atoms;
+    const float* atom_pos;     /* [n_atoms*3] */
+    const float* atom_vel;     /* [n_atoms*3] */
+    const float* atom_mass;    /* [n_atoms]   */
+    const float* atom_q;       /* [n_atoms]   */
+    const float* atom_sigma;   /* [n_atoms]   */
+    const float* atom_eps;     /* [n_atoms]   */
+    const uint8_t* atom_static;/* [n_atoms] or NULL */
+    /* rigid OPC waters: O, H0, H1 per molecule */
+    uint32_t n_water;
+    const float* water_pos;    /* [n_water*9] */
+    const float* water_vel;    /* [n_water*9] */
+    /* topology (atom indices) */
+    uint32_t n_excl;   const uint32_t* excl;     /* [n_excl*2] 1-2, 1-3  */
+    uint32_t n_pair14; const uint32_t* pair14;   /* [n_pair14*2]         */
+    uint32_t n_bonds;  const uint32_t* bonds;    /* [n_bonds*2]          */
+    const float* bond_k; const float* bond_r0;
+    uint32_t n_angles; const uint32_t* angles;   /* [n_angles*3]         */
+    const float* angle_k; const float* angle_theta0;
+    uint32_t n_dihedrals; const uint32_t* dihedrals; /* [n*4], one row per term */
+    const float* dihedral_k; const float* dihedral_n; const float* dihedral_phase;
+    uint32_t n_constraints; const uint32_t* constraints; /* [n*2] H bonds */
+    const float* constraint_r0;
+} dyn_system_desc_t;
+
+typedef struct {
+    double kinetic;         /* kcal/mol, all sites but M                   */
+    double kinetic_trans;   /* solute + water COM KE                       */
+    double potential;       /* per the reference or full convention        */
+    double e_lj;            /* short-range LJ                              */
+    double e_coul_short;    /* erfc real-space Coulomb                     */
+    double e_water_water_short;
+    double e_recip;         /* SPME incl. self term                        */
+    double e_corrections;   /* exclusion corrections (corrected mode)     */
+    double e_bonded;
+    double virial;          /* total virial, kcal/mol                      */
+    double virial_short, virial_recip, virial_bonded, virial_constraints;
+    double pressure_bar;
+    double temperature;
+    double box[3];
+    uint64_t step;
+    uint64_t list_rebuilds;
+    uint64_t pairs_in_list;   /* molecule/atom pair slots in the cluster lists */
+    double kinetic_rigid;     /* KE of the rigid-body motion of the waters (what the
+                               * next rigid drift keeps) + atomic KE of the atoms;
+                               * temperature and CSVR use this */
+    double pressure_atomic_bar; /* the reference's formula: COM KE with the site
+                               * virial (src/barostat.rs:419-431); pressure_bar
+                               * uses the molecular virial of the rigid waters */
+} dyn_energies_t;
+
+/* Creates a resident system (replaces MdState::new's device setup,
+ * src/lib.rs:1072-1099, and owns everything MdState::step touches). */
+int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_system_desc_t* sys,
+                   dyn_sys_t* out);
+
+/* Advances n_steps steps of length dt (ps): MdState::step
+ * (src/integrate.rs:72-473) with the configured integrator, fully on the
+ * device.  Asynchronous on the handle's stream. */
+int dyn_sys_step(dyn_sys_t h, uint32_t n_steps, float dt);
+
+/* One force evaluation at the current coordinates, as
+ * reset_f_acc_pe_virial + apply_all_forces (src/lib.rs:1220-1348); writes
+ * forces (float64, home order): f_atoms [n_atoms*3], f_water [n_water*12]
+ * with sites O, H0, H1, M.  Either pointer may be NULL.  Synchronous. */
+int dyn_sys_forces(dyn_sys_t h, double* f_atoms, double* f_water, dyn_energies_t* energies);
+
+/* Current state in home order (any pointer may be NULL).  water_pos and
+ * water_vel are [n_water*9] (O, H0, H1); water_m [n_water*3].  Synchronous. */
+int dyn_sys_get_state(dyn_sys_t h, float* atom_pos, float* atom_vel, float* water_pos,
+                      float* water_vel, float* water_m);
+
+/* Overwrites positions and velocities (home order, NULL = keep). */
+int dyn_sys_set_state(dyn_sys_t h, const float* atom_pos, const float* atom_vel,
+                      const float* water_pos, const float* water_vel);
+
+/* Energies of the last step that computed them (synchronous). */
+int dyn_sys_get_energies(dyn_sys_t h, dyn_energies_t* out);
+
+/* Blocks until the handle's stream is idle; returns DYN_ERR_NONFINITE if the
+ * device flagged non-finite coordinates since the last call. */
+int dyn_sys_sync(dyn_sys_t h);
+
+int dyn_sys_destroy(dyn_sys_t h);
+
+/* Drop-in step with the state on the host, as the reference's MdState keeps
+ * it (src/integrate.rs:72, README "state lives on the host"): copies the
+ * given positions/velocities (home order, NULL = keep the resident ones) to
+ * the device, advances n_steps, then copies positions, velocities and
+ * energies back (NULL outputs are skipped).  Synchronous.  Host buffers
+ * should be page-locked for full copy bandwidth. */
+int dyn_sys_step_host(dyn_sys_t h, uint32_t n_steps, float dt, const float* atom_pos_in,
+                      const float* atom_vel_in, const float* water_pos_in,
+                      const float* water_vel_in, float* atom_pos_out, float* atom_vel_out,
+                      float* water_pos_out, float* water_vel_out, dyn_energies_t* energies);
+
+/* Stage timing, the device counterpart of the reference's per-component
+ * timers (ComputationTimeSums, src/util.rs:111-180): runs n_steps steps
+ * without graphs, with CUDA events between stages on the handle's stream,
+ * and writes the mean milliseconds per step of each stage into ms[6]:
+ * [0] first half (kick/drift/thermostat), [1] displacement check and list
+ * rebuild, [2] short-range pair kernels, [3] 1-4 and bonded terms,
+ * [4] SPME (mean over the steps that ran it), [5] kick, reductions,
+ * thermostat/barostat and periodic tasks. */
+int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, double* ms);
+
+/* Number of this library's kernels one step launches (library kernels such
+ * as cuFFT's are not counted), for the step with SPME (spme != 0) or
+ * without. */
+int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DYNB200_H */

@@ -1,0 +1,255 @@
+"""Rigid-water drift, kicks, thermostats and pressure, float64 (oracle).
+
+Restates, vectorised over molecules:
+  integrate_rigid_water   src/solvent/opc_settle.rs:51-198
+  kick_and_drift          src/integrate.rs:478-511
+  kick_and_calc_accel     src/integrate.rs:515-562
+  drift                   src/integrate.rs:566-587
+  LangevinMiddle step     src/integrate.rs:100-212
+  VerletVelocity + CSVR   src/integrate.rs:213-317
+  measure_kinetic_energy(_translational)  src/thermostat.rs:46-84
+  apply_thermostat_csvr   src/thermostat.rs:258-304
+  apply_langevin_thermostat  src/thermostat.rs:308-362
+  measure_pressure        src/barostat.rs:419-431
+  zero_linear_momentum    src/com_zero.rs:57-81
+Noise comes from oracle.philox (the engine's stream) instead of the
+reference's unseeded ThreadRng.
+"""
+import numpy as np
+
+from . import opc, philox
+
+MAX_ACCEL = 1e5  # src/integrate.rs:26
+
+
+def min_image(d, ext):
+    return d - np.round(d / ext) * ext
+
+
+def wrap(p, lo, ext):
+    return lo + np.mod(p - lo, ext)
+
+
+def rodrigues(r, omega, dt):
+    """Rotate r by |omega| dt about omega (src/solvent/opc_settle.rs:51-67)."""
+    od = omega * dt
+    th = np.linalg.norm(od, axis=-1, keepdims=True)
+    small = th < 1e-12
+    ths = np.where(small, 1.0, th)
+    n = od / ths
+    c = np.cos(th)
+    s = np.sin(th)
+    rot = r * c + np.cross(n, r) * s + n * np.sum(n * r, axis=-1, keepdims=True) * (1.0 - c)
+    wxr = np.cross(od, r)
+    ser = r + wxr + np.cross(od, wxr) * 0.5
+    return np.where(small, ser, rot)
+
+
+def solve_sym3(ixx, iyy, izz, ixy, ixz, iyz, b):
+    """I^-1 b by the adjugate (src/solvent/opc_settle.rs:69-95)."""
+    det = (ixx * (iyy * izz - iyz * iyz) - ixy * (ixy * izz - iyz * ixz)
+           + ixz * (ixy * iyz - iyy * ixz))
+    ok = np.abs(det) >= 1e-12
+    inv_det = np.where(ok, 1.0 / np.where(ok, det, 1.0), 0.0)
+    i00 = (iyy * izz - iyz * iyz) * inv_det
+    i01 = (ixz * iyz - ixy * izz) * inv_det
+    i02 = (ixy * iyz - ixz * iyy) * inv_det
+    i11 = (ixx * izz - ixz * ixz) * inv_det
+    i12 = (ixz * ixy - ixx * iyz) * inv_det
+    i22 = (ixx * iyy - ixy * ixy) * inv_det
+    bx, by, bz = b[:, 0], b[:, 1], b[:, 2]
+    return np.stack([i00 * bx + i01 * by + i02 * bz,
+                     i01 * bx + i11 * by + i12 * bz,
+                     i02 * bx + i12 * by + i22 * bz], axis=1)
+
+
+def rigid_water_drift(wpos, wvel, dt, lo, ext):
+    """integrate_rigid_water for all molecules.
+
+    wpos, wvel: (nw, 3, 3) arrays [O, H0, H1].  Returns new (wpos, wvel, m,
+    constraint_virial).
+    """
+    mo, mh = float(opc.O_MASS), float(opc.H_MASS)
+    mt = float(opc.MASS_WATER_MOL)
+    o = wpos[:, 0]
+    h0 = o + min_image(wpos[:, 1] - o, ext)
+    h1 = o + min_image(wpos[:, 2] - o, ext)
+    vo, vh0, vh1 = wvel[:, 0], wvel[:, 1], wvel[:, 2]
+    r_com = (o * mo + h0 * mh + h1 * mh) / mt
+    v_com = (vo * mo + vh0 * mh + vh1 * mh) / mt
+    r_o, r_h0, r_h1 = o - r_com, h0 - r_com, h1 - r_com
+    u_o, u_h0, u_h1 = vo - v_com, vh0 - v_com, vh1 - v_com
+    L = np.cross(r_o, u_o) * mo + np.cross(r_h0, u_h0) * mh + np.cross(r_h1, u_h1) * mh
+
+    def acc(r, m):
+        x, y, z = r[:, 0], r[:, 1], r[:, 2]
+        r2 = x * x + y * y + z * z
+        return m * (r2 - x * x), m * (r2 - y * y), m * (r2 - z * z), -m * x * y, -m * x * z, -m * y * z
+
+    terms = [acc(r_o, mo), acc(r_h0, mh), acc(r_h1, mh)]
+    ixx, iyy, izz, ixy, ixz, iyz = (terms[0][k] + terms[1][k] + terms[2][k] for k in range(6))
+    w = solve_sym3(ixx, iyy, izz, ixy, ixz, iyz, L)
+    delta = v_com * dt
+    r_o2 = rodrigues(r_o, w, dt)
+    r_h02 = rodrigues(r_h0, w, dt)
+    r_h12 = rodrigues(r_h1, w, dt)
+    new_o = wrap(r_com + delta + r_o2, lo, ext)
+    new_h0 = new_o + min_image(r_com + delta + r_h02 - new_o, ext)
+    new_h1 = new_o + min_image(r_com + delta + r_h12 - new_o, ext)
+    v_o2 = np.cross(w, r_o2)
+    v_h02 = np.cross(w, r_h02)
+    v_h12 = np.cross(w, r_h12)
+    nv = np.stack([v_com + v_o2, v_com + v_h02, v_com + v_h12], axis=1)
+    npos = np.stack([new_o, new_h0, new_h1], axis=1)
+    bis = (new_h0 - new_o) + (new_h1 - new_o)
+    m = new_o + bis / np.linalg.norm(bis, axis=1, keepdims=True) * float(opc.O_EP_R)
+    dv_h0 = v_h02 - u_h0
+    dv_h1 = v_h12 - u_h1
+    vir = np.sum(np.sum((r_h02 - r_o2) * dv_h0 * (mh / dt), axis=1)
+                 + np.sum((r_h12 - r_o2) * dv_h1 * (mh / dt), axis=1))
+    return npos, nv, m, float(vir)
+
+
+def kinetic_energy(state):
+    """measure_kinetic_energy (src/thermostat.rs:46-64), kcal/mol."""
+    ke = 0.0
+    dyn = ~state["atom_static"]
+    if len(state["atom_vel"]):
+        v = state["atom_vel"][dyn]
+        ke += float(np.sum(state["atom_mass"][dyn] * np.sum(v * v, axis=1)))
+    wv = state["water_vel"]
+    if len(wv):
+        m = np.array([float(opc.O_MASS), float(opc.H_MASS), float(opc.H_MASS)])
+        ke += float(np.sum(m[None, :] * np.sum(wv * wv, axis=2)))
+    return ke * 0.5 / float(opc.KCAL_TO_NATIVE)
+
+
+def kinetic_energy_translational(state):
+    """measure_kinetic_energy_translational (src/thermostat.rs:69-84)."""
+    ke = 0.0
+    dyn = ~state["atom_static"]
+    if len(state["atom_vel"]):
+        v = state["atom_vel"][dyn]
+        ke += float(np.sum(state["atom_mass"][dyn] * np.sum(v * v, axis=1)))
+    wv = state["water_vel"]
+    if len(wv):
+        mo, mh, mt = float(opc.O_MASS), float(opc.H_MASS), float(opc.MASS_WATER_MOL)
+        vc = (wv[:, 0] * mo + wv[:, 1] * mh + wv[:, 2] * mh) / mt
+        ke += float(np.sum(mt * np.sum(vc * vc, axis=1)))
+    return ke * 0.5 / float(opc.KCAL_TO_NATIVE)
+
+
+def pressure_bar(ke_trans, virial_kcal, volume):
+    """measure_pressure (src/barostat.rs:419-431)."""
+    return (2.0 * ke_trans + virial_kcal) / (3.0 * volume) * opc.BAR_PER_KCAL_MOL_PER_ANSTROM_CUBED
+
+
+def langevin_ou(state, dt, gamma, temp, step, seed):
+    """apply_langevin_thermostat (src/thermostat.rs:308-362) with the engine's
+    Philox stream: particle id = atom index for solute atoms, n_atoms +
+    3*water + site for water sites (site 0 O, 1 H0, 2 H1)."""
+    c = np.exp(-gamma * dt)
+    s2 = max(1.0 - c * c, 0.0)
+    num = float(opc.KB_A2_PS2_PER_K_PER_AMU) * temp * s2
+    na = len(state["atom_vel"])
+    nw = len(state["water_vel"])
+    if na:
+        dyn = ~state["atom_static"]
+        xi = philox.ou_normals(np.arange(na, dtype=np.uint32), step, seed)
+        sig = np.sqrt(num / np.where(dyn, state["atom_mass"], 1.0))
+        newv = c * state["atom_vel"] + sig[:, None] * xi
+        state["atom_vel"] = np.where(dyn[:, None], newv, state["atom_vel"])
+    if nw:
+        ids = (na + np.arange(3 * nw)).astype(np.uint32)
+        xi = philox.ou_normals(ids, step, seed).reshape(nw, 3, 3)
+        m = np.array([float(opc.O_MASS), float(opc.H_MASS), float(opc.H_MASS)])
+        sig = np.sqrt(num / m)
+        state["water_vel"] = c * state["water_vel"] + sig[None, :, None] * xi
+
+
+def csvr(state, dt, tau, temp, dof, step, seed):
+    """apply_thermostat_csvr (src/thermostat.rs:258-304); chi-square draw as
+    2 * Gamma((dof-1)/2) from oracle.philox.gamma_marsaglia_tsang."""
+    if tau <= 0.0:
+        return
+    dof = float(max(dof, 2))
+    ke = kinetic_energy(state)
+    if ke < 1e-20:
+        return
+    c = np.exp(-dt / tau)
+    r = philox.csvr_normal(step, seed)
+    chi = 2.0 * philox.gamma_marsaglia_tsang(0.5 * (dof - 1.0), step, seed)
+    ke_t = 0.5 * dof * opc.GAS_CONST_R * temp
+    kp = ke * c + ke_t * (1.0 - c) * ((chi + r * r) / dof) + 2.0 * r * np.sqrt(c * (1.0 - c) * ke * ke_t / dof)
+    kp = max(kp, 1e-20)
+    lam = np.sqrt(kp / ke)
+    dyn = ~state["atom_static"]
+    state["atom_vel"][dyn] *= lam
+    state["water_vel"] *= lam
+
+
+def zero_linear_momentum(state):
+    """zero_linear_momentum (src/com_zero.rs:57-81)."""
+    dyn = ~state["atom_static"]
+    msum = float(np.sum(state["atom_mass"][dyn]))
+    p = np.sum(state["atom_mass"][dyn, None] * state["atom_vel"][dyn], axis=0) if dyn.any() else np.zeros(3)
+    nw = len(state["water_vel"])
+    if nw:
+        m = np.array([float(opc.O_MASS), float(opc.H_MASS), float(opc.H_MASS)])
+        msum += float(opc.MASS_WATER_MOL) * nw
+        p = p + np.sum(m[None, :, None] * state["water_vel"], axis=(0, 1))
+    if msum <= 1e-6:
+        return
+    vc = p / msum
+    state["atom_vel"][dyn] -= vc
+    state["water_vel"] -= vc[None, None, :]
+
+
+def kick_and_calc_accel(state, forces, dt):
+    """kick_and_calc_accel (src/integrate.rs:515-562) without H constraints.
+
+    ``forces``: dict with f_atoms (na,3), f_water (nw,4,3) [O,H0,H1,M].
+    """
+    na = len(state["atom_vel"])
+    if na:
+        dyn = ~state["atom_static"]
+        a = forces["f_atoms"] * (float(opc.KCAL_TO_NATIVE) / state["atom_mass"])[:, None]
+        amag = np.linalg.norm(a, axis=1)
+        big = amag * amag > MAX_ACCEL * MAX_ACCEL
+        a = np.where(big[:, None], a / np.where(big, amag, 1.0)[:, None] * MAX_ACCEL, a)
+        state["atom_accel"] = np.where(dyn[:, None], a, 0.0)
+        state["atom_vel"] = state["atom_vel"] + state["atom_accel"] * dt
+    fw = forces["f_water"]
+    if len(fw):
+        fo, fh0, fh1 = opc.project_ep_force(fw[:, 0], fw[:, 1], fw[:, 2], fw[:, 3])
+        acc = np.stack([fo * float(opc.ACCEL_CONV_WATER_O), fh0 * float(opc.ACCEL_CONV_WATER_H),
+                        fh1 * float(opc.ACCEL_CONV_WATER_H)], axis=1)
+        state["water_accel"] = acc
+        state["water_vel"] = state["water_vel"] + acc * dt
+
+
+def kick_and_drift(state, dt_kick, dt_drift, lo, ext):
+    """kick_and_drift (src/integrate.rs:478-511) without H constraints."""
+    if len(state["atom_vel"]):
+        dyn = ~state["atom_static"]
+        v = state["atom_vel"] + state["atom_accel"] * dt_kick
+        state["atom_vel"] = np.where(dyn[:, None], v, state["atom_vel"])
+        state["atom_pos"] = np.where(dyn[:, None], state["atom_pos"] + state["atom_vel"] * dt_drift,
+                                     state["atom_pos"])
+    if len(state["water_vel"]):
+        state["water_vel"] = state["water_vel"] + state["water_accel"] * dt_kick
+        p, v, m, vir = rigid_water_drift(state["water_pos"], state["water_vel"], dt_drift, lo, ext)
+        state["water_pos"], state["water_vel"], state["water_m"] = p, v, m
+        return vir
+    return 0.0
+
+
+def drift(state, dt, lo, ext):
+    """drift (src/integrate.rs:566-587) without H constraints."""
+    if len(state["atom_vel"]):
+        dyn = ~state["atom_static"]
+        state["atom_pos"] = np.where(dyn[:, None], state["atom_pos"] + state["atom_vel"] * dt,
+                                     state["atom_pos"])
+    if len(state["water_vel"]):
+        p, v, m, _ = rigid_water_drift(state["water_pos"], state["water_vel"], dt, lo, ext)
+        state["water_pos"], state["water_vel"], state["water_m"] = p, v, m

@@ -1,0 +1,181 @@
+"""Parity of the device-resident engine (dyn_sys_*) with the float64 oracle.
+
+Force evaluations are compared with oracle.method.all_forces, which finds
+every site pair within the cutoff with a periodic k-d tree (independent of
+any neighbour list), so a missing cluster pair or a wrong exclusion shows
+up as a force error.  Tolerances are the ones the engine is specified to:
+per-atom force relative RMS <= 1e-5 vs float64 (precision form), and
+potential energy relative error <= 1e-6.
+"""
+import numpy as np
+import pytest
+
+from dynamics_b200 import md, synth
+from oracle import integrate as oint
+from oracle import method
+
+from .systems import mixed, rel_rms, water_only
+
+pytestmark = pytest.mark.gpu
+
+FORCE_RTOL = 1e-5
+PE_RTOL = 1e-6
+
+
+def _cfg(sysd, mode="reference", integ=None, **kw):
+    grid = tuple(int(2 ** np.ceil(np.log2(x))) if x <= 32 else int(np.ceil(x / 8) * 8)
+                 for x in (sysd["box_hi"] - sysd["box_lo"]))
+    c = md.MdConfig(coulomb_cutoff=8.0, lj_cutoff=8.0, spme_alpha=synth.ewald_alpha(8.0),
+                    spme_grid=grid, ewald_corrections=(mode == "corrected"),
+                    full_energy=(mode == "corrected"), **kw)
+    if integ is not None:
+        c.integrator = integ
+    return c
+
+
+def _oracle(sysd, cfg):
+    return method.all_forces(sysd, {
+        "cutoff": cfg.coulomb_cutoff, "lj_cutoff": cfg.lj_cutoff, "alpha": cfg.spme_alpha,
+        "grid": cfg.spme_grid, "mode": "corrected" if cfg.ewald_corrections else "reference"})
+
+
+def _compare(got, ref):
+    fa = np.concatenate([got["f_atoms"].reshape(-1), got["f_water"].reshape(-1)])
+    fr = np.concatenate([ref["f_atoms"].reshape(-1), ref["f_water"].reshape(-1)])
+    return rel_rms(fa, fr)
+
+
+@pytest.mark.parametrize("mode", ["reference", "corrected"])
+@pytest.mark.parametrize("make", [water_only, mixed])
+def test_forces_match_oracle(gpu_lib, make, mode):
+    sysd = make()
+    cfg = _cfg(sysd, mode)
+    st = md.MdState(sysd, cfg)
+    got = st.forces()
+    ref = _oracle(sysd, cfg)
+    err = _compare(got, ref)
+    assert err < FORCE_RTOL, f"force rel-RMS {err:.3e}"
+    assert abs(got["potential"] - ref["pe"]) <= PE_RTOL * abs(ref["pe"]), (got["potential"], ref["pe"])
+    assert abs(got["e_recip"] - ref["e_recip"]) <= 1e-6 * abs(ref["e_recip"])
+    st.close()
+
+
+def test_config1_forces_match_oracle(gpu_lib):
+    sysd = synth.config1()
+    cfg = md.MdConfig(coulomb_cutoff=10.0, lj_cutoff=10.0, spme_alpha=synth.ewald_alpha(10.0),
+                      spme_grid=(32, 32, 32))
+    st = md.MdState(sysd, cfg)
+    got = st.forces()
+    ref = _oracle(sysd, cfg)
+    err = _compare(got, ref)
+    assert err < FORCE_RTOL, f"force rel-RMS {err:.3e}"
+    st.close()
+
+
+def test_forces_deterministic(gpu_lib):
+    sysd = mixed()
+    cfg = _cfg(sysd)
+    a = md.MdState(sysd, cfg)
+    b = md.MdState(sysd, cfg)
+    fa, fb = a.forces(), b.forces()
+    np.testing.assert_array_equal(fa["f_water"], fb["f_water"])
+    np.testing.assert_array_equal(fa["f_atoms"], fb["f_atoms"])
+    a.step(0.002, 20)
+    b.step(0.002, 20)
+    sa, sb = a.state(), b.state()
+    for k in sa:
+        np.testing.assert_array_equal(sa[k], sb[k])
+    a.close()
+    b.close()
+
+
+def _oracle_vv(sysd, cfg, n, dt):
+    """n velocity-Verlet steps without thermostat in float64, SPME every step."""
+    s = {
+        "atom_pos": sysd["atom_pos"].astype(np.float64), "atom_vel": sysd["atom_vel"].astype(np.float64),
+        "atom_mass": sysd["atom_mass"].astype(np.float64),
+        "atom_static": np.zeros(len(sysd["atom_pos"]), bool),
+        "water_pos": sysd["water_pos"].astype(np.float64), "water_vel": sysd["water_vel"].astype(np.float64),
+    }
+    lo = sysd["box_lo"].astype(np.float64)
+    ext = (sysd["box_hi"] - sysd["box_lo"]).astype(np.float64)
+
+    def forces(s):
+        d = dict(sysd)
+        d["atom_pos"] = s["atom_pos"]
+        d["water_pos"] = s["water_pos"]
+        d.pop("water_m", None)
+        return _oracle(d, cfg)
+
+    f = forces(s)
+    oint.kick_and_calc_accel(s, f, 0.0)
+    for _ in range(n):
+        oint.kick_and_drift(s, dt / 2, dt, lo, ext)
+        f = forces(s)
+        oint.kick_and_calc_accel(s, f, dt / 2)
+    return s
+
+
+def test_short_trajectory_matches_oracle(gpu_lib):
+    sysd = water_only()
+    cfg = _cfg(sysd, integ=md.VerletVelocity(thermostat=None), spme_interval=1,
+               zero_com_drift=False, recenter_sim_box=False)
+    st = md.MdState(sysd, cfg)
+    st.step(0.002, 5)
+    got = st.state()
+    ref = _oracle_vv(sysd, cfg, 5, 0.002)
+    d = got["water_pos"].astype(np.float64) - ref["water_pos"]
+    box = float(sysd["box_hi"][0] - sysd["box_lo"][0])
+    d -= np.round(d / box) * box
+    assert np.max(np.abs(d)) < 1e-4
+    assert rel_rms(got["water_vel"], ref["water_vel"]) < 1e-4
+    st.close()
+
+
+def test_nve_energy_conservation(gpu_lib):
+    sysd = water_only()
+    cfg = _cfg(sysd, "corrected", integ=md.VerletVelocity(thermostat=None), spme_interval=1,
+               zero_com_drift=False, recenter_sim_box=False, reset_angle=False)
+    cfg.spme_grid = (32, 32, 32)
+    sysd = md.equilibrate(sysd, cfg, n_steps=1000)
+    st = md.MdState(sysd, cfg)
+    e = []
+    for _ in range(20):
+        st.step(0.001, 10)
+        en = st.energies()
+        e.append(en["kinetic"] + en["potential"])
+    e = np.array(e)
+    drift = abs(e[-1] - e[0])
+    assert drift < 2e-3 * abs(e[0]), (e[0], e[-1])
+    st.close()
+
+
+def test_langevin_thermalises(gpu_lib):
+    sysd = synth.config1()
+    cfg = md.MdConfig(coulomb_cutoff=10.0, lj_cutoff=10.0, spme_alpha=synth.ewald_alpha(10.0),
+                      spme_grid=(32, 32, 32), integrator=md.LangevinMiddle(gamma=1.0), seed=7)
+    sysd = md.equilibrate(sysd, cfg, n_steps=1000)
+    st = md.MdState(sysd, cfg)
+    st.step(0.002, 200)
+    en = st.energies()
+    assert np.isfinite(en["potential"]) and 200.0 < en["temperature"] < 400.0
+    assert en["list_rebuilds"] >= 1
+    st.close()
+
+
+def test_csvr_holds_temperature(gpu_lib):
+    sysd = mixed()
+    cfg = _cfg(sysd, integ=md.VerletVelocity(thermostat=0.1), seed=3)
+    sysd = md.equilibrate(sysd, cfg, n_steps=1000)
+    st = md.MdState(sysd, cfg)
+    st.step(0.001, 300)
+    en = st.energies()
+    assert 220.0 < en["temperature"] < 380.0
+    st.close()
+
+
+def test_invalid_config_raises(gpu_lib):
+    from dynamics_b200 import DynError
+    sysd = water_only(n_side=3)
+    with pytest.raises(DynError):
+        md.MdState(sysd, md.MdConfig(coulomb_cutoff=10.0))  # box too small for the cutoff
