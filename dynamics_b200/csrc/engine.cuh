@@ -22,6 +22,9 @@
 #include "common.cuh"
 
 #define WCL 8             // waters per cluster
+#define GRPW 32           // waters per i-group of the water-water kernel (4 clusters)
+#define NPOLY 15          // coefficients of the screened-Coulomb polynomials
+#define LPW 8             // lanes per i-water in the water-water kernel
 #define ACL 8             // atoms per cluster
 #define INVALID_ID 0xFFFFFFFFu
 #define NACC 16           // accumulator slots
@@ -42,7 +45,8 @@ struct Scalars {
     unsigned int overflow;        // largest list length that did not fit (0 = ok)
     unsigned int nonfinite;       // set when a kernel saw NaN/Inf
     unsigned int max_disp2_bits;  // float bits, atomicMax over non-negative floats
-    unsigned int pad0, pad1;
+    unsigned int timeout;         // a bounded device wait gave up
+    unsigned int pad1;
     double acc[NACC];             // finalised accumulators of the last step
     double recip_cache[4];        // e_recip, vir_recip, e_corr, vir_corr of last SPME step
     double csvr_lambda;
@@ -98,11 +102,21 @@ struct SysView {
     // cluster bounding boxes (center xyz, half extent xyz)
     float4* wbb_c; float4* wbb_h; float4* abb_c; float4* abb_h;
     // cluster lists (fixed capacity per i cluster)
-    uint32_t cap_ww, cap_ws, cap_sw, cap_ss;
-    uint32_t* ww_n; uint32_t* ww_j;
+    uint32_t cap_ws, cap_sw, cap_ss;
     uint32_t* ws_n; uint32_t* ws_j;
     uint32_t* sw_n; uint32_t* sw_j;
     uint32_t* ss_n; uint32_t* ss_j; unsigned long long* ss_mask;
+    // water-water: per 32-water i-group the candidate j-clusters (tile_j),
+    // the union of the waters its members need, stored as runs of
+    // consecutive slots (staged in shared memory by bulk copies), and per
+    // i-water a list of indices into that union
+    uint32_t ngrp_cap, cap_tile, cap_nb, cap_union, cap_run;
+    float4* gbb_c; float4* gbb_h;
+    uint32_t* tile_n; uint32_t* tile_j;      // [ngrp_cap], [ngrp_cap*cap_tile]
+    uint32_t* grp_nrun; uint32_t* grp_nloc;  // [ngrp_cap]
+    uint2* grp_run;                          // [ngrp_cap*cap_run] (slot, union offset)
+    uint16_t* cand_loc;                      // [ngrp_cap*cap_tile*8] rebuild scratch
+    uint32_t* wnb_n; uint16_t* wnb;          // [nw_cap], [nw_cap*cap_nb]
     // 1-4 pairs, exclusions (pairs), bonded terms, constraints
     uint32_t n14; uint2* p14; float4* p14_par;     // sigma, eps, qq, unused
     uint32_t nexcl; uint2* excl; float* excl_qq;
@@ -131,6 +145,11 @@ struct SysView {
     uint32_t integrator, thermostat, barostat;
     uint32_t spme_interval, com_interval, recenter_interval;
     double e_self;          // Ewald self energy -alpha/sqrt(pi) sum q^2
+    // u(x) = erfc(x) + 2x/sqrt(pi) exp(-x^2) and erfc(x) at x = alpha r, as
+    // polynomials in s = 2r/rc - 1 on [-1, 1] (Chebyshev interpolation,
+    // power basis, Horner in float32): force = qq u / r^3, energy = qq erfc / r
+    float poly_f[NPOLY], poly_e[NPOLY];
+    float two_over_rc;
     uint32_t nb[NREGION];   // blocks each region's kernel is launched with
 };
 
@@ -148,6 +167,8 @@ void launch_gather_atoms(const SysView& v, cudaStream_t st);
 void launch_pairs(const SysView& v, cudaStream_t st, bool energy);
 void launch_pair14(const SysView& v, cudaStream_t st, bool energy);
 int pair_blocks_ww(const SysView& v);
+int pair_ww_setup(const SysView& v);
+int ww_tile_blocks(const SysView& v);
 int pair_blocks_ss(const SysView& v);
 int pair14_blocks(const SysView& v);
 

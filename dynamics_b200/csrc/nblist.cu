@@ -9,12 +9,17 @@
 //      multiple of 8, so every aligned 8-slot group is a compact cluster;
 //   3. cluster bounding boxes are tested against each other (all pairs,
 //      min-image on centres) and each i-cluster's hits are compacted with
-//      warp ballots into a fixed-capacity list, ascending in j.
+//      warp ballots into a fixed-capacity list, ascending in j;
+//   4. for water-water, 32-water groups get a tile of j-clusters and every
+//      water a compact list of tile-local molecule indices (O-O distance
+//      below cutoff + twice the O-H reach + buffer).
 // Every kernel of the rebuild returns immediately unless the displacement
 // check raised Scalars::need_rebuild, so the whole step is one static CUDA
 // graph.  The rebuild criterion is the reference's: max displacement since
 // the last rebuild >= buffer / 2 (src/neighbors.rs:159-169), tracking water
 // O only (src/neighbors.rs:71-82); water list radii add twice the O-H reach.
+#include <algorithm>
+
 #include "engine.cuh"
 
 namespace {
@@ -29,14 +34,19 @@ __device__ __forceinline__ float frac_box(float x, float lo, float inv_ext) {
     return f >= 1.0f ? 0.0f : f;
 }
 
+// Column rank along a boustrophedon path over the xy grid, and the sort key
+// inside the column: z ascending in even-ranked columns, descending in odd
+// ones, so consecutive slots are neighbours in space across column ends too.
 __device__ __forceinline__ uint32_t column_of(float3 p, const BoxDev& b, uint32_t ncx, uint32_t ncy,
-                                              float* zf) {
+                                              float* key) {
     const float fx = frac_box(p.x, b.lo[0], b.inv_ext[0]);
     const float fy = frac_box(p.y, b.lo[1], b.inv_ext[1]);
-    *zf = frac_box(p.z, b.lo[2], b.inv_ext[2]);
-    uint32_t cx = min((uint32_t)(fx * ncx), ncx - 1);
-    uint32_t cy = min((uint32_t)(fy * ncy), ncy - 1);
-    return cy * ncx + cx;
+    const float fz = frac_box(p.z, b.lo[2], b.inv_ext[2]);
+    const uint32_t cx = min((uint32_t)(fx * ncx), ncx - 1);
+    const uint32_t cy = min((uint32_t)(fy * ncy), ncy - 1);
+    const uint32_t rank = cy * ncx + ((cy & 1u) ? (ncx - 1 - cx) : cx);
+    *key = (rank & 1u) ? 1.0f - fz : fz;
+    return rank;
 }
 
 // ---------------------------------------------------------------------------
@@ -105,27 +115,26 @@ __global__ void k_col_assign(SysView v, bool force) {
     }
 }
 
-// Serial scan over columns (only at rebuilds; columns number a few hundred).
+// Serial scan over columns in path order (only at rebuilds; a few hundred
+// columns).  Slots are contiguous along the path; padding sits at the end.
 __global__ void k_col_scan(SysView v, bool force) {
     if (!rebuild_on(v, force)) return;
     if (threadIdx.x == 0) {
-        uint32_t p = 0, q = 0;
+        uint32_t q = 0;
         for (uint32_t c = 0; c < v.ncol; ++c) {
-            v.col_off[c] = p; v.col_boff[c] = q;
-            const uint32_t n = v.col_count[c];
-            p += (n + WCL - 1) / WCL * WCL; q += n;
+            v.col_off[c] = q; v.col_boff[c] = q;
+            q += v.col_count[c];
         }
-        v.col_off[v.ncol] = p; v.col_boff[v.ncol] = q;
-        v.sc->n_wclus = p / WCL;
+        v.col_off[v.ncol] = q; v.col_boff[v.ncol] = q;
+        v.sc->n_wclus = (q + WCL - 1) / WCL;
     } else if (threadIdx.x == 32) {
-        uint32_t p = 0, q = 0;
+        uint32_t q = 0;
         for (uint32_t c = 0; c < v.ncol; ++c) {
-            v.acol_off[c] = p; v.acol_boff[c] = q;
-            const uint32_t n = v.acol_count[c];
-            p += (n + ACL - 1) / ACL * ACL; q += n;
+            v.acol_off[c] = q; v.acol_boff[c] = q;
+            q += v.acol_count[c];
         }
-        v.acol_off[v.ncol] = p; v.acol_boff[v.ncol] = q;
-        v.sc->n_aclus = p / ACL;
+        v.acol_off[v.ncol] = q; v.acol_boff[v.ncol] = q;
+        v.sc->n_aclus = (q + ACL - 1) / ACL;
     }
 }
 
@@ -281,7 +290,7 @@ __device__ __forceinline__ bool excluded(const SysView& v, uint32_t a, uint32_t 
     return lo < v.ex_off[a + 1] && v.ex_idx[lo] == b;
 }
 
-// MODE: 0 water-water, 1 water(i)-atom(j), 2 atom(i)-water(j), 3 atom-atom
+// MODE: 1 water(i)-atom(j), 2 atom(i)-water(j), 3 atom-atom
 template <int MODE>
 __global__ void k_list(SysView v, bool force) {
     if (!rebuild_on(v, force)) return;
@@ -295,11 +304,11 @@ __global__ void k_list(SysView v, bool force) {
     const float4* bhi = (MODE < 2) ? v.wbb_h : v.abb_h;
     const float4* bcj = (MODE == 0 || MODE == 2) ? v.wbb_c : v.abb_c;
     const float4* bhj = (MODE == 0 || MODE == 2) ? v.wbb_h : v.abb_h;
-    const float r = MODE == 0 ? v.r_ww : (MODE == 3 ? v.r_ss : v.r_ws);
+    const float r = MODE == 3 ? v.r_ss : v.r_ws;
     const float r2 = r * r;
-    const uint32_t cap = MODE == 0 ? v.cap_ww : MODE == 1 ? v.cap_ws : MODE == 2 ? v.cap_sw : v.cap_ss;
-    uint32_t* out = MODE == 0 ? v.ww_j : MODE == 1 ? v.ws_j : MODE == 2 ? v.sw_j : v.ss_j;
-    uint32_t* outn = MODE == 0 ? v.ww_n : MODE == 1 ? v.ws_n : MODE == 2 ? v.sw_n : v.ss_n;
+    const uint32_t cap = MODE == 1 ? v.cap_ws : MODE == 2 ? v.cap_sw : v.cap_ss;
+    uint32_t* out = MODE == 1 ? v.ws_j : MODE == 2 ? v.sw_j : v.ss_j;
+    uint32_t* outn = MODE == 1 ? v.ws_n : MODE == 2 ? v.sw_n : v.ss_n;
     const float4 c0 = bci[ci], h0 = bhi[ci];
     uint32_t cnt = 0;
     for (uint32_t jb = 0; jb < nj; jb += 32) {
@@ -334,6 +343,180 @@ __global__ void k_list(SysView v, bool force) {
         outn[ci] = min(cnt, cap);
         if (cnt > cap) atomicMax(&v.sc->overflow, cnt);
         atomicAdd(&v.sc->list_pairs, (unsigned long long)min(cnt, cap));
+    }
+}
+
+// Group bounding boxes over the O positions of the group's waters,
+// min-imaged to the first one.
+__global__ void k_group_bbox(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const BoxDev b = *v.box;
+    const uint32_t nwc = v.sc->n_wclus;
+    const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        float3 lo = f3(1e30f, 1e30f, 1e30f), hi = f3(-1e30f, -1e30f, -1e30f);
+        bool have = false;
+        float3 ref = f3(0.f, 0.f, 0.f);
+        for (uint32_t k = 0; k < GRPW; ++k) {
+            const uint32_t s = g * GRPW + k;
+            if (s >= v.nw_cap || v.wid[s] == INVALID_ID) continue;
+            float3 p = xyz(v.wpos[4 * s]);
+            if (!have) { ref = p; have = true; }
+            p = ref + min_image_rint(p - ref, b);
+            lo = f3(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z));
+            hi = f3(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z));
+        }
+        if (!have) { lo = f3(0.f, 0.f, 0.f); hi = lo; }
+        v.gbb_c[g] = make_float4(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z), 0.f);
+        v.gbb_h[g] = make_float4(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z), 0.f);
+    }
+}
+
+// j-cluster tile of every group: clusters within the water list radius of
+// the group box, ascending (one warp per group, ballot compaction).
+__global__ void k_tile_list(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const BoxDev b = *v.box;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwc = v.sc->n_wclus;
+    const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
+    const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (g >= ng) return;
+    const float4 c0 = v.gbb_c[g], h0 = v.gbb_h[g];
+    const float r2 = v.r_ww * v.r_ww;
+    uint32_t cnt = 0;
+    for (uint32_t jb = 0; jb < nwc; jb += 32) {
+        const uint32_t cj = jb + lane;
+        const bool hit = cj < nwc && bb_dist2(c0, h0, v.wbb_c[cj], v.wbb_h[cj], b) < r2;
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const uint32_t k = cnt + __popc(m & ((1u << lane) - 1u));
+            if (k < v.cap_tile) v.tile_j[(size_t)g * v.cap_tile + k] = cj;
+        }
+        cnt += __popc(m);
+    }
+    if (lane == 0) {
+        v.tile_n[g] = min(cnt, v.cap_tile);
+        if (cnt > v.cap_tile) atomicMax(&v.sc->overflow, cnt);
+    }
+}
+
+// Union of the waters an i-group needs, as runs of consecutive slots, and
+// per i-water lists of indices into that union.  One CTA (256 threads) per
+// group.  Pass 1 marks every candidate water (waters of the group's tile
+// clusters, ascending slot order) that lies within the list radius of any
+// group member and numbers the marked ones with a block-wide scan; run
+// starts (a marked water whose predecessor is unmarked or not the previous
+// slot) get a run record.  Pass 2: 8 lanes per i-water test 8 consecutive
+// candidates at a time and compact hits with a ballot, so every list is in
+// ascending order.  Everything is deterministic.
+constexpr int UT = 256;
+
+__global__ void __launch_bounds__(UT) k_group_union(SysView v, bool force) {
+    if (!rebuild_on(v, force)) return;
+    const BoxDev b = *v.box;
+    const float r2 = v.r_ww * v.r_ww;
+    const uint32_t nwc = v.sc->n_wclus;
+    const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
+    const int tid = threadIdx.x, lane = tid & 31, wid_ = tid >> 5;
+    __shared__ float4 io[GRPW];
+    __shared__ uint32_t wn[UT / 32], wr[UT / 32];
+    __shared__ uint8_t sh_need[UT];
+    __shared__ uint32_t sh_slot[UT];
+    __shared__ uint32_t base_cnt, base_run, carry_slot;
+    __shared__ uint8_t carry_need;
+    for (uint32_t g = blockIdx.x; g < ng; g += gridDim.x) {
+        if (tid < GRPW) {
+            const uint32_t s = g * GRPW + tid;
+            const bool ok = s < v.nw_cap && v.wid[s] != INVALID_ID;
+            const float4 p = ok ? v.wpos[4 * s] : make_float4(0.f, 0.f, 0.f, 0.f);
+            io[tid] = make_float4(p.x, p.y, p.z, ok ? 1.f : 0.f);
+        }
+        if (tid == 0) { base_cnt = 0; base_run = 0; carry_need = 0; carry_slot = INVALID_ID; }
+        __syncthreads();
+        const uint32_t nt = v.tile_n[g];
+        const uint32_t ncand = nt * WCL;
+        const uint32_t* tl = v.tile_j + (size_t)g * v.cap_tile;
+        uint16_t* cl = v.cand_loc + (size_t)g * v.cap_tile * WCL;
+        for (uint32_t c0 = 0; c0 < ncand; c0 += UT) {
+            const uint32_t k = c0 + tid;
+            bool need = false;
+            uint32_t slot = INVALID_ID;
+            if (k < ncand) {
+                slot = tl[k / WCL] * WCL + (k % WCL);
+                if (v.wid[slot] != INVALID_ID) {
+                    const float3 o = xyz(v.wpos[4 * slot]);
+                    for (int i = 0; i < GRPW && !need; ++i) {
+                        const float4 q = io[i];
+                        if (q.w == 0.f) continue;
+                        const float3 d = min_image_rint(o - xyz(q), b);
+                        need = dot3(d, d) < r2;
+                    }
+                }
+            }
+            sh_need[tid] = need;
+            sh_slot[tid] = slot;
+            __syncthreads();
+            const bool pn = tid ? sh_need[tid - 1] != 0 : carry_need != 0;
+            const uint32_t ps = tid ? sh_slot[tid - 1] : carry_slot;
+            const bool start = need && (!pn || slot != ps + 1u);
+            const uint32_t mn = __ballot_sync(0xffffffffu, need), ms = __ballot_sync(0xffffffffu, start);
+            if (lane == 0) { wn[wid_] = __popc(mn); wr[wid_] = __popc(ms); }
+            __syncthreads();
+            uint32_t on = 0, os = 0;
+            for (int w = 0; w < wid_; ++w) { on += wn[w]; os += wr[w]; }
+            const uint32_t lm = (1u << lane) - 1u;
+            const uint32_t loc = base_cnt + on + __popc(mn & lm);
+            const uint32_t rid = base_run + os + __popc(ms & lm);
+            if (k < ncand) cl[k] = need && loc < v.cap_union ? (uint16_t)loc : (uint16_t)0xFFFFu;
+            if (start && rid < v.cap_run) v.grp_run[(size_t)g * v.cap_run + rid] = make_uint2(slot, loc);
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t tn = 0, ts = 0;
+                for (int w = 0; w < UT / 32; ++w) { tn += wn[w]; ts += wr[w]; }
+                base_cnt += tn; base_run += ts;
+                carry_need = sh_need[UT - 1]; carry_slot = sh_slot[UT - 1];
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            v.grp_nloc[g] = min(base_cnt, v.cap_union);
+            v.grp_nrun[g] = min(base_run, v.cap_run);
+            if (base_cnt > v.cap_union) atomicMax(&v.sc->overflow, base_cnt);
+            if (base_run > v.cap_run) atomicMax(&v.sc->overflow, base_run);
+        }
+        __syncthreads();
+        // pass 2: per i-water lists, LPW lanes per i-water
+        const int il = tid / LPW, l = tid % LPW;
+        const uint32_t si = g * GRPW + il;
+        const float4 qi = io[il];
+        const unsigned gmask = ((1u << LPW) - 1u) << ((lane / LPW) * LPW);
+        uint32_t cnt = 0;
+        uint16_t* out = v.wnb + (size_t)si * v.cap_nb;
+        for (uint32_t c0 = 0; c0 < ncand; c0 += LPW) {
+            const uint32_t k = c0 + l;
+            bool hit = false;
+            uint16_t loc = 0xFFFFu;
+            if (k < ncand && qi.w != 0.f) {
+                loc = cl[k];
+                const uint32_t slot = tl[k / WCL] * WCL + (k % WCL);
+                if (loc != 0xFFFFu && slot != si) {
+                    const float3 d = min_image_rint(xyz(qi) - xyz(v.wpos[4 * slot]), b);
+                    hit = dot3(d, d) < r2;
+                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, hit) & gmask;
+            if (hit) {
+                const uint32_t pos = cnt + __popc(m & ((1u << lane) - 1u));
+                if (pos < v.cap_nb) out[pos] = loc;
+            }
+            cnt += __popc(m);
+        }
+        if (l == 0 && si < v.nw_cap) {
+            v.wnb_n[si] = qi.w != 0.f ? min(cnt, v.cap_nb) : 0u;
+            if (cnt > v.cap_nb) atomicMax(&v.sc->overflow, cnt);
+        }
+        __syncthreads();
     }
 }
 
@@ -384,7 +567,11 @@ void launch_rebuild(const SysView& v, cudaStream_t st, bool force) {
     k_bbox<<<nblocks(v.nwclus_cap + v.naclus_cap, T), T, 0, st>>>(v, force);
     k_list_pairs_reset<<<1, 1, 0, st>>>(v, force);
     const int LT = 128;  // 4 warps per block, one i-cluster per warp
-    if (v.nw) k_list<0><<<nblocks((uint64_t)v.nwclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
+    if (v.nw) {
+        k_group_bbox<<<nblocks(v.ngrp_cap, T), T, 0, st>>>(v, force);
+        k_tile_list<<<nblocks((uint64_t)v.ngrp_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
+        k_group_union<<<std::min<uint32_t>(v.ngrp_cap, 148 * 8), UT, 0, st>>>(v, force);
+    }
     if (v.nw && v.na) {
         k_list<1><<<nblocks((uint64_t)v.nwclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
         k_list<2><<<nblocks((uint64_t)v.naclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);

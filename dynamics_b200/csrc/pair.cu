@@ -7,54 +7,66 @@
 // between charged sites, 1-2/1-3 exclusions, no intra-water pairs; 1-4 pairs
 // are excluded here and evaluated (scaled) by k_pair14.
 //
-// Work decomposition (one warp per i-cluster, full lists, no atomics on the
-// i side): a warp owns 8 i-waters (or 8 atoms); lane = (ii, jq) with
-// ii = lane & 7 and jq = lane >> 3, so each lane evaluates i-body ii against
-// j-bodies jq and jq + 4 of every j-cluster in the list.  Water pairs are
-// handled as molecule pairs: one min-image shift from the O-O vector serves
-// all 10 site pairs (1 LJ + 9 Coulomb), valid because the cutoff plus twice
-// the O-H reach is below half the box.  i-forces stay in registers over the
-// whole list, are reduced over the 4 lanes sharing ii with two shuffles and
-// stored once as int64 fixed point; the water-water and atom-atom kernels
-// store (first writers), the mixed kernels add.
+// Work decomposition (full lists, no atomics on the i side).  Water-water:
+// one CTA per 32-water i-group, j sites staged in shared memory, LPW lanes
+// per i-water over its compact molecule list (k_pair_ww_tile).  Mixed and
+// atom kernels: one warp per 8-body i-cluster; lane = (ii, jq) with
+// ii = lane & 7 and jq = lane >> 3 evaluates i-body ii against j-bodies jq and
+// jq + 4 of every j-cluster in its list.  Water pairs are handled as molecule
+// pairs: one min-image shift from the O-O vector serves all 10 site pairs
+// (1 LJ + 9 Coulomb), valid because the cutoff plus twice the O-H reach is
+// below half the box.  i-forces stay in registers over the whole list, are
+// reduced over the lanes sharing an i-body with shuffles and stored once as
+// int64 fixed point; the water-water and atom-atom kernels store (first
+// writers), the mixed kernels add.
 #include "engine.cuh"
 
 namespace {
 
 constexpr int PT = 128;  // threads per block (4 warps)
 
-struct Acc3 { float e_lj, e_c, w; };
+// e_lj, e_c accumulate per-pair energies in float64 (energy steps only);
+// w accumulates the virial in float32
+struct Acc3 { double e_lj, e_c; float w; };
 
+// erfc-screened Coulomb, branch-free: force q q u(alpha r) / r^3 with
+// u(x) = erfc(x) + 2x/sqrt(pi) exp(-x^2) from the host-fitted polynomial in
+// s = 2r/rc - 1; zero for r >= rc (src/cuda/cuda.cu:160-164).  On energy
+// steps the energy q q erfc(alpha r) / r uses erfcf and float64 sums, which
+// keeps the total potential energy within 1e-6 of float64 even where large
+// terms cancel.
 template <bool ENERGY>
-__device__ __forceinline__ void coul(float3 d, float qq, float rc2, float alpha, float c2a,
-                                     float3& f, Acc3& a) {
+__device__ __forceinline__ void coul(float3 d, float qq, const SysView& v, float3& f, Acc3& a) {
     const float r2 = dot3(d, d);
-    if (r2 < rc2) {
-        const float rinv = rsqrtf(r2);
-        const float r = r2 * rinv;
-        const float ar = alpha * r;
-        const float ex = __expf(-ar * ar);
-        const float ec = erfcf(ar);
-        const float fs = qq * fmaf(ec, rinv, c2a * ex) * (rinv * rinv);
-        f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
-        a.w = fmaf(fs, r2, a.w);
-        if (ENERGY) a.e_c = fmaf(qq * rinv, ec, a.e_c);
+    const float rinv = rsqrtf(r2);
+    const float sv = fmaf(r2 * rinv, v.two_over_rc, -1.0f);
+    float u = v.poly_f[NPOLY - 1];
+#pragma unroll
+    for (int k = NPOLY - 2; k >= 0; --k) u = fmaf(u, sv, v.poly_f[k]);
+    const float rinv2 = rinv * rinv;
+    float fs = qq * u * (rinv * rinv2);
+    fs = r2 < v.rc2 ? fs : 0.0f;
+    f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
+    a.w = fmaf(fs, r2, a.w);
+    if (ENERGY) {
+        if (r2 < v.rc2) a.e_c += (double)(qq * rinv) * (double)erfcf(v.alpha * r2 * rinv);
     }
 }
 
+// 12-6 LJ (force_e_lj, src/forces.rs:10-21), branch-free, r <= lj_cutoff.
 template <bool ENERGY>
 __device__ __forceinline__ void lj(float3 d, float sig2, float eps, float ljc2, float scale,
                                    float3& f, Acc3& a) {
     const float r2 = dot3(d, d);
-    if (r2 <= ljc2 && eps != 0.f) {
-        const float ir2 = __frcp_rn(r2);
-        const float sr2 = sig2 * ir2;
-        const float sr6 = sr2 * sr2 * sr2;
-        const float fs = scale * 24.0f * eps * fmaf(2.f, sr6 * sr6, -sr6) * ir2;
-        f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
-        a.w = fmaf(fs, r2, a.w);
-        if (ENERGY) a.e_lj = fmaf(scale * 4.0f * eps, sr6 * sr6 - sr6, a.e_lj);
-    }
+    const bool in = r2 <= ljc2;
+    const float ir2 = __frcp_rn(in ? r2 : 1.0f);
+    const float sr2 = sig2 * ir2;
+    const float sr6 = sr2 * sr2 * sr2;
+    float fs = scale * 24.0f * eps * fmaf(2.f, sr6 * sr6, -sr6) * ir2;
+    fs = in ? fs : 0.0f;
+    f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
+    a.w = fmaf(fs, r2, a.w);
+    if (ENERGY) a.e_lj += in ? (double)(scale * 4.0f * eps) * (double)(sr6 * sr6 - sr6) : 0.0;
 }
 
 __device__ __forceinline__ float3 shift_of(float3 d, const BoxDev& b) {
@@ -89,63 +101,144 @@ __device__ __forceinline__ void write_partials(const SysView& v, int region, dou
 }
 
 // ---------------------------------------------------------------------------
-// water(i) - water(j)
+// water(i) - water(j), tile form.  One CTA per 32-water i-group.  The waters
+// the group needs (its union, stored as runs of consecutive slots) are copied
+// global -> shared with one cp.async.bulk per run, completing on an mbarrier.
+// Each i-water is handled by LPW lanes walking its list of union indices;
+// j sites come from shared memory (4 x 16-byte loads per molecule pair).
 // ---------------------------------------------------------------------------
+constexpr int WT = GRPW * LPW;  // threads per CTA
+constexpr uint32_t WAIT_LIMIT = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: gives up after WAIT_LIMIT polls and reports it
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* timeout_flag) {
+    for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicExch(timeout_flag, 1u);
+    return false;
+}
+
+// Issues the bulk copies that bring union entries [lo, hi) of group g (from
+// its runs of consecutive slots) into buf; one lane per run.  Called by one
+// whole warp; lane 0 arms the barrier with the byte count.
+__device__ __forceinline__ uint32_t stage_chunk(const SysView& v, uint32_t g, uint32_t lo, uint32_t hi,
+                                                float4* buf, uint64_t* bar, int lane) {
+    const uint32_t nloc = v.grp_nloc[g], nrun = v.grp_nrun[g];
+    const uint2* runs = v.grp_run + (size_t)g * v.cap_run;
+    if (lane == 0) mbar_expect_tx(bar, (hi - lo) * (uint32_t)(4 * sizeof(float4)));
+    __syncwarp();
+    for (uint32_t t = lane; t < nrun; t += 32) {
+        const uint2 r = runs[t];
+        const uint32_t end = t + 1 < nrun ? runs[t + 1].y : nloc;
+        const uint32_t a = max(r.y, lo), e = min(end, hi);
+        if (a < e)
+            bulk_g2s(buf + (size_t)(a - lo) * 4, v.wpos + (size_t)(r.x + (a - r.y)) * 4,
+                     (e - a) * (uint32_t)(4 * sizeof(float4)), bar);
+    }
+    return hi - lo;
+}
+
 template <bool ENERGY>
-__global__ void __launch_bounds__(PT) k_pair_ww(SysView v) {
-    const int lane = threadIdx.x & 31;
-    const int ii = lane & 7, jq = lane >> 3;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+__global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
+    extern __shared__ __align__(128) float4 tile[];  // the group's union, 4 float4 per water
+    __shared__ __align__(8) uint64_t bar;
+    const int tid = threadIdx.x;
+    const int il = tid / LPW, l = tid % LPW;
     const uint32_t nwc = v.sc->n_wclus;
+    const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
+    const uint32_t nslots = nwc * WCL;
     const BoxDev b = *v.box;
-    const float rc2 = v.rc2, ljc2 = v.ljc2, alpha = v.alpha;
-    const float c2a = 2.0f * alpha * INV_SQRT_PI_F;
+    const float ljc2 = v.ljc2;
     const float sig2 = OPC_O_SIGMA * OPC_O_SIGMA;
     const float qhh = OPC_Q_H * OPC_Q_H, qhm = OPC_Q_H * OPC_Q_EP, qmm = OPC_Q_EP * OPC_Q_EP;
+    if (tid == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    uint32_t parity = 0;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t ci = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < nwc; ci += nwarps) {
-        const uint32_t si = ci * WCL + ii;
-        const bool vi = v.wid[si] != INVALID_ID;
-        const float3 iO = xyz(v.wpos[4 * si + 0]), iH0 = xyz(v.wpos[4 * si + 1]);
-        const float3 iH1 = xyz(v.wpos[4 * si + 2]), iM = xyz(v.wpos[4 * si + 3]);
-        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
-        Acc3 a{0.f, 0.f, 0.f};
-        const uint32_t n = v.ww_n[ci];
-        const uint32_t* lst = v.ww_j + (size_t)ci * v.cap_ww;
-        for (uint32_t k = 0; k < n; ++k) {
-            const uint32_t cj = lst[k];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int jj = jq + 4 * h;
-                const uint32_t sj = cj * WCL + jj;
-                const bool ok = vi && v.wid[sj] != INVALID_ID && !(cj == ci && jj == ii);
-                if (!ok) continue;
-                const float3 jO = xyz(v.wpos[4 * sj + 0]), jH0 = xyz(v.wpos[4 * sj + 1]);
-                const float3 jH1 = xyz(v.wpos[4 * sj + 2]), jM = xyz(v.wpos[4 * sj + 3]);
-                const float3 s = shift_of(iO - jO, b);
-                const float3 jOs = jO - s, jH0s = jH0 - s, jH1s = jH1 - s, jMs = jM - s;
-                lj<ENERGY>(iO - jOs, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
-                coul<ENERGY>(iH0 - jH0s, qhh, rc2, alpha, c2a, fH0, a);
-                coul<ENERGY>(iH0 - jH1s, qhh, rc2, alpha, c2a, fH0, a);
-                coul<ENERGY>(iH0 - jMs, qhm, rc2, alpha, c2a, fH0, a);
-                coul<ENERGY>(iH1 - jH0s, qhh, rc2, alpha, c2a, fH1, a);
-                coul<ENERGY>(iH1 - jH1s, qhh, rc2, alpha, c2a, fH1, a);
-                coul<ENERGY>(iH1 - jMs, qhm, rc2, alpha, c2a, fH1, a);
-                coul<ENERGY>(iM - jH0s, qhm, rc2, alpha, c2a, fM, a);
-                coul<ENERGY>(iM - jH1s, qhm, rc2, alpha, c2a, fM, a);
-                coul<ENERGY>(iM - jMs, qmm, rc2, alpha, c2a, fM, a);
-            }
+    for (uint32_t g = blockIdx.x; g < ng; g += gridDim.x) {
+        const uint32_t nloc = v.grp_nloc[g];
+        if (tid < 32 && nloc > 0) stage_chunk(v, g, 0, nloc, tile, &bar, tid);
+        const uint32_t s = g * GRPW + il;
+        const bool have = s < nslots;
+        const uint32_t n = have ? v.wnb_n[s] : 0u;
+        float3 iO = f3(0, 0, 0), iH0 = iO, iH1 = iO, iM = iO;
+        if (have) {
+            iO = xyz(v.wpos[4 * s + 0]); iH0 = xyz(v.wpos[4 * s + 1]);
+            iH1 = xyz(v.wpos[4 * s + 2]); iM = xyz(v.wpos[4 * s + 3]);
         }
-        fO = f3(red4(fO.x), red4(fO.y), red4(fO.z));
-        fH0 = f3(red4(fH0.x), red4(fH0.y), red4(fH0.z));
-        fH1 = f3(red4(fH1.x), red4(fH1.y), red4(fH1.z));
-        fM = f3(red4(fM.x), red4(fM.y), red4(fM.z));
-        if (jq == 0) {
-            long long* p = v.wforce + (size_t)si * 12;
+        if (nloc > 0) {
+            const bool ok = mbar_wait(&bar, parity, &v.sc->timeout);
+            if (!__syncthreads_and(ok)) {
+                // give the copies in flight one more bounded chance, then stop
+                if (!ok) mbar_wait(&bar, parity, &v.sc->timeout);
+                break;
+            }
+            parity ^= 1u;
+        }
+        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
+        Acc3 a{0.0, 0.0, 0.f};
+        const uint16_t* lst = v.wnb + (size_t)s * v.cap_nb;
+        for (uint32_t k = l; k < n; k += LPW) {
+            const float4* jw = tile + 4 * (uint32_t)lst[k];
+            const float3 jO = xyz(jw[0]), jH0 = xyz(jw[1]), jH1 = xyz(jw[2]), jM = xyz(jw[3]);
+            const float3 sh = shift_of(iO - jO, b);
+            const float3 jOs = jO - sh, jH0s = jH0 - sh, jH1s = jH1 - sh, jMs = jM - sh;
+            lj<ENERGY>(iO - jOs, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
+            coul<ENERGY>(iH0 - jH0s, qhh, v, fH0, a);
+            coul<ENERGY>(iH0 - jH1s, qhh, v, fH0, a);
+            coul<ENERGY>(iH0 - jMs, qhm, v, fH0, a);
+            coul<ENERGY>(iH1 - jH0s, qhh, v, fH1, a);
+            coul<ENERGY>(iH1 - jH1s, qhh, v, fH1, a);
+            coul<ENERGY>(iH1 - jMs, qhm, v, fH1, a);
+            coul<ENERGY>(iM - jH0s, qhm, v, fM, a);
+            coul<ENERGY>(iM - jH1s, qhm, v, fM, a);
+            coul<ENERGY>(iM - jMs, qmm, v, fM, a);
+        }
+#pragma unroll
+        for (int o = 1; o < LPW; o <<= 1) {
+            fO.x += __shfl_xor_sync(0xffffffffu, fO.x, o); fO.y += __shfl_xor_sync(0xffffffffu, fO.y, o);
+            fO.z += __shfl_xor_sync(0xffffffffu, fO.z, o);
+            fH0.x += __shfl_xor_sync(0xffffffffu, fH0.x, o); fH0.y += __shfl_xor_sync(0xffffffffu, fH0.y, o);
+            fH0.z += __shfl_xor_sync(0xffffffffu, fH0.z, o);
+            fH1.x += __shfl_xor_sync(0xffffffffu, fH1.x, o); fH1.y += __shfl_xor_sync(0xffffffffu, fH1.y, o);
+            fH1.z += __shfl_xor_sync(0xffffffffu, fH1.z, o);
+            fM.x += __shfl_xor_sync(0xffffffffu, fM.x, o); fM.y += __shfl_xor_sync(0xffffffffu, fM.y, o);
+            fM.z += __shfl_xor_sync(0xffffffffu, fM.z, o);
+        }
+        if (l == 0 && have) {
+            long long* p = v.wforce + (size_t)s * 12;
             store_fix3(p + 0, fO); store_fix3(p + 3, fH0); store_fix3(p + 6, fH1); store_fix3(p + 9, fM);
         }
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
+        __syncthreads();  // the tile is refilled by the next group's copies
     }
     write_partials<ENERGY>(v, REG_WW, el, ec, ew);
 }
@@ -160,8 +253,7 @@ __global__ void __launch_bounds__(PT) k_pair_ws(SysView v) {
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nwc = v.sc->n_wclus;
     const BoxDev b = *v.box;
-    const float rc2 = v.rc2, ljc2 = v.ljc2, alpha = v.alpha;
-    const float c2a = 2.0f * alpha * INV_SQRT_PI_F;
+    const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
     for (uint32_t ci = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < nwc; ci += nwarps) {
         const uint32_t n = v.ws_n[ci];
@@ -171,7 +263,7 @@ __global__ void __launch_bounds__(PT) k_pair_ws(SysView v) {
         const float3 iO = xyz(v.wpos[4 * si + 0]), iH0 = xyz(v.wpos[4 * si + 1]);
         const float3 iH1 = xyz(v.wpos[4 * si + 2]), iM = xyz(v.wpos[4 * si + 3]);
         float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
-        Acc3 a{0.f, 0.f, 0.f};
+        Acc3 a{0.0, 0.0, 0.f};
         const uint32_t* lst = v.ws_j + (size_t)ci * v.cap_ws;
         for (uint32_t k = 0; k < n; ++k) {
             const uint32_t cj = lst[k];
@@ -186,9 +278,9 @@ __global__ void __launch_bounds__(PT) k_pair_ws(SysView v) {
                 const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
                 const float ep = sqrtf(OPC_O_EPS * lj_j.y);
                 lj<ENERGY>(iO - jp, sg * sg, ep, ljc2, 1.0f, fO, a);
-                coul<ENERGY>(iH0 - jp, OPC_Q_H * pj.w, rc2, alpha, c2a, fH0, a);
-                coul<ENERGY>(iH1 - jp, OPC_Q_H * pj.w, rc2, alpha, c2a, fH1, a);
-                coul<ENERGY>(iM - jp, OPC_Q_EP * pj.w, rc2, alpha, c2a, fM, a);
+                coul<ENERGY>(iH0 - jp, OPC_Q_H * pj.w, v, fH0, a);
+                coul<ENERGY>(iH1 - jp, OPC_Q_H * pj.w, v, fH1, a);
+                coul<ENERGY>(iM - jp, OPC_Q_EP * pj.w, v, fM, a);
             }
         }
         fO = f3(red4(fO.x), red4(fO.y), red4(fO.z));
@@ -215,8 +307,7 @@ __global__ void __launch_bounds__(PT) k_pair_sw(SysView v) {
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nac = v.sc->n_aclus;
     const BoxDev b = *v.box;
-    const float rc2 = v.rc2, ljc2 = v.ljc2, alpha = v.alpha;
-    const float c2a = 2.0f * alpha * INV_SQRT_PI_F;
+    const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
     for (uint32_t ci = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < nac; ci += nwarps) {
         const uint32_t n = v.sw_n[ci];
@@ -229,7 +320,7 @@ __global__ void __launch_bounds__(PT) k_pair_sw(SysView v) {
         const float sg = 0.5f * (OPC_O_SIGMA + lji.x);
         const float ep = sqrtf(OPC_O_EPS * lji.y);
         float3 f = f3(0, 0, 0);
-        Acc3 a{0.f, 0.f, 0.f};
+        Acc3 a{0.0, 0.0, 0.f};
         const uint32_t* lst = v.sw_j + (size_t)ci * v.cap_sw;
         for (uint32_t k = 0; k < n; ++k) {
             const uint32_t cj = lst[k];
@@ -240,9 +331,9 @@ __global__ void __launch_bounds__(PT) k_pair_sw(SysView v) {
                 const float3 jO = xyz(v.wpos[4 * sj + 0]);
                 const float3 s = shift_of(xyz(pi) - jO, b);
                 lj<ENERGY>(xyz(pi) - (jO - s), sg * sg, ep, ljc2, 1.0f, f, a);
-                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 1]) - s), pi.w * OPC_Q_H, rc2, alpha, c2a, f, a);
-                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 2]) - s), pi.w * OPC_Q_H, rc2, alpha, c2a, f, a);
-                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 3]) - s), pi.w * OPC_Q_EP, rc2, alpha, c2a, f, a);
+                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 1]) - s), pi.w * OPC_Q_H, v, f, a);
+                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 2]) - s), pi.w * OPC_Q_H, v, f, a);
+                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 3]) - s), pi.w * OPC_Q_EP, v, f, a);
             }
         }
         f = f3(red4(f.x), red4(f.y), red4(f.z));
@@ -263,8 +354,7 @@ __global__ void __launch_bounds__(PT) k_pair_ss(SysView v) {
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nac = v.sc->n_aclus;
     const BoxDev b = *v.box;
-    const float rc2 = v.rc2, ljc2 = v.ljc2, alpha = v.alpha;
-    const float c2a = 2.0f * alpha * INV_SQRT_PI_F;
+    const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
     for (uint32_t ci = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < nac; ci += nwarps) {
         const uint32_t si = ci * ACL + ii;
@@ -272,7 +362,7 @@ __global__ void __launch_bounds__(PT) k_pair_ss(SysView v) {
         const float4 pi = v.spos[si];
         const float2 lji = v.slj[si];
         float3 f = f3(0, 0, 0);
-        Acc3 a{0.f, 0.f, 0.f};
+        Acc3 a{0.0, 0.0, 0.f};
         const uint32_t n = v.ss_n[ci];
         const uint32_t* lst = v.ss_j + (size_t)ci * v.cap_ss;
         const unsigned long long* msk = v.ss_mask + (size_t)ci * v.cap_ss;
@@ -289,7 +379,7 @@ __global__ void __launch_bounds__(PT) k_pair_ss(SysView v) {
                 const float3 d = min_image_rint(xyz(pi) - xyz(pj), b);
                 const float sg = 0.5f * (lji.x + ljj.x);
                 lj<ENERGY>(d, sg * sg, sqrtf(lji.y * ljj.y), ljc2, 1.0f, f, a);
-                coul<ENERGY>(d, pi.w * pj.w, rc2, alpha, c2a, f, a);
+                coul<ENERGY>(d, pi.w * pj.w, v, f, a);
             }
         }
         f = f3(red4(f.x), red4(f.y), red4(f.z));
@@ -306,18 +396,17 @@ __global__ void __launch_bounds__(PT) k_pair_ss(SysView v) {
 template <bool ENERGY>
 __global__ void k_pair14(SysView v) {
     const BoxDev b = *v.box;
-    const float c2a = 2.0f * v.alpha * INV_SQRT_PI_F;
     double e_acc = 0.0, w_acc = 0.0;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < v.n14; k += gridDim.x * blockDim.x) {
         const uint2 p = v.p14[k];
         const float4 par = v.p14_par[k];  // sigma, eps, qq
         const float3 d = min_image_rint(xyz(v.apos[p.x]) - xyz(v.apos[p.y]), b);
         float3 f = f3(0, 0, 0);
-        Acc3 a{0.f, 0.f, 0.f};
+        Acc3 a{0.0, 0.0, 0.f};
         lj<ENERGY>(d, par.x * par.x, par.y, v.ljc2, 0.5f, f, a);
         float3 fc = f3(0, 0, 0);
-        Acc3 ac{0.f, 0.f, 0.f};
-        coul<ENERGY>(d, par.z, v.rc2, v.alpha, c2a, fc, ac);
+        Acc3 ac{0.0, 0.0, 0.f};
+        coul<ENERGY>(d, par.z, v, fc, ac);
         const float s = 0.833333333f;
         f = f + fc * s;
         add_fix3(v.aforce + 3 * (size_t)p.x, f);
@@ -339,6 +428,19 @@ inline int pblocks(const SysView& v, uint64_t warps) {
 namespace dyn {
 
 int pair_blocks_ww(const SysView& v) { return pblocks(v, v.nwclus_cap); }
+
+int ww_tile_blocks(const SysView& v) {
+    return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
+}
+
+size_t ww_tile_smem(const SysView& v) { return (size_t)v.cap_union * 4 * sizeof(float4); }
+
+int pair_ww_setup(const SysView& v) {
+    const int bytes = (int)ww_tile_smem(v);
+    DYN_CUDA(cudaFuncSetAttribute(k_pair_ww_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    DYN_CUDA(cudaFuncSetAttribute(k_pair_ww_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    return DYN_OK;
+}
 int pair_blocks_ss(const SysView& v) { return pblocks(v, v.naclus_cap); }
 int pair14_blocks(const SysView& v) {
     uint64_t bl = (v.n14 + 255) / 256;
@@ -348,15 +450,17 @@ int pair14_blocks(const SysView& v) {
 
 void launch_pairs(const SysView& v, cudaStream_t st, bool energy) {
     const int bw = pblocks(v, v.nwclus_cap), ba = pblocks(v, v.naclus_cap);
+    const int bt = ww_tile_blocks(v);
+    const size_t sm = ww_tile_smem(v);
     if (energy) {
-        if (v.nw) k_pair_ww<true><<<bw, PT, 0, st>>>(v);
+        if (v.nw) k_pair_ww_tile<true><<<bt, WT, sm, st>>>(v);
         if (v.na) k_pair_ss<true><<<ba, PT, 0, st>>>(v);
         if (v.nw && v.na) {
             k_pair_ws<true><<<bw, PT, 0, st>>>(v);
             k_pair_sw<true><<<ba, PT, 0, st>>>(v);
         }
     } else {
-        if (v.nw) k_pair_ww<false><<<bw, PT, 0, st>>>(v);
+        if (v.nw) k_pair_ww_tile<false><<<bt, WT, sm, st>>>(v);
         if (v.na) k_pair_ss<false><<<ba, PT, 0, st>>>(v);
         if (v.nw && v.na) {
             k_pair_ws<false><<<bw, PT, 0, st>>>(v);

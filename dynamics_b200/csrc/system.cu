@@ -47,6 +47,35 @@ int upload(dyn_sys_s* h, T* d, const T* src, size_t n) {
 }
 
 inline uint32_t round8(uint32_t x) { return (x + 7u) / 8u * 8u; }
+inline uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1u) / m * m; }
+
+// Chebyshev interpolation of f(x) on x = xmax (s + 1) / 2, s in [-1, 1],
+// at NPOLY Chebyshev nodes, converted to power-basis coefficients in s.
+template <typename F>
+void cheb_poly(F f, double xmax, float* out) {
+    const int n = NPOLY;
+    double c[NPOLY];
+    for (int k = 0; k < n; ++k) {
+        double sum = 0.0;
+        for (int j = 0; j < n; ++j) {
+            const double th = M_PI * (j + 0.5) / n;
+            sum += f(xmax * (std::cos(th) + 1.0) * 0.5) * std::cos(k * th);
+        }
+        c[k] = 2.0 / n * sum;
+    }
+    c[0] *= 0.5;
+    double T[NPOLY][NPOLY] = {};
+    T[0][0] = 1.0;
+    if (n > 1) T[1][1] = 1.0;
+    for (int k = 1; k + 1 < n; ++k)
+        for (int m = 0; m < n; ++m)
+            T[k + 1][m] = (m > 0 ? 2.0 * T[k][m - 1] : 0.0) - T[k - 1][m];
+    for (int m = 0; m < n; ++m) {
+        double p = 0.0;
+        for (int k = 0; k < n; ++k) p += c[k] * T[k][m];
+        out[m] = (float)p;
+    }
+}
 
 // Water M site from O, H0, H1 on the host (src/solvent/mod.rs:411-422).
 void host_m_site(const float* o, const float* h0, const float* h1, float* m) {
@@ -58,7 +87,7 @@ void host_m_site(const float* o, const float* h0, const float* h1, float* m) {
 
 void set_block_counts(SysView& v) {
     for (int r = 0; r < NREGION; ++r) v.nb[r] = 0;
-    v.nb[REG_WW] = v.nw ? dyn::pair_blocks_ww(v) : 0;
+    v.nb[REG_WW] = v.nw ? dyn::ww_tile_blocks(v) : 0;
     v.nb[REG_WS] = (v.nw && v.na) ? dyn::pair_blocks_ww(v) : 0;
     v.nb[REG_SW] = (v.nw && v.na) ? dyn::pair_blocks_ss(v) : 0;
     v.nb[REG_SS] = v.na ? dyn::pair_blocks_ss(v) : 0;
@@ -119,6 +148,7 @@ int read_scalars(dyn_sys_s* h) {
         return dyn::fail(DYN_ERR_UNSUPPORTED, "cluster list capacity exceeded (list length " +
                                                   std::to_string(h->h_sc->overflow) + ")");
     if (h->h_sc->nonfinite) return dyn::fail(DYN_ERR_NONFINITE, "non-finite coordinates or forces");
+    if (h->h_sc->timeout) return dyn::fail(DYN_ERR_TIMEOUT, "a bounded device wait gave up");
     return DYN_OK;
 }
 
@@ -237,16 +267,18 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     v.com_interval = cfg->com_interval; v.recenter_interval = cfg->recenter_interval;
     for (int k = 0; k < 3; ++k) v.K[k] = cfg->grid[k];
 
-    // column grid: edge close to that of a cube holding 8 waters
+    // column grid: edge close to that of a cube holding one 32-water group
     const double vol = (double)ext[0] * ext[1] * ext[2];
     const double dens = (double)std::max<uint32_t>(1u, v.nw + v.na / 3) / vol;
-    const double edge = std::cbrt(8.0 / dens);
+    const double edge = std::cbrt((double)GRPW / dens);
     v.ncx = std::max(1u, (uint32_t)std::floor(ext[0] / edge));
     v.ncy = std::max(1u, (uint32_t)std::floor(ext[1] / edge));
     v.ncol = v.ncx * v.ncy;
-    v.nw_cap = v.nw ? round8(v.nw + 7 * v.ncol + 8) : 8;
+    // slots follow the column path without per-column padding; the tail is
+    // padded to whole 32-water groups
+    v.nw_cap = round_up(std::max(1u, v.nw), 2 * GRPW);
     v.nwclus_cap = v.nw_cap / WCL;
-    v.na_cap = v.na ? round8(v.na + 7 * v.ncol + 8) : 8;
+    v.na_cap = round8(v.na + 8);
     v.naclus_cap = v.na_cap / ACL;
     v.max_blocks = 148 * 16;
 
@@ -259,7 +291,34 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     };
     const double wcl_vol = v.nw ? vol / std::max(1.0, v.nw / 8.0) : vol;
     const double acl_vol = std::max(8.0 / 0.12, v.na ? 8.0 * vol / std::max(1u, v.nw * 4 + v.na) * 4.0 : vol);
-    v.cap_ww = v.nw ? est(v.r_ww, wcl_vol, v.nwclus_cap) : 1;
+    // water-water: 32-water groups; candidate clusters within r_ww of the
+    // group box; the union of needed waters; molecule lists within r_ww
+    // (liquid density as the bound)
+    const double dl = std::max(0.0334, v.nw / vol);
+    v.ngrp_cap = v.nw_cap / GRPW;
+    {
+        const double r = v.r_ww;
+        auto mink = [&](double a) {
+            return a * a * a + 6.0 * a * a * r + 3.0 * M_PI * a * r * r + 4.0 / 3.0 * M_PI * r * r * r;
+        };
+        const double ag = 1.4 * std::cbrt(GRPW / dl), ac = 2.0 * std::cbrt(WCL / dl);
+        v.cap_tile = std::min<uint32_t>((uint32_t)(1.5 * mink(ag + ac) * dl / WCL) + 16,
+                                        std::max<uint32_t>(1u, v.nwclus_cap));
+        v.cap_union = std::min<uint32_t>((uint32_t)(1.4 * mink(ag) * dl) + 64, 3200u);
+        v.cap_union = std::min<uint32_t>(v.cap_union, v.nw_cap);
+        v.cap_run = 256;
+        const double nb = 4.0 / 3.0 * M_PI * r * r * r * dl;
+        v.cap_nb = std::min<uint32_t>((uint32_t)(1.5 * nb) + 32, 65535u);
+    }
+    // screened-Coulomb polynomials on r in [0, rc]
+    {
+        const double a = v.alpha, xmax = (double)v.alpha * (double)v.rc;
+        (void)a;
+        cheb_poly([](double x) { return std::erfc(x) + 2.0 / std::sqrt(M_PI) * x * std::exp(-x * x); }, xmax,
+                  v.poly_f);
+        cheb_poly([](double x) { return std::erfc(x); }, xmax, v.poly_e);
+        v.two_over_rc = 2.0f / v.rc;
+    }
     v.cap_ws = (v.nw && v.na) ? est(v.r_ws, acl_vol, v.naclus_cap) : 1;
     v.cap_sw = (v.nw && v.na) ? est(v.r_ws, wcl_vol, v.nwclus_cap) : 1;
     v.cap_ss = v.na ? est(v.r_ss, acl_vol, v.naclus_cap) : 1;
@@ -307,8 +366,16 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dev_alloc(h, &v.wbb_h, v.nwclus_cap));
     TRY(dev_alloc(h, &v.abb_c, v.naclus_cap));
     TRY(dev_alloc(h, &v.abb_h, v.naclus_cap));
-    TRY(dev_alloc(h, &v.ww_n, v.nwclus_cap));
-    TRY(dev_alloc(h, &v.ww_j, (size_t)v.nwclus_cap * v.cap_ww));
+    TRY(dev_alloc(h, &v.gbb_c, v.ngrp_cap));
+    TRY(dev_alloc(h, &v.gbb_h, v.ngrp_cap));
+    TRY(dev_alloc(h, &v.tile_n, v.ngrp_cap));
+    TRY(dev_alloc(h, &v.tile_j, (size_t)v.ngrp_cap * v.cap_tile));
+    TRY(dev_alloc(h, &v.grp_nrun, v.ngrp_cap));
+    TRY(dev_alloc(h, &v.grp_nloc, v.ngrp_cap));
+    TRY(dev_alloc(h, &v.grp_run, (size_t)v.ngrp_cap * v.cap_run));
+    TRY(dev_alloc(h, &v.cand_loc, (size_t)v.ngrp_cap * v.cap_tile * WCL));
+    TRY(dev_alloc(h, &v.wnb_n, v.nw_cap));
+    TRY(dev_alloc(h, &v.wnb, (size_t)v.nw_cap * v.cap_nb));
     TRY(dev_alloc(h, &v.ws_n, v.nwclus_cap));
     TRY(dev_alloc(h, &v.ws_j, (size_t)v.nwclus_cap * v.cap_ws));
     TRY(dev_alloc(h, &v.sw_n, v.naclus_cap));
@@ -464,6 +531,7 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     h->allocs.push_back(v.qgrid_fix); h->allocs.push_back(v.qgrid); h->allocs.push_back(v.cgrid);
     for (int a = 0; a < 3; ++a) h->allocs.push_back(v.bmod[a]);
     set_block_counts(v);
+    if (v.nw) TRY(dyn::pair_ww_setup(v));
     TRYC(cudaStreamSynchronize(h->stream));
     // prime: first list build and forces -> accelerations
     enqueue_forces(h, true);
