@@ -20,6 +20,7 @@ DYN_ERR_NONFINITE = -5
 DYN_ERR_TIMEOUT = -6
 DYN_ERR_UNSUPPORTED = -7
 
+DYN_NB_STATIC_MAX_SITES = 131072
 DYN_OVR_COULOMB_DISABLED = 1
 DYN_OVR_LJ_DISABLED = 2
 DYN_PAIR_SCALE14 = 1
@@ -108,6 +109,9 @@ _SIGS = {
                             C.c_float, _P], C.c_int),
     "dyn_nb_get_pairs": ([_P, C.c_uint64] + [_P] * 9, C.c_int),
     "dyn_nb_forces": ([_P, _P, _P, _P, _P, _P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, _P], C.c_int),
+    "dyn_nb_forces_static": ([_P, C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P, C.c_uint64]
+                             + [_P] * 9 + [_P, C.c_float, C.c_float, C.c_float, C.c_uint32]
+                             + [_P] * 6, C.c_int),
     "dyn_nb_destroy": ([_P], C.c_int),
     "dyn_sys_create": ([_P, _P, _P, _P], C.c_int),
     "dyn_sys_step": ([_P, C.c_uint32, C.c_float], C.c_int),

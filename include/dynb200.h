@@ -152,6 +152,40 @@ int dyn_nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o, const 
 /* Releases everything dyn_nb_create allocated. */
 int dyn_nb_destroy(dyn_nb_t h);
 
+/* Largest n_dyn + 4*n_water that dyn_nb_forces_static accepts. */
+#define DYN_NB_STATIC_MAX_SITES 131072u
+
+/* No counterpart in the reference.  The pair-force evaluation of
+ * dyn_nb_forces for callers that must not allocate device memory (a host
+ * framework that owns every device buffer through its own pool, or code
+ * running where a cudaMalloc could block or fail): no handle, every array
+ * is a DEVICE pointer owned by the caller, and the call allocates nothing
+ * (no cudaMalloc / cudaFree / allocating library routine).
+ *   Inputs: positions as in dyn_nb_forces (float [3*n] per body); the flat
+ *   pair list in the unpacked form of dyn_nb_set_pairs (n_pairs entries per
+ *   array); cutoff_ewald, alpha_ewald and lj_cutoff as in dyn_nb_create.
+ *   Outputs: float64 [3*n] forces per body as in dyn_nb_forces, and
+ *   scalars[3] = {virial, energy, pairs skipped because of a body code > 4
+ *   or an index out of range}.
+ * Its scratch (64-bit fixed-point accumulators, block partials) is a
+ * fixed-size static device array sized for DYN_NB_STATIC_MAX_SITES sites,
+ * about 3 MiB, held on every device that loads the library until exit; a
+ * larger system is rejected with DYN_ERR_INVALID.  Every call on a device
+ * shares it: calls whose work overlaps on one device (unordered streams)
+ * race and give wrong results.  Each call clears what it uses first.  The
+ * call is asynchronous on `stream`; the first call on each device looks up
+ * the scratch address with that device current, so make it before any
+ * stream capture. */
+int dyn_nb_forces_static(void* stream, uint32_t n_dyn, uint32_t n_water, const float* pos_dyn,
+                         const float* pos_w_o, const float* pos_w_m, const float* pos_w_h0,
+                         const float* pos_w_h1, uint64_t n_pairs, const uint32_t* tgt,
+                         const uint32_t* src, const float* sigma, const float* eps,
+                         const float* q_tgt, const float* q_src, const uint8_t* body_tgt,
+                         const uint8_t* body_src, const uint8_t* flags,
+                         const float cell_extent[3], float cutoff_ewald, float alpha_ewald,
+                         float lj_cutoff, uint32_t override_bits, double* f_dyn, double* f_w_o,
+                         double* f_w_m, double* f_w_h0, double* f_w_h1, double* scalars);
+
 /* ------------------------------------------------------------------ */
 /* Layer 2: device-resident engine (MdState::step)                    */
 /* ------------------------------------------------------------------ */
