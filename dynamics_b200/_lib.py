@@ -60,6 +60,7 @@ class Config(C.Structure):
         ("spme_interval", C.c_uint32), ("com_interval", C.c_uint32),
         ("recenter_interval", C.c_uint32), ("energy_interval", C.c_uint32),
         ("flags", C.c_uint32), ("thermo_dof", C.c_uint32), ("seed", C.c_uint64),
+        ("ww_union_chunk", C.c_uint32), ("reserved0", C.c_uint32),
     ]
 
 
@@ -88,7 +89,7 @@ class Energies(C.Structure):
         "virial_bonded", "virial_constraints", "pressure_bar", "temperature")] + [
         ("box", C.c_double * 3), ("step", C.c_uint64), ("list_rebuilds", C.c_uint64),
         ("pairs_in_list", C.c_uint64), ("kinetic_rigid", C.c_double),
-        ("pressure_atomic_bar", C.c_double)]
+        ("pressure_atomic_bar", C.c_double), ("list_union_max", C.c_uint64)]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_ if n != "box"}
@@ -124,6 +125,7 @@ _SIGS = {
     "dyn_sys_step_host": ([_P, C.c_uint32, C.c_float] + [_P] * 9, C.c_int),
     "dyn_sys_stage_times": ([_P, C.c_uint32, C.c_float, _P], C.c_int),
     "dyn_sys_launches_per_step": ([_P, C.c_int, _P], C.c_int),
+    "dyn_sys_launches_conditional": ([_P, _P, _P], C.c_int),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -56,6 +56,10 @@ struct Scalars {
     double ke_rigid;              // rigid-body KE of the waters + atomic KE of atoms
     double pressure_atomic;       // the reference's site-virial pressure
     unsigned long long list_pairs;
+    unsigned int ctr_disp;        // blocks done in k_disp_check (last one decides)
+    unsigned int ctr_scale;       // blocks done in k_scale (last one scales the box)
+    unsigned int union_max;       // largest group union of the last rebuild
+    unsigned int pad2;
 };
 
 // Partial-sum regions (each kernel family writes 4 doubles per block).
@@ -111,6 +115,7 @@ struct SysView {
     // consecutive slots (staged in shared memory by bulk copies), and per
     // i-water a list of indices into that union
     uint32_t ngrp_cap, cap_tile, cap_nb, cap_union, cap_run;
+    uint32_t union_chunk;         // waters staged in shared memory at a time
     float4* gbb_c; float4* gbb_h;
     uint32_t* tile_n; uint32_t* tile_j;      // [ngrp_cap], [ngrp_cap*cap_tile]
     uint32_t* grp_nrun; uint32_t* grp_nloc;  // [ngrp_cap]
@@ -150,6 +155,11 @@ struct SysView {
     // power basis, Horner in float32): force = qq u / r^3, energy = qq erfc / r
     float poly_f[NPOLY], poly_e[NPOLY];
     float two_over_rc;
+    // IF-node handles of the captured step graph: the displacement check
+    // sets cond_rebuild, the step finalisation sets cond_periodic; only
+    // kernels captured for a graph (use_cond != 0) set them
+    cudaGraphConditionalHandle cond_rebuild, cond_periodic;
+    uint32_t use_cond;
     uint32_t nb[NREGION];   // blocks each region's kernel is launched with
 };
 
@@ -187,7 +197,6 @@ void launch_second_half(const SysView& v, cudaStream_t st, float dt);
 void launch_finalize(const SysView& v, cudaStream_t st, float dt, bool energy, bool thermo);
 void launch_periodic(const SysView& v, cudaStream_t st);
 void launch_bonded(const SysView& v, cudaStream_t st, bool energy);
-void launch_step_end(const SysView& v, cudaStream_t st);
 int kick_blocks_w(const SysView& v);
 int kick_blocks_a(const SysView& v);
 int bond_blocks(const SysView& v);

@@ -387,6 +387,17 @@ __global__ void k_finalize(SysView v, float dt, bool thermo) {
                  sc->acc[ACC_E_RECIP] + sc->acc[ACC_E_CORR] + sc->acc[ACC_E_BONDED];
         sc->pe = pe;
     }
+    if (thermo) {
+        // the step is complete; the periodic tasks that follow see its number
+        const uint64_t next = sc->step + 1;
+        unsigned int due = 0u;
+        if ((v.flags & DYN_FLAG_COM_REMOVAL) && v.com_interval && next % v.com_interval == 0) due = 1u;
+        if ((v.flags & DYN_FLAG_RECENTER) && v.recenter_interval && v.na && next % v.recenter_interval == 0)
+            due = 1u;
+        if ((v.flags & DYN_FLAG_RESET_ANGLE) && v.nw && next % 1000 == 0) due = 1u;
+        sc->step = next;
+        if (v.use_cond) cudaGraphSetConditional(v.cond_periodic, due);
+    }
 }
 
 // velocity scaling (CSVR) and C-rescale of positions / box
@@ -430,25 +441,28 @@ __global__ void k_scale(SysView v) {
             v.apos[a] = p;
         }
     }
-}
-
-__global__ void k_scale_box(SysView v) {
-    const double mu = v.sc->baro_mu;
-    if (mu == 1.0) return;
-    BoxDev b = *v.box;
+    if (mu_d == 1.0) return;
+    // the box itself is scaled (about its centre) by the last block to
+    // finish, after every block has read the old one
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    __threadfence();
+    if (atomicAdd(&v.sc->ctr_scale, 1u) != gridDim.x - 1) return;
+    BoxDev nb = b;
     for (int k = 0; k < 3; ++k) {
         const double c = (double)b.lo[k] + 0.5 * (double)b.ext[k];
-        const double e = (double)b.ext[k] * mu;
-        b.lo[k] = (float)(c - 0.5 * e);
-        b.ext[k] = (float)e;
-        b.inv_ext[k] = (float)(1.0 / e);
+        const double e = (double)b.ext[k] * mu_d;
+        nb.lo[k] = (float)(c - 0.5 * e);
+        nb.ext[k] = (float)e;
+        nb.inv_ext[k] = (float)(1.0 / e);
     }
-    *v.box = b;
+    *v.box = nb;
+    v.sc->ctr_scale = 0u;
 }
 
 // COM motion removal (src/com_zero.rs:57-81) every com_interval steps
 __global__ void k_com_reduce(SysView v) {
-    const uint64_t next = v.sc->step + 1;
+    const uint64_t next = v.sc->step;  // advanced by k_finalize
     const bool on = (v.flags & DYN_FLAG_COM_REMOVAL) && v.com_interval && (next % v.com_interval == 0);
     double x[4] = {0, 0, 0, 0};
     if (on) {
@@ -472,7 +486,7 @@ __global__ void k_com_reduce(SysView v) {
 }
 
 __global__ void k_com_apply(SysView v) {
-    const uint64_t next = v.sc->step + 1;
+    const uint64_t next = v.sc->step;  // advanced by k_finalize
     const bool on = (v.flags & DYN_FLAG_COM_REMOVAL) && v.com_interval && (next % v.com_interval == 0);
     if (!on) return;
     __shared__ float3 vc;
@@ -508,7 +522,7 @@ __global__ void k_com_apply(SysView v) {
 
 // SimBox::recenter (src/barostat.rs:111-137) every recenter_interval steps
 __global__ void k_recenter(SysView v) {
-    const uint64_t next = v.sc->step + 1;
+    const uint64_t next = v.sc->step;  // advanced by k_finalize
     const bool on = (v.flags & DYN_FLAG_RECENTER) && v.recenter_interval && v.na &&
                     (next % v.recenter_interval == 0);
     if (!on) return;
@@ -528,7 +542,7 @@ __global__ void k_recenter(SysView v) {
 
 // reset_angle (src/solvent/opc_settle.rs:202-219) every 1000 steps
 __global__ void k_reset_angle(SysView v) {
-    const uint64_t next = v.sc->step + 1;
+    const uint64_t next = v.sc->step;  // advanced by k_finalize
     if (!(v.flags & DYN_FLAG_RESET_ANGLE) || next % 1000 != 0) return;
     const BoxDev b = *v.box;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
@@ -553,7 +567,6 @@ __global__ void k_reset_angle(SysView v) {
     }
 }
 
-__global__ void k_step_end(SysView v) { v.sc->step += 1ull; }
 
 inline int iblocks(const SysView& v, uint64_t n) {
     uint64_t bl = (n + IT - 1) / IT;
@@ -586,7 +599,6 @@ void launch_finalize(const SysView& v, cudaStream_t st, float dt, bool energy, b
                         v.barostat == DYN_BARO_CRESCALE;
     if (!scales) return;
     k_scale<<<iblocks(v, (uint64_t)v.nw_cap + v.na), IT, 0, st>>>(v);
-    if (v.barostat == DYN_BARO_CRESCALE) k_scale_box<<<1, 1, 0, st>>>(v);
 }
 
 void launch_periodic(const SysView& v, cudaStream_t st) {
@@ -598,6 +610,5 @@ void launch_periodic(const SysView& v, cudaStream_t st) {
     if ((v.flags & DYN_FLAG_RESET_ANGLE) && v.nw) k_reset_angle<<<iblocks(v, v.nw_cap), IT, 0, st>>>(v);
 }
 
-void launch_step_end(const SysView& v, cudaStream_t st) { k_step_end<<<1, 1, 0, st>>>(v); }
 
 }  // namespace dyn

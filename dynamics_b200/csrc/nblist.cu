@@ -14,8 +14,9 @@
 //      water a compact list of tile-local molecule indices (O-O distance
 //      below cutoff + twice the O-H reach + buffer).
 // Every kernel of the rebuild returns immediately unless the displacement
-// check raised Scalars::need_rebuild, so the whole step is one static CUDA
-// graph.  The rebuild criterion is the reference's: max displacement since
+// check raised Scalars::need_rebuild; inside a captured step graph the
+// rebuild kernels also sit under a conditional (IF) node that the check
+// sets, so steps without a rebuild launch none of them.  The rebuild criterion is the reference's: max displacement since
 // the last rebuild >= buffer / 2 (src/neighbors.rs:159-169), tracking water
 // O only (src/neighbors.rs:71-82); water list radii add twice the O-H reach.
 #include <algorithm>
@@ -69,15 +70,24 @@ __global__ void k_disp_check(SysView v) {
         m = fmaxf(m, isfinite(d2) ? d2 : 1e30f);
     }
     m = warp_max_f(m);
-    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(&v.sc->max_disp2_bits, __float_as_uint(m));
-}
-
-__global__ void k_disp_decide(SysView v) {
-    const float m = __uint_as_float(v.sc->max_disp2_bits);
+    if ((threadIdx.x & 31) == 0 && m > 0.f) {
+        atomicMax(&v.sc->max_disp2_bits, __float_as_uint(m));
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    if (atomicAdd(&v.sc->ctr_disp, 1u) != gridDim.x - 1) return;
+    // the last block to finish sees every block's maximum and decides:
+    // rebuild when the largest displacement reaches half the buffer
+    __threadfence();
+    const float mx = __uint_as_float(atomicExch(&v.sc->max_disp2_bits, 0u));
     const float h = 0.5f * v.buffer;
-    if (m >= h * h) v.sc->need_rebuild = 1u;
-    if (m >= 1e29f) v.sc->nonfinite = 1u;
-    v.sc->max_disp2_bits = 0u;
+    unsigned int need = v.sc->need_rebuild;
+    if (mx >= h * h) need = 1u;
+    v.sc->need_rebuild = need;
+    if (mx >= 1e29f) v.sc->nonfinite = 1u;
+    v.sc->ctr_disp = 0u;
+    if (v.use_cond) cudaGraphSetConditional(v.cond_rebuild, need);
 }
 
 // ---------------------------------------------------------------------------
@@ -85,6 +95,10 @@ __global__ void k_disp_decide(SysView v) {
 // ---------------------------------------------------------------------------
 __global__ void k_col_clear(SysView v, bool force) {
     if (!rebuild_on(v, force)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        v.sc->list_pairs = 0ull;
+        v.sc->union_max = 0u;
+    }
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= v.ncol; c += gridDim.x * blockDim.x) {
         if (c < v.ncol) {
             v.col_count[c] = 0; v.col_fill[c] = 0;
@@ -483,6 +497,7 @@ __global__ void __launch_bounds__(UT) k_group_union(SysView v, bool force) {
             v.grp_nloc[g] = min(base_cnt, v.cap_union);
             v.grp_nrun[g] = min(base_run, v.cap_run);
             if (base_cnt > v.cap_union) atomicMax(&v.sc->overflow, base_cnt);
+            atomicMax(&v.sc->union_max, base_cnt);
             if (base_run > v.cap_run) atomicMax(&v.sc->overflow, base_run);
         }
         __syncthreads();
@@ -526,11 +541,6 @@ __global__ void k_rebuild_done(SysView v, bool force) {
     v.sc->rebuilds += 1ull;
 }
 
-__global__ void k_list_pairs_reset(SysView v, bool force) {
-    if (!rebuild_on(v, force)) return;
-    v.sc->list_pairs = 0ull;
-}
-
 __global__ void k_gather_atoms(SysView v) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.na_cap; s += gridDim.x * blockDim.x) {
         const uint32_t a = v.sidx[s];
@@ -550,7 +560,6 @@ namespace dyn {
 
 void launch_displacement_check(const SysView& v, cudaStream_t st) {
     k_disp_check<<<nblocks(v.nw_cap + v.na, 256), 256, 0, st>>>(v);
-    k_disp_decide<<<1, 1, 0, st>>>(v);
 }
 
 void launch_rebuild(const SysView& v, cudaStream_t st, bool force) {
@@ -565,7 +574,6 @@ void launch_rebuild(const SysView& v, cudaStream_t st, bool force) {
     k_perm_scatter<<<nblocks(nmax, T), T, 0, st>>>(v, force);
     k_perm_copyback<<<nblocks(v.nw_cap, T), T, 0, st>>>(v, force);
     k_bbox<<<nblocks(v.nwclus_cap + v.naclus_cap, T), T, 0, st>>>(v, force);
-    k_list_pairs_reset<<<1, 1, 0, st>>>(v, force);
     const int LT = 128;  // 4 warps per block, one i-cluster per warp
     if (v.nw) {
         k_group_bbox<<<nblocks(v.ngrp_cap, T), T, 0, st>>>(v, force);

@@ -19,6 +19,8 @@
 // reduced over the lanes sharing an i-body with shuffles and stored once as
 // int64 fixed point; the water-water and atom-atom kernels store (first
 // writers), the mixed kernels add.
+#include <algorithm>
+
 #include "engine.cuh"
 
 namespace {
@@ -103,9 +105,11 @@ __device__ __forceinline__ void write_partials(const SysView& v, int region, dou
 // ---------------------------------------------------------------------------
 // water(i) - water(j), tile form.  One CTA per 32-water i-group.  The waters
 // the group needs (its union, stored as runs of consecutive slots) are copied
-// global -> shared with one cp.async.bulk per run, completing on an mbarrier.
-// Each i-water is handled by LPW lanes walking its list of union indices;
-// j sites come from shared memory (4 x 16-byte loads per molecule pair).
+// global -> shared with one cp.async.bulk per run, completing on an mbarrier,
+// union_chunk waters at a time (one chunk for almost every group; the chunk
+// is sized so that two CTAs fit on an SM).  Each i-water is handled by LPW
+// lanes walking its list of union indices; j sites come from shared memory
+// (4 x 16-byte loads per molecule pair).
 // ---------------------------------------------------------------------------
 constexpr int WT = GRPW * LPW;  // threads per CTA
 constexpr uint32_t WAIT_LIMIT = 1u << 22;
@@ -167,13 +171,14 @@ __device__ __forceinline__ uint32_t stage_chunk(const SysView& v, uint32_t g, ui
 
 template <bool ENERGY>
 __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
-    extern __shared__ __align__(128) float4 tile[];  // the group's union, 4 float4 per water
+    extern __shared__ __align__(128) float4 tile[];  // union_chunk waters, 4 float4 each
     __shared__ __align__(8) uint64_t bar;
     const int tid = threadIdx.x;
     const int il = tid / LPW, l = tid % LPW;
     const uint32_t nwc = v.sc->n_wclus;
     const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
     const uint32_t nslots = nwc * WCL;
+    const uint32_t chunk = v.union_chunk;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     const float sig2 = OPC_O_SIGMA * OPC_O_SIGMA;
@@ -182,9 +187,10 @@ __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
     __syncthreads();
     uint32_t parity = 0;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t g = blockIdx.x; g < ng; g += gridDim.x) {
+    bool alive = true;
+    for (uint32_t g = blockIdx.x; g < ng && alive; g += gridDim.x) {
         const uint32_t nloc = v.grp_nloc[g];
-        if (tid < 32 && nloc > 0) stage_chunk(v, g, 0, nloc, tile, &bar, tid);
+        if (tid < 32 && nloc > 0) stage_chunk(v, g, 0, min(nloc, chunk), tile, &bar, tid);
         const uint32_t s = g * GRPW + il;
         const bool have = s < nslots;
         const uint32_t n = have ? v.wnb_n[s] : 0u;
@@ -193,34 +199,45 @@ __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
             iO = xyz(v.wpos[4 * s + 0]); iH0 = xyz(v.wpos[4 * s + 1]);
             iH1 = xyz(v.wpos[4 * s + 2]); iM = xyz(v.wpos[4 * s + 3]);
         }
-        if (nloc > 0) {
+        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
+        Acc3 a{0.0, 0.0, 0.f};
+        const uint16_t* lst = v.wnb + (size_t)s * v.cap_nb;
+        uint32_t k = l;  // this lane's next list entry (entries l, l + LPW, ...)
+        // a union larger than the shared buffer is processed in chunks; the
+        // lists hold ascending union indices, so each lane resumes where it
+        // stopped
+        for (uint32_t lo = 0; lo < nloc; lo += chunk) {
+            const uint32_t hi = min(nloc, lo + chunk);
+            if (lo > 0 && tid < 32) stage_chunk(v, g, lo, hi, tile, &bar, tid);
             const bool ok = mbar_wait(&bar, parity, &v.sc->timeout);
             if (!__syncthreads_and(ok)) {
                 // give the copies in flight one more bounded chance, then stop
                 if (!ok) mbar_wait(&bar, parity, &v.sc->timeout);
+                alive = false;
                 break;
             }
             parity ^= 1u;
+            for (; k < n; k += LPW) {
+                const uint32_t idx = lst[k];
+                if (idx >= hi) break;
+                const float4* jw = tile + 4 * (idx - lo);
+                const float3 jO = xyz(jw[0]), jH0 = xyz(jw[1]), jH1 = xyz(jw[2]), jM = xyz(jw[3]);
+                const float3 sh = shift_of(iO - jO, b);
+                const float3 jOs = jO - sh, jH0s = jH0 - sh, jH1s = jH1 - sh, jMs = jM - sh;
+                lj<ENERGY>(iO - jOs, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
+                coul<ENERGY>(iH0 - jH0s, qhh, v, fH0, a);
+                coul<ENERGY>(iH0 - jH1s, qhh, v, fH0, a);
+                coul<ENERGY>(iH0 - jMs, qhm, v, fH0, a);
+                coul<ENERGY>(iH1 - jH0s, qhh, v, fH1, a);
+                coul<ENERGY>(iH1 - jH1s, qhh, v, fH1, a);
+                coul<ENERGY>(iH1 - jMs, qhm, v, fH1, a);
+                coul<ENERGY>(iM - jH0s, qhm, v, fM, a);
+                coul<ENERGY>(iM - jH1s, qhm, v, fM, a);
+                coul<ENERGY>(iM - jMs, qmm, v, fM, a);
+            }
+            __syncthreads();  // the tile is refilled by the next chunk's or group's copies
         }
-        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
-        Acc3 a{0.0, 0.0, 0.f};
-        const uint16_t* lst = v.wnb + (size_t)s * v.cap_nb;
-        for (uint32_t k = l; k < n; k += LPW) {
-            const float4* jw = tile + 4 * (uint32_t)lst[k];
-            const float3 jO = xyz(jw[0]), jH0 = xyz(jw[1]), jH1 = xyz(jw[2]), jM = xyz(jw[3]);
-            const float3 sh = shift_of(iO - jO, b);
-            const float3 jOs = jO - sh, jH0s = jH0 - sh, jH1s = jH1 - sh, jMs = jM - sh;
-            lj<ENERGY>(iO - jOs, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
-            coul<ENERGY>(iH0 - jH0s, qhh, v, fH0, a);
-            coul<ENERGY>(iH0 - jH1s, qhh, v, fH0, a);
-            coul<ENERGY>(iH0 - jMs, qhm, v, fH0, a);
-            coul<ENERGY>(iH1 - jH0s, qhh, v, fH1, a);
-            coul<ENERGY>(iH1 - jH1s, qhh, v, fH1, a);
-            coul<ENERGY>(iH1 - jMs, qhm, v, fH1, a);
-            coul<ENERGY>(iM - jH0s, qhm, v, fM, a);
-            coul<ENERGY>(iM - jH1s, qhm, v, fM, a);
-            coul<ENERGY>(iM - jMs, qmm, v, fM, a);
-        }
+        if (!alive) break;
 #pragma unroll
         for (int o = 1; o < LPW; o <<= 1) {
             fO.x += __shfl_xor_sync(0xffffffffu, fO.x, o); fO.y += __shfl_xor_sync(0xffffffffu, fO.y, o);
@@ -238,7 +255,6 @@ __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
         }
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
-        __syncthreads();  // the tile is refilled by the next group's copies
     }
     write_partials<ENERGY>(v, REG_WW, el, ec, ew);
 }
@@ -433,12 +449,23 @@ int ww_tile_blocks(const SysView& v) {
     return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
 }
 
-size_t ww_tile_smem(const SysView& v) { return (size_t)v.cap_union * 4 * sizeof(float4); }
+size_t ww_tile_smem(const SysView& v) { return (size_t)v.union_chunk * 4 * sizeof(float4); }
 
+// The limit is a property of the kernel, shared by every system in the
+// process, so it is raised to the device maximum once rather than set to one
+// system's chunk size (which would break systems with larger chunks).
 int pair_ww_setup(const SysView& v) {
-    const int bytes = (int)ww_tile_smem(v);
-    DYN_CUDA(cudaFuncSetAttribute(k_pair_ww_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    DYN_CUDA(cudaFuncSetAttribute(k_pair_ww_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    int dev = 0, optin = 0;
+    DYN_CUDA(cudaGetDevice(&dev));
+    DYN_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fe, fn;
+    DYN_CUDA(cudaFuncGetAttributes(&fe, k_pair_ww_tile<true>));
+    DYN_CUDA(cudaFuncGetAttributes(&fn, k_pair_ww_tile<false>));
+    const int le = optin - (int)fe.sharedSizeBytes, ln = optin - (int)fn.sharedSizeBytes;
+    DYN_CHECK(ww_tile_smem(v) <= (size_t)std::min(le, ln), DYN_ERR_UNSUPPORTED,
+              "water-water chunk exceeds shared memory");
+    DYN_CUDA(cudaFuncSetAttribute(k_pair_ww_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, le));
+    DYN_CUDA(cudaFuncSetAttribute(k_pair_ww_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ln));
     return DYN_OK;
 }
 int pair_blocks_ss(const SysView& v) { return pblocks(v, v.naclus_cap); }
@@ -452,15 +479,21 @@ void launch_pairs(const SysView& v, cudaStream_t st, bool energy) {
     const int bw = pblocks(v, v.nwclus_cap), ba = pblocks(v, v.naclus_cap);
     const int bt = ww_tile_blocks(v);
     const size_t sm = ww_tile_smem(v);
+    // water-water short-range energy is part of the potential only with
+    // DYN_FLAG_FULL_ENERGY (the reference leaves it out,
+    // src/non_bonded.rs:335-342), so other energy steps skip it
+    const bool eww = energy && (v.flags & DYN_FLAG_FULL_ENERGY);
+    if (v.nw) {
+        if (eww) k_pair_ww_tile<true><<<bt, WT, sm, st>>>(v);
+        else k_pair_ww_tile<false><<<bt, WT, sm, st>>>(v);
+    }
     if (energy) {
-        if (v.nw) k_pair_ww_tile<true><<<bt, WT, sm, st>>>(v);
         if (v.na) k_pair_ss<true><<<ba, PT, 0, st>>>(v);
         if (v.nw && v.na) {
             k_pair_ws<true><<<bw, PT, 0, st>>>(v);
             k_pair_sw<true><<<ba, PT, 0, st>>>(v);
         }
     } else {
-        if (v.nw) k_pair_ww_tile<false><<<bt, WT, sm, st>>>(v);
         if (v.na) k_pair_ss<false><<<ba, PT, 0, st>>>(v);
         if (v.nw && v.na) {
             k_pair_ws<false><<<bw, PT, 0, st>>>(v);

@@ -13,6 +13,7 @@
 struct dyn_sys_s {
     cudaStream_t stream = nullptr;
     bool own_stream = false;       // created here because the caller passed NULL
+    cudaStream_t aux = nullptr;    // captures the bodies of conditional graph nodes
     SysView v{};
     dyn_config_t cfg{};
     cufftHandle plan_f = 0, plan_b = 0;
@@ -103,25 +104,92 @@ void set_block_counts(SysView& v) {
                                                                    : dyn::kick_blocks_a(v);
 }
 
-// Everything one step enqueues (MdState::step, src/integrate.rs:100-473).
-void enqueue_step(dyn_sys_s* h, float dt, bool spme, bool energy) {
-    const SysView& v = h->v;
+// Inside an active capture on st: appends an IF node on hc after everything
+// captured so far (later work depends on it) and starts capturing its body
+// on aux.
+int begin_if_body(cudaStream_t st, cudaStream_t aux, cudaGraphConditionalHandle hc, cudaGraph_t* body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    DYN_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = hc;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    DYN_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &cp));
+    DYN_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    *body = cp.conditional.phGraph_out[0];
+    DYN_CUDA(cudaStreamBeginCaptureToGraph(aux, *body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    return DYN_OK;
+}
+
+int end_if_body(cudaStream_t aux) {
+    cudaGraph_t g = nullptr;
+    DYN_CUDA(cudaStreamEndCapture(aux, &g));
+    return DYN_OK;
+}
+
+// Captures one step (MdState::step, src/integrate.rs:100-473) into a graph.
+// The list rebuild and the periodic tasks (COM removal, recentering,
+// reset_angle) sit under IF nodes that the displacement check and the step
+// finalisation set on the device, so a step that needs neither launches none
+// of their kernels.  body_rebuild / body_periodic receive the bodies (owned
+// by *out).
+int capture_step(dyn_sys_s* h, float dt, bool spme, bool energy, cudaGraph_t* out,
+                 cudaGraph_t* body_rebuild = nullptr, cudaGraph_t* body_periodic = nullptr) {
+    SysView& v = h->v;
     cudaStream_t st = h->stream;
-    dyn::launch_first_half(v, st, dt);
-    dyn::launch_displacement_check(v, st);
-    dyn::launch_rebuild(v, st, false);
-    dyn::launch_gather_atoms(v, st);
-    dyn::launch_pairs(v, st, energy);
-    dyn::launch_pair14(v, st, energy);
-    dyn::launch_bonded(v, st, energy);
-    if (spme) {
-        dyn::launch_pme(v, st, h->plan_f, h->plan_b);
-        dyn::launch_corrections(v, st);
+    *out = nullptr;
+    DYN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = DYN_OK;
+    cudaGraph_t br = nullptr, bp = nullptr;
+    do {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, nullptr, nullptr);
+        if (e == cudaSuccess)
+            e = cudaGraphConditionalHandleCreate(&v.cond_rebuild, cg, 0, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess)
+            e = cudaGraphConditionalHandleCreate(&v.cond_periodic, cg, 0, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) { rc = dyn::cuda_fail(e, "cudaGraphConditionalHandleCreate"); break; }
+        v.use_cond = 1;
+        dyn::launch_first_half(v, st, dt);
+        dyn::launch_displacement_check(v, st);
+        if ((rc = begin_if_body(st, h->aux, v.cond_rebuild, &br)) != DYN_OK) break;
+        dyn::launch_rebuild(v, h->aux, false);
+        if ((rc = end_if_body(h->aux)) != DYN_OK) break;
+        dyn::launch_gather_atoms(v, st);
+        dyn::launch_pairs(v, st, energy);
+        dyn::launch_pair14(v, st, energy);
+        dyn::launch_bonded(v, st, energy);
+        if (spme) {
+            dyn::launch_pme(v, st, h->plan_f, h->plan_b);
+            dyn::launch_corrections(v, st);
+        }
+        dyn::launch_second_half(v, st, dt);
+        dyn::launch_finalize(v, st, dt, energy, true);
+        if ((rc = begin_if_body(st, h->aux, v.cond_periodic, &bp)) != DYN_OK) break;
+        dyn::launch_periodic(v, h->aux);
+        if ((rc = end_if_body(h->aux)) != DYN_OK) break;
+    } while (0);
+    v.use_cond = 0;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc == DYN_OK && e != cudaSuccess) rc = dyn::cuda_fail(e, "cudaStreamEndCapture");
+    if (rc == DYN_OK) {
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) rc = dyn::cuda_fail(le, "kernel launch during capture");
     }
-    dyn::launch_second_half(v, st, dt);
-    dyn::launch_finalize(v, st, dt, energy, true);
-    dyn::launch_periodic(v, st);
-    dyn::launch_step_end(v, st);
+    if (rc != DYN_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    *out = g;
+    if (body_rebuild) *body_rebuild = br;
+    if (body_periodic) *body_periodic = bp;
+    return DYN_OK;
 }
 
 // Forces at the current coordinates (no integration); dt = 0 kicks set the
@@ -176,6 +244,7 @@ void fill_energies(dyn_sys_s* h, dyn_energies_t* e) {
     e->pairs_in_list = s.list_pairs;
     e->kinetic_rigid = s.ke_rigid;
     e->pressure_atomic_bar = s.pressure_atomic;
+    e->list_union_max = s.union_max;
 }
 
 }  // namespace
@@ -190,6 +259,7 @@ extern "C" int dyn_sys_destroy(dyn_sys_t h) {
     for (void* p : h->allocs) cudaFree(p);
     if (h->h_sc) cudaFreeHost(h->h_sc);
     if (h->own_stream) cudaStreamDestroy(h->stream);
+    if (h->aux) cudaStreamDestroy(h->aux);
     delete h;
     return DYN_OK;
 }
@@ -241,6 +311,14 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) { delete h; return dyn::cuda_fail(e, "cudaStreamCreateWithFlags"); }
         h->own_stream = true;
+    }
+    {
+        cudaError_t e = cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            if (h->own_stream) cudaStreamDestroy(h->stream);
+            delete h;
+            return dyn::cuda_fail(e, "cudaStreamCreateWithFlags");
+        }
     }
     h->cfg = *cfg;
     SysView& v = h->v;
@@ -304,8 +382,22 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         const double ag = 1.4 * std::cbrt(GRPW / dl), ac = 2.0 * std::cbrt(WCL / dl);
         v.cap_tile = std::min<uint32_t>((uint32_t)(1.5 * mink(ag + ac) * dl / WCL) + 16,
                                         std::max<uint32_t>(1u, v.nwclus_cap));
-        v.cap_union = std::min<uint32_t>((uint32_t)(1.4 * mink(ag) * dl) + 64, 3200u);
+        // unions larger than the shared-memory chunk are processed in
+        // several chunks, so this is only the list-build capacity
+        v.cap_union = std::min<uint32_t>((uint32_t)(2.8 * mink(ag) * dl) + 64, 65534u);
         v.cap_union = std::min<uint32_t>(v.cap_union, v.nw_cap);
+        // shared-memory chunk of the water-water kernel: two CTAs per SM
+        // (each CTA also needs 1 KB reserved plus < 2 KB static shared)
+        int dev = 0, smem_sm = 0, smem_blk = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        size_t per_cta = smem_sm > 6144 ? (size_t)smem_sm / 2 - 3072 : 48 * 1024;
+        per_cta = std::min<size_t>(per_cta, smem_blk > 0 ? (size_t)smem_blk : per_cta);
+        const uint32_t fit = (uint32_t)(per_cta / (4 * sizeof(float4))) / 32 * 32;
+        v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(fit, (v.cap_union + 31) / 32 * 32));
+        if (cfg->ww_union_chunk)
+            v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(v.union_chunk, cfg->ww_union_chunk / 32 * 32));
         v.cap_run = 256;
         const double nb = 4.0 / 3.0 * M_PI * r * r * r * dl;
         v.cap_nb = std::min<uint32_t>((uint32_t)(1.5 * nb) + 32, 65535u);
@@ -554,10 +646,9 @@ extern "C" int dyn_sys_step(dyn_sys_t h, uint32_t n_steps, float dt) {
         const int g = (spme ? 1 : 0) | (energy ? 2 : 0);
         if (!h->graph[g] || h->graph_dt[g] != dt) {
             if (h->graph[g]) { cudaGraphExecDestroy(h->graph[g]); h->graph[g] = nullptr; }
-            cudaGraph_t graph;
-            DYN_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            enqueue_step(h, dt, spme, energy);
-            DYN_CUDA(cudaStreamEndCapture(h->stream, &graph));
+            cudaGraph_t graph = nullptr;
+            const int rc = capture_step(h, dt, spme, energy, &graph);
+            if (rc != DYN_OK) return rc;
             cudaError_t e = cudaGraphInstantiate(&h->graph[g], graph, 0);
             cudaGraphDestroy(graph);
             if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaGraphInstantiate");
@@ -889,7 +980,6 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
         dyn::launch_second_half(v, st, dt);
         dyn::launch_finalize(v, st, dt, energy, true);
         dyn::launch_periodic(v, st);
-        dyn::launch_step_end(v, st);
         cudaEventRecord(ev[6], st);
         DYN_CUDA(cudaGetLastError());
         DYN_CUDA(cudaEventSynchronize(ev[6]));
@@ -907,26 +997,62 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
     return read_scalars(h);
 }
 
+// Kernel counts of a step's three parts, each captured on its own into a
+// plain graph that is only inspected, never launched: the fixed part (with
+// or without SPME; cuFFT's kernels excluded), the list rebuild and the
+// periodic tasks.
+int count_step_kernels(dyn_sys_s* h, bool spme, uint32_t* fixed, uint32_t* rebuild, uint32_t* periodic) {
+    const SysView& v = h->v;
+    cudaStream_t st = h->stream;
+    DYN_CUDA(cudaStreamSynchronize(st));
+    auto count = [&](auto&& enqueue, uint32_t* n) -> int {
+        cudaGraph_t g = nullptr;
+        DYN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        enqueue();
+        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaStreamEndCapture");
+        const int rc = count_graph_kernels(g, n);
+        cudaGraphDestroy(g);
+        return rc;
+    };
+    int rc = DYN_OK;
+    if (fixed) {
+        uint32_t total = 0, fft = 0;
+        rc = count([&] {
+            dyn::launch_first_half(v, st, 0.002f);
+            dyn::launch_displacement_check(v, st);
+            dyn::launch_gather_atoms(v, st);
+            dyn::launch_pairs(v, st, true);
+            dyn::launch_pair14(v, st, true);
+            dyn::launch_bonded(v, st, true);
+            if (spme) {
+                dyn::launch_pme(v, st, h->plan_f, h->plan_b);
+                dyn::launch_corrections(v, st);
+            }
+            dyn::launch_second_half(v, st, 0.002f);
+            dyn::launch_finalize(v, st, 0.002f, true, true);
+        }, &total);
+        if (rc) return rc;
+        if (spme) {
+            rc = count([&] {
+                cufftExecR2C(h->plan_f, h->v.qgrid, (cufftComplex*)h->v.cgrid);
+                cufftExecC2R(h->plan_b, (cufftComplex*)h->v.cgrid, h->v.qgrid);
+            }, &fft);
+            if (rc) return rc;
+        }
+        *fixed = total - fft;
+    }
+    if (rebuild && (rc = count([&] { dyn::launch_rebuild(v, st, false); }, rebuild))) return rc;
+    if (periodic && (rc = count([&] { dyn::launch_periodic(v, st); }, periodic))) return rc;
+    return DYN_OK;
+}
+
 extern "C" int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out) {
     DYN_CHECK(h && out, DYN_ERR_INVALID, "dyn_sys_launches_per_step: NULL argument");
-    DYN_CUDA(cudaStreamSynchronize(h->stream));
-    cudaGraph_t g = nullptr, gf = nullptr;
-    DYN_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(h, 0.002f, spme != 0, true);
-    DYN_CUDA(cudaStreamEndCapture(h->stream, &g));
-    uint32_t total = 0, fft = 0;
-    int rc = count_graph_kernels(g, &total);
-    cudaGraphDestroy(g);
-    if (rc) return rc;
-    if (spme) {
-        DYN_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        cufftExecR2C(h->plan_f, h->v.qgrid, (cufftComplex*)h->v.cgrid);
-        cufftExecC2R(h->plan_b, (cufftComplex*)h->v.cgrid, h->v.qgrid);
-        DYN_CUDA(cudaStreamEndCapture(h->stream, &gf));
-        rc = count_graph_kernels(gf, &fft);
-        cudaGraphDestroy(gf);
-        if (rc) return rc;
-    }
-    *out = total - fft;
-    return DYN_OK;
+    return count_step_kernels(h, spme != 0, out, nullptr, nullptr);
+}
+
+extern "C" int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic) {
+    DYN_CHECK(h && rebuild && periodic, DYN_ERR_INVALID, "dyn_sys_launches_conditional: NULL argument");
+    return count_step_kernels(h, false, nullptr, rebuild, periodic);
 }

@@ -70,6 +70,7 @@ class MdConfig:
     full_energy: bool = False
     reset_angle: bool = True
     seed: int = 0
+    ww_union_chunk: int = 0         # 0 = automatic (tuning knob only)
 
 
 def thermo_dof(system, cfg):
@@ -130,6 +131,7 @@ def _config_struct(system, cfg):
     c.flags = flags
     c.thermo_dof = thermo_dof(system, cfg)
     c.seed = int(cfg.seed) & 0xFFFFFFFFFFFFFFFF
+    c.ww_union_chunk = int(cfg.ww_union_chunk)
     return c
 
 
@@ -264,9 +266,16 @@ class MdState:
         return dict(zip(self.STAGES, ms.tolist()))
 
     def launches_per_step(self, spme=True):
+        """Kernels of a step without a list rebuild or periodic task."""
         n = C.c_uint32()
         check(lib().dyn_sys_launches_per_step(self.handle, 1 if spme else 0, C.byref(n)))
         return n.value
+
+    def launches_conditional(self):
+        """(kernels added by a list rebuild, kernels added by a periodic task)."""
+        r, p = C.c_uint32(), C.c_uint32()
+        check(lib().dyn_sys_launches_conditional(self.handle, C.byref(r), C.byref(p)))
+        return r.value, p.value
 
     def set_state(self, atom_pos=None, atom_vel=None, water_pos=None, water_vel=None):
         conv = [None if x is None else f32(x).reshape(-1) for x in (atom_pos, atom_vel, water_pos, water_vel)]

@@ -29,8 +29,10 @@
  *    Device memory is owned by the library and released by *_destroy.
  *  - Units: Angstrom, ps, amu, kcal/mol.  Charges are pre-scaled by
  *    18.2223 = sqrt(332.0522) as in the reference (src/non_bonded.rs:58-63).
- *  - Streams are passed as `void*` holding a cudaStream_t (NULL = legacy
- *    default stream).
+ *  - Streams are passed as `void*` holding a cudaStream_t.  For dyn_nb_*
+ *    NULL means the legacy default stream; dyn_sys_create with NULL creates
+ *    a non-blocking stream of its own (a captured CUDA graph cannot be
+ *    launched on the legacy stream).
  */
 #ifndef DYNB200_H
 #define DYNB200_H
@@ -104,7 +106,7 @@ int dyn_nb_create(void* stream, uint32_t n_dyn, uint32_t n_water, float cutoff_e
  * flat pair list.  tgt/src index the atom array (body 0) or the water
  * molecule (bodies 1..4).  body_tgt/body_src: DYN_BODY_* per pair.
  * flags: DYN_PAIR_* per pair.  The library re-packs these into its own
- * 16-byte-per-pair layout. */
+ * 20-byte-per-pair layout. */
 int dyn_nb_set_pairs(dyn_nb_t h, uint64_t n_pairs, const uint32_t* tgt, const uint32_t* src,
                      const float* sigma, const float* eps, const float* q_tgt,
                      const float* q_src, const uint8_t* body_tgt, const uint8_t* body_src,
@@ -245,6 +247,11 @@ typedef struct {
     uint32_t flags;         /* DYN_FLAG_*                                   */
     uint32_t thermo_dof;    /* degrees of freedom (src/thermostat.rs:220)   */
     uint64_t seed;          /* Philox key for all stochastic terms          */
+    uint32_t ww_union_chunk;/* waters per shared-memory chunk of the
+                             * water-water kernel; 0 = the largest that lets
+                             * two CTAs share an SM (a tuning knob: results
+                             * do not depend on it)                         */
+    uint32_t reserved0;
 } dyn_config_t;
 
 typedef struct {
@@ -280,7 +287,7 @@ typedef struct {
     double potential;       /* per the reference or full convention        */
     double e_lj;            /* short-range LJ                              */
     double e_coul_short;    /* erfc real-space Coulomb                     */
-    double e_water_water_short;
+    double e_water_water_short; /* with DYN_FLAG_FULL_ENERGY only (else 0)  */
     double e_recip;         /* SPME incl. self term                        */
     double e_corrections;   /* exclusion corrections (corrected mode)     */
     double e_bonded;
@@ -298,6 +305,8 @@ typedef struct {
     double pressure_atomic_bar; /* the reference's formula: COM KE with the site
                                * virial (src/barostat.rs:419-431); pressure_bar
                                * uses the molecular virial of the rigid waters */
+    uint64_t list_union_max;  /* largest set of j-waters one 32-water group
+                               * needed at the last list build */
 } dyn_energies_t;
 
 /* Creates a resident system (replaces MdState::new's device setup,
@@ -357,8 +366,14 @@ int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, double* ms);
 
 /* Number of this library's kernels one step launches (library kernels such
  * as cuFFT's are not counted), for the step with SPME (spme != 0) or
- * without. */
+ * without, when the step neither rebuilds the lists nor runs a periodic task
+ * (COM removal, recentering, reset_angle). */
 int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
+
+/* Kernels a step adds when it rebuilds the lists (*rebuild) and when a
+ * periodic task is due (*periodic); in the captured step graph these sit
+ * under conditional nodes that the device sets. */
+int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic);
 
 #ifdef __cplusplus
 }

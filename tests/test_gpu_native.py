@@ -179,3 +179,42 @@ def test_invalid_config_raises(gpu_lib):
     sysd = water_only(n_side=3)
     with pytest.raises(DynError):
         md.MdState(sysd, md.MdConfig(coulomb_cutoff=10.0))  # box too small for the cutoff
+
+
+def test_union_chunking_bit_identical(gpu_lib):
+    """The water-water kernel stages a group's j-waters in shared-memory
+    chunks; forces and trajectories must not depend on the chunk size."""
+    sysd = water_only()
+    a = md.MdState(sysd, _cfg(sysd))
+    b = md.MdState(sysd, _cfg(sysd, ww_union_chunk=64))
+    fa, fb = a.forces(), b.forces()
+    np.testing.assert_array_equal(fa["f_water"], fb["f_water"])
+    assert fa["virial"] == fb["virial"]
+    a.step(0.002, 30)
+    b.step(0.002, 30)
+    np.testing.assert_array_equal(a.state()["water_pos"], b.state()["water_pos"])
+    assert a.energies()["list_union_max"] > 64
+    a.close()
+    b.close()
+
+
+def test_graph_counters_and_periodic_tasks(gpu_lib):
+    """Steps run as captured graphs whose list rebuild and periodic tasks
+    are conditional nodes set on the device: the step counter, the rebuild
+    count and the COM removal at step 100 must all happen."""
+    sysd = md.equilibrate(mixed(), _cfg(mixed()), n_steps=50, dt=0.001)
+    cfg = _cfg(sysd, integ=md.LangevinMiddle(gamma=5.0), com_removal_interval=100)
+    st = md.MdState(sysd, cfg)
+    st.step(0.002, 100)
+    e = st.energies()
+    assert e["step"] == 100
+    assert e["list_rebuilds"] >= 1
+    s = st.state()
+    m_w = np.array([16.0, 1.008, 1.008])  # site masses the engine uses
+    p = (s["water_vel"] * m_w[None, :, None]).sum(axis=(0, 1))
+    p += (s["atom_vel"] * np.asarray(sysd["atom_mass"])[:, None]).sum(axis=0)
+    p_scale = np.abs(s["water_vel"] * m_w[None, :, None]).sum()
+    assert np.linalg.norm(p) < 1e-4 * p_scale, (p, p_scale)
+    st.step(0.002, 7)
+    assert st.energies()["step"] == 107
+    st.close()
