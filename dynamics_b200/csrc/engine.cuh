@@ -23,7 +23,7 @@
 
 #define WCL 8             // waters per cluster
 #define GRPW 32           // waters per i-group of the water-water kernel (4 clusters)
-#define NPOLY 15          // coefficients of the screened-Coulomb polynomials
+#define NPOLY_G 12        // coefficients of the screened-Coulomb force polynomial
 #define LPW 8             // lanes per i-water in the water-water kernel
 #define ACL 8             // atoms per cluster
 #define INVALID_ID 0xFFFFFFFFu
@@ -153,8 +153,8 @@ struct SysView {
     // u(x) = erfc(x) + 2x/sqrt(pi) exp(-x^2) and erfc(x) at x = alpha r, as
     // polynomials in s = 2r/rc - 1 on [-1, 1] (Chebyshev interpolation,
     // power basis, Horner in float32): force = qq u / r^3, energy = qq erfc / r
-    float poly_f[NPOLY], poly_e[NPOLY];
-    float two_over_rc;
+    float poly_g[NPOLY_G];        // g(r^2) in t = 2 r^2 / rc^2 - 1 (power basis)
+    float two_over_rc2;
     // IF-node handles of the captured step graph: the displacement check
     // sets cond_rebuild, the step finalisation sets cond_periodic; only
     // kernels captured for a graph (use_cond != 0) set them

@@ -31,22 +31,21 @@ constexpr int PT = 128;  // threads per block (4 warps)
 // w accumulates the virial in float32
 struct Acc3 { double e_lj, e_c; float w; };
 
-// erfc-screened Coulomb, branch-free: force q q u(alpha r) / r^3 with
-// u(x) = erfc(x) + 2x/sqrt(pi) exp(-x^2) from the host-fitted polynomial in
-// s = 2r/rc - 1; zero for r >= rc (src/cuda/cuda.cu:160-164).  On energy
-// steps the energy q q erfc(alpha r) / r uses erfcf and float64 sums, which
-// keeps the total potential energy within 1e-6 of float64 even where large
-// terms cancel.
+// erfc-screened Coulomb, branch-free: force q q (r^-3 + g(r^2)) d with
+// g(z) = 2 d/dz [erf(alpha sqrt z) / sqrt z] from the host-fitted polynomial
+// in t = 2 r^2 / rc^2 - 1 (no square root needed for the argument); zero for
+// r >= rc (src/cuda/cuda.cu:160-164).  On energy steps the energy
+// q q erfc(alpha r) / r uses erfcf and float64 sums, which keeps the total
+// potential energy within 1e-6 of float64 even where large terms cancel.
 template <bool ENERGY>
 __device__ __forceinline__ void coul(float3 d, float qq, const SysView& v, float3& f, Acc3& a) {
     const float r2 = dot3(d, d);
     const float rinv = rsqrtf(r2);
-    const float sv = fmaf(r2 * rinv, v.two_over_rc, -1.0f);
-    float u = v.poly_f[NPOLY - 1];
+    const float t = fmaf(r2, v.two_over_rc2, -1.0f);
+    float g = v.poly_g[NPOLY_G - 1];
 #pragma unroll
-    for (int k = NPOLY - 2; k >= 0; --k) u = fmaf(u, sv, v.poly_f[k]);
-    const float rinv2 = rinv * rinv;
-    float fs = qq * u * (rinv * rinv2);
+    for (int k = NPOLY_G - 2; k >= 0; --k) g = fmaf(g, t, v.poly_g[k]);
+    float fs = qq * fmaf(rinv * rinv, rinv, g);
     fs = r2 < v.rc2 ? fs : 0.0f;
     f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
     a.w = fmaf(fs, r2, a.w);
@@ -203,6 +202,9 @@ __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
         Acc3 a{0.0, 0.0, 0.f};
         const uint16_t* lst = v.wnb + (size_t)s * v.cap_nb;
         uint32_t k = l;  // this lane's next list entry (entries l, l + LPW, ...)
+        // the next entry's index is loaded one iteration ahead, so the
+        // global-memory latency of the list overlaps the arithmetic
+        uint32_t idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
         // a union larger than the shared buffer is processed in chunks; the
         // lists hold ascending union indices, so each lane resumes where it
         // stopped
@@ -217,9 +219,10 @@ __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
                 break;
             }
             parity ^= 1u;
-            for (; k < n; k += LPW) {
-                const uint32_t idx = lst[k];
-                if (idx >= hi) break;
+            while (idx_next < hi) {
+                const uint32_t idx = idx_next;
+                k += LPW;
+                idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
                 const float4* jw = tile + 4 * (idx - lo);
                 const float3 jO = xyz(jw[0]), jH0 = xyz(jw[1]), jH1 = xyz(jw[2]), jM = xyz(jw[3]);
                 const float3 sh = shift_of(iO - jO, b);

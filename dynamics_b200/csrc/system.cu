@@ -51,11 +51,11 @@ inline uint32_t round8(uint32_t x) { return (x + 7u) / 8u * 8u; }
 inline uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1u) / m * m; }
 
 // Chebyshev interpolation of f(x) on x = xmax (s + 1) / 2, s in [-1, 1],
-// at NPOLY Chebyshev nodes, converted to power-basis coefficients in s.
-template <typename F>
+// at N Chebyshev nodes, converted to power-basis coefficients in s.
+template <int N, typename F>
 void cheb_poly(F f, double xmax, float* out) {
-    const int n = NPOLY;
-    double c[NPOLY];
+    const int n = N;
+    double c[N];
     for (int k = 0; k < n; ++k) {
         double sum = 0.0;
         for (int j = 0; j < n; ++j) {
@@ -65,7 +65,7 @@ void cheb_poly(F f, double xmax, float* out) {
         c[k] = 2.0 / n * sum;
     }
     c[0] *= 0.5;
-    double T[NPOLY][NPOLY] = {};
+    double T[N][N] = {};
     T[0][0] = 1.0;
     if (n > 1) T[1][1] = 1.0;
     for (int k = 1; k + 1 < n; ++k)
@@ -402,14 +402,30 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         const double nb = 4.0 / 3.0 * M_PI * r * r * r * dl;
         v.cap_nb = std::min<uint32_t>((uint32_t)(1.5 * nb) + 32, 65535u);
     }
-    // screened-Coulomb polynomials on r in [0, rc]
+    // screened-Coulomb force: F = q q (r^-3 + g(r^2)) d for r < rc with
+    // g(z) = 2 d/dz [erf(alpha sqrt z) / sqrt z], an entire function of z
+    // fitted on [0, rc^2]; the r^-3 part is exact, so no cancellation-free
+    // form of erfc is needed
     {
-        const double a = v.alpha, xmax = (double)v.alpha * (double)v.rc;
-        (void)a;
-        cheb_poly([](double x) { return std::erfc(x) + 2.0 / std::sqrt(M_PI) * x * std::exp(-x * x); }, xmax,
-                  v.poly_f);
-        cheb_poly([](double x) { return std::erfc(x); }, xmax, v.poly_e);
-        v.two_over_rc = 2.0f / v.rc;
+        const double a = v.alpha;
+        auto g = [a](double z) {
+            const double x2 = a * a * z;
+            const double c = 2.0 * a / std::sqrt(M_PI);
+            if (x2 < 0.25) {
+                // h = c sum_n (-a^2 z)^n / (n! (2n+1)) (the series of
+                // erf(x)/x), differentiated term by term in z
+                double sum = 0.0, t = 1.0;  // t = (-a^2)^n / n!
+                for (int n = 1; n < 20; ++n) {
+                    t *= -a * a / n;
+                    sum += t * n * std::pow(z, n - 1) / (2 * n + 1);
+                }
+                return 2.0 * c * sum;
+            }
+            const double r = std::sqrt(z), x = a * r;
+            return (c * std::exp(-x * x) / r - std::erf(x) / z) / r;
+        };
+        cheb_poly<NPOLY_G>(g, (double)v.rc * (double)v.rc, v.poly_g);
+        v.two_over_rc2 = (float)(2.0 / ((double)v.rc * (double)v.rc));
     }
     v.cap_ws = (v.nw && v.na) ? est(v.r_ws, acl_vol, v.naclus_cap) : 1;
     v.cap_sw = (v.nw && v.na) ? est(v.r_ws, wcl_vol, v.nwclus_cap) : 1;
