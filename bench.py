@@ -37,6 +37,10 @@ WORKLOADS = {
                 barostat=True),
 }
 DEFAULT_WORKLOAD = "c3w"
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the water-water pair kernel, from an ncu --set full capture of this
+# workload (cold L2, as in the timed loop, which flushes L2 between steps)
+PAIR_DRAM_BYTES = {"c3w": 17306880}
 DT = 0.002
 
 
@@ -253,7 +257,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "fp32", "kernel": "short-range pair kernels",
                      "achieved": round(achieved, 3), "peak": round(peak.value, 2), "unit": "TFLOP/s",
-                     "frac": round(achieved / peak.value, 4), "traffic": None,
+                     "frac": round(achieved / peak.value, 4), "traffic": PAIR_DRAM_BYTES.get(name),
                      "peak_source": "measured FP32 FMA probe (dyn_probe_fp32_peak)",
                      "algorithmic_flops": int(flops), "pairs_lj": n_lj, "pairs_coulomb": n_c},
         "roofline_spme": {"bound": "hbm", "achieved": round(pme_bytes / (pme_ms * 1e-3) / 1e9, 1),
