@@ -35,6 +35,11 @@ WORKLOADS = {
     # ~100k atoms: 24,000 OPC waters in a 98 A cube, rc 10, 96^3, CSVR 300 K + C-rescale 1 bar
     "c3w": dict(n_water=24000, box=98.0, cutoff=10.0, grid=(96, 96, 96), integrator="vv_csvr",
                 barostat=True),
+    # batched form: 64 water boxes, 512-8000 waters log-uniform, 0.0334 / A^3,
+    # rc 9, grid ~1 A (FFT-friendly), Langevin-middle 300 K; one launch per
+    # stage for all 64 (compared with the same systems one by one)
+    "c4w": dict(kind="batch", n_sys=64, cutoff=9.0, integrator="langevin", barostat=False,
+                n_water=None),
 }
 DEFAULT_WORKLOAD = "c3w"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
@@ -58,6 +63,138 @@ def build_system(name, seed):
     if w["barostat"]:
         cfg.barostat_cfg = md.BarostatCfg(pressure_target=1.0, tau=5.0, solvent_compressibility=4.5e-5)
     return sysd, cfg
+
+
+def build_batch(name, seed):
+    from dynamics_b200 import md, synth
+    w = WORKLOADS[name]
+    sizes = synth.config4_sizes(w["n_sys"], seed=seed)
+    systems, cfgs = [], []
+    alpha = synth.ewald_alpha(w["cutoff"])
+    for i, n in enumerate(sizes):
+        sysd, grid = synth.batch_member(int(n), seed=seed * 1000 + i)
+        cfg = md.MdConfig(coulomb_cutoff=w["cutoff"], lj_cutoff=w["cutoff"], spme_alpha=alpha,
+                          spme_grid=grid, seed=seed * 1000 + i,
+                          integrator=md.LangevinMiddle(gamma=1.0))
+        systems.append(sysd)
+        cfgs.append(cfg)
+    return systems, cfgs
+
+
+def run_batch(args):
+    """Batched form: aggregate ns/day of all members advanced together,
+    against the same systems stepped one by one through the plain path."""
+    import torch
+
+    from dynamics_b200 import md
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    name = args.workload
+    w = WORKLOADS[name]
+    systems, cfgs = build_batch(name, seed=1 + rank)
+    systems = [md.equilibrate(s, c, n_steps=min(args.equil, 200), dt=0.001) for s, c in zip(systems, cfgs)]
+    n_sys = len(systems)
+    n_water = int(sum(len(s["water_pos"]) for s in systems))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    # ---- plain path, one system at a time (each its own graph per step) ----
+    k_plain = max(10, min(args.steps, 100))
+    plain_ms = 0.0
+    for s, c in zip(systems, cfgs):
+        st = md.MdState(s, c, stream=stream.cuda_stream)
+        st.step(DT, args.warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        st.step(DT, k_plain)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_ms += e0.elapsed_time(e1) / k_plain
+        st.close()
+    # ---- batched ----
+    batch = md.MdBatch(systems, cfgs, stream=stream.cuda_stream)
+    batch.step(DT, args.warmup)
+    torch.cuda.synchronize(dev)
+    r0 = sum(m.energies()["list_rebuilds"] for m in batch.members)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+                          if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_rank{rank}.csv")
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            ev0[k].record(stream)
+            batch.step(DT, 1)
+            ev1[k].record(stream)
+        torch.cuda.synchronize(dev)
+    batch.sync()
+    ms = float(np.sum([ev0[k].elapsed_time(ev1[k]) for k in range(args.steps)]))
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    rebuilds = sum(m.energies()["list_rebuilds"] for m in batch.members) - r0
+    fixed_s, reb_k, per_k = batch.launches(True)
+    fixed_n, _, _ = batch.launches(False)
+    launches = (fixed_s + fixed_n) / 2.0 * args.steps + reb_k * min(rebuilds, args.steps)
+    value = args.steps * DT * 1e-3 * n_sys * world / (ms * 1e-3) * 86400.0
+    plain_value = DT * 1e-3 * n_sys / (plain_ms * 1e-3) * 86400.0
+    # ---- end to end: every member's positions/velocities in and out per step ----
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory().numpy()
+    host = []
+    for m in batch.members:
+        s0 = m.state()
+        host.append((pin(s0["water_pos"]), pin(s0["water_vel"])))
+    n_e2e = max(5, args.steps // 20)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        for m, (wp, wv) in zip(batch.members, host):
+            m.set_state(water_pos=wp, water_vel=wv)
+        batch.step(DT, 1)
+        for m, (wp, wv) in zip(batch.members, host):
+            s1 = m.state()
+            wp[:] = s1["water_pos"]
+            wv[:] = s1["water_vel"]
+    t_e2e = time.perf_counter() - t0
+    e2e_value = n_e2e * DT * 1e-3 * n_sys * world / t_e2e * 86400.0
+    io_bytes = int(sum(wp.nbytes + wv.nbytes for wp, wv in host))
+    clk = clocks.summary(local)
+    batch.close()
+    if dist:
+        dist.barrier()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    out = {
+        "metric": "ns/day", "value": round(value, 2), "unit": "ns/day (aggregate over members)",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded OPC water boxes, equilibrated on device)",
+        "config": {"workload": name, "members": n_sys, "n_water_total": n_water,
+                   "sizes": "512-8000 waters, log-uniform", "cutoff_A": w["cutoff"],
+                   "grid": "FFT-friendly ~1 A", "integrator": "langevin_middle", "dt_fs": DT * 1e3,
+                   "l2": "256 MiB flush between timed steps", "parallelism": f"replicas x{world}"},
+        "plain_one_by_one": {"value": round(plain_value, 2), "unit": "ns/day (aggregate)",
+                             "ms_per_round": round(plain_ms, 4), "steps_each": k_plain,
+                             "batch_over_plain": round(value / world / plain_value, 3)},
+        "e2e": {"value": round(e2e_value, 2), "unit": "ns/day (aggregate)",
+                "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+        "gpu_launches": int(round(launches)),
+        "launches_per_step": {"spme": fixed_s, "no_spme": fixed_n, "rebuild_extra": reb_k,
+                              "periodic_extra": per_k},
+        "clocks": clk, "cpu_baseline": None,
+    }
+    print(json.dumps(out))
+    if dist:
+        dist.destroy_process_group()
 
 
 def count_pairs(sysd, cutoff):
@@ -326,6 +463,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif WORKLOADS[args.workload].get("kind") == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

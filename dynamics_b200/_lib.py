@@ -126,6 +126,13 @@ _SIGS = {
     "dyn_sys_stage_times": ([_P, C.c_uint32, C.c_float, _P], C.c_int),
     "dyn_sys_launches_per_step": ([_P, C.c_int, _P], C.c_int),
     "dyn_sys_launches_conditional": ([_P, _P, _P], C.c_int),
+    "dyn_batch_create": ([_P, C.c_uint32, _P, _P, _P], C.c_int),
+    "dyn_batch_step": ([_P, C.c_uint32, C.c_float], C.c_int),
+    "dyn_batch_size": ([_P, _P], C.c_int),
+    "dyn_batch_member": ([_P, C.c_uint32, _P], C.c_int),
+    "dyn_batch_sync": ([_P], C.c_int),
+    "dyn_batch_launches": ([_P, C.c_int, _P, _P, _P], C.c_int),
+    "dyn_batch_destroy": ([_P], C.c_int),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libdynb200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["errors.cu", "nb_compat.cu", "nblist.cu", "pair.cu", "pme.cu", "integrate.cu",
-           "bonded.cu", "system.cu", "nb_static.cu"]
+           "bonded.cu", "system.cu", "batch.cu", "nb_static.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -42,7 +42,7 @@ def build(force=False, verbose=False):
     if not force and not _stale():
         return LIB
     lib64 = os.path.join(cuda_home(), "lib64")
-    cmd = [nvcc(), "-shared", "-std=c++17", "-O3", "-lineinfo", *ARCH,
+    cmd = [nvcc(), "-shared", "-std=c++17", "-O3", "-lineinfo", "-fmad=false", *ARCH,
            "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=default",
            "-cudart", "static",
            "-I" + INCLUDE,

@@ -1,0 +1,307 @@
+// Batched form: many independent systems of uneven size advanced together.
+//
+// Every stage of a step is ONE launch for all member systems: the same
+// kernel body as the single-system engine, in its NAME##_batch form, with a
+// block map that gives each system the block range its single-system launch
+// would have had (per-system offsets into one grid).  A step is one captured
+// CUDA graph whose list rebuild and periodic tasks sit under IF nodes that
+// any member can raise; each member's kernels still check its own flags, so
+// a member's trajectory is bit-identical to running it alone.  cuFFT runs
+// once per member on the batch stream (its plans are per grid size).
+//
+// The reference has no counterpart (it advances one MdState per call,
+// src/integrate.rs:72); the batch is built from the same dyn_sys members, so
+// dyn_sys_get_state / get_energies read any member's results.
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "sys_internal.cuh"
+
+struct BatchCtx {
+    std::vector<SysView> views;                       // host copies of the members' views
+    const SysView* d_views = nullptr;                 // device copy used by the graph being built
+    bool collecting = false;                          // recording block maps, launching nothing
+    std::map<std::vector<uint32_t>, BlockMap> maps;   // per-system block counts -> device map
+    bool map_missing = false;
+    bool map_too_large = false;
+    uint32_t launches = 0;                            // batched launches recorded while collecting
+};
+
+uint32_t batch_size(const BatchCtx* b) { return (uint32_t)b->views.size(); }
+const SysView& batch_view(const BatchCtx* b, uint32_t i) { return b->views[i]; }
+const SysView* batch_dviews(const BatchCtx* b) { return b->d_views; }
+bool batch_collecting(const BatchCtx* b) { return b->collecting; }
+
+BlockMap batch_map(BatchCtx* b, const std::vector<uint32_t>& blocks) {
+    if (!b->collecting) {
+        auto it = b->maps.find(blocks);
+        if (it != b->maps.end()) return it->second;
+        b->map_missing = true;
+        return BlockMap{0, nullptr};
+    }
+    uint32_t total = 0;
+    for (uint32_t x : blocks) total += x;
+    if (total) ++b->launches;
+    auto it2 = b->maps.find(blocks);
+    if (it2 != b->maps.end()) return it2->second;
+    total = 0;
+    for (uint32_t x : blocks) {
+        if (x > 0xFFFFu) b->map_too_large = true;
+        total += x;
+    }
+    b->maps[blocks] = BlockMap{total, nullptr};
+    return BlockMap{total, nullptr};
+}
+
+struct dyn_batch_s {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaStream_t aux = nullptr;
+    std::vector<dyn_sys_t> members;
+    BatchCtx ctx;
+    SysView* d_views[4] = {nullptr, nullptr, nullptr, nullptr};  // one per graph variant
+    std::vector<void*> map_allocs;
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    float graph_dt[4] = {0, 0, 0, 0};
+    uint64_t host_step = 0;
+    uint32_t spme_interval = 1, energy_interval = 1;
+};
+
+namespace {
+
+// Device copies of the block maps recorded by a collecting pass.
+int upload_maps(dyn_batch_s* b) {
+    if (b->ctx.map_too_large)
+        return dyn::fail(DYN_ERR_UNSUPPORTED, "batch: a member needs more than 65535 blocks in one stage");
+    for (auto& kv : b->ctx.maps) {
+        if (kv.second.d_map || kv.second.total == 0) continue;
+        std::vector<uint2> m;
+        m.reserve(kv.second.total);
+        const std::vector<uint32_t>& bl = kv.first;
+        for (uint32_t i = 0; i < bl.size(); ++i)
+            for (uint32_t j = 0; j < bl[i]; ++j) m.push_back(make_uint2(i, j | (bl[i] << 16)));
+        uint2* d = nullptr;
+        DYN_CUDA(cudaMalloc(&d, m.size() * sizeof(uint2)));
+        b->map_allocs.push_back(d);
+        DYN_CUDA(cudaMemcpy(d, m.data(), m.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+        kv.second.d_map = d;
+    }
+    return DYN_OK;
+}
+
+// The stages of one step, for all members at once (MdState::step,
+// src/integrate.rs:100-473).  With cond, the rebuild and the periodic tasks
+// go under IF nodes of the capture in progress.
+int enqueue_batch_step(dyn_batch_s* b, float dt, bool spme, bool energy, bool cond,
+                       cudaGraphConditionalHandle c_rebuild, cudaGraphConditionalHandle c_periodic) {
+    const Target T{nullptr, &b->ctx, b->stream}, TA{nullptr, &b->ctx, b->aux};
+    cudaGraph_t body = nullptr;
+    int rc = DYN_OK;
+    dyn::launch_first_half(T, dt);
+    dyn::launch_displacement_check(T);
+    if (cond && (rc = dyn::begin_if_body(b->stream, b->aux, c_rebuild, &body)) != DYN_OK) return rc;
+    dyn::launch_rebuild(cond ? TA : T, false);
+    if (cond && (rc = dyn::end_if_body(b->aux)) != DYN_OK) return rc;
+    dyn::launch_gather_atoms(T);
+    dyn::launch_pairs(T, energy);
+    dyn::launch_pair14(T, energy);
+    dyn::launch_bonded(T, energy);
+    if (spme) {
+        dyn::launch_pme(T);
+        dyn::launch_corrections(T);
+    }
+    dyn::launch_second_half(T, dt);
+    dyn::launch_finalize(T, dt, energy, true);
+    if (cond && (rc = dyn::begin_if_body(b->stream, b->aux, c_periodic, &body)) != DYN_OK) return rc;
+    dyn::launch_periodic(cond ? TA : T);
+    if (cond && (rc = dyn::end_if_body(b->aux)) != DYN_OK) return rc;
+    return DYN_OK;
+}
+
+// Records the block maps of a step variant (no launches) and uploads them.
+int collect_maps(dyn_batch_s* b, float dt, bool spme, bool energy) {
+    b->ctx.collecting = true;
+    const int rc = enqueue_batch_step(b, dt, spme, energy, false, 0, 0);
+    b->ctx.collecting = false;
+    if (rc) return rc;
+    return upload_maps(b);
+}
+
+int capture_batch_step(dyn_batch_s* b, int g, float dt, bool spme, bool energy, cudaGraph_t* out) {
+    *out = nullptr;
+    DYN_CUDA(cudaStreamSynchronize(b->stream));  // d_views[g] may be read by work in flight
+    b->ctx.views.clear();
+    for (dyn_sys_t m : b->members) b->ctx.views.push_back(m->v);
+    int rc = collect_maps(b, dt, spme, energy);
+    if (rc) return rc;
+    b->ctx.d_views = b->d_views[g];
+    b->ctx.map_missing = false;
+    DYN_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaGraphConditionalHandle hr = 0, hp = 0;
+    {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        cudaError_t e = cudaStreamGetCaptureInfo(b->stream, &cs, nullptr, &cg, nullptr, nullptr);
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hr, cg, 0, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hp, cg, 0, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) rc = dyn::cuda_fail(e, "cudaGraphConditionalHandleCreate");
+    }
+    if (rc == DYN_OK) rc = enqueue_batch_step(b, dt, spme, energy, true, hr, hp);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    if (rc == DYN_OK && e != cudaSuccess) rc = dyn::cuda_fail(e, "cudaStreamEndCapture");
+    if (rc == DYN_OK) {
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) rc = dyn::cuda_fail(le, "kernel launch during capture");
+    }
+    if (rc == DYN_OK && b->ctx.map_missing) rc = dyn::fail(DYN_ERR_INVALID, "batch: block map missing");
+    if (rc != DYN_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    // the graph's kernels read the views at run time: give them this
+    // graph's conditional handles
+    for (SysView& v : b->ctx.views) {
+        v.cond_rebuild = hr;
+        v.cond_periodic = hp;
+        v.use_cond = 1;
+    }
+    const cudaError_t ue = cudaMemcpy(b->d_views[g], b->ctx.views.data(), b->ctx.views.size() * sizeof(SysView),
+                                      cudaMemcpyHostToDevice);
+    if (ue != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return dyn::cuda_fail(ue, "batch views upload");
+    }
+    *out = graph;
+    return DYN_OK;
+}
+
+}  // namespace
+
+extern "C" int dyn_batch_destroy(dyn_batch_t b) {
+    if (!b) return DYN_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (int g = 0; g < 4; ++g) {
+        if (b->graph[g]) cudaGraphExecDestroy(b->graph[g]);
+        if (b->d_views[g]) cudaFree(b->d_views[g]);
+    }
+    for (void* p : b->map_allocs) cudaFree(p);
+    for (dyn_sys_t m : b->members) dyn_sys_destroy(m);
+    if (b->aux) cudaStreamDestroy(b->aux);
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cfgs,
+                                const dyn_system_desc_t* systems, dyn_batch_t* out) {
+    DYN_CHECK(out && cfgs && systems, DYN_ERR_INVALID, "dyn_batch_create: NULL argument");
+    DYN_CHECK(n > 0, DYN_ERR_INVALID, "dyn_batch_create: empty batch");
+    *out = nullptr;
+    for (uint32_t i = 1; i < n; ++i) {
+        DYN_CHECK(std::max(1u, cfgs[i].spme_interval) == std::max(1u, cfgs[0].spme_interval) &&
+                      std::max(1u, cfgs[i].energy_interval) == std::max(1u, cfgs[0].energy_interval),
+                  DYN_ERR_INVALID, "dyn_batch_create: members must share spme_interval and energy_interval");
+    }
+    dyn_batch_s* b = new dyn_batch_s();
+    b->stream = (cudaStream_t)stream;
+    if (!b->stream) {
+        const cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete b; return dyn::cuda_fail(e, "cudaStreamCreateWithFlags"); }
+        b->own_stream = true;
+    }
+    {
+        const cudaError_t e = cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { dyn_batch_destroy(b); return dyn::cuda_fail(e, "cudaStreamCreateWithFlags"); }
+    }
+    b->spme_interval = std::max(1u, cfgs[0].spme_interval);
+    b->energy_interval = std::max(1u, cfgs[0].energy_interval);
+    for (uint32_t i = 0; i < n; ++i) {
+        dyn_sys_t m = nullptr;
+        const int rc = dyn_sys_create(b->stream, &cfgs[i], &systems[i], &m);
+        if (rc != DYN_OK) {
+            const std::string msg = "dyn_batch_create: member " + std::to_string(i) + ": " + dyn_last_error();
+            dyn_batch_destroy(b);
+            return dyn::fail(rc, msg);
+        }
+        b->members.push_back(m);
+    }
+    for (int g = 0; g < 4; ++g) {
+        const cudaError_t e = cudaMalloc(&b->d_views[g], n * sizeof(SysView));
+        if (e != cudaSuccess) { dyn_batch_destroy(b); return dyn::cuda_fail(e, "cudaMalloc"); }
+    }
+    *out = b;
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_step(dyn_batch_t b, uint32_t n_steps, float dt) {
+    DYN_CHECK(b, DYN_ERR_INVALID, "dyn_batch_step: NULL handle");
+    DYN_CHECK(dt > 0.f && std::isfinite(dt), DYN_ERR_INVALID, "dyn_batch_step: dt must be > 0");
+    for (uint32_t i = 0; i < n_steps; ++i) {
+        const uint64_t s = b->host_step;
+        const bool spme = (s % b->spme_interval) == 0;
+        const bool energy = ((s + 1) % b->energy_interval) == 0;
+        const int g = (spme ? 1 : 0) | (energy ? 2 : 0);
+        if (!b->graph[g] || b->graph_dt[g] != dt) {
+            if (b->graph[g]) { cudaGraphExecDestroy(b->graph[g]); b->graph[g] = nullptr; }
+            cudaGraph_t graph = nullptr;
+            const int rc = capture_batch_step(b, g, dt, spme, energy, &graph);
+            if (rc != DYN_OK) return rc;
+            const cudaError_t e = cudaGraphInstantiate(&b->graph[g], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaGraphInstantiate");
+            b->graph_dt[g] = dt;
+        }
+        DYN_CUDA(cudaGraphLaunch(b->graph[g], b->stream));
+        b->host_step += 1;
+        for (dyn_sys_t m : b->members) m->host_step += 1;
+    }
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_size(dyn_batch_t b, uint32_t* n) {
+    DYN_CHECK(b && n, DYN_ERR_INVALID, "dyn_batch_size: NULL argument");
+    *n = (uint32_t)b->members.size();
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_member(dyn_batch_t b, uint32_t i, dyn_sys_t* out) {
+    DYN_CHECK(b && out, DYN_ERR_INVALID, "dyn_batch_member: NULL argument");
+    DYN_CHECK(i < b->members.size(), DYN_ERR_INVALID, "dyn_batch_member: index out of range");
+    *out = b->members[i];
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_sync(dyn_batch_t b) {
+    DYN_CHECK(b, DYN_ERR_INVALID, "dyn_batch_sync: NULL handle");
+    DYN_CUDA(cudaStreamSynchronize(b->stream));
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        const int rc = dyn::read_scalars(b->members[i]);
+        if (rc != DYN_OK) return dyn::fail(rc, "member " + std::to_string(i) + ": " + dyn_last_error());
+    }
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_launches(dyn_batch_t b, int spme, uint32_t* fixed, uint32_t* rebuild,
+                                  uint32_t* periodic) {
+    DYN_CHECK(b && fixed && rebuild && periodic, DYN_ERR_INVALID, "dyn_batch_launches: NULL argument");
+    DYN_CUDA(cudaStreamSynchronize(b->stream));
+    b->ctx.views.clear();
+    for (dyn_sys_t m : b->members) b->ctx.views.push_back(m->v);
+    const Target T{nullptr, &b->ctx, b->stream};
+    // a collecting pass records one entry per batched launch and launches
+    // nothing; cuFFT's per-member kernels are not counted
+    auto count = [&](auto&& enqueue) {
+        b->ctx.collecting = true;
+        b->ctx.launches = 0;
+        enqueue();
+        b->ctx.collecting = false;
+        return b->ctx.launches;
+    };
+    const uint32_t all = count([&] { enqueue_batch_step(b, 0.002f, spme != 0, true, false, 0, 0); });
+    *rebuild = count([&] { dyn::launch_rebuild(T, false); });
+    *periodic = count([&] { dyn::launch_periodic(T); });
+    *fixed = all - *rebuild - *periodic;
+    return upload_maps(b);
+}

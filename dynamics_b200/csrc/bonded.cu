@@ -18,12 +18,26 @@ __device__ __forceinline__ void addf(long long* f, uint32_t i, float3 v) {
     fix_atomic_add(p + 2, fix_from_float(v.z));
 }
 
-template <bool ENERGY>
-__global__ void k_bonded(SysView v) {
+// Exact float64 minimum-image displacement b - a of two float32 positions
+// (the shift is a whole number of box extents), for the energies.
+__device__ __forceinline__ double3 dd_min_image(float3 a, float3 bpos, const BoxDev& b) {
+    const float3 d = bpos - a;
+    double3 r;
+    r.x = (double)bpos.x - (double)a.x - (double)rintf(d.x * b.inv_ext[0]) * (double)b.ext[0];
+    r.y = (double)bpos.y - (double)a.y - (double)rintf(d.y * b.inv_ext[1]) * (double)b.ext[1];
+    r.z = (double)bpos.z - (double)a.z - (double)rintf(d.z * b.inv_ext[2]) * (double)b.ext[2];
+    return r;
+}
+__device__ __forceinline__ double ddot(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double3 dcross(double3 a, double3 b) {
+    return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_bonded, (), ()) {
     const BoxDev b = *v.box;
     double e_acc = 0.0, w_acc = 0.0;
     const uint32_t total = v.nbond + v.nangle + v.ndih;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
         if (t < v.nbond) {
             const uint2 ij = v.bond[t];
             const float2 par = v.bond_par[t];  // k, r0
@@ -33,7 +47,11 @@ __global__ void k_bonded(SysView v) {
             const float3 f0 = d * (2.0f * par.x * dr / fmaxf(r, 1e-8f));
             addf(v.aforce, ij.x, f0);
             addf(v.aforce, ij.y, f3(-f0.x, -f0.y, -f0.z));
-            if (ENERGY) e_acc += (double)(par.x * dr * dr);
+            if (ENERGY) {
+                const double3 e = dd_min_image(xyz(v.apos[ij.x]), xyz(v.apos[ij.y]), b);
+                const double de = sqrt(ddot(e, e)) - (double)par.y;
+                e_acc += (double)par.x * de * de;
+            }
             w_acc += (double)dot3(d, f0);
         } else if (t < v.nbond + v.nangle) {
             const uint4 ijk = v.angle[t - v.nbond];
@@ -57,7 +75,14 @@ __global__ void k_bonded(SysView v) {
             addf(v.aforce, ijk.x, f0);
             addf(v.aforce, ijk.y, f1);
             addf(v.aforce, ijk.z, f2);
-            if (ENERGY) e_acc += (double)(par.x * dth * dth);
+            if (ENERGY) {
+                const double3 a0 = dd_min_image(p1, xyz(v.apos[ijk.x]), b);
+                const double3 a2 = dd_min_image(p1, xyz(v.apos[ijk.z]), b);
+                double c = ddot(a0, a2) / sqrt(ddot(a0, a0) * ddot(a2, a2));
+                c = c > 1.0 ? 1.0 : (c < -1.0 ? -1.0 : c);
+                const double dt = acos(c) - (double)par.y;
+                e_acc += (double)par.x * dt * dt;
+            }
             w_acc += (double)(dot3(v01, f0) + dot3(v21, f2));
         } else {
             const uint32_t k = t - v.nbond - v.nangle;
@@ -87,7 +112,16 @@ __global__ void k_bonded(SysView v) {
             addf(v.aforce, q.y, f1);
             addf(v.aforce, q.z, f2);
             addf(v.aforce, q.w, f3v);
-            if (ENERGY) e_acc += (double)(par.x * (1.0f + cn));
+            if (ENERGY) {
+                const double3 c1 = dd_min_image(p0, xyz(v.apos[q.y]), b);
+                const double3 c2 = dd_min_image(xyz(v.apos[q.y]), xyz(v.apos[q.z]), b);
+                const double3 c3 = dd_min_image(xyz(v.apos[q.z]), xyz(v.apos[q.w]), b);
+                const double3 m1 = dcross(c1, c2), m2 = dcross(c2, c3);
+                const double xx = ddot(m1, m2);
+                const double yy = ddot(dcross(m1, m2), c2) / sqrt(ddot(c2, c2));
+                const double ph = atan2(yy, xx);
+                e_acc += (double)par.x * (1.0 + cos((double)par.y * ph - (double)par.z));
+            }
             // virial relative to atom 1 (src/bonded.rs:123-130)
             w_acc += (double)(dot3(f3(-b1.x, -b1.y, -b1.z), f0) + dot3(b2, f2) + dot3(b2 + b3, f3v));
         }
@@ -95,7 +129,7 @@ __global__ void k_bonded(SysView v) {
     double xs[3] = {e_acc, 0.0, w_acc};
     block_sum_d<3>(xs);
     if (threadIdx.x == 0) {
-        double* p = v.partials + ((size_t)REG_BOND * v.max_blocks + blockIdx.x) * 4;
+        double* p = v.partials + ((size_t)REG_BOND * v.max_blocks + bk.idx) * 4;
         p[0] = xs[0]; p[1] = xs[1]; p[2] = xs[2]; p[3] = 0.0;
     }
 }
@@ -111,10 +145,10 @@ int bond_blocks(const SysView& v) {
     return (int)(bl < v.max_blocks ? bl : v.max_blocks);
 }
 
-void launch_bonded(const SysView& v, cudaStream_t st, bool energy) {
-    if (v.nbond + v.nangle + v.ndih == 0) return;
-    if (energy) k_bonded<true><<<v.nb[REG_BOND], BT, 0, st>>>(v);
-    else k_bonded<false><<<v.nb[REG_BOND], BT, 0, st>>>(v);
+void launch_bonded(const Target& t, bool energy) {
+    auto g = [](const SysView& v) { return v.nbond + v.nangle + v.ndih ? (int)v.nb[REG_BOND] : 0; };
+    if (energy) t.launch(k_bonded<true>, k_bonded_batch<true>, g, BT, 0);
+    else t.launch(k_bonded<false>, k_bonded_batch<false>, g, BT, 0);
 }
 
 }  // namespace dyn

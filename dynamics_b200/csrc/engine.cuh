@@ -19,6 +19,9 @@
 
 #include <cufft.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "common.cuh"
 
 #define WCL 8             // waters per cluster
@@ -150,10 +153,10 @@ struct SysView {
     uint32_t integrator, thermostat, barostat;
     uint32_t spme_interval, com_interval, recenter_interval;
     double e_self;          // Ewald self energy -alpha/sqrt(pi) sum q^2
-    // u(x) = erfc(x) + 2x/sqrt(pi) exp(-x^2) and erfc(x) at x = alpha r, as
-    // polynomials in s = 2r/rc - 1 on [-1, 1] (Chebyshev interpolation,
-    // power basis, Horner in float32): force = qq u / r^3, energy = qq erfc / r
-    float poly_g[NPOLY_G];        // g(r^2) in t = 2 r^2 / rc^2 - 1 (power basis)
+    // screened-Coulomb force q q (r^-3 + g(r^2)) d: g as a polynomial in
+    // t = 2 r^2 / rc^2 - 1 (Chebyshev interpolation, power basis, Horner in
+    // float32)
+    float poly_g[NPOLY_G];
     float two_over_rc2;
     // IF-node handles of the captured step graph: the displacement check
     // sets cond_rebuild, the step finalisation sets cond_periodic; only
@@ -161,6 +164,111 @@ struct SysView {
     cudaGraphConditionalHandle cond_rebuild, cond_periodic;
     uint32_t use_cond;
     uint32_t nb[NREGION];   // blocks each region's kernel is launched with
+    int plan_f, plan_b;     // cuFFT plans (host-side handles, used by launch code only)
+};
+
+// ---------------------------------------------------------------------------
+// One kernel body, two launch forms.  Every step kernel is written once as
+// the body of NAME##_B::run(v, bk, ...), where bk is the block's index and
+// the block count within its system.  NAME is the single-system kernel (the
+// SysView in parameter space); NAME##_batch runs the same body for many
+// systems in one launch: block b works on system bm[b].x as its local block
+// bm[b].y & 0xFFFF of bm[b].y >> 16, reading that system's SysView from
+// global memory.  The block ranges are laid out by Target::launch below.
+// ---------------------------------------------------------------------------
+struct Blk { uint32_t idx, cnt; };
+
+#define DYN_UNPAREN(...) __VA_ARGS__
+
+#define DYN_KERNEL(LB, NAME, PARAMS, ARGS)                                                          \
+    struct NAME##_B {                                                                                \
+        static __device__ __forceinline__ void run(const SysView& v, Blk bk DYN_UNPAREN PARAMS);     \
+    };                                                                                               \
+    __global__ void LB NAME(const __grid_constant__ SysView v DYN_UNPAREN PARAMS) {                  \
+        NAME##_B::run(v, Blk{blockIdx.x, gridDim.x} DYN_UNPAREN ARGS);                               \
+    }                                                                                                \
+    __global__ void LB NAME##_batch(const SysView* __restrict__ vs,                                  \
+                                    const uint2* __restrict__ bm DYN_UNPAREN PARAMS) {               \
+        const uint2 m = bm[blockIdx.x];                                                              \
+        NAME##_B::run(vs[m.x], Blk{m.y & 0xFFFFu, m.y >> 16} DYN_UNPAREN ARGS);                      \
+    }                                                                                                \
+    __device__ __forceinline__ void NAME##_B::run(const SysView& v, Blk bk DYN_UNPAREN PARAMS)
+
+#define DYN_KERNEL_T(TDECL, TARGS, LB, NAME, PARAMS, ARGS)                                          \
+    template <DYN_UNPAREN TDECL>                                                                     \
+    struct NAME##_B {                                                                                \
+        static __device__ __forceinline__ void run(const SysView& v, Blk bk DYN_UNPAREN PARAMS);     \
+    };                                                                                               \
+    template <DYN_UNPAREN TDECL>                                                                     \
+    __global__ void LB NAME(const __grid_constant__ SysView v DYN_UNPAREN PARAMS) {                  \
+        NAME##_B<DYN_UNPAREN TARGS>::run(v, Blk{blockIdx.x, gridDim.x} DYN_UNPAREN ARGS);            \
+    }                                                                                                \
+    template <DYN_UNPAREN TDECL>                                                                     \
+    __global__ void LB NAME##_batch(const SysView* __restrict__ vs,                                  \
+                                    const uint2* __restrict__ bm DYN_UNPAREN PARAMS) {               \
+        const uint2 m = bm[blockIdx.x];                                                              \
+        NAME##_B<DYN_UNPAREN TARGS>::run(vs[m.x], Blk{m.y & 0xFFFFu, m.y >> 16} DYN_UNPAREN ARGS);   \
+    }                                                                                                \
+    template <DYN_UNPAREN TDECL>                                                                     \
+    __device__ __forceinline__ void NAME##_B<DYN_UNPAREN TARGS>::run(const SysView& v,               \
+                                                                     Blk bk DYN_UNPAREN PARAMS)
+
+// ---------------------------------------------------------------------------
+// Launch target: one system, or every system of a batch.  The launch code
+// of each stage is written once against a Target; grid(v) gives the blocks
+// one system needs (0 = skip it).  For a batch, the per-system ranges are
+// concatenated into one block map and the NAME##_batch kernel runs them all.
+// ---------------------------------------------------------------------------
+struct BatchCtx;
+struct BlockMap { uint32_t total; const uint2* d_map; };
+uint32_t batch_size(const BatchCtx* b);
+const SysView& batch_view(const BatchCtx* b, uint32_t i);
+const SysView* batch_dviews(const BatchCtx* b);
+bool batch_collecting(const BatchCtx* b);
+BlockMap batch_map(BatchCtx* b, const std::vector<uint32_t>& blocks);
+
+struct Target {
+    const SysView* v = nullptr;   // single system
+    BatchCtx* b = nullptr;        // batch (v == nullptr)
+    cudaStream_t st = nullptr;
+
+    template <typename KP, typename KB, typename G, typename... A>
+    void launch(KP kp, KB kb, G grid, int threads, size_t smem, A... a) const {
+        if (v) {
+            const int g = grid(*v);
+            if (g > 0) kp<<<g, threads, smem, st>>>(*v, a...);
+            return;
+        }
+        const uint32_t n = batch_size(b);
+        std::vector<uint32_t> bl(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const int g = grid(batch_view(b, i));
+            bl[i] = g > 0 ? (uint32_t)g : 0u;
+        }
+        const BlockMap m = batch_map(b, bl);
+        if (m.total && !batch_collecting(b)) kb<<<m.total, threads, smem, st>>>(batch_dviews(b), m.d_map, a...);
+    }
+    // host-side work per system (library calls such as cuFFT); skipped
+    // while a batch only collects its block maps
+    template <typename F>
+    void each(F f) const {
+        if (v) { f(*v); return; }
+        if (batch_collecting(b)) return;
+        for (uint32_t i = 0; i < batch_size(b); ++i) f(batch_view(b, i));
+    }
+    template <typename F>
+    size_t max_over(F f) const {
+        if (v) return f(*v);
+        size_t m = 0;
+        for (uint32_t i = 0; i < batch_size(b); ++i) m = std::max<size_t>(m, f(batch_view(b, i)));
+        return m;
+    }
+    bool any(bool (*pred)(const SysView&)) const {
+        if (v) return pred(*v);
+        for (uint32_t i = 0; i < batch_size(b); ++i)
+            if (pred(batch_view(b, i))) return true;
+        return false;
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -169,13 +277,13 @@ struct SysView {
 namespace dyn {
 
 // nblist.cu
-void launch_displacement_check(const SysView& v, cudaStream_t st);
-void launch_rebuild(const SysView& v, cudaStream_t st, bool force);
-void launch_gather_atoms(const SysView& v, cudaStream_t st);
+void launch_displacement_check(const Target& t);
+void launch_rebuild(const Target& t, bool force);
+void launch_gather_atoms(const Target& t);
 
 // pair.cu
-void launch_pairs(const SysView& v, cudaStream_t st, bool energy);
-void launch_pair14(const SysView& v, cudaStream_t st, bool energy);
+void launch_pairs(const Target& t, bool energy);
+void launch_pair14(const Target& t, bool energy);
 int pair_blocks_ww(const SysView& v);
 int pair_ww_setup(const SysView& v);
 int ww_tile_blocks(const SysView& v);
@@ -185,18 +293,18 @@ int pair14_blocks(const SysView& v);
 // pme.cu
 int pme_init(SysView& v, cufftHandle* plan_f, cufftHandle* plan_b, cudaStream_t st);
 void pme_free(SysView& v, cufftHandle plan_f, cufftHandle plan_b);
-void launch_pme(const SysView& v, cudaStream_t st, cufftHandle plan_f, cufftHandle plan_b);
-void launch_corrections(const SysView& v, cudaStream_t st);
+void launch_pme(const Target& t);
+void launch_corrections(const Target& t);
 int pme_blocks(const SysView& v);
 int gather_blocks(const SysView& v);
 int corr_blocks(const SysView& v);
 
 // integrate.cu
-void launch_first_half(const SysView& v, cudaStream_t st, float dt);
-void launch_second_half(const SysView& v, cudaStream_t st, float dt);
-void launch_finalize(const SysView& v, cudaStream_t st, float dt, bool energy, bool thermo);
-void launch_periodic(const SysView& v, cudaStream_t st);
-void launch_bonded(const SysView& v, cudaStream_t st, bool energy);
+void launch_first_half(const Target& t, float dt);
+void launch_second_half(const Target& t, float dt);
+void launch_finalize(const Target& t, float dt, bool energy, bool thermo);
+void launch_periodic(const Target& t);
+void launch_bonded(const Target& t, bool energy);
 int kick_blocks_w(const SysView& v);
 int kick_blocks_a(const SysView& v);
 int bond_blocks(const SysView& v);

@@ -110,14 +110,14 @@ __device__ __forceinline__ bool finite3(float3 a) {
 // ---------------------------------------------------------------------------
 // first half of the step
 // ---------------------------------------------------------------------------
-__global__ void k_water_first(SysView v, float dt) {
+DYN_KERNEL(, k_water_first, (, float dt), (, dt)) {
     const BoxDev b = *v.box;
     const uint64_t step = v.sc->step;
     const bool lm = v.integrator == DYN_INTEGRATOR_LANGEVIN_MIDDLE;
     const float c = expf(-v.gamma * dt);
     const float num = KB_NATIVE * v.temperature * fmaxf(1.0f - c * c, 0.f);
     const float sg_o = sqrtf(num / OPC_O_MASS), sg_h = sqrtf(num / OPC_H_MASS);
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+    for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.nw_cap; s += bk.cnt * blockDim.x) {
         const uint32_t id = v.wid[s];
         if (id == INVALID_ID) continue;
         float3 o = xyz(v.wpos[4 * s]), h0 = xyz(v.wpos[4 * s + 1]), h1 = xyz(v.wpos[4 * s + 2]);
@@ -148,12 +148,12 @@ __global__ void k_water_first(SysView v, float dt) {
     }
 }
 
-__global__ void k_atom_first(SysView v, float dt) {
+DYN_KERNEL(, k_atom_first, (, float dt), (, dt)) {
     const uint64_t step = v.sc->step;
     const bool lm = v.integrator == DYN_INTEGRATOR_LANGEVIN_MIDDLE;
     const float c = expf(-v.gamma * dt);
     const float num = KB_NATIVE * v.temperature * fmaxf(1.0f - c * c, 0.f);
-    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+    for (uint32_t a = bk.idx * blockDim.x + threadIdx.x; a < v.na; a += bk.cnt * blockDim.x) {
         if (v.astatic && v.astatic[a]) continue;
         float4 p = v.apos[a];
         float3 x = xyz(p), vel = xyz(v.avel[a]);
@@ -190,10 +190,10 @@ __device__ __forceinline__ float3 ldfix3sum(const long long* p, const long long*
 // keeps (M v_com^2 + omega . L), and the intramolecular virial
 // sum_s (r_s - R_com) . F_s, which turns the site virial into the molecular
 // virial a rigid-water pressure needs.
-__global__ void k_water_kick(SysView v, float dt) {
+DYN_KERNEL(, k_water_kick, (, float dt), (, dt)) {
     const BoxDev b = *v.box;
     double ke = 0.0, ket = 0.0, ker = 0.0, wi = 0.0;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+    for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.nw_cap; s += bk.cnt * blockDim.x) {
         const uint32_t id = v.wid[s];
         if (id == INVALID_ID) continue;
         const long long* f = v.wforce + (size_t)s * 12;
@@ -230,14 +230,14 @@ __global__ void k_water_kick(SysView v, float dt) {
     double x[4] = {ke, ket, ker, wi};
     block_sum_d<4>(x);
     if (threadIdx.x == 0) {
-        double* p = v.partials + ((size_t)REG_KICK_W * v.max_blocks + blockIdx.x) * 4;
+        double* p = v.partials + ((size_t)REG_KICK_W * v.max_blocks + bk.idx) * 4;
         p[0] = x[0]; p[1] = x[1]; p[2] = x[2]; p[3] = x[3];
     }
 }
 
-__global__ void k_atom_kick(SysView v, float dt) {
+DYN_KERNEL(, k_atom_kick, (, float dt), (, dt)) {
     double ke = 0.0;
-    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+    for (uint32_t a = bk.idx * blockDim.x + threadIdx.x; a < v.na; a += bk.cnt * blockDim.x) {
         if (v.astatic && v.astatic[a]) continue;
         const float3 f = ldfix3sum(v.aforce + 3 * (size_t)a, v.arecip + 3 * (size_t)a);
         // kick_and_calc_accel with the MAX_ACCEL clamp (src/integrate.rs:521-535)
@@ -253,7 +253,7 @@ __global__ void k_atom_kick(SysView v, float dt) {
     double x[2] = {ke, ke};
     block_sum_d<2>(x);
     if (threadIdx.x == 0) {
-        double* p = v.partials + ((size_t)REG_KICK_A * v.max_blocks + blockIdx.x) * 4;
+        double* p = v.partials + ((size_t)REG_KICK_A * v.max_blocks + bk.idx) * 4;
         p[0] = x[0]; p[1] = x[1]; p[2] = x[0]; p[3] = 0.0;
     }
 }
@@ -286,8 +286,7 @@ __device__ double gamma_mt(double shape, uint64_t step, uint64_t seed) {
     return d;
 }
 
-template <bool ENERGY>
-__global__ void k_finalize(SysView v, float dt, bool thermo) {
+DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (, dt, thermo)) {
     double ww[4] = {0, 0, 0, 0}, ws[4] = {0, 0, 0, 0}, sw[4] = {0, 0, 0, 0}, ss[4] = {0, 0, 0, 0};
     double p14[4] = {0, 0, 0, 0}, bo[4] = {0, 0, 0, 0}, kw[4] = {0, 0, 0, 0}, ka[4] = {0, 0, 0, 0};
     double co[4] = {0, 0, 0, 0};
@@ -396,19 +395,19 @@ __global__ void k_finalize(SysView v, float dt, bool thermo) {
             due = 1u;
         if ((v.flags & DYN_FLAG_RESET_ANGLE) && v.nw && next % 1000 == 0) due = 1u;
         sc->step = next;
-        if (v.use_cond) cudaGraphSetConditional(v.cond_periodic, due);
+        if (v.use_cond && due) cudaGraphSetConditional(v.cond_periodic, 1u);
     }
 }
 
 // velocity scaling (CSVR) and C-rescale of positions / box
-__global__ void k_scale(SysView v) {
+DYN_KERNEL(, k_scale, (), ()) {
     const double lam_d = v.sc->csvr_lambda, mu_d = v.sc->baro_mu;
     if (lam_d == 1.0 && mu_d == 1.0) return;
     const float lam = (float)lam_d, mu = (float)mu_d;
     const BoxDev b = *v.box;
     const float3 cen = f3(b.lo[0] + 0.5f * b.ext[0], b.lo[1] + 0.5f * b.ext[1], b.lo[2] + 0.5f * b.ext[2]);
     const float vs = lam / mu;  // C-rescale scales momenta by 1/mu
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x, stride = bk.cnt * blockDim.x;
     for (uint32_t s = tid; s < v.nw_cap; s += stride) {
         if (v.wid[s] == INVALID_ID) continue;
         for (int k = 0; k < 3; ++k) {
@@ -447,7 +446,7 @@ __global__ void k_scale(SysView v) {
     __syncthreads();
     if (threadIdx.x != 0) return;
     __threadfence();
-    if (atomicAdd(&v.sc->ctr_scale, 1u) != gridDim.x - 1) return;
+    if (atomicAdd(&v.sc->ctr_scale, 1u) != bk.cnt - 1) return;
     BoxDev nb = b;
     for (int k = 0; k < 3; ++k) {
         const double c = (double)b.lo[k] + 0.5 * (double)b.ext[k];
@@ -461,18 +460,18 @@ __global__ void k_scale(SysView v) {
 }
 
 // COM motion removal (src/com_zero.rs:57-81) every com_interval steps
-__global__ void k_com_reduce(SysView v) {
+DYN_KERNEL(, k_com_reduce, (), ()) {
     const uint64_t next = v.sc->step;  // advanced by k_finalize
     const bool on = (v.flags & DYN_FLAG_COM_REMOVAL) && v.com_interval && (next % v.com_interval == 0);
     double x[4] = {0, 0, 0, 0};
     if (on) {
-        for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+        for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.nw_cap; s += bk.cnt * blockDim.x) {
             if (v.wid[s] == INVALID_ID) continue;
             const float3 p = xyz(v.wvel[3 * s]) * OPC_O_MASS + xyz(v.wvel[3 * s + 1]) * OPC_H_MASS +
                              xyz(v.wvel[3 * s + 2]) * OPC_H_MASS;
             x[0] += p.x; x[1] += p.y; x[2] += p.z; x[3] += OPC_MASS_MOL;
         }
-        for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+        for (uint32_t a = bk.idx * blockDim.x + threadIdx.x; a < v.na; a += bk.cnt * blockDim.x) {
             if (v.astatic && v.astatic[a]) continue;
             const float3 p = xyz(v.avel[a]) * v.amass[a];
             x[0] += p.x; x[1] += p.y; x[2] += p.z; x[3] += v.amass[a];
@@ -480,12 +479,12 @@ __global__ void k_com_reduce(SysView v) {
     }
     block_sum_d<4>(x);
     if (threadIdx.x == 0) {
-        double* p = v.partials + ((size_t)REG_COM * v.max_blocks + blockIdx.x) * 4;
+        double* p = v.partials + ((size_t)REG_COM * v.max_blocks + bk.idx) * 4;
         p[0] = x[0]; p[1] = x[1]; p[2] = x[2]; p[3] = x[3];
     }
 }
 
-__global__ void k_com_apply(SysView v) {
+DYN_KERNEL(, k_com_apply, (), ()) {
     const uint64_t next = v.sc->step;  // advanced by k_finalize
     const bool on = (v.flags & DYN_FLAG_COM_REMOVAL) && v.com_interval && (next % v.com_interval == 0);
     if (!on) return;
@@ -504,7 +503,7 @@ __global__ void k_com_apply(SysView v) {
     }
     __syncthreads();
     const float3 c = vc;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+    for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.nw_cap; s += bk.cnt * blockDim.x) {
         if (v.wid[s] == INVALID_ID) continue;
         for (int k = 0; k < 3; ++k) {
             float4 q = v.wvel[3 * s + k];
@@ -512,7 +511,7 @@ __global__ void k_com_apply(SysView v) {
             v.wvel[3 * s + k] = q;
         }
     }
-    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
+    for (uint32_t a = bk.idx * blockDim.x + threadIdx.x; a < v.na; a += bk.cnt * blockDim.x) {
         if (v.astatic && v.astatic[a]) continue;
         float4 q = v.avel[a];
         q.x -= c.x; q.y -= c.y; q.z -= c.z;
@@ -521,7 +520,7 @@ __global__ void k_com_apply(SysView v) {
 }
 
 // SimBox::recenter (src/barostat.rs:111-137) every recenter_interval steps
-__global__ void k_recenter(SysView v) {
+DYN_KERNEL(, k_recenter, (), ()) {
     const uint64_t next = v.sc->step;  // advanced by k_finalize
     const bool on = (v.flags & DYN_FLAG_RECENTER) && v.recenter_interval && v.na &&
                     (next % v.recenter_interval == 0);
@@ -541,11 +540,11 @@ __global__ void k_recenter(SysView v) {
 }
 
 // reset_angle (src/solvent/opc_settle.rs:202-219) every 1000 steps
-__global__ void k_reset_angle(SysView v) {
+DYN_KERNEL(, k_reset_angle, (), ()) {
     const uint64_t next = v.sc->step;  // advanced by k_finalize
     if (!(v.flags & DYN_FLAG_RESET_ANGLE) || next % 1000 != 0) return;
     const BoxDev b = *v.box;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
+    for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.nw_cap; s += bk.cnt * blockDim.x) {
         if (v.wid[s] == INVALID_ID) continue;
         const float3 o = xyz(v.wpos[4 * s]);
         const float3 h0 = o + min_image_rint(xyz(v.wpos[4 * s + 1]) - o, b);
@@ -581,34 +580,44 @@ namespace dyn {
 int kick_blocks_w(const SysView& v) { return iblocks(v, v.nw_cap); }
 int kick_blocks_a(const SysView& v) { return iblocks(v, v.na); }
 
-void launch_first_half(const SysView& v, cudaStream_t st, float dt) {
-    if (v.nw) k_water_first<<<iblocks(v, v.nw_cap), IT, 0, st>>>(v, dt);
-    if (v.na) k_atom_first<<<iblocks(v, v.na), IT, 0, st>>>(v, dt);
+void launch_first_half(const Target& t, float dt) {
+    t.launch(k_water_first, k_water_first_batch, [](const SysView& v) { return v.nw ? iblocks(v, v.nw_cap) : 0; },
+             IT, 0, dt);
+    t.launch(k_atom_first, k_atom_first_batch, [](const SysView& v) { return v.na ? iblocks(v, v.na) : 0; }, IT, 0,
+             dt);
 }
 
-void launch_second_half(const SysView& v, cudaStream_t st, float dt) {
-    if (v.nw) k_water_kick<<<v.nb[REG_KICK_W], IT, 0, st>>>(v, dt);
-    if (v.na) k_atom_kick<<<v.nb[REG_KICK_A], IT, 0, st>>>(v, dt);
+void launch_second_half(const Target& t, float dt) {
+    t.launch(k_water_kick, k_water_kick_batch, [](const SysView& v) { return v.nw ? (int)v.nb[REG_KICK_W] : 0; },
+             IT, 0, dt);
+    t.launch(k_atom_kick, k_atom_kick_batch, [](const SysView& v) { return v.na ? (int)v.nb[REG_KICK_A] : 0; }, IT,
+             0, dt);
 }
 
-void launch_finalize(const SysView& v, cudaStream_t st, float dt, bool energy, bool thermo) {
-    if (energy) k_finalize<true><<<1, 256, 0, st>>>(v, dt, thermo);
-    else k_finalize<false><<<1, 256, 0, st>>>(v, dt, thermo);
+void launch_finalize(const Target& t, float dt, bool energy, bool thermo) {
+    auto one = [](const SysView&) { return 1; };
+    if (energy) t.launch(k_finalize<true>, k_finalize_batch<true>, one, 256, 0, dt, thermo);
+    else t.launch(k_finalize<false>, k_finalize_batch<false>, one, 256, 0, dt, thermo);
     if (!thermo) return;
-    const bool scales = (v.integrator == DYN_INTEGRATOR_VERLET_VELOCITY && v.thermostat == DYN_THERMO_CSVR) ||
-                        v.barostat == DYN_BARO_CRESCALE;
-    if (!scales) return;
-    k_scale<<<iblocks(v, (uint64_t)v.nw_cap + v.na), IT, 0, st>>>(v);
+    t.launch(k_scale, k_scale_batch,
+             [](const SysView& v) {
+                 const bool scales =
+                     (v.integrator == DYN_INTEGRATOR_VERLET_VELOCITY && v.thermostat == DYN_THERMO_CSVR) ||
+                     v.barostat == DYN_BARO_CRESCALE;
+                 return scales ? iblocks(v, (uint64_t)v.nw_cap + v.na) : 0;
+             },
+             IT, 0);
 }
 
-void launch_periodic(const SysView& v, cudaStream_t st) {
-    if (v.flags & DYN_FLAG_COM_REMOVAL) {
-        k_com_reduce<<<v.nb[REG_COM], IT, 0, st>>>(v);
-        k_com_apply<<<v.nb[REG_COM], IT, 0, st>>>(v);
-    }
-    if ((v.flags & DYN_FLAG_RECENTER) && v.na) k_recenter<<<1, 256, 0, st>>>(v);
-    if ((v.flags & DYN_FLAG_RESET_ANGLE) && v.nw) k_reset_angle<<<iblocks(v, v.nw_cap), IT, 0, st>>>(v);
+void launch_periodic(const Target& t) {
+    auto com = [](const SysView& v) { return (v.flags & DYN_FLAG_COM_REMOVAL) ? (int)v.nb[REG_COM] : 0; };
+    t.launch(k_com_reduce, k_com_reduce_batch, com, IT, 0);
+    t.launch(k_com_apply, k_com_apply_batch, com, IT, 0);
+    t.launch(k_recenter, k_recenter_batch,
+             [](const SysView& v) { return ((v.flags & DYN_FLAG_RECENTER) && v.na) ? 1 : 0; }, 256, 0);
+    t.launch(k_reset_angle, k_reset_angle_batch,
+             [](const SysView& v) { return ((v.flags & DYN_FLAG_RESET_ANGLE) && v.nw) ? iblocks(v, v.nw_cap) : 0; },
+             IT, 0);
 }
-
 
 }  // namespace dyn

@@ -53,11 +53,11 @@ __device__ __forceinline__ uint32_t column_of(float3 p, const BoxDev& b, uint32_
 // ---------------------------------------------------------------------------
 // displacement check
 // ---------------------------------------------------------------------------
-__global__ void k_disp_check(SysView v) {
+DYN_KERNEL(, k_disp_check, (), ()) {
     const BoxDev b = *v.box;
     float m = 0.f;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x;
+    const uint32_t stride = bk.cnt * blockDim.x;
     for (uint32_t s = tid; s < v.nw_cap; s += stride) {
         if (v.wid[s] == INVALID_ID) continue;
         const float3 d = min_image_rint(xyz(v.wpos[4 * s]) - xyz(v.wref[s]), b);
@@ -76,7 +76,7 @@ __global__ void k_disp_check(SysView v) {
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    if (atomicAdd(&v.sc->ctr_disp, 1u) != gridDim.x - 1) return;
+    if (atomicAdd(&v.sc->ctr_disp, 1u) != bk.cnt - 1) return;
     // the last block to finish sees every block's maximum and decides:
     // rebuild when the largest displacement reaches half the buffer
     __threadfence();
@@ -87,19 +87,19 @@ __global__ void k_disp_check(SysView v) {
     v.sc->need_rebuild = need;
     if (mx >= 1e29f) v.sc->nonfinite = 1u;
     v.sc->ctr_disp = 0u;
-    if (v.use_cond) cudaGraphSetConditional(v.cond_rebuild, need);
+    if (v.use_cond && need) cudaGraphSetConditional(v.cond_rebuild, 1u);
 }
 
 // ---------------------------------------------------------------------------
 // column binning
 // ---------------------------------------------------------------------------
-__global__ void k_col_clear(SysView v, bool force) {
+DYN_KERNEL(, k_col_clear, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bk.idx == 0 && threadIdx.x == 0) {
         v.sc->list_pairs = 0ull;
         v.sc->union_max = 0u;
     }
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= v.ncol; c += gridDim.x * blockDim.x) {
+    for (uint32_t c = bk.idx * blockDim.x + threadIdx.x; c <= v.ncol; c += bk.cnt * blockDim.x) {
         if (c < v.ncol) {
             v.col_count[c] = 0; v.col_fill[c] = 0;
             v.acol_count[c] = 0; v.acol_fill[c] = 0;
@@ -107,11 +107,11 @@ __global__ void k_col_clear(SysView v, bool force) {
     }
 }
 
-__global__ void k_col_assign(SysView v, bool force) {
+DYN_KERNEL(, k_col_assign, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x;
+    const uint32_t stride = bk.cnt * blockDim.x;
     for (uint32_t s = tid; s < v.nw_cap; s += stride) {
         if (v.wid[s] == INVALID_ID) continue;
         float zf;
@@ -131,7 +131,7 @@ __global__ void k_col_assign(SysView v, bool force) {
 
 // Serial scan over columns in path order (only at rebuilds; a few hundred
 // columns).  Slots are contiguous along the path; padding sits at the end.
-__global__ void k_col_scan(SysView v, bool force) {
+DYN_KERNEL(, k_col_scan, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     if (threadIdx.x == 0) {
         uint32_t q = 0;
@@ -152,10 +152,10 @@ __global__ void k_col_scan(SysView v, bool force) {
     }
 }
 
-__global__ void k_col_bucket(SysView v, bool force) {
+DYN_KERNEL(, k_col_bucket, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x;
+    const uint32_t stride = bk.cnt * blockDim.x;
     for (uint32_t s = tid; s < v.nw_cap; s += stride) {
         if (v.wid[s] == INVALID_ID) continue;
         const uint32_t c = v.wcol[s];
@@ -168,10 +168,10 @@ __global__ void k_col_bucket(SysView v, bool force) {
 }
 
 // Rank inside the column by (z, original index): deterministic order.
-__global__ void k_col_rank(SysView v, bool force) {
+DYN_KERNEL(, k_col_rank, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x;
+    const uint32_t stride = bk.cnt * blockDim.x;
     for (uint32_t s = tid; s < v.nw_cap; s += stride) {
         if (v.wid[s] == INVALID_ID) continue;
         const uint32_t c = v.wcol[s];
@@ -198,10 +198,10 @@ __global__ void k_col_rank(SysView v, bool force) {
     }
 }
 
-__global__ void k_perm_init(SysView v, bool force) {
+DYN_KERNEL(, k_perm_init, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x;
+    const uint32_t stride = bk.cnt * blockDim.x;
     for (uint32_t s = tid; s < v.nw_cap; s += stride) {
         v.wtmp_id[s] = INVALID_ID;
         for (int k = 0; k < 10; ++k) v.wtmp[10 * s + k] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -213,10 +213,10 @@ __global__ void k_perm_init(SysView v, bool force) {
     }
 }
 
-__global__ void k_perm_scatter(SysView v, bool force) {
+DYN_KERNEL(, k_perm_scatter, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x;
+    const uint32_t stride = bk.cnt * blockDim.x;
     for (uint32_t s = tid; s < v.nw_cap; s += stride) {
         if (v.wid[s] == INVALID_ID) continue;
         const uint32_t n = v.wnew[s];
@@ -234,10 +234,10 @@ __global__ void k_perm_scatter(SysView v, bool force) {
     }
 }
 
-__global__ void k_perm_copyback(SysView v, bool force) {
+DYN_KERNEL(, k_perm_copyback, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x;
+    const uint32_t stride = bk.cnt * blockDim.x;
     for (uint32_t s = tid; s < v.nw_cap; s += stride) {
         for (int k = 0; k < 4; ++k) v.wpos[4 * s + k] = v.wtmp[10 * s + k];
         for (int k = 0; k < 3; ++k) v.wvel[3 * s + k] = v.wtmp[10 * s + 4 + k];
@@ -248,12 +248,12 @@ __global__ void k_perm_copyback(SysView v, bool force) {
 }
 
 // Bounding boxes of water clusters (O positions) and atom clusters.
-__global__ void k_bbox(SysView v, bool force) {
+DYN_KERNEL(, k_bbox, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
     const uint32_t nwc = v.sc->n_wclus, nac = v.sc->n_aclus;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x;
+    const uint32_t stride = bk.cnt * blockDim.x;
     for (uint32_t c = tid; c < nwc + nac; c += stride) {
         float3 lo = f3(1e30f, 1e30f, 1e30f), hi = f3(-1e30f, -1e30f, -1e30f);
         const bool is_w = c < nwc;
@@ -305,12 +305,11 @@ __device__ __forceinline__ bool excluded(const SysView& v, uint32_t a, uint32_t 
 }
 
 // MODE: 1 water(i)-atom(j), 2 atom(i)-water(j), 3 atom-atom
-template <int MODE>
-__global__ void k_list(SysView v, bool force) {
+DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
     const int lane = threadIdx.x & 31;
-    const uint32_t ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t ci = (bk.idx * blockDim.x + threadIdx.x) >> 5;
     const uint32_t ni = (MODE < 2) ? v.sc->n_wclus : v.sc->n_aclus;
     const uint32_t nj = (MODE == 0 || MODE == 2) ? v.sc->n_wclus : v.sc->n_aclus;
     if (ci >= ni) return;
@@ -362,12 +361,12 @@ __global__ void k_list(SysView v, bool force) {
 
 // Group bounding boxes over the O positions of the group's waters,
 // min-imaged to the first one.
-__global__ void k_group_bbox(SysView v, bool force) {
+DYN_KERNEL(, k_group_bbox, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
     const uint32_t nwc = v.sc->n_wclus;
     const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    for (uint32_t g = bk.idx * blockDim.x + threadIdx.x; g < ng; g += bk.cnt * blockDim.x) {
         float3 lo = f3(1e30f, 1e30f, 1e30f), hi = f3(-1e30f, -1e30f, -1e30f);
         bool have = false;
         float3 ref = f3(0.f, 0.f, 0.f);
@@ -388,13 +387,13 @@ __global__ void k_group_bbox(SysView v, bool force) {
 
 // j-cluster tile of every group: clusters within the water list radius of
 // the group box, ascending (one warp per group, ballot compaction).
-__global__ void k_tile_list(SysView v, bool force) {
+DYN_KERNEL(, k_tile_list, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
     const int lane = threadIdx.x & 31;
     const uint32_t nwc = v.sc->n_wclus;
     const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
-    const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t g = (bk.idx * blockDim.x + threadIdx.x) >> 5;
     if (g >= ng) return;
     const float4 c0 = v.gbb_c[g], h0 = v.gbb_h[g];
     const float r2 = v.r_ww * v.r_ww;
@@ -426,7 +425,7 @@ __global__ void k_tile_list(SysView v, bool force) {
 // ascending order.  Everything is deterministic.
 constexpr int UT = 256;
 
-__global__ void __launch_bounds__(UT) k_group_union(SysView v, bool force) {
+DYN_KERNEL(__launch_bounds__(UT), k_group_union, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
     const float r2 = v.r_ww * v.r_ww;
@@ -439,7 +438,7 @@ __global__ void __launch_bounds__(UT) k_group_union(SysView v, bool force) {
     __shared__ uint32_t sh_slot[UT];
     __shared__ uint32_t base_cnt, base_run, carry_slot;
     __shared__ uint8_t carry_need;
-    for (uint32_t g = blockIdx.x; g < ng; g += gridDim.x) {
+    for (uint32_t g = bk.idx; g < ng; g += bk.cnt) {
         if (tid < GRPW) {
             const uint32_t s = g * GRPW + tid;
             const bool ok = s < v.nw_cap && v.wid[s] != INVALID_ID;
@@ -535,14 +534,14 @@ __global__ void __launch_bounds__(UT) k_group_union(SysView v, bool force) {
     }
 }
 
-__global__ void k_rebuild_done(SysView v, bool force) {
+DYN_KERNEL(, k_rebuild_done, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     v.sc->need_rebuild = 0u;
     v.sc->rebuilds += 1ull;
 }
 
-__global__ void k_gather_atoms(SysView v) {
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.na_cap; s += gridDim.x * blockDim.x) {
+DYN_KERNEL(, k_gather_atoms, (), ()) {
+    for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.na_cap; s += bk.cnt * blockDim.x) {
         const uint32_t a = v.sidx[s];
         if (a != INVALID_ID) v.spos[s] = v.apos[a];
     }
@@ -558,38 +557,49 @@ inline int nblocks(uint64_t n, int threads, int cap = 148 * 8) {
 
 namespace dyn {
 
-void launch_displacement_check(const SysView& v, cudaStream_t st) {
-    k_disp_check<<<nblocks(v.nw_cap + v.na, 256), 256, 0, st>>>(v);
+void launch_displacement_check(const Target& t) {
+    t.launch(k_disp_check, k_disp_check_batch, [](const SysView& v) { return nblocks(v.nw_cap + v.na, 256); },
+             256, 0);
 }
 
-void launch_rebuild(const SysView& v, cudaStream_t st, bool force) {
+void launch_rebuild(const Target& t, bool force) {
     const int T = 256;
-    const uint32_t nmax = v.nw_cap > v.na_cap ? v.nw_cap : v.na_cap;
-    k_col_clear<<<nblocks(v.ncol + 1, T), T, 0, st>>>(v, force);
-    k_col_assign<<<nblocks(nmax, T), T, 0, st>>>(v, force);
-    k_col_scan<<<1, 64, 0, st>>>(v, force);
-    k_col_bucket<<<nblocks(nmax, T), T, 0, st>>>(v, force);
-    k_col_rank<<<nblocks(nmax, T), T, 0, st>>>(v, force);
-    k_perm_init<<<nblocks(nmax, T), T, 0, st>>>(v, force);
-    k_perm_scatter<<<nblocks(nmax, T), T, 0, st>>>(v, force);
-    k_perm_copyback<<<nblocks(v.nw_cap, T), T, 0, st>>>(v, force);
-    k_bbox<<<nblocks(v.nwclus_cap + v.naclus_cap, T), T, 0, st>>>(v, force);
+    auto nmax = [](const SysView& v) { return v.nw_cap > v.na_cap ? v.nw_cap : v.na_cap; };
+    t.launch(k_col_clear, k_col_clear_batch, [](const SysView& v) { return nblocks(v.ncol + 1, 256); }, T, 0, force);
+    t.launch(k_col_assign, k_col_assign_batch, [&](const SysView& v) { return nblocks(nmax(v), 256); }, T, 0, force);
+    t.launch(k_col_scan, k_col_scan_batch, [](const SysView&) { return 1; }, 64, 0, force);
+    t.launch(k_col_bucket, k_col_bucket_batch, [&](const SysView& v) { return nblocks(nmax(v), 256); }, T, 0, force);
+    t.launch(k_col_rank, k_col_rank_batch, [&](const SysView& v) { return nblocks(nmax(v), 256); }, T, 0, force);
+    t.launch(k_perm_init, k_perm_init_batch, [&](const SysView& v) { return nblocks(nmax(v), 256); }, T, 0, force);
+    t.launch(k_perm_scatter, k_perm_scatter_batch, [&](const SysView& v) { return nblocks(nmax(v), 256); }, T, 0,
+             force);
+    t.launch(k_perm_copyback, k_perm_copyback_batch, [](const SysView& v) { return nblocks(v.nw_cap, 256); }, T, 0,
+             force);
+    t.launch(k_bbox, k_bbox_batch, [](const SysView& v) { return nblocks(v.nwclus_cap + v.naclus_cap, 256); }, T, 0,
+             force);
     const int LT = 128;  // 4 warps per block, one i-cluster per warp
-    if (v.nw) {
-        k_group_bbox<<<nblocks(v.ngrp_cap, T), T, 0, st>>>(v, force);
-        k_tile_list<<<nblocks((uint64_t)v.ngrp_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
-        k_group_union<<<std::min<uint32_t>(v.ngrp_cap, 148 * 8), UT, 0, st>>>(v, force);
-    }
-    if (v.nw && v.na) {
-        k_list<1><<<nblocks((uint64_t)v.nwclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
-        k_list<2><<<nblocks((uint64_t)v.naclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
-    }
-    if (v.na) k_list<3><<<nblocks((uint64_t)v.naclus_cap * 32, LT, 1 << 30), LT, 0, st>>>(v, force);
-    k_rebuild_done<<<1, 1, 0, st>>>(v, force);
+    t.launch(k_group_bbox, k_group_bbox_batch, [](const SysView& v) { return v.nw ? nblocks(v.ngrp_cap, 256) : 0; },
+             T, 0, force);
+    t.launch(k_tile_list, k_tile_list_batch,
+             [](const SysView& v) { return v.nw ? nblocks((uint64_t)v.ngrp_cap * 32, 128, 1 << 30) : 0; }, LT, 0,
+             force);
+    t.launch(k_group_union, k_group_union_batch,
+             [](const SysView& v) { return v.nw ? (int)std::min<uint32_t>(v.ngrp_cap, 148 * 8) : 0; }, UT, 0, force);
+    t.launch(k_list<1>, k_list_batch<1>,
+             [](const SysView& v) { return v.nw && v.na ? nblocks((uint64_t)v.nwclus_cap * 32, 128, 1 << 30) : 0; },
+             LT, 0, force);
+    t.launch(k_list<2>, k_list_batch<2>,
+             [](const SysView& v) { return v.nw && v.na ? nblocks((uint64_t)v.naclus_cap * 32, 128, 1 << 30) : 0; },
+             LT, 0, force);
+    t.launch(k_list<3>, k_list_batch<3>,
+             [](const SysView& v) { return v.na ? nblocks((uint64_t)v.naclus_cap * 32, 128, 1 << 30) : 0; }, LT, 0,
+             force);
+    t.launch(k_rebuild_done, k_rebuild_done_batch, [](const SysView&) { return 1; }, 1, 0, force);
 }
 
-void launch_gather_atoms(const SysView& v, cudaStream_t st) {
-    if (v.na) k_gather_atoms<<<nblocks(v.na_cap, 256), 256, 0, st>>>(v);
+void launch_gather_atoms(const Target& t) {
+    t.launch(k_gather_atoms, k_gather_atoms_batch,
+             [](const SysView& v) { return v.na ? nblocks(v.na_cap, 256) : 0; }, 256, 0);
 }
 
 }  // namespace dyn

@@ -31,14 +31,27 @@ constexpr int PT = 128;  // threads per block (4 warps)
 // w accumulates the virial in float32
 struct Acc3 { double e_lj, e_c; float w; };
 
-// erfc-screened Coulomb, branch-free: force q q (r^-3 + g(r^2)) d with
+// Site positions are float32 and a periodic shift is a whole number of box
+// extents, so the displacement pi - (pj - sh) is exact in float64: energies
+// use that exact value (and float64 charge products) so that a total that
+// cancels to a small number keeps its relative accuracy; forces use the
+// float32 displacement.
+__device__ __forceinline__ void exact_disp(float3 pi, float3 pj, float3 sh, double& x, double& y, double& z) {
+    x = (double)pi.x - ((double)pj.x - (double)sh.x);
+    y = (double)pi.y - ((double)pj.y - (double)sh.y);
+    z = (double)pi.z - ((double)pj.z - (double)sh.z);
+}
+
+// erfc-screened Coulomb between site pi and site pj shifted by sh
+// (d = pi - (pj - sh)), branch-free: force q q (r^-3 + g(r^2)) d with
 // g(z) = 2 d/dz [erf(alpha sqrt z) / sqrt z] from the host-fitted polynomial
 // in t = 2 r^2 / rc^2 - 1 (no square root needed for the argument); zero for
 // r >= rc (src/cuda/cuda.cu:160-164).  On energy steps the energy
-// q q erfc(alpha r) / r uses erfcf and float64 sums, which keeps the total
-// potential energy within 1e-6 of float64 even where large terms cancel.
+// qqe erfc(alpha r) / r is evaluated in float64 from the exact displacement.
 template <bool ENERGY>
-__device__ __forceinline__ void coul(float3 d, float qq, const SysView& v, float3& f, Acc3& a) {
+__device__ __forceinline__ void coul(float3 pi, float3 pj, float3 sh, float qq, double qqe, const SysView& v,
+                                     float3& f, Acc3& a) {
+    const float3 d = pi - (pj - sh);
     const float r2 = dot3(d, d);
     const float rinv = rsqrtf(r2);
     const float t = fmaf(r2, v.two_over_rc2, -1.0f);
@@ -50,14 +63,23 @@ __device__ __forceinline__ void coul(float3 d, float qq, const SysView& v, float
     f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
     a.w = fmaf(fs, r2, a.w);
     if (ENERGY) {
-        if (r2 < v.rc2) a.e_c += (double)(qq * rinv) * (double)erfcf(v.alpha * r2 * rinv);
+        double x, y, z;
+        exact_disp(pi, pj, sh, x, y, z);
+        const double r2d = x * x + y * y + z * z;
+        const double rcd = (double)v.rc;
+        if (r2d < rcd * rcd) {
+            const double rd = sqrt(r2d);
+            a.e_c += qqe * erfc((double)v.alpha * rd) / rd;
+        }
     }
 }
 
-// 12-6 LJ (force_e_lj, src/forces.rs:10-21), branch-free, r <= lj_cutoff.
+// 12-6 LJ (force_e_lj, src/forces.rs:10-21) between pi and pj shifted by sh,
+// branch-free, r <= lj_cutoff; float64 energy from the exact displacement.
 template <bool ENERGY>
-__device__ __forceinline__ void lj(float3 d, float sig2, float eps, float ljc2, float scale,
-                                   float3& f, Acc3& a) {
+__device__ __forceinline__ void lj(float3 pi, float3 pj, float3 sh, float sig2, float eps, float ljc2,
+                                   float scale, float3& f, Acc3& a) {
+    const float3 d = pi - (pj - sh);
     const float r2 = dot3(d, d);
     const bool in = r2 <= ljc2;
     const float ir2 = __frcp_rn(in ? r2 : 1.0f);
@@ -67,7 +89,13 @@ __device__ __forceinline__ void lj(float3 d, float sig2, float eps, float ljc2, 
     fs = in ? fs : 0.0f;
     f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
     a.w = fmaf(fs, r2, a.w);
-    if (ENERGY) a.e_lj += in ? (double)(scale * 4.0f * eps) * (double)(sr6 * sr6 - sr6) : 0.0;
+    if (ENERGY && in) {
+        double x, y, z;
+        exact_disp(pi, pj, sh, x, y, z);
+        const double s2 = (double)sig2 / (x * x + y * y + z * z);
+        const double s6 = s2 * s2 * s2;
+        a.e_lj += 4.0 * (double)scale * (double)eps * (s6 * s6 - s6);
+    }
 }
 
 __device__ __forceinline__ float3 shift_of(float3 d, const BoxDev& b) {
@@ -91,12 +119,12 @@ __device__ __forceinline__ void add_fix3(long long* p, float3 f) {
 }
 
 template <bool ENERGY>
-__device__ __forceinline__ void write_partials(const SysView& v, int region, double el, double ec,
-                                               double w) {
+__device__ __forceinline__ void write_partials(const SysView& v, Blk bk, int region, double el,
+                                               double ec, double w) {
     double x[3] = {el, ec, w};
     block_sum_d<3>(x);
     if (threadIdx.x == 0) {
-        double* p = v.partials + ((size_t)region * v.max_blocks + blockIdx.x) * 4;
+        double* p = v.partials + ((size_t)region * v.max_blocks + bk.idx) * 4;
         p[0] = x[0]; p[1] = x[1]; p[2] = x[2]; p[3] = 0.0;
     }
 }
@@ -168,8 +196,7 @@ __device__ __forceinline__ uint32_t stage_chunk(const SysView& v, uint32_t g, ui
     return hi - lo;
 }
 
-template <bool ENERGY>
-__global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
+DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, (), ()) {
     extern __shared__ __align__(128) float4 tile[];  // union_chunk waters, 4 float4 each
     __shared__ __align__(8) uint64_t bar;
     const int tid = threadIdx.x;
@@ -182,12 +209,14 @@ __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
     const float ljc2 = v.ljc2;
     const float sig2 = OPC_O_SIGMA * OPC_O_SIGMA;
     const float qhh = OPC_Q_H * OPC_Q_H, qhm = OPC_Q_H * OPC_Q_EP, qmm = OPC_Q_EP * OPC_Q_EP;
+    const double ehh = (double)OPC_Q_H * (double)OPC_Q_H, ehm = (double)OPC_Q_H * (double)OPC_Q_EP,
+                 emm = (double)OPC_Q_EP * (double)OPC_Q_EP;
     if (tid == 0) mbar_init(&bar, 1);
     __syncthreads();
     uint32_t parity = 0;
     double el = 0.0, ec = 0.0, ew = 0.0;
     bool alive = true;
-    for (uint32_t g = blockIdx.x; g < ng && alive; g += gridDim.x) {
+    for (uint32_t g = bk.idx; g < ng && alive; g += bk.cnt) {
         const uint32_t nloc = v.grp_nloc[g];
         if (tid < 32 && nloc > 0) stage_chunk(v, g, 0, min(nloc, chunk), tile, &bar, tid);
         const uint32_t s = g * GRPW + il;
@@ -226,17 +255,16 @@ __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
                 const float4* jw = tile + 4 * (idx - lo);
                 const float3 jO = xyz(jw[0]), jH0 = xyz(jw[1]), jH1 = xyz(jw[2]), jM = xyz(jw[3]);
                 const float3 sh = shift_of(iO - jO, b);
-                const float3 jOs = jO - sh, jH0s = jH0 - sh, jH1s = jH1 - sh, jMs = jM - sh;
-                lj<ENERGY>(iO - jOs, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
-                coul<ENERGY>(iH0 - jH0s, qhh, v, fH0, a);
-                coul<ENERGY>(iH0 - jH1s, qhh, v, fH0, a);
-                coul<ENERGY>(iH0 - jMs, qhm, v, fH0, a);
-                coul<ENERGY>(iH1 - jH0s, qhh, v, fH1, a);
-                coul<ENERGY>(iH1 - jH1s, qhh, v, fH1, a);
-                coul<ENERGY>(iH1 - jMs, qhm, v, fH1, a);
-                coul<ENERGY>(iM - jH0s, qhm, v, fM, a);
-                coul<ENERGY>(iM - jH1s, qhm, v, fM, a);
-                coul<ENERGY>(iM - jMs, qmm, v, fM, a);
+                lj<ENERGY>(iO, jO, sh, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
+                coul<ENERGY>(iH0, jH0, sh, qhh, ehh, v, fH0, a);
+                coul<ENERGY>(iH0, jH1, sh, qhh, ehh, v, fH0, a);
+                coul<ENERGY>(iH0, jM, sh, qhm, ehm, v, fH0, a);
+                coul<ENERGY>(iH1, jH0, sh, qhh, ehh, v, fH1, a);
+                coul<ENERGY>(iH1, jH1, sh, qhh, ehh, v, fH1, a);
+                coul<ENERGY>(iH1, jM, sh, qhm, ehm, v, fH1, a);
+                coul<ENERGY>(iM, jH0, sh, qhm, ehm, v, fM, a);
+                coul<ENERGY>(iM, jH1, sh, qhm, ehm, v, fM, a);
+                coul<ENERGY>(iM, jM, sh, qmm, emm, v, fM, a);
             }
             __syncthreads();  // the tile is refilled by the next chunk's or group's copies
         }
@@ -259,22 +287,21 @@ __global__ void __launch_bounds__(WT, 2) k_pair_ww_tile(SysView v) {
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
     }
-    write_partials<ENERGY>(v, REG_WW, el, ec, ew);
+    write_partials<ENERGY>(v, bk, REG_WW, el, ec, ew);
 }
 
 // ---------------------------------------------------------------------------
 // water(i) - atom(j): forces on the water sites
 // ---------------------------------------------------------------------------
-template <bool ENERGY>
-__global__ void __launch_bounds__(PT) k_pair_ws(SysView v) {
+DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ws, (), ()) {
     const int lane = threadIdx.x & 31;
     const int ii = lane & 7, jq = lane >> 3;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nwc = v.sc->n_wclus;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t ci = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < nwc; ci += nwarps) {
+    for (uint32_t ci = ((bk.idx * blockDim.x + threadIdx.x) >> 5); ci < nwc; ci += nwarps) {
         const uint32_t n = v.ws_n[ci];
         if (n == 0) continue;
         const uint32_t si = ci * WCL + ii;
@@ -292,14 +319,14 @@ __global__ void __launch_bounds__(PT) k_pair_ws(SysView v) {
                 if (!vi || v.sidx[sj] == INVALID_ID) continue;
                 const float4 pj = v.spos[sj];
                 const float2 lj_j = v.slj[sj];
-                const float3 s = shift_of(iO - xyz(pj), b);
-                const float3 jp = xyz(pj) - s;
+                const float3 jp = xyz(pj);
+                const float3 s = shift_of(iO - jp, b);
                 const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
                 const float ep = sqrtf(OPC_O_EPS * lj_j.y);
-                lj<ENERGY>(iO - jp, sg * sg, ep, ljc2, 1.0f, fO, a);
-                coul<ENERGY>(iH0 - jp, OPC_Q_H * pj.w, v, fH0, a);
-                coul<ENERGY>(iH1 - jp, OPC_Q_H * pj.w, v, fH1, a);
-                coul<ENERGY>(iM - jp, OPC_Q_EP * pj.w, v, fM, a);
+                lj<ENERGY>(iO, jp, s, sg * sg, ep, ljc2, 1.0f, fO, a);
+                coul<ENERGY>(iH0, jp, s, OPC_Q_H * pj.w, (double)OPC_Q_H * (double)pj.w, v, fH0, a);
+                coul<ENERGY>(iH1, jp, s, OPC_Q_H * pj.w, (double)OPC_Q_H * (double)pj.w, v, fH1, a);
+                coul<ENERGY>(iM, jp, s, OPC_Q_EP * pj.w, (double)OPC_Q_EP * (double)pj.w, v, fM, a);
             }
         }
         fO = f3(red4(fO.x), red4(fO.y), red4(fO.z));
@@ -313,22 +340,21 @@ __global__ void __launch_bounds__(PT) k_pair_ws(SysView v) {
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
     }
-    write_partials<ENERGY>(v, REG_WS, el, ec, ew);
+    write_partials<ENERGY>(v, bk, REG_WS, el, ec, ew);
 }
 
 // ---------------------------------------------------------------------------
 // atom(i) - water(j): forces on the atoms
 // ---------------------------------------------------------------------------
-template <bool ENERGY>
-__global__ void __launch_bounds__(PT) k_pair_sw(SysView v) {
+DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_sw, (), ()) {
     const int lane = threadIdx.x & 31;
     const int ii = lane & 7, jq = lane >> 3;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nac = v.sc->n_aclus;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t ci = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < nac; ci += nwarps) {
+    for (uint32_t ci = ((bk.idx * blockDim.x + threadIdx.x) >> 5); ci < nac; ci += nwarps) {
         const uint32_t n = v.sw_n[ci];
         if (n == 0) continue;
         const uint32_t si = ci * ACL + ii;
@@ -349,10 +375,11 @@ __global__ void __launch_bounds__(PT) k_pair_sw(SysView v) {
                 if (!vi || v.wid[sj] == INVALID_ID) continue;
                 const float3 jO = xyz(v.wpos[4 * sj + 0]);
                 const float3 s = shift_of(xyz(pi) - jO, b);
-                lj<ENERGY>(xyz(pi) - (jO - s), sg * sg, ep, ljc2, 1.0f, f, a);
-                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 1]) - s), pi.w * OPC_Q_H, v, f, a);
-                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 2]) - s), pi.w * OPC_Q_H, v, f, a);
-                coul<ENERGY>(xyz(pi) - (xyz(v.wpos[4 * sj + 3]) - s), pi.w * OPC_Q_EP, v, f, a);
+                const double eh = (double)pi.w * (double)OPC_Q_H, em = (double)pi.w * (double)OPC_Q_EP;
+                lj<ENERGY>(xyz(pi), jO, s, sg * sg, ep, ljc2, 1.0f, f, a);
+                coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 1]), s, pi.w * OPC_Q_H, eh, v, f, a);
+                coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 2]), s, pi.w * OPC_Q_H, eh, v, f, a);
+                coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 3]), s, pi.w * OPC_Q_EP, em, v, f, a);
             }
         }
         f = f3(red4(f.x), red4(f.y), red4(f.z));
@@ -360,22 +387,21 @@ __global__ void __launch_bounds__(PT) k_pair_sw(SysView v) {
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
     }
-    write_partials<ENERGY>(v, REG_SW, el, ec, ew);
+    write_partials<ENERGY>(v, bk, REG_SW, el, ec, ew);
 }
 
 // ---------------------------------------------------------------------------
 // atom(i) - atom(j): interaction mask from the list build
 // ---------------------------------------------------------------------------
-template <bool ENERGY>
-__global__ void __launch_bounds__(PT) k_pair_ss(SysView v) {
+DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) {
     const int lane = threadIdx.x & 31;
     const int ii = lane & 7, jq = lane >> 3;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nac = v.sc->n_aclus;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t ci = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); ci < nac; ci += nwarps) {
+    for (uint32_t ci = ((bk.idx * blockDim.x + threadIdx.x) >> 5); ci < nac; ci += nwarps) {
         const uint32_t si = ci * ACL + ii;
         const uint32_t ai = v.sidx[si];
         const float4 pi = v.spos[si];
@@ -395,10 +421,10 @@ __global__ void __launch_bounds__(PT) k_pair_ss(SysView v) {
                 const uint32_t sj = cj * ACL + jj;
                 const float4 pj = v.spos[sj];
                 const float2 ljj = v.slj[sj];
-                const float3 d = min_image_rint(xyz(pi) - xyz(pj), b);
+                const float3 s = shift_of(xyz(pi) - xyz(pj), b);
                 const float sg = 0.5f * (lji.x + ljj.x);
-                lj<ENERGY>(d, sg * sg, sqrtf(lji.y * ljj.y), ljc2, 1.0f, f, a);
-                coul<ENERGY>(d, pi.w * pj.w, v, f, a);
+                lj<ENERGY>(xyz(pi), xyz(pj), s, sg * sg, sqrtf(lji.y * ljj.y), ljc2, 1.0f, f, a);
+                coul<ENERGY>(xyz(pi), xyz(pj), s, pi.w * pj.w, (double)pi.w * (double)pj.w, v, f, a);
             }
         }
         f = f3(red4(f.x), red4(f.y), red4(f.z));
@@ -406,34 +432,34 @@ __global__ void __launch_bounds__(PT) k_pair_ss(SysView v) {
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
     }
-    write_partials<ENERGY>(v, REG_SS, el, ec, ew);
+    write_partials<ENERGY>(v, bk, REG_SS, el, ec, ew);
 }
 
 // ---------------------------------------------------------------------------
 // 1-4 pairs: LJ x0.5, Coulomb x1/1.2 (src/non_bonded.rs:55-56,1014-1042)
 // ---------------------------------------------------------------------------
-template <bool ENERGY>
-__global__ void k_pair14(SysView v) {
+DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_pair14, (), ()) {
     const BoxDev b = *v.box;
     double e_acc = 0.0, w_acc = 0.0;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < v.n14; k += gridDim.x * blockDim.x) {
+    for (uint32_t k = bk.idx * blockDim.x + threadIdx.x; k < v.n14; k += bk.cnt * blockDim.x) {
         const uint2 p = v.p14[k];
         const float4 par = v.p14_par[k];  // sigma, eps, qq
-        const float3 d = min_image_rint(xyz(v.apos[p.x]) - xyz(v.apos[p.y]), b);
+        const float4 pa = v.apos[p.x], pb = v.apos[p.y];
+        const float3 sh = shift_of(xyz(pa) - xyz(pb), b);
         float3 f = f3(0, 0, 0);
         Acc3 a{0.0, 0.0, 0.f};
-        lj<ENERGY>(d, par.x * par.x, par.y, v.ljc2, 0.5f, f, a);
+        lj<ENERGY>(xyz(pa), xyz(pb), sh, par.x * par.x, par.y, v.ljc2, 0.5f, f, a);
         float3 fc = f3(0, 0, 0);
         Acc3 ac{0.0, 0.0, 0.f};
-        coul<ENERGY>(d, par.z, v, fc, ac);
+        coul<ENERGY>(xyz(pa), xyz(pb), sh, par.z, (double)pa.w * (double)pb.w, v, fc, ac);
         const float s = 0.833333333f;
         f = f + fc * s;
         add_fix3(v.aforce + 3 * (size_t)p.x, f);
         add_fix3(v.aforce + 3 * (size_t)p.y, f3(-f.x, -f.y, -f.z));
-        if (ENERGY) e_acc += (double)a.e_lj + (double)ac.e_c * s;
+        if (ENERGY) e_acc += a.e_lj + ac.e_c / 1.2;
         w_acc += (double)a.w + (double)ac.w * s;
     }
-    write_partials<ENERGY>(v, REG_14, e_acc, 0.0, w_acc);
+    write_partials<ENERGY>(v, bk, REG_14, e_acc, 0.0, w_acc);
 }
 
 inline int pblocks(const SysView& v, uint64_t warps) {
@@ -461,14 +487,15 @@ int pair_ww_setup(const SysView& v) {
     int dev = 0, optin = 0;
     DYN_CUDA(cudaGetDevice(&dev));
     DYN_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    cudaFuncAttributes fe, fn;
-    DYN_CUDA(cudaFuncGetAttributes(&fe, k_pair_ww_tile<true>));
-    DYN_CUDA(cudaFuncGetAttributes(&fn, k_pair_ww_tile<false>));
-    const int le = optin - (int)fe.sharedSizeBytes, ln = optin - (int)fn.sharedSizeBytes;
-    DYN_CHECK(ww_tile_smem(v) <= (size_t)std::min(le, ln), DYN_ERR_UNSUPPORTED,
-              "water-water chunk exceeds shared memory");
-    DYN_CUDA(cudaFuncSetAttribute(k_pair_ww_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, le));
-    DYN_CUDA(cudaFuncSetAttribute(k_pair_ww_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ln));
+    const void* ks[4] = {(const void*)k_pair_ww_tile<true>, (const void*)k_pair_ww_tile<false>,
+                         (const void*)k_pair_ww_tile_batch<true>, (const void*)k_pair_ww_tile_batch<false>};
+    for (const void* k : ks) {
+        cudaFuncAttributes fa;
+        DYN_CUDA(cudaFuncGetAttributes(&fa, k));
+        const int lim = optin - (int)fa.sharedSizeBytes;
+        DYN_CHECK(ww_tile_smem(v) <= (size_t)lim, DYN_ERR_UNSUPPORTED, "water-water chunk exceeds shared memory");
+        DYN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    }
     return DYN_OK;
 }
 int pair_blocks_ss(const SysView& v) { return pblocks(v, v.naclus_cap); }
@@ -478,37 +505,34 @@ int pair14_blocks(const SysView& v) {
     return (int)(bl < v.max_blocks ? bl : v.max_blocks);
 }
 
-void launch_pairs(const SysView& v, cudaStream_t st, bool energy) {
-    const int bw = pblocks(v, v.nwclus_cap), ba = pblocks(v, v.naclus_cap);
-    const int bt = ww_tile_blocks(v);
-    const size_t sm = ww_tile_smem(v);
+void launch_pairs(const Target& t, bool energy) {
+    const size_t sm = t.max_over([](const SysView& v) { return v.nw ? ww_tile_smem(v) : (size_t)0; });
     // water-water short-range energy is part of the potential only with
     // DYN_FLAG_FULL_ENERGY (the reference leaves it out,
     // src/non_bonded.rs:335-342), so other energy steps skip it
-    const bool eww = energy && (v.flags & DYN_FLAG_FULL_ENERGY);
-    if (v.nw) {
-        if (eww) k_pair_ww_tile<true><<<bt, WT, sm, st>>>(v);
-        else k_pair_ww_tile<false><<<bt, WT, sm, st>>>(v);
-    }
+    auto eww = [energy](const SysView& v) { return energy && (v.flags & DYN_FLAG_FULL_ENERGY); };
+    t.launch(k_pair_ww_tile<true>, k_pair_ww_tile_batch<true>,
+             [&](const SysView& v) { return v.nw && eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
+    t.launch(k_pair_ww_tile<false>, k_pair_ww_tile_batch<false>,
+             [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
+    auto ss = [](const SysView& v) { return v.na ? pblocks(v, v.naclus_cap) : 0; };
+    auto ws = [](const SysView& v) { return v.nw && v.na ? pblocks(v, v.nwclus_cap) : 0; };
+    auto sw = [](const SysView& v) { return v.nw && v.na ? pblocks(v, v.naclus_cap) : 0; };
     if (energy) {
-        if (v.na) k_pair_ss<true><<<ba, PT, 0, st>>>(v);
-        if (v.nw && v.na) {
-            k_pair_ws<true><<<bw, PT, 0, st>>>(v);
-            k_pair_sw<true><<<ba, PT, 0, st>>>(v);
-        }
+        t.launch(k_pair_ss<true>, k_pair_ss_batch<true>, ss, PT, 0);
+        t.launch(k_pair_ws<true>, k_pair_ws_batch<true>, ws, PT, 0);
+        t.launch(k_pair_sw<true>, k_pair_sw_batch<true>, sw, PT, 0);
     } else {
-        if (v.na) k_pair_ss<false><<<ba, PT, 0, st>>>(v);
-        if (v.nw && v.na) {
-            k_pair_ws<false><<<bw, PT, 0, st>>>(v);
-            k_pair_sw<false><<<ba, PT, 0, st>>>(v);
-        }
+        t.launch(k_pair_ss<false>, k_pair_ss_batch<false>, ss, PT, 0);
+        t.launch(k_pair_ws<false>, k_pair_ws_batch<false>, ws, PT, 0);
+        t.launch(k_pair_sw<false>, k_pair_sw_batch<false>, sw, PT, 0);
     }
 }
 
-void launch_pair14(const SysView& v, cudaStream_t st, bool energy) {
-    if (!v.n14) return;
-    if (energy) k_pair14<true><<<pair14_blocks(v), 256, 0, st>>>(v);
-    else k_pair14<false><<<pair14_blocks(v), 256, 0, st>>>(v);
+void launch_pair14(const Target& t, bool energy) {
+    auto g = [](const SysView& v) { return v.n14 ? pair14_blocks(v) : 0; };
+    if (energy) t.launch(k_pair14<true>, k_pair14_batch<true>, g, 256, 0);
+    else t.launch(k_pair14<false>, k_pair14_batch<false>, g, 256, 0);
 }
 
 }  // namespace dyn

@@ -33,17 +33,20 @@ __device__ __forceinline__ void bspline4(float w, float* th, float* dth) {
     }
 }
 
-// grid coordinate of a position: u = K * frac((x - lo) / L)
+// grid coordinate of a position: u = K * frac((x - lo) / L), in float64 (a
+// float32 u near K = 96 is only good to ~4e-6 grid units, which would put
+// relative errors of 1e-6 into the B-spline weights); base[a] = floor(u),
+// w[a] = u - floor(u)
 __device__ __forceinline__ void grid_coord(float3 p, const BoxDev& b, const uint32_t* K, int* base,
-                                           float* w) {
+                                           double* w) {
     const float c[3] = {p.x, p.y, p.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        float f = (c[a] - b.lo[a]) * b.inv_ext[a];
-        f -= floorf(f);
-        float u = f * (float)K[a];
-        int i = (int)floorf(u);
-        float ww = u - (float)i;
+        double f = ((double)c[a] - (double)b.lo[a]) / (double)b.ext[a];
+        f -= floor(f);
+        const double u = f * (double)K[a];
+        int i = (int)floor(u);
+        const double ww = u - (double)i;
         if (i >= (int)K[a]) { i -= K[a]; }
         if (i < 0) { i += K[a]; }
         base[a] = i;
@@ -51,14 +54,24 @@ __device__ __forceinline__ void grid_coord(float3 p, const BoxDev& b, const uint
     }
 }
 
+__device__ __forceinline__ void bspline4d(double w, double* th) {
+    const double w2 = w * w, w3 = w2 * w, om = 1.0 - w;
+    th[0] = om * om * om * (1.0 / 6.0);
+    th[1] = (3.0 * w3 - 6.0 * w2 + 4.0) * (1.0 / 6.0);
+    th[2] = (-3.0 * w3 + 3.0 * w2 + 3.0 * w + 1.0) * (1.0 / 6.0);
+    th[3] = w3 * (1.0 / 6.0);
+}
+
+// Charge spreading with float64 weights and products, accumulated as 64-bit
+// fixed point (exact, order-independent sums).
 __device__ __forceinline__ void spread_one(const SysView& v, float3 p, float q, const BoxDev& b) {
     int base[3];
-    float w[3];
+    double w[3];
     grid_coord(p, b, v.K, base, w);
-    float tx[4], ty[4], tz[4];
-    bspline4(w[0], tx, nullptr);
-    bspline4(w[1], ty, nullptr);
-    bspline4(w[2], tz, nullptr);
+    double tx[4], ty[4], tz[4];
+    bspline4d(w[0], tx);
+    bspline4d(w[1], ty);
+    bspline4d(w[2], tz);
     const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
     int iz[4];
 #pragma unroll
@@ -66,23 +79,23 @@ __device__ __forceinline__ void spread_one(const SysView& v, float3 p, float q, 
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         int x = base[0] - 3 + a; x = x < 0 ? x + K0 : x;
-        const float qa = q * tx[a];
+        const double qa = (double)q * tx[a];
 #pragma unroll
         for (int bb = 0; bb < 4; ++bb) {
             int y = base[1] - 3 + bb; y = y < 0 ? y + K1 : y;
-            const float qab = qa * ty[bb];
+            const double qab = qa * ty[bb];
             long long* row = v.qgrid_fix + ((size_t)x * K1 + y) * K2;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) fix_atomic_add(row + iz[c], fix_from_float(qab * tz[c]));
+            for (int c = 0; c < 4; ++c) fix_atomic_add(row + iz[c], fix_from_double(qab * tz[c]));
         }
     }
 }
 
 // one thread per charged site: atoms (q != 0), then water H0, H1, M
-__global__ void k_spread(SysView v) {
+DYN_KERNEL(, k_spread, (), ()) {
     const BoxDev b = *v.box;
     const uint32_t total = v.na + 3 * v.nw_cap;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
         if (t < v.na) {
             const float4 p = v.apos[t];
             if (p.w != 0.f) spread_one(v, xyz(p), p.w, b);
@@ -96,8 +109,9 @@ __global__ void k_spread(SysView v) {
     }
 }
 
-__global__ void k_fix2real(SysView v, uint32_t n) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+DYN_KERNEL(, k_fix2real, (), ()) {
+    const uint32_t n = v.K[0] * v.K[1] * v.K[2];
+    for (uint32_t i = bk.idx * blockDim.x + threadIdx.x; i < n; i += bk.cnt * blockDim.x) {
         v.qgrid[i] = (float)((double)v.qgrid_fix[i] * DYN_FIX_INV);
         v.qgrid_fix[i] = 0;
     }
@@ -105,7 +119,7 @@ __global__ void k_fix2real(SysView v, uint32_t n) {
 
 // Influence function B(m) C(m) applied in place; energy and virial of the
 // reciprocal sum (Essmann eq. 2.10 and the trace of the k-space virial).
-__global__ void k_convolve(SysView v) {
+DYN_KERNEL(, k_convolve, (), ()) {
     const BoxDev b = *v.box;
     const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
     const int K2h = K2 / 2 + 1;
@@ -114,7 +128,7 @@ __global__ void k_convolve(SysView v) {
     const float pa2 = (float)(M_PI * M_PI) / (v.alpha * v.alpha);
     const float pref = inv_vol * (float)(1.0 / M_PI);
     double e = 0.0, w = 0.0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = bk.idx * blockDim.x + threadIdx.x; i < n; i += bk.cnt * blockDim.x) {
         const int kz = i % K2h;
         const int ky = (i / K2h) % K1;
         const int kx = i / (K2h * K1);
@@ -137,19 +151,19 @@ __global__ void k_convolve(SysView v) {
     double x[2] = {e, w};
     block_sum_d<2>(x);
     if (threadIdx.x == 0) {
-        double* p = v.partials + ((size_t)REG_PME * v.max_blocks + blockIdx.x) * 4;
+        double* p = v.partials + ((size_t)REG_PME * v.max_blocks + bk.idx) * 4;
         p[0] = x[0]; p[1] = x[1]; p[2] = 0.0; p[3] = 0.0;
     }
 }
 
 __device__ __forceinline__ float3 gather_one(const SysView& v, float3 p, float q, const BoxDev& b) {
     int base[3];
-    float w[3];
-    grid_coord(p, b, v.K, base, w);
+    double wd[3];
+    grid_coord(p, b, v.K, base, wd);
     float tx[4], ty[4], tz[4], dx[4], dy[4], dz[4];
-    bspline4(w[0], tx, dx);
-    bspline4(w[1], ty, dy);
-    bspline4(w[2], tz, dz);
+    bspline4((float)wd[0], tx, dx);
+    bspline4((float)wd[1], ty, dy);
+    bspline4((float)wd[2], tz, dz);
     const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
     int iz[4];
 #pragma unroll
@@ -177,9 +191,10 @@ __device__ __forceinline__ float3 gather_one(const SysView& v, float3 p, float q
     return f3(-q * K0 * b.inv_ext[0] * gx, -q * K1 * b.inv_ext[1] * gy, -q * K2 * b.inv_ext[2] * gz);
 }
 
-// -q q erf(alpha r)/r between two sites, float64; returns force on the first
-__device__ __forceinline__ double excl_corr(float3 d, double qq, double alpha, double3* f) {
-    const double dx = d.x, dy = d.y, dz = d.z;
+// -q q erf(alpha r)/r between two sites, float64 from the exact float64
+// displacement (dx, dy, dz); returns the energy and the force on the first
+__device__ __forceinline__ double excl_corr(double dx, double dy, double dz, double qq, double alpha,
+                                           double3* f) {
     const double r2 = dx * dx + dy * dy + dz * dz;
     const double r = sqrt(r2);
     const double ar = alpha * r;
@@ -193,12 +208,12 @@ __device__ __forceinline__ double excl_corr(float3 d, double qq, double alpha, d
 // Gather: one thread per atom, or per water (its H0, H1, M), writing the
 // reciprocal cache.  With Ewald corrections on, the intra-water exclusion
 // corrections (H0-H1, H0-M, H1-M) are added here in float64.
-__global__ void k_gather(SysView v) {
+DYN_KERNEL(, k_gather, (), ()) {
     const BoxDev b = *v.box;
     const bool corr = v.flags & DYN_FLAG_EWALD_CORRECTIONS;
     double e_c = 0.0, w_c = 0.0;
     const uint32_t total = v.na + v.nw_cap;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
         if (t < v.na) {
             const float4 p = v.apos[t];
             float3 f = f3(0.f, 0.f, 0.f);
@@ -222,9 +237,11 @@ __global__ void k_gather(SysView v) {
                 const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
                 for (int k = 0; k < 3; ++k) {
                     double3 f;
-                    const float3 d = ps[pa[k]] - ps[pb[k]];
-                    e_c += excl_corr(d, q[pa[k]] * q[pb[k]], (double)v.alpha, &f);
-                    w_c += f.x * d.x + f.y * d.y + f.z * d.z;
+                    const double dx = (double)ps[pa[k]].x - (double)ps[pb[k]].x;
+                    const double dy = (double)ps[pa[k]].y - (double)ps[pb[k]].y;
+                    const double dz = (double)ps[pa[k]].z - (double)ps[pb[k]].z;
+                    e_c += excl_corr(dx, dy, dz, q[pa[k]] * q[pb[k]], (double)v.alpha, &f);
+                    w_c += f.x * dx + f.y * dy + f.z * dz;
                     fs[pa[k]].x += f.x; fs[pa[k]].y += f.y; fs[pa[k]].z += f.z;
                     fs[pb[k]].x -= f.x; fs[pb[k]].y -= f.y; fs[pb[k]].z -= f.z;
                 }
@@ -240,7 +257,7 @@ __global__ void k_gather(SysView v) {
     double x[2] = {e_c, w_c};
     block_sum_d<2>(x);
     if (threadIdx.x == 0) {
-        double* p = v.partials + ((size_t)REG_CORR * v.max_blocks + blockIdx.x) * 4;
+        double* p = v.partials + ((size_t)REG_CORR * v.max_blocks + bk.idx) * 4;
         p[0] = x[0]; p[1] = x[1]; p[2] = 0.0; p[3] = 0.0;
     }
 }
@@ -250,12 +267,12 @@ __global__ void k_gather(SysView v) {
 // only, its virial kept with the reciprocal virial.  Corrected mode: float64
 // exclusion corrections for 1-2/1-3 pairs (full) and 1-4 pairs (1 - 1/1.2),
 // into the reciprocal cache.
-__global__ void k_corr_atoms(SysView v) {
+DYN_KERNEL(, k_corr_atoms, (), ()) {
     const BoxDev b = *v.box;
     const bool corr = v.flags & DYN_FLAG_EWALD_CORRECTIONS;
     double e_c = 0.0, w_c = 0.0;
     const uint32_t total = v.n14 + (corr ? v.nexcl : 0u);
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    for (uint32_t k = bk.idx * blockDim.x + threadIdx.x; k < total; k += bk.cnt * blockDim.x) {
         uint2 p;
         double qq;
         double scale = 1.0;
@@ -278,8 +295,19 @@ __global__ void k_corr_atoms(SysView v) {
             w_c += (double)dot3(dir * r, df);
         } else {
             double3 f;
-            e_c += excl_corr(d, qq * scale, (double)v.alpha, &f);
-            w_c += f.x * d.x + f.y * d.y + f.z * d.z;
+            // exact float64 displacement: positions are float32 and the
+            // periodic shift is a whole number of box extents
+            const float3 pa = xyz(v.apos[p.x]), pb = xyz(v.apos[p.y]);
+            const float3 dr = pa - pb;
+            const double sx = -(double)rintf(dr.x * b.inv_ext[0]) * (double)b.ext[0];
+            const double sy = -(double)rintf(dr.y * b.inv_ext[1]) * (double)b.ext[1];
+            const double sz = -(double)rintf(dr.z * b.inv_ext[2]) * (double)b.ext[2];
+            const double dx = (double)pa.x - (double)pb.x + sx;
+            const double dy = (double)pa.y - (double)pb.y + sy;
+            const double dz = (double)pa.z - (double)pb.z + sz;
+            const double qqe = (double)v.apos[p.x].w * (double)v.apos[p.y].w;
+            e_c += excl_corr(dx, dy, dz, qqe * scale, (double)v.alpha, &f);
+            w_c += f.x * dx + f.y * dy + f.z * dz;
             long long* fa = v.arecip + 3 * (size_t)p.x;
             long long* fb = v.arecip + 3 * (size_t)p.y;
             fix_atomic_add(fa + 0, fix_from_double(f.x)); fix_atomic_add(fa + 1, fix_from_double(f.y));
@@ -291,13 +319,13 @@ __global__ void k_corr_atoms(SysView v) {
     double x[2] = {e_c, w_c};
     block_sum_d<2>(x);
     if (threadIdx.x == 0) {
-        double* pp = v.partials + ((size_t)REG_CORR_A * v.max_blocks + blockIdx.x) * 4;
+        double* pp = v.partials + ((size_t)REG_CORR_A * v.max_blocks + bk.idx) * 4;
         pp[0] = x[0]; pp[1] = x[1]; pp[2] = 0.0; pp[3] = 0.0;
     }
 }
 
 // Sums the reciprocal-step partials (fixed order) into the cache.
-__global__ void k_recip_finalize(SysView v) {
+DYN_KERNEL(, k_recip_finalize, (), ()) {
     double x[4] = {0.0, 0.0, 0.0, 0.0};
     for (uint32_t i = threadIdx.x; i < v.nb[REG_PME]; i += blockDim.x) {
         const double* p = v.partials + ((size_t)REG_PME * v.max_blocks + i) * 4;
@@ -376,19 +404,20 @@ void pme_free(SysView& v, cufftHandle plan_f, cufftHandle plan_b) {
     for (int a = 0; a < 3; ++a) cudaFree(v.bmod[a]);
 }
 
-void launch_pme(const SysView& v, cudaStream_t st, cufftHandle plan_f, cufftHandle plan_b) {
-    const uint32_t n = v.K[0] * v.K[1] * v.K[2];
-    k_spread<<<gblocks(v, (uint64_t)v.na + 3ull * v.nw_cap), GT, 0, st>>>(v);
-    k_fix2real<<<gblocks(v, n), GT, 0, st>>>(v, n);
-    cufftExecR2C(plan_f, v.qgrid, (cufftComplex*)v.cgrid);
-    k_convolve<<<v.nb[REG_PME], GT, 0, st>>>(v);
-    cufftExecC2R(plan_b, (cufftComplex*)v.cgrid, v.qgrid);
-    k_gather<<<v.nb[REG_CORR], GT, 0, st>>>(v);
+void launch_pme(const Target& t) {
+    t.launch(k_spread, k_spread_batch, [](const SysView& v) { return gblocks(v, (uint64_t)v.na + 3ull * v.nw_cap); },
+             GT, 0);
+    t.launch(k_fix2real, k_fix2real_batch,
+             [](const SysView& v) { return gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]); }, GT, 0);
+    t.each([](const SysView& v) { cufftExecR2C(v.plan_f, v.qgrid, (cufftComplex*)v.cgrid); });
+    t.launch(k_convolve, k_convolve_batch, [](const SysView& v) { return (int)v.nb[REG_PME]; }, GT, 0);
+    t.each([](const SysView& v) { cufftExecC2R(v.plan_b, (cufftComplex*)v.cgrid, v.qgrid); });
+    t.launch(k_gather, k_gather_batch, [](const SysView& v) { return (int)v.nb[REG_CORR]; }, GT, 0);
 }
 
-void launch_corrections(const SysView& v, cudaStream_t st) {
-    k_corr_atoms<<<v.nb[REG_CORR_A], GT, 0, st>>>(v);
-    k_recip_finalize<<<1, 256, 0, st>>>(v);
+void launch_corrections(const Target& t) {
+    t.launch(k_corr_atoms, k_corr_atoms_batch, [](const SysView& v) { return (int)v.nb[REG_CORR_A]; }, GT, 0);
+    t.launch(k_recip_finalize, k_recip_finalize_batch, [](const SysView&) { return 1; }, 256, 0);
 }
 
 }  // namespace dyn

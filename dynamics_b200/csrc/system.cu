@@ -8,21 +8,12 @@
 #include <cstring>
 #include <vector>
 
-#include "engine.cuh"
+#include "sys_internal.cuh"
 
-struct dyn_sys_s {
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;       // created here because the caller passed NULL
-    cudaStream_t aux = nullptr;    // captures the bodies of conditional graph nodes
-    SysView v{};
-    dyn_config_t cfg{};
-    cufftHandle plan_f = 0, plan_b = 0;
-    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
-    float graph_dt[4] = {0, 0, 0, 0};
-    uint64_t host_step = 0;        // steps enqueued so far
-    std::vector<void*> allocs;     // every device allocation, freed on destroy
-    Scalars* h_sc = nullptr;       // pinned mirror of the scalars
-};
+using dyn::begin_if_body;
+using dyn::count_graph_kernels;
+using dyn::end_if_body;
+using dyn::read_scalars;
 
 namespace {
 
@@ -107,6 +98,8 @@ void set_block_counts(SysView& v) {
 // Inside an active capture on st: appends an IF node on hc after everything
 // captured so far (later work depends on it) and starts capturing its body
 // on aux.
+}  // namespace
+namespace dyn {
 int begin_if_body(cudaStream_t st, cudaStream_t aux, cudaGraphConditionalHandle hc, cudaGraph_t* body) {
     cudaStreamCaptureStatus cs;
     cudaGraph_t cg = nullptr;
@@ -124,12 +117,18 @@ int begin_if_body(cudaStream_t st, cudaStream_t aux, cudaGraphConditionalHandle 
     DYN_CUDA(cudaStreamBeginCaptureToGraph(aux, *body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     return DYN_OK;
 }
+}  // namespace dyn
+namespace {
 
+}  // namespace
+namespace dyn {
 int end_if_body(cudaStream_t aux) {
     cudaGraph_t g = nullptr;
     DYN_CUDA(cudaStreamEndCapture(aux, &g));
     return DYN_OK;
 }
+}  // namespace dyn
+namespace {
 
 // Captures one step (MdState::step, src/integrate.rs:100-473) into a graph.
 // The list rebuild and the periodic tasks (COM removal, recentering,
@@ -141,6 +140,8 @@ int capture_step(dyn_sys_s* h, float dt, bool spme, bool energy, cudaGraph_t* ou
                  cudaGraph_t* body_rebuild = nullptr, cudaGraph_t* body_periodic = nullptr) {
     SysView& v = h->v;
     cudaStream_t st = h->stream;
+    const Target T{&v, nullptr, st};
+    const Target TA{&v, nullptr, h->aux};
     *out = nullptr;
     DYN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = DYN_OK;
@@ -155,23 +156,23 @@ int capture_step(dyn_sys_s* h, float dt, bool spme, bool energy, cudaGraph_t* ou
             e = cudaGraphConditionalHandleCreate(&v.cond_periodic, cg, 0, cudaGraphCondAssignDefault);
         if (e != cudaSuccess) { rc = dyn::cuda_fail(e, "cudaGraphConditionalHandleCreate"); break; }
         v.use_cond = 1;
-        dyn::launch_first_half(v, st, dt);
-        dyn::launch_displacement_check(v, st);
+        dyn::launch_first_half(T, dt);
+        dyn::launch_displacement_check(T);
         if ((rc = begin_if_body(st, h->aux, v.cond_rebuild, &br)) != DYN_OK) break;
-        dyn::launch_rebuild(v, h->aux, false);
+        dyn::launch_rebuild(TA, false);
         if ((rc = end_if_body(h->aux)) != DYN_OK) break;
-        dyn::launch_gather_atoms(v, st);
-        dyn::launch_pairs(v, st, energy);
-        dyn::launch_pair14(v, st, energy);
-        dyn::launch_bonded(v, st, energy);
+        dyn::launch_gather_atoms(T);
+        dyn::launch_pairs(T, energy);
+        dyn::launch_pair14(T, energy);
+        dyn::launch_bonded(T, energy);
         if (spme) {
-            dyn::launch_pme(v, st, h->plan_f, h->plan_b);
-            dyn::launch_corrections(v, st);
+            dyn::launch_pme(T);
+            dyn::launch_corrections(T);
         }
-        dyn::launch_second_half(v, st, dt);
-        dyn::launch_finalize(v, st, dt, energy, true);
+        dyn::launch_second_half(T, dt);
+        dyn::launch_finalize(T, dt, energy, true);
         if ((rc = begin_if_body(st, h->aux, v.cond_periodic, &bp)) != DYN_OK) break;
-        dyn::launch_periodic(v, h->aux);
+        dyn::launch_periodic(TA);
         if ((rc = end_if_body(h->aux)) != DYN_OK) break;
     } while (0);
     v.use_cond = 0;
@@ -197,18 +198,21 @@ int capture_step(dyn_sys_s* h, float dt, bool spme, bool energy, cudaGraph_t* ou
 void enqueue_forces(dyn_sys_s* h, bool force_rebuild) {
     const SysView& v = h->v;
     cudaStream_t st = h->stream;
-    if (!force_rebuild) dyn::launch_displacement_check(v, st);
-    dyn::launch_rebuild(v, st, force_rebuild);
-    dyn::launch_gather_atoms(v, st);
-    dyn::launch_pairs(v, st, true);
-    dyn::launch_pair14(v, st, true);
-    dyn::launch_bonded(v, st, true);
-    dyn::launch_pme(v, st, h->plan_f, h->plan_b);
-    dyn::launch_corrections(v, st);
-    dyn::launch_second_half(v, st, 0.0f);
-    dyn::launch_finalize(v, st, 0.0f, true, false);
+    const Target T{&v, nullptr, st};
+    if (!force_rebuild) dyn::launch_displacement_check(T);
+    dyn::launch_rebuild(T, force_rebuild);
+    dyn::launch_gather_atoms(T);
+    dyn::launch_pairs(T, true);
+    dyn::launch_pair14(T, true);
+    dyn::launch_bonded(T, true);
+    dyn::launch_pme(T);
+    dyn::launch_corrections(T);
+    dyn::launch_second_half(T, 0.0f);
+    dyn::launch_finalize(T, 0.0f, true, false);
 }
 
+}  // namespace
+namespace dyn {
 int read_scalars(dyn_sys_s* h) {
     DYN_CUDA(cudaMemcpyAsync(h->h_sc, h->v.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
     DYN_CUDA(cudaStreamSynchronize(h->stream));
@@ -219,6 +223,8 @@ int read_scalars(dyn_sys_s* h) {
     if (h->h_sc->timeout) return dyn::fail(DYN_ERR_TIMEOUT, "a bounded device wait gave up");
     return DYN_OK;
 }
+}  // namespace dyn
+namespace {
 
 void fill_energies(dyn_sys_s* h, dyn_energies_t* e) {
     const Scalars& s = *h->h_sc;
@@ -398,7 +404,7 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(fit, (v.cap_union + 31) / 32 * 32));
         if (cfg->ww_union_chunk)
             v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(v.union_chunk, cfg->ww_union_chunk / 32 * 32));
-        v.cap_run = 256;
+        v.cap_run = v.cap_union;  // a run per union water at worst
         const double nb = 4.0 / 3.0 * M_PI * r * r * r * dl;
         v.cap_nb = std::min<uint32_t>((uint32_t)(1.5 * nb) + 32, 65535u);
     }
@@ -636,6 +642,8 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     }
     TRY(upload(h, v.box, &bx, 1));
     TRY(dyn::pme_init(v, &h->plan_f, &h->plan_b, h->stream));
+    v.plan_f = (int)h->plan_f;
+    v.plan_b = (int)h->plan_b;
     h->allocs.push_back(v.qgrid_fix); h->allocs.push_back(v.qgrid); h->allocs.push_back(v.cgrid);
     for (int a = 0; a < 3; ++a) h->allocs.push_back(v.bmod[a]);
     set_block_counts(v);
@@ -895,6 +903,8 @@ HostStage& stage_of(dyn_sys_s* h) {
     return tbl.back().second;
 }
 
+}  // namespace
+namespace dyn {
 int count_graph_kernels(cudaGraph_t g, uint32_t* n) {
     size_t cnt = 0;
     DYN_CUDA(cudaGraphGetNodes(g, nullptr, &cnt));
@@ -909,6 +919,8 @@ int count_graph_kernels(cudaGraph_t g, uint32_t* n) {
     *n = k;
     return DYN_OK;
 }
+}  // namespace dyn
+namespace {
 
 }  // namespace
 
@@ -967,6 +979,7 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
     DYN_CHECK(dt > 0.f, DYN_ERR_INVALID, "dyn_sys_stage_times: dt must be > 0");
     const SysView& v = h->v;
     cudaStream_t st = h->stream;
+    const Target T{&v, nullptr, st};
     cudaEvent_t ev[7];
     for (int i = 0; i < 7; ++i) DYN_CUDA(cudaEventCreate(&ev[i]));
     double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -977,25 +990,25 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
         const bool spme = (s % v.spme_interval) == 0;
         const bool energy = ((s + 1) % e_int) == 0;
         cudaEventRecord(ev[0], st);
-        dyn::launch_first_half(v, st, dt);
+        dyn::launch_first_half(T, dt);
         cudaEventRecord(ev[1], st);
-        dyn::launch_displacement_check(v, st);
-        dyn::launch_rebuild(v, st, false);
+        dyn::launch_displacement_check(T);
+        dyn::launch_rebuild(T, false);
         cudaEventRecord(ev[2], st);
-        dyn::launch_gather_atoms(v, st);
-        dyn::launch_pairs(v, st, energy);
+        dyn::launch_gather_atoms(T);
+        dyn::launch_pairs(T, energy);
         cudaEventRecord(ev[3], st);
-        dyn::launch_pair14(v, st, energy);
-        dyn::launch_bonded(v, st, energy);
+        dyn::launch_pair14(T, energy);
+        dyn::launch_bonded(T, energy);
         cudaEventRecord(ev[4], st);
         if (spme) {
-            dyn::launch_pme(v, st, h->plan_f, h->plan_b);
-            dyn::launch_corrections(v, st);
+            dyn::launch_pme(T);
+            dyn::launch_corrections(T);
         }
         cudaEventRecord(ev[5], st);
-        dyn::launch_second_half(v, st, dt);
-        dyn::launch_finalize(v, st, dt, energy, true);
-        dyn::launch_periodic(v, st);
+        dyn::launch_second_half(T, dt);
+        dyn::launch_finalize(T, dt, energy, true);
+        dyn::launch_periodic(T);
         cudaEventRecord(ev[6], st);
         DYN_CUDA(cudaGetLastError());
         DYN_CUDA(cudaEventSynchronize(ev[6]));
@@ -1020,6 +1033,7 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
 int count_step_kernels(dyn_sys_s* h, bool spme, uint32_t* fixed, uint32_t* rebuild, uint32_t* periodic) {
     const SysView& v = h->v;
     cudaStream_t st = h->stream;
+    const Target T{&v, nullptr, st};
     DYN_CUDA(cudaStreamSynchronize(st));
     auto count = [&](auto&& enqueue, uint32_t* n) -> int {
         cudaGraph_t g = nullptr;
@@ -1035,18 +1049,18 @@ int count_step_kernels(dyn_sys_s* h, bool spme, uint32_t* fixed, uint32_t* rebui
     if (fixed) {
         uint32_t total = 0, fft = 0;
         rc = count([&] {
-            dyn::launch_first_half(v, st, 0.002f);
-            dyn::launch_displacement_check(v, st);
-            dyn::launch_gather_atoms(v, st);
-            dyn::launch_pairs(v, st, true);
-            dyn::launch_pair14(v, st, true);
-            dyn::launch_bonded(v, st, true);
+            dyn::launch_first_half(T, 0.002f);
+            dyn::launch_displacement_check(T);
+            dyn::launch_gather_atoms(T);
+            dyn::launch_pairs(T, true);
+            dyn::launch_pair14(T, true);
+            dyn::launch_bonded(T, true);
             if (spme) {
-                dyn::launch_pme(v, st, h->plan_f, h->plan_b);
-                dyn::launch_corrections(v, st);
+                dyn::launch_pme(T);
+                dyn::launch_corrections(T);
             }
-            dyn::launch_second_half(v, st, 0.002f);
-            dyn::launch_finalize(v, st, 0.002f, true, true);
+            dyn::launch_second_half(T, 0.002f);
+            dyn::launch_finalize(T, 0.002f, true, true);
         }, &total);
         if (rc) return rc;
         if (spme) {
@@ -1058,8 +1072,8 @@ int count_step_kernels(dyn_sys_s* h, bool spme, uint32_t* fixed, uint32_t* rebui
         }
         *fixed = total - fft;
     }
-    if (rebuild && (rc = count([&] { dyn::launch_rebuild(v, st, false); }, rebuild))) return rc;
-    if (periodic && (rc = count([&] { dyn::launch_periodic(v, st); }, periodic))) return rc;
+    if (rebuild && (rc = count([&] { dyn::launch_rebuild(T, false); }, rebuild))) return rc;
+    if (periodic && (rc = count([&] { dyn::launch_periodic(T); }, periodic))) return rc;
     return DYN_OK;
 }
 

@@ -135,72 +135,91 @@ def _config_struct(system, cfg):
     return c
 
 
+def _system_desc(system):
+    """dyn_system_desc_t for a system dict; returns (desc, arrays kept alive,
+    n_water, n_atoms)."""
+    wp = f32(system.get("water_pos", np.zeros((0, 3, 3)))).reshape(-1, 9)
+    wv = f32(system.get("water_vel", np.zeros_like(wp))).reshape(-1, 9)
+    ap = f32(system.get("atom_pos", np.zeros((0, 3)))).reshape(-1, 3)
+    na = len(ap)
+    nw = len(wp)
+    keep = {}
+
+    def arr(name, conv, shape=None):
+        if name not in system or system[name] is None or len(system[name]) == 0:
+            return None
+        a = conv(system[name])
+        if shape is not None:
+            a = a.reshape(shape)
+        keep[name] = a
+        return a
+
+    d = _lib.SystemDesc()
+    d.n_atoms = na
+    d.atom_pos = ptr(arr("atom_pos", f32, -1))
+    d.atom_vel = ptr(arr("atom_vel", f32, -1))
+    d.atom_mass = ptr(arr("atom_mass", f32))
+    d.atom_q = ptr(arr("atom_q", f32))
+    d.atom_sigma = ptr(arr("atom_sigma", f32))
+    d.atom_eps = ptr(arr("atom_eps", f32))
+    d.atom_static = ptr(arr("atom_static", u8))
+    d.n_water = nw
+    keep["wp"] = np.ascontiguousarray(wp)
+    keep["wv"] = np.ascontiguousarray(wv)
+    d.water_pos = ptr(keep["wp"]) if nw else None
+    d.water_vel = ptr(keep["wv"]) if nw else None
+    for name in ("excl", "pair14"):
+        a = arr(name, u32, -1)
+        setattr(d, "n_" + name, 0 if a is None else len(a) // 2)
+        setattr(d, name, ptr(a))
+    b = arr("bonds", u32, -1)
+    d.n_bonds = 0 if b is None else len(b) // 2
+    d.bonds = ptr(b)
+    d.bond_k = ptr(arr("bond_k", f32))
+    d.bond_r0 = ptr(arr("bond_r0", f32))
+    a = arr("angles", u32, -1)
+    d.n_angles = 0 if a is None else len(a) // 3
+    d.angles = ptr(a)
+    d.angle_k = ptr(arr("angle_k", f32))
+    d.angle_theta0 = ptr(arr("angle_theta0", f32))
+    dh = arr("dihedrals", u32, -1)
+    d.n_dihedrals = 0 if dh is None else len(dh) // 4
+    d.dihedrals = ptr(dh)
+    d.dihedral_k = ptr(arr("dihedral_k", f32))
+    d.dihedral_n = ptr(arr("dihedral_n", f32))
+    d.dihedral_phase = ptr(arr("dihedral_phase", f32))
+    cn = arr("constraints", u32, -1)
+    d.n_constraints = 0 if cn is None else len(cn) // 2
+    d.constraints = ptr(cn)
+    d.constraint_r0 = ptr(arr("constraint_r0", f32))
+    return d, keep, nw, na
+
+
 class MdState:
     """A device-resident simulation (MdState, src/lib.rs:610-705)."""
 
     def __init__(self, system, cfg=None, stream=None):
         self.cfg = cfg or MdConfig()
         self.system = system
-        wp = f32(system.get("water_pos", np.zeros((0, 3, 3)))).reshape(-1, 9)
-        wv = f32(system.get("water_vel", np.zeros_like(wp))).reshape(-1, 9)
-        ap = f32(system.get("atom_pos", np.zeros((0, 3)))).reshape(-1, 3)
-        na = len(ap)
-        self.n_water = len(wp)
-        self.n_atoms = na
-        keep = {}
-
-        def arr(name, conv, shape=None, default=None):
-            if name not in system or system[name] is None or len(system[name]) == 0:
-                return None
-            a = conv(system[name])
-            if shape is not None:
-                a = a.reshape(shape)
-            keep[name] = a
-            return a
-
-        d = _lib.SystemDesc()
-        d.n_atoms = na
-        d.atom_pos = ptr(arr("atom_pos", f32, -1))
-        d.atom_vel = ptr(arr("atom_vel", f32, -1))
-        d.atom_mass = ptr(arr("atom_mass", f32))
-        d.atom_q = ptr(arr("atom_q", f32))
-        d.atom_sigma = ptr(arr("atom_sigma", f32))
-        d.atom_eps = ptr(arr("atom_eps", f32))
-        d.atom_static = ptr(arr("atom_static", u8))
-        d.n_water = self.n_water
-        keep["wp"] = np.ascontiguousarray(wp)
-        keep["wv"] = np.ascontiguousarray(wv)
-        d.water_pos = ptr(keep["wp"]) if self.n_water else None
-        d.water_vel = ptr(keep["wv"]) if self.n_water else None
-        for name, width, pfx in (("excl", 2, None), ("pair14", 2, None)):
-            a = arr(name, u32, -1)
-            setattr(d, "n_" + name, 0 if a is None else len(a) // width)
-            setattr(d, name, ptr(a))
-        b = arr("bonds", u32, -1)
-        d.n_bonds = 0 if b is None else len(b) // 2
-        d.bonds = ptr(b)
-        d.bond_k = ptr(arr("bond_k", f32))
-        d.bond_r0 = ptr(arr("bond_r0", f32))
-        a = arr("angles", u32, -1)
-        d.n_angles = 0 if a is None else len(a) // 3
-        d.angles = ptr(a)
-        d.angle_k = ptr(arr("angle_k", f32))
-        d.angle_theta0 = ptr(arr("angle_theta0", f32))
-        dh = arr("dihedrals", u32, -1)
-        d.n_dihedrals = 0 if dh is None else len(dh) // 4
-        d.dihedrals = ptr(dh)
-        d.dihedral_k = ptr(arr("dihedral_k", f32))
-        d.dihedral_n = ptr(arr("dihedral_n", f32))
-        d.dihedral_phase = ptr(arr("dihedral_phase", f32))
-        cn = arr("constraints", u32, -1)
-        d.n_constraints = 0 if cn is None else len(cn) // 2
-        d.constraints = ptr(cn)
-        d.constraint_r0 = ptr(arr("constraint_r0", f32))
+        d, keep, self.n_water, self.n_atoms = _system_desc(system)
         c = _config_struct(system, self.cfg)
         h = C.c_void_p()
         check(lib().dyn_sys_create(stream, C.byref(c), C.byref(d), C.byref(h)))
         self._h = h
+        self._owned = True
         self._cstruct = c
+
+    @classmethod
+    def _member(cls, handle, system, cfg):
+        """A view of a batch member (owned by the batch, never destroyed here)."""
+        self = cls.__new__(cls)
+        self.cfg = cfg
+        self.system = system
+        self.n_water = len(np.asarray(system.get("water_pos", np.zeros((0, 3, 3)))).reshape(-1, 9))
+        self.n_atoms = len(np.asarray(system.get("atom_pos", np.zeros((0, 3)))).reshape(-1, 3))
+        self._h = handle
+        self._owned = False
+        return self
 
     @property
     def handle(self):
@@ -283,7 +302,61 @@ class MdState:
 
     def close(self):
         if self._h is not None:
-            lib().dyn_sys_destroy(self._h)
+            if self._owned:
+                lib().dyn_sys_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MdBatch:
+    """Independent systems advanced together (dyn_batch_*): every stage of a
+    step is one kernel launch over all members with per-member block ranges,
+    and a step is one CUDA graph.  ``members[i]`` is an MdState view of
+    system i (state, energies, forces); results equal running it alone."""
+
+    def __init__(self, systems, cfgs, stream=None):
+        if isinstance(cfgs, MdConfig):
+            cfgs = [cfgs] * len(systems)
+        n = len(systems)
+        descs = (_lib.SystemDesc * n)()
+        confs = (_lib.Config * n)()
+        keep = []
+        for i, (sysd, cfg) in enumerate(zip(systems, cfgs)):
+            d, k, _, _ = _system_desc(sysd)
+            descs[i] = d
+            confs[i] = _config_struct(sysd, cfg)
+            keep.append(k)
+        h = C.c_void_p()
+        check(lib().dyn_batch_create(stream, n, confs, descs, C.byref(h)))
+        self._h = h
+        self.members = []
+        for i in range(n):
+            m = C.c_void_p()
+            check(lib().dyn_batch_member(h, i, C.byref(m)))
+            self.members.append(MdState._member(m, systems[i], cfgs[i]))
+
+    def step(self, dt, n_steps=1):
+        check(lib().dyn_batch_step(self._h, int(n_steps), float(dt)))
+
+    def sync(self):
+        check(lib().dyn_batch_sync(self._h))
+
+    def launches(self, spme=True):
+        """(fixed, rebuild, periodic) batched launches of one step."""
+        f, r, p = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib().dyn_batch_launches(self._h, 1 if spme else 0, C.byref(f), C.byref(r), C.byref(p)))
+        return f.value, r.value, p.value
+
+    def close(self):
+        if self._h is not None:
+            for m in self.members:
+                m._h = None
+            lib().dyn_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

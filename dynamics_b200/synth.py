@@ -182,3 +182,32 @@ def ewald_alpha(cutoff, rtol=1e-5):
     """alpha with erfc(alpha * cutoff) = rtol (GROMACS ewald-rtol rule)."""
     from scipy.special import erfcinv
     return float(erfcinv(rtol) / cutoff)
+
+
+def fft_size(n):
+    """Smallest m >= n whose prime factors are all in {2, 3, 5, 7}."""
+    m = max(1, int(n))
+    while True:
+        k = m
+        for p in (2, 3, 5, 7):
+            while k % p == 0:
+                k //= p
+        if k == 1:
+            return m
+        m += 1
+
+
+def config4_sizes(n_sys=64, seed=0, lo=512, hi=8000):
+    """Water counts drawn log-uniform from [lo, hi] (seeded)."""
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), n_sys)).round().astype(int)
+
+
+def batch_member(n_water, seed=0, density=0.0334, spacing=1.0):
+    """One water box of the batched form: box sized to ``density`` waters per
+    cubic angstrom and an FFT-friendly SPME grid of about ``spacing`` A.
+    Returns (system, grid)."""
+    box = float((n_water / density) ** (1.0 / 3.0))
+    sysd = water_box(int(n_water), box, seed=seed)
+    k = fft_size(int(np.ceil(box / spacing)))
+    return sysd, (k, k, k)

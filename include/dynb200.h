@@ -375,6 +375,45 @@ int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
  * under conditional nodes that the device sets. */
 int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic);
 
+/* ------------------------------------------------------------------ */
+/* Batched form: many independent systems, one launch per stage      */
+/* ------------------------------------------------------------------ */
+
+typedef struct dyn_batch_s* dyn_batch_t;
+
+/* Creates n resident systems (cfgs[i], systems[i], as dyn_sys_create) that
+ * are advanced together: every stage of a step is one kernel launch for all
+ * members, with per-member block ranges, and a step is one captured CUDA
+ * graph.  Members must share spme_interval and energy_interval; sizes,
+ * boxes, grids and integrators may differ.  No counterpart in the reference
+ * (it advances one MdState per call, src/integrate.rs:72). */
+int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cfgs,
+                     const dyn_system_desc_t* systems, dyn_batch_t* out);
+
+/* Advances every member n_steps steps of length dt (asynchronous). */
+int dyn_batch_step(dyn_batch_t b, uint32_t n_steps, float dt);
+
+/* Number of members. */
+int dyn_batch_size(dyn_batch_t b, uint32_t* n);
+
+/* Handle of member i for dyn_sys_get_state / get_energies / set_state /
+ * forces / step.  Owned by the batch: do not destroy it. */
+int dyn_batch_member(dyn_batch_t b, uint32_t i, dyn_sys_t* out);
+
+/* Waits for the batch stream; returns the first member's device-side error
+ * (DYN_ERR_NONFINITE, DYN_ERR_TIMEOUT, capacity overflow), if any. */
+int dyn_batch_sync(dyn_batch_t b);
+
+/* Batched kernel launches of one step (spme != 0: a step with SPME):
+ * *fixed every step, *rebuild more on a step that rebuilds any member's
+ * lists, *periodic more on a step with a periodic task.  cuFFT's kernels
+ * (one R2C and one C2R per member on SPME steps) are not counted. */
+int dyn_batch_launches(dyn_batch_t b, int spme, uint32_t* fixed, uint32_t* rebuild,
+                       uint32_t* periodic);
+
+/* Releases the batch and all its members. */
+int dyn_batch_destroy(dyn_batch_t b);
+
 #ifdef __cplusplus
 }
 #endif

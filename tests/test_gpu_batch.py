@@ -1,0 +1,80 @@
+"""The batched form (dyn_batch_*): systems of different sizes advanced in
+one launch per stage must give exactly the trajectories they give alone.
+
+Every force is accumulated as 64-bit fixed point and every stochastic term
+is keyed by (site, step, seed), so "the same" means bit-identical positions,
+velocities and energies, not a tolerance.
+"""
+import numpy as np
+import pytest
+
+from dynamics_b200 import md, synth
+
+from .systems import mixed, water_only
+
+pytestmark = pytest.mark.gpu
+
+
+def _cfg(sysd, integ=None, **kw):
+    box = float(sysd["box_hi"][0] - sysd["box_lo"][0])
+    k = synth.fft_size(int(np.ceil(box)))
+    c = md.MdConfig(coulomb_cutoff=8.0, lj_cutoff=8.0, spme_alpha=synth.ewald_alpha(8.0),
+                    spme_grid=(k, k, k), **kw)
+    if integ is not None:
+        c.integrator = integ
+    return c
+
+
+def _members():
+    systems = [water_only(n_side=7, seed=3), synth.water_box(512, 24.8, seed=4),
+               synth.water_box(729, 27.9, seed=5), mixed()]
+    cfgs = [
+        _cfg(systems[0], integ=md.LangevinMiddle(gamma=1.0), seed=11),
+        _cfg(systems[1], integ=md.VerletVelocity(thermostat=0.1), seed=12),
+        _cfg(systems[2], integ=md.VerletVelocity(thermostat=0.1), seed=13,
+             barostat_cfg=md.BarostatCfg()),
+        _cfg(systems[3], integ=md.LangevinMiddle(gamma=1.0), seed=14),
+    ]
+    systems = [md.equilibrate(s, c, n_steps=40, dt=0.001) for s, c in zip(systems, cfgs)]
+    return systems, cfgs
+
+
+def test_batch_matches_members_alone(gpu_lib):
+    systems, cfgs = _members()
+    n_steps = 60  # crosses list rebuilds, SPME and non-SPME steps
+    batch = md.MdBatch(systems, cfgs)
+    batch.step(0.002, n_steps)
+    batch.sync()
+    for i, (s, c) in enumerate(zip(systems, cfgs)):
+        alone = md.MdState(s, c)
+        alone.step(0.002, n_steps)
+        a, b = alone.state(), batch.members[i].state()
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=f"member {i} {k}")
+        ea, eb = alone.energies(), batch.members[i].energies()
+        for k in ("potential", "kinetic", "virial", "temperature", "pressure_bar", "step", "list_rebuilds"):
+            assert ea[k] == eb[k], (i, k, ea[k], eb[k])
+        alone.close()
+    batch.close()
+
+
+def test_batch_is_one_launch_per_stage(gpu_lib):
+    systems, cfgs = _members()
+    batch = md.MdBatch(systems, cfgs)
+    fixed, rebuild, periodic = batch.launches(spme=True)
+    per_system = [md.MdState(s, c) for s, c in zip(systems, cfgs)]
+    plain = sum(p.launches_per_step(True) for p in per_system)
+    # one launch per stage for all members, against one per stage per member
+    assert fixed < plain / 2, (fixed, plain)
+    assert fixed <= max(p.launches_per_step(True) for p in per_system) + 2
+    assert rebuild > 0 and periodic > 0
+    for p in per_system:
+        p.close()
+    batch.close()
+
+
+def test_batch_rejects_mixed_intervals(gpu_lib):
+    systems, cfgs = _members()
+    cfgs[1] = _cfg(systems[1], spme_interval=1)
+    with pytest.raises(Exception):
+        md.MdBatch(systems[:2], cfgs[:2])

@@ -33,9 +33,15 @@ def _cfg(sysd, mode="reference", integ=None, **kw):
     return c
 
 
-def _oracle(sysd, cfg):
+def _oracle(sysd, cfg, st=None):
+    """FP64 forces and energies of the kernel's own FP32 site coordinates:
+    with ``st`` the M sites are the engine's (its float32 virtual-site
+    placement), so both evaluate exactly the same coordinates."""
+    if st is not None:
+        sysd = {**sysd, "water_m": st.state()["water_m"]}
+    # the engine's parameters are float32: the oracle evaluates the same values
     return method.all_forces(sysd, {
-        "cutoff": cfg.coulomb_cutoff, "lj_cutoff": cfg.lj_cutoff, "alpha": cfg.spme_alpha,
+        "cutoff": cfg.coulomb_cutoff, "lj_cutoff": cfg.lj_cutoff, "alpha": float(np.float32(cfg.spme_alpha)),
         "grid": cfg.spme_grid, "mode": "corrected" if cfg.ewald_corrections else "reference"})
 
 
@@ -52,7 +58,7 @@ def test_forces_match_oracle(gpu_lib, make, mode):
     cfg = _cfg(sysd, mode)
     st = md.MdState(sysd, cfg)
     got = st.forces()
-    ref = _oracle(sysd, cfg)
+    ref = _oracle(sysd, cfg, st)
     err = _compare(got, ref)
     assert err < FORCE_RTOL, f"force rel-RMS {err:.3e}"
     assert abs(got["potential"] - ref["pe"]) <= PE_RTOL * abs(ref["pe"]), (got["potential"], ref["pe"])
