@@ -133,6 +133,10 @@ _SIGS = {
     "dyn_batch_sync": ([_P], C.c_int),
     "dyn_batch_launches": ([_P, C.c_int, _P, _P, _P], C.c_int),
     "dyn_batch_destroy": ([_P], C.c_int),
+    "dyn_batch_add": ([_P, _P, _P, _P], C.c_int),
+    "dyn_batch_remove": ([_P, C.c_uint32], C.c_int),
+    "dyn_batch_memory": ([_P, _P], C.c_int),
+    "dyn_sys_memory": ([_P, _P], C.c_int),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -66,6 +66,8 @@ struct dyn_batch_s {
     float graph_dt[4] = {0, 0, 0, 0};
     uint64_t host_step = 0;
     uint32_t spme_interval = 1, energy_interval = 1;
+    bool fixed_intervals = false;   // set by the first member
+    uint32_t views_cap = 0;         // members the device view arrays hold
 };
 
 namespace {
@@ -135,6 +137,17 @@ int capture_batch_step(dyn_batch_s* b, int g, float dt, bool spme, bool energy, 
     for (dyn_sys_t m : b->members) b->ctx.views.push_back(m->v);
     int rc = collect_maps(b, dt, spme, energy);
     if (rc) return rc;
+    if (b->views_cap < b->members.size()) {
+        // grow the per-variant view arrays (no graph that reads them is alive)
+        for (int k = 0; k < 4; ++k) {
+            if (b->graph[k]) { cudaGraphExecDestroy(b->graph[k]); b->graph[k] = nullptr; }
+            if (b->d_views[k]) cudaFree(b->d_views[k]);
+            b->d_views[k] = nullptr;
+        }
+        const uint32_t cap = std::max<uint32_t>(8u, (uint32_t)b->members.size() * 2);
+        for (int k = 0; k < 4; ++k) DYN_CUDA(cudaMalloc(&b->d_views[k], cap * sizeof(SysView)));
+        b->views_cap = cap;
+    }
     b->ctx.d_views = b->d_views[g];
     b->ctx.map_missing = false;
     DYN_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -196,8 +209,7 @@ extern "C" int dyn_batch_destroy(dyn_batch_t b) {
 
 extern "C" int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cfgs,
                                 const dyn_system_desc_t* systems, dyn_batch_t* out) {
-    DYN_CHECK(out && cfgs && systems, DYN_ERR_INVALID, "dyn_batch_create: NULL argument");
-    DYN_CHECK(n > 0, DYN_ERR_INVALID, "dyn_batch_create: empty batch");
+    DYN_CHECK(out && (n == 0 || (cfgs && systems)), DYN_ERR_INVALID, "dyn_batch_create: NULL argument");
     *out = nullptr;
     for (uint32_t i = 1; i < n; ++i) {
         DYN_CHECK(std::max(1u, cfgs[i].spme_interval) == std::max(1u, cfgs[0].spme_interval) &&
@@ -215,8 +227,11 @@ extern "C" int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cf
         const cudaError_t e = cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking);
         if (e != cudaSuccess) { dyn_batch_destroy(b); return dyn::cuda_fail(e, "cudaStreamCreateWithFlags"); }
     }
-    b->spme_interval = std::max(1u, cfgs[0].spme_interval);
-    b->energy_interval = std::max(1u, cfgs[0].energy_interval);
+    if (n > 0) {
+        b->spme_interval = std::max(1u, cfgs[0].spme_interval);
+        b->energy_interval = std::max(1u, cfgs[0].energy_interval);
+        b->fixed_intervals = true;
+    }
     for (uint32_t i = 0; i < n; ++i) {
         dyn_sys_t m = nullptr;
         const int rc = dyn_sys_create(b->stream, &cfgs[i], &systems[i], &m);
@@ -227,10 +242,6 @@ extern "C" int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cf
         }
         b->members.push_back(m);
     }
-    for (int g = 0; g < 4; ++g) {
-        const cudaError_t e = cudaMalloc(&b->d_views[g], n * sizeof(SysView));
-        if (e != cudaSuccess) { dyn_batch_destroy(b); return dyn::cuda_fail(e, "cudaMalloc"); }
-    }
     *out = b;
     return DYN_OK;
 }
@@ -238,6 +249,7 @@ extern "C" int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cf
 extern "C" int dyn_batch_step(dyn_batch_t b, uint32_t n_steps, float dt) {
     DYN_CHECK(b, DYN_ERR_INVALID, "dyn_batch_step: NULL handle");
     DYN_CHECK(dt > 0.f && std::isfinite(dt), DYN_ERR_INVALID, "dyn_batch_step: dt must be > 0");
+    if (b->members.empty()) return DYN_OK;
     for (uint32_t i = 0; i < n_steps; ++i) {
         const uint64_t s = b->host_step;
         const bool spme = (s % b->spme_interval) == 0;
@@ -304,4 +316,66 @@ extern "C" int dyn_batch_launches(dyn_batch_t b, int spme, uint32_t* fixed, uint
     *periodic = count([&] { dyn::launch_periodic(T); });
     *fixed = all - *rebuild - *periodic;
     return upload_maps(b);
+}
+
+namespace {
+
+// After a membership change: the graphs and the block maps they reference
+// describe the old member set.
+void drop_graphs(dyn_batch_s* b) {
+    for (int g = 0; g < 4; ++g)
+        if (b->graph[g]) { cudaGraphExecDestroy(b->graph[g]); b->graph[g] = nullptr; }
+    for (void* p : b->map_allocs) cudaFree(p);
+    b->map_allocs.clear();
+    b->ctx.maps.clear();
+}
+
+}  // namespace
+
+extern "C" int dyn_batch_add(dyn_batch_t b, const dyn_config_t* cfg, const dyn_system_desc_t* system,
+                             uint32_t* index) {
+    DYN_CHECK(b && cfg && system, DYN_ERR_INVALID, "dyn_batch_add: NULL argument");
+    if (b->fixed_intervals) {
+        DYN_CHECK(std::max(1u, cfg->spme_interval) == b->spme_interval &&
+                      std::max(1u, cfg->energy_interval) == b->energy_interval,
+                  DYN_ERR_INVALID, "dyn_batch_add: members must share spme_interval and energy_interval");
+    }
+    // a member joins at a step where its SPME and energy schedule (counted
+    // from its own step 0) matches the batch's
+    DYN_CHECK(b->host_step % b->spme_interval == 0 && b->host_step % b->energy_interval == 0,
+              DYN_ERR_INVALID, "dyn_batch_add: join only at a step that is a multiple of the SPME and "
+              "energy intervals");
+    DYN_CUDA(cudaStreamSynchronize(b->stream));
+    dyn_sys_t m = nullptr;
+    const int rc = dyn_sys_create(b->stream, cfg, system, &m);
+    if (rc != DYN_OK) return rc;
+    if (!b->fixed_intervals) {
+        b->spme_interval = std::max(1u, cfg->spme_interval);
+        b->energy_interval = std::max(1u, cfg->energy_interval);
+        b->fixed_intervals = true;
+    }
+    m->host_step = 0;
+    drop_graphs(b);
+    b->members.push_back(m);
+    if (index) *index = (uint32_t)(b->members.size() - 1);
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_remove(dyn_batch_t b, uint32_t i) {
+    DYN_CHECK(b, DYN_ERR_INVALID, "dyn_batch_remove: NULL handle");
+    DYN_CHECK(i < b->members.size(), DYN_ERR_INVALID, "dyn_batch_remove: index out of range");
+    DYN_CUDA(cudaStreamSynchronize(b->stream));
+    drop_graphs(b);
+    dyn_sys_destroy(b->members[i]);
+    b->members.erase(b->members.begin() + i);
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_memory(dyn_batch_t b, uint64_t* bytes) {
+    DYN_CHECK(b && bytes, DYN_ERR_INVALID, "dyn_batch_memory: NULL argument");
+    uint64_t t = (uint64_t)b->views_cap * sizeof(SysView) * 4;
+    for (dyn_sys_t m : b->members) t += m->bytes;
+    for (auto& kv : b->ctx.maps) t += (uint64_t)kv.second.total * sizeof(uint2);
+    *bytes = t;
+    return DYN_OK;
 }

@@ -17,6 +17,7 @@ struct dyn_sys_s {
     float graph_dt[4] = {0, 0, 0, 0};
     uint64_t host_step = 0;        // steps enqueued so far
     std::vector<void*> allocs;     // every device allocation, freed on destroy
+    size_t bytes = 0;              // device memory held (allocations, PME grids, cuFFT work)
     Scalars* h_sc = nullptr;       // pinned mirror of the scalars
 };
 

@@ -23,6 +23,7 @@ int dev_alloc(dyn_sys_s* h, T** p, size_t n, bool zero = true) {
     cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
     if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaMalloc");
     h->allocs.push_back((void*)*p);
+    h->bytes += n * sizeof(T);
     if (zero) {
         e = cudaMemsetAsync(*p, 0, n * sizeof(T), h->stream);
         if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaMemsetAsync");
@@ -644,6 +645,14 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dyn::pme_init(v, &h->plan_f, &h->plan_b, h->stream));
     v.plan_f = (int)h->plan_f;
     v.plan_b = (int)h->plan_b;
+    {
+        const size_t ng = (size_t)v.K[0] * v.K[1] * v.K[2], nc = (size_t)v.K[0] * v.K[1] * (v.K[2] / 2 + 1);
+        size_t wf = 0, wb = 0;
+        cufftGetSize(h->plan_f, &wf);
+        cufftGetSize(h->plan_b, &wb);
+        h->bytes += ng * (sizeof(long long) + sizeof(float)) + nc * sizeof(float2) +
+                    (v.K[0] + v.K[1] + v.K[2]) * sizeof(float) + wf + wb;
+    }
     h->allocs.push_back(v.qgrid_fix); h->allocs.push_back(v.qgrid); h->allocs.push_back(v.cgrid);
     for (int a = 0; a < 3; ++a) h->allocs.push_back(v.bmod[a]);
     set_block_counts(v);
@@ -1085,4 +1094,10 @@ extern "C" int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out) {
 extern "C" int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic) {
     DYN_CHECK(h && rebuild && periodic, DYN_ERR_INVALID, "dyn_sys_launches_conditional: NULL argument");
     return count_step_kernels(h, false, nullptr, rebuild, periodic);
+}
+
+extern "C" int dyn_sys_memory(dyn_sys_t h, uint64_t* bytes) {
+    DYN_CHECK(h && bytes, DYN_ERR_INVALID, "dyn_sys_memory: NULL argument");
+    *bytes = h->bytes;
+    return DYN_OK;
 }

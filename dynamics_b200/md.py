@@ -284,6 +284,12 @@ class MdState:
         check(lib().dyn_sys_stage_times(self.handle, int(n_steps), float(dt), ptr(ms)))
         return dict(zip(self.STAGES, ms.tolist()))
 
+    def memory(self):
+        """Device bytes this system holds."""
+        b = C.c_uint64()
+        check(lib().dyn_sys_memory(self.handle, C.byref(b)))
+        return b.value
+
     def launches_per_step(self, spme=True):
         """Kernels of a step without a list rebuild or periodic task."""
         n = C.c_uint32()
@@ -319,12 +325,14 @@ class MdBatch:
     and a step is one CUDA graph.  ``members[i]`` is an MdState view of
     system i (state, energies, forces); results equal running it alone."""
 
-    def __init__(self, systems, cfgs, stream=None):
+    def __init__(self, systems=(), cfgs=(), stream=None):
+        systems = list(systems)
         if isinstance(cfgs, MdConfig):
             cfgs = [cfgs] * len(systems)
+        cfgs = list(cfgs)
         n = len(systems)
-        descs = (_lib.SystemDesc * n)()
-        confs = (_lib.Config * n)()
+        descs = (_lib.SystemDesc * max(n, 1))()
+        confs = (_lib.Config * max(n, 1))()
         keep = []
         for i, (sysd, cfg) in enumerate(zip(systems, cfgs)):
             d, k, _, _ = _system_desc(sysd)
@@ -345,6 +353,31 @@ class MdBatch:
 
     def sync(self):
         check(lib().dyn_batch_sync(self._h))
+
+    def add(self, system, cfg):
+        """Adds a member between steps (continuous batching); returns its
+        MdState view."""
+        d, keep, _, _ = _system_desc(system)
+        c = _config_struct(system, cfg)
+        idx = C.c_uint32()
+        check(lib().dyn_batch_add(self._h, C.byref(c), C.byref(d), C.byref(idx)))
+        h = C.c_void_p()
+        check(lib().dyn_batch_member(self._h, idx.value, C.byref(h)))
+        m = MdState._member(h, system, cfg)
+        self.members.append(m)
+        return m
+
+    def remove(self, member):
+        """Removes (destroys) a member between steps."""
+        i = self.members.index(member)
+        check(lib().dyn_batch_remove(self._h, i))
+        member._h = None
+        del self.members[i]
+
+    def memory(self):
+        b = C.c_uint64()
+        check(lib().dyn_batch_memory(self._h, C.byref(b)))
+        return b.value
 
     def launches(self, spme=True):
         """(fixed, rebuild, periodic) batched launches of one step."""

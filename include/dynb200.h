@@ -343,6 +343,9 @@ int dyn_sys_sync(dyn_sys_t h);
 
 int dyn_sys_destroy(dyn_sys_t h);
 
+/* Device memory the system holds (its arrays, PME grids, cuFFT work areas). */
+int dyn_sys_memory(dyn_sys_t h, uint64_t* bytes);
+
 /* Drop-in step with the state on the host, as the reference's MdState keeps
  * it (src/integrate.rs:72, README "state lives on the host"): copies the
  * given positions/velocities (home order, NULL = keep the resident ones) to
@@ -410,6 +413,21 @@ int dyn_batch_sync(dyn_batch_t b);
  * (one R2C and one C2R per member on SPME steps) are not counted. */
 int dyn_batch_launches(dyn_batch_t b, int spme, uint32_t* fixed, uint32_t* rebuild,
                        uint32_t* periodic);
+
+/* Continuous batching: adds a member (as dyn_sys_create, on the batch
+ * stream) between steps; *index receives its position.  A member joins only
+ * at a batch step that is a multiple of the SPME and energy intervals, so
+ * that its schedule, counted from its own step 0, is the one it would have
+ * alone.  n = 0 in dyn_batch_create makes an empty batch to add to. */
+int dyn_batch_add(dyn_batch_t b, const dyn_config_t* cfg, const dyn_system_desc_t* system,
+                  uint32_t* index);
+
+/* Removes (and destroys) member i between steps; later members move down by
+ * one index. */
+int dyn_batch_remove(dyn_batch_t b, uint32_t i);
+
+/* Device memory the batch holds (members, block maps, views), in bytes. */
+int dyn_batch_memory(dyn_batch_t b, uint64_t* bytes);
 
 /* Releases the batch and all its members. */
 int dyn_batch_destroy(dyn_batch_t b);
