@@ -60,7 +60,8 @@ class Config(C.Structure):
         ("spme_interval", C.c_uint32), ("com_interval", C.c_uint32),
         ("recenter_interval", C.c_uint32), ("energy_interval", C.c_uint32),
         ("flags", C.c_uint32), ("thermo_dof", C.c_uint32), ("seed", C.c_uint64),
-        ("ww_union_chunk", C.c_uint32), ("reserved0", C.c_uint32),
+        ("ww_union_chunk", C.c_uint32), ("lincs_order", C.c_uint32), ("lincs_iter", C.c_uint32),
+        ("reserved0", C.c_uint32),
     ]
 
 

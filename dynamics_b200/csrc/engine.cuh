@@ -27,6 +27,7 @@
 #define WCL 8             // waters per cluster
 #define GRPW 32           // waters per i-group of the water-water kernel (4 clusters)
 #define NPOLY_G 12        // coefficients of the screened-Coulomb force polynomial
+#define UMAX 5            // atoms per constraint unit (a heavy atom and up to 4 H)
 #define LPW 8             // lanes per i-water in the water-water kernel
 #define ACL 8             // atoms per cluster
 #define INVALID_ID 0xFFFFFFFFu
@@ -132,6 +133,11 @@ struct SysView {
     uint32_t nangle; uint4* angle; float2* angle_par;
     uint32_t ndih; uint4* dih; float4* dih_par;      // k, n, phase
     uint32_t ncons; uint2* cons; float* cons_r0;
+    // atoms grouped for the constraints: unit u = atoms unit_idx[unit_off[u]
+    // .. unit_off[u+1]), the heavy atom first, then its constrained H (with
+    // r0^2 in unit_r02); unconstrained atoms are units of one
+    uint32_t nunit; uint32_t* unit_off; uint32_t* unit_idx; float* unit_r02;
+    uint32_t lincs_order, lincs_iter;
     // PME
     uint32_t K[3];
     long long* qgrid_fix;   // [K0*K1*K2]

@@ -148,28 +148,133 @@ DYN_KERNEL(, k_water_first, (, float dt), (, dt)) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// constraint units: a heavy atom (slot 0) and the H constrained to it
+// (slots 1..n-1), processed by one thread so the reference's sequential
+// constraint loops run unchanged on each unit (src/bonded.rs:141-304)
+// ---------------------------------------------------------------------------
+struct Unit {
+    int n;
+    uint32_t id[UMAX];
+    float3 x[UMAX], vel[UMAX];
+    float m[UMAX], r02[UMAX];
+    bool fixed[UMAX];
+};
+
+__device__ __forceinline__ void load_unit(const SysView& v, uint32_t u, Unit& U) {
+    const uint32_t b = v.unit_off[u], e = v.unit_off[u + 1];
+    U.n = (int)(e - b);
+#pragma unroll
+    for (int k = 0; k < UMAX; ++k) {
+        if (k >= U.n) break;
+        const uint32_t a = v.unit_idx[b + k];
+        U.id[k] = a;
+        U.x[k] = xyz(v.apos[a]);
+        U.vel[k] = xyz(v.avel[a]);
+        U.m[k] = v.amass[a];
+        U.r02[k] = v.unit_r02[b + k];
+        U.fixed[k] = v.astatic && v.astatic[a];
+    }
+}
+
+// lincs_hydrogens (src/bonded.rs:218-284): order projection passes along the
+// bond, then iter SHAKE-style passes; returns the constraint virial
+// sum r_ij . f_i (native units) with f_i the heavy atom's displacement times
+// m / dt^2 (the reference's estimate, :273-283)
+__device__ __forceinline__ double constrain_unit(Unit& U, uint32_t order, uint32_t iter, float inv_dt2) {
+    if (U.n < 2) return 0.0;
+    const float3 x0 = U.x[0];
+    for (uint32_t o = 0; o < order; ++o) {
+        for (int k = 1; k < U.n; ++k) {
+            const float3 d = U.x[k] - U.x[0];
+            const float dl = fmaxf(sqrtf(dot3(d, d)), 1.1920929e-7f);
+            const float3 bv = d * (1.0f / dl);
+            const float im = 1.0f / U.m[0] + 1.0f / U.m[k];
+            const float lam = (sqrtf(U.r02[k]) - dot3(bv, d)) / im;
+            const float3 corr = bv * lam;
+            if (!U.fixed[0]) U.x[0] = U.x[0] - corr * (1.0f / U.m[0]);
+            if (!U.fixed[k]) U.x[k] = U.x[k] + corr * (1.0f / U.m[k]);
+        }
+    }
+    for (uint32_t it = 0; it < iter; ++it) {
+        for (int k = 1; k < U.n; ++k) {
+            const float3 d = U.x[k] - U.x[0];
+            const float d2 = dot3(d, d);
+            const float im = 1.0f / U.m[0] + 1.0f / U.m[k];
+            const float lam = (d2 - U.r02[k]) / (2.0f * im * fmaxf(d2, 1e-8f));
+            const float3 corr = d * lam;
+            if (!U.fixed[0]) U.x[0] = U.x[0] + corr * (1.0f / U.m[0]);
+            if (!U.fixed[k]) U.x[k] = U.x[k] - corr * (1.0f / U.m[k]);
+        }
+    }
+    const float3 fi = (U.x[0] - x0) * (U.m[0] * inv_dt2);
+    double w = 0.0;
+    for (int k = 1; k < U.n; ++k) w += (double)dot3(U.x[k] - U.x[0], fi);
+    return w;
+}
+
+// rattle_hydrogens (src/bonded.rs:288-304): remove the velocity component
+// along each constrained bond
+__device__ __forceinline__ void rattle_unit(Unit& U) {
+    for (int k = 1; k < U.n; ++k) {
+        const float3 r = U.x[k] - U.x[0];
+        const float3 dv = U.vel[k] - U.vel[0];
+        const float r2 = dot3(r, r);
+        const float im = 1.0f / U.m[0] + 1.0f / U.m[k];
+        const float lam = dot3(dv, r) / (im * fmaxf(r2, 1e-8f));
+        const float3 corr = r * lam;
+        U.vel[0] = U.vel[0] + corr * (1.0f / U.m[0]);
+        U.vel[k] = U.vel[k] - corr * (1.0f / U.m[k]);
+    }
+}
+
+// First half for non-water atoms, one constraint unit per thread:
+// Langevin-middle kick dt/2 + drift dt/2, constrain + rattle, OU, rattle,
+// drift dt/2, constrain (src/integrate.rs:100-160,478-511,566-587);
+// velocity Verlet kick dt/2 + drift dt, constrain + rattle.  The constraint
+// virial of the first projection (dt/2) is the step's (src/integrate.rs:105-165).
 DYN_KERNEL(, k_atom_first, (, float dt), (, dt)) {
     const uint64_t step = v.sc->step;
     const bool lm = v.integrator == DYN_INTEGRATOR_LANGEVIN_MIDDLE;
     const float c = expf(-v.gamma * dt);
     const float num = KB_NATIVE * v.temperature * fmaxf(1.0f - c * c, 0.f);
-    for (uint32_t a = bk.idx * blockDim.x + threadIdx.x; a < v.na; a += bk.cnt * blockDim.x) {
-        if (v.astatic && v.astatic[a]) continue;
-        float4 p = v.apos[a];
-        float3 x = xyz(p), vel = xyz(v.avel[a]);
-        const float hk = 0.5f * dt;
-        vel = vel + xyz(v.aacc[a]) * hk;
-        if (lm) {
-            x = x + vel * hk;
-            const float sg = sqrtf(num / v.amass[a]);
-            vel = vel * c + ou_normals(a, step, v.seed) * sg;
-            x = x + vel * hk;
-        } else {
-            x = x + vel * dt;
+    const float hk = 0.5f * dt;
+    const float inv_dt2 = 1.0f / (hk * hk);
+    double vir = 0.0;
+    for (uint32_t u = bk.idx * blockDim.x + threadIdx.x; u < v.nunit; u += bk.cnt * blockDim.x) {
+        Unit U;
+        load_unit(v, u, U);
+        for (int k = 0; k < U.n; ++k) {
+            if (U.fixed[k]) continue;
+            U.vel[k] = U.vel[k] + xyz(v.aacc[U.id[k]]) * hk;
+            U.x[k] = U.x[k] + U.vel[k] * (lm ? hk : dt);
         }
-        v.apos[a] = make_float4(x.x, x.y, x.z, p.w);
-        v.avel[a] = make_float4(vel.x, vel.y, vel.z, 0.f);
-        if (!finite3(x)) v.sc->nonfinite = 1u;
+        vir += constrain_unit(U, v.lincs_order, v.lincs_iter, inv_dt2);
+        rattle_unit(U);
+        if (lm) {
+            for (int k = 0; k < U.n; ++k) {
+                if (U.fixed[k]) continue;
+                const float sg = sqrtf(num / U.m[k]);
+                U.vel[k] = U.vel[k] * c + ou_normals(U.id[k], step, v.seed) * sg;
+            }
+            rattle_unit(U);
+            for (int k = 0; k < U.n; ++k)
+                if (!U.fixed[k]) U.x[k] = U.x[k] + U.vel[k] * hk;
+            constrain_unit(U, v.lincs_order, v.lincs_iter, inv_dt2);
+        }
+        for (int k = 0; k < U.n; ++k) {
+            const uint32_t a = U.id[k];
+            if (U.fixed[k]) continue;
+            v.apos[a] = make_float4(U.x[k].x, U.x[k].y, U.x[k].z, v.apos[a].w);
+            v.avel[a] = make_float4(U.vel[k].x, U.vel[k].y, U.vel[k].z, 0.f);
+            if (!finite3(U.x[k])) v.sc->nonfinite = 1u;
+        }
+    }
+    double x[1] = {vir};
+    block_sum_d<1>(x);
+    if (threadIdx.x == 0) {
+        double* p = v.partials + ((size_t)REG_CONS * v.max_blocks + bk.idx) * 4;
+        p[0] = x[0]; p[1] = 0.0; p[2] = 0.0; p[3] = 0.0;
     }
 }
 
@@ -237,18 +342,27 @@ DYN_KERNEL(, k_water_kick, (, float dt), (, dt)) {
 
 DYN_KERNEL(, k_atom_kick, (, float dt), (, dt)) {
     double ke = 0.0;
-    for (uint32_t a = bk.idx * blockDim.x + threadIdx.x; a < v.na; a += bk.cnt * blockDim.x) {
-        if (v.astatic && v.astatic[a]) continue;
-        const float3 f = ldfix3sum(v.aforce + 3 * (size_t)a, v.arecip + 3 * (size_t)a);
-        // kick_and_calc_accel with the MAX_ACCEL clamp (src/integrate.rs:521-535)
-        float3 acc = f * (KCAL_TO_NATIVE / v.amass[a]);
-        const float a2 = dot3(acc, acc);
-        if (a2 > MAX_ACCEL * MAX_ACCEL) acc = acc * (MAX_ACCEL * rsqrtf(a2));
-        const float3 vel = xyz(v.avel[a]) + acc * (0.5f * dt);
-        v.aacc[a] = make_float4(acc.x, acc.y, acc.z, 0.f);
-        v.avel[a] = make_float4(vel.x, vel.y, vel.z, 0.f);
-        ke += (double)(v.amass[a] * dot3(vel, vel));
-        if (!finite3(acc)) v.sc->nonfinite = 1u;
+    for (uint32_t u = bk.idx * blockDim.x + threadIdx.x; u < v.nunit; u += bk.cnt * blockDim.x) {
+        Unit U;
+        load_unit(v, u, U);
+        for (int k = 0; k < U.n; ++k) {
+            if (U.fixed[k]) continue;
+            const uint32_t a = U.id[k];
+            const float3 f = ldfix3sum(v.aforce + 3 * (size_t)a, v.arecip + 3 * (size_t)a);
+            // kick_and_calc_accel with the MAX_ACCEL clamp (src/integrate.rs:521-535)
+            float3 acc = f * (KCAL_TO_NATIVE / U.m[k]);
+            const float a2 = dot3(acc, acc);
+            if (a2 > MAX_ACCEL * MAX_ACCEL) acc = acc * (MAX_ACCEL * rsqrtf(a2));
+            U.vel[k] = U.vel[k] + acc * (0.5f * dt);
+            v.aacc[a] = make_float4(acc.x, acc.y, acc.z, 0.f);
+            if (!finite3(acc)) v.sc->nonfinite = 1u;
+        }
+        rattle_unit(U);  // src/integrate.rs:554-559
+        for (int k = 0; k < U.n; ++k) {
+            if (U.fixed[k]) continue;
+            v.avel[U.id[k]] = make_float4(U.vel[k].x, U.vel[k].y, U.vel[k].z, 0.f);
+            ke += (double)(U.m[k] * dot3(U.vel[k], U.vel[k]));
+        }
     }
     double x[2] = {ke, ke};
     block_sum_d<2>(x);
@@ -578,13 +692,13 @@ inline int iblocks(const SysView& v, uint64_t n) {
 namespace dyn {
 
 int kick_blocks_w(const SysView& v) { return iblocks(v, v.nw_cap); }
-int kick_blocks_a(const SysView& v) { return iblocks(v, v.na); }
+int kick_blocks_a(const SysView& v) { return iblocks(v, v.nunit); }
 
 void launch_first_half(const Target& t, float dt) {
     t.launch(k_water_first, k_water_first_batch, [](const SysView& v) { return v.nw ? iblocks(v, v.nw_cap) : 0; },
              IT, 0, dt);
-    t.launch(k_atom_first, k_atom_first_batch, [](const SysView& v) { return v.na ? iblocks(v, v.na) : 0; }, IT, 0,
-             dt);
+    t.launch(k_atom_first, k_atom_first_batch, [](const SysView& v) { return v.na ? (int)v.nb[REG_CONS] : 0; },
+             IT, 0, dt);
 }
 
 void launch_second_half(const Target& t, float dt) {

@@ -88,7 +88,7 @@ void set_block_counts(SysView& v) {
     v.nb[REG_BOND] = (v.nbond + v.nangle + v.ndih) ? dyn::bond_blocks(v) : 0;
     v.nb[REG_KICK_W] = v.nw ? dyn::kick_blocks_w(v) : 0;
     v.nb[REG_KICK_A] = v.na ? dyn::kick_blocks_a(v) : 0;
-    v.nb[REG_CONS] = 0;
+    v.nb[REG_CONS] = v.na ? dyn::kick_blocks_a(v) : 0;  // written by the atoms' first half
     v.nb[REG_PME] = dyn::pme_blocks(v);
     v.nb[REG_CORR] = dyn::gather_blocks(v);
     v.nb[REG_CORR_A] = dyn::corr_blocks(v);
@@ -310,6 +310,28 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     for (uint32_t i = 0; i < d->n_atoms; ++i)
         DYN_CHECK(d->atom_mass[i] > 0.f || (d->atom_static && d->atom_static[i]), DYN_ERR_INVALID,
                   "dyn_sys_create: non-static atoms need mass > 0");
+    // constraint units: each heavy atom with the H constrained to it
+    std::vector<std::vector<uint32_t>> unit_h(d->n_atoms);
+    std::vector<float> h_r02(d->n_atoms, 0.f);
+    {
+        std::vector<uint8_t> role(d->n_atoms, 0);  // 1 heavy end, 2 H end
+        for (uint32_t c = 0; c < d->n_constraints; ++c) {
+            DYN_CHECK(d->constraints && d->constraint_r0, DYN_ERR_INVALID, "dyn_sys_create: NULL constraint array");
+            const uint32_t a = d->constraints[2 * c], b = d->constraints[2 * c + 1];
+            DYN_CHECK(a < d->n_atoms && b < d->n_atoms && a != b, DYN_ERR_INVALID,
+                      "dyn_sys_create: constraint index out of range");
+            DYN_CHECK(d->constraint_r0[c] > 0.f, DYN_ERR_INVALID, "dyn_sys_create: constraint_r0 must be > 0");
+            const uint32_t hv = d->atom_mass[a] >= d->atom_mass[b] ? a : b, hy = hv == a ? b : a;
+            DYN_CHECK(role[hy] == 0 && role[hv] != 2, DYN_ERR_UNSUPPORTED,
+                      "dyn_sys_create: constraints must be bonds from a heavy atom to its own hydrogens");
+            role[hy] = 2;
+            role[hv] = 1;
+            unit_h[hv].push_back(hy);
+            h_r02[hy] = d->constraint_r0[c] * d->constraint_r0[c];
+            DYN_CHECK(unit_h[hv].size() < UMAX, DYN_ERR_UNSUPPORTED,
+                      "dyn_sys_create: more than 4 hydrogens constrained to one atom");
+        }
+    }
 
     dyn_sys_s* h = new dyn_sys_s();
     h->stream = (cudaStream_t)stream;
@@ -652,6 +674,35 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         cufftGetSize(h->plan_b, &wb);
         h->bytes += ng * (sizeof(long long) + sizeof(float)) + nc * sizeof(float2) +
                     (v.K[0] + v.K[1] + v.K[2]) * sizeof(float) + wf + wb;
+    }
+    {
+        // units in atom order; an H goes with its heavy atom
+        std::vector<uint32_t> off(1, 0), idx;
+        std::vector<float> r02;
+        std::vector<uint8_t> is_h(d->n_atoms, 0);
+        for (uint32_t a = 0; a < d->n_atoms; ++a)
+            for (uint32_t hy : unit_h[a]) is_h[hy] = 1;
+        for (uint32_t a = 0; a < d->n_atoms; ++a) {
+            if (is_h[a]) continue;
+            idx.push_back(a);
+            r02.push_back(0.f);
+            for (uint32_t hy : unit_h[a]) {
+                idx.push_back(hy);
+                r02.push_back(h_r02[hy]);
+            }
+            off.push_back((uint32_t)idx.size());
+        }
+        v.nunit = (uint32_t)off.size() - 1;
+        v.ncons = d->n_constraints;
+        v.lincs_order = cfg->lincs_order ? cfg->lincs_order : 4u;
+        v.lincs_iter = cfg->lincs_iter ? cfg->lincs_iter : 1u;
+        TRY(dev_alloc(h, &v.unit_off, off.size()));
+        TRY(dev_alloc(h, &v.unit_idx, std::max<size_t>(1, idx.size())));
+        TRY(dev_alloc(h, &v.unit_r02, std::max<size_t>(1, r02.size())));
+        TRY(upload(h, v.unit_off, off.data(), off.size()));
+        TRY(upload(h, v.unit_idx, idx.data(), idx.size()));
+        TRY(upload(h, v.unit_r02, r02.data(), r02.size()));
+        TRYC(cudaStreamSynchronize(h->stream));
     }
     h->allocs.push_back(v.qgrid_fix); h->allocs.push_back(v.qgrid); h->allocs.push_back(v.cgrid);
     for (int a = 0; a < 3; ++a) h->allocs.push_back(v.bmod[a]);

@@ -71,6 +71,8 @@ class MdConfig:
     reset_angle: bool = True
     seed: int = 0
     ww_union_chunk: int = 0         # 0 = automatic (tuning knob only)
+    lincs_order: int = 4            # HydrogenConstraint::Linear { order, iter } (src/prep.rs:77)
+    lincs_iter: int = 1
 
 
 def thermo_dof(system, cfg):
@@ -132,6 +134,8 @@ def _config_struct(system, cfg):
     c.thermo_dof = thermo_dof(system, cfg)
     c.seed = int(cfg.seed) & 0xFFFFFFFFFFFFFFFF
     c.ww_union_chunk = int(cfg.ww_union_chunk)
+    c.lincs_order = int(cfg.lincs_order)
+    c.lincs_iter = int(cfg.lincs_iter)
     return c
 
 

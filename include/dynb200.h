@@ -251,6 +251,10 @@ typedef struct {
                              * water-water kernel; 0 = the largest that lets
                              * two CTAs share an SM (a tuning knob: results
                              * do not depend on it)                         */
+    uint32_t lincs_order;   /* bond-to-H constraints: projection passes of
+                             * HydrogenConstraint::Linear (src/prep.rs:55-78);
+                             * 0 = 4 (the reference default)                */
+    uint32_t lincs_iter;    /* SHAKE-style correction passes; 0 = 1         */
     uint32_t reserved0;
 } dyn_config_t;
 
@@ -277,7 +281,10 @@ typedef struct {
     const float* angle_k; const float* angle_theta0;
     uint32_t n_dihedrals; const uint32_t* dihedrals; /* [n*4], one row per term */
     const float* dihedral_k; const float* dihedral_n; const float* dihedral_phase;
-    uint32_t n_constraints; const uint32_t* constraints; /* [n*2] H bonds */
+    /* bonds to hydrogen held at constraint_r0 (src/bonded.rs:141-304): each
+     * pair is (heavy atom, H) in either order; every H in at most one pair,
+     * at most 4 H per heavy atom, no H as the heavy end of another pair */
+    uint32_t n_constraints; const uint32_t* constraints; /* [n*2] */
     const float* constraint_r0;
 } dyn_system_desc_t;
 

@@ -205,8 +205,88 @@ def zero_linear_momentum(state):
     state["water_vel"] -= vc[None, None, :]
 
 
+def _constraints(state):
+    """(heavy, H, r0^2, inverse-mass sum) per constraint, heavy end first."""
+    c = state.get("constraints")
+    if c is None or len(c) == 0:
+        return None
+    c = np.asarray(c, np.int64).reshape(-1, 2)
+    m = state["atom_mass"]
+    heavy = np.where(m[c[:, 0]] >= m[c[:, 1]], c[:, 0], c[:, 1])
+    hyd = np.where(heavy == c[:, 0], c[:, 1], c[:, 0])
+    r02 = np.asarray(state["constraint_r0"], np.float64) ** 2
+    return heavy, hyd, r02, 1.0 / m[heavy] + 1.0 / m[hyd]
+
+
+def _in_unit_order(state):
+    """Constraint indices grouped by heavy atom in atom order (the order in
+    which each unit's constraints are applied)."""
+    cs = _constraints(state)
+    heavy = cs[0]
+    return np.argsort(heavy, kind="stable")
+
+
+def lincs_hydrogens(state, dt, order=4, iters=1):
+    """lincs_hydrogens (src/bonded.rs:218-284): ``order`` projection passes
+    along each bond, then ``iters`` SHAKE-style passes, sequentially over
+    the constraints; returns the constraint virial estimate sum r_ij . f_i
+    with f_i from the heavy atom's displacement (native units)."""
+    cs = _constraints(state)
+    if cs is None:
+        return 0.0
+    heavy, hyd, r02, im = cs
+    x = state["atom_pos"]
+    m = state["atom_mass"]
+    fixed = state["atom_static"]
+    x0 = x.copy()
+    seq = _in_unit_order(state)
+    for _ in range(order):
+        for c in seq:
+            i, j = heavy[c], hyd[c]
+            d = x[j] - x[i]
+            dl = max(np.linalg.norm(d), 1.1920929e-7)
+            b = d / dl
+            corr = b * ((np.sqrt(r02[c]) - b @ d) / im[c])
+            if not fixed[i]:
+                x[i] -= corr / m[i]
+            if not fixed[j]:
+                x[j] += corr / m[j]
+    for _ in range(iters):
+        for c in seq:
+            i, j = heavy[c], hyd[c]
+            d = x[j] - x[i]
+            d2 = d @ d
+            corr = d * ((d2 - r02[c]) / (2.0 * im[c] * max(d2, 1e-8)))
+            if not fixed[i]:
+                x[i] += corr / m[i]
+            if not fixed[j]:
+                x[j] -= corr / m[j]
+    inv_dt2 = 1.0 / (dt * dt)
+    w = 0.0
+    for c in seq:
+        i, j = heavy[c], hyd[c]
+        w += float((x[j] - x[i]) @ ((x[i] - x0[i]) * (m[i] * inv_dt2)))
+    return w
+
+
+def rattle_hydrogens(state):
+    """rattle_hydrogens (src/bonded.rs:288-304)."""
+    cs = _constraints(state)
+    if cs is None:
+        return
+    heavy, hyd, _, im = cs
+    x, vel, m = state["atom_pos"], state["atom_vel"], state["atom_mass"]
+    for c in _in_unit_order(state):
+        i, j = heavy[c], hyd[c]
+        r = x[j] - x[i]
+        corr = r * (((vel[j] - vel[i]) @ r) / (im[c] * max(r @ r, 1e-8)))
+        vel[i] += corr / m[i]
+        vel[j] -= corr / m[j]
+
+
 def kick_and_calc_accel(state, forces, dt):
-    """kick_and_calc_accel (src/integrate.rs:515-562) without H constraints.
+    """kick_and_calc_accel (src/integrate.rs:515-562), with RATTLE when the
+    state carries constraints.
 
     ``forces``: dict with f_atoms (na,3), f_water (nw,4,3) [O,H0,H1,M].
     """
@@ -219,6 +299,7 @@ def kick_and_calc_accel(state, forces, dt):
         a = np.where(big[:, None], a / np.where(big, amag, 1.0)[:, None] * MAX_ACCEL, a)
         state["atom_accel"] = np.where(dyn[:, None], a, 0.0)
         state["atom_vel"] = state["atom_vel"] + state["atom_accel"] * dt
+        rattle_hydrogens(state)
     fw = forces["f_water"]
     if len(fw):
         fo, fh0, fh1 = opc.project_ep_force(fw[:, 0], fw[:, 1], fw[:, 2], fw[:, 3])
@@ -229,13 +310,16 @@ def kick_and_calc_accel(state, forces, dt):
 
 
 def kick_and_drift(state, dt_kick, dt_drift, lo, ext):
-    """kick_and_drift (src/integrate.rs:478-511) without H constraints."""
+    """kick_and_drift (src/integrate.rs:478-511); with constraints,
+    lincs_hydrogens(dt_kick) and RATTLE follow (:498-507)."""
     if len(state["atom_vel"]):
         dyn = ~state["atom_static"]
         v = state["atom_vel"] + state["atom_accel"] * dt_kick
         state["atom_vel"] = np.where(dyn[:, None], v, state["atom_vel"])
         state["atom_pos"] = np.where(dyn[:, None], state["atom_pos"] + state["atom_vel"] * dt_drift,
                                      state["atom_pos"])
+        state["virial_constraints"] = lincs_hydrogens(state, dt_kick)
+        rattle_hydrogens(state)
     if len(state["water_vel"]):
         state["water_vel"] = state["water_vel"] + state["water_accel"] * dt_kick
         p, v, m, vir = rigid_water_drift(state["water_pos"], state["water_vel"], dt_drift, lo, ext)

@@ -1,0 +1,84 @@
+"""ff19SB peptides in OPC water with ions and bond-to-H constraints: forces
+against the float64 oracle, a constrained velocity-Verlet trajectory against
+the oracle's restatement of lincs_hydrogens / rattle_hydrogens
+(src/bonded.rs:218-304), and constraint satisfaction under Langevin
+dynamics."""
+import numpy as np
+import pytest
+
+from dynamics_b200 import md, peptide, synth
+from oracle import integrate as oint
+
+from .systems import rel_rms
+from .test_gpu_native import FORCE_RTOL, PE_RTOL, _cfg, _compare, _oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(seed=4):
+    sysd, _ = peptide.solvated_system(28.0, 700, n_res=(10,), seed=seed, nacl_molar=0.15)
+    return sysd
+
+
+@pytest.fixture(scope="module")
+def relaxed():
+    sysd = _system()
+    return md.equilibrate(sysd, _cfg(sysd), n_steps=200, dt=0.0005)
+
+
+@pytest.mark.parametrize("mode", ["reference", "corrected"])
+def test_peptide_forces_match_oracle(gpu_lib, relaxed, mode):
+    cfg = _cfg(relaxed, mode)
+    st = md.MdState(relaxed, cfg)
+    got = st.forces()
+    ref = _oracle(relaxed, cfg, st)
+    err = _compare(got, ref)
+    assert err < FORCE_RTOL, f"force rel-RMS {err:.3e}"
+    assert abs(got["potential"] - ref["pe"]) <= PE_RTOL * abs(ref["pe"]), (got["potential"], ref["pe"])
+    st.close()
+
+
+def test_constrained_trajectory_matches_oracle(gpu_lib, relaxed):
+    cfg = _cfg(relaxed, integ=md.VerletVelocity(thermostat=None), spme_interval=1, zero_com_drift=False,
+               recenter_sim_box=False, reset_angle=False)
+    st = md.MdState(relaxed, cfg)
+    n, dt = 5, 0.002
+    st.step(dt, n)
+    got = st.state()
+    s = {"atom_pos": relaxed["atom_pos"].astype(np.float64), "atom_vel": relaxed["atom_vel"].astype(np.float64),
+         "atom_mass": relaxed["atom_mass"].astype(np.float64),
+         "atom_static": np.zeros(len(relaxed["atom_pos"]), bool),
+         "water_pos": relaxed["water_pos"].astype(np.float64),
+         "water_vel": relaxed["water_vel"].astype(np.float64),
+         "constraints": relaxed["constraints"], "constraint_r0": relaxed["constraint_r0"]}
+    lo = relaxed["box_lo"].astype(np.float64)
+    ext = (relaxed["box_hi"] - relaxed["box_lo"]).astype(np.float64)
+
+    def forces(s):
+        d = dict(relaxed)
+        d["atom_pos"], d["water_pos"] = s["atom_pos"], s["water_pos"]
+        d.pop("water_m", None)
+        return _oracle(d, cfg)
+
+    oint.kick_and_calc_accel(s, forces(s), 0.0)
+    for _ in range(n):
+        oint.kick_and_drift(s, dt / 2, dt, lo, ext)
+        oint.kick_and_calc_accel(s, forces(s), dt / 2)
+    d = got["atom_pos"].astype(np.float64) - s["atom_pos"]
+    d -= np.round(d / ext) * ext
+    assert np.max(np.abs(d)) < 2e-4
+    assert rel_rms(got["atom_vel"], s["atom_vel"]) < 2e-3
+    st.close()
+
+
+def test_constraints_hold_under_langevin(gpu_lib, relaxed):
+    cfg = _cfg(relaxed, integ=md.LangevinMiddle(gamma=1.0))
+    st = md.MdState(relaxed, cfg)
+    st.step(0.002, 100)
+    e = st.energies()
+    assert np.isfinite(e["temperature"]) and 150.0 < e["temperature"] < 600.0
+    p = st.state()["atom_pos"].astype(np.float64)
+    c = relaxed["constraints"].astype(int)
+    r = np.linalg.norm(p[c[:, 0]] - p[c[:, 1]], axis=1)
+    assert np.max(np.abs(r - relaxed["constraint_r0"]) / relaxed["constraint_r0"]) < 1e-3
+    st.close()
