@@ -33,6 +33,16 @@ WORKLOADS = {
     "c1": dict(n_water=512, box=24.8, cutoff=10.0, grid=(32, 32, 32), integrator="langevin",
                barostat=False),
     # ~100k atoms: 24,000 OPC waters in a 98 A cube, rc 10, 96^3, CSVR 300 K + C-rescale 1 bar
+    # ~32k atoms: a 40-residue ff19SB peptide, counter-ions, 7,800 OPC waters
+    # in a 62 A cube, rc 9, 64^3, CSVR 300 K, bond-to-H constraints
+    "c2": dict(n_water=7800, box=62.0, cutoff=9.0, grid=(64, 64, 64), integrator="vv_csvr",
+               barostat=False, n_res=(40,), nacl=0.0),
+    # ~100k atoms: a 300-residue ff19SB peptide, 24,000 OPC waters with NaCl
+    # at 0.15 M (plus counter-ions; ions replace waters) in a 98 A cube,
+    # rc 10, 96^3, CSVR 300 K + C-rescale 1 bar, bond-to-H constraints
+    "c3": dict(n_water=24000, box=98.0, cutoff=10.0, grid=(96, 96, 96), integrator="vv_csvr",
+               barostat=True, n_res=(300,), nacl=0.15),
+    # the same box with water only
     "c3w": dict(n_water=24000, box=98.0, cutoff=10.0, grid=(96, 96, 96), integrator="vv_csvr",
                 barostat=True),
     # batched form: 64 water boxes, 512-8000 waters log-uniform, 0.0334 / A^3,
@@ -45,7 +55,7 @@ WORKLOADS = {
     "c5w": dict(kind="serve", n_req=48, rate=20.0, steps_each=5000, cutoff=9.0, budget=150e9,
                 integrator="langevin", barostat=False, n_water=None),
 }
-DEFAULT_WORKLOAD = "c3w"
+DEFAULT_WORKLOAD = "c3"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
 # the water-water pair kernel, from an ncu --set full capture of this
 # workload (cold L2, as in the timed loop, which flushes L2 between steps)
@@ -56,7 +66,12 @@ DT = 0.002
 def build_system(name, seed):
     from dynamics_b200 import md, synth
     w = WORKLOADS[name]
-    sysd = synth.water_box(w["n_water"], w["box"], seed=seed)
+    if w.get("n_res"):
+        from dynamics_b200 import peptide
+        sysd, _ = peptide.solvated_system(w["box"], w["n_water"], n_res=w["n_res"], seed=seed,
+                                          nacl_molar=w.get("nacl", 0.0))
+    else:
+        sysd = synth.water_box(w["n_water"], w["box"], seed=seed)
     alpha = synth.ewald_alpha(w["cutoff"])
     cfg = md.MdConfig(coulomb_cutoff=w["cutoff"], lj_cutoff=w["cutoff"], spme_alpha=alpha,
                       spme_grid=w["grid"], seed=seed)
@@ -293,22 +308,49 @@ def run_serve(args):
 
 def count_pairs(sysd, cutoff):
     """Interacting site pairs within the cutoff (the algorithmic pair count):
-    water O-O LJ pairs and charged-site Coulomb pairs of different molecules."""
+    LJ pairs between LJ sites (water O, atoms with eps > 0) and Coulomb pairs
+    between charged sites, not in the same water and not excluded (1-2, 1-3;
+    1-4 pairs count once, as scaled pairs)."""
     from scipy.spatial import cKDTree
     lo = np.asarray(sysd["box_lo"], np.float64)
     ext = (np.asarray(sysd["box_hi"], np.float64) - lo)
     wp = np.asarray(sysd["water_pos"], np.float64)
+    nw = len(wp)
     o = wp[:, 0]
     bis = (wp[:, 1] - o) + (wp[:, 2] - o)
     m = o + bis / np.linalg.norm(bis, axis=1, keepdims=True) * 0.15939833
-    def npairs(pts, mol):
+    ap = np.asarray(sysd.get("atom_pos", np.zeros((0, 3))), np.float64).reshape(-1, 3)
+    na = len(ap)
+    excl = set()
+    if na and "excl" in sysd and len(sysd["excl"]):
+        excl = set(map(tuple, np.sort(np.asarray(sysd["excl"], np.int64), axis=1).tolist()))
+
+    def npairs(pts, mol, atom_id):
         t = cKDTree(np.mod(pts - lo, ext), boxsize=ext)
         p = t.query_pairs(cutoff, output_type="ndarray")
-        return int(np.count_nonzero(mol[p[:, 0]] != mol[p[:, 1]]))
-    nw = len(o)
-    n_lj = npairs(o, np.arange(nw))
-    q = np.concatenate([wp[:, 1], wp[:, 2], m], axis=0)
-    n_c = npairs(q, np.tile(np.arange(nw), 3))
+        keep = mol[p[:, 0]] != mol[p[:, 1]]
+        p = p[keep]
+        if excl:
+            a, b = atom_id[p[:, 0]], atom_id[p[:, 1]]
+            both = (a >= 0) & (b >= 0)
+            if both.any():
+                pa = np.sort(np.stack([a[both], b[both]], 1), axis=1)
+                ex = np.array([tuple(x) in excl for x in pa.tolist()])
+                return int(len(p) - np.count_nonzero(ex))
+        return int(len(p))
+
+    ljm = np.asarray(sysd.get("atom_eps", np.zeros(na))) > 0
+    qm = np.asarray(sysd.get("atom_q", np.zeros(na))) != 0
+    amol = -1 - np.arange(na)
+    aid = np.arange(na)
+    lj_pts = np.concatenate([o, ap[ljm]])
+    lj_mol = np.concatenate([np.arange(nw), amol[ljm]])
+    lj_id = np.concatenate([np.full(nw, -1), aid[ljm]])
+    n_lj = npairs(lj_pts, lj_mol, lj_id)
+    q_pts = np.concatenate([wp[:, 1], wp[:, 2], m, ap[qm]])
+    q_mol = np.concatenate([np.tile(np.arange(nw), 3), amol[qm]])
+    q_id = np.concatenate([np.full(3 * nw, -1), aid[qm]])
+    n_c = npairs(q_pts, q_mol, q_id)
     return n_lj, n_c
 
 
@@ -429,26 +471,28 @@ def run_ours(args):
     peak = C.c_double()
     _lib.check(_lib.lib().dyn_probe_fp32_peak(stream.cuda_stream, C.byref(peak)))
     # PME: algorithmic bytes of spread + gather per SPME step
-    nq = 3 * w["n_water"]
+    nq = 3 * st.n_water + st.n_atoms
     K = np.prod(w["grid"])
     pme_bytes = nq * 16 + K * 4 + nq * 16 + K * 4 + nq * 12
     pme_ms = stages["spme"]
     # ---- end-to-end through the host-buffer C-ABI step ----
-    nw = st.n_water
+    nw, na = st.n_water, st.n_atoms
+    st_nw, st_na = nw, na
     pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
     s0 = st.state()
-    wp_in, wv_in = pin((nw, 3, 3)), pin((nw, 3, 3))
-    wp_out, wv_out = pin((nw, 3, 3)), pin((nw, 3, 3))
-    wp_in[:] = s0["water_pos"]
-    wv_in[:] = s0["water_vel"]
+    io = {"water_pos": pin((nw, 3, 3)), "water_vel": pin((nw, 3, 3))}
+    if na:
+        io.update({"atom_pos": pin((na, 3)), "atom_vel": pin((na, 3))})
+    for k in io:
+        io[k][:] = s0[k][:len(io[k])]
     n_e2e = max(20, args.steps // 5)
-    st.step_host(DT, 1, {"water_pos": wp_in, "water_vel": wv_in}, {"water_pos": wp_out, "water_vel": wv_out})
+    st.step_host(DT, 1, io, io)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for _ in range(n_e2e):
-        st.step_host(DT, 1, {"water_pos": wp_out, "water_vel": wv_out},
-                     {"water_pos": wp_out, "water_vel": wv_out})
+        st.step_host(DT, 1, io, io)
     t_e2e = time.perf_counter() - t0
+    io_bytes = int(sum(a.nbytes for a in io.values()))
     e2e_value = n_e2e * DT * 1e-3 * world / t_e2e * 86400.0
     # kernels in the timed region: every step's fixed set, plus the rebuild
     # and periodic-task kernels on the steps whose conditional nodes fired
@@ -457,7 +501,8 @@ def run_ours(args):
     s0 = e_before["step"]
     due = sum(1 for t in range(s0 + 1, s0 + args.steps + 1)
               if (cfg.zero_com_drift and t % cfg.com_removal_interval == 0)
-              or (cfg.reset_angle and t % 1000 == 0))
+              or (cfg.reset_angle and t % 1000 == 0)
+              or (cfg.recenter_sim_box and na and t % 30 == 0))
     launches = ((st.launches_per_step(True) + st.launches_per_step(False)) / 2.0 * args.steps
                 + rebuilds * n_rebuild_k + due * n_periodic_k)
     clk = clocks.summary(local)
@@ -474,13 +519,15 @@ def run_ours(args):
     except Exception:
         pass
     hbm = peaks.get("hbm_gbs")
-    cpu = cpu_baseline(name, args) if (world == 1 and not args.no_cpu) else None
+    cpu = cpu_baseline(name, args, sysd) if (world == 1 and not args.no_cpu) else None
     out = {
         "metric": "ns/day", "value": round(value, 2), "unit": "ns/day", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded OPC water lattice, equilibrated on device)",
-        "config": {"workload": name, "n_water": w["n_water"], "atoms": 4 * w["n_water"],
+        "data": "synthetic (seeded ff19SB peptide / ions / OPC water, equilibrated on device)"
+                if w.get("n_res") else "synthetic (seeded OPC water lattice, equilibrated on device)",
+        "config": {"workload": name, "n_water": st_nw, "atoms": 4 * st_nw + st_na,
+                   "peptide_residues": list(w.get("n_res", ())), "nacl_molar": w.get("nacl", 0.0),
                    "box_A": w["box"], "cutoff_A": w["cutoff"], "spme_grid": list(w["grid"]),
                    "spme_interval": cfg.spme_interval, "dt_fs": DT * 1e3,
                    "integrator": w["integrator"], "barostat": w["barostat"],
@@ -497,8 +544,7 @@ def run_ours(args):
                           "note": "whole SPME stage incl. cuFFT; grid is L2-resident"},
         "stage_ms": {k: round(v, 5) for k, v in stages.items()},
         "e2e": {"value": round(e2e_value, 2), "unit": "ns/day",
-                "h2d_bytes_per_step": int(wp_in.nbytes + wv_in.nbytes),
-                "d2h_bytes_per_step": int(wp_out.nbytes + wv_out.nbytes + 256)},
+                "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes + 256},
         "gpu_launches": int(round(launches)),
         "clocks": clk,
         "cpu_baseline": cpu,
@@ -511,16 +557,56 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def cpu_baseline(name, args):
-    """The C++ restatement of the reference CPU path on a bounded sample."""
+def cpu_baseline(name, args, sysd=None):
+    """The C++ restatement of the reference CPU path on a bounded sample of
+    the same system."""
     try:
         from oracle import cpu_ref
     except ImportError:
         return None
     try:
-        return cpu_ref.run_sample(WORKLOADS[name], name, seconds=args.cpu_seconds)
+        return cpu_ref.run_sample(WORKLOADS[name], name, seconds=args.cpu_seconds, sysd=sysd)
     except Exception as e:  # the baseline is reported, never required
         return {"error": str(e)[:200]}
+
+
+def run_reference_members(args, name):
+    """Reference arm of the batched and serving workloads: the CPU
+    restatement steps every member system one after another (the reference
+    advances one MdState per call), each on a bounded sample."""
+    from oracle import cpu_ref
+    w = WORKLOADS[name]
+    if w["kind"] == "batch":
+        systems, _ = build_batch(name, seed=1)
+        steps_each = 1
+    else:
+        from dynamics_b200 import synth
+        sizes = synth.config4_sizes(w["n_req"], seed=7)
+        systems = [synth.batch_member(int(n), seed=7000 + i)[0] for i, n in enumerate(sizes)]
+        steps_each = w["steps_each"]
+    per = max(0.5, args.cpu_seconds / len(systems))
+    sec_per_step = 0.0
+    cores = None
+    for i, sysd in enumerate(systems):
+        box = float(sysd["box_hi"][0])
+        from dynamics_b200 import synth
+        k = synth.fft_size(int(np.ceil(box)))
+        wl = dict(n_water=len(sysd["water_pos"]), box=box, cutoff=w["cutoff"], grid=(k, k, k),
+                  integrator=w["integrator"])
+        res = cpu_ref.run_sample(wl, f"{name}[{i}]", seconds=per, steps=100000, warmup=1, sysd=sysd)
+        sec_per_step += DT * 1e-3 * 86400.0 / res["value"]   # seconds per step of this member
+        cores = res["cores"]
+    value = len(systems) * DT * 1e-3 / sec_per_step * 86400.0
+    cpu = {"value": round(value, 4), "unit": "ns/day (aggregate)", "cores": cores, "kind": "port",
+           "sample": f"each of {len(systems)} members timed alone for ~{per:.1f} s, stepped one after another"}
+    out = {"impl": "reference", "metric": "ns/day", "value": cpu["value"], "unit": cpu["unit"],
+           "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "config": {"workload": name, "members": len(systems),
+                                           "steps_each": steps_each},
+           "cpu_baseline": cpu,
+           "e2e": {"value": cpu["value"], "unit": cpu["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
 
 
 def run_reference(args):
@@ -529,13 +615,17 @@ def run_reference(args):
         return
     from oracle import cpu_ref
     name = args.workload
+    if WORKLOADS[name].get("kind") in ("batch", "serve"):
+        run_reference_members(args, name)
+        return
+    sysd, _ = build_system(name, seed=1000)
     res = cpu_ref.run_sample(WORKLOADS[name], name, seconds=args.cpu_seconds, steps=args.steps,
-                             warmup=args.warmup)
+                             warmup=args.warmup, sysd=sysd)
     out = {"impl": "reference", "metric": "ns/day", "value": res["value"], "unit": "ns/day",
            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": res.get("steps"),
            "warmup": res.get("warmup"), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": name, "n_water": WORKLOADS[name]["n_water"]},
+           "config": {"workload": name, "n_water": len(sysd["water_pos"]), "atoms": len(sysd["atom_pos"])},
            "cpu_baseline": res,
            "e2e": {"value": res["value"], "unit": "ns/day", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}

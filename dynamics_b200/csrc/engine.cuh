@@ -100,6 +100,7 @@ struct SysView {
     uint32_t* ex_off; uint32_t* ex_idx;
     // columns
     uint32_t ncx, ncy, ncol;
+    uint32_t ancx, ancy, ancol;   // a finer column grid for non-water atoms
     uint32_t* col_count; uint32_t* col_off; uint32_t* col_fill;   // [ncol(+1)]
     uint32_t* col_boff;                         // unpadded bucket offsets [ncol+1]
     uint32_t* acol_count; uint32_t* acol_off; uint32_t* acol_fill; uint32_t* acol_boff;
@@ -294,6 +295,7 @@ int pair_blocks_ww(const SysView& v);
 int pair_ww_setup(const SysView& v);
 int ww_tile_blocks(const SysView& v);
 int pair_blocks_ss(const SysView& v);
+int pair_blocks_sw(const SysView& v);
 int pair14_blocks(const SysView& v);
 
 // pme.cu

@@ -99,11 +99,10 @@ DYN_KERNEL(, k_col_clear, (, bool force), (, force)) {
         v.sc->list_pairs = 0ull;
         v.sc->union_max = 0u;
     }
-    for (uint32_t c = bk.idx * blockDim.x + threadIdx.x; c <= v.ncol; c += bk.cnt * blockDim.x) {
-        if (c < v.ncol) {
-            v.col_count[c] = 0; v.col_fill[c] = 0;
-            v.acol_count[c] = 0; v.acol_fill[c] = 0;
-        }
+    const uint32_t nc = v.ncol > v.ancol ? v.ncol : v.ancol;
+    for (uint32_t c = bk.idx * blockDim.x + threadIdx.x; c < nc; c += bk.cnt * blockDim.x) {
+        if (c < v.ncol) { v.col_count[c] = 0; v.col_fill[c] = 0; }
+        if (c < v.ancol) { v.acol_count[c] = 0; v.acol_fill[c] = 0; }
     }
 }
 
@@ -122,7 +121,7 @@ DYN_KERNEL(, k_col_assign, (, bool force), (, force)) {
     }
     for (uint32_t a = tid; a < v.na; a += stride) {
         float zf;
-        const uint32_t c = column_of(xyz(v.apos[a]), b, v.ncx, v.ncy, &zf);
+        const uint32_t c = column_of(xyz(v.apos[a]), b, v.ancx, v.ancy, &zf);
         v.acol[a] = c;
         v.akey[a] = zf;
         atomicAdd(&v.acol_count[c], 1u);
@@ -143,11 +142,11 @@ DYN_KERNEL(, k_col_scan, (, bool force), (, force)) {
         v.sc->n_wclus = (q + WCL - 1) / WCL;
     } else if (threadIdx.x == 32) {
         uint32_t q = 0;
-        for (uint32_t c = 0; c < v.ncol; ++c) {
+        for (uint32_t c = 0; c < v.ancol; ++c) {
             v.acol_off[c] = q; v.acol_boff[c] = q;
             q += v.acol_count[c];
         }
-        v.acol_off[v.ncol] = q; v.acol_boff[v.ncol] = q;
+        v.acol_off[v.ancol] = q; v.acol_boff[v.ancol] = q;
         v.sc->n_aclus = (q + ACL - 1) / ACL;
     }
 }
@@ -540,10 +539,15 @@ DYN_KERNEL(, k_rebuild_done, (, bool force), (, force)) {
     v.sc->rebuilds += 1ull;
 }
 
+// Copies positions into cluster order and zeroes the atoms' short-range
+// force accumulators (every pair kernel adds to them).
 DYN_KERNEL(, k_gather_atoms, (), ()) {
     for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.na_cap; s += bk.cnt * blockDim.x) {
         const uint32_t a = v.sidx[s];
-        if (a != INVALID_ID) v.spos[s] = v.apos[a];
+        if (a != INVALID_ID) {
+            v.spos[s] = v.apos[a];
+            v.aforce[3 * (size_t)a + 0] = 0; v.aforce[3 * (size_t)a + 1] = 0; v.aforce[3 * (size_t)a + 2] = 0;
+        }
     }
 }
 
@@ -565,7 +569,8 @@ void launch_displacement_check(const Target& t) {
 void launch_rebuild(const Target& t, bool force) {
     const int T = 256;
     auto nmax = [](const SysView& v) { return v.nw_cap > v.na_cap ? v.nw_cap : v.na_cap; };
-    t.launch(k_col_clear, k_col_clear_batch, [](const SysView& v) { return nblocks(v.ncol + 1, 256); }, T, 0, force);
+    t.launch(k_col_clear, k_col_clear_batch,
+             [](const SysView& v) { return nblocks((v.ncol > v.ancol ? v.ncol : v.ancol) + 1, 256); }, T, 0, force);
     t.launch(k_col_assign, k_col_assign_batch, [&](const SysView& v) { return nblocks(nmax(v), 256); }, T, 0, force);
     t.launch(k_col_scan, k_col_scan_batch, [](const SysView&) { return 1; }, 64, 0, force);
     t.launch(k_col_bucket, k_col_bucket_batch, [&](const SysView& v) { return nblocks(nmax(v), 256); }, T, 0, force);

@@ -26,6 +26,7 @@
 namespace {
 
 constexpr int PT = 128;  // threads per block (4 warps)
+constexpr uint32_t CH_MIX = 16;  // list entries per warp in the mixed kernels
 
 // e_lj, e_c accumulate per-pair energies in float64 (energy steps only);
 // w accumulates the virial in float32
@@ -298,12 +299,15 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ws, (), ()) 
     const int ii = lane & 7, jq = lane >> 3;
     const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nwc = v.sc->n_wclus;
+    const uint32_t nch = (v.cap_ws + CH_MIX - 1) / CH_MIX;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t ci = ((bk.idx * blockDim.x + threadIdx.x) >> 5); ci < nwc; ci += nwarps) {
-        const uint32_t n = v.ws_n[ci];
-        if (n == 0) continue;
+    // one warp per (i-cluster, chunk of CH_MIX list entries)
+    for (uint32_t wv = ((bk.idx * blockDim.x + threadIdx.x) >> 5); wv < nwc * nch; wv += nwarps) {
+        const uint32_t ci = wv / nch, k0 = (wv % nch) * CH_MIX;
+        const uint32_t n = min(v.ws_n[ci], k0 + CH_MIX);
+        if (n <= k0) continue;
         const uint32_t si = ci * WCL + ii;
         const bool vi = v.wid[si] != INVALID_ID;
         const float3 iO = xyz(v.wpos[4 * si + 0]), iH0 = xyz(v.wpos[4 * si + 1]);
@@ -311,7 +315,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ws, (), ()) 
         float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
         Acc3 a{0.0, 0.0, 0.f};
         const uint32_t* lst = v.ws_j + (size_t)ci * v.cap_ws;
-        for (uint32_t k = 0; k < n; ++k) {
+        for (uint32_t k = k0; k < n; ++k) {
             const uint32_t cj = lst[k];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -351,12 +355,14 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_sw, (), ()) 
     const int ii = lane & 7, jq = lane >> 3;
     const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nac = v.sc->n_aclus;
+    const uint32_t nch = (v.cap_sw + CH_MIX - 1) / CH_MIX;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t ci = ((bk.idx * blockDim.x + threadIdx.x) >> 5); ci < nac; ci += nwarps) {
-        const uint32_t n = v.sw_n[ci];
-        if (n == 0) continue;
+    for (uint32_t wv = ((bk.idx * blockDim.x + threadIdx.x) >> 5); wv < nac * nch; wv += nwarps) {
+        const uint32_t ci = wv / nch, k0 = (wv % nch) * CH_MIX;
+        const uint32_t n = min(v.sw_n[ci], k0 + CH_MIX);
+        if (n <= k0) continue;
         const uint32_t si = ci * ACL + ii;
         const uint32_t ai = v.sidx[si];
         const bool vi = ai != INVALID_ID;
@@ -367,7 +373,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_sw, (), ()) 
         float3 f = f3(0, 0, 0);
         Acc3 a{0.0, 0.0, 0.f};
         const uint32_t* lst = v.sw_j + (size_t)ci * v.cap_sw;
-        for (uint32_t k = 0; k < n; ++k) {
+        for (uint32_t k = k0; k < n; ++k) {
             const uint32_t cj = lst[k];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -398,20 +404,23 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) 
     const int ii = lane & 7, jq = lane >> 3;
     const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nac = v.sc->n_aclus;
+    const uint32_t nch = (v.cap_ss + CH_MIX - 1) / CH_MIX;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t ci = ((bk.idx * blockDim.x + threadIdx.x) >> 5); ci < nac; ci += nwarps) {
+    for (uint32_t wv = ((bk.idx * blockDim.x + threadIdx.x) >> 5); wv < nac * nch; wv += nwarps) {
+        const uint32_t ci = wv / nch, k0 = (wv % nch) * CH_MIX;
+        const uint32_t n = min(v.ss_n[ci], k0 + CH_MIX);
+        if (n <= k0) continue;
         const uint32_t si = ci * ACL + ii;
         const uint32_t ai = v.sidx[si];
         const float4 pi = v.spos[si];
         const float2 lji = v.slj[si];
         float3 f = f3(0, 0, 0);
         Acc3 a{0.0, 0.0, 0.f};
-        const uint32_t n = v.ss_n[ci];
         const uint32_t* lst = v.ss_j + (size_t)ci * v.cap_ss;
         const unsigned long long* msk = v.ss_mask + (size_t)ci * v.cap_ss;
-        for (uint32_t k = 0; k < n; ++k) {
+        for (uint32_t k = k0; k < n; ++k) {
             const uint32_t cj = lst[k];
             const unsigned long long m = msk[k];
 #pragma unroll
@@ -428,7 +437,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) 
             }
         }
         f = f3(red4(f.x), red4(f.y), red4(f.z));
-        if (jq == 0 && ai != INVALID_ID) store_fix3(v.aforce + 3 * (size_t)ai, f);
+        if (jq == 0 && ai != INVALID_ID) add_fix3(v.aforce + 3 * (size_t)ai, f);
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
     }
@@ -472,7 +481,8 @@ inline int pblocks(const SysView& v, uint64_t warps) {
 
 namespace dyn {
 
-int pair_blocks_ww(const SysView& v) { return pblocks(v, v.nwclus_cap); }
+int pair_blocks_ww(const SysView& v) { return pblocks(v, (uint64_t)v.nwclus_cap * ((v.cap_ws + CH_MIX - 1) / CH_MIX)); }
+int pair_blocks_sw(const SysView& v) { return pblocks(v, (uint64_t)v.naclus_cap * ((v.cap_sw + CH_MIX - 1) / CH_MIX)); }
 
 int ww_tile_blocks(const SysView& v) {
     return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
@@ -498,7 +508,7 @@ int pair_ww_setup(const SysView& v) {
     }
     return DYN_OK;
 }
-int pair_blocks_ss(const SysView& v) { return pblocks(v, v.naclus_cap); }
+int pair_blocks_ss(const SysView& v) { return pblocks(v, (uint64_t)v.naclus_cap * ((v.cap_ss + CH_MIX - 1) / CH_MIX)); }
 int pair14_blocks(const SysView& v) {
     uint64_t bl = (v.n14 + 255) / 256;
     if (bl < 1) bl = 1;
@@ -515,9 +525,9 @@ void launch_pairs(const Target& t, bool energy) {
              [&](const SysView& v) { return v.nw && eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
     t.launch(k_pair_ww_tile<false>, k_pair_ww_tile_batch<false>,
              [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
-    auto ss = [](const SysView& v) { return v.na ? pblocks(v, v.naclus_cap) : 0; };
-    auto ws = [](const SysView& v) { return v.nw && v.na ? pblocks(v, v.nwclus_cap) : 0; };
-    auto sw = [](const SysView& v) { return v.nw && v.na ? pblocks(v, v.naclus_cap) : 0; };
+    auto ss = [](const SysView& v) { return v.na ? (int)v.nb[REG_SS] : 0; };
+    auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
+    auto sw = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_SW] : 0; };
     if (energy) {
         t.launch(k_pair_ss<true>, k_pair_ss_batch<true>, ss, PT, 0);
         t.launch(k_pair_ws<true>, k_pair_ws_batch<true>, ws, PT, 0);

@@ -82,7 +82,7 @@ void set_block_counts(SysView& v) {
     for (int r = 0; r < NREGION; ++r) v.nb[r] = 0;
     v.nb[REG_WW] = v.nw ? dyn::ww_tile_blocks(v) : 0;
     v.nb[REG_WS] = (v.nw && v.na) ? dyn::pair_blocks_ww(v) : 0;
-    v.nb[REG_SW] = (v.nw && v.na) ? dyn::pair_blocks_ss(v) : 0;
+    v.nb[REG_SW] = (v.nw && v.na) ? dyn::pair_blocks_sw(v) : 0;
     v.nb[REG_SS] = v.na ? dyn::pair_blocks_ss(v) : 0;
     v.nb[REG_14] = v.n14 ? dyn::pair14_blocks(v) : 0;
     v.nb[REG_BOND] = (v.nbond + v.nangle + v.ndih) ? dyn::bond_blocks(v) : 0;
@@ -381,6 +381,11 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     v.ncx = std::max(1u, (uint32_t)std::floor(ext[0] / edge));
     v.ncy = std::max(1u, (uint32_t)std::floor(ext[1] / edge));
     v.ncol = v.ncx * v.ncy;
+    // atoms (peptide density ~0.1 per A^3): columns about one 8-atom cube wide
+    const double aedge = std::cbrt(8.0 / 0.1);
+    v.ancx = std::min(1024u, std::max(1u, (uint32_t)std::floor(ext[0] / aedge)));
+    v.ancy = std::min(1024u, std::max(1u, (uint32_t)std::floor(ext[1] / aedge)));
+    v.ancol = v.ancx * v.ancy;
     // slots follow the column path without per-column padding; the tail is
     // padded to whole 32-water groups
     v.nw_cap = round_up(std::max(1u, v.nw), 2 * GRPW);
@@ -397,7 +402,7 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         return std::max(1u, std::min(e, ncl));
     };
     const double wcl_vol = v.nw ? vol / std::max(1.0, v.nw / 8.0) : vol;
-    const double acl_vol = std::max(8.0 / 0.12, v.na ? 8.0 * vol / std::max(1u, v.nw * 4 + v.na) * 4.0 : vol);
+    const double acl_vol = 8.0 / 0.1;  // clusters of a dense solute; ions are few
     // water-water: 32-water groups; candidate clusters within r_ww of the
     // group box; the union of needed waters; molecule lists within r_ww
     // (liquid density as the bound)
@@ -456,9 +461,15 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         cheb_poly<NPOLY_G>(g, (double)v.rc * (double)v.rc, v.poly_g);
         v.two_over_rc2 = (float)(2.0 / ((double)v.rc * (double)v.rc));
     }
-    v.cap_ws = (v.nw && v.na) ? est(v.r_ws, acl_vol, v.naclus_cap) : 1;
-    v.cap_sw = (v.nw && v.na) ? est(v.r_ws, wcl_vol, v.nwclus_cap) : 1;
-    v.cap_ss = v.na ? est(v.r_ss, acl_vol, v.naclus_cap) : 1;
+    // mixed lists: every cluster while that stays small (sparse atoms such as
+    // ions form clusters with wide bounding boxes), else the estimate
+    auto cap_mixed = [&](double r, double vol_cl, uint32_t n_i, uint32_t n_j) -> uint32_t {
+        if ((uint64_t)n_i * n_j <= (1ull << 24)) return std::max(1u, n_j);
+        return est(r, vol_cl, n_j);
+    };
+    v.cap_ws = (v.nw && v.na) ? cap_mixed(v.r_ws, acl_vol, v.nwclus_cap, v.naclus_cap) : 1;
+    v.cap_sw = (v.nw && v.na) ? cap_mixed(v.r_ws, wcl_vol, v.naclus_cap, v.nwclus_cap) : 1;
+    v.cap_ss = v.na ? cap_mixed(v.r_ss, acl_vol, v.naclus_cap, v.naclus_cap) : 1;
 
     // ---- allocations ----
     TRY(dev_alloc(h, &v.wpos, 4 * (size_t)v.nw_cap));
@@ -495,10 +506,10 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dev_alloc(h, &v.col_off, v.ncol + 1));
     TRY(dev_alloc(h, &v.col_fill, v.ncol + 1));
     TRY(dev_alloc(h, &v.col_boff, v.ncol + 1));
-    TRY(dev_alloc(h, &v.acol_count, v.ncol + 1));
-    TRY(dev_alloc(h, &v.acol_off, v.ncol + 1));
-    TRY(dev_alloc(h, &v.acol_fill, v.ncol + 1));
-    TRY(dev_alloc(h, &v.acol_boff, v.ncol + 1));
+    TRY(dev_alloc(h, &v.acol_count, v.ancol + 1));
+    TRY(dev_alloc(h, &v.acol_off, v.ancol + 1));
+    TRY(dev_alloc(h, &v.acol_fill, v.ancol + 1));
+    TRY(dev_alloc(h, &v.acol_boff, v.ancol + 1));
     TRY(dev_alloc(h, &v.wbb_c, v.nwclus_cap));
     TRY(dev_alloc(h, &v.wbb_h, v.nwclus_cap));
     TRY(dev_alloc(h, &v.abb_c, v.naclus_cap));

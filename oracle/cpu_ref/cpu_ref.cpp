@@ -4,7 +4,8 @@
 //
 // The reference (Rust crate `dynamics` 0.2.2) cannot be compiled here, so this
 // restates its CPU algorithm for one step, MdState::step
-// (src/integrate.rs:72-473), for rigid-water systems:
+// (src/integrate.rs:72-473), for rigid OPC water plus non-water atoms
+// (peptides, ions) with bonded terms and bond-to-H constraints:
 //   * neighbour lists: O(N^2) brute force, |min_image(d)|^2 < (rc + skin)^2,
 //     half lists mirrored, rows in parallel (src/neighbors.rs:102-281);
 //     rebuilt when the max O displacement since the last build reaches
@@ -18,6 +19,9 @@
 //     function, gather, k-space virial; the PME tables are rebuilt every step
 //     as regen_pme does (src/integrate.rs:192);
 //   * rigid water drift, serial (src/solvent/opc_settle.rs:107-198);
+//   * bonds, angles, dihedrals, serial (src/bonded.rs:23-135); the 1-4
+//     vacuum Coulomb correction after SPME (src/non_bonded.rs:763-790);
+//     lincs_hydrogens + rattle_hydrogens (src/bonded.rs:218-304);
 //   * Langevin-middle OU step, serial (src/thermostat.rs:308-362), or
 //     velocity Verlet + CSVR (src/thermostat.rs:258-304);
 //   * KE (src/thermostat.rs:46-84), pressure (src/barostat.rs:419-431),
@@ -32,6 +36,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <random>
 #include <vector>
@@ -87,22 +92,38 @@ struct Water {
     V3 fo, fh0, fh1, fm;       // forces
 };
 
-struct Pair {  // NonBondedPair (src/non_bonded.rs:219-232) for water-water
+struct Pair {  // NonBondedPair (src/non_bonded.rs:219-232)
     uint32_t i, j;
-    uint8_t s0, s1;  // 0 O, 1 M, 2 H0, 3 H1
-    uint8_t lj, coul;
+    uint8_t s0, s1;  // water sites 0 O, 1 M, 2 H0, 3 H1; 4 = a non-water atom
+    uint8_t lj, coul, scale14;
 };
+
+struct Atom {
+    V3 p, v, a, f;
+    float m, q, sig, eps;
+};
+struct Bond { uint32_t i, j; float k, r0; };
+struct Angle { uint32_t i, j, l; float k, t0; };
+struct Dihedral { uint32_t i, j, k, l; float kk, n, ph; };
+struct Constraint { uint32_t h, x; float r02, im; };  // heavy, hydrogen
 
 struct Sim {
     Box box;
     std::vector<Water> w;
+    std::vector<Atom> at;
+    std::vector<uint64_t> excl, p14;  // sorted keys i * 2^32 + j, i < j
+    std::vector<Bond> bonds;
+    std::vector<Angle> angles;
+    std::vector<Dihedral> dih;
+    std::vector<Constraint> cons;
+    double vir_cons = 0;
     float rc, lj_cutoff, alpha, skin;
     int grid[3];
     int integrator;  // 0 Langevin-middle, 1 VV + CSVR
     float gamma, temp, tau;
     uint64_t step = 0;
     std::vector<Pair> pairs;
-    std::vector<V3> o_last;
+    std::vector<V3> o_last, a_last;
     float max_disp2 = 0.f;
     // SPME cache (src/lib.rs:1296-1340)
     std::vector<V3> spme_f;
@@ -114,6 +135,11 @@ struct Sim {
 };
 
 V3 site_pos(const Water& w, int s) { return s == 0 ? w.o : s == 1 ? w.m : s == 2 ? w.h0 : w.h1; }
+
+inline uint64_t key(uint32_t a, uint32_t b) {
+    return a < b ? ((uint64_t)a << 32) | b : ((uint64_t)b << 32) | a;
+}
+inline bool has(const std::vector<uint64_t>& v, uint64_t k) { return std::binary_search(v.begin(), v.end(), k); }
 
 // ---------------------------------------------------------------- lists --
 void build_neighbors(Sim& S) {
@@ -130,26 +156,54 @@ void build_neighbors(Sim& S) {
             if (d.x * d.x + d.y * d.y + d.z * d.z < thr) half[i].push_back((uint32_t)j);
         }
     }
-    // setup_pairs water-water block: i0 < i1, sites O,M,H0,H1 x O,M,H0,H1
+    // non-water atoms: std-std (i < j) and std-water lists (src/neighbors.rs:180-281)
+    const int na = (int)S.at.size();
+    std::vector<std::vector<uint32_t>> ss(na), sw(na);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < na; ++i) {
+        const V3 pi = S.box.wrap(S.at[i].p);
+        for (int j = i + 1; j < na; ++j) {
+            const V3 d = S.box.min_image(pi - S.box.wrap(S.at[j].p));
+            if (dot(d, d) < thr) ss[i].push_back((uint32_t)j);
+        }
+        for (int j = 0; j < n; ++j) {
+            const V3 d = S.box.min_image(pi - o[j]);
+            if (dot(d, d) < thr) sw[i].push_back((uint32_t)j);
+        }
+    }
+    // setup_pairs order: std-std, std-water, water-water (src/non_bonded.rs:541-677);
+    // 1-2 / 1-3 pairs are left out, 1-4 pairs flagged
     S.pairs.clear();
+    for (int i = 0; i < na; ++i)
+        for (uint32_t j : ss[i]) {
+            const uint64_t k = key((uint32_t)i, j);
+            if (has(S.excl, k)) continue;
+            S.pairs.push_back({(uint32_t)i, j, 4, 4, 1, 1, (uint8_t)has(S.p14, k)});
+        }
+    for (int i = 0; i < na; ++i)
+        for (uint32_t j : sw[i])
+            for (uint8_t b = 0; b < 4; ++b) S.pairs.push_back({(uint32_t)i, j, 4, b, (uint8_t)(b == 0), (uint8_t)(b != 0), 0});
     for (int i = 0; i < n; ++i)
         for (uint32_t j : half[i])
             for (uint8_t a = 0; a < 4; ++a)
                 for (uint8_t b = 0; b < 4; ++b) {
                     const bool lj = a == 0 && b == 0, co = a != 0 && b != 0;
                     if (!(lj || co)) continue;
-                    S.pairs.push_back({(uint32_t)i, j, a, b, (uint8_t)lj, (uint8_t)co});
+                    S.pairs.push_back({(uint32_t)i, j, a, b, (uint8_t)lj, (uint8_t)co, 0});
                 }
     S.o_last = o;
+    S.a_last.resize(na);
+    for (int i = 0; i < na; ++i) S.a_last[i] = S.at[i].p;
     S.max_disp2 = 0.f;
     S.rebuilds++;
 }
 
 // -------------------------------------------------------- pair forces --
 void pair_forces(Sim& S) {
-    const int n = (int)S.w.size();
+    const int n = (int)S.w.size(), na = (int)S.at.size();
+    const size_t nf = 12 * (size_t)n + 3 * (size_t)na;  // waters, then atoms
     const int nt = omp_get_max_threads();
-    std::vector<std::vector<double>> acc(nt, std::vector<double>(12 * (size_t)n, 0.0));
+    std::vector<std::vector<double>> acc(nt, std::vector<double>(nf, 0.0));
     std::vector<double> vir(nt, 0.0);
     const float rc = S.rc, a = S.alpha, ljc = S.lj_cutoff;
     const float q[4] = {0.f, Q_EP, Q_H, Q_H};
@@ -161,35 +215,49 @@ void pair_forces(Sim& S) {
 #pragma omp for schedule(static)
         for (long long p = 0; p < (long long)S.pairs.size(); ++p) {
             const Pair& pr = S.pairs[p];
-            const V3 d = S.box.min_image(site_pos(S.w[pr.i], pr.s0) - site_pos(S.w[pr.j], pr.s1));
+            const bool ai = pr.s0 == 4, aj = pr.s1 == 4;
+            const V3 pi = ai ? S.at[pr.i].p : site_pos(S.w[pr.i], pr.s0);
+            const V3 pj = aj ? S.at[pr.j].p : site_pos(S.w[pr.j], pr.s1);
+            const V3 d = S.box.min_image(pi - pj);
             const float r2 = dot(d, d);
             if (r2 < 1e-12f) continue;
             const float r = std::sqrt(r2);
             const float ir = 1.0f / r;
             const V3 dir = d * ir;
             float fm = 0.f;
-            if (pr.lj && r <= ljc) {
-                const float sr = O_SIGMA * ir, sr2 = sr * sr, sr4 = sr2 * sr2, sr6 = sr4 * sr2, sr12 = sr6 * sr6;
-                fm += 24.f * O_EPS * (2.f * sr12 - sr6) * ir;
+            float sig = O_SIGMA, eps = O_EPS;
+            if (ai || aj) {  // LjTables / combine_lj_params (src/non_bonded.rs:1081-1086)
+                const float si = ai ? S.at[pr.i].sig : O_SIGMA, ei = ai ? S.at[pr.i].eps : O_EPS;
+                const float sj = aj ? S.at[pr.j].sig : O_SIGMA, ej = aj ? S.at[pr.j].eps : O_EPS;
+                sig = 0.5f * (si + sj);
+                eps = std::sqrt(ei * ej);
             }
-            if (pr.coul && r < rc) {
+            if (pr.lj && r <= ljc && eps != 0.f) {
+                const float sr = sig * ir, sr2 = sr * sr, sr4 = sr2 * sr2, sr6 = sr4 * sr2, sr12 = sr6 * sr6;
+                float fl = 24.f * eps * (2.f * sr12 - sr6) * ir;
+                if (pr.scale14) fl *= 0.5f;
+                fm += fl;
+            }
+            const float qi = ai ? S.at[pr.i].q : q[pr.s0], qj = aj ? S.at[pr.j].q : q[pr.s1];
+            if (pr.coul && r < rc && qi * qj != 0.f) {
                 const float ar = a * r;
-                const float qq = q[pr.s0] * q[pr.s1];
-                fm += qq * (std::erfc(ar) * ir * ir + 2.f * a * std::exp(-ar * ar) * INV_SQRT_PI * ir);
+                float fc = qi * qj * (std::erfc(ar) * ir * ir + 2.f * a * std::exp(-ar * ar) * INV_SQRT_PI * ir);
+                if (pr.scale14) fc *= 1.0f / 1.2f;
+                fm += fc;
             }
             const V3 f = dir * fm;
             w_acc += (double)dot(d, f);
-            double* fi = F + 12 * (size_t)pr.i + 3 * pr.s0;
-            double* fj = F + 12 * (size_t)pr.j + 3 * pr.s1;
+            double* fi = ai ? F + 12 * (size_t)n + 3 * (size_t)pr.i : F + 12 * (size_t)pr.i + 3 * pr.s0;
+            double* fj = aj ? F + 12 * (size_t)n + 3 * (size_t)pr.j : F + 12 * (size_t)pr.j + 3 * pr.s1;
             fi[0] += f.x; fi[1] += f.y; fi[2] += f.z;
             fj[0] -= f.x; fj[1] -= f.y; fj[2] -= f.z;
         }
         vir[t] = w_acc;
     }
     // reduce (src/non_bonded.rs:373-411)
-    std::vector<double> tot(12 * (size_t)n, 0.0);
+    std::vector<double> tot(nf, 0.0);
 #pragma omp parallel for schedule(static)
-    for (long long k = 0; k < 12LL * n; ++k) {
+    for (long long k = 0; k < (long long)nf; ++k) {
         double s = 0;
         for (int t = 0; t < nt; ++t) s += acc[t][k];
         tot[k] = s;
@@ -204,6 +272,57 @@ void pair_forces(Sim& S) {
         w.fh0 = w.fh0 + V3{(float)f[6], (float)f[7], (float)f[8]};
         w.fh1 = w.fh1 + V3{(float)f[9], (float)f[10], (float)f[11]};
     }
+    for (int i = 0; i < na; ++i) {
+        const double* f = &tot[12 * (size_t)n + 3 * (size_t)i];
+        S.at[i].f = S.at[i].f + V3{(float)f[0], (float)f[1], (float)f[2]};
+    }
+}
+
+// ------------------------------------------------------------- bonded --
+// apply_bonded_forces (src/bonded.rs:23-135), f_bond_stretching /
+// f_angle_bending / f_dihedral (src/bonded_forces.rs:11-178), serial
+void bonded_forces(Sim& S) {
+    auto& A = S.at;
+    double vir = 0;
+    for (const Bond& b : S.bonds) {
+        const V3 d = S.box.min_image(A[b.j].p - A[b.i].p);
+        const float r = std::sqrt(dot(d, d));
+        const V3 f = d * (2.f * b.k * (r - b.r0) / std::max(r, 1e-8f));
+        A[b.i].f = A[b.i].f + f;
+        A[b.j].f = A[b.j].f - f;
+        vir += dot(d, f);
+    }
+    for (const Angle& g : S.angles) {
+        const V3 v01 = S.box.min_image(A[g.i].p - A[g.j].p), v21 = S.box.min_image(A[g.l].p - A[g.j].p);
+        const float l01 = std::sqrt(dot(v01, v01)), l21 = std::sqrt(dot(v21, v21));
+        if (l01 < 1e-4f || l21 < 1e-4f) continue;
+        const V3 u01 = v01 * (1.f / l01), u21 = v21 * (1.f / l21);
+        const float ct = std::min(1.f, std::max(-1.f, dot(u01, u21)));
+        const float st = std::max(std::sqrt(1.f - ct * ct), 1e-8f);
+        const float de = 2.f * g.k * (std::acos(ct) - g.t0);
+        const V3 f0 = (u01 * ct - u21) * (-de / (l01 * st));
+        const V3 f2 = (u21 * ct - u01) * (-de / (l21 * st));
+        A[g.i].f = A[g.i].f + f0;
+        A[g.l].f = A[g.l].f + f2;
+        A[g.j].f = A[g.j].f - f0 - f2;
+        vir += dot(v01, f0) + dot(v21, f2);
+    }
+    for (const Dihedral& q : S.dih) {
+        const V3 b1 = S.box.min_image(A[q.j].p - A[q.i].p), b2 = S.box.min_image(A[q.k].p - A[q.j].p),
+                 b3 = S.box.min_image(A[q.l].p - A[q.k].p);
+        const V3 n1 = cross(b1, b2), n2 = cross(b2, b3);
+        const float n1s = dot(n1, n1), n2s = dot(n2, n2), b2s = dot(b2, b2), b2n = std::sqrt(b2s);
+        if (n1s < 1e-6f || n2s < 1e-6f || b2n < 1e-6f) continue;
+        const float phi = std::atan2(dot(cross(n1, n2), b2) / b2n, dot(n1, n2));
+        const float dv = -q.kk * q.n * std::sin(q.n * phi - q.ph);
+        const V3 g0 = n1 * (-b2n / n1s), g3 = n2 * (b2n / n2s);
+        const float ta = dot(b1, b2) / b2s, tb = dot(b3, b2) / b2s;
+        const V3 g1 = g0 * (-1.f - ta) + g3 * tb, g2 = g3 * (-1.f - tb) + g0 * ta;
+        A[q.i].f = A[q.i].f + g0 * (-dv); A[q.j].f = A[q.j].f + g1 * (-dv);
+        A[q.k].f = A[q.k].f + g2 * (-dv); A[q.l].f = A[q.l].f + g3 * (-dv);
+        vir += dot(b1 * -1.f, g0 * (-dv)) + dot(b2, g2 * (-dv)) + dot(b2 + b3, g3 * (-dv));
+    }
+    S.virial += vir;
 }
 
 // ---------------------------------------------------------------- FFT --
@@ -287,9 +406,10 @@ void spme(Sim& S) {
             bm[a][m] = 1.0 / (re * re + im * im);
         }
     }
-    // pack_pme_pos_q (src/non_bonded.rs:800-826): M, H0, H1 per water
-    const int n = (int)S.w.size();
-    const int nq = 3 * n;
+    // pack_pme_pos_q (src/non_bonded.rs:800-826): M, H0, H1 per water,
+    // then the atoms
+    const int n = (int)S.w.size(), na = (int)S.at.size();
+    const int nq = 3 * n + na;
     std::vector<V3> pos(nq);
     std::vector<float> q(nq);
     for (int i = 0; i < n; ++i) {
@@ -297,6 +417,7 @@ void spme(Sim& S) {
         pos[3 * i + 1] = S.box.wrap(S.w[i].h0); q[3 * i + 1] = Q_H;
         pos[3 * i + 2] = S.box.wrap(S.w[i].h1); q[3 * i + 2] = Q_H;
     }
+    for (int i = 0; i < na; ++i) { pos[3 * n + i] = S.box.wrap(S.at[i].p); q[3 * n + i] = S.at[i].q; }
     std::vector<cd> grid(ng, 0.0);
     std::vector<int> base(3 * (size_t)nq);
     std::vector<double> th(12 * (size_t)nq), dth(12 * (size_t)nq);
@@ -370,6 +491,17 @@ void spme(Sim& S) {
     for (int i = 0; i < nq; ++i) qs += (double)q[i] * q[i];
     S.spme_e = e - S.alpha / std::sqrt(M_PI) * qs;
     S.spme_w = w;
+    // 1-4 vacuum Coulomb correction, cached with the SPME forces
+    // (src/non_bonded.rs:763-790)
+    for (const uint64_t k : S.p14) {
+        const uint32_t i = (uint32_t)(k >> 32), j = (uint32_t)(k & 0xFFFFFFFFu);
+        const V3 d = S.box.min_image(S.at[i].p - S.at[j].p);
+        const float r = std::sqrt(dot(d, d));
+        if (r < 1e-6f) continue;
+        const V3 df = d * (S.at[i].q * S.at[j].q / (r * r * r) * (1.0f / 1.2f - 1.0f));
+        S.spme_f[3 * n + i] = S.spme_f[3 * n + i] + df;
+        S.spme_f[3 * n + j] = S.spme_f[3 * n + j] - df;
+    }
 }
 
 // -------------------------------------------------------- rigid water --
@@ -426,11 +558,13 @@ double kinetic(const Sim& S) {  // src/thermostat.rs:46-64
     double k = 0;
     for (const Water& w : S.w)
         k += (double)(O_MASS * dot(w.vo, w.vo)) + (double)(H_MASS * dot(w.vh0, w.vh0)) + (double)(H_MASS * dot(w.vh1, w.vh1));
+    for (const Atom& a : S.at) k += (double)(a.m * dot(a.v, a.v));
     return k * 0.5 / KCAL_TO_NATIVE;
 }
 
 double kinetic_trans(const Sim& S) {
     double k = 0;
+    for (const Atom& a : S.at) k += (double)(a.m * dot(a.v, a.v));
     for (const Water& w : S.w) {
         const V3 vc = (w.vo * O_MASS + w.vh0 * H_MASS + w.vh1 * H_MASS) * (1.0f / MASS_MOL);
         k += (double)(MASS_MOL * dot(vc, vc));
@@ -440,14 +574,56 @@ double kinetic_trans(const Sim& S) {
 
 void all_forces(Sim& S) {
     for (Water& w : S.w) w.fo = w.fh0 = w.fh1 = w.fm = V3{0, 0, 0};
+    for (Atom& a : S.at) a.f = V3{0, 0, 0};
     pair_forces(S);
+    bonded_forces(S);
     if (S.step % 2 == 0) spme(S);  // SPME_RATIO (src/lib.rs:208)
-    for (size_t i = 0; i < S.w.size(); ++i) {
+    const size_t n = S.w.size();
+    for (size_t i = 0; i < n; ++i) {
         S.w[i].fm = S.w[i].fm + S.spme_f[3 * i];
         S.w[i].fh0 = S.w[i].fh0 + S.spme_f[3 * i + 1];
         S.w[i].fh1 = S.w[i].fh1 + S.spme_f[3 * i + 2];
     }
+    for (size_t i = 0; i < S.at.size(); ++i) S.at[i].f = S.at[i].f + S.spme_f[3 * n + i];
     S.pe = S.spme_e;
+}
+
+// lincs_hydrogens (src/bonded.rs:218-284), order 4, iter 1, sequential
+void lincs(Sim& S, float dt) {
+    if (S.cons.empty()) return;
+    std::vector<V3> x0(S.at.size());
+    for (size_t i = 0; i < S.at.size(); ++i) x0[i] = S.at[i].p;
+    for (int o = 0; o < 4; ++o)
+        for (const Constraint& c : S.cons) {
+            Atom &ai = S.at[c.h], &aj = S.at[c.x];
+            const V3 d = aj.p - ai.p;
+            const float dl = std::max(std::sqrt(dot(d, d)), 1.1920929e-7f);
+            const V3 b = d * (1.f / dl);
+            const V3 corr = b * ((std::sqrt(c.r02) - dot(b, d)) / c.im);
+            ai.p = ai.p - corr * (1.f / ai.m);
+            aj.p = aj.p + corr * (1.f / aj.m);
+        }
+    for (const Constraint& c : S.cons) {
+        Atom &ai = S.at[c.h], &aj = S.at[c.x];
+        const V3 d = aj.p - ai.p;
+        const float d2 = dot(d, d);
+        const V3 corr = d * ((d2 - c.r02) / (2.f * c.im * std::max(d2, 1e-8f)));
+        ai.p = ai.p + corr * (1.f / ai.m);
+        aj.p = aj.p - corr * (1.f / aj.m);
+    }
+    const float inv = 1.f / (dt * dt);
+    for (const Constraint& c : S.cons)
+        S.vir_cons += dot(S.box.min_image(S.at[c.x].p - S.at[c.h].p), (S.at[c.h].p - x0[c.h]) * (S.at[c.h].m * inv));
+}
+
+void rattle(Sim& S) {  // rattle_hydrogens (src/bonded.rs:288-304)
+    for (const Constraint& c : S.cons) {
+        Atom &ai = S.at[c.h], &aj = S.at[c.x];
+        const V3 r = aj.p - ai.p;
+        const V3 corr = r * (dot(aj.v - ai.v, r) / (c.im * std::max(dot(r, r), 1e-8f)));
+        ai.v = ai.v + corr * (1.f / ai.m);
+        aj.v = aj.v - corr * (1.f / aj.m);
+    }
 }
 
 void kick_calc_accel(Sim& S, float dt) {  // src/integrate.rs:515-562
@@ -456,16 +632,27 @@ void kick_calc_accel(Sim& S, float dt) {  // src/integrate.rs:515-562
         w.ao = w.fo * (KCAL_TO_NATIVE / O_MASS); w.ah0 = w.fh0 * (KCAL_TO_NATIVE / H_MASS); w.ah1 = w.fh1 * (KCAL_TO_NATIVE / H_MASS);
         w.vo = w.vo + w.ao * dt; w.vh0 = w.vh0 + w.ah0 * dt; w.vh1 = w.vh1 + w.ah1 * dt;
     }
+    for (Atom& a : S.at) {
+        a.a = a.f * (KCAL_TO_NATIVE / a.m);
+        const float a2 = dot(a.a, a.a);
+        if (a2 > 1e10f) a.a = a.a * (1e5f / std::sqrt(a2));  // MAX_ACCEL (src/integrate.rs:26-27)
+        a.v = a.v + a.a * dt;
+    }
+    rattle(S);
     S.ke = kinetic(S);
 }
 
 void step(Sim& S, float dt) {
     const float hdt = 0.5f * dt;
     if (S.integrator == 0) {
+        S.vir_cons = 0;
         for (Water& w : S.w) {  // kick_and_drift(dt/2, dt/2)
             w.vo = w.vo + w.ao * hdt; w.vh0 = w.vh0 + w.ah0 * hdt; w.vh1 = w.vh1 + w.ah1 * hdt;
             rigid(w, hdt, S.box);
         }
+        for (Atom& a : S.at) { a.v = a.v + a.a * hdt; a.p = a.p + a.v * hdt; }
+        lincs(S, hdt);
+        rattle(S);
         S.ke = kinetic(S);
         // apply_langevin_thermostat (src/thermostat.rs:308-362), serial
         const float c = std::exp(-S.gamma * dt);
@@ -476,22 +663,30 @@ void step(Sim& S, float dt) {
             w.vh0 = w.vh0 * c + V3{S.nd(S.rng), S.nd(S.rng), S.nd(S.rng)} * sh;
             w.vh1 = w.vh1 * c + V3{S.nd(S.rng), S.nd(S.rng), S.nd(S.rng)} * sh;
         }
+        for (Atom& a : S.at) a.v = a.v * c + V3{S.nd(S.rng), S.nd(S.rng), S.nd(S.rng)} * std::sqrt(num / a.m);
+        rattle(S);
         S.ke = kinetic(S);
         for (Water& w : S.w) rigid(w, hdt, S.box);  // drift(dt/2)
+        for (Atom& a : S.at) a.p = a.p + a.v * hdt;
+        { const double keep = S.vir_cons; lincs(S, hdt); S.vir_cons = keep; }
         all_forces(S);
         (void)((2.0 * kinetic_trans(S) + S.virial + S.spme_w) / (3.0 * S.box.volume()) * BAR);
         kick_calc_accel(S, hdt);
     } else {
+        S.vir_cons = 0;
         for (Water& w : S.w) {  // kick_and_drift(dt/2, dt)
             w.vo = w.vo + w.ao * hdt; w.vh0 = w.vh0 + w.ah0 * hdt; w.vh1 = w.vh1 + w.ah1 * hdt;
             rigid(w, dt, S.box);
         }
+        for (Atom& a : S.at) { a.v = a.v + a.a * hdt; a.p = a.p + a.v * dt; }
+        lincs(S, hdt);
+        rattle(S);
         S.ke = kinetic(S);
         all_forces(S);
         (void)((2.0 * kinetic_trans(S) + S.virial + S.spme_w) / (3.0 * S.box.volume()) * BAR);
         kick_calc_accel(S, hdt);
         // CSVR (src/thermostat.rs:258-304)
-        const double dof = 6.0 * S.w.size() - 3.0;
+        const double dof = 6.0 * S.w.size() + 3.0 * S.at.size() - (double)S.cons.size() - 3.0;
         const double ke = kinetic(S);
         const double c = std::exp(-dt / S.tau);
         std::normal_distribution<double> nd(0, 1);
@@ -501,6 +696,7 @@ void step(Sim& S, float dt) {
         double kp = ke * c + kt * (1 - c) * ((x + r * r) / dof) + 2 * r * std::sqrt(c * (1 - c) * ke * kt / dof);
         const float lam = (float)std::sqrt(std::max(kp, 1e-20) / ke);
         for (Water& w : S.w) { w.vo = w.vo * lam; w.vh0 = w.vh0 * lam; w.vh1 = w.vh1 * lam; }
+        for (Atom& a : S.at) a.v = a.v * lam;
         S.ke = kinetic(S);
     }
     S.step++;
@@ -510,12 +706,18 @@ void step(Sim& S, float dt) {
             const V3 q = w.vo * O_MASS + w.vh0 * H_MASS + w.vh1 * H_MASS;
             p[0] += q.x; p[1] += q.y; p[2] += q.z; m += MASS_MOL;
         }
+        for (const Atom& a : S.at) { p[0] += a.m * a.v.x; p[1] += a.m * a.v.y; p[2] += a.m * a.v.z; m += a.m; }
         const V3 vc{(float)(p[0] / m), (float)(p[1] / m), (float)(p[2] / m)};
         for (Water& w : S.w) { w.vo = w.vo - vc; w.vh0 = w.vh0 - vc; w.vh1 = w.vh1 - vc; }
+        for (Atom& a : S.at) a.v = a.v - vc;
     }
     // update_max_displacement_since_rebuild + build_neighbors_if_needed
     for (size_t i = 0; i < S.w.size(); ++i) {
         const V3 d = S.box.min_image(S.w[i].o - S.o_last[i]);
+        S.max_disp2 = std::max(S.max_disp2, dot(d, d));
+    }
+    for (size_t i = 0; i < S.at.size(); ++i) {
+        const V3 d = S.at[i].p - S.a_last[i];
         S.max_disp2 = std::max(S.max_disp2, dot(d, d));
     }
     if (S.max_disp2 >= (S.skin * 0.5f) * (S.skin * 0.5f)) build_neighbors(S);
@@ -553,6 +755,50 @@ int main(int argc, char** argv) {
     if (std::fread(wp.data(), 4, wp.size(), f) != wp.size() || std::fread(wv.data(), 4, wv.size(), f) != wv.size()) {
         std::fprintf(stderr, "short body\n");
         return 2;
+    }
+    // optional tail: int32 n_atoms; pos[3n], vel[3n], mass, q, sigma, eps [n];
+    // int32 n + pairs for exclusions and 1-4; int32 n + (i, j) + (k, r0)
+    // bonds; int32 n + (i, j, k) + (k, theta0) angles; int32 n + (i, j, k, l)
+    // + (k, n, phase) dihedrals; int32 n + (i, j) + r0 constraints
+    int32_t na = 0;
+    if (std::fread(&na, 4, 1, f) == 1 && na > 0) {
+        std::vector<float> ap(3 * (size_t)na), av(3 * (size_t)na), am(na), aq(na), as(na), ae(na);
+        bool ok = std::fread(ap.data(), 4, ap.size(), f) == ap.size() && std::fread(av.data(), 4, av.size(), f) == av.size() &&
+                  std::fread(am.data(), 4, na, f) == (size_t)na && std::fread(aq.data(), 4, na, f) == (size_t)na &&
+                  std::fread(as.data(), 4, na, f) == (size_t)na && std::fread(ae.data(), 4, na, f) == (size_t)na;
+        if (!ok) { std::fprintf(stderr, "short atoms\n"); return 2; }
+        S.at.resize(na);
+        for (int i = 0; i < na; ++i) {
+            Atom& a = S.at[i];
+            a.p = {ap[3 * i], ap[3 * i + 1], ap[3 * i + 2]};
+            a.v = {av[3 * i], av[3 * i + 1], av[3 * i + 2]};
+            a.a = a.f = V3{0, 0, 0};
+            a.m = am[i]; a.q = aq[i]; a.sig = as[i]; a.eps = ae[i];
+        }
+        auto rd_u = [&](std::vector<uint32_t>& v, size_t k) { v.resize(k); return std::fread(v.data(), 4, k, f) == k; };
+        auto rd_f = [&](std::vector<float>& v, size_t k) { v.resize(k); return std::fread(v.data(), 4, k, f) == k; };
+        int32_t m = 0;
+        std::vector<uint32_t> u;
+        std::vector<float> fl;
+        for (int pass = 0; pass < 2; ++pass) {
+            if (std::fread(&m, 4, 1, f) != 1 || !rd_u(u, 2 * (size_t)m)) { std::fprintf(stderr, "short pairs\n"); return 2; }
+            std::vector<uint64_t>& dst = pass == 0 ? S.excl : S.p14;
+            for (int k = 0; k < m; ++k) dst.push_back(key(u[2 * k], u[2 * k + 1]));
+            std::sort(dst.begin(), dst.end());
+        }
+        if (std::fread(&m, 4, 1, f) != 1 || !rd_u(u, 2 * (size_t)m) || !rd_f(fl, 2 * (size_t)m)) return 2;
+        for (int k = 0; k < m; ++k) S.bonds.push_back({u[2 * k], u[2 * k + 1], fl[2 * k], fl[2 * k + 1]});
+        if (std::fread(&m, 4, 1, f) != 1 || !rd_u(u, 3 * (size_t)m) || !rd_f(fl, 2 * (size_t)m)) return 2;
+        for (int k = 0; k < m; ++k) S.angles.push_back({u[3 * k], u[3 * k + 1], u[3 * k + 2], fl[2 * k], fl[2 * k + 1]});
+        if (std::fread(&m, 4, 1, f) != 1 || !rd_u(u, 4 * (size_t)m) || !rd_f(fl, 3 * (size_t)m)) return 2;
+        for (int k = 0; k < m; ++k)
+            S.dih.push_back({u[4 * k], u[4 * k + 1], u[4 * k + 2], u[4 * k + 3], fl[3 * k], fl[3 * k + 1], fl[3 * k + 2]});
+        if (std::fread(&m, 4, 1, f) != 1 || !rd_u(u, 2 * (size_t)m) || !rd_f(fl, (size_t)m)) return 2;
+        for (int k = 0; k < m; ++k) {
+            uint32_t h = u[2 * k], x = u[2 * k + 1];
+            if (S.at[h].m < S.at[x].m) std::swap(h, x);
+            S.cons.push_back({h, x, fl[k] * fl[k], 1.f / S.at[h].m + 1.f / S.at[x].m});
+        }
     }
     std::fclose(f);
     S.w.resize(n);
