@@ -63,7 +63,7 @@ struct Scalars {
     unsigned int ctr_disp;        // blocks done in k_disp_check (last one decides)
     unsigned int ctr_scale;       // blocks done in k_scale (last one scales the box)
     unsigned int union_max;       // largest group union of the last rebuild
-    unsigned int pad2;
+    unsigned int a_sparse_base;   // first slot of the single-atom clusters
 };
 
 // Partial-sum regions (each kernel family writes 4 doubles per block).
@@ -96,6 +96,9 @@ struct SysView {
     // atom cluster copy
     float4* spos; float2* slj; uint32_t* sidx;   // [na_cap]
     uint32_t* aslot;              // home index -> cluster slot [na]
+    // atoms without bonds (ions) get a cluster each: their rank among such
+    // atoms, INVALID_ID for the others [na]
+    uint32_t* asparse; uint32_t n_sparse;
     // exclusion CSR over home indices (1-2, 1-3 and 1-4 partners)
     uint32_t* ex_off; uint32_t* ex_idx;
     // columns
@@ -111,8 +114,7 @@ struct SysView {
     // cluster bounding boxes (center xyz, half extent xyz)
     float4* wbb_c; float4* wbb_h; float4* abb_c; float4* abb_h;
     // cluster lists (fixed capacity per i cluster)
-    uint32_t cap_ws, cap_sw, cap_ss;
-    uint32_t* ws_n; uint32_t* ws_j;
+    uint32_t cap_sw, cap_ss;
     uint32_t* sw_n; uint32_t* sw_j;
     uint32_t* ss_n; uint32_t* ss_j; unsigned long long* ss_mask;
     // water-water: per 32-water i-group the candidate j-clusters (tile_j),
@@ -291,7 +293,6 @@ void launch_gather_atoms(const Target& t);
 // pair.cu
 void launch_pairs(const Target& t, bool energy);
 void launch_pair14(const Target& t, bool energy);
-int pair_blocks_ww(const SysView& v);
 int pair_ww_setup(const SysView& v);
 int ww_tile_blocks(const SysView& v);
 int pair_blocks_ss(const SysView& v);

@@ -120,6 +120,7 @@ DYN_KERNEL(, k_col_assign, (, bool force), (, force)) {
         atomicAdd(&v.col_count[c], 1u);
     }
     for (uint32_t a = tid; a < v.na; a += stride) {
+        if (v.asparse[a] != INVALID_ID) continue;
         float zf;
         const uint32_t c = column_of(xyz(v.apos[a]), b, v.ancx, v.ancy, &zf);
         v.acol[a] = c;
@@ -147,7 +148,11 @@ DYN_KERNEL(, k_col_scan, (, bool force), (, force)) {
             q += v.acol_count[c];
         }
         v.acol_off[v.ancol] = q; v.acol_boff[v.ancol] = q;
-        v.sc->n_aclus = (q + ACL - 1) / ACL;
+        // clustered atoms fill whole clusters from slot 0; each atom without
+        // bonds then gets a cluster of its own
+        const uint32_t base = (q + ACL - 1) / ACL * ACL;
+        v.sc->a_sparse_base = base;
+        v.sc->n_aclus = base / ACL + v.n_sparse;
     }
 }
 
@@ -161,6 +166,7 @@ DYN_KERNEL(, k_col_bucket, (, bool force), (, force)) {
         v.bucket[v.col_boff[c] + atomicAdd(&v.col_fill[c], 1u)] = s;
     }
     for (uint32_t a = tid; a < v.na; a += stride) {
+        if (v.asparse[a] != INVALID_ID) continue;
         const uint32_t c = v.acol[a];
         v.abucket[v.acol_boff[c] + atomicAdd(&v.acol_fill[c], 1u)] = a;
     }
@@ -185,6 +191,10 @@ DYN_KERNEL(, k_col_rank, (, bool force), (, force)) {
         v.wnew[s] = v.col_off[c] + r;
     }
     for (uint32_t a = tid; a < v.na; a += stride) {
+        if (v.asparse[a] != INVALID_ID) {
+            v.aslot[a] = v.sc->a_sparse_base + ACL * v.asparse[a];
+            continue;
+        }
         const uint32_t c = v.acol[a];
         const float z = v.akey[a];
         uint32_t r = 0;
@@ -303,30 +313,30 @@ __device__ __forceinline__ bool excluded(const SysView& v, uint32_t a, uint32_t 
     return lo < v.ex_off[a + 1] && v.ex_idx[lo] == b;
 }
 
-// MODE: 1 water(i)-atom(j), 2 atom(i)-water(j), 3 atom-atom
+// One warp per atom i-cluster.  MODE 2: water j-clusters; MODE 3: atom
+// j-clusters with cj >= ci (each cluster pair once), with the interaction
+// mask of the cluster pair (jj > ii on the diagonal, exclusions removed).
 DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
     const int lane = threadIdx.x & 31;
     const uint32_t ci = (bk.idx * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t ni = (MODE < 2) ? v.sc->n_wclus : v.sc->n_aclus;
-    const uint32_t nj = (MODE == 0 || MODE == 2) ? v.sc->n_wclus : v.sc->n_aclus;
+    const uint32_t ni = v.sc->n_aclus;
+    const uint32_t nj = MODE == 2 ? v.sc->n_wclus : v.sc->n_aclus;
     if (ci >= ni) return;
-    const float4* bci = (MODE < 2) ? v.wbb_c : v.abb_c;
-    const float4* bhi = (MODE < 2) ? v.wbb_h : v.abb_h;
-    const float4* bcj = (MODE == 0 || MODE == 2) ? v.wbb_c : v.abb_c;
-    const float4* bhj = (MODE == 0 || MODE == 2) ? v.wbb_h : v.abb_h;
+    const float4* bcj = MODE == 2 ? v.wbb_c : v.abb_c;
+    const float4* bhj = MODE == 2 ? v.wbb_h : v.abb_h;
     const float r = MODE == 3 ? v.r_ss : v.r_ws;
     const float r2 = r * r;
-    const uint32_t cap = MODE == 1 ? v.cap_ws : MODE == 2 ? v.cap_sw : v.cap_ss;
-    uint32_t* out = MODE == 1 ? v.ws_j : MODE == 2 ? v.sw_j : v.ss_j;
-    uint32_t* outn = MODE == 1 ? v.ws_n : MODE == 2 ? v.sw_n : v.ss_n;
-    const float4 c0 = bci[ci], h0 = bhi[ci];
+    const uint32_t cap = MODE == 2 ? v.cap_sw : v.cap_ss;
+    uint32_t* out = MODE == 2 ? v.sw_j : v.ss_j;
+    uint32_t* outn = MODE == 2 ? v.sw_n : v.ss_n;
+    const float4 c0 = v.abb_c[ci], h0 = v.abb_h[ci];
     uint32_t cnt = 0;
-    for (uint32_t jb = 0; jb < nj; jb += 32) {
+    for (uint32_t jb = MODE == 3 ? (ci & ~31u) : 0u; jb < nj; jb += 32) {
         const uint32_t cj = jb + lane;
         bool hit = false;
-        if (cj < nj) hit = bb_dist2(c0, h0, bcj[cj], bhj[cj], b) < r2;
+        if (cj < nj && (MODE != 3 || cj >= ci)) hit = bb_dist2(c0, h0, bcj[cj], bhj[cj], b) < r2;
         const uint32_t m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
             const uint32_t k = cnt + __popc(m & ((1u << lane) - 1u));
@@ -339,7 +349,7 @@ DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
                         if (a == INVALID_ID) continue;
                         for (int jj = 0; jj < ACL; ++jj) {
                             const uint32_t c = v.sidx[cj * ACL + jj];
-                            if (c == INVALID_ID || c == a) continue;
+                            if (c == INVALID_ID || (cj == ci && jj <= ii)) continue;
                             if (v.astatic && v.astatic[a] && v.astatic[c]) continue;
                             if (v.ex_off && excluded(v, a, c)) continue;
                             mask |= 1ull << (ii * ACL + jj);
@@ -590,9 +600,6 @@ void launch_rebuild(const Target& t, bool force) {
              force);
     t.launch(k_group_union, k_group_union_batch,
              [](const SysView& v) { return v.nw ? (int)std::min<uint32_t>(v.ngrp_cap, 148 * 8) : 0; }, UT, 0, force);
-    t.launch(k_list<1>, k_list_batch<1>,
-             [](const SysView& v) { return v.nw && v.na ? nblocks((uint64_t)v.nwclus_cap * 32, 128, 1 << 30) : 0; },
-             LT, 0, force);
     t.launch(k_list<2>, k_list_batch<2>,
              [](const SysView& v) { return v.nw && v.na ? nblocks((uint64_t)v.naclus_cap * 32, 128, 1 << 30) : 0; },
              LT, 0, force);

@@ -7,18 +7,20 @@
 // between charged sites, 1-2/1-3 exclusions, no intra-water pairs; 1-4 pairs
 // are excluded here and evaluated (scaled) by k_pair14.
 //
-// Work decomposition (full lists, no atomics on the i side).  Water-water:
-// one CTA per 32-water i-group, j sites staged in shared memory, LPW lanes
-// per i-water over its compact molecule list (k_pair_ww_tile).  Mixed and
-// atom kernels: one warp per 8-body i-cluster; lane = (ii, jq) with
-// ii = lane & 7 and jq = lane >> 3 evaluates i-body ii against j-bodies jq and
-// jq + 4 of every j-cluster in its list.  Water pairs are handled as molecule
-// pairs: one min-image shift from the O-O vector serves all 10 site pairs
-// (1 LJ + 9 Coulomb), valid because the cutoff plus twice the O-H reach is
-// below half the box.  i-forces stay in registers over the whole list, are
-// reduced over the lanes sharing an i-body with shuffles and stored once as
-// int64 fixed point; the water-water and atom-atom kernels store (first
-// writers), the mixed kernels add.
+// Work decomposition.  Water-water (full list, no atomics): one CTA per
+// 32-water i-group, j sites staged in shared memory, LPW lanes per i-water
+// over its compact molecule list (k_pair_ww_tile).  Atom-water and atom-atom
+// (half lists: every pair once): one warp per 8-atom i-cluster; lane =
+// (ii, jq) with ii = lane & 7 and jq = lane >> 3 evaluates i-atom ii against
+// j-bodies jq and jq + 4 of every j-cluster in its list.  Water pairs are
+// handled as molecule pairs: one min-image shift from the O-O vector serves
+// all site pairs, valid because the cutoff plus twice the O-H reach is below
+// half the box.  i-forces stay in registers over the whole list, are reduced
+// over the lanes sharing an i-body with shuffles and written once as int64
+// fixed point; the water-water kernel stores (first writer), the others add,
+// and j-side forces go out as integer atomics after a reduce-scatter over
+// the lanes of a j-body.  Integer sums do not depend on order, so the
+// result is deterministic.
 #include <algorithm>
 
 #include "engine.cuh"
@@ -64,13 +66,15 @@ __device__ __forceinline__ void coul(float3 pi, float3 pj, float3 sh, float qq, 
     f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
     a.w = fmaf(fs, r2, a.w);
     if (ENERGY) {
+        // r^2 from the exact displacement, rounded once to float32; erfc(alpha
+        // r) / r in float32 (correctly rounded sqrt and divide), scaled by the
+        // float64 charge product and summed in float64
         double x, y, z;
         exact_disp(pi, pj, sh, x, y, z);
-        const double r2d = x * x + y * y + z * z;
-        const double rcd = (double)v.rc;
-        if (r2d < rcd * rcd) {
-            const double rd = sqrt(r2d);
-            a.e_c += qqe * erfc((double)v.alpha * rd) / rd;
+        const float r2e = (float)(x * x + y * y + z * z);
+        if (r2e < v.rc2) {
+            const float re = __fsqrt_rn(r2e);
+            a.e_c += qqe * (double)__fdiv_rn(erfcf(v.alpha * re), re);
         }
     }
 }
@@ -93,8 +97,8 @@ __device__ __forceinline__ void lj(float3 pi, float3 pj, float3 sh, float sig2, 
     if (ENERGY && in) {
         double x, y, z;
         exact_disp(pi, pj, sh, x, y, z);
-        const double s2 = (double)sig2 / (x * x + y * y + z * z);
-        const double s6 = s2 * s2 * s2;
+        const float s2 = __fdiv_rn(sig2, (float)(x * x + y * y + z * z));
+        const double s6 = (double)(s2 * s2 * s2);
         a.e_lj += 4.0 * (double)scale * (double)eps * (s6 * s6 - s6);
     }
 }
@@ -291,64 +295,33 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
     write_partials<ENERGY>(v, bk, REG_WW, el, ec, ew);
 }
 
-// ---------------------------------------------------------------------------
-// water(i) - atom(j): forces on the water sites
-// ---------------------------------------------------------------------------
-DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ws, (), ()) {
-    const int lane = threadIdx.x & 31;
-    const int ii = lane & 7, jq = lane >> 3;
-    const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
-    const uint32_t nwc = v.sc->n_wclus;
-    const uint32_t nch = (v.cap_ws + CH_MIX - 1) / CH_MIX;
-    const BoxDev b = *v.box;
-    const float ljc2 = v.ljc2;
-    double el = 0.0, ec = 0.0, ew = 0.0;
-    // one warp per (i-cluster, chunk of CH_MIX list entries)
-    for (uint32_t wv = ((bk.idx * blockDim.x + threadIdx.x) >> 5); wv < nwc * nch; wv += nwarps) {
-        const uint32_t ci = wv / nch, k0 = (wv % nch) * CH_MIX;
-        const uint32_t n = min(v.ws_n[ci], k0 + CH_MIX);
-        if (n <= k0) continue;
-        const uint32_t si = ci * WCL + ii;
-        const bool vi = v.wid[si] != INVALID_ID;
-        const float3 iO = xyz(v.wpos[4 * si + 0]), iH0 = xyz(v.wpos[4 * si + 1]);
-        const float3 iH1 = xyz(v.wpos[4 * si + 2]), iM = xyz(v.wpos[4 * si + 3]);
-        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
-        Acc3 a{0.0, 0.0, 0.f};
-        const uint32_t* lst = v.ws_j + (size_t)ci * v.cap_ws;
-        for (uint32_t k = k0; k < n; ++k) {
-            const uint32_t cj = lst[k];
+// Reduce-scatter over the 8 lanes that share jq (lane bits 0-2): N values
+// per lane in, N/8 out; lane ii ends with the sums of values
+// [ii N/8, (ii + 1) N/8).  The pairing order is fixed, so the result is
+// deterministic.
+template <int N>
+__device__ __forceinline__ void reduce_scatter8(float (&x)[N], int ii) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const uint32_t sj = cj * ACL + jq + 4 * h;
-                if (!vi || v.sidx[sj] == INVALID_ID) continue;
-                const float4 pj = v.spos[sj];
-                const float2 lj_j = v.slj[sj];
-                const float3 jp = xyz(pj);
-                const float3 s = shift_of(iO - jp, b);
-                const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
-                const float ep = sqrtf(OPC_O_EPS * lj_j.y);
-                lj<ENERGY>(iO, jp, s, sg * sg, ep, ljc2, 1.0f, fO, a);
-                coul<ENERGY>(iH0, jp, s, OPC_Q_H * pj.w, (double)OPC_Q_H * (double)pj.w, v, fH0, a);
-                coul<ENERGY>(iH1, jp, s, OPC_Q_H * pj.w, (double)OPC_Q_H * (double)pj.w, v, fH1, a);
-                coul<ENERGY>(iM, jp, s, OPC_Q_EP * pj.w, (double)OPC_Q_EP * (double)pj.w, v, fM, a);
-            }
+    for (int m = 4, h = N / 2; m >= 1; m >>= 1, h >>= 1) {
+        const bool up = (ii & m) != 0;
+#pragma unroll
+        for (int k = 0; k < h; ++k) {
+            const float keep = up ? x[k + h] : x[k];
+            const float send = up ? x[k] : x[k + h];
+            x[k] = keep + __shfl_xor_sync(0xffffffffu, send, m);
         }
-        fO = f3(red4(fO.x), red4(fO.y), red4(fO.z));
-        fH0 = f3(red4(fH0.x), red4(fH0.y), red4(fH0.z));
-        fH1 = f3(red4(fH1.x), red4(fH1.y), red4(fH1.z));
-        fM = f3(red4(fM.x), red4(fM.y), red4(fM.z));
-        if (jq == 0 && vi) {
-            long long* p = v.wforce + (size_t)si * 12;
-            add_fix3(p + 0, fO); add_fix3(p + 3, fH0); add_fix3(p + 6, fH1); add_fix3(p + 9, fM);
-        }
-        if (ENERGY) { el += a.e_lj; ec += a.e_c; }
-        ew += a.w;
     }
-    write_partials<ENERGY>(v, bk, REG_WS, el, ec, ew);
+}
+
+__device__ __forceinline__ void add_fix(long long* p, float f) {
+    if (f != 0.0f) fix_atomic_add(p, fix_from_float(f));
 }
 
 // ---------------------------------------------------------------------------
-// atom(i) - water(j): forces on the atoms
+// atom(i) - water(j), each pair once: the atom's force stays in registers
+// over its list; the water sites' forces (the opposite of the pair forces)
+// are summed over the 8 i-atoms of a lane group and added with integer
+// atomics, which makes the total independent of order.
 // ---------------------------------------------------------------------------
 DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_sw, (), ()) {
     const int lane = threadIdx.x & 31;
@@ -370,22 +343,41 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_sw, (), ()) 
         const float2 lji = v.slj[si];
         const float sg = 0.5f * (OPC_O_SIGMA + lji.x);
         const float ep = sqrtf(OPC_O_EPS * lji.y);
+        const float qh = pi.w * OPC_Q_H, qm = pi.w * OPC_Q_EP;
+        const double eh = (double)pi.w * (double)OPC_Q_H, em = (double)pi.w * (double)OPC_Q_EP;
         float3 f = f3(0, 0, 0);
         Acc3 a{0.0, 0.0, 0.f};
         const uint32_t* lst = v.sw_j + (size_t)ci * v.cap_sw;
         for (uint32_t k = k0; k < n; ++k) {
             const uint32_t cj = lst[k];
+            float wf[24];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const uint32_t sj = cj * WCL + jq + 4 * h;
-                if (!vi || v.wid[sj] == INVALID_ID) continue;
-                const float3 jO = xyz(v.wpos[4 * sj + 0]);
-                const float3 s = shift_of(xyz(pi) - jO, b);
-                const double eh = (double)pi.w * (double)OPC_Q_H, em = (double)pi.w * (double)OPC_Q_EP;
-                lj<ENERGY>(xyz(pi), jO, s, sg * sg, ep, ljc2, 1.0f, f, a);
-                coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 1]), s, pi.w * OPC_Q_H, eh, v, f, a);
-                coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 2]), s, pi.w * OPC_Q_H, eh, v, f, a);
-                coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 3]), s, pi.w * OPC_Q_EP, em, v, f, a);
+                float3 fo = f3(0, 0, 0), f0 = fo, f1 = fo, fm = fo;
+                if (vi && v.wid[sj] != INVALID_ID) {
+                    const float3 jO = xyz(v.wpos[4 * sj + 0]);
+                    const float3 s = shift_of(xyz(pi) - jO, b);
+                    lj<ENERGY>(xyz(pi), jO, s, sg * sg, ep, ljc2, 1.0f, fo, a);
+                    coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 1]), s, qh, eh, v, f0, a);
+                    coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 2]), s, qh, eh, v, f1, a);
+                    coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 3]), s, qm, em, v, fm, a);
+                }
+                f = f + ((fo + f0) + (f1 + fm));
+                const float3 q[4] = {fo, f0, f1, fm};
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    wf[12 * h + 3 * t + 0] = -q[t].x;
+                    wf[12 * h + 3 * t + 1] = -q[t].y;
+                    wf[12 * h + 3 * t + 2] = -q[t].z;
+                }
+            }
+            // lane ii now holds site (ii & 3) of water jq + 4 (ii >> 2)
+            reduce_scatter8(wf, ii);
+            const uint32_t sj = cj * WCL + jq + 4 * (ii >> 2);
+            if (v.wid[sj] != INVALID_ID) {
+                long long* p = v.wforce + (size_t)sj * 12 + 3 * (ii & 3);
+                add_fix(p + 0, wf[0]); add_fix(p + 1, wf[1]); add_fix(p + 2, wf[2]);
             }
         }
         f = f3(red4(f.x), red4(f.y), red4(f.z));
@@ -397,7 +389,9 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_sw, (), ()) 
 }
 
 // ---------------------------------------------------------------------------
-// atom(i) - atom(j): interaction mask from the list build
+// atom(i) - atom(j), each pair once (cluster pairs with cj >= ci; the
+// interaction mask from the list build holds jj > ii on the diagonal and
+// drops exclusions); j forces go out through integer atomics as above.
 // ---------------------------------------------------------------------------
 DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) {
     const int lane = threadIdx.x & 31;
@@ -423,17 +417,29 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) 
         for (uint32_t k = k0; k < n; ++k) {
             const uint32_t cj = lst[k];
             const unsigned long long m = msk[k];
+            float jf[8];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int jj = jq + 4 * h;
-                if (!((m >> (ii * ACL + jj)) & 1ull)) continue;
-                const uint32_t sj = cj * ACL + jj;
-                const float4 pj = v.spos[sj];
-                const float2 ljj = v.slj[sj];
-                const float3 s = shift_of(xyz(pi) - xyz(pj), b);
-                const float sg = 0.5f * (lji.x + ljj.x);
-                lj<ENERGY>(xyz(pi), xyz(pj), s, sg * sg, sqrtf(lji.y * ljj.y), ljc2, 1.0f, f, a);
-                coul<ENERGY>(xyz(pi), xyz(pj), s, pi.w * pj.w, (double)pi.w * (double)pj.w, v, f, a);
+                float3 fp = f3(0, 0, 0);
+                if ((m >> (ii * ACL + jj)) & 1ull) {
+                    const uint32_t sj = cj * ACL + jj;
+                    const float4 pj = v.spos[sj];
+                    const float2 ljj = v.slj[sj];
+                    const float3 s = shift_of(xyz(pi) - xyz(pj), b);
+                    const float sg = 0.5f * (lji.x + ljj.x);
+                    lj<ENERGY>(xyz(pi), xyz(pj), s, sg * sg, sqrtf(lji.y * ljj.y), ljc2, 1.0f, fp, a);
+                    coul<ENERGY>(xyz(pi), xyz(pj), s, pi.w * pj.w, (double)pi.w * (double)pj.w, v, fp, a);
+                }
+                f = f + fp;
+                jf[3 * h + 0] = -fp.x; jf[3 * h + 1] = -fp.y; jf[3 * h + 2] = -fp.z;
+            }
+            jf[6] = 0.f; jf[7] = 0.f;
+            // lane ii < 6 now holds component ii % 3 of atom jq + 4 (ii / 3)
+            reduce_scatter8(jf, ii);
+            if (ii < 6) {
+                const uint32_t aj = v.sidx[cj * ACL + jq + 4 * (ii / 3)];
+                if (aj != INVALID_ID) add_fix(v.aforce + 3 * (size_t)aj + ii % 3, jf[0]);
             }
         }
         f = f3(red4(f.x), red4(f.y), red4(f.z));
@@ -481,7 +487,6 @@ inline int pblocks(const SysView& v, uint64_t warps) {
 
 namespace dyn {
 
-int pair_blocks_ww(const SysView& v) { return pblocks(v, (uint64_t)v.nwclus_cap * ((v.cap_ws + CH_MIX - 1) / CH_MIX)); }
 int pair_blocks_sw(const SysView& v) { return pblocks(v, (uint64_t)v.naclus_cap * ((v.cap_sw + CH_MIX - 1) / CH_MIX)); }
 
 int ww_tile_blocks(const SysView& v) {
@@ -526,15 +531,13 @@ void launch_pairs(const Target& t, bool energy) {
     t.launch(k_pair_ww_tile<false>, k_pair_ww_tile_batch<false>,
              [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
     auto ss = [](const SysView& v) { return v.na ? (int)v.nb[REG_SS] : 0; };
-    auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
     auto sw = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_SW] : 0; };
+    // the mixed kernels add to the water forces the water-water kernel stores
     if (energy) {
         t.launch(k_pair_ss<true>, k_pair_ss_batch<true>, ss, PT, 0);
-        t.launch(k_pair_ws<true>, k_pair_ws_batch<true>, ws, PT, 0);
         t.launch(k_pair_sw<true>, k_pair_sw_batch<true>, sw, PT, 0);
     } else {
         t.launch(k_pair_ss<false>, k_pair_ss_batch<false>, ss, PT, 0);
-        t.launch(k_pair_ws<false>, k_pair_ws_batch<false>, ws, PT, 0);
         t.launch(k_pair_sw<false>, k_pair_sw_batch<false>, sw, PT, 0);
     }
 }

@@ -81,7 +81,7 @@ void host_m_site(const float* o, const float* h0, const float* h1, float* m) {
 void set_block_counts(SysView& v) {
     for (int r = 0; r < NREGION; ++r) v.nb[r] = 0;
     v.nb[REG_WW] = v.nw ? dyn::ww_tile_blocks(v) : 0;
-    v.nb[REG_WS] = (v.nw && v.na) ? dyn::pair_blocks_ww(v) : 0;
+    v.nb[REG_WS] = 0;
     v.nb[REG_SW] = (v.nw && v.na) ? dyn::pair_blocks_sw(v) : 0;
     v.nb[REG_SS] = v.na ? dyn::pair_blocks_ss(v) : 0;
     v.nb[REG_14] = v.n14 ? dyn::pair14_blocks(v) : 0;
@@ -390,7 +390,18 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     // padded to whole 32-water groups
     v.nw_cap = round_up(std::max(1u, v.nw), 2 * GRPW);
     v.nwclus_cap = v.nw_cap / WCL;
-    v.na_cap = round8(v.na + 8);
+    // atoms without bonds (ions) take a cluster each, after the others
+    std::vector<uint32_t> sparse_rank(std::max(1u, v.na), INVALID_ID);
+    {
+        std::vector<uint8_t> bonded(v.na, 0);
+        for (uint32_t i = 0; i < 2 * d->n_bonds; ++i) bonded[d->bonds[i]] = 1;
+        for (uint32_t i = 0; i < 2 * d->n_constraints; ++i) bonded[d->constraints[i]] = 1;
+        uint32_t k = 0;
+        for (uint32_t a = 0; a < v.na; ++a)
+            if (!bonded[a]) sparse_rank[a] = k++;
+        v.n_sparse = k;
+    }
+    v.na_cap = round8(v.na - v.n_sparse + 8) + ACL * v.n_sparse;
     v.naclus_cap = v.na_cap / ACL;
     v.max_blocks = 148 * 16;
 
@@ -467,7 +478,6 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         if ((uint64_t)n_i * n_j <= (1ull << 24)) return std::max(1u, n_j);
         return est(r, vol_cl, n_j);
     };
-    v.cap_ws = (v.nw && v.na) ? cap_mixed(v.r_ws, acl_vol, v.nwclus_cap, v.naclus_cap) : 1;
     v.cap_sw = (v.nw && v.na) ? cap_mixed(v.r_ws, wcl_vol, v.naclus_cap, v.nwclus_cap) : 1;
     v.cap_ss = v.na ? cap_mixed(v.r_ss, acl_vol, v.naclus_cap, v.naclus_cap) : 1;
 
@@ -494,6 +504,8 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dev_alloc(h, &v.aforce, 3 * (size_t)std::max(1u, v.na)));
     TRY(dev_alloc(h, &v.arecip, 3 * (size_t)std::max(1u, v.na)));
     TRY(dev_alloc(h, &v.aref, std::max(1u, v.na)));
+    TRY(dev_alloc(h, &v.asparse, std::max(1u, v.na), false));
+    TRY(upload(h, v.asparse, sparse_rank.data(), v.na));
     TRY(dev_alloc(h, &v.spos, v.na_cap));
     TRY(dev_alloc(h, &v.slj, v.na_cap));
     TRY(dev_alloc(h, &v.sidx, v.na_cap, false));
@@ -524,8 +536,6 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dev_alloc(h, &v.cand_loc, (size_t)v.ngrp_cap * v.cap_tile * WCL));
     TRY(dev_alloc(h, &v.wnb_n, v.nw_cap));
     TRY(dev_alloc(h, &v.wnb, (size_t)v.nw_cap * v.cap_nb));
-    TRY(dev_alloc(h, &v.ws_n, v.nwclus_cap));
-    TRY(dev_alloc(h, &v.ws_j, (size_t)v.nwclus_cap * v.cap_ws));
     TRY(dev_alloc(h, &v.sw_n, v.naclus_cap));
     TRY(dev_alloc(h, &v.sw_j, (size_t)v.naclus_cap * v.cap_sw));
     TRY(dev_alloc(h, &v.ss_n, v.naclus_cap));
