@@ -5,10 +5,13 @@ Residue templates, charges and bonded / LJ parameters come from the
 reference's ff19SB files (amino19.lib, parm19.dat, frcmod.ff19SB, extracted
 by data/make_ff19sb.py into data/ff19sb.json).  The chain is built from
 ideal backbone internal coordinates (NeRF placement of N, CA, C), each
-residue template superposed on its N, CA, C.  A chain longer than the box is
-laid out as a meander of extended strands joined by two-residue turns, so it
-fits without touching its periodic image; the termini are the internal
-templates (no caps).  Ions: the reference's Joung-Cheatham OPC parameters
+residue template superposed on its N, CA, C.  The chain is grown as a
+self-avoiding random coil inside a sphere well inside the box (torsions from
+the Ramachandran basins), so a chain far longer than the box (300 residues
+in a 98 A cube) fits without touching its periodic image; an extended
+meander of that length spans the whole box and drifts into its own
+periodic image once it moves.  The termini are the internal templates (no
+caps).  Ions: the reference's Joung-Cheatham OPC parameters
 (src/lib.rs:1568-1658), placed on water sites that they replace.
 """
 import json
