@@ -30,6 +30,7 @@
 #define UMAX 5            // atoms per constraint unit (a heavy atom and up to 4 H)
 #define LPW 8             // lanes per i-water in the water-water kernel
 #define ACL 8             // atoms per cluster
+#define CH_MIX 16         // list entries per work item of the atom pair kernels
 #define INVALID_ID 0xFFFFFFFFu
 #define NACC 16           // accumulator slots
 
@@ -64,6 +65,8 @@ struct Scalars {
     unsigned int ctr_scale;       // blocks done in k_scale (last one scales the box)
     unsigned int union_max;       // largest group union of the last rebuild
     unsigned int a_sparse_base;   // first slot of the single-atom clusters
+    unsigned int n_ws_items;      // work items of the water-atom pair kernel
+    unsigned int n_ss_items;      // work items of the atom-atom pair kernel
 };
 
 // Partial-sum regions (each kernel family writes 4 doubles per block).
@@ -113,10 +116,14 @@ struct SysView {
     uint32_t* wcol; uint32_t* acol;             // column of each water / atom
     // cluster bounding boxes (center xyz, half extent xyz)
     float4* wbb_c; float4* wbb_h; float4* abb_c; float4* abb_h;
-    // cluster lists (fixed capacity per i cluster)
-    uint32_t cap_sw, cap_ss;
-    uint32_t* sw_n; uint32_t* sw_j;
+    // cluster lists (fixed capacity per i cluster): water cluster -> atom
+    // clusters, atom cluster -> atom clusters (cj >= ci) with masks; work
+    // items {i cluster, first entry} of CH_MIX list entries, in i order
+    uint32_t cap_ws, cap_ss;
+    uint32_t* ws_n; uint32_t* ws_j;
     uint32_t* ss_n; uint32_t* ss_j; unsigned long long* ss_mask;
+    uint2* ws_item; uint2* ss_item;
+    uint32_t ws_item_cap, ss_item_cap;
     // water-water: per 32-water i-group the candidate j-clusters (tile_j),
     // the union of the waters its members need, stored as runs of
     // consecutive slots (staged in shared memory by bulk copies), and per
@@ -296,7 +303,7 @@ void launch_pair14(const Target& t, bool energy);
 int pair_ww_setup(const SysView& v);
 int ww_tile_blocks(const SysView& v);
 int pair_blocks_ss(const SysView& v);
-int pair_blocks_sw(const SysView& v);
+int pair_blocks_ws(const SysView& v);
 int pair14_blocks(const SysView& v);
 
 // pme.cu

@@ -401,21 +401,21 @@ __device__ double gamma_mt(double shape, uint64_t step, uint64_t seed) {
 }
 
 DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (, dt, thermo)) {
-    double ww[4] = {0, 0, 0, 0}, sw[4] = {0, 0, 0, 0}, ss[4] = {0, 0, 0, 0};
+    double ww[4] = {0, 0, 0, 0}, ws[4] = {0, 0, 0, 0}, ss[4] = {0, 0, 0, 0};
     double p14[4] = {0, 0, 0, 0}, bo[4] = {0, 0, 0, 0}, kw[4] = {0, 0, 0, 0}, ka[4] = {0, 0, 0, 0};
     double co[4] = {0, 0, 0, 0};
     region_sum(v, REG_WW, ww);
     if (v.na) {
         region_sum(v, REG_SS, ss);
-        if (v.nw) region_sum(v, REG_SW, sw);
+        if (v.nw) region_sum(v, REG_WS, ws);
         region_sum(v, REG_14, p14);
         region_sum(v, REG_BOND, bo);
         region_sum(v, REG_KICK_A, ka);
         region_sum(v, REG_CONS, co);
     }
     region_sum(v, REG_KICK_W, kw);
-    double x[16] = {ww[0], ww[1], ww[2], sw[0] + ss[0], sw[1] + ss[1],
-                    sw[2] + ss[2], p14[0], p14[2], bo[0], bo[2], kw[0] + ka[0],
+    double x[16] = {ww[0], ww[1], ww[2], ws[0] + ss[0], ws[1] + ss[1],
+                    ws[2] + ss[2], p14[0], p14[2], bo[0], bo[2], kw[0] + ka[0],
                     kw[1] + ka[1], co[0], kw[2] + ka[2], kw[3], 0};
     block_sum_d<16>(x);
     if (threadIdx.x != 0) return;

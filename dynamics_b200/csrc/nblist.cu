@@ -313,25 +313,27 @@ __device__ __forceinline__ bool excluded(const SysView& v, uint32_t a, uint32_t 
     return lo < v.ex_off[a + 1] && v.ex_idx[lo] == b;
 }
 
-// One warp per atom i-cluster.  MODE 2: water j-clusters; MODE 3: atom
-// j-clusters with cj >= ci (each cluster pair once), with the interaction
-// mask of the cluster pair (jj > ii on the diagonal, exclusions removed).
+// One warp per i-cluster.  MODE 1: water i-clusters against atom
+// j-clusters; MODE 3: atom i-clusters against atom j-clusters with cj >= ci
+// (each cluster pair once), with the interaction mask of the cluster pair
+// (jj > ii on the diagonal, exclusions removed).
 DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
     const int lane = threadIdx.x & 31;
     const uint32_t ci = (bk.idx * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t ni = v.sc->n_aclus;
-    const uint32_t nj = MODE == 2 ? v.sc->n_wclus : v.sc->n_aclus;
+    const uint32_t ni = MODE == 1 ? v.sc->n_wclus : v.sc->n_aclus;
+    const uint32_t nj = v.sc->n_aclus;
     if (ci >= ni) return;
-    const float4* bcj = MODE == 2 ? v.wbb_c : v.abb_c;
-    const float4* bhj = MODE == 2 ? v.wbb_h : v.abb_h;
+    const float4* bcj = v.abb_c;
+    const float4* bhj = v.abb_h;
     const float r = MODE == 3 ? v.r_ss : v.r_ws;
     const float r2 = r * r;
-    const uint32_t cap = MODE == 2 ? v.cap_sw : v.cap_ss;
-    uint32_t* out = MODE == 2 ? v.sw_j : v.ss_j;
-    uint32_t* outn = MODE == 2 ? v.sw_n : v.ss_n;
-    const float4 c0 = v.abb_c[ci], h0 = v.abb_h[ci];
+    const uint32_t cap = MODE == 1 ? v.cap_ws : v.cap_ss;
+    uint32_t* out = MODE == 1 ? v.ws_j : v.ss_j;
+    uint32_t* outn = MODE == 1 ? v.ws_n : v.ss_n;
+    const float4 c0 = MODE == 1 ? v.wbb_c[ci] : v.abb_c[ci];
+    const float4 h0 = MODE == 1 ? v.wbb_h[ci] : v.abb_h[ci];
     uint32_t cnt = 0;
     for (uint32_t jb = MODE == 3 ? (ci & ~31u) : 0u; jb < nj; jb += 32) {
         const uint32_t cj = jb + lane;
@@ -365,6 +367,52 @@ DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
         outn[ci] = min(cnt, cap);
         if (cnt > cap) atomicMax(&v.sc->overflow, cnt);
         atomicAdd(&v.sc->list_pairs, (unsigned long long)min(cnt, cap));
+    }
+}
+
+// Work items of the atom pair kernels: for every i-cluster (in order) one
+// item per CH_MIX entries of its list, {cluster, first entry}.  One block;
+// an exclusive scan of the per-cluster item counts, tile by tile.
+constexpr int IT_T = 1024;
+DYN_KERNEL_T((int MODE), (MODE), __launch_bounds__(IT_T), k_items, (, bool force), (, force)) {
+    if (!rebuild_on(v, force)) return;
+    const uint32_t ni = MODE == 1 ? v.sc->n_wclus : v.sc->n_aclus;
+    const uint32_t* cnt = MODE == 1 ? v.ws_n : v.ss_n;
+    uint2* items = MODE == 1 ? v.ws_item : v.ss_item;
+    const uint32_t icap = MODE == 1 ? v.ws_item_cap : v.ss_item_cap;
+    __shared__ uint32_t wsum[IT_T / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t base = 0;
+    for (uint32_t c0 = 0; c0 < ni; c0 += IT_T) {
+        const uint32_t c = c0 + threadIdx.x;
+        const uint32_t k = c < ni ? (cnt[c] + CH_MIX - 1) / CH_MIX : 0u;
+        uint32_t x = k;  // inclusive scan inside the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            uint32_t t = lane < IT_T / 32 ? wsum[lane] : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            if (lane < IT_T / 32) wsum[lane] = t;  // inclusive warp totals
+        }
+        __syncthreads();
+        const uint32_t off = base + (w ? wsum[w - 1] : 0u) + x - k;
+        for (uint32_t t = 0; t < k; ++t)
+            if (off + t < icap) items[off + t] = make_uint2(c, t * CH_MIX);
+        base += wsum[IT_T / 32 - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (MODE == 1) v.sc->n_ws_items = min(base, icap);
+        else v.sc->n_ss_items = min(base, icap);
     }
 }
 
@@ -600,12 +648,14 @@ void launch_rebuild(const Target& t, bool force) {
              force);
     t.launch(k_group_union, k_group_union_batch,
              [](const SysView& v) { return v.nw ? (int)std::min<uint32_t>(v.ngrp_cap, 148 * 8) : 0; }, UT, 0, force);
-    t.launch(k_list<2>, k_list_batch<2>,
-             [](const SysView& v) { return v.nw && v.na ? nblocks((uint64_t)v.naclus_cap * 32, 128, 1 << 30) : 0; },
+    t.launch(k_list<1>, k_list_batch<1>,
+             [](const SysView& v) { return v.nw && v.na ? nblocks((uint64_t)v.nwclus_cap * 32, 128, 1 << 30) : 0; },
              LT, 0, force);
     t.launch(k_list<3>, k_list_batch<3>,
              [](const SysView& v) { return v.na ? nblocks((uint64_t)v.naclus_cap * 32, 128, 1 << 30) : 0; }, LT, 0,
              force);
+    t.launch(k_items<1>, k_items_batch<1>, [](const SysView& v) { return v.nw && v.na ? 1 : 0; }, IT_T, 0, force);
+    t.launch(k_items<3>, k_items_batch<3>, [](const SysView& v) { return v.na ? 1 : 0; }, IT_T, 0, force);
     t.launch(k_rebuild_done, k_rebuild_done_batch, [](const SysView&) { return 1; }, 1, 0, force);
 }
 

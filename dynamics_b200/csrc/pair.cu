@@ -10,9 +10,10 @@
 // Work decomposition.  Water-water (full list, no atomics): one CTA per
 // 32-water i-group, j sites staged in shared memory, LPW lanes per i-water
 // over its compact molecule list (k_pair_ww_tile).  Atom-water and atom-atom
-// (half lists: every pair once): one warp per 8-atom i-cluster; lane =
-// (ii, jq) with ii = lane & 7 and jq = lane >> 3 evaluates i-atom ii against
-// j-bodies jq and jq + 4 of every j-cluster in its list.  Water pairs are
+// (half lists: every pair once): one warp per work item (an 8-body
+// i-cluster and up to CH_MIX entries of its list); lane = (ii, jq) with
+// ii = lane & 7 and jq = lane >> 3 evaluates i-body ii against j-atoms jq and
+// jq + 4 of every j-cluster in the item.  Water pairs are
 // handled as molecule pairs: one min-image shift from the O-O vector serves
 // all site pairs, valid because the cutoff plus twice the O-H reach is below
 // half the box.  i-forces stay in registers over the whole list, are reduced
@@ -28,7 +29,6 @@
 namespace {
 
 constexpr int PT = 128;  // threads per block (4 warps)
-constexpr uint32_t CH_MIX = 16;  // list entries per warp in the mixed kernels
 
 // e_lj, e_c accumulate per-pair energies in float64 (energy steps only);
 // w accumulates the virial in float32
@@ -317,115 +317,129 @@ __device__ __forceinline__ void add_fix(long long* p, float f) {
     if (f != 0.0f) fix_atomic_add(p, fix_from_float(f));
 }
 
+// j-atom data of one list entry for lane group jq: atoms jq and jq + 4 of
+// cluster cj (position + charge, sigma/eps, home index or INVALID_ID)
+struct JAtoms { float4 p0, p1; float2 l0, l1; uint32_t a0, a1; };
+__device__ __forceinline__ JAtoms load_jatoms(const SysView& v, uint32_t cj, int jq) {
+    const uint32_t s = cj * ACL + jq;
+    return JAtoms{v.spos[s], v.spos[s + 4], v.slj[s], v.slj[s + 4], v.sidx[s], v.sidx[s + 4]};
+}
+
 // ---------------------------------------------------------------------------
-// atom(i) - water(j), each pair once: the atom's force stays in registers
-// over its list; the water sites' forces (the opposite of the pair forces)
-// are summed over the 8 i-atoms of a lane group and added with integer
-// atomics, which makes the total independent of order.
+// water(i) - atom(j), each pair once.  One warp per work item (a water
+// i-cluster and CH_MIX entries of its atom-cluster list); the list entries
+// are read once per item (one per lane) and the next entry's j-atoms are
+// loaded while the current one is evaluated.  The water forces stay in
+// registers over the item; the j-atom forces (the opposite of the pair
+// forces) are reduce-scattered over the 8 water lanes of a j-group and added
+// with integer atomics (24 per entry).
 // ---------------------------------------------------------------------------
-DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_sw, (), ()) {
+DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT, 4), k_pair_ws, (), ()) {
     const int lane = threadIdx.x & 31;
     const int ii = lane & 7, jq = lane >> 3;
     const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
-    const uint32_t nac = v.sc->n_aclus;
-    const uint32_t nch = (v.cap_sw + CH_MIX - 1) / CH_MIX;
+    const uint32_t nit = v.sc->n_ws_items;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t wv = ((bk.idx * blockDim.x + threadIdx.x) >> 5); wv < nac * nch; wv += nwarps) {
-        const uint32_t ci = wv / nch, k0 = (wv % nch) * CH_MIX;
-        const uint32_t n = min(v.sw_n[ci], k0 + CH_MIX);
-        if (n <= k0) continue;
-        const uint32_t si = ci * ACL + ii;
-        const uint32_t ai = v.sidx[si];
-        const bool vi = ai != INVALID_ID;
-        const float4 pi = v.spos[si];
-        const float2 lji = v.slj[si];
-        const float sg = 0.5f * (OPC_O_SIGMA + lji.x);
-        const float ep = sqrtf(OPC_O_EPS * lji.y);
-        const float qh = pi.w * OPC_Q_H, qm = pi.w * OPC_Q_EP;
-        const double eh = (double)pi.w * (double)OPC_Q_H, em = (double)pi.w * (double)OPC_Q_EP;
-        float3 f = f3(0, 0, 0);
+    for (uint32_t it = ((bk.idx * blockDim.x + threadIdx.x) >> 5); it < nit; it += nwarps) {
+        const uint2 item = v.ws_item[it];
+        const uint32_t ci = item.x, k0 = item.y;
+        const uint32_t n = min(v.ws_n[ci], k0 + CH_MIX) - k0;
+        const uint32_t si = ci * WCL + ii;
+        const bool vi = v.wid[si] != INVALID_ID;
+        const float3 iO = xyz(v.wpos[4 * si + 0]), iH0 = xyz(v.wpos[4 * si + 1]);
+        const float3 iH1 = xyz(v.wpos[4 * si + 2]), iM = xyz(v.wpos[4 * si + 3]);
+        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
         Acc3 a{0.0, 0.0, 0.f};
-        const uint32_t* lst = v.sw_j + (size_t)ci * v.cap_sw;
-        for (uint32_t k = k0; k < n; ++k) {
-            const uint32_t cj = lst[k];
-            float wf[24];
+        const uint32_t my_j = (uint32_t)lane < n ? v.ws_j[(size_t)ci * v.cap_ws + k0 + lane] : 0u;
+        JAtoms nx = load_jatoms(v, __shfl_sync(0xffffffffu, my_j, 0), jq);
+        for (uint32_t k = 0; k < n; ++k) {
+            const JAtoms cur = nx;
+            if (k + 1 < n) nx = load_jatoms(v, __shfl_sync(0xffffffffu, my_j, k + 1), jq);
+            float jf[8];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                const uint32_t sj = cj * WCL + jq + 4 * h;
+                const float4 pj = h ? cur.p1 : cur.p0;
+                const float2 lj_j = h ? cur.l1 : cur.l0;
+                const uint32_t aj = h ? cur.a1 : cur.a0;
                 float3 fo = f3(0, 0, 0), f0 = fo, f1 = fo, fm = fo;
-                if (vi && v.wid[sj] != INVALID_ID) {
-                    const float3 jO = xyz(v.wpos[4 * sj + 0]);
-                    const float3 s = shift_of(xyz(pi) - jO, b);
-                    lj<ENERGY>(xyz(pi), jO, s, sg * sg, ep, ljc2, 1.0f, fo, a);
-                    coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 1]), s, qh, eh, v, f0, a);
-                    coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 2]), s, qh, eh, v, f1, a);
-                    coul<ENERGY>(xyz(pi), xyz(v.wpos[4 * sj + 3]), s, qm, em, v, fm, a);
+                if (vi && aj != INVALID_ID) {
+                    const float3 jp = xyz(pj);
+                    const float3 s = shift_of(iO - jp, b);
+                    const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
+                    const float ep = sqrtf(OPC_O_EPS * lj_j.y);
+                    const double qe = (double)pj.w;
+                    lj<ENERGY>(iO, jp, s, sg * sg, ep, ljc2, 1.0f, fo, a);
+                    coul<ENERGY>(iH0, jp, s, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
+                    coul<ENERGY>(iH1, jp, s, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
+                    coul<ENERGY>(iM, jp, s, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
                 }
-                f = f + ((fo + f0) + (f1 + fm));
-                const float3 q[4] = {fo, f0, f1, fm};
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    wf[12 * h + 3 * t + 0] = -q[t].x;
-                    wf[12 * h + 3 * t + 1] = -q[t].y;
-                    wf[12 * h + 3 * t + 2] = -q[t].z;
-                }
+                fO = fO + fo; fH0 = fH0 + f0; fH1 = fH1 + f1; fM = fM + fm;
+                const float3 t = (fo + f0) + (f1 + fm);
+                jf[3 * h + 0] = -t.x; jf[3 * h + 1] = -t.y; jf[3 * h + 2] = -t.z;
             }
-            // lane ii now holds site (ii & 3) of water jq + 4 (ii >> 2)
-            reduce_scatter8(wf, ii);
-            const uint32_t sj = cj * WCL + jq + 4 * (ii >> 2);
-            if (v.wid[sj] != INVALID_ID) {
-                long long* p = v.wforce + (size_t)sj * 12 + 3 * (ii & 3);
-                add_fix(p + 0, wf[0]); add_fix(p + 1, wf[1]); add_fix(p + 2, wf[2]);
+            jf[6] = 0.f; jf[7] = 0.f;
+            // lane ii < 6 now holds component ii % 3 of atom jq + 4 (ii / 3)
+            reduce_scatter8(jf, ii);
+            if (ii < 6) {
+                const uint32_t aj = ii < 3 ? cur.a0 : cur.a1;
+                if (aj != INVALID_ID) add_fix(v.aforce + 3 * (size_t)aj + ii % 3, jf[0]);
             }
         }
-        f = f3(red4(f.x), red4(f.y), red4(f.z));
-        if (jq == 0 && vi) add_fix3(v.aforce + 3 * (size_t)ai, f);
+        fO = f3(red4(fO.x), red4(fO.y), red4(fO.z));
+        fH0 = f3(red4(fH0.x), red4(fH0.y), red4(fH0.z));
+        fH1 = f3(red4(fH1.x), red4(fH1.y), red4(fH1.z));
+        fM = f3(red4(fM.x), red4(fM.y), red4(fM.z));
+        if (jq == 0 && vi) {
+            long long* p = v.wforce + (size_t)si * 12;
+            add_fix3(p + 0, fO); add_fix3(p + 3, fH0); add_fix3(p + 6, fH1); add_fix3(p + 9, fM);
+        }
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
     }
-    write_partials<ENERGY>(v, bk, REG_SW, el, ec, ew);
+    write_partials<ENERGY>(v, bk, REG_WS, el, ec, ew);
 }
 
 // ---------------------------------------------------------------------------
 // atom(i) - atom(j), each pair once (cluster pairs with cj >= ci; the
 // interaction mask from the list build holds jj > ii on the diagonal and
-// drops exclusions); j forces go out through integer atomics as above.
+// drops exclusions); work items, prefetch and j-side atomics as above.
 // ---------------------------------------------------------------------------
 DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) {
     const int lane = threadIdx.x & 31;
     const int ii = lane & 7, jq = lane >> 3;
     const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
-    const uint32_t nac = v.sc->n_aclus;
-    const uint32_t nch = (v.cap_ss + CH_MIX - 1) / CH_MIX;
+    const uint32_t nit = v.sc->n_ss_items;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0;
-    for (uint32_t wv = ((bk.idx * blockDim.x + threadIdx.x) >> 5); wv < nac * nch; wv += nwarps) {
-        const uint32_t ci = wv / nch, k0 = (wv % nch) * CH_MIX;
-        const uint32_t n = min(v.ss_n[ci], k0 + CH_MIX);
-        if (n <= k0) continue;
+    for (uint32_t it = ((bk.idx * blockDim.x + threadIdx.x) >> 5); it < nit; it += nwarps) {
+        const uint2 item = v.ss_item[it];
+        const uint32_t ci = item.x, k0 = item.y;
+        const uint32_t n = min(v.ss_n[ci], k0 + CH_MIX) - k0;
         const uint32_t si = ci * ACL + ii;
         const uint32_t ai = v.sidx[si];
         const float4 pi = v.spos[si];
         const float2 lji = v.slj[si];
         float3 f = f3(0, 0, 0);
         Acc3 a{0.0, 0.0, 0.f};
-        const uint32_t* lst = v.ss_j + (size_t)ci * v.cap_ss;
-        const unsigned long long* msk = v.ss_mask + (size_t)ci * v.cap_ss;
-        for (uint32_t k = k0; k < n; ++k) {
-            const uint32_t cj = lst[k];
-            const unsigned long long m = msk[k];
+        const size_t row = (size_t)ci * v.cap_ss + k0;
+        const uint32_t my_j = (uint32_t)lane < n ? v.ss_j[row + lane] : 0u;
+        const unsigned long long my_m = (uint32_t)lane < n ? v.ss_mask[row + lane] : 0ull;
+        JAtoms nx = load_jatoms(v, __shfl_sync(0xffffffffu, my_j, 0), jq);
+        for (uint32_t k = 0; k < n; ++k) {
+            const JAtoms cur = nx;
+            const unsigned long long m = __shfl_sync(0xffffffffu, my_m, k);
+            if (k + 1 < n) nx = load_jatoms(v, __shfl_sync(0xffffffffu, my_j, k + 1), jq);
             float jf[8];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int jj = jq + 4 * h;
+                const float4 pj = h ? cur.p1 : cur.p0;
+                const float2 ljj = h ? cur.l1 : cur.l0;
                 float3 fp = f3(0, 0, 0);
                 if ((m >> (ii * ACL + jj)) & 1ull) {
-                    const uint32_t sj = cj * ACL + jj;
-                    const float4 pj = v.spos[sj];
-                    const float2 ljj = v.slj[sj];
                     const float3 s = shift_of(xyz(pi) - xyz(pj), b);
                     const float sg = 0.5f * (lji.x + ljj.x);
                     lj<ENERGY>(xyz(pi), xyz(pj), s, sg * sg, sqrtf(lji.y * ljj.y), ljc2, 1.0f, fp, a);
@@ -438,7 +452,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) 
             // lane ii < 6 now holds component ii % 3 of atom jq + 4 (ii / 3)
             reduce_scatter8(jf, ii);
             if (ii < 6) {
-                const uint32_t aj = v.sidx[cj * ACL + jq + 4 * (ii / 3)];
+                const uint32_t aj = ii < 3 ? cur.a0 : cur.a1;
                 if (aj != INVALID_ID) add_fix(v.aforce + 3 * (size_t)aj + ii % 3, jf[0]);
             }
         }
@@ -487,7 +501,7 @@ inline int pblocks(const SysView& v, uint64_t warps) {
 
 namespace dyn {
 
-int pair_blocks_sw(const SysView& v) { return pblocks(v, (uint64_t)v.naclus_cap * ((v.cap_sw + CH_MIX - 1) / CH_MIX)); }
+int pair_blocks_ws(const SysView& v) { return pblocks(v, v.ws_item_cap); }
 
 int ww_tile_blocks(const SysView& v) {
     return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
@@ -513,7 +527,7 @@ int pair_ww_setup(const SysView& v) {
     }
     return DYN_OK;
 }
-int pair_blocks_ss(const SysView& v) { return pblocks(v, (uint64_t)v.naclus_cap * ((v.cap_ss + CH_MIX - 1) / CH_MIX)); }
+int pair_blocks_ss(const SysView& v) { return pblocks(v, v.ss_item_cap); }
 int pair14_blocks(const SysView& v) {
     uint64_t bl = (v.n14 + 255) / 256;
     if (bl < 1) bl = 1;
@@ -531,14 +545,14 @@ void launch_pairs(const Target& t, bool energy) {
     t.launch(k_pair_ww_tile<false>, k_pair_ww_tile_batch<false>,
              [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
     auto ss = [](const SysView& v) { return v.na ? (int)v.nb[REG_SS] : 0; };
-    auto sw = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_SW] : 0; };
-    // the mixed kernels add to the water forces the water-water kernel stores
+    auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
+    // the water-atom kernel adds to the water forces the water-water kernel stores
     if (energy) {
         t.launch(k_pair_ss<true>, k_pair_ss_batch<true>, ss, PT, 0);
-        t.launch(k_pair_sw<true>, k_pair_sw_batch<true>, sw, PT, 0);
+        t.launch(k_pair_ws<true>, k_pair_ws_batch<true>, ws, PT, 0);
     } else {
         t.launch(k_pair_ss<false>, k_pair_ss_batch<false>, ss, PT, 0);
-        t.launch(k_pair_sw<false>, k_pair_sw_batch<false>, sw, PT, 0);
+        t.launch(k_pair_ws<false>, k_pair_ws_batch<false>, ws, PT, 0);
     }
 }
 

@@ -81,8 +81,8 @@ void host_m_site(const float* o, const float* h0, const float* h1, float* m) {
 void set_block_counts(SysView& v) {
     for (int r = 0; r < NREGION; ++r) v.nb[r] = 0;
     v.nb[REG_WW] = v.nw ? dyn::ww_tile_blocks(v) : 0;
-    v.nb[REG_WS] = 0;
-    v.nb[REG_SW] = (v.nw && v.na) ? dyn::pair_blocks_sw(v) : 0;
+    v.nb[REG_WS] = (v.nw && v.na) ? dyn::pair_blocks_ws(v) : 0;
+    v.nb[REG_SW] = 0;
     v.nb[REG_SS] = v.na ? dyn::pair_blocks_ss(v) : 0;
     v.nb[REG_14] = v.n14 ? dyn::pair14_blocks(v) : 0;
     v.nb[REG_BOND] = (v.nbond + v.nangle + v.ndih) ? dyn::bond_blocks(v) : 0;
@@ -478,8 +478,10 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         if ((uint64_t)n_i * n_j <= (1ull << 24)) return std::max(1u, n_j);
         return est(r, vol_cl, n_j);
     };
-    v.cap_sw = (v.nw && v.na) ? cap_mixed(v.r_ws, wcl_vol, v.naclus_cap, v.nwclus_cap) : 1;
+    v.cap_ws = (v.nw && v.na) ? cap_mixed(v.r_ws, acl_vol, v.nwclus_cap, v.naclus_cap) : 1;
     v.cap_ss = v.na ? cap_mixed(v.r_ss, acl_vol, v.naclus_cap, v.naclus_cap) : 1;
+    v.ws_item_cap = v.nwclus_cap * ((v.cap_ws + CH_MIX - 1) / CH_MIX);
+    v.ss_item_cap = v.naclus_cap * ((v.cap_ss + CH_MIX - 1) / CH_MIX);
 
     // ---- allocations ----
     TRY(dev_alloc(h, &v.wpos, 4 * (size_t)v.nw_cap));
@@ -536,8 +538,10 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dev_alloc(h, &v.cand_loc, (size_t)v.ngrp_cap * v.cap_tile * WCL));
     TRY(dev_alloc(h, &v.wnb_n, v.nw_cap));
     TRY(dev_alloc(h, &v.wnb, (size_t)v.nw_cap * v.cap_nb));
-    TRY(dev_alloc(h, &v.sw_n, v.naclus_cap));
-    TRY(dev_alloc(h, &v.sw_j, (size_t)v.naclus_cap * v.cap_sw));
+    TRY(dev_alloc(h, &v.ws_n, v.nwclus_cap));
+    TRY(dev_alloc(h, &v.ws_j, (size_t)v.nwclus_cap * v.cap_ws));
+    TRY(dev_alloc(h, &v.ws_item, std::max(1u, v.ws_item_cap)));
+    TRY(dev_alloc(h, &v.ss_item, std::max(1u, v.ss_item_cap)));
     TRY(dev_alloc(h, &v.ss_n, v.naclus_cap));
     TRY(dev_alloc(h, &v.ss_j, (size_t)v.naclus_cap * v.cap_ss));
     TRY(dev_alloc(h, &v.ss_mask, (size_t)v.naclus_cap * v.cap_ss));
