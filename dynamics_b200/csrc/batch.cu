@@ -58,6 +58,7 @@ struct dyn_batch_s {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t aux = nullptr;
+    Branches br;
     std::vector<dyn_sys_t> members;
     BatchCtx ctx;
     SysView* d_views[4] = {nullptr, nullptr, nullptr, nullptr};  // one per graph variant
@@ -98,22 +99,18 @@ int upload_maps(dyn_batch_s* b) {
 int enqueue_batch_step(dyn_batch_s* b, float dt, bool spme, bool energy, bool cond,
                        cudaGraphConditionalHandle c_rebuild, cudaGraphConditionalHandle c_periodic) {
     const Target T{nullptr, &b->ctx, b->stream}, TA{nullptr, &b->ctx, b->aux};
+    const Target S0{nullptr, &b->ctx, b->br.side[0]}, S1{nullptr, &b->ctx, b->br.side[1]};
     cudaGraph_t body = nullptr;
     int rc = DYN_OK;
-    dyn::launch_first_half(T, dt);
+    // cond: capturing (parallel branches); otherwise a collecting pass
+    if ((rc = dyn::enqueue_first_half(T, S0, b->br, cond, dt)) != DYN_OK) return rc;
     dyn::launch_displacement_check(T);
     if (cond && (rc = dyn::begin_if_body(b->stream, b->aux, c_rebuild, &body)) != DYN_OK) return rc;
     dyn::launch_rebuild(cond ? TA : T, false);
     if (cond && (rc = dyn::end_if_body(b->aux)) != DYN_OK) return rc;
     dyn::launch_gather_atoms(T);
-    dyn::launch_pairs(T, energy);
-    dyn::launch_pair14(T, energy);
-    dyn::launch_bonded(T, energy);
-    if (spme) {
-        dyn::launch_pme(T);
-        dyn::launch_corrections(T);
-    }
-    dyn::launch_second_half(T, dt);
+    if ((rc = dyn::enqueue_forces(T, S0, S1, b->br, cond, spme, energy)) != DYN_OK) return rc;
+    if ((rc = dyn::enqueue_second_half(T, S0, b->br, cond, dt)) != DYN_OK) return rc;
     dyn::launch_finalize(T, dt, energy, true);
     if (cond && (rc = dyn::begin_if_body(b->stream, b->aux, c_periodic, &body)) != DYN_OK) return rc;
     dyn::launch_periodic(cond ? TA : T);
@@ -202,6 +199,7 @@ extern "C" int dyn_batch_destroy(dyn_batch_t b) {
     for (void* p : b->map_allocs) cudaFree(p);
     for (dyn_sys_t m : b->members) dyn_sys_destroy(m);
     if (b->aux) cudaStreamDestroy(b->aux);
+    b->br.destroy();
     if (b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return DYN_OK;
@@ -226,6 +224,8 @@ extern "C" int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cf
     {
         const cudaError_t e = cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking);
         if (e != cudaSuccess) { dyn_batch_destroy(b); return dyn::cuda_fail(e, "cudaStreamCreateWithFlags"); }
+        const int rc = b->br.create();
+        if (rc != DYN_OK) { dyn_batch_destroy(b); return rc; }
     }
     if (n > 0) {
         b->spme_interval = std::max(1u, cfgs[0].spme_interval);

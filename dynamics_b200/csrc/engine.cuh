@@ -299,6 +299,10 @@ void launch_gather_atoms(const Target& t);
 
 // pair.cu
 void launch_pairs(const Target& t, bool energy);
+// the two independent parts of launch_pairs: water-water then water-atom
+// (the latter adds to the water forces the former stores), and atom-atom
+void launch_pairs_water(const Target& t, bool energy);
+void launch_pairs_atoms(const Target& t, bool energy);
 void launch_pair14(const Target& t, bool energy);
 int pair_ww_setup(const SysView& v);
 int ww_tile_blocks(const SysView& v);
@@ -318,6 +322,11 @@ int corr_blocks(const SysView& v);
 // integrate.cu
 void launch_first_half(const Target& t, float dt);
 void launch_second_half(const Target& t, float dt);
+// their water and atom parts, which touch disjoint data
+void launch_first_half_water(const Target& t, float dt);
+void launch_first_half_atoms(const Target& t, float dt);
+void launch_second_half_water(const Target& t, float dt);
+void launch_second_half_atoms(const Target& t, float dt);
 void launch_finalize(const Target& t, float dt, bool energy, bool thermo);
 void launch_periodic(const Target& t);
 void launch_bonded(const Target& t, bool energy);

@@ -695,18 +695,30 @@ namespace dyn {
 int kick_blocks_w(const SysView& v) { return iblocks(v, v.nw_cap); }
 int kick_blocks_a(const SysView& v) { return iblocks(v, v.nunit); }
 
-void launch_first_half(const Target& t, float dt) {
+void launch_first_half_water(const Target& t, float dt) {
     t.launch(k_water_first, k_water_first_batch, [](const SysView& v) { return v.nw ? iblocks(v, v.nw_cap) : 0; },
              IT, 0, dt);
+}
+void launch_first_half_atoms(const Target& t, float dt) {
     t.launch(k_atom_first, k_atom_first_batch, [](const SysView& v) { return v.na ? (int)v.nb[REG_CONS] : 0; },
              IT, 0, dt);
 }
+void launch_first_half(const Target& t, float dt) {
+    launch_first_half_water(t, dt);
+    launch_first_half_atoms(t, dt);
+}
 
-void launch_second_half(const Target& t, float dt) {
+void launch_second_half_water(const Target& t, float dt) {
     t.launch(k_water_kick, k_water_kick_batch, [](const SysView& v) { return v.nw ? (int)v.nb[REG_KICK_W] : 0; },
              IT, 0, dt);
+}
+void launch_second_half_atoms(const Target& t, float dt) {
     t.launch(k_atom_kick, k_atom_kick_batch, [](const SysView& v) { return v.na ? (int)v.nb[REG_KICK_A] : 0; }, IT,
              0, dt);
+}
+void launch_second_half(const Target& t, float dt) {
+    launch_second_half_water(t, dt);
+    launch_second_half_atoms(t, dt);
 }
 
 void launch_finalize(const Target& t, float dt, bool energy, bool thermo) {

@@ -535,6 +535,17 @@ int pair14_blocks(const SysView& v) {
 }
 
 void launch_pairs(const Target& t, bool energy) {
+    launch_pairs_water(t, energy);
+    launch_pairs_atoms(t, energy);
+}
+
+void launch_pairs_atoms(const Target& t, bool energy) {
+    auto ss = [](const SysView& v) { return v.na ? (int)v.nb[REG_SS] : 0; };
+    if (energy) t.launch(k_pair_ss<true>, k_pair_ss_batch<true>, ss, PT, 0);
+    else t.launch(k_pair_ss<false>, k_pair_ss_batch<false>, ss, PT, 0);
+}
+
+void launch_pairs_water(const Target& t, bool energy) {
     const size_t sm = t.max_over([](const SysView& v) { return v.nw ? ww_tile_smem(v) : (size_t)0; });
     // water-water short-range energy is part of the potential only with
     // DYN_FLAG_FULL_ENERGY (the reference leaves it out,
@@ -544,16 +555,10 @@ void launch_pairs(const Target& t, bool energy) {
              [&](const SysView& v) { return v.nw && eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
     t.launch(k_pair_ww_tile<false>, k_pair_ww_tile_batch<false>,
              [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
-    auto ss = [](const SysView& v) { return v.na ? (int)v.nb[REG_SS] : 0; };
     auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
     // the water-atom kernel adds to the water forces the water-water kernel stores
-    if (energy) {
-        t.launch(k_pair_ss<true>, k_pair_ss_batch<true>, ss, PT, 0);
-        t.launch(k_pair_ws<true>, k_pair_ws_batch<true>, ws, PT, 0);
-    } else {
-        t.launch(k_pair_ss<false>, k_pair_ss_batch<false>, ss, PT, 0);
-        t.launch(k_pair_ws<false>, k_pair_ws_batch<false>, ws, PT, 0);
-    }
+    if (energy) t.launch(k_pair_ws<true>, k_pair_ws_batch<true>, ws, PT, 0);
+    else t.launch(k_pair_ws<false>, k_pair_ws_batch<false>, ws, PT, 0);
 }
 
 void launch_pair14(const Target& t, bool energy) {

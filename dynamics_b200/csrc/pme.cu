@@ -409,9 +409,18 @@ void launch_pme(const Target& t) {
              GT, 0);
     t.launch(k_fix2real, k_fix2real_batch,
              [](const SysView& v) { return gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]); }, GT, 0);
-    t.each([](const SysView& v) { cufftExecR2C(v.plan_f, v.qgrid, (cufftComplex*)v.cgrid); });
+    // the plans run on the target's stream (a graph branch may differ from
+    // the stream the plans were made on)
+    const cudaStream_t st = t.st;
+    t.each([st](const SysView& v) {
+        cufftSetStream(v.plan_f, st);
+        cufftExecR2C(v.plan_f, v.qgrid, (cufftComplex*)v.cgrid);
+    });
     t.launch(k_convolve, k_convolve_batch, [](const SysView& v) { return (int)v.nb[REG_PME]; }, GT, 0);
-    t.each([](const SysView& v) { cufftExecC2R(v.plan_b, (cufftComplex*)v.cgrid, v.qgrid); });
+    t.each([st](const SysView& v) {
+        cufftSetStream(v.plan_b, st);
+        cufftExecC2R(v.plan_b, (cufftComplex*)v.cgrid, v.qgrid);
+    });
     t.launch(k_gather, k_gather_batch, [](const SysView& v) { return (int)v.nb[REG_CORR]; }, GT, 0);
 }
 

@@ -6,10 +6,21 @@
 
 #include "engine.cuh"
 
+// Side streams and events that split a captured step into parallel graph
+// branches (the atom half of the integrator, the atom-atom / 1-4 / bonded
+// terms and SPME run beside the water work).
+struct Branches {
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev[8] = {};
+    int create();
+    void destroy();
+};
+
 struct dyn_sys_s {
     cudaStream_t stream = nullptr;
     bool own_stream = false;       // created here because the caller passed NULL
     cudaStream_t aux = nullptr;    // captures the bodies of conditional graph nodes
+    Branches br;
     SysView v{};
     dyn_config_t cfg{};
     cufftHandle plan_f = 0, plan_b = 0;
@@ -31,5 +42,19 @@ int end_if_body(cudaStream_t aux);
 int read_scalars(dyn_sys_s* h);
 // Kernel nodes of a graph (library kernels included).
 int count_graph_kernels(cudaGraph_t g, uint32_t* n);
+
+// The parts of a step, enqueued on T's stream; with fork (only while a graph
+// is being captured) the independent work goes to the side targets A and P
+// (same systems, the side streams of br) as parallel branches that join
+// back into T.  The launch order is the same either way, which a batch needs
+// (it records its block maps in launch order).
+//   first half:  water drift/thermostat on T | atom drift + constraints on A
+//   forces:      water-water, water-atom on T | atom-atom, 1-4, bonded on A |
+//                SPME and its corrections on P (spme steps)
+//   second half: water kick on T | atom kick + RATTLE on A
+int enqueue_first_half(const Target& T, const Target& A, const Branches& br, bool fork, float dt);
+int enqueue_forces(const Target& T, const Target& A, const Target& P, const Branches& br, bool fork, bool spme,
+                   bool energy);
+int enqueue_second_half(const Target& T, const Target& A, const Branches& br, bool fork, float dt);
 
 }  // namespace dyn

@@ -128,7 +128,66 @@ int end_if_body(cudaStream_t aux) {
     DYN_CUDA(cudaStreamEndCapture(aux, &g));
     return DYN_OK;
 }
+
+// Work enqueued on `to` after this call depends on everything enqueued on
+// `from` before it.
+static int link_streams(cudaStream_t from, cudaStream_t to, cudaEvent_t e) {
+    DYN_CUDA(cudaEventRecord(e, from));
+    DYN_CUDA(cudaStreamWaitEvent(to, e, 0));
+    return DYN_OK;
+}
+
+int enqueue_first_half(const Target& T, const Target& A, const Branches& br, bool fork, float dt) {
+    int rc;
+    if (fork && (rc = link_streams(T.st, A.st, br.ev[0])) != DYN_OK) return rc;
+    launch_first_half_water(T, dt);
+    launch_first_half_atoms(fork ? A : T, dt);
+    if (fork && (rc = link_streams(A.st, T.st, br.ev[1])) != DYN_OK) return rc;
+    return DYN_OK;
+}
+
+int enqueue_forces(const Target& T, const Target& A, const Target& P, const Branches& br, bool fork, bool spme,
+                   bool energy) {
+    int rc;
+    if (fork && (rc = link_streams(T.st, A.st, br.ev[2])) != DYN_OK) return rc;
+    if (fork && spme && (rc = link_streams(T.st, P.st, br.ev[3])) != DYN_OK) return rc;
+    const Target& a = fork ? A : T;
+    const Target& p = fork ? P : T;
+    if (spme) {
+        launch_pme(p);
+        launch_corrections(p);
+    }
+    launch_pairs_atoms(a, energy);
+    launch_pair14(a, energy);
+    launch_bonded(a, energy);
+    launch_pairs_water(T, energy);
+    if (fork && (rc = link_streams(A.st, T.st, br.ev[4])) != DYN_OK) return rc;
+    if (fork && spme && (rc = link_streams(P.st, T.st, br.ev[5])) != DYN_OK) return rc;
+    return DYN_OK;
+}
+
+int enqueue_second_half(const Target& T, const Target& A, const Branches& br, bool fork, float dt) {
+    int rc;
+    if (fork && (rc = link_streams(T.st, A.st, br.ev[6])) != DYN_OK) return rc;
+    launch_second_half_water(T, dt);
+    launch_second_half_atoms(fork ? A : T, dt);
+    if (fork && (rc = link_streams(A.st, T.st, br.ev[7])) != DYN_OK) return rc;
+    return DYN_OK;
+}
 }  // namespace dyn
+
+int Branches::create() {
+    for (int i = 0; i < 2; ++i) DYN_CUDA(cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking));
+    for (int i = 0; i < 8; ++i) DYN_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+    return DYN_OK;
+}
+
+void Branches::destroy() {
+    for (int i = 0; i < 2; ++i)
+        if (side[i]) { cudaStreamDestroy(side[i]); side[i] = nullptr; }
+    for (int i = 0; i < 8; ++i)
+        if (ev[i]) { cudaEventDestroy(ev[i]); ev[i] = nullptr; }
+}
 namespace {
 
 // Captures one step (MdState::step, src/integrate.rs:100-473) into a graph.
@@ -143,6 +202,7 @@ int capture_step(dyn_sys_s* h, float dt, bool spme, bool energy, cudaGraph_t* ou
     cudaStream_t st = h->stream;
     const Target T{&v, nullptr, st};
     const Target TA{&v, nullptr, h->aux};
+    const Target S0{&v, nullptr, h->br.side[0]}, S1{&v, nullptr, h->br.side[1]};
     *out = nullptr;
     DYN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = DYN_OK;
@@ -157,20 +217,14 @@ int capture_step(dyn_sys_s* h, float dt, bool spme, bool energy, cudaGraph_t* ou
             e = cudaGraphConditionalHandleCreate(&v.cond_periodic, cg, 0, cudaGraphCondAssignDefault);
         if (e != cudaSuccess) { rc = dyn::cuda_fail(e, "cudaGraphConditionalHandleCreate"); break; }
         v.use_cond = 1;
-        dyn::launch_first_half(T, dt);
+        if ((rc = dyn::enqueue_first_half(T, S0, h->br, true, dt)) != DYN_OK) break;
         dyn::launch_displacement_check(T);
         if ((rc = begin_if_body(st, h->aux, v.cond_rebuild, &br)) != DYN_OK) break;
         dyn::launch_rebuild(TA, false);
         if ((rc = end_if_body(h->aux)) != DYN_OK) break;
         dyn::launch_gather_atoms(T);
-        dyn::launch_pairs(T, energy);
-        dyn::launch_pair14(T, energy);
-        dyn::launch_bonded(T, energy);
-        if (spme) {
-            dyn::launch_pme(T);
-            dyn::launch_corrections(T);
-        }
-        dyn::launch_second_half(T, dt);
+        if ((rc = dyn::enqueue_forces(T, S0, S1, h->br, true, spme, energy)) != DYN_OK) break;
+        if ((rc = dyn::enqueue_second_half(T, S0, h->br, true, dt)) != DYN_OK) break;
         dyn::launch_finalize(T, dt, energy, true);
         if ((rc = begin_if_body(st, h->aux, v.cond_periodic, &bp)) != DYN_OK) break;
         dyn::launch_periodic(TA);
@@ -267,6 +321,7 @@ extern "C" int dyn_sys_destroy(dyn_sys_t h) {
     if (h->h_sc) cudaFreeHost(h->h_sc);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     if (h->aux) cudaStreamDestroy(h->aux);
+    h->br.destroy();
     delete h;
     return DYN_OK;
 }
@@ -347,6 +402,11 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
             if (h->own_stream) cudaStreamDestroy(h->stream);
             delete h;
             return dyn::cuda_fail(e, "cudaStreamCreateWithFlags");
+        }
+        const int rc = h->br.create();
+        if (rc != DYN_OK) {
+            dyn_sys_destroy(h);
+            return rc;
         }
     }
     h->cfg = *cfg;
@@ -1150,6 +1210,8 @@ int count_step_kernels(dyn_sys_s* h, bool spme, uint32_t* fixed, uint32_t* rebui
         if (rc) return rc;
         if (spme) {
             rc = count([&] {
+                cufftSetStream(h->plan_f, st);
+                cufftSetStream(h->plan_b, st);
                 cufftExecR2C(h->plan_f, h->v.qgrid, (cufftComplex*)h->v.cgrid);
                 cufftExecC2R(h->plan_b, (cufftComplex*)h->v.cgrid, h->v.qgrid);
             }, &fft);
