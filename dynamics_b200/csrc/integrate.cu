@@ -185,7 +185,9 @@ __device__ __forceinline__ double constrain_unit(Unit& U, uint32_t order, uint32
     if (U.n < 2) return 0.0;
     const float3 x0 = U.x[0];
     for (uint32_t o = 0; o < order; ++o) {
-        for (int k = 1; k < U.n; ++k) {
+#pragma unroll
+        for (int k = 1; k < UMAX; ++k) {
+            if (k >= U.n) break;
             const float3 d = U.x[k] - U.x[0];
             const float dl = fmaxf(sqrtf(dot3(d, d)), 1.1920929e-7f);
             const float3 bv = d * (1.0f / dl);
@@ -197,7 +199,9 @@ __device__ __forceinline__ double constrain_unit(Unit& U, uint32_t order, uint32
         }
     }
     for (uint32_t it = 0; it < iter; ++it) {
-        for (int k = 1; k < U.n; ++k) {
+#pragma unroll
+        for (int k = 1; k < UMAX; ++k) {
+            if (k >= U.n) break;
             const float3 d = U.x[k] - U.x[0];
             const float d2 = dot3(d, d);
             const float im = 1.0f / U.m[0] + 1.0f / U.m[k];
@@ -209,14 +213,18 @@ __device__ __forceinline__ double constrain_unit(Unit& U, uint32_t order, uint32
     }
     const float3 fi = (U.x[0] - x0) * (U.m[0] * inv_dt2);
     double w = 0.0;
-    for (int k = 1; k < U.n; ++k) w += (double)dot3(U.x[k] - U.x[0], fi);
+#pragma unroll
+    for (int k = 1; k < UMAX; ++k)
+        if (k < U.n) w += (double)dot3(U.x[k] - U.x[0], fi);
     return w;
 }
 
 // rattle_hydrogens (src/bonded.rs:288-304): remove the velocity component
 // along each constrained bond
 __device__ __forceinline__ void rattle_unit(Unit& U) {
-    for (int k = 1; k < U.n; ++k) {
+#pragma unroll
+    for (int k = 1; k < UMAX; ++k) {
+        if (k >= U.n) break;
         const float3 r = U.x[k] - U.x[0];
         const float3 dv = U.vel[k] - U.vel[0];
         const float r2 = dot3(r, r);
@@ -244,7 +252,9 @@ DYN_KERNEL(, k_atom_first, (, float dt), (, dt)) {
     for (uint32_t u = bk.idx * blockDim.x + threadIdx.x; u < v.nunit; u += bk.cnt * blockDim.x) {
         Unit U;
         load_unit(v, u, U);
-        for (int k = 0; k < U.n; ++k) {
+#pragma unroll
+        for (int k = 0; k < UMAX; ++k) {
+            if (k >= U.n) break;
             if (U.fixed[k]) continue;
             U.vel[k] = U.vel[k] + xyz(v.aacc[U.id[k]]) * hk;
             U.x[k] = U.x[k] + U.vel[k] * (lm ? hk : dt);
@@ -252,17 +262,22 @@ DYN_KERNEL(, k_atom_first, (, float dt), (, dt)) {
         vir += constrain_unit(U, v.lincs_order, v.lincs_iter, inv_dt2);
         rattle_unit(U);
         if (lm) {
-            for (int k = 0; k < U.n; ++k) {
+#pragma unroll
+            for (int k = 0; k < UMAX; ++k) {
+                if (k >= U.n) break;
                 if (U.fixed[k]) continue;
                 const float sg = sqrtf(num / U.m[k]);
                 U.vel[k] = U.vel[k] * c + ou_normals(U.id[k], step, v.seed) * sg;
             }
             rattle_unit(U);
-            for (int k = 0; k < U.n; ++k)
-                if (!U.fixed[k]) U.x[k] = U.x[k] + U.vel[k] * hk;
+#pragma unroll
+            for (int k = 0; k < UMAX; ++k)
+                if (k < U.n && !U.fixed[k]) U.x[k] = U.x[k] + U.vel[k] * hk;
             constrain_unit(U, v.lincs_order, v.lincs_iter, inv_dt2);
         }
-        for (int k = 0; k < U.n; ++k) {
+#pragma unroll
+        for (int k = 0; k < UMAX; ++k) {
+            if (k >= U.n) break;
             const uint32_t a = U.id[k];
             if (U.fixed[k]) continue;
             v.apos[a] = make_float4(U.x[k].x, U.x[k].y, U.x[k].z, v.apos[a].w);
@@ -345,7 +360,9 @@ DYN_KERNEL(, k_atom_kick, (, float dt), (, dt)) {
     for (uint32_t u = bk.idx * blockDim.x + threadIdx.x; u < v.nunit; u += bk.cnt * blockDim.x) {
         Unit U;
         load_unit(v, u, U);
-        for (int k = 0; k < U.n; ++k) {
+#pragma unroll
+        for (int k = 0; k < UMAX; ++k) {
+            if (k >= U.n) break;
             if (U.fixed[k]) continue;
             const uint32_t a = U.id[k];
             const float3 f = ldfix3sum(v.aforce + 3 * (size_t)a, v.arecip + 3 * (size_t)a);
@@ -358,7 +375,9 @@ DYN_KERNEL(, k_atom_kick, (, float dt), (, dt)) {
             if (!finite3(acc)) v.sc->nonfinite = 1u;
         }
         rattle_unit(U);  // src/integrate.rs:554-559
-        for (int k = 0; k < U.n; ++k) {
+#pragma unroll
+        for (int k = 0; k < UMAX; ++k) {
+            if (k >= U.n) break;
             if (U.fixed[k]) continue;
             v.avel[U.id[k]] = make_float4(U.vel[k].x, U.vel[k].y, U.vel[k].z, 0.f);
             ke += (double)(U.m[k] * dot3(U.vel[k], U.vel[k]));
@@ -376,10 +395,23 @@ DYN_KERNEL(, k_atom_kick, (, float dt), (, dt)) {
 // finalize: fixed-order sums of all partials, pressure, temperature, CSVR
 // and C-rescale scalars (single block)
 // ---------------------------------------------------------------------------
+// Adds this thread's share of a region's block partials to out, four
+// partials in flight at a time (the loads are independent; the sum order per
+// thread is fixed).
 __device__ __forceinline__ void region_sum(const SysView& v, int reg, double* out) {
-    for (uint32_t i = threadIdx.x; i < v.nb[reg]; i += blockDim.x) {
-        const double* p = v.partials + ((size_t)reg * v.max_blocks + i) * 4;
-        out[0] += p[0]; out[1] += p[1]; out[2] += p[2]; out[3] += p[3];
+    const double4* p = reinterpret_cast<const double4*>(v.partials) + (size_t)reg * v.max_blocks;
+    const uint32_t n = v.nb[reg], st = blockDim.x;
+    uint32_t i = threadIdx.x;
+    for (; i + 3 * st < n; i += 4 * st) {
+        const double4 a = p[i], b = p[i + st], c = p[i + 2 * st], d = p[i + 3 * st];
+        out[0] += a.x; out[1] += a.y; out[2] += a.z; out[3] += a.w;
+        out[0] += b.x; out[1] += b.y; out[2] += b.z; out[3] += b.w;
+        out[0] += c.x; out[1] += c.y; out[2] += c.z; out[3] += c.w;
+        out[0] += d.x; out[1] += d.y; out[2] += d.z; out[3] += d.w;
+    }
+    for (; i < n; i += st) {
+        const double4 a = p[i];
+        out[0] += a.x; out[1] += a.y; out[2] += a.z; out[3] += a.w;
     }
 }
 

@@ -342,23 +342,30 @@ DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
         const uint32_t m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
             const uint32_t k = cnt + __popc(m & ((1u << lane) - 1u));
-            if (k < cap) {
-                out[(size_t)ci * cap + k] = cj;
-                if (MODE == 3) {
-                    unsigned long long mask = 0ull;
-                    for (int ii = 0; ii < ACL; ++ii) {
-                        const uint32_t a = v.sidx[ci * ACL + ii];
-                        if (a == INVALID_ID) continue;
-                        for (int jj = 0; jj < ACL; ++jj) {
-                            const uint32_t c = v.sidx[cj * ACL + jj];
-                            if (c == INVALID_ID || (cj == ci && jj <= ii)) continue;
-                            if (v.astatic && v.astatic[a] && v.astatic[c]) continue;
-                            if (v.ex_off && excluded(v, a, c)) continue;
-                            mask |= 1ull << (ii * ACL + jj);
-                        }
-                    }
-                    v.ss_mask[(size_t)ci * cap + k] = mask;
+            if (k < cap) out[(size_t)ci * cap + k] = cj;
+        }
+        if (MODE == 3) {
+            // interaction masks, one hit at a time with the whole warp: lane
+            // decides the pairs (ii, jj) = (lane / 8, lane % 8) and
+            // (lane / 8 + 4, lane % 8); bit ii * 8 + jj
+            for (uint32_t mm = m; mm; mm &= mm - 1u) {
+                const int src = __ffs(mm) - 1;
+                const uint32_t k = cnt + __popc(m & ((1u << src) - 1u));
+                const uint32_t cjh = jb + (uint32_t)src;
+                bool pb[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int ii = (lane >> 3) + 4 * h, jj = lane & 7;
+                    const uint32_t a = v.sidx[ci * ACL + ii];
+                    const uint32_t c = v.sidx[cjh * ACL + jj];
+                    bool on = a != INVALID_ID && c != INVALID_ID && !(cjh == ci && jj <= ii);
+                    if (on && v.astatic && v.astatic[a] && v.astatic[c]) on = false;
+                    if (on && v.ex_off && excluded(v, a, c)) on = false;
+                    pb[h] = on;
                 }
+                const uint32_t lo = __ballot_sync(0xffffffffu, pb[0]);
+                const uint32_t hi = __ballot_sync(0xffffffffu, pb[1]);
+                if (lane == 0 && k < cap) v.ss_mask[(size_t)ci * cap + k] = (unsigned long long)hi << 32 | lo;
             }
         }
         cnt += __popc(m);

@@ -491,10 +491,14 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_pair14, (), ()) {
     write_partials<ENERGY>(v, bk, REG_14, e_acc, 0.0, w_acc);
 }
 
+// Blocks of the atom pair kernels: one per 4 work items, at most one
+// resident wave (4 blocks per SM; the kernels loop over the items), which
+// also bounds the block partials the step finalisation sums.
 inline int pblocks(const SysView& v, uint64_t warps) {
     uint64_t bl = (warps * 32 + PT - 1) / PT;
     if (bl < 1) bl = 1;
-    return (int)(bl < v.max_blocks ? bl : v.max_blocks);
+    const uint64_t cap = std::min<uint64_t>(v.max_blocks, 148u * 4u);
+    return (int)(bl < cap ? bl : cap);
 }
 
 }  // namespace
