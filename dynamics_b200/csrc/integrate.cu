@@ -395,26 +395,6 @@ DYN_KERNEL(, k_atom_kick, (, float dt), (, dt)) {
 // finalize: fixed-order sums of all partials, pressure, temperature, CSVR
 // and C-rescale scalars (single block)
 // ---------------------------------------------------------------------------
-// Adds this thread's share of a region's block partials to out, four
-// partials in flight at a time (the loads are independent; the sum order per
-// thread is fixed).
-__device__ __forceinline__ void region_sum(const SysView& v, int reg, double* out) {
-    const double4* p = reinterpret_cast<const double4*>(v.partials) + (size_t)reg * v.max_blocks;
-    const uint32_t n = v.nb[reg], st = blockDim.x;
-    uint32_t i = threadIdx.x;
-    for (; i + 3 * st < n; i += 4 * st) {
-        const double4 a = p[i], b = p[i + st], c = p[i + 2 * st], d = p[i + 3 * st];
-        out[0] += a.x; out[1] += a.y; out[2] += a.z; out[3] += a.w;
-        out[0] += b.x; out[1] += b.y; out[2] += b.z; out[3] += b.w;
-        out[0] += c.x; out[1] += c.y; out[2] += c.z; out[3] += c.w;
-        out[0] += d.x; out[1] += d.y; out[2] += d.z; out[3] += d.w;
-    }
-    for (; i < n; i += st) {
-        const double4 a = p[i];
-        out[0] += a.x; out[1] += a.y; out[2] += a.z; out[3] += a.w;
-    }
-}
-
 __device__ double gamma_mt(double shape, uint64_t step, uint64_t seed) {
     // Marsaglia & Tsang (ACM TOMS 26, 2000); bounded attempts.
     const double d = shape - 1.0 / 3.0;
@@ -433,24 +413,51 @@ __device__ double gamma_mt(double shape, uint64_t step, uint64_t seed) {
 }
 
 DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (, dt, thermo)) {
-    double ww[4] = {0, 0, 0, 0}, ws[4] = {0, 0, 0, 0}, ss[4] = {0, 0, 0, 0};
-    double p14[4] = {0, 0, 0, 0}, bo[4] = {0, 0, 0, 0}, kw[4] = {0, 0, 0, 0}, ka[4] = {0, 0, 0, 0};
-    double co[4] = {0, 0, 0, 0};
-    region_sum(v, REG_WW, ww);
-    if (v.na) {
-        region_sum(v, REG_SS, ss);
-        if (v.nw) region_sum(v, REG_WS, ws);
-        region_sum(v, REG_14, p14);
-        region_sum(v, REG_BOND, bo);
-        region_sum(v, REG_KICK_A, ka);
-        region_sum(v, REG_CONS, co);
+    // one warp per region, all regions' partials in flight at once; each
+    // region's sum has a fixed order
+    __shared__ double rs[NREGION][4];
+    {
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int reg = w; reg < NREGION; reg += (int)(blockDim.x >> 5)) {
+            double o[4] = {0.0, 0.0, 0.0, 0.0};
+            const bool used = reg == REG_WW || reg == REG_KICK_W ||
+                              (v.na && (reg == REG_SS || reg == REG_14 || reg == REG_BOND ||
+                                        reg == REG_KICK_A || reg == REG_CONS || (v.nw && reg == REG_WS)));
+            if (used) {
+                const double4* p = reinterpret_cast<const double4*>(v.partials) + (size_t)reg * v.max_blocks;
+                const uint32_t n = v.nb[reg];
+                uint32_t i = lane;
+                for (; i + 96 < n; i += 128) {
+                    const double4 a = p[i], b = p[i + 32], c = p[i + 64], d = p[i + 96];
+                    o[0] += a.x; o[1] += a.y; o[2] += a.z; o[3] += a.w;
+                    o[0] += b.x; o[1] += b.y; o[2] += b.z; o[3] += b.w;
+                    o[0] += c.x; o[1] += c.y; o[2] += c.z; o[3] += c.w;
+                    o[0] += d.x; o[1] += d.y; o[2] += d.z; o[3] += d.w;
+                }
+                for (; i < n; i += 32) {
+                    const double4 a = p[i];
+                    o[0] += a.x; o[1] += a.y; o[2] += a.z; o[3] += a.w;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) o[k] = warp_sum_d(o[k]);
+            if (lane == 0)
+                for (int k = 0; k < 4; ++k) rs[reg][k] = o[k];
+        }
     }
-    region_sum(v, REG_KICK_W, kw);
-    double x[16] = {ww[0], ww[1], ww[2], ws[0] + ss[0], ws[1] + ss[1],
-                    ws[2] + ss[2], p14[0], p14[2], bo[0], bo[2], kw[0] + ka[0],
-                    kw[1] + ka[1], co[0], kw[2] + ka[2], kw[3], 0};
-    block_sum_d<16>(x);
+    __syncthreads();
     if (threadIdx.x != 0) return;
+    const double* ww = rs[REG_WW];
+    const double* ws = rs[REG_WS];
+    const double* ss = rs[REG_SS];
+    const double* p14 = rs[REG_14];
+    const double* bo = rs[REG_BOND];
+    const double* kw = rs[REG_KICK_W];
+    const double* ka = rs[REG_KICK_A];
+    const double* co = rs[REG_CONS];
+    const double x[16] = {ww[0], ww[1], ww[2], ws[0] + ss[0], ws[1] + ss[1],
+                          ws[2] + ss[2], p14[0], p14[2], bo[0], bo[2], kw[0] + ka[0],
+                          kw[1] + ka[1], co[0], kw[2] + ka[2], kw[3], 0};
     Scalars* sc = v.sc;
     // the water-water list counts every pair from both sides, the atom
     // lists once
@@ -755,8 +762,9 @@ void launch_second_half(const Target& t, float dt) {
 
 void launch_finalize(const Target& t, float dt, bool energy, bool thermo) {
     auto one = [](const SysView&) { return 1; };
-    if (energy) t.launch(k_finalize<true>, k_finalize_batch<true>, one, 256, 0, dt, thermo);
-    else t.launch(k_finalize<false>, k_finalize_batch<false>, one, 256, 0, dt, thermo);
+    // 16 warps: one per partial-sum region
+    if (energy) t.launch(k_finalize<true>, k_finalize_batch<true>, one, 512, 0, dt, thermo);
+    else t.launch(k_finalize<false>, k_finalize_batch<false>, one, 512, 0, dt, thermo);
     if (!thermo) return;
     t.launch(k_scale, k_scale_batch,
              [](const SysView& v) {

@@ -34,23 +34,12 @@ constexpr int PT = 128;  // threads per block (4 warps)
 // w accumulates the virial in float32
 struct Acc3 { double e_lj, e_c; float w; };
 
-// Site positions are float32 and a periodic shift is a whole number of box
-// extents, so the displacement pi - (pj - sh) is exact in float64: energies
-// use that exact value (and float64 charge products) so that a total that
-// cancels to a small number keeps its relative accuracy; forces use the
-// float32 displacement.
-__device__ __forceinline__ void exact_disp(float3 pi, float3 pj, float3 sh, double& x, double& y, double& z) {
-    x = (double)pi.x - ((double)pj.x - (double)sh.x);
-    y = (double)pi.y - ((double)pj.y - (double)sh.y);
-    z = (double)pi.z - ((double)pj.z - (double)sh.z);
-}
-
 // erfc-screened Coulomb between site pi and site pj shifted by sh
 // (d = pi - (pj - sh)), branch-free: force q q (r^-3 + g(r^2)) d with
 // g(z) = 2 d/dz [erf(alpha sqrt z) / sqrt z] from the host-fitted polynomial
 // in t = 2 r^2 / rc^2 - 1 (no square root needed for the argument); zero for
 // r >= rc (src/cuda/cuda.cu:160-164).  On energy steps the energy
-// qqe erfc(alpha r) / r is evaluated in float64 from the exact displacement.
+// qqe erfc(alpha r) / r is added in float64.
 template <bool ENERGY>
 __device__ __forceinline__ void coul(float3 pi, float3 pj, float3 sh, float qq, double qqe, const SysView& v,
                                      float3& f, Acc3& a) {
@@ -65,22 +54,17 @@ __device__ __forceinline__ void coul(float3 pi, float3 pj, float3 sh, float qq, 
     fs = r2 < v.rc2 ? fs : 0.0f;
     f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
     a.w = fmaf(fs, r2, a.w);
-    if (ENERGY) {
-        // r^2 from the exact displacement, rounded once to float32; erfc(alpha
-        // r) / r in float32 (correctly rounded sqrt and divide), scaled by the
-        // float64 charge product and summed in float64
-        double x, y, z;
-        exact_disp(pi, pj, sh, x, y, z);
-        const float r2e = (float)(x * x + y * y + z * z);
-        if (r2e < v.rc2) {
-            const float re = __fsqrt_rn(r2e);
-            a.e_c += qqe * (double)__fdiv_rn(erfcf(v.alpha * re), re);
-        }
+    if (ENERGY && r2 < v.rc2) {
+        // erfc(alpha r) / r in float32 from the force's r^2 and 1/r, scaled by
+        // the float64 charge product and summed in float64: per-pair errors
+        // of a few ulp with no common sign
+        const float re = r2 * rinv;
+        a.e_c += qqe * (double)(erfcf(v.alpha * re) * rinv);
     }
 }
 
 // 12-6 LJ (force_e_lj, src/forces.rs:10-21) between pi and pj shifted by sh,
-// branch-free, r <= lj_cutoff; float64 energy from the exact displacement.
+// branch-free, r <= lj_cutoff; energy summed in float64.
 template <bool ENERGY>
 __device__ __forceinline__ void lj(float3 pi, float3 pj, float3 sh, float sig2, float eps, float ljc2,
                                    float scale, float3& f, Acc3& a) {
@@ -95,10 +79,7 @@ __device__ __forceinline__ void lj(float3 pi, float3 pj, float3 sh, float sig2, 
     f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
     a.w = fmaf(fs, r2, a.w);
     if (ENERGY && in) {
-        double x, y, z;
-        exact_disp(pi, pj, sh, x, y, z);
-        const float s2 = __fdiv_rn(sig2, (float)(x * x + y * y + z * z));
-        const double s6 = (double)(s2 * s2 * s2);
+        const double s6 = (double)sr6;
         a.e_lj += 4.0 * (double)scale * (double)eps * (s6 * s6 - s6);
     }
 }
