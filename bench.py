@@ -54,6 +54,12 @@ WORKLOADS = {
     # size distribution, 5000 steps each, Langevin-middle 300 K, 150 GB budget
     "c5w": dict(kind="serve", n_req=48, rate=20.0, steps_each=5000, cutoff=9.0, budget=150e9,
                 integrator="langevin", barostat=False, n_water=None),
+    # as c4w / c5w with 0-3 ten-residue ff19SB peptides (and counter-ions,
+    # bond-to-H constraints) in every member
+    "c4": dict(kind="batch", n_sys=64, cutoff=9.0, integrator="langevin", barostat=False,
+               n_water=None, peptides=3),
+    "c5": dict(kind="serve", n_req=48, rate=20.0, steps_each=5000, cutoff=9.0, budget=150e9,
+               integrator="langevin", barostat=False, n_water=None, peptides=3),
 }
 DEFAULT_WORKLOAD = "c3"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
@@ -84,14 +90,27 @@ def build_system(name, seed):
     return sysd, cfg
 
 
+def member_system(w, n_water, seed, rng):
+    """One batched / served member: a water box, or with w["peptides"] a box
+    with 0..w["peptides"] ten-residue peptides (count drawn from rng)."""
+    from dynamics_b200 import synth
+    if w.get("peptides"):
+        from dynamics_b200 import peptide
+        n_pep = int(rng.integers(0, w["peptides"] + 1))
+        sysd, grid, _ = peptide.batch_member(int(n_water), n_pep, seed=seed)
+        return sysd, grid
+    return synth.batch_member(int(n_water), seed=seed)
+
+
 def build_batch(name, seed):
     from dynamics_b200 import md, synth
     w = WORKLOADS[name]
     sizes = synth.config4_sizes(w["n_sys"], seed=seed)
+    rng = np.random.default_rng(seed + 7919)
     systems, cfgs = [], []
     alpha = synth.ewald_alpha(w["cutoff"])
     for i, n in enumerate(sizes):
-        sysd, grid = synth.batch_member(int(n), seed=seed * 1000 + i)
+        sysd, grid = member_system(w, n, seed * 1000 + i, rng)
         cfg = md.MdConfig(coulomb_cutoff=w["cutoff"], lj_cutoff=w["cutoff"], spme_alpha=alpha,
                           spme_grid=grid, seed=seed * 1000 + i,
                           integrator=md.LangevinMiddle(gamma=1.0))
@@ -117,6 +136,7 @@ def run_batch(args):
     systems = [md.equilibrate(s, c, n_steps=min(args.equil, 200), dt=0.001) for s, c in zip(systems, cfgs)]
     n_sys = len(systems)
     n_water = int(sum(len(s["water_pos"]) for s in systems))
+    n_atoms = int(sum(len(s.get("atom_pos", ())) for s in systems))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     # ---- plain path, one system at a time (each its own graph per step) ----
     k_plain = max(10, min(args.steps, 100))
@@ -165,24 +185,25 @@ def run_batch(args):
     plain_value = DT * 1e-3 * n_sys / (plain_ms * 1e-3) * 86400.0
     # ---- end to end: every member's positions/velocities in and out per step ----
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory().numpy()
+    keys = ("water_pos", "water_vel", "atom_pos", "atom_vel")
     host = []
     for m in batch.members:
         s0 = m.state()
-        host.append((pin(s0["water_pos"]), pin(s0["water_vel"])))
+        host.append({k: pin(s0[k]) for k in keys if k in s0 and s0[k].size})
     n_e2e = max(5, args.steps // 20)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for _ in range(n_e2e):
-        for m, (wp, wv) in zip(batch.members, host):
-            m.set_state(water_pos=wp, water_vel=wv)
+        for m, hb in zip(batch.members, host):
+            m.set_state(**hb)
         batch.step(DT, 1)
-        for m, (wp, wv) in zip(batch.members, host):
+        for m, hb in zip(batch.members, host):
             s1 = m.state()
-            wp[:] = s1["water_pos"]
-            wv[:] = s1["water_vel"]
+            for k in hb:
+                hb[k][:] = s1[k]
     t_e2e = time.perf_counter() - t0
     e2e_value = n_e2e * DT * 1e-3 * n_sys * world / t_e2e * 86400.0
-    io_bytes = int(sum(wp.nbytes + wv.nbytes for wp, wv in host))
+    io_bytes = int(sum(a.nbytes for hb in host for a in hb.values()))
     clk = clocks.summary(local)
     batch.close()
     if dist:
@@ -196,9 +217,11 @@ def run_batch(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded OPC water boxes, equilibrated on device)",
+        "data": "synthetic (seeded OPC water boxes" + (", 0-3 ten-residue ff19SB peptides each"
+                                                        if w.get("peptides") else "")
+                + ", equilibrated on device)",
         "config": {"workload": name, "members": n_sys, "n_water_total": n_water,
-                   "sizes": "512-8000 waters, log-uniform", "cutoff_A": w["cutoff"],
+                   "n_atoms_total": n_atoms, "sizes": "512-8000 waters, log-uniform", "cutoff_A": w["cutoff"],
                    "grid": "FFT-friendly ~1 A", "integrator": "langevin_middle", "dt_fs": DT * 1e3,
                    "l2": "256 MiB flush between timed steps", "parallelism": f"replicas x{world}"},
         "plain_one_by_one": {"value": round(plain_value, 2), "unit": "ns/day (aggregate)",
@@ -235,8 +258,9 @@ def run_serve(args):
     arrivals = serve.poisson_arrivals(w["n_req"], w["rate"], seed=seed)
     alpha = synth.ewald_alpha(w["cutoff"])
     reqs = []
+    rng = np.random.default_rng(seed + 7919)
     for i, (n, t) in enumerate(zip(sizes, arrivals)):
-        sysd, grid = synth.batch_member(int(n), seed=seed * 1000 + i)
+        sysd, grid = member_system(w, n, seed * 1000 + i, rng)
         cfg = md.MdConfig(coulomb_cutoff=w["cutoff"], lj_cutoff=w["cutoff"], spme_alpha=alpha, spme_grid=grid,
                           seed=seed * 1000 + i, integrator=md.LangevinMiddle(gamma=1.0))
         sysd = md.equilibrate(sysd, cfg, n_steps=min(args.equil, 200), dt=0.001)
@@ -280,7 +304,9 @@ def run_serve(args):
         "n_gpus": world, "steps": rep.steps_total, "warmup": args.warmup,
         "ms_per_step": round(rep.wall_s / rep.rounds / 100 * 1e3, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded OPC water boxes, equilibrated on device before arrival)",
+        "data": "synthetic (seeded OPC water boxes" + (", 0-3 ten-residue ff19SB peptides each"
+                                                        if w.get("peptides") else "")
+                + ", equilibrated on device before arrival)",
         "config": {"workload": name, "requests": len(reqs), "arrival_rate_per_s": w["rate"],
                    "steps_each": w["steps_each"], "sizes": "512-8000 waters, log-uniform",
                    "budget_GB": w["budget"] / 1e9, "round_steps": 100, "integrator": "langevin_middle",

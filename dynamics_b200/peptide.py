@@ -571,16 +571,21 @@ def solvated_system(box, n_water, n_res=(), seed=0, nacl_molar=0.0, temperature=
         seq = random_sequence(int(nr), rng)
         p = build_peptide(seq, seed=seed * 100 + k)
         pos = p["atom_pos"].astype(np.float64)
+        ok = False
         for _ in range(200):
             # first peptide at the centre; others anywhere clear of the rest
             c = np.full(3, box / 2.0) if k == 0 else rng.uniform(0.0, box, 3)
             trial = pos + c
             if len(placed) == 0:
+                ok = True
                 break
             t = cKDTree(np.mod(placed, box), boxsize=box)
             d, _ = t.query(np.mod(trial, box))
             if d.min() > 4.0:
+                ok = True
                 break
+        if not ok:
+            raise ValueError(f"no room for peptide {k} in a {box:.1f} A box")
         p["atom_pos"] = trial.astype(np.float32)
         placed = np.concatenate([placed, trial])
         peps.append(p)
@@ -653,3 +658,23 @@ def solvated_system(box, n_water, n_res=(), seed=0, nacl_molar=0.0, temperature=
     sysd["water_vel"] = sysd["water_vel"].astype(np.float32)
     sysd["atom_vel"] = sysd["atom_vel"].astype(np.float32)
     return sysd, seqs
+
+
+def batch_member(n_water, n_peptides, seed=0, n_res=10, density=0.0334, spacing=1.0):
+    """One member of the batched / served workloads: ``n_peptides`` random
+    ``n_res``-residue peptides with counter-ions in a box of ``n_water`` OPC
+    waters at ``density`` per cubic angstrom, and an FFT-friendly SPME grid
+    of about ``spacing`` A.  If the peptides do not fit clear of each other
+    (small boxes), other placements are tried, then one peptide fewer.
+    Returns (system, grid, peptides placed)."""
+    box = float((n_water / density) ** (1.0 / 3.0))
+    k = synth.fft_size(int(np.ceil(box / spacing)))
+    for n_pep in range(int(n_peptides), -1, -1):
+        for attempt in range(4):
+            try:
+                sysd, _ = solvated_system(box, int(n_water), n_res=(n_res,) * n_pep,
+                                          seed=seed * 16 + attempt)
+                return sysd, (k, k, k), n_pep
+            except ValueError:
+                continue
+    raise ValueError("batch member could not be built")

@@ -8,7 +8,7 @@ velocities and energies, not a tolerance.
 import numpy as np
 import pytest
 
-from dynamics_b200 import md, synth
+from dynamics_b200 import md, peptide, synth
 
 from .systems import mixed, water_only
 
@@ -26,14 +26,18 @@ def _cfg(sysd, integ=None, **kw):
 
 
 def _members():
+    # the last member: a ten-residue peptide with counter-ions and
+    # bond-to-hydrogen constraints
+    pep, _, _ = peptide.batch_member(600, 1, seed=6)
     systems = [water_only(n_side=7, seed=3), synth.water_box(512, 24.8, seed=4),
-               synth.water_box(729, 27.9, seed=5), mixed()]
+               synth.water_box(729, 27.9, seed=5), mixed(), pep]
     cfgs = [
         _cfg(systems[0], integ=md.LangevinMiddle(gamma=1.0), seed=11),
         _cfg(systems[1], integ=md.VerletVelocity(thermostat=0.1), seed=12),
         _cfg(systems[2], integ=md.VerletVelocity(thermostat=0.1), seed=13,
              barostat_cfg=md.BarostatCfg()),
         _cfg(systems[3], integ=md.LangevinMiddle(gamma=1.0), seed=14),
+        _cfg(systems[4], integ=md.LangevinMiddle(gamma=1.0), seed=15),
     ]
     systems = [md.equilibrate(s, c, n_steps=40, dt=0.001) for s, c in zip(systems, cfgs)]
     return systems, cfgs

@@ -13,8 +13,8 @@ pytestmark = pytest.mark.gpu
 
 def _requests():
     systems, cfgs = _members()
-    arrivals = [0.0, 0.0, 0.001, 0.002]
-    n_steps = [100, 50, 100, 150]
+    arrivals = [0.0, 0.0, 0.001, 0.002, 0.003]
+    n_steps = [100, 50, 100, 150, 50]
     return [serve.Request(rid=i, system=s, cfg=c, n_steps=n, arrival=t)
             for i, (s, c, n, t) in enumerate(zip(systems, cfgs, n_steps, arrivals))]
 
