@@ -194,6 +194,16 @@ struct SysView {
 // ---------------------------------------------------------------------------
 struct Blk { uint32_t idx, cnt; };
 
+// Programmatic dependent launch: every step kernel is launched allowed to
+// overlap its launch with the end of the kernel before it on the stream; it
+// waits here until that kernel has completed and its writes are visible.
+// No kernel triggers its dependents early: blocks of the next kernel parked
+// on SMs while the current one runs cost more than the launch they hide
+// (measured on the step graphs).
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 #define DYN_UNPAREN(...) __VA_ARGS__
 
 #define DYN_KERNEL(LB, NAME, PARAMS, ARGS)                                                          \
@@ -201,10 +211,12 @@ struct Blk { uint32_t idx, cnt; };
         static __device__ __forceinline__ void run(const SysView& v, Blk bk DYN_UNPAREN PARAMS);     \
     };                                                                                               \
     __global__ void LB NAME(const __grid_constant__ SysView v DYN_UNPAREN PARAMS) {                  \
+        pdl_enter();                                                                                 \
         NAME##_B::run(v, Blk{blockIdx.x, gridDim.x} DYN_UNPAREN ARGS);                               \
     }                                                                                                \
     __global__ void LB NAME##_batch(const SysView* __restrict__ vs,                                  \
                                     const uint2* __restrict__ bm DYN_UNPAREN PARAMS) {               \
+        pdl_enter();                                                                                 \
         const uint2 m = bm[blockIdx.x];                                                              \
         NAME##_B::run(vs[m.x], Blk{m.y & 0xFFFFu, m.y >> 16} DYN_UNPAREN ARGS);                      \
     }                                                                                                \
@@ -217,11 +229,13 @@ struct Blk { uint32_t idx, cnt; };
     };                                                                                               \
     template <DYN_UNPAREN TDECL>                                                                     \
     __global__ void LB NAME(const __grid_constant__ SysView v DYN_UNPAREN PARAMS) {                  \
+        pdl_enter();                                                                                 \
         NAME##_B<DYN_UNPAREN TARGS>::run(v, Blk{blockIdx.x, gridDim.x} DYN_UNPAREN ARGS);            \
     }                                                                                                \
     template <DYN_UNPAREN TDECL>                                                                     \
     __global__ void LB NAME##_batch(const SysView* __restrict__ vs,                                  \
                                     const uint2* __restrict__ bm DYN_UNPAREN PARAMS) {               \
+        pdl_enter();                                                                                 \
         const uint2 m = bm[blockIdx.x];                                                              \
         NAME##_B<DYN_UNPAREN TARGS>::run(vs[m.x], Blk{m.y & 0xFFFFu, m.y >> 16} DYN_UNPAREN ARGS);   \
     }                                                                                                \
@@ -248,11 +262,26 @@ struct Target {
     BatchCtx* b = nullptr;        // batch (v == nullptr)
     cudaStream_t st = nullptr;
 
+    template <typename K, typename... A>
+    static void launch_pdl(K k, int grid, int threads, size_t smem, cudaStream_t s, A... a) {
+        cudaLaunchConfig_t c = {};
+        c.gridDim = dim3((unsigned)grid);
+        c.blockDim = dim3((unsigned)threads);
+        c.dynamicSmemBytes = smem;
+        c.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        c.attrs = at;
+        c.numAttrs = 1;
+        cudaLaunchKernelEx(&c, k, a...);
+    }
+
     template <typename KP, typename KB, typename G, typename... A>
     void launch(KP kp, KB kb, G grid, int threads, size_t smem, A... a) const {
         if (v) {
             const int g = grid(*v);
-            if (g > 0) kp<<<g, threads, smem, st>>>(*v, a...);
+            if (g > 0) launch_pdl(kp, g, threads, smem, st, *v, a...);
             return;
         }
         const uint32_t n = batch_size(b);
@@ -262,7 +291,8 @@ struct Target {
             bl[i] = g > 0 ? (uint32_t)g : 0u;
         }
         const BlockMap m = batch_map(b, bl);
-        if (m.total && !batch_collecting(b)) kb<<<m.total, threads, smem, st>>>(batch_dviews(b), m.d_map, a...);
+        if (m.total && !batch_collecting(b))
+            launch_pdl(kb, (int)m.total, threads, smem, st, batch_dviews(b), m.d_map, a...);
     }
     // host-side work per system (library calls such as cuFFT); skipped
     // while a batch only collects its block maps

@@ -239,18 +239,22 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
                 k += LPW;
                 idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
                 const float4* jw = tile + 4 * (idx - lo);
-                const float3 jO = xyz(jw[0]), jH0 = xyz(jw[1]), jH1 = xyz(jw[2]), jM = xyz(jw[3]);
+                const float3 jO = xyz(jw[0]);
                 const float3 sh = shift_of(iO - jO, b);
-                lj<ENERGY>(iO, jO, sh, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
-                coul<ENERGY>(iH0, jH0, sh, qhh, ehh, v, fH0, a);
-                coul<ENERGY>(iH0, jH1, sh, qhh, ehh, v, fH0, a);
-                coul<ENERGY>(iH0, jM, sh, qhm, ehm, v, fH0, a);
-                coul<ENERGY>(iH1, jH0, sh, qhh, ehh, v, fH1, a);
-                coul<ENERGY>(iH1, jH1, sh, qhh, ehh, v, fH1, a);
-                coul<ENERGY>(iH1, jM, sh, qhm, ehm, v, fH1, a);
-                coul<ENERGY>(iM, jH0, sh, qhm, ehm, v, fM, a);
-                coul<ENERGY>(iM, jH1, sh, qhm, ehm, v, fM, a);
-                coul<ENERGY>(iM, jM, sh, qmm, emm, v, fM, a);
+                // the j sites moved by the shift once (the same float values
+                // pj - sh that each site pair would form), then zero shift
+                const float3 z0 = f3(0.f, 0.f, 0.f);
+                const float3 sO = jO - sh, sH0 = xyz(jw[1]) - sh, sH1 = xyz(jw[2]) - sh, sM = xyz(jw[3]) - sh;
+                lj<ENERGY>(iO, sO, z0, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
+                coul<ENERGY>(iH0, sH0, z0, qhh, ehh, v, fH0, a);
+                coul<ENERGY>(iH0, sH1, z0, qhh, ehh, v, fH0, a);
+                coul<ENERGY>(iH0, sM, z0, qhm, ehm, v, fH0, a);
+                coul<ENERGY>(iH1, sH0, z0, qhh, ehh, v, fH1, a);
+                coul<ENERGY>(iH1, sH1, z0, qhh, ehh, v, fH1, a);
+                coul<ENERGY>(iH1, sM, z0, qhm, ehm, v, fH1, a);
+                coul<ENERGY>(iM, sH0, z0, qhm, ehm, v, fM, a);
+                coul<ENERGY>(iM, sH1, z0, qhm, ehm, v, fM, a);
+                coul<ENERGY>(iM, sM, z0, qmm, emm, v, fM, a);
             }
             __syncthreads();  // the tile is refilled by the next chunk's or group's copies
         }
@@ -347,14 +351,15 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT, 4), k_pair_ws, (), (
                 float3 fo = f3(0, 0, 0), f0 = fo, f1 = fo, fm = fo;
                 if (vi && aj != INVALID_ID) {
                     const float3 jp = xyz(pj);
-                    const float3 s = shift_of(iO - jp, b);
+                    // the atom moved by the shift once, then zero shift
+                    const float3 js = jp - shift_of(iO - jp, b), z0 = f3(0.f, 0.f, 0.f);
                     const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
                     const float ep = sqrtf(OPC_O_EPS * lj_j.y);
                     const double qe = (double)pj.w;
-                    lj<ENERGY>(iO, jp, s, sg * sg, ep, ljc2, 1.0f, fo, a);
-                    coul<ENERGY>(iH0, jp, s, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
-                    coul<ENERGY>(iH1, jp, s, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
-                    coul<ENERGY>(iM, jp, s, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
+                    lj<ENERGY>(iO, js, z0, sg * sg, ep, ljc2, 1.0f, fo, a);
+                    coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
+                    coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
+                    coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
                 }
                 fO = fO + fo; fH0 = fH0 + f0; fH1 = fH1 + f1; fM = fM + fm;
                 const float3 t = (fo + f0) + (f1 + fm);
