@@ -62,10 +62,11 @@ WORKLOADS = {
                integrator="langevin", barostat=False, n_water=None, peptides=3),
 }
 DEFAULT_WORKLOAD = "c3"
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
-# the water-water pair kernel, from an ncu --set full capture of this
-# workload (cold L2, as in the timed loop, which flushes L2 between steps)
-PAIR_DRAM_BYTES = {"c3w": 17306880}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one step's
+# short-range pair kernels (water-water, water-atom, atom-atom), from an
+# ncu --set full capture of the workload (cold L2, as in the timed loop,
+# which flushes L2 between steps)
+PAIR_DRAM_BYTES = {"c3w": 17306880, "c3": 17521920 + 4850944 + 903168}
 DT = 0.002
 
 
