@@ -39,6 +39,7 @@ DYN_FLAG_FULL_ENERGY = 2
 DYN_FLAG_COM_REMOVAL = 4
 DYN_FLAG_RECENTER = 8
 DYN_FLAG_RESET_ANGLE = 16
+DYN_FLAG_RATTLE_VELOCITIES = 32
 
 
 class DynError(RuntimeError):

@@ -241,26 +241,87 @@ __device__ __forceinline__ void rattle_unit(Unit& U) {
 // drift dt/2, constrain (src/integrate.rs:100-160,478-511,566-587);
 // velocity Verlet kick dt/2 + drift dt, constrain + rattle.  The constraint
 // virial of the first projection (dt/2) is the step's (src/integrate.rs:105-165).
+// RATTLE (Andersen, J. Comput. Phys. 52, 24 (1983)), used with
+// DYN_FLAG_RATTLE_VELOCITIES.  Position stage: SHAKE iterations with the
+// corrections along the bond vectors at the start of the drift (xr), which
+// makes the map symplectic, until every |d|^2 is within 1e-6 of r0^2 (at
+// most RATTLE_SWEEPS sweeps); the velocities then follow the displacement
+// (v += dx / t_drift).  Velocity stage: the projection of rattle_unit,
+// repeated so that the coupled bonds of a unit (CH3, NH3) all hold.
+constexpr int RATTLE_SWEEPS = 32;
+
+__device__ __forceinline__ double shake_unit(Unit& U, const float3 (&xr)[UMAX], float inv_dt2) {
+    if (U.n < 2) return 0.0;
+    const float3 x0 = U.x[0];
+    for (int it = 0; it < RATTLE_SWEEPS; ++it) {
+        bool done = true;
+#pragma unroll
+        for (int k = 1; k < UMAX; ++k) {
+            if (k >= U.n) break;
+            const float3 d = U.x[k] - U.x[0];
+            const float diff = dot3(d, d) - U.r02[k];
+            if (fabsf(diff) > 1e-6f * U.r02[k]) done = false;
+            const float3 ro = xr[k] - xr[0];
+            const float im = 1.0f / U.m[0] + 1.0f / U.m[k];
+            const float g = diff / (2.0f * im * dot3(d, ro));
+            const float3 corr = ro * g;
+            if (!U.fixed[0]) U.x[0] = U.x[0] + corr * (1.0f / U.m[0]);
+            if (!U.fixed[k]) U.x[k] = U.x[k] - corr * (1.0f / U.m[k]);
+        }
+        if (done) break;
+    }
+    const float3 fi = (U.x[0] - x0) * (U.m[0] * inv_dt2);
+    double w = 0.0;
+#pragma unroll
+    for (int k = 1; k < UMAX; ++k)
+        if (k < U.n) w += (double)dot3(U.x[k] - U.x[0], fi);
+    return w;
+}
+
+__device__ __forceinline__ void follow_constraint(Unit& U, const float3 (&xu)[UMAX], float inv_t) {
+#pragma unroll
+    for (int k = 0; k < UMAX; ++k)
+        if (k < U.n && !U.fixed[k]) U.vel[k] = U.vel[k] + (U.x[k] - xu[k]) * inv_t;
+}
+
+__device__ __forceinline__ void rattle_unit_converged(Unit& U) {
+    if (U.n < 2) return;
+    const int sweeps = U.n > 2 ? 8 : 1;  // one bond: the projection is exact
+    for (int it = 0; it < sweeps; ++it) rattle_unit(U);
+}
+
 DYN_KERNEL(, k_atom_first, (, float dt), (, dt)) {
     const uint64_t step = v.sc->step;
     const bool lm = v.integrator == DYN_INTEGRATOR_LANGEVIN_MIDDLE;
+    const bool rv = (v.flags & DYN_FLAG_RATTLE_VELOCITIES) != 0u;
     const float c = expf(-v.gamma * dt);
     const float num = KB_NATIVE * v.temperature * fmaxf(1.0f - c * c, 0.f);
     const float hk = 0.5f * dt;
     const float inv_dt2 = 1.0f / (hk * hk);
+    const float t_drift = lm ? hk : dt;
+    const float inv_td = 1.0f / t_drift, inv_hk = 1.0f / hk;
     double vir = 0.0;
     for (uint32_t u = bk.idx * blockDim.x + threadIdx.x; u < v.nunit; u += bk.cnt * blockDim.x) {
         Unit U;
         load_unit(v, u, U);
+        float3 xr[UMAX], xu[UMAX];  // positions at the start of a drift, before its constraint pass
 #pragma unroll
         for (int k = 0; k < UMAX; ++k) {
             if (k >= U.n) break;
-            if (U.fixed[k]) continue;
-            U.vel[k] = U.vel[k] + xyz(v.aacc[U.id[k]]) * hk;
-            U.x[k] = U.x[k] + U.vel[k] * (lm ? hk : dt);
+            xr[k] = U.x[k];
+            if (!U.fixed[k]) {
+                U.vel[k] = U.vel[k] + xyz(v.aacc[U.id[k]]) * hk;
+                U.x[k] = U.x[k] + U.vel[k] * t_drift;
+            }
+            xu[k] = U.x[k];
         }
-        vir += constrain_unit(U, v.lincs_order, v.lincs_iter, inv_dt2);
-        rattle_unit(U);
+        if (rv) {
+            vir += shake_unit(U, xr, inv_dt2);
+            follow_constraint(U, xu, inv_td);
+        } else {
+            vir += constrain_unit(U, v.lincs_order, v.lincs_iter, inv_dt2);
+            rattle_unit(U);
+        }
         if (lm) {
 #pragma unroll
             for (int k = 0; k < UMAX; ++k) {
@@ -269,11 +330,22 @@ DYN_KERNEL(, k_atom_first, (, float dt), (, dt)) {
                 const float sg = sqrtf(num / U.m[k]);
                 U.vel[k] = U.vel[k] * c + ou_normals(U.id[k], step, v.seed) * sg;
             }
-            rattle_unit(U);
+            // the noise, projected onto the constraints
+            if (rv) rattle_unit_converged(U);
+            else rattle_unit(U);
 #pragma unroll
-            for (int k = 0; k < UMAX; ++k)
-                if (k < U.n && !U.fixed[k]) U.x[k] = U.x[k] + U.vel[k] * hk;
-            constrain_unit(U, v.lincs_order, v.lincs_iter, inv_dt2);
+            for (int k = 0; k < UMAX; ++k) {
+                if (k >= U.n) break;
+                xr[k] = U.x[k];
+                if (!U.fixed[k]) U.x[k] = U.x[k] + U.vel[k] * hk;
+                xu[k] = U.x[k];
+            }
+            if (rv) {
+                shake_unit(U, xr, inv_dt2);
+                follow_constraint(U, xu, inv_hk);
+            } else {
+                constrain_unit(U, v.lincs_order, v.lincs_iter, inv_dt2);
+            }
         }
 #pragma unroll
         for (int k = 0; k < UMAX; ++k) {
@@ -374,7 +446,9 @@ DYN_KERNEL(, k_atom_kick, (, float dt), (, dt)) {
             v.aacc[a] = make_float4(acc.x, acc.y, acc.z, 0.f);
             if (!finite3(acc)) v.sc->nonfinite = 1u;
         }
-        rattle_unit(U);  // src/integrate.rs:554-559
+        // src/integrate.rs:554-559
+        if (v.flags & DYN_FLAG_RATTLE_VELOCITIES) rattle_unit_converged(U);
+        else rattle_unit(U);
 #pragma unroll
         for (int k = 0; k < UMAX; ++k) {
             if (k >= U.n) break;

@@ -73,6 +73,10 @@ class MdConfig:
     ww_union_chunk: int = 0         # 0 = automatic (tuning knob only)
     lincs_order: int = 4            # HydrogenConstraint::Linear { order, iter } (src/prep.rs:77)
     lincs_iter: int = 1
+    # constraint position corrections also correct the velocities (RATTLE);
+    # False = the reference's position-only correction, which dissipates
+    # kinetic energy of the constrained bonds
+    rattle_velocities: bool = False
 
 
 def thermo_dof(system, cfg):
@@ -130,6 +134,8 @@ def _config_struct(system, cfg):
         flags |= _lib.DYN_FLAG_RECENTER
     if cfg.reset_angle:
         flags |= _lib.DYN_FLAG_RESET_ANGLE
+    if cfg.rattle_velocities:
+        flags |= _lib.DYN_FLAG_RATTLE_VELOCITIES
     c.flags = flags
     c.thermo_dof = thermo_dof(system, cfg)
     c.seed = int(cfg.seed) & 0xFFFFFFFFFFFFFFFF

@@ -222,6 +222,15 @@ typedef struct dyn_sys_s* dyn_sys_t;
 /* Re-establish the water geometry every 1000 steps
  * (src/solvent/opc_settle.rs:202-219, src/integrate.rs:445-449). */
 #define DYN_FLAG_RESET_ANGLE 16u
+/* RATTLE for the bond-to-hydrogen constraints: SHAKE iterations along the
+ * bond vectors at the start of each drift, velocities corrected by the
+ * constraint displacement, velocity projection iterated for coupled bonds:
+ * a symplectic, energy-conserving constrained integrator.  Off = the
+ * reference's lincs_hydrogens + rattle_hydrogens (src/bonded.rs:218-304,
+ * src/integrate.rs:498-507), which corrects positions along the current
+ * bond vectors and leaves the velocities to one projection; that map is not
+ * symplectic and drains energy at a rate proportional to dt. */
+#define DYN_FLAG_RATTLE_VELOCITIES 32u
 
 typedef struct {
     float box_lo[3];

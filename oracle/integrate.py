@@ -269,6 +269,51 @@ def lincs_hydrogens(state, dt, order=4, iters=1):
     return w
 
 
+def shake_old_bonds(state, x_ref, dt, sweeps=32, tol=1e-6):
+    """RATTLE's position stage (Andersen 1983): SHAKE iterations with the
+    corrections along the bond vectors of ``x_ref`` (the positions at the
+    start of the drift), per unit, until every |d|^2 is within ``tol`` of
+    r0^2; returns the constraint virial estimate as lincs_hydrogens does."""
+    cs = _constraints(state)
+    if cs is None:
+        return 0.0
+    heavy, hyd, r02, im = cs
+    x = state["atom_pos"]
+    m = state["atom_mass"]
+    fixed = state["atom_static"]
+    x0 = x.copy()
+    seq = _in_unit_order(state)
+    for _ in range(sweeps):
+        done = True
+        for c in seq:
+            i, j = heavy[c], hyd[c]
+            d = x[j] - x[i]
+            diff = d @ d - r02[c]
+            if abs(diff) > tol * r02[c]:
+                done = False
+            ro = x_ref[j] - x_ref[i]
+            corr = ro * (diff / (2.0 * im[c] * (d @ ro)))
+            if not fixed[i]:
+                x[i] += corr / m[i]
+            if not fixed[j]:
+                x[j] -= corr / m[j]
+        if done:
+            break
+    inv_dt2 = 1.0 / (dt * dt)
+    w = 0.0
+    for c in range(len(heavy)):
+        i, j = heavy[c], hyd[c]
+        fi = (x[i] - x0[i]) * (m[i] * inv_dt2)
+        w += (x[j] - x[i]) @ fi
+    return w
+
+
+def rattle_hydrogens_converged(state, sweeps=8):
+    """The velocity projection repeated so that coupled bonds all hold."""
+    for _ in range(sweeps):
+        rattle_hydrogens(state)
+
+
 def rattle_hydrogens(state):
     """rattle_hydrogens (src/bonded.rs:288-304)."""
     cs = _constraints(state)
@@ -284,9 +329,10 @@ def rattle_hydrogens(state):
         vel[j] -= corr / m[j]
 
 
-def kick_and_calc_accel(state, forces, dt):
+def kick_and_calc_accel(state, forces, dt, rattle_velocities=False):
     """kick_and_calc_accel (src/integrate.rs:515-562), with RATTLE when the
-    state carries constraints.
+    state carries constraints (iterated to convergence with
+    ``rattle_velocities``).
 
     ``forces``: dict with f_atoms (na,3), f_water (nw,4,3) [O,H0,H1,M].
     """
@@ -299,7 +345,10 @@ def kick_and_calc_accel(state, forces, dt):
         a = np.where(big[:, None], a / np.where(big, amag, 1.0)[:, None] * MAX_ACCEL, a)
         state["atom_accel"] = np.where(dyn[:, None], a, 0.0)
         state["atom_vel"] = state["atom_vel"] + state["atom_accel"] * dt
-        rattle_hydrogens(state)
+        if rattle_velocities:
+            rattle_hydrogens_converged(state)
+        else:
+            rattle_hydrogens(state)
     fw = forces["f_water"]
     if len(fw):
         fo, fh0, fh1 = opc.project_ep_force(fw[:, 0], fw[:, 1], fw[:, 2], fw[:, 3])
@@ -309,17 +358,27 @@ def kick_and_calc_accel(state, forces, dt):
         state["water_vel"] = state["water_vel"] + acc * dt
 
 
-def kick_and_drift(state, dt_kick, dt_drift, lo, ext):
+def kick_and_drift(state, dt_kick, dt_drift, lo, ext, rattle_velocities=False):
     """kick_and_drift (src/integrate.rs:478-511); with constraints,
-    lincs_hydrogens(dt_kick) and RATTLE follow (:498-507)."""
+    lincs_hydrogens(dt_kick) and RATTLE follow (:498-507).  With
+    ``rattle_velocities``: RATTLE's position stage instead (shake_old_bonds,
+    velocities following the displacement, v += dx / dt_drift), the engine's
+    DYN_FLAG_RATTLE_VELOCITIES."""
     if len(state["atom_vel"]):
         dyn = ~state["atom_static"]
+        x_ref = state["atom_pos"].copy()
         v = state["atom_vel"] + state["atom_accel"] * dt_kick
         state["atom_vel"] = np.where(dyn[:, None], v, state["atom_vel"])
         state["atom_pos"] = np.where(dyn[:, None], state["atom_pos"] + state["atom_vel"] * dt_drift,
                                      state["atom_pos"])
-        state["virial_constraints"] = lincs_hydrogens(state, dt_kick)
-        rattle_hydrogens(state)
+        if rattle_velocities:
+            x_before = state["atom_pos"].copy()
+            state["virial_constraints"] = shake_old_bonds(state, x_ref, dt_kick)
+            dx = (state["atom_pos"] - x_before) / dt_drift
+            state["atom_vel"] = np.where(dyn[:, None], state["atom_vel"] + dx, state["atom_vel"])
+        else:
+            state["virial_constraints"] = lincs_hydrogens(state, dt_kick)
+            rattle_hydrogens(state)
     if len(state["water_vel"]):
         state["water_vel"] = state["water_vel"] + state["water_accel"] * dt_kick
         p, v, m, vir = rigid_water_drift(state["water_pos"], state["water_vel"], dt_drift, lo, ext)

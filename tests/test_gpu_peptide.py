@@ -38,9 +38,10 @@ def test_peptide_forces_match_oracle(gpu_lib, relaxed, mode):
     st.close()
 
 
-def test_constrained_trajectory_matches_oracle(gpu_lib, relaxed):
+@pytest.mark.parametrize("rattle_velocities", [False, True])
+def test_constrained_trajectory_matches_oracle(gpu_lib, relaxed, rattle_velocities):
     cfg = _cfg(relaxed, integ=md.VerletVelocity(thermostat=None), spme_interval=1, zero_com_drift=False,
-               recenter_sim_box=False, reset_angle=False)
+               recenter_sim_box=False, reset_angle=False, rattle_velocities=rattle_velocities)
     st = md.MdState(relaxed, cfg)
     n, dt = 5, 0.002
     st.step(dt, n)
@@ -62,7 +63,7 @@ def test_constrained_trajectory_matches_oracle(gpu_lib, relaxed):
 
     oint.kick_and_calc_accel(s, forces(s), 0.0)
     for _ in range(n):
-        oint.kick_and_drift(s, dt / 2, dt, lo, ext)
+        oint.kick_and_drift(s, dt / 2, dt, lo, ext, rattle_velocities=rattle_velocities)
         oint.kick_and_calc_accel(s, forces(s), dt / 2)
     d = got["atom_pos"].astype(np.float64) - s["atom_pos"]
     d -= np.round(d / ext) * ext
@@ -82,3 +83,22 @@ def test_constraints_hold_under_langevin(gpu_lib, relaxed):
     r = np.linalg.norm(p[c[:, 0]] - p[c[:, 1]], axis=1)
     assert np.max(np.abs(r - relaxed["constraint_r0"]) / relaxed["constraint_r0"]) < 1e-3
     st.close()
+
+
+def test_rattle_velocities_conserve_energy(gpu_lib, relaxed):
+    """Velocity Verlet without thermostat: with the velocities following
+    the constraint corrections the total energy holds; the reference's
+    position-only correction loses kinetic energy every step."""
+    drift = {}
+    for rv in (False, True):
+        cfg = _cfg(relaxed, "corrected", integ=md.VerletVelocity(thermostat=None), spme_interval=1,
+                   zero_com_drift=False, recenter_sim_box=False, reset_angle=False, rattle_velocities=rv)
+        st = md.MdState(relaxed, cfg)
+        e = []
+        for _ in range(20):
+            st.step(0.002, 25)
+            en = st.energies()
+            e.append(en["kinetic_rigid"] + en["potential"])
+        st.close()
+        drift[rv] = np.polyfit(np.arange(len(e)), np.array(e), 1)[0]
+    assert abs(drift[True]) < 0.25 * abs(drift[False]), drift
