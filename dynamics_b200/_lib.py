@@ -99,6 +99,23 @@ class Energies(C.Structure):
         return d
 
 
+class Frame(C.Structure):
+    """dyn_frame_t: one snapshot frame's scalars."""
+    _fields_ = [("step", C.c_uint64)] + [(n, C.c_double) for n in (
+        "time_ps", "kinetic", "potential", "potential_bonded", "temperature", "pressure_bar")] + [
+        ("box_lo", C.c_double * 3), ("box_hi", C.c_double * 3), ("volume", C.c_double),
+        ("density", C.c_double)]
+
+    def as_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_ if n not in ("box_lo", "box_hi")}
+        d["box_lo"] = [self.box_lo[i] for i in range(3)]
+        d["box_hi"] = [self.box_hi[i] for i in range(3)]
+        return d
+
+
+DYN_SNAP_VELOCITIES = 1
+DYN_SNAP_FORCES = 2
+
 _lib = None
 
 _SIGS = {
@@ -139,6 +156,8 @@ _SIGS = {
     "dyn_batch_remove": ([_P, C.c_uint32], C.c_int),
     "dyn_batch_memory": ([_P, _P], C.c_int),
     "dyn_sys_memory": ([_P, _P], C.c_int),
+    "dyn_sys_snapshots": ([_P, C.c_uint32, C.c_uint32, C.c_uint32], C.c_int),
+    "dyn_sys_snapshots_read": ([_P, C.c_uint32, _P, _P, _P, _P, _P, _P], C.c_int),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -67,6 +67,8 @@ struct Scalars {
     unsigned int a_sparse_base;   // first slot of the single-atom clusters
     unsigned int n_ws_items;      // work items of the water-atom pair kernel
     unsigned int n_ss_items;      // work items of the atom-atom pair kernel
+    double time_ps;               // simulated time (sum of the steps' dt)
+    unsigned long long snap_count;  // snapshot frames recorded
 };
 
 // Partial-sum regions (each kernel family writes 4 doubles per block).
@@ -168,6 +170,13 @@ struct SysView {
     uint32_t thermo_dof;
     uint32_t integrator, thermostat, barostat;
     uint32_t spme_interval, com_interval, recenter_interval;
+    // snapshot ring (dyn_sys_snapshots): every snap_ratio steps one frame of
+    // snap_cap; positions / velocities [n_atoms + 3 n_water][3], forces
+    // [n_atoms][3] (NULL = not recorded)
+    uint32_t snap_ratio, snap_cap;
+    float* snap_pos; float* snap_vel; float* snap_force;
+    dyn_frame_t* snap_frames;
+    double total_mass;            // amu, for the frame density
     double e_self;          // Ewald self energy -alpha/sqrt(pi) sum q^2
     // screened-Coulomb force q q (r^-3 + g(r^2)) d: g as a polynomial in
     // t = 2 r^2 / rc^2 - 1 (Chebyshev interpolation, power basis, Horner in

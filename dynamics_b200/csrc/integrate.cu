@@ -622,7 +622,9 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (
         if ((v.flags & DYN_FLAG_RECENTER) && v.recenter_interval && v.na && next % v.recenter_interval == 0)
             due = 1u;
         if ((v.flags & DYN_FLAG_RESET_ANGLE) && v.nw && next % 1000 == 0) due = 1u;
+        if (v.snap_ratio && next % v.snap_ratio == 0) due = 1u;
         sc->step = next;
+        sc->time_ps += (double)dt;
         if (v.use_cond && due) cudaGraphSetConditional(v.cond_periodic, 1u);
     }
 }
@@ -795,6 +797,80 @@ DYN_KERNEL(, k_reset_angle, (), ()) {
 }
 
 
+// ---------------------------------------------------------------------------
+// snapshots (MdState::handle_snapshots, src/snapshot.rs:753-833): after a
+// step whose number is a multiple of snap_ratio, the state goes into frame
+// snap_count % snap_cap of the device ring
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool snapshot_due(const SysView& v) {
+    return v.snap_ratio && v.sc->step % v.snap_ratio == 0;
+}
+
+DYN_KERNEL(, k_snapshot, (), ()) {
+    if (!snapshot_due(v)) return;
+    const uint64_t f = v.sc->snap_count % v.snap_cap;
+    const size_t ns = (size_t)v.na + 3 * (size_t)v.nw;
+    float* P = v.snap_pos + f * ns * 3;
+    float* V = v.snap_vel ? v.snap_vel + f * ns * 3 : nullptr;
+    float* F = v.snap_force ? v.snap_force + f * (size_t)v.na * 3 : nullptr;
+    const BoxDev b = *v.box;
+    const uint32_t tid = bk.idx * blockDim.x + threadIdx.x, stride = bk.cnt * blockDim.x;
+    for (uint32_t a = tid; a < v.na; a += stride) {
+        // atoms in the primary cell (Snapshot::new, src/snapshot.rs:158-161)
+        const float3 p = xyz(v.apos[a]);
+        float w[3] = {p.x, p.y, p.z};
+        for (int k = 0; k < 3; ++k) w[k] -= floorf((w[k] - b.lo[k]) * b.inv_ext[k]) * b.ext[k];
+        P[3 * (size_t)a + 0] = w[0]; P[3 * (size_t)a + 1] = w[1]; P[3 * (size_t)a + 2] = w[2];
+        if (V) {
+            const float4 q = v.avel[a];
+            V[3 * (size_t)a + 0] = q.x; V[3 * (size_t)a + 1] = q.y; V[3 * (size_t)a + 2] = q.z;
+        }
+        if (F) {
+            const long long* fa = v.aforce + 3 * (size_t)a;
+            const long long* fr = v.arecip + 3 * (size_t)a;
+            for (int k = 0; k < 3; ++k) F[3 * (size_t)a + k] = (float)((double)(fa[k] + fr[k]) * DYN_FIX_INV);
+        }
+    }
+    for (uint32_t s = tid; s < v.nw_cap; s += stride) {
+        const uint32_t id = v.wid[s];
+        if (id == INVALID_ID) continue;
+        const size_t o = 3 * ((size_t)v.na + 3 * (size_t)id);
+        for (int k = 0; k < 3; ++k) {
+            const float4 q = v.wpos[4 * s + k];
+            P[o + 3 * k + 0] = q.x; P[o + 3 * k + 1] = q.y; P[o + 3 * k + 2] = q.z;
+            if (V) {
+                const float4 u = v.wvel[3 * s + k];
+                V[o + 3 * k + 0] = u.x; V[o + 3 * k + 1] = u.y; V[o + 3 * k + 2] = u.z;
+            }
+        }
+    }
+}
+
+// the frame's scalars, then the frame count (after k_snapshot has read it)
+DYN_KERNEL(, k_snapshot_done, (), ()) {
+    if (!snapshot_due(v) || bk.idx != 0 || threadIdx.x != 0) return;
+    Scalars* sc = v.sc;
+    const BoxDev b = *v.box;
+    dyn_frame_t r;
+    r.step = sc->step;
+    r.time_ps = sc->time_ps;
+    r.kinetic = sc->acc[ACC_KE];
+    r.potential = sc->pe;
+    r.potential_bonded = sc->acc[ACC_E_BONDED] + sc->acc[ACC_E_14];
+    r.temperature = sc->temperature;
+    r.pressure_bar = sc->pressure;
+    double vol = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        r.box_lo[k] = b.lo[k];
+        r.box_hi[k] = (double)b.lo[k] + (double)b.ext[k];
+        vol *= (double)b.ext[k];
+    }
+    r.volume = vol;
+    r.density = v.total_mass / vol;
+    v.snap_frames[sc->snap_count % v.snap_cap] = r;
+    sc->snap_count += 1ull;
+}
+
 inline int iblocks(const SysView& v, uint64_t n) {
     uint64_t bl = (n + IT - 1) / IT;
     if (bl < 1) bl = 1;
@@ -850,6 +926,13 @@ void launch_finalize(const Target& t, float dt, bool energy, bool thermo) {
              IT, 0);
 }
 
+void launch_snapshot(const Target& t) {
+    t.launch(k_snapshot, k_snapshot_batch,
+             [](const SysView& v) { return v.snap_ratio ? iblocks(v, std::max<uint64_t>(v.na, v.nw_cap)) : 0; },
+             IT, 0);
+    t.launch(k_snapshot_done, k_snapshot_done_batch, [](const SysView& v) { return v.snap_ratio ? 1 : 0; }, 32, 0);
+}
+
 void launch_periodic(const Target& t) {
     auto com = [](const SysView& v) { return (v.flags & DYN_FLAG_COM_REMOVAL) ? (int)v.nb[REG_COM] : 0; };
     t.launch(k_com_reduce, k_com_reduce_batch, com, IT, 0);
@@ -859,6 +942,7 @@ void launch_periodic(const Target& t) {
     t.launch(k_reset_angle, k_reset_angle_batch,
              [](const SysView& v) { return ((v.flags & DYN_FLAG_RESET_ANGLE) && v.nw) ? iblocks(v, v.nw_cap) : 0; },
              IT, 0);
+    launch_snapshot(t);  // after the periodic tasks, as handle_snapshots
 }
 
 }  // namespace dyn

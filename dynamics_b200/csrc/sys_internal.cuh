@@ -30,6 +30,10 @@ struct dyn_sys_s {
     std::vector<void*> allocs;     // every device allocation, freed on destroy
     size_t bytes = 0;              // device memory held (allocations, PME grids, cuFFT work)
     Scalars* h_sc = nullptr;       // pinned mirror of the scalars
+    bool batch_member = false;     // owned by a dyn_batch_t
+    void* snap_mem = nullptr;      // snapshot ring (dyn_sys_snapshots)
+    size_t snap_bytes = 0;
+    uint64_t snap_read = 0;        // frames handed to the host so far
 };
 
 namespace dyn {

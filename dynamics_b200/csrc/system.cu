@@ -318,6 +318,7 @@ extern "C" int dyn_sys_destroy(dyn_sys_t h) {
     if (h->plan_f) cufftDestroy(h->plan_f);
     if (h->plan_b) cufftDestroy(h->plan_b);
     for (void* p : h->allocs) cudaFree(p);
+    if (h->snap_mem) cudaFree(h->snap_mem);
     if (h->h_sc) cudaFreeHost(h->h_sc);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     if (h->aux) cudaStreamDestroy(h->aux);
@@ -419,6 +420,8 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
 
     v.nw = d->n_water;
     v.na = d->n_atoms;
+    v.total_mass = (double)v.nw * (double)OPC_MASS_MOL;
+    for (uint32_t a = 0; a < v.na && d->atom_mass; ++a) v.total_mass += (double)d->atom_mass[a];
     // parameters
     v.rc = rc; v.rc2 = rc * rc; v.ljc2 = ljc * ljc; v.alpha = cfg->ewald_alpha;
     v.buffer = cfg->list_buffer;
@@ -1236,6 +1239,91 @@ extern "C" int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint
 
 extern "C" int dyn_sys_memory(dyn_sys_t h, uint64_t* bytes) {
     DYN_CHECK(h && bytes, DYN_ERR_INVALID, "dyn_sys_memory: NULL argument");
-    *bytes = h->bytes;
+    *bytes = h->bytes + h->snap_bytes;
+    return DYN_OK;
+}
+
+extern "C" int dyn_sys_snapshots(dyn_sys_t h, uint32_t ratio, uint32_t capacity, uint32_t fields) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_snapshots: NULL handle");
+    DYN_CHECK(!h->batch_member, DYN_ERR_UNSUPPORTED, "dyn_sys_snapshots: not for a batch member");
+    DYN_CHECK(ratio == 0 || capacity > 0, DYN_ERR_INVALID, "dyn_sys_snapshots: capacity must be > 0");
+    DYN_CHECK((fields & ~(DYN_SNAP_VELOCITIES | DYN_SNAP_FORCES)) == 0, DYN_ERR_INVALID,
+              "dyn_sys_snapshots: unknown field bits");
+    SysView& v = h->v;
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    // the step graphs carry the view: capture them again with the new ring
+    for (int g = 0; g < 4; ++g)
+        if (h->graph[g]) { cudaGraphExecDestroy(h->graph[g]); h->graph[g] = nullptr; }
+    if (h->snap_mem) { DYN_CUDA(cudaFree(h->snap_mem)); h->snap_mem = nullptr; }
+    h->snap_bytes = 0;
+    v.snap_ratio = 0; v.snap_cap = 0;
+    v.snap_pos = v.snap_vel = v.snap_force = nullptr;
+    v.snap_frames = nullptr;
+    h->snap_read = 0;
+    DYN_CUDA(cudaMemsetAsync(&v.sc->snap_count, 0, sizeof(v.sc->snap_count), h->stream));
+    if (ratio == 0) return DYN_OK;
+    const size_t ns = (size_t)v.na + 3 * (size_t)v.nw;
+    const size_t pos_b = (size_t)capacity * ns * 3 * sizeof(float);
+    const size_t vel_b = (fields & DYN_SNAP_VELOCITIES) ? pos_b : 0;
+    const size_t frc_b = (fields & DYN_SNAP_FORCES) ? (size_t)capacity * v.na * 3 * sizeof(float) : 0;
+    const size_t frm_b = (size_t)capacity * sizeof(dyn_frame_t);
+    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t total = up(pos_b) + up(vel_b) + up(frc_b) + up(frm_b);
+    void* mem = nullptr;
+    const cudaError_t e = cudaMalloc(&mem, total);
+    if (e != cudaSuccess) return dyn::cuda_fail(e, "cudaMalloc (snapshot ring)");
+    h->snap_mem = mem;
+    h->snap_bytes = total;
+    char* p = (char*)mem;
+    v.snap_pos = (float*)p; p += up(pos_b);
+    if (vel_b) v.snap_vel = (float*)p;
+    p += up(vel_b);
+    if (frc_b) v.snap_force = (float*)p;
+    p += up(frc_b);
+    v.snap_frames = (dyn_frame_t*)p;
+    v.snap_ratio = ratio;
+    v.snap_cap = capacity;
+    return DYN_OK;
+}
+
+extern "C" int dyn_sys_snapshots_read(dyn_sys_t h, uint32_t max_frames, float* pos, float* vel, float* force,
+                                      dyn_frame_t* frames, uint32_t* n_read, uint64_t* n_lost) {
+    DYN_CHECK(h && n_read, DYN_ERR_INVALID, "dyn_sys_snapshots_read: NULL argument");
+    *n_read = 0;
+    if (n_lost) *n_lost = 0;
+    const SysView& v = h->v;
+    if (!v.snap_ratio) return DYN_OK;
+    DYN_CHECK(pos || max_frames == 0, DYN_ERR_INVALID, "dyn_sys_snapshots_read: NULL pos");
+    DYN_CHECK(!vel || v.snap_vel, DYN_ERR_INVALID, "dyn_sys_snapshots_read: velocities are not recorded");
+    DYN_CHECK(!force || v.snap_force, DYN_ERR_INVALID, "dyn_sys_snapshots_read: forces are not recorded");
+    unsigned long long count = 0;
+    DYN_CUDA(cudaMemcpyAsync(&count, &v.sc->snap_count, sizeof(count), cudaMemcpyDeviceToHost, h->stream));
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    const uint64_t cap = v.snap_cap;
+    const uint64_t first = std::max<uint64_t>(h->snap_read, count > cap ? count - cap : 0);
+    if (n_lost) *n_lost = first - h->snap_read;
+    const uint64_t n = std::min<uint64_t>(count - first, max_frames);
+    const size_t ns = (size_t)v.na + 3 * (size_t)v.nw;
+    const size_t fp = ns * 3, ff = (size_t)v.na * 3;
+    // frames first .. first + n - 1 sit in at most two contiguous ranges of the ring
+    for (uint64_t i = 0; i < n;) {
+        const uint64_t slot = (first + i) % cap;
+        const uint64_t run = std::min<uint64_t>(n - i, cap - slot);
+        DYN_CUDA(cudaMemcpyAsync(pos + i * fp, v.snap_pos + slot * fp, run * fp * sizeof(float),
+                                 cudaMemcpyDeviceToHost, h->stream));
+        if (vel)
+            DYN_CUDA(cudaMemcpyAsync(vel + i * fp, v.snap_vel + slot * fp, run * fp * sizeof(float),
+                                     cudaMemcpyDeviceToHost, h->stream));
+        if (force && ff)
+            DYN_CUDA(cudaMemcpyAsync(force + i * ff, v.snap_force + slot * ff, run * ff * sizeof(float),
+                                     cudaMemcpyDeviceToHost, h->stream));
+        if (frames)
+            DYN_CUDA(cudaMemcpyAsync(frames + i, v.snap_frames + slot, run * sizeof(dyn_frame_t),
+                                     cudaMemcpyDeviceToHost, h->stream));
+        i += run;
+    }
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    h->snap_read = first + n;
+    *n_read = (uint32_t)n;
     return DYN_OK;
 }

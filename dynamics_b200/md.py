@@ -300,6 +300,47 @@ class MdState:
         check(lib().dyn_sys_memory(self.handle, C.byref(b)))
         return b.value
 
+    def enable_snapshots(self, ratio, capacity=256, velocities=False, forces=False):
+        """Record a snapshot into a device ring every ``ratio`` steps
+        (SnapshotHandlers.memory, src/snapshot.rs:33-57 and 753-776): the
+        step graph writes the frames; read_snapshots() copies them out.
+        ratio 0 stops recording."""
+        fields = (_lib.DYN_SNAP_VELOCITIES if velocities else 0) | (_lib.DYN_SNAP_FORCES if forces else 0)
+        check(lib().dyn_sys_snapshots(self.handle, int(ratio), int(capacity), fields))
+        self._snap = (int(ratio), int(capacity), bool(velocities), bool(forces))
+
+    def read_snapshots(self, max_frames=None):
+        """The frames recorded since the last read, oldest first: a list of
+        dicts with step, time_ps, energies, box, ``pos`` (n_sites, 3) in the
+        layout atoms (wrapped into the box) then O, H0, H1 of each water,
+        ``vel`` (same layout) and ``force`` (n_atoms, 3) when recorded, and
+        ``lost`` on the first frame (frames overwritten unread)."""
+        ratio, cap, with_v, with_f = getattr(self, "_snap", (0, 0, False, False))
+        if not ratio:
+            return []
+        n = cap if max_frames is None else min(cap, int(max_frames))
+        ns = self.n_atoms + 3 * self.n_water
+        pos = np.zeros((n, ns, 3), np.float32)
+        vel = np.zeros((n, ns, 3), np.float32) if with_v else None
+        frc = np.zeros((n, max(self.n_atoms, 1), 3), np.float32) if with_f else None
+        frames = (_lib.Frame * max(n, 1))()
+        got, lost = C.c_uint32(), C.c_uint64()
+        check(lib().dyn_sys_snapshots_read(self.handle, n, ptr(pos), ptr(vel) if with_v else None,
+                                           ptr(frc) if with_f and self.n_atoms else None, C.addressof(frames),
+                                           C.byref(got), C.byref(lost)))
+        out = []
+        for i in range(got.value):
+            d = frames[i].as_dict()
+            d["pos"] = pos[i]
+            if with_v:
+                d["vel"] = vel[i]
+            if with_f:
+                d["force"] = frc[i][:self.n_atoms]
+            out.append(d)
+        if out:
+            out[0]["lost"] = lost.value
+        return out
+
     def launches_per_step(self, spme=True):
         """Kernels of a step without a list rebuild or periodic task."""
         n = C.c_uint32()

@@ -395,6 +395,52 @@ int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
 int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic);
 
 /* ------------------------------------------------------------------ */
+/* Device-resident snapshots (trajectory output)                      */
+/* ------------------------------------------------------------------ */
+
+/* dyn_sys_snapshots fields */
+#define DYN_SNAP_VELOCITIES 1u  /* velocities, same layout as positions      */
+#define DYN_SNAP_FORCES 2u      /* total force on each atom (float32)        */
+
+/* One recorded frame's scalars (Snapshot / SnapshotEnergyData,
+ * src/snapshot.rs:59-220).  Energies are those of the last step that
+ * computed them (every energy_interval steps). */
+typedef struct {
+    uint64_t step;
+    double time_ps;
+    double kinetic;           /* kcal/mol, as dyn_energies_t.kinetic        */
+    double potential;         /* kcal/mol                                   */
+    double potential_bonded;  /* kcal/mol (bonded + 1-4)                    */
+    double temperature;       /* K                                          */
+    double pressure_bar;
+    double box_lo[3], box_hi[3];
+    double volume;            /* A^3                                        */
+    double density;           /* amu / A^3 (src/snapshot.rs:206-211)        */
+} dyn_frame_t;
+
+/* Device side of MdState::handle_snapshots (src/snapshot.rs:753-833):
+ * after every step whose number is a multiple of ratio, after the periodic
+ * tasks as in the reference (src/integrate.rs:408-466), the step graph
+ * copies the state into a ring of capacity frames in device memory, with
+ * no host synchronisation.  A frame holds the positions of every site in
+ * home order -- the atoms wrapped into the box, then O, H0, H1 of each
+ * water (the reference's DCD layout, src/snapshot.rs:293-313) -- as float
+ * [n_sites * 3] with n_sites = n_atoms + 3 * n_water, optionally the
+ * velocities (same layout) and the atoms' total forces [n_atoms * 3], and a
+ * dyn_frame_t.  ratio = 0 turns recording off and frees the ring.  Resets
+ * the ring; not for a batch member. */
+int dyn_sys_snapshots(dyn_sys_t h, uint32_t ratio, uint32_t capacity, uint32_t fields);
+
+/* Copies the frames recorded since the last read, oldest first, at most
+ * max_frames, into host buffers (pos [n * n_sites * 3]; vel likewise or
+ * NULL; force [n * n_atoms * 3] or NULL; frames [n] or NULL), after the
+ * work queued on the handle's stream.  *n_read receives the frames copied,
+ * *n_lost (may be NULL) the frames overwritten in the ring before they
+ * were read.  Host buffers should be page-locked for full bandwidth. */
+int dyn_sys_snapshots_read(dyn_sys_t h, uint32_t max_frames, float* pos, float* vel, float* force,
+                           dyn_frame_t* frames, uint32_t* n_read, uint64_t* n_lost);
+
+/* ------------------------------------------------------------------ */
 /* Batched form: many independent systems, one launch per stage      */
 /* ------------------------------------------------------------------ */
 

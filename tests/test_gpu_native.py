@@ -224,3 +224,40 @@ def test_graph_counters_and_periodic_tasks(gpu_lib):
     st.step(0.002, 7)
     assert st.energies()["step"] == 107
     st.close()
+
+
+def test_snapshots_match_state(gpu_lib):
+    """Frames recorded by the step graph equal the state read back at the
+    same steps; frames that overflow the ring are counted as lost."""
+    sysd = mixed()
+    cfg = _cfg(sysd, integ=md.LangevinMiddle(gamma=1.0), seed=5)
+    st = md.MdState(sysd, cfg)
+    st.enable_snapshots(ratio=5, capacity=4, velocities=True, forces=True)
+    ref = []
+    for _ in range(3):
+        st.step(0.002, 5)
+        s = st.state()
+        ref.append(s)
+    frames = st.read_snapshots()
+    assert [f["step"] for f in frames] == [5, 10, 15]
+    lo = sysd["box_lo"].astype(np.float64)
+    ext = (sysd["box_hi"] - sysd["box_lo"]).astype(np.float64)
+    for f, s in zip(frames, ref):
+        na = len(s["atom_pos"])
+        wrapped = s["atom_pos"] - np.floor((s["atom_pos"] - lo) / ext) * ext
+        np.testing.assert_allclose(f["pos"][:na], wrapped, atol=1e-4)
+        np.testing.assert_array_equal(f["pos"][na:], s["water_pos"].reshape(-1, 3))
+        np.testing.assert_array_equal(f["vel"][:na], s["atom_vel"])
+        np.testing.assert_array_equal(f["vel"][na:], s["water_vel"].reshape(-1, 3))
+        assert f["force"].shape == (na, 3) and np.all(np.isfinite(f["force"]))
+        # time is the sum of the float32 step lengths
+        assert abs(f["time_ps"] - float(np.float32(0.002)) * f["step"]) < 1e-9
+        assert f["volume"] > 0 and f["density"] > 0
+    assert frames[0]["lost"] == 0
+    st.step(0.002, 30)  # 6 frames into a ring of 4
+    more = st.read_snapshots()
+    assert [f["step"] for f in more] == [30, 35, 40, 45] and more[0]["lost"] == 2
+    st.enable_snapshots(0)
+    st.step(0.002, 5)
+    assert st.read_snapshots() == []
+    st.close()
