@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libdynb200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["errors.cu", "nb_compat.cu", "nblist.cu", "pair.cu", "pme.cu", "integrate.cu",
-           "bonded.cu", "system.cu", "batch.cu", "nb_static.cu"]
+           "bonded.cu", "system.cu", "batch.cu", "nb_static.cu", "minimize.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -69,6 +69,11 @@ struct Scalars {
     unsigned int n_ss_items;      // work items of the atom-atom pair kernel
     double time_ps;               // simulated time (sum of the steps' dt)
     unsigned long long snap_count;  // snapshot frames recorded
+    // steepest-descent minimizer (dyn_sys_minimize)
+    double min_e_prev;            // energy of the last accepted geometry
+    float min_alpha, min_alpha_try, min_fmax, min_step;
+    unsigned int min_fmax_bits, min_ctr;
+    unsigned int min_accepted, min_trials, min_done, min_action;
 };
 
 // Partial-sum regions (each kernel family writes 4 doubles per block).
@@ -342,6 +347,8 @@ void launch_pairs(const Target& t, bool energy);
 // (the latter adds to the water forces the former stores), and atom-atom
 void launch_pairs_water(const Target& t, bool energy);
 void launch_pairs_atoms(const Target& t, bool energy);
+// the water-atom kernel alone (part of launch_pairs_water)
+void launch_pairs_ws(const Target& t, bool energy);
 void launch_pair14(const Target& t, bool energy);
 int pair_ww_setup(const SysView& v);
 int ww_tile_blocks(const SysView& v);

@@ -545,8 +545,12 @@ void launch_pairs_water(const Target& t, bool energy) {
              [&](const SysView& v) { return v.nw && eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
     t.launch(k_pair_ww_tile<false>, k_pair_ww_tile_batch<false>,
              [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
-    auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
     // the water-atom kernel adds to the water forces the water-water kernel stores
+    launch_pairs_ws(t, energy);
+}
+
+void launch_pairs_ws(const Target& t, bool energy) {
+    auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
     if (energy) t.launch(k_pair_ws<true>, k_pair_ws_batch<true>, ws, PT, 0);
     else t.launch(k_pair_ws<false>, k_pair_ws_batch<false>, ws, PT, 0);
 }

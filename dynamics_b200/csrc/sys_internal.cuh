@@ -46,6 +46,9 @@ int end_if_body(cudaStream_t aux);
 int read_scalars(dyn_sys_s* h);
 // Kernel nodes of a graph (library kernels included).
 int count_graph_kernels(cudaGraph_t g, uint32_t* n);
+// Full forces, energies and accelerations at the current coordinates (list
+// rebuilt), synchronous.
+int evaluate_forces(dyn_sys_s* h);
 
 // The parts of a step, enqueued on T's stream; with fork (only while a graph
 // is being captured) the independent work goes to the side targets A and P

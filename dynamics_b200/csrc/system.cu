@@ -266,6 +266,11 @@ void enqueue_forces(dyn_sys_s* h, bool force_rebuild) {
     dyn::launch_finalize(T, 0.0f, true, false);
 }
 
+int evaluate_forces_now(dyn_sys_s* h) {
+    enqueue_forces(h, true);
+    return dyn::read_scalars(h);
+}
+
 }  // namespace
 namespace dyn {
 int read_scalars(dyn_sys_s* h) {
@@ -1327,3 +1332,7 @@ extern "C" int dyn_sys_snapshots_read(dyn_sys_t h, uint32_t max_frames, float* p
     *n_read = (uint32_t)n;
     return DYN_OK;
 }
+
+namespace dyn {
+int evaluate_forces(dyn_sys_s* h) { return evaluate_forces_now(h); }
+}  // namespace dyn

@@ -300,6 +300,17 @@ class MdState:
         check(lib().dyn_sys_memory(self.handle, C.byref(b)))
         return b.value
 
+    def minimize_energy(self, max_iters=1000, tolerance=1000.0 * 0.0239005):
+        """Steepest-descent relaxation of the atoms on the device
+        (MdState::minimize_energy, src/minimize_energy.rs:60-260; the
+        defaults are the reference's max_init_relaxation_iters and
+        energy_minimization_tolerance, src/config.rs:122-126).  Returns
+        (accepted steps, potential energy of the atom terms without the
+        reciprocal part, kcal/mol)."""
+        it, e = C.c_uint32(), C.c_double()
+        check(lib().dyn_sys_minimize(self.handle, int(max_iters), float(tolerance), C.byref(it), C.byref(e)))
+        return it.value, e.value
+
     def enable_snapshots(self, ratio, capacity=256, velocities=False, forces=False):
         """Record a snapshot into a device ring every ``ratio`` steps
         (SnapshotHandlers.memory, src/snapshot.rs:33-57 and 753-776): the

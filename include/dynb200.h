@@ -394,6 +394,22 @@ int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
  * under conditional nodes that the device sets. */
 int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic);
 
+/* Steepest-descent energy minimization of the atoms
+ * (MdState::minimize_energy, src/minimize_energy.rs:60-260), the
+ * reference's algorithm: waters and static atoms fixed, reciprocal-space
+ * forces off, each trial moving every atom by F * step / F_max with step =
+ * min(alpha F_max, 0.2 A); a trial that does not raise the potential energy
+ * is accepted (alpha * 1.2, at most 0.01), one that does is reverted (alpha
+ * / 2; stop below 1e-8).  Stops after max_iters accepted steps or when the
+ * largest force is at most tolerance (kcal/mol/A; the reference's default
+ * is 23.9005).  All decisions are taken on the device; the host only reads
+ * a done flag every few trials.  Velocities are kept; forces and
+ * accelerations are evaluated again (with the reciprocal part) at the end.
+ * *iters (may be NULL): accepted steps; *energy (may be NULL): potential
+ * energy of the atom terms without the reciprocal part, kcal/mol.
+ * Synchronous; not for a batch member. */
+int dyn_sys_minimize(dyn_sys_t h, uint32_t max_iters, float tolerance, uint32_t* iters, double* energy);
+
 /* ------------------------------------------------------------------ */
 /* Device-resident snapshots (trajectory output)                      */
 /* ------------------------------------------------------------------ */

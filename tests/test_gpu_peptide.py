@@ -102,3 +102,38 @@ def test_rattle_velocities_conserve_energy(gpu_lib, relaxed):
         st.close()
         drift[rv] = np.polyfit(np.arange(len(e)), np.array(e), 1)[0]
     assert abs(drift[True]) < 0.25 * abs(drift[False]), drift
+
+
+def test_minimizer_matches_oracle(gpu_lib):
+    """Steepest descent on the device against the float64 restatement of
+    src/minimize_energy.rs: same accepted steps, positions and energy."""
+    from oracle import minimize as omin
+    sysd = _system(seed=9)
+    cfg = _cfg(sysd)
+    st = md.MdState(sysd, cfg)
+    n_it, e = st.minimize_energy(max_iters=12, tolerance=0.0)
+    got = st.state()["atom_pos"].astype(np.float64)
+    st.close()
+    params = {"cutoff": cfg.coulomb_cutoff, "lj_cutoff": cfg.lj_cutoff,
+              "alpha": float(np.float32(cfg.spme_alpha)), "grid": cfg.spme_grid, "mode": "reference"}
+    x, n_ref, e_ref = omin.minimize_energy(sysd, params, 12, 0.0)
+    assert n_it == n_ref == 12
+    assert abs(e - e_ref) <= 1e-5 * abs(e_ref), (e, e_ref)
+    box = (sysd["box_hi"] - sysd["box_lo"]).astype(np.float64)
+    d = got - x
+    d -= np.round(d / box) * box
+    assert np.max(np.abs(d)) < 2e-3
+
+
+def test_minimizer_lowers_energy_and_forces(gpu_lib):
+    sysd = _system(seed=10)
+    cfg = _cfg(sysd)
+    st = md.MdState(sysd, cfg)
+    f0 = np.linalg.norm(st.forces()["f_atoms"], axis=1).max()
+    n_it, e = st.minimize_energy(max_iters=300)
+    f1 = np.linalg.norm(st.forces()["f_atoms"], axis=1).max()
+    assert 0 < n_it <= 300 and np.isfinite(e)
+    assert f1 < f0
+    st.step(0.002, 20)  # the system runs on from the minimized geometry
+    assert np.isfinite(st.energies()["temperature"])
+    st.close()
