@@ -158,6 +158,7 @@ _SIGS = {
     "dyn_sys_memory": ([_P, _P], C.c_int),
     "dyn_sys_snapshots": ([_P, C.c_uint32, C.c_uint32, C.c_uint32], C.c_int),
     "dyn_sys_minimize": ([_P, C.c_uint32, C.c_float, _P, _P], C.c_int),
+    "dyn_sys_set_static": ([_P, _P, C.c_uint32], C.c_int),
     "dyn_sys_snapshots_read": ([_P, C.c_uint32, _P, _P, _P, _P, _P, _P], C.c_int),
 }
 

@@ -1248,6 +1248,42 @@ extern "C" int dyn_sys_memory(dyn_sys_t h, uint64_t* bytes) {
     return DYN_OK;
 }
 
+#define TRYC_ALLOC(ptr_, n_)                                       \
+    do {                                                           \
+        const int rc_a = dev_alloc(h, &(ptr_), (n_), true);        \
+        if (rc_a != DYN_OK) return rc_a;                           \
+    } while (0)
+
+extern "C" int dyn_sys_set_static(dyn_sys_t h, const uint8_t* atom_static, uint32_t thermo_dof) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_set_static: NULL handle");
+    DYN_CHECK(!h->batch_member, DYN_ERR_UNSUPPORTED, "dyn_sys_set_static: not for a batch member");
+    SysView& v = h->v;
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    if (v.na) {
+        if (!v.astatic) {
+            // the step graphs carry the view: capture them again
+            for (int g = 0; g < 4; ++g)
+                if (h->graph[g]) { cudaGraphExecDestroy(h->graph[g]); h->graph[g] = nullptr; }
+            TRYC_ALLOC(v.astatic, v.na);
+        }
+        if (atom_static)
+            DYN_CUDA(cudaMemcpyAsync(v.astatic, atom_static, v.na, cudaMemcpyHostToDevice, h->stream));
+        else
+            DYN_CUDA(cudaMemsetAsync(v.astatic, 0, v.na, h->stream));
+    }
+    if (thermo_dof && thermo_dof != v.thermo_dof) {
+        for (int g = 0; g < 4; ++g)
+            if (h->graph[g]) { cudaGraphExecDestroy(h->graph[g]); h->graph[g] = nullptr; }
+        v.thermo_dof = thermo_dof;
+        h->cfg.thermo_dof = thermo_dof;
+    }
+    // the cluster-pair masks leave out pairs of two static atoms
+    const unsigned int one = 1u;
+    DYN_CUDA(cudaMemcpyAsync(&v.sc->need_rebuild, &one, sizeof(one), cudaMemcpyHostToDevice, h->stream));
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    return DYN_OK;
+}
+
 extern "C" int dyn_sys_snapshots(dyn_sys_t h, uint32_t ratio, uint32_t capacity, uint32_t fields) {
     DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_snapshots: NULL handle");
     DYN_CHECK(!h->batch_member, DYN_ERR_UNSUPPORTED, "dyn_sys_snapshots: not for a batch member");

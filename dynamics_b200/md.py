@@ -80,12 +80,19 @@ class MdConfig:
 
 
 def thermo_dof(system, cfg):
-    """dof_for_thermo (src/thermostat.rs:220-251)."""
+    """dof_for_thermo (src/thermostat.rs:220-251): 6 per water, 3 per
+    non-static atom, minus 3 with COM removal.  The reference subtracts the
+    constrained hydrogens only for its SHAKE constraints, not for the
+    default LINCS-style ones; here they are subtracted (non-static ones)
+    with the RATTLE option, the constrained integrator that holds them."""
     nw = len(np.asarray(system.get("water_pos", np.zeros((0, 3, 3)))).reshape(-1, 3, 3))
     na = len(np.asarray(system.get("atom_pos", np.zeros((0, 3)))).reshape(-1, 3))
     st = np.asarray(system.get("atom_static", np.zeros(na, bool)), dtype=bool)
     dof = 6 * nw + 3 * int(np.count_nonzero(~st))
-    dof -= len(np.asarray(system.get("constraints", np.zeros((0, 2)))).reshape(-1, 2))
+    if getattr(cfg, "rattle_velocities", False):
+        cons = np.asarray(system.get("constraints", np.zeros((0, 2))), np.int64).reshape(-1, 2)
+        if len(cons):
+            dof -= int(np.count_nonzero(~st[cons[:, 1]]))
     if cfg.zero_com_drift:
         dof -= 3
     return max(dof, 0)
@@ -218,6 +225,7 @@ class MdState:
         self._h = h
         self._owned = True
         self._cstruct = c
+        self._static = np.asarray(system.get("atom_static", np.zeros(self.n_atoms, bool)), bool).reshape(-1)
 
     @classmethod
     def _member(cls, handle, system, cfg):
@@ -229,6 +237,7 @@ class MdState:
         self.n_atoms = len(np.asarray(system.get("atom_pos", np.zeros((0, 3)))).reshape(-1, 3))
         self._h = handle
         self._owned = False
+        self._static = np.asarray(system.get("atom_static", np.zeros(self.n_atoms, bool)), bool).reshape(-1)
         return self
 
     @property
@@ -299,6 +308,29 @@ class MdState:
         b = C.c_uint64()
         check(lib().dyn_sys_memory(self.handle, C.byref(b)))
         return b.value
+
+    def set_static(self, mask=None):
+        """Atoms held fixed (bool (n_atoms,), None = none), with the
+        thermostat's degrees of freedom following (dof_for_thermo)."""
+        na = self.n_atoms
+        m = np.zeros(na, bool) if mask is None else np.asarray(mask, bool).reshape(na)
+        sysd = dict(self.system, atom_static=m)
+        mu = np.ascontiguousarray(m, np.uint8)  # alive through the call
+        check(lib().dyn_sys_set_static(self.handle, ptr(mu) if na else None, int(thermo_dof(sysd, self.cfg))))
+        self._static = m
+
+    def relax_solvent(self, n_steps=200, dt=0.0005):
+        """The solvent relaxes around the frozen solute: every atom static
+        for ``n_steps`` steps of ``dt`` ps, then the atoms' own static
+        flags back (MdState::md_on_solute_only, src/solvent/init.rs:773-805;
+        200 steps of 0.5 fs are the reference's values for water,
+        :64-69)."""
+        keep = self._static.copy()
+        self.set_static(np.ones(self.n_atoms, bool))
+        try:
+            self.step(dt, n_steps)
+        finally:
+            self.set_static(keep)
 
     def minimize_energy(self, max_iters=1000, tolerance=1000.0 * 0.0239005):
         """Steepest-descent relaxation of the atoms on the device

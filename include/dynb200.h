@@ -394,6 +394,14 @@ int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
  * under conditional nodes that the device sets. */
 int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic);
 
+/* Replaces the atoms' static flags (1 = held fixed; NULL = none) and the
+ * thermostat degrees of freedom (0 = keep), between steps, e.g. to freeze
+ * the solute while the solvent relaxes around it (MdState::md_on_solute_only,
+ * src/solvent/init.rs:773-805, with mark_solute_static_for_init_relaxation
+ * and restore_static_state, :745-762).  The next step rebuilds the lists
+ * (pairs of two static atoms are skipped). */
+int dyn_sys_set_static(dyn_sys_t h, const uint8_t* atom_static, uint32_t thermo_dof);
+
 /* Steepest-descent energy minimization of the atoms
  * (MdState::minimize_energy, src/minimize_energy.rs:60-260), the
  * reference's algorithm: waters and static atoms fixed, reciprocal-space

@@ -137,3 +137,19 @@ def test_minimizer_lowers_energy_and_forces(gpu_lib):
     st.step(0.002, 20)  # the system runs on from the minimized geometry
     assert np.isfinite(st.energies()["temperature"])
     st.close()
+
+
+def test_relax_solvent_holds_the_solute(gpu_lib):
+    """md_on_solute_only: the atoms stay put while the waters move; the
+    atoms' own static flags come back afterwards."""
+    sysd = _system(seed=11)
+    cfg = _cfg(sysd, integ=md.LangevinMiddle(gamma=1.0))
+    st = md.MdState(sysd, cfg)
+    a0 = st.state()
+    st.relax_solvent(n_steps=50, dt=0.0005)
+    a1 = st.state()
+    np.testing.assert_array_equal(a1["atom_pos"], a0["atom_pos"])
+    assert np.max(np.abs(a1["water_pos"] - a0["water_pos"])) > 1e-3
+    st.step(0.002, 10)
+    assert np.max(np.abs(st.state()["atom_pos"] - a1["atom_pos"])) > 1e-4
+    st.close()
