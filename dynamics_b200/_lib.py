@@ -63,6 +63,8 @@ class Config(C.Structure):
         ("flags", C.c_uint32), ("thermo_dof", C.c_uint32), ("seed", C.c_uint64),
         ("ww_union_chunk", C.c_uint32), ("lincs_order", C.c_uint32), ("lincs_iter", C.c_uint32),
         ("reserved0", C.c_uint32),
+        ("alch_begin", C.c_uint32), ("alch_end", C.c_uint32), ("alch_lambda", C.c_float),
+        ("reserved1", C.c_uint32),
     ]
 
 
@@ -91,7 +93,7 @@ class Energies(C.Structure):
         "virial_bonded", "virial_constraints", "pressure_bar", "temperature")] + [
         ("box", C.c_double * 3), ("step", C.c_uint64), ("list_rebuilds", C.c_uint64),
         ("pairs_in_list", C.c_uint64), ("kinetic_rigid", C.c_double),
-        ("pressure_atomic_bar", C.c_double), ("list_union_max", C.c_uint64)]
+        ("pressure_atomic_bar", C.c_double), ("list_union_max", C.c_uint64), ("dh_dl", C.c_double)]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_ if n != "box"}
@@ -104,7 +106,7 @@ class Frame(C.Structure):
     _fields_ = [("step", C.c_uint64)] + [(n, C.c_double) for n in (
         "time_ps", "kinetic", "potential", "potential_bonded", "temperature", "pressure_bar")] + [
         ("box_lo", C.c_double * 3), ("box_hi", C.c_double * 3), ("volume", C.c_double),
-        ("density", C.c_double)]
+        ("density", C.c_double), ("dh_dl", C.c_double)]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_ if n not in ("box_lo", "box_hi")}
@@ -159,6 +161,7 @@ _SIGS = {
     "dyn_sys_snapshots": ([_P, C.c_uint32, C.c_uint32, C.c_uint32], C.c_int),
     "dyn_sys_minimize": ([_P, C.c_uint32, C.c_float, _P, _P], C.c_int),
     "dyn_sys_set_static": ([_P, _P, C.c_uint32], C.c_int),
+    "dyn_sys_set_lambda": ([_P, C.c_float], C.c_int),
     "dyn_sys_snapshots_read": ([_P, C.c_uint32, _P, _P, _P, _P, _P, _P], C.c_int),
 }
 

@@ -69,6 +69,11 @@ struct Scalars {
     unsigned int n_ss_items;      // work items of the atom-atom pair kernel
     double time_ps;               // simulated time (sum of the steps' dt)
     unsigned long long snap_count;  // snapshot frames recorded
+    // reciprocal energy / virial of the SPME passes of one evaluation, their
+    // dH/dlambda (alchemical cross term), its cached value and the step's
+    // total dH/dlambda
+    double recip_acc[2];
+    double recip_dh, recip_dh_cache, dh_dl;
     // steepest-descent minimizer (dyn_sys_minimize)
     double min_e_prev;            // energy of the last accepted geometry
     float min_alpha, min_alpha_try, min_fmax, min_step;
@@ -182,6 +187,11 @@ struct SysView {
     float* snap_pos; float* snap_vel; float* snap_force;
     dyn_frame_t* snap_frames;
     double total_mass;            // amu, for the frame density
+    // alchemical decoupling of atoms [alch_lo, alch_hi) on the staged
+    // schedule: Coulomb scale and its lambda derivative, soft-core LJ
+    // lambda and its lambda derivative
+    uint32_t alch_on, alch_lo, alch_hi;
+    float alch_cs, alch_dcs, alch_ll, alch_dll;
     double e_self;          // Ewald self energy -alpha/sqrt(pi) sum q^2
     // screened-Coulomb force q q (r^-3 + g(r^2)) d: g as a polynomial in
     // t = 2 r^2 / rc^2 - 1 (Chebyshev interpolation, power basis, Horner in

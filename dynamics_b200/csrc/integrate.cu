@@ -542,6 +542,8 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (
         sc->acc[ACC_E_COUL_S] = x[4];
         sc->acc[ACC_E_14] = x[6];
         sc->acc[ACC_E_BONDED] = x[8];
+        // alchemical dH/dlambda: short-range cross pairs + SPME cross term
+        sc->dh_dl = ws[3] + ss[3] + sc->recip_dh_cache;
     }
     sc->acc[ACC_VIR_SHORT] = 0.5 * x[2] + x[5] + x[7];
     sc->acc[ACC_VIR_14] = x[7];
@@ -867,6 +869,7 @@ DYN_KERNEL(, k_snapshot_done, (), ()) {
     }
     r.volume = vol;
     r.density = v.total_mass / vol;
+    r.dh_dl = sc->dh_dl;
     v.snap_frames[sc->snap_count % v.snap_cap] = r;
     sc->snap_count += 1ull;
 }

@@ -84,6 +84,42 @@ __device__ __forceinline__ void lj(float3 pi, float3 pj, float3 sh, float sig2, 
     }
 }
 
+// Soft-core LJ of a pair between the alchemical molecule and the rest
+// (Beutler et al., Chem. Phys. Lett. 222, 529 (1994), as
+// alchemical_lj_soft_core_decouple, src/non_bonded.rs:883-941, with the
+// reference's sc-alpha 0.5, power 1 and soft-core sigma >= 3 A,
+// src/alchemical.rs:55-65): V = (1 - l) V_LJ(r_sc) with
+// r_sc^6 = r^6 + 0.5 s^6 l, s = max(sigma, 3); force (1 - l) F_LJ(r_sc)
+// (r / r_sc)^5; dV/dl = -V_LJ(r_sc) - (1 - l) F_LJ(r_sc) 0.5 s^6 / (6 r_sc^5),
+// times dl/dlambda of the schedule (dlam) into dh.
+template <bool ENERGY>
+__device__ __forceinline__ void lj_soft(float3 pi, float3 pj, float3 sh, float sig, float eps, float ljc2,
+                                        float lam, float dlam, float3& f, Acc3& a, double& dh) {
+    const float3 d = pi - (pj - sh);
+    const float r2 = dot3(d, d);
+    if (!(r2 <= ljc2) || !(r2 > 0.f) || eps == 0.f) return;
+    const float ss = fmaxf(sig, 3.0f), ss2 = ss * ss;
+    const float ss6 = ss2 * ss2 * ss2;
+    const float rsc6 = fmaf(0.5f * ss6, lam, r2 * r2 * r2);
+    const float rsc = sqrtf(cbrtf(rsc6));
+    const float inv_rsc = 1.0f / rsc;
+    const float sr = sig * inv_rsc, sr2 = sr * sr;
+    const float sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
+    const float hf = 24.0f * eps * fmaf(2.0f, sr12, -sr6) * inv_rsc;
+    const float he = 4.0f * eps * (sr12 - sr6);
+    const float scale = 1.0f - lam;
+    const float r = sqrtf(r2);
+    const float q = r * inv_rsc, q2 = q * q;
+    const float fs = hf * scale * (q2 * q2 * q) / r;
+    f.x = fmaf(fs, d.x, f.x); f.y = fmaf(fs, d.y, f.y); f.z = fmaf(fs, d.z, f.z);
+    a.w = fmaf(fs, r2, a.w);
+    if (ENERGY) {
+        const double rsc5 = (double)rsc6 / (double)rsc;
+        a.e_lj += (double)scale * (double)he;
+        dh += (double)dlam * (-(double)he - (double)scale * (double)hf * (0.5 * (double)ss6) / (6.0 * rsc5));
+    }
+}
+
 __device__ __forceinline__ float3 shift_of(float3 d, const BoxDev& b) {
     return f3(-rintf(d.x * b.inv_ext[0]) * b.ext[0], -rintf(d.y * b.inv_ext[1]) * b.ext[1],
               -rintf(d.z * b.inv_ext[2]) * b.ext[2]);
@@ -106,12 +142,12 @@ __device__ __forceinline__ void add_fix3(long long* p, float3 f) {
 
 template <bool ENERGY>
 __device__ __forceinline__ void write_partials(const SysView& v, Blk bk, int region, double el,
-                                               double ec, double w) {
-    double x[3] = {el, ec, w};
-    block_sum_d<3>(x);
+                                               double ec, double w, double dh = 0.0) {
+    double x[4] = {el, ec, w, dh};
+    block_sum_d<4>(x);
     if (threadIdx.x == 0) {
         double* p = v.partials + ((size_t)region * v.max_blocks + bk.idx) * 4;
-        p[0] = x[0]; p[1] = x[1]; p[2] = x[2]; p[3] = 0.0;
+        p[0] = x[0]; p[1] = x[1]; p[2] = x[2]; p[3] = x[3];
     }
 }
 
@@ -319,14 +355,14 @@ __device__ __forceinline__ JAtoms load_jatoms(const SysView& v, uint32_t cj, int
 // forces) are reduce-scattered over the 8 water lanes of a j-group and added
 // with integer atomics (24 per entry).
 // ---------------------------------------------------------------------------
-DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT, 4), k_pair_ws, (), ()) {
+DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT, 4), k_pair_ws, (), ()) {
     const int lane = threadIdx.x & 31;
     const int ii = lane & 7, jq = lane >> 3;
     const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nit = v.sc->n_ws_items;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
-    double el = 0.0, ec = 0.0, ew = 0.0;
+    double el = 0.0, ec = 0.0, ew = 0.0, dh = 0.0;
     for (uint32_t it = ((bk.idx * blockDim.x + threadIdx.x) >> 5); it < nit; it += nwarps) {
         const uint2 item = v.ws_item[it];
         const uint32_t ci = item.x, k0 = item.y;
@@ -356,10 +392,23 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT, 4), k_pair_ws, (), (
                     const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
                     const float ep = sqrtf(OPC_O_EPS * lj_j.y);
                     const double qe = (double)pj.w;
-                    lj<ENERGY>(iO, js, z0, sg * sg, ep, ljc2, 1.0f, fo, a);
-                    coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
-                    coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
-                    coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
+                    if (ALCH && aj >= v.alch_lo && aj < v.alch_hi) {
+                        // a water and an atom of the alchemical molecule
+                        lj_soft<ENERGY>(iO, js, z0, sg, ep, ljc2, v.alch_ll, v.alch_dll, fo, a, dh);
+                        Acc3 t{0.0, 0.0, 0.f};
+                        coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, t);
+                        coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, t);
+                        coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, t);
+                        const float cs = v.alch_cs;
+                        f0 = f0 * cs; f1 = f1 * cs; fm = fm * cs;
+                        a.w = fmaf(cs, t.w, a.w);
+                        if (ENERGY) { a.e_c += (double)cs * t.e_c; dh += (double)v.alch_dcs * t.e_c; }
+                    } else {
+                        lj<ENERGY>(iO, js, z0, sg * sg, ep, ljc2, 1.0f, fo, a);
+                        coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
+                        coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
+                        coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
+                    }
                 }
                 fO = fO + fo; fH0 = fH0 + f0; fH1 = fH1 + f1; fM = fM + fm;
                 const float3 t = (fo + f0) + (f1 + fm);
@@ -384,7 +433,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT, 4), k_pair_ws, (), (
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
     }
-    write_partials<ENERGY>(v, bk, REG_WS, el, ec, ew);
+    write_partials<ENERGY>(v, bk, REG_WS, el, ec, ew, dh);
 }
 
 // ---------------------------------------------------------------------------
@@ -392,14 +441,14 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT, 4), k_pair_ws, (), (
 // interaction mask from the list build holds jj > ii on the diagonal and
 // drops exclusions); work items, prefetch and j-side atomics as above.
 // ---------------------------------------------------------------------------
-DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) {
+DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT), k_pair_ss, (), ()) {
     const int lane = threadIdx.x & 31;
     const int ii = lane & 7, jq = lane >> 3;
     const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nit = v.sc->n_ss_items;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
-    double el = 0.0, ec = 0.0, ew = 0.0;
+    double el = 0.0, ec = 0.0, ew = 0.0, dh = 0.0;
     for (uint32_t it = ((bk.idx * blockDim.x + threadIdx.x) >> 5); it < nit; it += nwarps) {
         const uint2 item = v.ss_item[it];
         const uint32_t ci = item.x, k0 = item.y;
@@ -428,8 +477,22 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) 
                 if ((m >> (ii * ACL + jj)) & 1ull) {
                     const float3 s = shift_of(xyz(pi) - xyz(pj), b);
                     const float sg = 0.5f * (lji.x + ljj.x);
-                    lj<ENERGY>(xyz(pi), xyz(pj), s, sg * sg, sqrtf(lji.y * ljj.y), ljc2, 1.0f, fp, a);
-                    coul<ENERGY>(xyz(pi), xyz(pj), s, pi.w * pj.w, (double)pi.w * (double)pj.w, v, fp, a);
+                    const uint32_t aj = h ? cur.a1 : cur.a0;
+                    if (ALCH && ((ai >= v.alch_lo && ai < v.alch_hi) != (aj >= v.alch_lo && aj < v.alch_hi))) {
+                        // exactly one atom of the pair in the alchemical molecule
+                        lj_soft<ENERGY>(xyz(pi), xyz(pj), s, sg, sqrtf(lji.y * ljj.y), ljc2, v.alch_ll, v.alch_dll,
+                                        fp, a, dh);
+                        Acc3 t{0.0, 0.0, 0.f};
+                        float3 fc = f3(0.f, 0.f, 0.f);
+                        coul<ENERGY>(xyz(pi), xyz(pj), s, pi.w * pj.w, (double)pi.w * (double)pj.w, v, fc, t);
+                        const float cs = v.alch_cs;
+                        fp = fp + fc * cs;
+                        a.w = fmaf(cs, t.w, a.w);
+                        if (ENERGY) { a.e_c += (double)cs * t.e_c; dh += (double)v.alch_dcs * t.e_c; }
+                    } else {
+                        lj<ENERGY>(xyz(pi), xyz(pj), s, sg * sg, sqrtf(lji.y * ljj.y), ljc2, 1.0f, fp, a);
+                        coul<ENERGY>(xyz(pi), xyz(pj), s, pi.w * pj.w, (double)pi.w * (double)pj.w, v, fp, a);
+                    }
                 }
                 f = f + fp;
                 jf[3 * h + 0] = -fp.x; jf[3 * h + 1] = -fp.y; jf[3 * h + 2] = -fp.z;
@@ -447,7 +510,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(PT), k_pair_ss, (), ()) 
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
         ew += a.w;
     }
-    write_partials<ENERGY>(v, bk, REG_SS, el, ec, ew);
+    write_partials<ENERGY>(v, bk, REG_SS, el, ec, ew, dh);
 }
 
 // ---------------------------------------------------------------------------
@@ -529,10 +592,18 @@ void launch_pairs(const Target& t, bool energy) {
     launch_pairs_atoms(t, energy);
 }
 
+// the alchemical variants wherever a system decouples a molecule
+inline bool any_alch(const Target& t) {
+    return t.any([](const SysView& v) { return v.alch_on != 0u; });
+}
+
 void launch_pairs_atoms(const Target& t, bool energy) {
     auto ss = [](const SysView& v) { return v.na ? (int)v.nb[REG_SS] : 0; };
-    if (energy) t.launch(k_pair_ss<true>, k_pair_ss_batch<true>, ss, PT, 0);
-    else t.launch(k_pair_ss<false>, k_pair_ss_batch<false>, ss, PT, 0);
+    const bool al = any_alch(t);
+    if (energy && al) t.launch(k_pair_ss<true, true>, k_pair_ss_batch<true, true>, ss, PT, 0);
+    else if (energy) t.launch(k_pair_ss<true, false>, k_pair_ss_batch<true, false>, ss, PT, 0);
+    else if (al) t.launch(k_pair_ss<false, true>, k_pair_ss_batch<false, true>, ss, PT, 0);
+    else t.launch(k_pair_ss<false, false>, k_pair_ss_batch<false, false>, ss, PT, 0);
 }
 
 void launch_pairs_water(const Target& t, bool energy) {
@@ -551,8 +622,11 @@ void launch_pairs_water(const Target& t, bool energy) {
 
 void launch_pairs_ws(const Target& t, bool energy) {
     auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
-    if (energy) t.launch(k_pair_ws<true>, k_pair_ws_batch<true>, ws, PT, 0);
-    else t.launch(k_pair_ws<false>, k_pair_ws_batch<false>, ws, PT, 0);
+    const bool al = any_alch(t);
+    if (energy && al) t.launch(k_pair_ws<true, true>, k_pair_ws_batch<true, true>, ws, PT, 0);
+    else if (energy) t.launch(k_pair_ws<true, false>, k_pair_ws_batch<true, false>, ws, PT, 0);
+    else if (al) t.launch(k_pair_ws<false, true>, k_pair_ws_batch<false, true>, ws, PT, 0);
+    else t.launch(k_pair_ws<false, false>, k_pair_ws_batch<false, false>, ws, PT, 0);
 }
 
 void launch_pair14(const Target& t, bool energy) {

@@ -91,14 +91,29 @@ __device__ __forceinline__ void spread_one(const SysView& v, float3 p, float q, 
     }
 }
 
+// Which charges an SPME pass spreads and gathers: pass 0 all of them;
+// with an alchemical molecule, pass 1 all but the molecule's (the
+// environment) and pass 2 the molecule's only (src/non_bonded.rs:709-743).
+__device__ __forceinline__ bool pass_has_atom(const SysView& v, int pass, uint32_t a) {
+    if (pass == 0) return true;
+    const bool in = a >= v.alch_lo && a < v.alch_hi;
+    return pass == 1 ? !in : in;
+}
+// weight of a pass in the mixed forces / energies: lambda-scaled full
+// evaluation plus the unscaled environment and molecule evaluations
+__device__ __forceinline__ float pass_weight(const SysView& v, int pass) {
+    if (!v.alch_on) return 1.0f;
+    return pass == 0 ? v.alch_cs : 1.0f - v.alch_cs;
+}
+
 // one thread per charged site: atoms (q != 0), then water H0, H1, M
-DYN_KERNEL(, k_spread, (), ()) {
+DYN_KERNEL(, k_spread, (, int pass), (, pass)) {
     const BoxDev b = *v.box;
-    const uint32_t total = v.na + 3 * v.nw_cap;
+    const uint32_t total = v.na + (pass == 2 ? 0u : 3 * v.nw_cap);
     for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
         if (t < v.na) {
             const float4 p = v.apos[t];
-            if (p.w != 0.f) spread_one(v, xyz(p), p.w, b);
+            if (p.w != 0.f && pass_has_atom(v, pass, t)) spread_one(v, xyz(p), p.w, b);
         } else {
             const uint32_t k = t - v.na;
             const uint32_t s = k / 3, site = 1 + k % 3;
@@ -208,18 +223,25 @@ __device__ __forceinline__ double excl_corr(double dx, double dy, double dz, dou
 // Gather: one thread per atom, or per water (its H0, H1, M), writing the
 // reciprocal cache.  With Ewald corrections on, the intra-water exclusion
 // corrections (H0-H1, H0-M, H1-M) are added here in float64.
-DYN_KERNEL(, k_gather, (), ()) {
+// Pass 0 stores its (weighted) forces, later passes add theirs.
+DYN_KERNEL(, k_gather, (, int pass), (, pass)) {
     const BoxDev b = *v.box;
-    const bool corr = v.flags & DYN_FLAG_EWALD_CORRECTIONS;
+    const bool corr = pass == 0 && (v.flags & DYN_FLAG_EWALD_CORRECTIONS);
+    const float wt = pass_weight(v, pass);
     double e_c = 0.0, w_c = 0.0;
-    const uint32_t total = v.na + v.nw_cap;
+    const uint32_t total = v.na + (pass == 2 ? 0u : v.nw_cap);
     for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
         if (t < v.na) {
+            if (!pass_has_atom(v, pass, t)) continue;
             const float4 p = v.apos[t];
             float3 f = f3(0.f, 0.f, 0.f);
-            if (p.w != 0.f) f = gather_one(v, xyz(p), p.w, b);
+            if (p.w != 0.f) f = gather_one(v, xyz(p), p.w, b) * wt;
             long long* c = v.arecip + 3 * (size_t)t;
-            c[0] = fix_from_float(f.x); c[1] = fix_from_float(f.y); c[2] = fix_from_float(f.z);
+            if (pass == 0) {
+                c[0] = fix_from_float(f.x); c[1] = fix_from_float(f.y); c[2] = fix_from_float(f.z);
+            } else {
+                c[0] += fix_from_float(f.x); c[1] += fix_from_float(f.y); c[2] += fix_from_float(f.z);
+            }
         } else {
             const uint32_t s = t - v.na;
             const uint32_t id = v.wid[s];
@@ -229,7 +251,7 @@ DYN_KERNEL(, k_gather, (), ()) {
             for (int k = 0; k < 3; ++k) {
                 const float4 p = v.wpos[4 * s + 1 + k];
                 ps[k] = xyz(p);
-                const float3 f = gather_one(v, ps[k], p.w, b);
+                const float3 f = gather_one(v, ps[k], p.w, b) * wt;
                 fs[k] = make_double3(f.x, f.y, f.z);
             }
             if (corr) {
@@ -248,12 +270,14 @@ DYN_KERNEL(, k_gather, (), ()) {
             }
             long long* c = v.wrecip + 9 * (size_t)id;
             for (int k = 0; k < 3; ++k) {
-                c[3 * k + 0] = fix_from_double(fs[k].x);
-                c[3 * k + 1] = fix_from_double(fs[k].y);
-                c[3 * k + 2] = fix_from_double(fs[k].z);
+                const long long fx = fix_from_double(fs[k].x), fy = fix_from_double(fs[k].y),
+                                fz = fix_from_double(fs[k].z);
+                if (pass == 0) { c[3 * k + 0] = fx; c[3 * k + 1] = fy; c[3 * k + 2] = fz; }
+                else { c[3 * k + 0] += fx; c[3 * k + 1] += fy; c[3 * k + 2] += fz; }
             }
         }
     }
+    if (pass != 0) return;  // the intra-water corrections belong to pass 0
     double x[2] = {e_c, w_c};
     block_sum_d<2>(x);
     if (threadIdx.x == 0) {
@@ -324,13 +348,35 @@ DYN_KERNEL(, k_corr_atoms, (), ()) {
     }
 }
 
-// Sums the reciprocal-step partials (fixed order) into the cache.
-DYN_KERNEL(, k_recip_finalize, (), ()) {
-    double x[4] = {0.0, 0.0, 0.0, 0.0};
+// Energy and virial of one SPME pass (fixed-order sums), weighted into the
+// evaluation's totals; with an alchemical molecule the cross term
+// E_full - E_env - E_mol times dcoulomb_scale/dlambda goes to dH/dlambda.
+DYN_KERNEL(, k_recip_pass, (, int pass), (, pass)) {
+    double x[2] = {0.0, 0.0};
     for (uint32_t i = threadIdx.x; i < v.nb[REG_PME]; i += blockDim.x) {
         const double* p = v.partials + ((size_t)REG_PME * v.max_blocks + i) * 4;
         x[0] += p[0]; x[1] += p[1];
     }
+    block_sum_d<2>(x);
+    if (threadIdx.x != 0) return;
+    Scalars* sc = v.sc;
+    const double w = (double)pass_weight(v, pass);
+    const double dc = v.alch_on ? (double)v.alch_dcs : 0.0;
+    if (pass == 0) {
+        sc->recip_acc[0] = w * x[0];
+        sc->recip_acc[1] = w * x[1];
+        sc->recip_dh = dc * x[0];
+    } else {
+        sc->recip_acc[0] += w * x[0];
+        sc->recip_acc[1] += w * x[1];
+        sc->recip_dh -= dc * x[0];
+    }
+}
+
+// The evaluation's reciprocal energy (with the self term), virial and
+// corrections into the cache the steps between SPME evaluations reuse.
+DYN_KERNEL(, k_recip_finalize, (), ()) {
+    double x[4] = {0.0, 0.0, 0.0, 0.0};
     for (uint32_t i = threadIdx.x; i < v.nb[REG_CORR]; i += blockDim.x) {
         const double* p = v.partials + ((size_t)REG_CORR * v.max_blocks + i) * 4;
         x[2] += p[0]; x[3] += p[1];
@@ -341,10 +387,12 @@ DYN_KERNEL(, k_recip_finalize, (), ()) {
     }
     block_sum_d<4>(x);
     if (threadIdx.x == 0) {
-        v.sc->recip_cache[0] = x[0] + v.e_self;
-        v.sc->recip_cache[1] = x[1];
-        v.sc->recip_cache[2] = x[2];
-        v.sc->recip_cache[3] = x[3];
+        Scalars* sc = v.sc;
+        sc->recip_cache[0] = sc->recip_acc[0] + v.e_self;
+        sc->recip_cache[1] = sc->recip_acc[1];
+        sc->recip_cache[2] = x[2];
+        sc->recip_cache[3] = x[3];
+        sc->recip_dh_cache = sc->recip_dh;
     }
 }
 
@@ -405,23 +453,35 @@ void pme_free(SysView& v, cufftHandle plan_f, cufftHandle plan_b) {
 }
 
 void launch_pme(const Target& t) {
-    t.launch(k_spread, k_spread_batch, [](const SysView& v) { return gblocks(v, (uint64_t)v.na + 3ull * v.nw_cap); },
-             GT, 0);
-    t.launch(k_fix2real, k_fix2real_batch,
-             [](const SysView& v) { return gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]); }, GT, 0);
-    // the plans run on the target's stream (a graph branch may differ from
-    // the stream the plans were made on)
+    // one pass, or three with an alchemical molecule in any system (systems
+    // without one skip passes 1 and 2)
+    const int npass = t.any([](const SysView& v) { return v.alch_on != 0u; }) ? 3 : 1;
     const cudaStream_t st = t.st;
-    t.each([st](const SysView& v) {
-        cufftSetStream(v.plan_f, st);
-        cufftExecR2C(v.plan_f, v.qgrid, (cufftComplex*)v.cgrid);
-    });
-    t.launch(k_convolve, k_convolve_batch, [](const SysView& v) { return (int)v.nb[REG_PME]; }, GT, 0);
-    t.each([st](const SysView& v) {
-        cufftSetStream(v.plan_b, st);
-        cufftExecC2R(v.plan_b, (cufftComplex*)v.cgrid, v.qgrid);
-    });
-    t.launch(k_gather, k_gather_batch, [](const SysView& v) { return (int)v.nb[REG_CORR]; }, GT, 0);
+    for (int pass = 0; pass < npass; ++pass) {
+        auto on = [pass](const SysView& v) { return pass == 0 || v.alch_on != 0u; };
+        t.launch(k_spread, k_spread_batch,
+                 [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.na + 3ull * v.nw_cap) : 0; }, GT, 0,
+                 pass);
+        t.launch(k_fix2real, k_fix2real_batch,
+                 [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]) : 0; }, GT, 0);
+        // the plans run on the target's stream (a graph branch may differ
+        // from the stream the plans were made on)
+        t.each([st, on](const SysView& v) {
+            if (!on(v)) return;
+            cufftSetStream(v.plan_f, st);
+            cufftExecR2C(v.plan_f, v.qgrid, (cufftComplex*)v.cgrid);
+        });
+        t.launch(k_convolve, k_convolve_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_PME] : 0; }, GT,
+                 0);
+        t.each([st, on](const SysView& v) {
+            if (!on(v)) return;
+            cufftSetStream(v.plan_b, st);
+            cufftExecC2R(v.plan_b, (cufftComplex*)v.cgrid, v.qgrid);
+        });
+        t.launch(k_gather, k_gather_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_CORR] : 0; }, GT, 0,
+                 pass);
+        t.launch(k_recip_pass, k_recip_pass_batch, [&](const SysView& v) { return on(v) ? 1 : 0; }, 256, 0, pass);
+    }
 }
 
 void launch_corrections(const Target& t) {

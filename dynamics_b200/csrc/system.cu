@@ -311,6 +311,20 @@ void fill_energies(dyn_sys_s* h, dyn_energies_t* e) {
     e->kinetic_rigid = s.ke_rigid;
     e->pressure_atomic_bar = s.pressure_atomic;
     e->list_union_max = s.union_max;
+    e->dh_dl = s.dh_dl;
+}
+
+// staged_decoupling_schedule (src/alchemical.rs:77-96): Coulomb scaled
+// 1 - 2 lambda over lambda < 0.5, then LJ soft-core lambda 2 lambda - 1
+void set_alch_schedule(SysView& v, float lambda) {
+    const float l = std::min(1.0f, std::max(0.0f, lambda));
+    if (l < 0.5f) {
+        v.alch_cs = 1.0f - 2.0f * l; v.alch_dcs = -2.0f;
+        v.alch_ll = 0.0f; v.alch_dll = 0.0f;
+    } else {
+        v.alch_cs = 0.0f; v.alch_dcs = 0.0f;
+        v.alch_ll = 2.0f * l - 1.0f; v.alch_dll = 2.0f;
+    }
 }
 
 }  // namespace
@@ -425,6 +439,14 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
 
     v.nw = d->n_water;
     v.na = d->n_atoms;
+    if (cfg->alch_end > cfg->alch_begin) {
+        DYN_CHECK(cfg->alch_end <= d->n_atoms, DYN_ERR_INVALID, "dyn_sys_create: alchemical range beyond the atoms");
+        DYN_CHECK(std::isfinite(cfg->alch_lambda), DYN_ERR_INVALID, "dyn_sys_create: alch_lambda not finite");
+        v.alch_on = 1u;
+        v.alch_lo = cfg->alch_begin;
+        v.alch_hi = cfg->alch_end;
+    }
+    set_alch_schedule(v, cfg->alch_lambda);
     v.total_mass = (double)v.nw * (double)OPC_MASS_MOL;
     for (uint32_t a = 0; a < v.na && d->atom_mass; ++a) v.total_mass += (double)d->atom_mass[a];
     // parameters
@@ -1253,6 +1275,20 @@ extern "C" int dyn_sys_memory(dyn_sys_t h, uint64_t* bytes) {
         const int rc_a = dev_alloc(h, &(ptr_), (n_), true);        \
         if (rc_a != DYN_OK) return rc_a;                           \
     } while (0)
+
+extern "C" int dyn_sys_set_lambda(dyn_sys_t h, float lambda) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_set_lambda: NULL handle");
+    DYN_CHECK(std::isfinite(lambda), DYN_ERR_INVALID, "dyn_sys_set_lambda: lambda not finite");
+    DYN_CHECK(h->v.alch_on, DYN_ERR_INVALID, "dyn_sys_set_lambda: no alchemical molecule");
+    DYN_CHECK(!h->batch_member, DYN_ERR_UNSUPPORTED, "dyn_sys_set_lambda: not for a batch member");
+    DYN_CUDA(cudaStreamSynchronize(h->stream));
+    for (int g = 0; g < 4; ++g)
+        if (h->graph[g]) { cudaGraphExecDestroy(h->graph[g]); h->graph[g] = nullptr; }
+    set_alch_schedule(h->v, lambda);
+    h->cfg.alch_lambda = lambda;
+    // the cached reciprocal forces belong to the old lambda
+    return dyn::evaluate_forces(h);
+}
 
 extern "C" int dyn_sys_set_static(dyn_sys_t h, const uint8_t* atom_static, uint32_t thermo_dof) {
     DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_set_static: NULL handle");

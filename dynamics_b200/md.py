@@ -77,6 +77,10 @@ class MdConfig:
     # False = the reference's position-only correction, which dissipates
     # kinetic energy of the constrained bonds
     rattle_velocities: bool = False
+    # alchemical decoupling of the atoms [begin, end) (one molecule) at
+    # alch_lambda on the reference's staged schedule (src/alchemical.rs)
+    alch_range: Optional[tuple] = None
+    alch_lambda: float = 0.0
 
 
 def thermo_dof(system, cfg):
@@ -144,6 +148,9 @@ def _config_struct(system, cfg):
     if cfg.rattle_velocities:
         flags |= _lib.DYN_FLAG_RATTLE_VELOCITIES
     c.flags = flags
+    if cfg.alch_range is not None:
+        c.alch_begin, c.alch_end = int(cfg.alch_range[0]), int(cfg.alch_range[1])
+    c.alch_lambda = float(cfg.alch_lambda)
     c.thermo_dof = thermo_dof(system, cfg)
     c.seed = int(cfg.seed) & 0xFFFFFFFFFFFFFFFF
     c.ww_union_chunk = int(cfg.ww_union_chunk)
@@ -308,6 +315,12 @@ class MdState:
         b = C.c_uint64()
         check(lib().dyn_sys_memory(self.handle, C.byref(b)))
         return b.value
+
+    def set_lambda(self, lam):
+        """Another lambda window for the alchemical molecule; forces are
+        evaluated again at once."""
+        check(lib().dyn_sys_set_lambda(self.handle, float(lam)))
+        self.cfg.alch_lambda = float(lam)
 
     def set_static(self, mask=None):
         """Atoms held fixed (bool (n_atoms,), None = none), with the

@@ -265,6 +265,17 @@ typedef struct {
                              * 0 = 4 (the reference default)                */
     uint32_t lincs_iter;    /* SHAKE-style correction passes; 0 = 1         */
     uint32_t reserved0;
+    /* Alchemical decoupling of the atoms [alch_begin, alch_end) (one
+     * molecule, StateAlchemical, src/alchemical.rs:98-121): pairs between
+     * them and the rest use soft-core LJ and scaled Coulomb, SPME is
+     * evaluated three times and mixed, and dH/dlambda is reported, on the
+     * reference's staged schedule (staged_decoupling_schedule,
+     * src/alchemical.rs:77-96: Coulomb off over lambda 0..0.5, LJ soft-core
+     * decoupled over 0.5..1).  alch_end <= alch_begin: off. */
+    uint32_t alch_begin;
+    uint32_t alch_end;
+    float alch_lambda;      /* 0 = fully coupled, 1 = decoupled             */
+    uint32_t reserved1;
 } dyn_config_t;
 
 typedef struct {
@@ -323,6 +334,8 @@ typedef struct {
                                * uses the molecular virial of the rigid waters */
     uint64_t list_union_max;  /* largest set of j-waters one 32-water group
                                * needed at the last list build */
+    double dh_dl;             /* alchemical dH/dlambda, kcal/mol (short-range
+                               * cross pairs + SPME cross term), energy steps */
 } dyn_energies_t;
 
 /* Creates a resident system (replaces MdState::new's device setup,
@@ -394,6 +407,10 @@ int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
  * under conditional nodes that the device sets. */
 int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic);
 
+/* Moves an alchemical system to another lambda (a new window of the
+ * thermodynamic integration, set_alchemical_window, src/alchemical.rs). */
+int dyn_sys_set_lambda(dyn_sys_t h, float lambda);
+
 /* Replaces the atoms' static flags (1 = held fixed; NULL = none) and the
  * thermostat degrees of freedom (0 = keep), between steps, e.g. to freeze
  * the solute while the solvent relaxes around it (MdState::md_on_solute_only,
@@ -440,6 +457,7 @@ typedef struct {
     double box_lo[3], box_hi[3];
     double volume;            /* A^3                                        */
     double density;           /* amu / A^3 (src/snapshot.rs:206-211)        */
+    double dh_dl;             /* alchemical dH/dlambda, kcal/mol            */
 } dyn_frame_t;
 
 /* Device side of MdState::handle_snapshots (src/snapshot.rs:753-833):

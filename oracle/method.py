@@ -62,12 +62,43 @@ def _site_tables(sysd):
     return pos, q, sig, eps, has_lj, mol, na, nw
 
 
-def short_range(sysd, cutoff, alpha, lj_cutoff=None, lj_disabled=False, coulomb_disabled=False):
+def decoupling_schedule(lam):
+    """staged_decoupling_schedule (src/alchemical.rs:77-96): (Coulomb scale,
+    its lambda derivative, LJ soft-core lambda, its lambda derivative)."""
+    lam = min(max(float(lam), 0.0), 1.0)
+    if lam < 0.5:
+        return 1.0 - 2.0 * lam, -2.0, 0.0, 0.0
+    return 0.0, 0.0, 2.0 * lam - 1.0, 2.0
+
+
+SC_ALPHA, SC_SIGMA_MIN = 0.5, 3.0  # src/alchemical.rs:55-65 (power 1)
+
+
+def soft_core_lj(r, sig, eps, lam):
+    """alchemical_lj_soft_core_decouple (src/non_bonded.rs:883-941) per
+    pair: (force magnitude along r, energy, dV/dl)."""
+    ss6 = np.maximum(sig, SC_SIGMA_MIN) ** 6
+    rsc6 = r ** 6 + SC_ALPHA * ss6 * lam
+    rsc = rsc6 ** (1.0 / 6.0)
+    sr6 = (sig / rsc) ** 6
+    hf = 24.0 * eps * (2.0 * sr6 * sr6 - sr6) / rsc
+    he = 4.0 * eps * (sr6 * sr6 - sr6)
+    scale = 1.0 - lam
+    fmag = hf * scale * (r / rsc) ** 5
+    dvdl = -he - scale * hf * SC_ALPHA * ss6 / (6.0 * rsc ** 5)
+    return np.where(eps != 0.0, fmag, 0.0), np.where(eps != 0.0, scale * he, 0.0), np.where(eps != 0.0, dvdl, 0.0)
+
+
+def short_range(sysd, cutoff, alpha, lj_cutoff=None, lj_disabled=False, coulomb_disabled=False, alch=None):
     """Short-range forces over all site pairs within the cutoff (FP64).
 
     Returns dict with per-site forces (n_sites, 3), energy split into
     water-water and solute-involving parts, virial and the pair count.
     Sites are ordered atoms first, then water O, H0, H1, M per molecule.
+    ``alch`` = (begin, end, lambda): pairs with exactly one atom in
+    [begin, end) take soft-core LJ and scaled Coulomb on the staged schedule
+    (f_nonbonded_cpu, src/non_bonded.rs:950-1057); their dH/dlambda is
+    returned as ``dh_dl``.
     """
     pos, q, sig, eps, has_lj, mol, na, nw = _site_tables(sysd)
     lo = np.asarray(sysd["box_lo"], dtype=np.float32).astype(np.float64)
@@ -116,6 +147,20 @@ def short_range(sysd, cutoff, alpha, lj_cutoff=None, lj_disabled=False, coulomb_
     f_c = np.where(co_on, qq * (erfc(ar) * inv_r * inv_r
                                 + 2.0 * alpha / np.sqrt(np.pi) * np.exp(-ar * ar) * inv_r), 0.0) * scale
     e_c = np.where(co_on, qq * erfc(ar) * inv_r, 0.0) * scale
+    dh_dl = 0.0
+    if alch is not None:
+        a0, a1, lam = alch
+        cs, dcs, ll, dll = decoupling_schedule(lam)
+        in_i = (i < na) & (i >= a0) & (i < a1)
+        in_j = (j < na) & (j >= a0) & (j < a1)
+        cross = in_i != in_j
+        fs, es, dv = soft_core_lj(r, sg, ep, ll)
+        f_lj = np.where(cross, np.where(lj_on, fs, 0.0), f_lj)
+        e_lj = np.where(cross, np.where(lj_on, es, 0.0), e_lj)
+        dh_dl = float(np.sum(np.where(cross & lj_on, dv, 0.0))) * dll
+        dh_dl += float(np.sum(np.where(cross, e_c, 0.0))) * dcs
+        f_c = np.where(cross, f_c * cs, f_c)
+        e_c = np.where(cross, e_c * cs, e_c)
     fmag = f_lj + f_c
     f = d * (fmag * inv_r)[:, None]
     n = len(pos)
@@ -134,7 +179,7 @@ def short_range(sysd, cutoff, alpha, lj_cutoff=None, lj_disabled=False, coulomb_
         "n_lj_pairs": int(np.count_nonzero(lj_on)),
         "n_coul_pairs": int(np.count_nonzero(co_on)),
         "n_pairs_within": int(np.count_nonzero(lj_on | co_on)),
-        "na": na, "nw": nw,
+        "na": na, "nw": nw, "dh_dl": dh_dl,
     }
 
 
@@ -166,8 +211,12 @@ def all_forces(sysd, cfg):
     cutoff = float(cfg["cutoff"])
     alpha = float(cfg["alpha"])
     mode = cfg.get("mode", "reference")
+    alch = None
+    if cfg.get("alch_range") is not None:
+        alch = (int(cfg["alch_range"][0]), int(cfg["alch_range"][1]), float(cfg.get("alch_lambda", 0.0)))
     sr = short_range(sysd, cutoff, alpha, cfg.get("lj_cutoff"), cfg.get("lj_disabled", False),
-                     cfg.get("coulomb_disabled", False))
+                     cfg.get("coulomb_disabled", False), alch)
+    dh_dl = sr["dh_dl"]
     na, nw = sr["na"], sr["nw"]
     forces = sr["forces"].copy()
     out = {"e_lj": sr["e_lj"], "e_coul_short": sr["e_coul"], "e_water_water_short": sr["e_water_water"],
@@ -181,7 +230,22 @@ def all_forces(sysd, cfg):
     w_corr = 0.0
     if not cfg.get("recip_disabled", False) and not cfg.get("coulomb_disabled", False):
         p, qq, _, _ = charged_sites(sysd)
-        e_recip, f_rec, w_recip = spme.recip(p, qq, lo, ext, cfg["grid"], alpha, include_self=True)
+        if alch is None:
+            e_recip, f_rec, w_recip = spme.recip(p, qq, lo, ext, cfg["grid"], alpha, include_self=True)
+        else:
+            # full, environment-only and molecule-only charges; the cross
+            # term scaled (src/non_bonded.rs:709-743)
+            a0, a1, lam = alch
+            cs, dcs, _, _ = decoupling_schedule(lam)
+            mol = np.zeros(len(qq), bool)
+            mol[a0:a1] = True
+            ef, ff, wf = spme.recip(p, qq, lo, ext, cfg["grid"], alpha, include_self=True)
+            ee, fe, we = spme.recip(p, np.where(mol, 0.0, qq), lo, ext, cfg["grid"], alpha, include_self=True)
+            em, fm_, wm = spme.recip(p, np.where(mol, qq, 0.0), lo, ext, cfg["grid"], alpha, include_self=True)
+            e_recip = ee + em + cs * (ef - ee - em)
+            f_rec = fe + fm_ + cs * (ff - fe - fm_)
+            w_recip = we + wm + cs * (wf - we - wm)
+            dh_dl += dcs * (ef - ee - em)
         forces[:na] += f_rec[:na]
         fw = f_rec[na:].reshape(nw, 3, 3)  # M, H0, H1
         fsite = forces[na:].reshape(nw, 4, 3)
@@ -244,4 +308,5 @@ def all_forces(sysd, cfg):
     out["virial"] = sr["virial"] + w_recip + w_corr + w_b
     out["f_atoms"] = forces[:na]
     out["f_water"] = forces[na:].reshape(nw, 4, 3)
+    out["dh_dl"] = dh_dl
     return out

@@ -153,3 +153,36 @@ def test_relax_solvent_holds_the_solute(gpu_lib):
     st.step(0.002, 10)
     assert np.max(np.abs(st.state()["atom_pos"] - a1["atom_pos"])) > 1e-4
     st.close()
+
+
+@pytest.mark.parametrize("lam", [0.25, 0.75])
+@pytest.mark.parametrize("mode", ["reference", "corrected"])
+def test_alchemical_forces_match_oracle(gpu_lib, relaxed, lam, mode):
+    """The peptide decoupled at lambda (Coulomb stage, then soft-core LJ
+    stage): forces, potential energy and dH/dlambda against the oracle."""
+    n_pep = int(np.max(relaxed["bonds"])) + 1
+    cfg = _cfg(relaxed, mode, alch_range=(0, n_pep), alch_lambda=lam)
+    st = md.MdState(relaxed, cfg)
+    got = st.forces()
+    ref = method_alch(relaxed, cfg, st)
+    err = _compare(got, ref)
+    assert err < FORCE_RTOL, f"force rel-RMS {err:.3e}"
+    assert abs(got["potential"] - ref["pe"]) <= PE_RTOL * abs(ref["pe"]), (got["potential"], ref["pe"])
+    assert abs(got["dh_dl"] - ref["dh_dl"]) <= 1e-4 * max(1.0, abs(ref["dh_dl"])), (got["dh_dl"], ref["dh_dl"])
+    # another window through set_lambda
+    st.set_lambda(1.0 - lam)
+    got2 = st.forces()
+    cfg2 = _cfg(relaxed, mode, alch_range=(0, n_pep), alch_lambda=1.0 - lam)
+    ref2 = method_alch(relaxed, cfg2, st)
+    assert _compare(got2, ref2) < FORCE_RTOL
+    assert abs(got2["dh_dl"] - ref2["dh_dl"]) <= 1e-4 * max(1.0, abs(ref2["dh_dl"]))
+    st.close()
+
+
+def method_alch(sysd, cfg, st):
+    from oracle import method
+    d = {**sysd, "water_m": st.state()["water_m"]}
+    return method.all_forces(d, {
+        "cutoff": cfg.coulomb_cutoff, "lj_cutoff": cfg.lj_cutoff, "alpha": float(np.float32(cfg.spme_alpha)),
+        "grid": cfg.spme_grid, "mode": "corrected" if cfg.ewald_corrections else "reference",
+        "alch_range": cfg.alch_range, "alch_lambda": float(np.float32(cfg.alch_lambda))})

@@ -1,0 +1,55 @@
+"""The oracle's alchemical decoupling (soft-core LJ, scaled Coulomb, mixed
+SPME on the staged schedule, src/alchemical.rs and src/non_bonded.rs):
+dH/dlambda equals the finite difference of the potential energy, and the
+forces are the energy's negative gradient."""
+import numpy as np
+import pytest
+
+from dynamics_b200 import peptide, synth
+from oracle import method
+
+
+@pytest.fixture(scope="module")
+def small():
+    sysd, _ = peptide.solvated_system(24.8, 420, n_res=(2,), seed=5)
+    n_pep = int(np.max(sysd["bonds"])) + 1  # the peptide's atoms come first; ions have no bonds
+    return sysd, n_pep
+
+
+def _params(n_pep, lam, mode="corrected"):
+    return {"cutoff": 9.0, "lj_cutoff": 9.0, "alpha": synth.ewald_alpha(9.0), "grid": (24, 24, 24),
+            "mode": mode, "alch_range": (0, n_pep), "alch_lambda": lam}
+
+
+def test_schedule():
+    assert method.decoupling_schedule(0.0) == (1.0, -2.0, 0.0, 0.0)
+    assert method.decoupling_schedule(0.25) == (0.5, -2.0, 0.0, 0.0)
+    assert method.decoupling_schedule(0.75) == (0.0, 0.0, 0.5, 2.0)
+    assert method.decoupling_schedule(1.0) == (0.0, 0.0, 1.0, 2.0)
+
+
+@pytest.mark.parametrize("lam", [0.3, 0.7])
+def test_dhdl_is_energy_derivative(small, lam):
+    sysd, n_pep = small
+    h = 1e-4
+    ep = method.all_forces(sysd, _params(n_pep, lam + h))["pe"]
+    em = method.all_forces(sysd, _params(n_pep, lam - h))["pe"]
+    dh = method.all_forces(sysd, _params(n_pep, lam))["dh_dl"]
+    assert abs((ep - em) / (2 * h) - dh) <= 1e-5 * max(1.0, abs(dh)), ((ep - em) / (2 * h), dh)
+
+
+@pytest.mark.parametrize("lam", [0.3, 0.7])
+def test_alchemical_force_is_gradient(small, lam):
+    sysd, n_pep = small
+    r = method.all_forces(sysd, _params(n_pep, lam))
+    a = 0  # an atom of the decoupled molecule
+    h = 1e-4
+    g = np.zeros(3)
+    for k in range(3):
+        d = {**sysd, "atom_pos": sysd["atom_pos"].astype(np.float64).copy()}
+        d["atom_pos"][a, k] += h
+        e1 = method.all_forces(d, _params(n_pep, lam))["pe"]
+        d["atom_pos"][a, k] -= 2 * h
+        e0 = method.all_forces(d, _params(n_pep, lam))["pe"]
+        g[k] = (e1 - e0) / (2 * h)
+    np.testing.assert_allclose(r["f_atoms"][a], -g, rtol=2e-3, atol=2e-3)
