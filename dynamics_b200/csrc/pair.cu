@@ -360,6 +360,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT, 4),
     const int ii = lane & 7, jq = lane >> 3;
     const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
     const uint32_t nit = v.sc->n_ws_items;
+    const uint32_t first_single = v.sc->a_sparse_base / ACL;  // first single-atom cluster
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0, dh = 0.0;
@@ -374,10 +375,26 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT, 4),
         float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
         Acc3 a{0.0, 0.0, 0.f};
         const uint32_t my_j = (uint32_t)lane < n ? v.ws_j[(size_t)ci * v.cap_ws + k0 + lane] : 0u;
-        JAtoms nx = load_jatoms(v, __shfl_sync(0xffffffffu, my_j, 0), jq);
-        for (uint32_t k = 0; k < n; ++k) {
+        // Single-atom clusters (ions) come last in every list.  Four of them
+        // are taken per iteration, one per lane group jq (its atom in the
+        // h = 0 slot), instead of one cluster with seven empty slots.
+        auto load_at = [&](uint32_t k) -> JAtoms {
+            const uint32_t c0 = __shfl_sync(0xffffffffu, my_j, k);
+            const uint32_t kk = k + (uint32_t)jq;
+            const uint32_t cq = __shfl_sync(0xffffffffu, my_j, kk < n ? kk : k);
+            if (c0 < first_single) return load_jatoms(v, c0, jq);
+            const uint32_t sq = cq * ACL;
+            return JAtoms{v.spos[sq], make_float4(0.f, 0.f, 0.f, 0.f), v.slj[sq], make_float2(0.f, 0.f),
+                          kk < n ? v.sidx[sq] : INVALID_ID, INVALID_ID};
+        };
+        auto advance = [&](uint32_t k) -> uint32_t {
+            return __shfl_sync(0xffffffffu, my_j, k) < first_single ? 1u : 4u;
+        };
+        JAtoms nx = load_at(0);
+        for (uint32_t k = 0; k < n;) {
             const JAtoms cur = nx;
-            if (k + 1 < n) nx = load_jatoms(v, __shfl_sync(0xffffffffu, my_j, k + 1), jq);
+            k += advance(k);
+            if (k < n) nx = load_at(k);
             float jf[8];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -415,7 +432,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT, 4),
                 jf[3 * h + 0] = -t.x; jf[3 * h + 1] = -t.y; jf[3 * h + 2] = -t.z;
             }
             jf[6] = 0.f; jf[7] = 0.f;
-            // lane ii < 6 now holds component ii % 3 of atom jq + 4 (ii / 3)
+            // lane ii < 6 now holds component ii % 3 of the group's j-atom a0 (ii < 3) or a1
             reduce_scatter8(jf, ii);
             if (ii < 6) {
                 const uint32_t aj = ii < 3 ? cur.a0 : cur.a1;

@@ -507,15 +507,19 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     // water-water: 32-water groups; candidate clusters within r_ww of the
     // group box; the union of needed waters; molecule lists within r_ww
     // (liquid density as the bound)
+    // counts at liquid density or the system's, whichever is higher;
+    // extents of groups and clusters at the lower of the two (a group drawn
+    // from a dilute region spans more space, and may sit next to liquid)
     const double dl = std::max(0.0334, v.nw / vol);
+    const double dx = std::max(1e-3, std::min(0.0334, v.nw / vol));
     v.ngrp_cap = v.nw_cap / GRPW;
     {
         const double r = v.r_ww;
         auto mink = [&](double a) {
             return a * a * a + 6.0 * a * a * r + 3.0 * M_PI * a * r * r + 4.0 / 3.0 * M_PI * r * r * r;
         };
-        const double ag = 1.4 * std::cbrt(GRPW / dl), ac = 2.0 * std::cbrt(WCL / dl);
-        v.cap_tile = std::min<uint32_t>((uint32_t)(1.5 * mink(ag + ac) * dl / WCL) + 16,
+        const double ag = 1.4 * std::cbrt(GRPW / dx), ac = 2.0 * std::cbrt(WCL / dx);
+        v.cap_tile = std::min<uint32_t>((uint32_t)(2.0 * mink(ag + ac) * dl / WCL) + 16,
                                         std::max<uint32_t>(1u, v.nwclus_cap));
         // unions larger than the shared-memory chunk are processed in
         // several chunks, so this is only the list-build capacity
