@@ -27,6 +27,7 @@ DYN_PAIR_SCALE14 = 1
 DYN_PAIR_LJ = 2
 DYN_PAIR_COULOMB = 4
 DYN_PAIR_SYMMETRIC = 8
+DYN_PAIR_ALCH = 16
 
 DYN_INTEGRATOR_LANGEVIN_MIDDLE = 0
 DYN_INTEGRATOR_VERLET_VELOCITY = 1
@@ -131,6 +132,9 @@ _SIGS = {
                             C.c_float, _P], C.c_int),
     "dyn_nb_get_pairs": ([_P, C.c_uint64] + [_P] * 9, C.c_int),
     "dyn_nb_forces": ([_P, _P, _P, _P, _P, _P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, _P], C.c_int),
+    "dyn_nb_forces_alch": ([_P, _P, _P, _P, _P, _P, _P, C.c_uint32, C.c_double]
+                           + [_P] * 8, C.c_int),
+    "dyn_nb_mark_alch": ([_P, C.c_uint32, C.c_uint32, _P], C.c_int),
     "dyn_nb_forces_static": ([_P, C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P, C.c_uint64]
                              + [_P] * 9 + [_P, C.c_float, C.c_float, C.c_float, C.c_uint32]
                              + [_P] * 6, C.c_int),

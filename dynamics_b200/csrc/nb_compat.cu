@@ -9,7 +9,12 @@
 // forces, so results are bit-identical run to run.  The pair-list build
 // (dyn_nb_build_pairs) replaces the reference's O(N^2) host rebuild with a
 // GPU brute-force scan in the reference's exact float32 arithmetic.
+// Pairs flagged alchemical (DYN_PAIR_ALCH, or marked by dyn_nb_mark_alch)
+// take the reference's soft-core LJ and scaled Coulomb on the staged
+// decoupling schedule (nonbonded_force_alchemical_kernel,
+// src/cuda/cuda.cu:367-566; f_nonbonded_cpu, src/non_bonded.rs:950-1057).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -17,7 +22,12 @@
 
 namespace {
 
+// packed pair words: w.x = target index (bits 0-26) | alchemical (27) |
+// body (28-30) | scale14 (31); w.y = source index (0-27) | body | symmetric
 constexpr uint32_t IDX_MASK = 0x0FFFFFFFu;
+constexpr uint32_t TGT_MASK = 0x07FFFFFFu;
+constexpr uint32_t ALCH_BIT = 0x08000000u;
+constexpr int NB_PART = 3;  // virial, energy, dH/dlambda per block
 constexpr int NB_BLOCK = 256;
 constexpr int NB_MAX_BLOCKS = 148 * 8;
 
@@ -29,8 +39,9 @@ struct dyn_nb_s {
     float rc = 10.f, alpha = 0.3f, ljc = 0.f;
     float* d_pos[5] = {};          // dyn, O, M, H0, H1: [3n] floats
     long long* d_f[5] = {};        // fixed-point forces [3n]
-    double* d_partials = nullptr;  // [NB_MAX_BLOCKS * 2]
-    double* d_scalars = nullptr;   // virial, energy
+    double* d_partials = nullptr;  // [NB_MAX_BLOCKS * NB_PART]
+    double* d_scalars = nullptr;   // virial, energy, dH/dlambda
+    uint64_t n_alch = 0;           // installed pairs with the alchemical bit
     uint64_t n_pairs = 0, cap_pairs = 0;
     uint2* d_pidx = nullptr;       // packed target/source words
     float2* d_plj = nullptr;       // sigma, eps
@@ -60,26 +71,71 @@ __device__ __forceinline__ float round_half_away(float q) {
 struct PosPtrs { const float* p[5]; };
 struct ForcePtrs { long long* f[5]; };
 
+// The staged decoupling schedule of one lambda (staged_decoupling_schedule,
+// src/alchemical.rs:77-100): Coulomb scale and its lambda derivative over
+// lambda 0..0.5, then the soft-core LJ lambda and its derivative over 0.5..1.
+struct AlchSched { float cs, dcs, ll, dll; };
+
+AlchSched alch_schedule(double lambda) {
+    float l = (float)lambda;
+    l = std::min(1.0f, std::max(0.0f, l));
+    if (l < 0.5f) return {1.0f - 2.0f * l, -2.0f, 0.0f, 0.0f};
+    return {0.0f, 0.0f, 2.0f * l - 1.0f, 2.0f};
+}
+
+// Beutler soft-core LJ of a decoupled pair (alchemical_lj_soft_core_decouple,
+// src/non_bonded.rs:883-941; sc-alpha 0.5, power 1, soft-core sigma >= 3 A,
+// src/alchemical.rs:55-65): V = (1 - l) V_LJ(r_sc), r_sc^6 = r^6 + 0.5 s^6 l.
+// Returns the force magnitude along the pair direction (F_LJ(r_sc) (1 - l)
+// (r / r_sc)^5), the energy and dV/dl = -V_LJ(r_sc) - (1 - l) F_LJ(r_sc)
+// 0.5 s^6 / (6 r_sc^5).  r2 = 0 gives the energy at contact and no force.
+__device__ __forceinline__ void soft_core(float r2, float sig, float eps, float lam, float& fmag,
+                                          float& e, float& dvdl) {
+    fmag = 0.f; e = 0.f; dvdl = 0.f;
+    if (eps == 0.f || !isfinite(eps) || !isfinite(sig)) return;
+    const float ss = fmaxf(sig, 3.0f), ss2 = ss * ss;
+    const float ss6 = ss2 * ss2 * ss2;
+    const float rsc6 = fmaf(0.5f * ss6, lam, r2 * r2 * r2);
+    if (!(rsc6 > 0.f) || !isfinite(rsc6)) return;
+    const float rsc = sqrtf(cbrtf(rsc6));
+    const float inv_rsc = 1.0f / rsc;
+    const float sr = sig * inv_rsc, sr2 = sr * sr;
+    const float sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
+    const float hf = 24.0f * eps * fmaf(2.0f, sr12, -sr6) * inv_rsc;
+    const float he = 4.0f * eps * (sr12 - sr6);
+    const float scale = 1.0f - lam;
+    const float q = sqrtf(r2) * inv_rsc, q2 = q * q;
+    fmag = hf * scale * (q2 * q2 * q);
+    e = he * scale;
+    dvdl = -he - scale * hf * (0.5f * ss6) / (6.0f * (rsc6 * inv_rsc));
+}
+
 // CPU_SEM = false: the reference CUDA kernel's conventions
-//   (src/cuda/cuda.cu:239-316): rint min-image by multiplication, r^2 < 1e-16
-//   skip, no LJ cutoff, energy only for atom targets.
+//   (src/cuda/cuda.cu:239-316, alchemical form 367-566): rint min-image by
+//   multiplication, r^2 < 1e-16 skip, no LJ cutoff, energy only for atom
+//   targets.
 // CPU_SEM = true: f_nonbonded_cpu's conventions (src/non_bonded.rs:967-1054):
-//   min-image by division with ties away from zero, r^2 < 1e-12 skip, LJ only
-//   for r <= lj_cutoff, energy when either body is an atom.
-template <bool CPU_SEM>
+//   min-image by division with ties away from zero, r^2 < 1e-12 skip (an
+//   alchemical pair there keeps its soft-core contact energy), LJ only for
+//   r <= lj_cutoff, energy when either body is an atom.
+// ALCH: pairs with the alchemical bit take soft-core LJ at the schedule's LJ
+//   lambda and Coulomb times its scale; their dH/dlambda is summed.
+template <bool CPU_SEM, bool ALCH>
 __global__ void __launch_bounds__(NB_BLOCK) nb_pair_kernel(
     PosPtrs pos, ForcePtrs out, const uint2* __restrict__ pidx, const float2* __restrict__ plj,
     const float* __restrict__ pqq, uint64_t n, float3 ext, float3 inv_ext, float rc, float alpha,
-    float ljc, uint32_t ovr, double* __restrict__ partials) {
-    double w_acc = 0.0, e_acc = 0.0;
+    float ljc, uint32_t ovr, AlchSched al, double* __restrict__ partials) {
+    double w_acc = 0.0, e_acc = 0.0, h_acc = 0.0;
     const bool lj_off = ovr & DYN_OVR_LJ_DISABLED;
     const bool co_off = ovr & DYN_OVR_COULOMB_DISABLED;
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (uint64_t)gridDim.x * blockDim.x) {
         const uint2 w = pidx[p];
         const uint32_t bt = (w.x >> 28) & 7u, bs = (w.y >> 28) & 7u;
-        const uint32_t it = w.x & IDX_MASK, is = w.y & IDX_MASK;
+        const uint32_t it = w.x & TGT_MASK, is = w.y & IDX_MASK;
         const bool scale14 = w.x >> 31, sym = w.y >> 31;
+        const bool alch = ALCH && (w.x & ALCH_BIT);
+        const bool e_counts = CPU_SEM ? (bt == 0 || bs == 0) : (bt == 0);
         const float3 pt = ld_pos(pos.p, bt, it);
         const float3 ps = ld_pos(pos.p, bs, is);
         float3 d = pt - ps;
@@ -93,19 +149,34 @@ __global__ void __launch_bounds__(NB_BLOCK) nb_pair_kernel(
             d.z -= rintf(d.z * inv_ext.z) * ext.z;
         }
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        if (r2 < (CPU_SEM ? 1e-12f : 1e-16f)) continue;
+        const float2 lj = plj[p];
+        if (r2 < (CPU_SEM ? 1e-12f : 1e-16f)) {
+            if (CPU_SEM && alch && !lj_off && lj.y != 0.f) {
+                float fs, es, dv;
+                soft_core(0.f, lj.x, lj.y, al.ll, fs, es, dv);
+                if (scale14) { es *= 0.5f; dv *= 0.5f; }
+                if (e_counts) e_acc += (double)es;
+                h_acc += (double)(dv * al.dll);
+            }
+            continue;
+        }
         const float inv_r = rsqrtf(r2);
         const float r = r2 * inv_r;
-        const float2 lj = plj[p];
-        float fmag = 0.f, e = 0.f;
+        float fmag = 0.f, e = 0.f, dh = 0.f;
         if (!lj_off && lj.y != 0.f && (!CPU_SEM || r <= ljc)) {
-            const float sr = lj.x * inv_r;
-            const float sr2 = sr * sr;
-            const float sr6 = sr2 * sr2 * sr2;
-            const float sr12 = sr6 * sr6;
-            float fl = 24.0f * lj.y * fmaf(2.f, sr12, -sr6) * inv_r;
-            float el = 4.f * lj.y * (sr12 - sr6);
-            if (scale14) { fl *= 0.5f; el *= 0.5f; }
+            float fl, el;
+            if (alch) {
+                soft_core(r2, lj.x, lj.y, al.ll, fl, el, dh);
+                dh *= al.dll;
+            } else {
+                const float sr = lj.x * inv_r;
+                const float sr2 = sr * sr;
+                const float sr6 = sr2 * sr2 * sr2;
+                const float sr12 = sr6 * sr6;
+                fl = 24.0f * lj.y * fmaf(2.f, sr12, -sr6) * inv_r;
+                el = 4.f * lj.y * (sr12 - sr6);
+            }
+            if (scale14) { fl *= 0.5f; el *= 0.5f; dh *= 0.5f; }
             fmag += fl; e += el;
         }
         const float qq = pqq[p];
@@ -116,11 +187,17 @@ __global__ void __launch_bounds__(NB_BLOCK) nb_pair_kernel(
             float fc = qq * fmaf(ec, inv_r * inv_r, 2.0f * alpha * ex * INV_SQRT_PI_F * inv_r);
             float eco = qq * inv_r * ec;
             if (scale14) { fc *= 0.833333333f; eco *= 0.833333333f; }
-            fmag += fc; e += eco;
+            if (alch) {
+                fmag += fc * al.cs; e += eco * al.cs;
+                dh += eco * al.dcs;
+            } else {
+                fmag += fc; e += eco;
+            }
         }
         const float3 f = d * (fmag * inv_r);
         w_acc += (double)d.x * (double)f.x + (double)d.y * (double)f.y + (double)d.z * (double)f.z;
-        if (CPU_SEM ? (bt == 0 || bs == 0) : (bt == 0)) e_acc += (double)e;
+        if (e_counts) e_acc += (double)e;
+        if (ALCH) h_acc += (double)dh;
         long long* ft = out.f[bt] + 3 * (size_t)it;
         fix_atomic_add(ft + 0, fix_from_float(f.x));
         fix_atomic_add(ft + 1, fix_from_float(f.y));
@@ -132,24 +209,45 @@ __global__ void __launch_bounds__(NB_BLOCK) nb_pair_kernel(
             fix_atomic_add(fs + 2, -fix_from_float(f.z));
         }
     }
-    double v[2] = {w_acc, e_acc};
-    block_sum_d<2>(v);
-    if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x + 0] = v[0];
-        partials[2 * blockIdx.x + 1] = v[1];
-    }
+    double v[NB_PART] = {w_acc, e_acc, h_acc};
+    block_sum_d<NB_PART>(v);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NB_PART; ++k) partials[NB_PART * blockIdx.x + k] = v[k];
 }
 
 // Sums block partials in a fixed order (deterministic).
 __global__ void nb_finalize_kernel(const double* __restrict__ partials, int nblocks,
                                    double* __restrict__ scalars) {
-    double v[2] = {0.0, 0.0};
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-        v[0] += partials[2 * b];
-        v[1] += partials[2 * b + 1];
+    double v[NB_PART] = {0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        for (int k = 0; k < NB_PART; ++k) v[k] += partials[NB_PART * b + k];
+    block_sum_d<NB_PART>(v);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NB_PART; ++k) scalars[k] = v[k];
+}
+
+// Marks the installed pairs that cross the boundary of the atom range
+// [lo, hi) as alchemical, as setup_pairs does for the alchemical molecule
+// (src/non_bonded.rs:581-612): atom-atom pairs with exactly one end inside,
+// atom-water pairs whose atom is inside; water-water pairs never.  Clears
+// the bit on every other pair and counts the marked ones.
+__global__ void mark_alch_kernel(uint64_t n, uint32_t lo, uint32_t hi, uint2* __restrict__ pidx,
+                                 unsigned long long* __restrict__ count) {
+    uint32_t c = 0;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        uint2 w = pidx[p];
+        const uint32_t bt = (w.x >> 28) & 7u, bs = (w.y >> 28) & 7u;
+        const uint32_t it = w.x & TGT_MASK, is = w.y & IDX_MASK;
+        const bool in_t = bt == 0 && it >= lo && it < hi;
+        const bool in_s = bs == 0 && is >= lo && is < hi;
+        const bool a = in_t != in_s;
+        w.x = a ? (w.x | ALCH_BIT) : (w.x & ~ALCH_BIT);
+        pidx[p] = w;
+        c += a;
     }
-    block_sum_d<2>(v);
-    if (threadIdx.x == 0) { scalars[0] = v[0]; scalars[1] = v[1]; }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
 }
 
 __global__ void pack_pairs_kernel(uint64_t n, const uint32_t* __restrict__ tgt,
@@ -163,7 +261,8 @@ __global__ void pack_pairs_kernel(uint64_t n, const uint32_t* __restrict__ tgt,
          p += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t f = fl[p];
         uint2 w;
-        w.x = (tgt[p] & IDX_MASK) | ((uint32_t)(bt[p] & 7u) << 28) | ((f & DYN_PAIR_SCALE14) ? 0x80000000u : 0u);
+        w.x = (tgt[p] & TGT_MASK) | ((uint32_t)(bt[p] & 7u) << 28) |
+              ((f & DYN_PAIR_SCALE14) ? 0x80000000u : 0u) | ((f & DYN_PAIR_ALCH) ? ALCH_BIT : 0u);
         w.y = (src[p] & IDX_MASK) | ((uint32_t)(bs[p] & 7u) << 28) | ((f & DYN_PAIR_SYMMETRIC) ? 0x80000000u : 0u);
         pidx[p] = w;
         plj[p] = make_float2(sig[p], (f & DYN_PAIR_LJ) ? eps[p] : 0.f);
@@ -406,8 +505,8 @@ extern "C" int dyn_nb_create(void* stream, uint32_t n_dyn, uint32_t n_water, flo
     DYN_CHECK(out != nullptr, DYN_ERR_INVALID, "dyn_nb_create: out is NULL");
     DYN_CHECK(cutoff_ewald > 0.f && alpha_ewald > 0.f, DYN_ERR_INVALID,
               "dyn_nb_create: cutoff and alpha must be > 0");
-    DYN_CHECK(n_dyn < (1u << 28) && n_water < (1u << 28), DYN_ERR_INVALID,
-              "dyn_nb_create: at most 2^28 atoms / waters");
+    DYN_CHECK(n_dyn < (1u << 27) && n_water < (1u << 27), DYN_ERR_INVALID,
+              "dyn_nb_create: fewer than 2^27 atoms / waters");
     *out = nullptr;
     dyn_nb_s* h = new dyn_nb_s();
     h->stream = (cudaStream_t)stream;
@@ -420,9 +519,9 @@ extern "C" int dyn_nb_create(void* stream, uint32_t n_dyn, uint32_t n_water, flo
             (rc = halloc(&h->h_pos[a], n3)) || (rc = halloc(&h->h_f[a], n3)))
             break;
     }
-    if (rc == DYN_OK) rc = dalloc(&h->d_partials, 2 * NB_MAX_BLOCKS);
-    if (rc == DYN_OK) rc = dalloc(&h->d_scalars, 2);
-    if (rc == DYN_OK) rc = halloc(&h->h_scalars, 2);
+    if (rc == DYN_OK) rc = dalloc(&h->d_partials, NB_PART * NB_MAX_BLOCKS);
+    if (rc == DYN_OK) rc = dalloc(&h->d_scalars, NB_PART);
+    if (rc == DYN_OK) rc = halloc(&h->h_scalars, NB_PART);
     if (rc != DYN_OK) {
         dyn_nb_destroy(h);
         return rc;
@@ -461,6 +560,8 @@ extern "C" int dyn_nb_set_pairs(dyn_nb_t h, uint64_t n, const uint32_t* tgt, con
     int rc = ensure_pair_capacity(h, n);
     if (rc) return rc;
     h->n_pairs = n;
+    h->n_alch = 0;
+    for (uint64_t p = 0; p < n; ++p) h->n_alch += (flags[p] & DYN_PAIR_ALCH) != 0;
     if (n == 0) return DYN_OK;
     // stage through temporary device buffers, then pack
     void* tmp = nullptr;
@@ -511,7 +612,7 @@ extern "C" int dyn_nb_get_pairs(dyn_nb_t h, uint64_t n, uint32_t* tgt, uint32_t*
     DYN_CUDA(cudaStreamSynchronize(st));
     for (uint64_t p = 0; p < n; ++p) {
         const uint32_t bt = (idx[p].x >> 28) & 7u, bs = (idx[p].y >> 28) & 7u;
-        if (tgt) tgt[p] = idx[p].x & IDX_MASK;
+        if (tgt) tgt[p] = idx[p].x & TGT_MASK;
         if (src) src[p] = idx[p].y & IDX_MASK;
         if (body_tgt) body_tgt[p] = (uint8_t)bt;
         if (body_src) body_src[p] = (uint8_t)bs;
@@ -523,6 +624,7 @@ extern "C" int dyn_nb_get_pairs(dyn_nb_t h, uint64_t n, uint32_t* tgt, uint32_t*
             uint8_t f = 0;
             if (idx[p].x >> 31) f |= DYN_PAIR_SCALE14;
             if (idx[p].y >> 31) f |= DYN_PAIR_SYMMETRIC;
+            if (idx[p].x & ALCH_BIT) f |= DYN_PAIR_ALCH;
             if (lj[p].y != 0.f) f |= DYN_PAIR_LJ;
             // setup_pairs sets calc_coulomb for every pair but water O ones
             const bool o_t = bt == DYN_BODY_W_O, o_s = bs == DYN_BODY_W_O;
@@ -645,6 +747,7 @@ extern "C" int dyn_nb_build_pairs(dyn_nb_t h, const float* pos_dyn, const float*
     TRYC(cudaGetLastError());
     TRYC(cudaStreamSynchronize(st));
     h->n_pairs = total;
+    h->n_alch = 0;
     if (n_pairs_out) *n_pairs_out = total;
     cleanup();
 #undef TRY
@@ -652,11 +755,13 @@ extern "C" int dyn_nb_build_pairs(dyn_nb_t h, const float* pos_dyn, const float*
     return DYN_OK;
 }
 
-extern "C" int dyn_nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o,
+namespace {
+
+int nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o,
                              const float* pos_w_m, const float* pos_w_h0, const float* pos_w_h1,
                              const float cell_extent[3], uint32_t override_bits, double* f_dyn,
                              double* f_w_o, double* f_w_m, double* f_w_h0, double* f_w_h1,
-                             double* virial, double* energy) {
+                             double* virial, double* energy, double lambda, double* dh_dl) {
     DYN_CHECK(h && cell_extent, DYN_ERR_INVALID, "dyn_nb_forces: NULL argument");
     const float* in[5] = {pos_dyn, pos_w_o, pos_w_m, pos_w_h0, pos_w_h1};
     double* outp[5] = {f_dyn, f_w_o, f_w_m, f_w_h0, f_w_h1};
@@ -684,14 +789,14 @@ extern "C" int dyn_nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_
     PosPtrs pp;
     ForcePtrs fp;
     for (int a = 0; a < 5; ++a) { pp.p[a] = h->d_pos[a]; fp.f[a] = h->d_f[a]; }
-    if (h->ljc > 0.f)
-        nb_pair_kernel<true><<<blocks, NB_BLOCK, 0, st>>>(pp, fp, h->d_pidx, h->d_plj, h->d_pqq, h->n_pairs,
-                                                          ext, inv_ext, h->rc, h->alpha, h->ljc,
-                                                          override_bits, h->d_partials);
-    else
-        nb_pair_kernel<false><<<blocks, NB_BLOCK, 0, st>>>(pp, fp, h->d_pidx, h->d_plj, h->d_pqq, h->n_pairs,
-                                                           ext, inv_ext, h->rc, h->alpha, h->ljc,
-                                                           override_bits, h->d_partials);
+    // the alchemical kernel runs when any installed pair is alchemical, as
+    // force_nonbonded_gpu picks it (src/gpu_interface.rs:488-499)
+    const AlchSched al = alch_schedule(lambda);
+    const bool cpu = h->ljc > 0.f, alch = h->n_alch > 0;
+    auto kern = cpu ? (alch ? nb_pair_kernel<true, true> : nb_pair_kernel<true, false>)
+                    : (alch ? nb_pair_kernel<false, true> : nb_pair_kernel<false, false>);
+    kern<<<blocks, NB_BLOCK, 0, st>>>(pp, fp, h->d_pidx, h->d_plj, h->d_pqq, h->n_pairs, ext, inv_ext,
+                                      h->rc, h->alpha, h->ljc, override_bits, al, h->d_partials);
     DYN_CUDA(cudaGetLastError());
     nb_finalize_kernel<<<1, 256, 0, st>>>(h->d_partials, blocks, h->d_scalars);
     DYN_CUDA(cudaGetLastError());
@@ -700,7 +805,7 @@ extern "C" int dyn_nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_
         if (!n3) continue;
         DYN_CUDA(cudaMemcpyAsync(h->h_f[a], h->d_f[a], n3 * sizeof(long long), cudaMemcpyDeviceToHost, st));
     }
-    DYN_CUDA(cudaMemcpyAsync(h->h_scalars, h->d_scalars, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    DYN_CUDA(cudaMemcpyAsync(h->h_scalars, h->d_scalars, NB_PART * sizeof(double), cudaMemcpyDeviceToHost, st));
     DYN_CUDA(cudaStreamSynchronize(st));
     for (int a = 0; a < 5; ++a) {
         const size_t n3 = 3 * (size_t)h->n_of(a);
@@ -709,5 +814,52 @@ extern "C" int dyn_nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_
     }
     if (virial) *virial = h->h_scalars[0];
     if (energy) *energy = h->h_scalars[1];
+    if (dh_dl) *dh_dl = alch ? h->h_scalars[2] : 0.0;
+    return DYN_OK;
+}
+
+}  // namespace
+
+extern "C" int dyn_nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o,
+                             const float* pos_w_m, const float* pos_w_h0, const float* pos_w_h1,
+                             const float cell_extent[3], uint32_t override_bits, double* f_dyn,
+                             double* f_w_o, double* f_w_m, double* f_w_h0, double* f_w_h1,
+                             double* virial, double* energy) {
+    return nb_forces(h, pos_dyn, pos_w_o, pos_w_m, pos_w_h0, pos_w_h1, cell_extent, override_bits,
+                     f_dyn, f_w_o, f_w_m, f_w_h0, f_w_h1, virial, energy, 0.0, nullptr);
+}
+
+extern "C" int dyn_nb_forces_alch(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o,
+                                  const float* pos_w_m, const float* pos_w_h0,
+                                  const float* pos_w_h1, const float cell_extent[3],
+                                  uint32_t override_bits, double lambda_alch, double* f_dyn,
+                                  double* f_w_o, double* f_w_m, double* f_w_h0, double* f_w_h1,
+                                  double* virial, double* energy, double* dh_dl) {
+    DYN_CHECK(std::isfinite(lambda_alch), DYN_ERR_INVALID, "dyn_nb_forces_alch: lambda is not finite");
+    return nb_forces(h, pos_dyn, pos_w_o, pos_w_m, pos_w_h0, pos_w_h1, cell_extent, override_bits,
+                     f_dyn, f_w_o, f_w_m, f_w_h0, f_w_h1, virial, energy, lambda_alch, dh_dl);
+}
+
+extern "C" int dyn_nb_mark_alch(dyn_nb_t h, uint32_t atom_begin, uint32_t atom_end,
+                                uint64_t* n_marked) {
+    DYN_CHECK(h, DYN_ERR_INVALID, "dyn_nb_mark_alch: NULL handle");
+    DYN_CHECK(atom_begin <= atom_end && atom_end <= h->n_dyn, DYN_ERR_INVALID,
+              "dyn_nb_mark_alch: range outside the atoms");
+    cudaStream_t st = h->stream;
+    unsigned long long* d_cnt = nullptr;
+    DYN_CUDA(cudaMalloc(&d_cnt, sizeof(unsigned long long)));
+    cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st);
+    if (h->n_pairs) {
+        const int blocks = (int)std::min<uint64_t>((h->n_pairs + 255) / 256, 148 * 8);
+        mark_alch_kernel<<<blocks, 256, 0, st>>>(h->n_pairs, atom_begin, atom_end, h->d_pidx, d_cnt);
+    }
+    unsigned long long c = 0;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_cnt);
+    if (e != cudaSuccess) return dyn::cuda_fail(e, "dyn_nb_mark_alch");
+    h->n_alch = c;
+    if (n_marked) *n_marked = c;
     return DYN_OK;
 }

@@ -13,7 +13,9 @@ line by line:
     force_nonbonded_gpu(stream, kernels, pairs, atoms_dyn, water, cell_extent,
                         forces, per_neighbor, overrides, lambda_alch)
         -> force_nonbonded_gpu(forces, per_neighbor, pos_dyn, pos_water,
-                               cell_extent, overrides)
+                               cell_extent, overrides, lambda_alch)
+    setup_pairs' alch_interaction for molecule m (atoms [b, e))
+        -> PerNeighborGpu.mark_alchemical(b, e), or the ``alch`` column
 
 Errors raise DynError instead of panicking or printing (the reference
 unwraps and eprintln!s, src/gpu_interface.rs:557-564).
@@ -67,6 +69,8 @@ def pack_flags(pairs):
     fl |= np.asarray(pairs["calc_lj"], dtype=np.uint8) * _lib.DYN_PAIR_LJ
     fl |= np.asarray(pairs["calc_coulomb"], dtype=np.uint8) * _lib.DYN_PAIR_COULOMB
     fl |= np.asarray(pairs["symmetric"], dtype=np.uint8) * _lib.DYN_PAIR_SYMMETRIC
+    if "alch" in pairs:
+        fl |= np.asarray(pairs["alch"], dtype=np.uint8) * _lib.DYN_PAIR_ALCH
     return fl
 
 
@@ -76,7 +80,7 @@ class PerNeighborGpu:
     ``pairs`` is the flat SoA the reference builds: tgt, src (uint32), sigma,
     eps, q_tgt, q_src (float32), body_tgt / body_src (0 atom, 1..4 water
     O, M, H0, H1) and the bool arrays scale_14, calc_lj, calc_coulomb,
-    symmetric.  (The reference's atom_types_* + water_types_* pair maps onto
+    symmetric and, optionally, alch (alch_interaction).  (The reference's atom_types_* + water_types_* pair maps onto
     body_* as body = water_type for water ends and 0 otherwise.)
     """
 
@@ -123,6 +127,14 @@ class PerNeighborGpu:
         self.n_pairs = n.value
         return self
 
+    def mark_alchemical(self, atom_begin, atom_end):
+        """Flags the pairs crossing the boundary of the alchemical molecule
+        (atoms [atom_begin, atom_end)) as setup_pairs does
+        (src/non_bonded.rs:581-612); returns the number flagged."""
+        n = C.c_uint64()
+        check(lib().dyn_nb_mark_alch(self.forces.handle, int(atom_begin), int(atom_end), C.byref(n)))
+        return n.value
+
     def get_pairs(self):
         """The installed list: tgt, src, body_tgt, body_src, flags, sigma,
         eps and qq (= q_tgt * q_src as stored on the device)."""
@@ -142,12 +154,14 @@ class PerNeighborGpu:
         return out
 
 
-def force_nonbonded_gpu(forces, per_neighbor, pos_dyn, pos_water, cell_extent, overrides=0):
+def force_nonbonded_gpu(forces, per_neighbor, pos_dyn, pos_water, cell_extent, overrides=0,
+                        lambda_alch=None):
     """force_nonbonded_gpu (src/gpu_interface.rs:463-632).
 
     pos_water: dict {1: O, 2: M, 3: H0, 4: H1} or a sequence (O, M, H0, H1)
     of (n_water, 3) arrays.  Returns (f_dyn (n,3), f_water dict {1..4: (n,3)},
-    virial, energy) in float64.
+    virial, energy) in float64; with ``lambda_alch`` given, a fifth element,
+    the alchemical pairs' dH/dlambda (0 when none is installed).
     """
     del per_neighbor  # the handle owns the installed list
     nd, nw = forces.n_dyn, forces.n_water
@@ -162,6 +176,13 @@ def force_nonbonded_gpu(forces, per_neighbor, pos_dyn, pos_water, cell_extent, o
     fw = [np.zeros((max(nw, 1), 3)) for _ in range(4)]
     vir = C.c_double()
     en = C.c_double()
-    check(lib().dyn_nb_forces(forces.handle, ptr(pd), *[ptr(p) for p in pws], ptr(ext),
-                              int(overrides), ptr(fd), *[ptr(f) for f in fw], C.byref(vir), C.byref(en)))
-    return fd[:nd], {k + 1: fw[k][:nw] for k in range(4)}, vir.value, en.value
+    if lambda_alch is None:
+        check(lib().dyn_nb_forces(forces.handle, ptr(pd), *[ptr(p) for p in pws], ptr(ext),
+                                  int(overrides), ptr(fd), *[ptr(f) for f in fw], C.byref(vir),
+                                  C.byref(en)))
+        return fd[:nd], {k + 1: fw[k][:nw] for k in range(4)}, vir.value, en.value
+    dh = C.c_double()
+    check(lib().dyn_nb_forces_alch(forces.handle, ptr(pd), *[ptr(p) for p in pws], ptr(ext),
+                                   int(overrides), float(lambda_alch), ptr(fd),
+                                   *[ptr(f) for f in fw], C.byref(vir), C.byref(en), C.byref(dh)))
+    return fd[:nd], {k + 1: fw[k][:nw] for k in range(4)}, vir.value, en.value, dh.value

@@ -84,6 +84,11 @@ typedef struct dyn_nb_s* dyn_nb_t;
 #define DYN_PAIR_LJ 2u
 #define DYN_PAIR_COULOMB 4u
 #define DYN_PAIR_SYMMETRIC 8u
+/* The pair crosses the alchemical molecule's boundary (the reference's
+ * alch_interactions array, src/gpu_interface.rs:238,267-338): soft-core LJ
+ * and scaled Coulomb on the staged decoupling schedule in
+ * dyn_nb_forces_alch.  dyn_nb_forces_static ignores it (full coupling). */
+#define DYN_PAIR_ALCH 16u
 
 /* Body codes, one byte per pair end: 0 = non-water atom, 1..4 = water site
  * O, M, H0, H1 (the reference's atom_types_* + water_types_* arrays,
@@ -101,6 +106,7 @@ typedef struct dyn_nb_s* dyn_nb_t;
  * (LJ only for r <= lj_cutoff, src/non_bonded.rs:1001). */
 int dyn_nb_create(void* stream, uint32_t n_dyn, uint32_t n_water, float cutoff_ewald,
                   float alpha_ewald, float lj_cutoff, dyn_nb_t* out);
+/* n_dyn and n_water must each be below 2^27. */
 
 /* Replaces PerNeighborGpu::new (src/gpu_interface.rs:243-410): uploads the
  * flat pair list.  tgt/src index the atom array (body 0) or the water
@@ -150,6 +156,29 @@ int dyn_nb_forces(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o, const 
                   const float* pos_w_h0, const float* pos_w_h1, const float cell_extent[3],
                   uint32_t override_bits, double* f_dyn, double* f_w_o, double* f_w_m,
                   double* f_w_h0, double* f_w_h1, double* virial, double* energy);
+
+/* force_nonbonded_gpu with its lambda_alch argument (src/gpu_interface.rs:
+ * 463-632, kernel src/cuda/cuda.cu:367-566).  When any installed pair
+ * carries DYN_PAIR_ALCH, those pairs take Beutler soft-core LJ (alpha 0.5,
+ * power 1, soft-core sigma >= 3 A) at the schedule's LJ lambda and
+ * short-range Coulomb times the schedule's scale (staged schedule: Coulomb
+ * off over lambda 0..0.5, LJ decoupled over 0.5..1, lambda clamped to
+ * [0, 1]), and *dh_dl receives the sum of their dH/dlambda.  With no
+ * alchemical pair installed this is dyn_nb_forces and *dh_dl = 0.
+ * dyn_nb_forces is this call with lambda_alch = 0 and no dh_dl. */
+int dyn_nb_forces_alch(dyn_nb_t h, const float* pos_dyn, const float* pos_w_o,
+                       const float* pos_w_m, const float* pos_w_h0, const float* pos_w_h1,
+                       const float cell_extent[3], uint32_t override_bits, double lambda_alch,
+                       double* f_dyn, double* f_w_o, double* f_w_m, double* f_w_h0,
+                       double* f_w_h1, double* virial, double* energy, double* dh_dl);
+
+/* Sets DYN_PAIR_ALCH on the installed pairs as setup_pairs does for the
+ * alchemical molecule (src/non_bonded.rs:581-612) when that molecule is the
+ * atoms [atom_begin, atom_end): atom-atom pairs with exactly one end in the
+ * range and atom-water pairs whose atom is in it.  Clears it on every other
+ * pair; an empty range clears all.  n_marked (may be NULL) receives the
+ * number of marked pairs. */
+int dyn_nb_mark_alch(dyn_nb_t h, uint32_t atom_begin, uint32_t atom_end, uint64_t* n_marked);
 
 /* Releases everything dyn_nb_create allocated. */
 int dyn_nb_destroy(dyn_nb_t h);

@@ -127,9 +127,13 @@ def build_all_neighbors(sysd, skin, cutoff):
 # flat pair list (setup_pairs + PerNeighborGpu layout)
 # --------------------------------------------------------------------------
 
-def setup_pairs(sysd, lists):
+def setup_pairs(sysd, lists, alch_range=None):
     """setup_pairs (src/non_bonded.rs:541-677) flattened to the SoA that
     PerNeighborGpu::new builds (src/gpu_interface.rs:243-340).
+
+    ``alch_range`` = (begin, end): the alchemical molecule's atoms; the
+    ``alch`` column flags atom-atom pairs with exactly one end inside and
+    atom-water pairs whose atom is inside (src/non_bonded.rs:581-612).
 
     Returns a dict of numpy arrays, one entry per pair, in the reference's
     canonical order: std-std (i<j), std-water (sites O,M,H0,H1), water-water
@@ -147,9 +151,14 @@ def setup_pairs(sysd, lists):
 
     cols = {k: [] for k in ("tgt", "src", "sigma", "eps", "q_tgt", "q_src", "atype_tgt",
                             "wtype_tgt", "atype_src", "wtype_src", "scale_14", "calc_lj",
-                            "calc_coulomb", "symmetric")}
+                            "calc_coulomb", "symmetric", "alch")}
+    ab, ae = alch_range if alch_range is not None else (0, 0)
 
-    def push(t, s, sg, ep, qt, qs, at, wt, as_, ws, sc, lj, co):
+    def in_alch(i):
+        return ab <= i < ae
+
+    def push(t, s, sg, ep, qt, qs, at, wt, as_, ws, sc, lj, co, al=0):
+        cols["alch"].append(al)
         cols["tgt"].append(t); cols["src"].append(s)
         cols["sigma"].append(sg); cols["eps"].append(ep)
         cols["q_tgt"].append(qt); cols["q_src"].append(qs)
@@ -170,7 +179,8 @@ def setup_pairs(sysd, lists):
                 continue
             sg = f32(f32(0.5) * (sig[i] + sig[j]))
             ep = f32(np.sqrt(f32(eps[i] * eps[j]), dtype=f32))
-            push(i, j, sg, ep, q_atom[i], q_atom[j], 0, 0, 0, 0, int((i, j) in s14), 1, 1)
+            push(i, j, sg, ep, q_atom[i], q_atom[j], 0, 0, 0, 0, int((i, j) in s14), 1, 1,
+                 int(in_alch(i) != in_alch(j)))
     # std-water (src/non_bonded.rs:605-625); LJ row src/non_bonded.rs:139-145
     for i in range(n_std):
         sg = f32(f32(0.5) * (sig[i] + opc.O_SIGMA))
@@ -178,7 +188,7 @@ def setup_pairs(sysd, lists):
         for w in std_water[i]:
             for site in SITES_ORDER:
                 push(i, int(w), sg, ep, q_atom[i], site_q[site], 0, 0, 1, site, 0,
-                     int(site == SITE_O), int(site != SITE_O))
+                     int(site == SITE_O), int(site != SITE_O), int(in_alch(i)))
     # water-water (src/non_bonded.rs:628-664)
     for i0 in range(len(water_water)):
         for i1 in water_water[i0]:
@@ -231,8 +241,15 @@ def _gather(pos_dyn, pos_w, atype, wtype, idx):
 
 
 def pair_forces(pairs, pos_dyn, pos_w, ext, cutoff, alpha, lj_cutoff=None,
-                lj_disabled=False, coulomb_disabled=False, gpu_semantics=False):
+                lj_disabled=False, coulomb_disabled=False, gpu_semantics=False,
+                lambda_alch=None):
     """Per-pair force on the target, energy and virial in float64.
+
+    With ``lambda_alch`` given, pairs whose ``alch`` column is set take
+    soft-core LJ and scaled Coulomb on the staged decoupling schedule
+    (nonbonded_force_alchemical_kernel, src/cuda/cuda.cu:367-566;
+    f_nonbonded_cpu, src/non_bonded.rs:950-1057) and the function returns
+    a fifth value, their summed dH/dlambda.
 
     ``gpu_semantics`` selects the reference CUDA kernel's conventions
     (src/cuda/cuda.cu:239-316): no LJ cutoff, r^2 < 1e-16 skip, energy only
@@ -274,8 +291,28 @@ def pair_forces(pairs, pos_dyn, pos_w, ext, cutoff, alpha, lj_cutoff=None,
     e_lj = np.where(sc, e_lj * 0.5, e_lj)
     f_c = np.where(sc, f_c / 1.2, f_c)
     e_c = np.where(sc, e_c / 1.2, e_c)
+    dh = np.zeros(len(r))
+    alch = None
+    if lambda_alch is not None and "alch" in pairs:
+        from .method import decoupling_schedule, soft_core_lj
+        cs, dcs, ll, dll = decoupling_schedule(np.float32(lambda_alch))
+        alch = pairs["alch"].astype(bool)
+        # the CPU path evaluates a coincident alchemical pair at r = 0
+        r_sc = np.where(skip, 0.0, r)
+        fs, es, dv = _soft_core_at(r_sc, sig, eps, ll, soft_core_lj)
+        lj_sc = lj_on | (skip & ~np.bool_(gpu_semantics) & pairs["calc_lj"].astype(bool)
+                         & (not lj_disabled))
+        w14 = np.where(sc, 0.5, 1.0)
+        f_lj = np.where(alch, np.where(lj_on, fs * w14, 0.0), f_lj)
+        e_lj = np.where(alch, np.where(lj_sc, es * w14, 0.0), e_lj)
+        dh = np.where(alch & lj_sc, dv * dll * w14, 0.0)
+        dh = dh + np.where(alch & ~skip, e_c * dcs, 0.0)
+        f_c = np.where(alch, f_c * cs, f_c)
+        e_c = np.where(alch, e_c * cs, e_c)
     fmag = np.where(skip, 0.0, f_lj + f_c)
     e = np.where(skip, 0.0, e_lj + e_c)
+    if alch is not None and not gpu_semantics:
+        e = np.where(skip & alch, e_lj, e)
     f = d * (fmag * inv_r)[:, None]
     virial = float(np.sum(fmag * r))
     if gpu_semantics:
@@ -283,7 +320,18 @@ def pair_forces(pairs, pos_dyn, pos_w, ext, cutoff, alpha, lj_cutoff=None,
     else:
         e_mask = (pairs["atype_tgt"] == 0) | (pairs["atype_src"] == 0)
     energy = float(np.sum(e[e_mask]))
+    if lambda_alch is not None:
+        return f, energy, virial, e, float(np.sum(dh))
     return f, energy, virial, e
+
+
+def _soft_core_at(r, sig, eps, lam, soft_core_lj):
+    """soft_core_lj with the reference's guards: zero where eps is 0 or the
+    soft-core radius is 0 (r = 0 at lambda 0)."""
+    ss6 = np.maximum(sig, 3.0) ** 6
+    ok = (eps != 0.0) & (r ** 6 + 0.5 * ss6 * lam > 0.0)
+    fs, es, dv = soft_core_lj(np.where(ok, r, 1.0), sig, np.where(ok, eps, 0.0), lam)
+    return np.where(ok, fs, 0.0), np.where(ok, es, 0.0), np.where(ok, dv, 0.0)
 
 
 def accumulate_pair_forces(pairs, f, n_dyn, n_water):

@@ -6,7 +6,10 @@
 * dyn_nb_forces matches the float64 evaluation of the same pair list with
   the reference CUDA kernel's conventions (src/cuda/cuda.cu:239-316) and with
   the CPU path's (src/non_bonded.rs:950-1057);
-* results are bit-identical from call to call (64-bit fixed-point sums).
+* results are bit-identical from call to call (64-bit fixed-point sums);
+* with one molecule decoupled (alch_interaction pairs), dyn_nb_forces_alch
+  matches the float64 evaluation of the alchemical pair kernel
+  (src/cuda/cuda.cu:367-566) and of the CPU path, dH/dlambda included.
 """
 import numpy as np
 import pytest
@@ -150,6 +153,59 @@ def test_set_pairs_matches_build(gpu_lib):
     fp2.close()
 
 
+ALCH_MOL = (5, 10)  # the second chain of systems.mixed
+
+
+@pytest.mark.parametrize("lam", [0.0, 0.3, 0.75, 1.0])
+@pytest.mark.parametrize("lj_cutoff", [0.0, CUTOFF])
+def test_alchemical_forces_match_float64(gpu_lib, lam, lj_cutoff):
+    sysd = mixed()
+    fp, pn = _build(sysd, lj_cutoff)
+    n_marked = pn.mark_alchemical(*ALCH_MOL)
+    ref = opairs.setup_pairs(sysd, opairs.build_all_neighbors(sysd, SKIN, CUTOFF), alch_range=ALCH_MOL)
+    assert n_marked == int(ref["alch"].sum()) > 0
+    np.testing.assert_array_equal((pn.get_pairs()["flags"] & 16) != 0, ref["alch"] == 1)
+    pos_dyn, pw = _positions(sysd)
+    ext = (sysd["box_hi"] - sysd["box_lo"]).astype(np.float32)
+    fd, fw, vir, en, dh = gi.force_nonbonded_gpu(fp, pn, pos_dyn, pw, ext, lambda_alch=lam)
+    f, e_ref, v_ref, _, dh_ref = opairs.pair_forces(
+        ref, pos_dyn, pw, ext, CUTOFF, ALPHA, lj_cutoff=lj_cutoff if lj_cutoff > 0 else None,
+        gpu_semantics=lj_cutoff <= 0, lambda_alch=lam)
+    rd, rw = opairs.accumulate_pair_forces(ref, f, len(pos_dyn), len(pw[1]))
+    got = np.concatenate([fd.reshape(-1)] + [fw[k].reshape(-1) for k in (1, 2, 3, 4)])
+    exp = np.concatenate([rd.reshape(-1)] + [rw[k].reshape(-1) for k in (1, 2, 3, 4)])
+    assert rel_rms(got, exp) < FORCE_RTOL
+    assert abs(vir - v_ref) <= SCALAR_RTOL * abs(v_ref)
+    assert abs(en - e_ref) <= SCALAR_RTOL * max(abs(e_ref), 1.0)
+    assert abs(dh - dh_ref) <= SCALAR_RTOL * max(abs(dh_ref), 1.0)
+    fp.close()
+
+
+def test_alchemical_flags_from_set_pairs(gpu_lib):
+    """An alch column passed to set_pairs gives the same forces as marking
+    the built list; clearing the marks restores the plain kernel."""
+    sysd = mixed()
+    ref = opairs.setup_pairs(sysd, opairs.build_all_neighbors(sysd, SKIN, CUTOFF), alch_range=ALCH_MOL)
+    na, nw = len(sysd["atom_pos"]), len(sysd["water_pos"])
+    fp1, pn1 = _build(sysd)
+    pn1.mark_alchemical(*ALCH_MOL)
+    fp2 = gi.ForcesPositsGpu(na, nw, CUTOFF, ALPHA)
+    pn2 = gi.PerNeighborGpu(fp2, ref)
+    pos_dyn, pw = _positions(sysd)
+    ext = (sysd["box_hi"] - sysd["box_lo"]).astype(np.float32)
+    a = gi.force_nonbonded_gpu(fp1, pn1, pos_dyn, pw, ext, lambda_alch=0.6)
+    b = gi.force_nonbonded_gpu(fp2, pn2, pos_dyn, pw, ext, lambda_alch=0.6)
+    np.testing.assert_array_equal(a[0], b[0])
+    assert a[2] == b[2] and a[3] == b[3] and a[4] == b[4]
+    assert pn1.mark_alchemical(0, 0) == 0
+    plain = gi.force_nonbonded_gpu(fp1, pn1, pos_dyn, pw, ext)
+    cleared = gi.force_nonbonded_gpu(fp1, pn1, pos_dyn, pw, ext, lambda_alch=0.6)
+    np.testing.assert_array_equal(plain[0], cleared[0])
+    assert cleared[4] == 0.0
+    fp1.close()
+    fp2.close()
+
+
 def test_overrides_disable_terms(gpu_lib):
     sysd = mixed()
     fp, pn = _build(sysd)
@@ -174,4 +230,10 @@ def test_invalid_arguments_raise(gpu_lib):
            "symmetric": [1]}
     with pytest.raises(DynError):
         gi.PerNeighborGpu(fp, bad)
+    pn = gi.PerNeighborGpu(fp)
+    with pytest.raises(DynError):
+        pn.mark_alchemical(1, 3)   # beyond the two atoms
+    with pytest.raises(DynError):
+        gi.force_nonbonded_gpu(fp, pn, np.zeros((2, 3)), [np.zeros((0, 3))] * 4, [20.0] * 3,
+                               lambda_alch=float("nan"))
     fp.close()

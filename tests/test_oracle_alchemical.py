@@ -53,3 +53,32 @@ def test_alchemical_force_is_gradient(small, lam):
         e0 = method.all_forces(d, _params(n_pep, lam))["pe"]
         g[k] = (e1 - e0) / (2 * h)
     np.testing.assert_allclose(r["f_atoms"][a], -g, rtol=2e-3, atol=2e-3)
+
+
+@pytest.mark.parametrize("lam", [0.0, 0.3, 0.75, 1.0])
+def test_flat_pair_list_agrees_with_site_pairs(lam):
+    """The flat-pair-list restatement (setup_pairs' alch_interaction column
+    and the alchemical pair kernel's arithmetic) and the site-pair
+    restatement (f_nonbonded_cpu over all site pairs) give the same forces,
+    solute energy and dH/dlambda for one decoupled molecule."""
+    from oracle import pairs as opairs
+    from .systems import mixed
+    cut = 10.0
+    alpha = synth.ewald_alpha(cut)
+    sysd = mixed()
+    ref = opairs.setup_pairs(sysd, opairs.build_all_neighbors(sysd, 4.0, cut), alch_range=(5, 10))
+    assert ref["alch"].sum() > 0
+    pos_dyn, pw = opairs.site_positions(sysd)
+    ext = (sysd["box_hi"] - sysd["box_lo"]).astype(np.float32)
+    f, e, _, _, dh = opairs.pair_forces(ref, pos_dyn, pw, ext, cut, alpha, lj_cutoff=cut,
+                                        lambda_alch=lam)
+    fd, _ = opairs.accumulate_pair_forces(ref, f, len(pos_dyn), len(pw[1]))
+    sr = method.short_range(sysd, cut, alpha, lj_cutoff=cut, alch=(5, 10, lam))
+    assert abs(dh - sr["dh_dl"]) <= 1e-5 * max(abs(dh), 1.0)
+    assert abs(e - sr["e_solute"]) <= 1e-5 * max(abs(e), 1.0)
+    fs = sr["forces"][:len(pos_dyn)]
+    assert np.sqrt(np.mean((fd - fs) ** 2)) <= 1e-5 * np.sqrt(np.mean(fs ** 2))
+    if lam == 0.0:
+        f0, e0, _, _ = opairs.pair_forces(ref, pos_dyn, pw, ext, cut, alpha, lj_cutoff=cut)
+        np.testing.assert_allclose(f, f0, rtol=0, atol=1e-12)
+        assert abs(e - e0) < 1e-10
