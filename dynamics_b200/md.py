@@ -45,6 +45,39 @@ class BarostatCfg:
 
 
 @dataclass
+class SnapshotEnergyData:
+    """SnapshotEnergyData (src/snapshot.rs:61-93): the scalars of a frame
+    (kcal/mol, K, bar, A^3, amu/A^3)."""
+    energy_kinetic: float
+    energy_potential: float
+    energy_potential_nonbonded: float
+    energy_potential_bonded: float
+    temperature: float
+    pressure: float
+    dh_dl: Optional[float]
+    volume: float
+    density: float
+
+
+@dataclass
+class Snapshot:
+    """Snapshot (src/snapshot.rs:124-175): time (ps), atom positions wrapped
+    into the cell, water O / H0 / H1 positions, and, when recorded, atom and
+    water-O velocities and atom forces; ``cell`` = (box_lo, box_hi)."""
+    time: float
+    step: int
+    atom_posits: np.ndarray
+    water_o_posits: np.ndarray
+    water_h0_posits: np.ndarray
+    water_h1_posits: np.ndarray
+    energy_data: SnapshotEnergyData
+    cell: tuple
+    atom_velocities: Optional[np.ndarray] = None
+    water_velocities: Optional[np.ndarray] = None
+    force: Optional[np.ndarray] = None
+
+
+@dataclass
 class MdConfig:
     """The fields of MdConfig (src/config.rs:43-107) this engine uses.
 
@@ -81,6 +114,11 @@ class MdConfig:
     # alch_lambda on the reference's staged schedule (src/alchemical.rs)
     alch_range: Optional[tuple] = None
     alch_lambda: float = 0.0
+    # SnapshotHandlers.memory (src/snapshot.rs:34-46): record a snapshot
+    # every this many steps into the device ring (None = off); the frames
+    # come back through MdState.snapshots
+    snapshot_memory: Optional[int] = None
+    snapshot_capacity: int = 256
 
 
 def thermo_dof(system, cfg):
@@ -233,6 +271,9 @@ class MdState:
         self._owned = True
         self._cstruct = c
         self._static = np.asarray(system.get("atom_static", np.zeros(self.n_atoms, bool)), bool).reshape(-1)
+        self._snapshots = []
+        if self.cfg.snapshot_memory:
+            self.enable_snapshots(self.cfg.snapshot_memory, self.cfg.snapshot_capacity, velocities=True)
 
     @classmethod
     def _member(cls, handle, system, cfg):
@@ -396,6 +437,36 @@ class MdState:
         if out:
             out[0]["lost"] = lost.value
         return out
+
+    @property
+    def snapshots(self):
+        """The snapshots recorded so far (MdState.snapshots,
+        src/lib.rs:635-637), oldest first, as Snapshot objects; frames still
+        in the device ring are copied out first."""
+        na, nw = self.n_atoms, self.n_water
+        for d in self.read_snapshots():
+            pos = d["pos"]
+            w = pos[na:].reshape(nw, 3, 3)
+            vel = d.get("vel")
+            e = SnapshotEnergyData(
+                energy_kinetic=d["kinetic"], energy_potential=d["potential"],
+                energy_potential_nonbonded=d["potential"] - d["potential_bonded"],
+                energy_potential_bonded=d["potential_bonded"], temperature=d["temperature"],
+                pressure=d["pressure_bar"], dh_dl=d["dh_dl"] if self.cfg.alch_range else None,
+                volume=d["volume"], density=d["density"])
+            self._snapshots.append(Snapshot(
+                time=d["time_ps"], step=d["step"], atom_posits=pos[:na], water_o_posits=w[:, 0],
+                water_h0_posits=w[:, 1], water_h1_posits=w[:, 2], energy_data=e,
+                cell=(tuple(d["box_lo"]), tuple(d["box_hi"])),
+                atom_velocities=None if vel is None else vel[:na],
+                water_velocities=None if vel is None else vel[na:].reshape(nw, 3, 3)[:, 0],
+                force=d.get("force")))
+        return self._snapshots
+
+    def __str__(self):
+        e = self.energies()
+        return (f"MdState: {self.n_atoms} atoms, {self.n_water} waters, step {e['step']}, "
+                f"T {e['temperature']:.2f} K, PE {e['potential']:.3f} kcal/mol")
 
     def launches_per_step(self, spme=True):
         """Kernels of a step without a list rebuild or periodic task."""

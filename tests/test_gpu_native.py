@@ -204,6 +204,35 @@ def test_union_chunking_bit_identical(gpu_lib):
     b.close()
 
 
+def test_snapshot_memory_handler(gpu_lib):
+    """MdConfig.snapshot_memory (SnapshotHandlers.memory) records a frame
+    every N steps; MdState.snapshots returns them as Snapshot objects with
+    the reference's field names, accumulating across reads."""
+    sysd = mixed()
+    cfg = _cfg(sysd, integ=md.LangevinMiddle(gamma=1.0), seed=3, snapshot_memory=4)
+    st = md.MdState(sysd, cfg)
+    st.step(0.002, 8)
+    s8 = st.state()
+    snaps = st.snapshots
+    assert [x.step for x in snaps] == [4, 8]
+    st.step(0.002, 4)
+    snaps = st.snapshots
+    assert [x.step for x in snaps] == [4, 8, 12]
+    x = snaps[1]
+    nw, na = len(s8["water_pos"]), len(s8["atom_pos"])
+    np.testing.assert_array_equal(x.water_o_posits, s8["water_pos"][:, 0])
+    np.testing.assert_array_equal(x.water_h1_posits, s8["water_pos"][:, 2])
+    np.testing.assert_array_equal(x.water_velocities, s8["water_vel"][:, 0])
+    np.testing.assert_array_equal(x.atom_velocities, s8["atom_vel"])
+    assert x.atom_posits.shape == (na, 3) and x.water_h0_posits.shape == (nw, 3)
+    assert abs(x.time - float(np.float32(0.002)) * 8) < 1e-9
+    e = x.energy_data
+    assert e.temperature > 0 and e.volume > 0 and e.density > 0 and e.dh_dl is None
+    assert abs(e.energy_potential_nonbonded + e.energy_potential_bonded - e.energy_potential) < 1e-6
+    assert "MdState" in str(st)
+    st.close()
+
+
 def test_graph_counters_and_periodic_tasks(gpu_lib):
     """Steps run as captured graphs whose list rebuild and periodic tasks
     are conditional nodes set on the device: the step counter, the rebuild
