@@ -66,7 +66,7 @@ DEFAULT_WORKLOAD = "c3"
 # short-range pair kernels (water-water, water-atom, atom-atom), from an
 # ncu --set full capture of the workload (cold L2, as in the timed loop,
 # which flushes L2 between steps)
-PAIR_DRAM_BYTES = {"c3w": 17306880, "c3": 17521920 + 4850944 + 903168}
+PAIR_DRAM_BYTES = {"c3w": 17306880, "c3": 17521920 + 4856576 + 905984}
 DT = 0.002
 
 
