@@ -440,6 +440,18 @@ def dist_setup(n_gpus):
     return rank, world, local, pg
 
 
+def plain_config(name, cfg, n_water, n_atoms, world):
+    """The config object of a plain-workload JSON line (both arms)."""
+    w = WORKLOADS[name]
+    return {"workload": name, "n_water": n_water, "atoms": 4 * n_water + n_atoms,
+            "peptide_residues": list(w.get("n_res", ())), "nacl_molar": w.get("nacl", 0.0),
+            "box_A": w["box"], "cutoff_A": w["cutoff"], "spme_grid": list(w["grid"]),
+            "spme_interval": cfg.spme_interval, "dt_fs": DT * 1e3,
+            "integrator": w["integrator"], "barostat": w["barostat"],
+            "l2": "256 MiB flush between timed steps",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_ours(args):
     import torch
 
@@ -553,13 +565,7 @@ def run_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded ff19SB peptide / ions / OPC water, equilibrated on device)"
                 if w.get("n_res") else "synthetic (seeded OPC water lattice, equilibrated on device)",
-        "config": {"workload": name, "n_water": st_nw, "atoms": 4 * st_nw + st_na,
-                   "peptide_residues": list(w.get("n_res", ())), "nacl_molar": w.get("nacl", 0.0),
-                   "box_A": w["box"], "cutoff_A": w["cutoff"], "spme_grid": list(w["grid"]),
-                   "spme_interval": cfg.spme_interval, "dt_fs": DT * 1e3,
-                   "integrator": w["integrator"], "barostat": w["barostat"],
-                   "l2": "256 MiB flush between timed steps",
-                   "parallelism": f"replicas x{world}"},
+        "config": plain_config(name, cfg, st_nw, st_na, world),
         "roofline": {"bound": "fp32", "kernel": "short-range pair kernels",
                      "achieved": round(achieved, 3), "peak": round(peak.value, 2), "unit": "TFLOP/s",
                      "frac": round(achieved / peak.value, 4), "traffic": PAIR_DRAM_BYTES.get(name),
@@ -645,14 +651,15 @@ def run_reference(args):
     if WORKLOADS[name].get("kind") in ("batch", "serve"):
         run_reference_members(args, name)
         return
-    sysd, _ = build_system(name, seed=1000)
+    sysd, cfg = build_system(name, seed=1000)
     res = cpu_ref.run_sample(WORKLOADS[name], name, seconds=args.cpu_seconds, steps=args.steps,
                              warmup=args.warmup, sysd=sysd)
     out = {"impl": "reference", "metric": "ns/day", "value": res["value"], "unit": "ns/day",
            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": res.get("steps"),
            "warmup": res.get("warmup"), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": name, "n_water": len(sysd["water_pos"]), "atoms": len(sysd["atom_pos"])},
+           "config": plain_config(name, cfg, len(sysd["water_pos"]), len(sysd["atom_pos"]),
+                                  int(os.environ.get("WORLD_SIZE", "1"))),
            "cpu_baseline": res,
            "e2e": {"value": res["value"], "unit": "ns/day", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
