@@ -26,7 +26,19 @@ struct BatchCtx {
     bool map_missing = false;
     bool map_too_large = false;
     uint32_t launches = 0;                            // batched launches recorded while collecting
+    // the members' FFTs (one cuFFT plan per member) run over these streams
+    // side by side instead of one after another on the batch stream
+    static constexpr int N_FFT = 8;
+    cudaStream_t fft_st[N_FFT] = {};
+    cudaEvent_t fft_ev[N_FFT + 1] = {};
+    int n_fft = 0;
 };
+
+int batch_fft_streams(BatchCtx* b, cudaStream_t** st, cudaEvent_t** ev) {
+    *st = b->fft_st;
+    *ev = b->fft_ev;
+    return b->n_fft;
+}
 
 uint32_t batch_size(const BatchCtx* b) { return (uint32_t)b->views.size(); }
 const SysView& batch_view(const BatchCtx* b, uint32_t i) { return b->views[i]; }
@@ -200,6 +212,10 @@ extern "C" int dyn_batch_destroy(dyn_batch_t b) {
     for (dyn_sys_t m : b->members) dyn_sys_destroy(m);
     if (b->aux) cudaStreamDestroy(b->aux);
     b->br.destroy();
+    for (int i = 0; i < BatchCtx::N_FFT; ++i)
+        if (b->ctx.fft_st[i]) cudaStreamDestroy(b->ctx.fft_st[i]);
+    for (int i = 0; i <= BatchCtx::N_FFT; ++i)
+        if (b->ctx.fft_ev[i]) cudaEventDestroy(b->ctx.fft_ev[i]);
     if (b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return DYN_OK;
@@ -226,6 +242,15 @@ extern "C" int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cf
         if (e != cudaSuccess) { dyn_batch_destroy(b); return dyn::cuda_fail(e, "cudaStreamCreateWithFlags"); }
         const int rc = b->br.create();
         if (rc != DYN_OK) { dyn_batch_destroy(b); return rc; }
+        for (int i = 0; i < BatchCtx::N_FFT; ++i) {
+            const cudaError_t e2 = cudaStreamCreateWithFlags(&b->ctx.fft_st[i], cudaStreamNonBlocking);
+            if (e2 != cudaSuccess) { dyn_batch_destroy(b); return dyn::cuda_fail(e2, "cudaStreamCreateWithFlags"); }
+        }
+        for (int i = 0; i <= BatchCtx::N_FFT; ++i) {
+            const cudaError_t e2 = cudaEventCreateWithFlags(&b->ctx.fft_ev[i], cudaEventDisableTiming);
+            if (e2 != cudaSuccess) { dyn_batch_destroy(b); return dyn::cuda_fail(e2, "cudaEventCreateWithFlags"); }
+        }
+        b->ctx.n_fft = BatchCtx::N_FFT;
     }
     if (n > 0) {
         b->spme_interval = std::max(1u, cfgs[0].spme_interval);

@@ -280,6 +280,9 @@ const SysView& batch_view(const BatchCtx* b, uint32_t i);
 const SysView* batch_dviews(const BatchCtx* b);
 bool batch_collecting(const BatchCtx* b);
 BlockMap batch_map(BatchCtx* b, const std::vector<uint32_t>& blocks);
+// Side streams (and fork/join events: ev[0..n) join, ev[n] forks) over
+// which a batch spreads its members' cuFFT executions; n = 0 for none.
+int batch_fft_streams(BatchCtx* b, cudaStream_t** st, cudaEvent_t** ev);
 
 struct Target {
     const SysView* v = nullptr;   // single system

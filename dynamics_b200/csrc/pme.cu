@@ -452,11 +452,35 @@ void pme_free(SysView& v, cufftHandle plan_f, cufftHandle plan_b) {
     for (int a = 0; a < 3; ++a) cudaFree(v.bmod[a]);
 }
 
+// Runs f(view, stream) for every system; a batch forks onto its FFT side
+// streams (members round-robin) and joins back, so the members' small
+// transforms run side by side.
+template <typename F>
+void each_fft(const Target& t, F f) {
+    if (t.v) { f(*t.v, t.st); return; }
+    if (batch_collecting(t.b)) return;
+    const uint32_t n = batch_size(t.b);
+    cudaStream_t* fs = nullptr;
+    cudaEvent_t* fe = nullptr;
+    const int nf = batch_fft_streams(t.b, &fs, &fe);
+    if (nf <= 0 || n <= 1) {
+        for (uint32_t i = 0; i < n; ++i) f(batch_view(t.b, i), t.st);
+        return;
+    }
+    const int use = (int)std::min<uint32_t>((uint32_t)nf, n);
+    cudaEventRecord(fe[nf], t.st);
+    for (int k = 0; k < use; ++k) cudaStreamWaitEvent(fs[k], fe[nf], 0);
+    for (uint32_t i = 0; i < n; ++i) f(batch_view(t.b, i), fs[i % (uint32_t)use]);
+    for (int k = 0; k < use; ++k) {
+        cudaEventRecord(fe[k], fs[k]);
+        cudaStreamWaitEvent(t.st, fe[k], 0);
+    }
+}
+
 void launch_pme(const Target& t) {
     // one pass, or three with an alchemical molecule in any system (systems
     // without one skip passes 1 and 2)
     const int npass = t.any([](const SysView& v) { return v.alch_on != 0u; }) ? 3 : 1;
-    const cudaStream_t st = t.st;
     for (int pass = 0; pass < npass; ++pass) {
         auto on = [pass](const SysView& v) { return pass == 0 || v.alch_on != 0u; };
         t.launch(k_spread, k_spread_batch,
@@ -464,18 +488,18 @@ void launch_pme(const Target& t) {
                  pass);
         t.launch(k_fix2real, k_fix2real_batch,
                  [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]) : 0; }, GT, 0);
-        // the plans run on the target's stream (a graph branch may differ
-        // from the stream the plans were made on)
-        t.each([st, on](const SysView& v) {
+        // the plans run on the target's stream or a batch's FFT streams (a
+        // graph branch may differ from the stream the plans were made on)
+        each_fft(t, [on](const SysView& v, cudaStream_t s) {
             if (!on(v)) return;
-            cufftSetStream(v.plan_f, st);
+            cufftSetStream(v.plan_f, s);
             cufftExecR2C(v.plan_f, v.qgrid, (cufftComplex*)v.cgrid);
         });
         t.launch(k_convolve, k_convolve_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_PME] : 0; }, GT,
                  0);
-        t.each([st, on](const SysView& v) {
+        each_fft(t, [on](const SysView& v, cudaStream_t s) {
             if (!on(v)) return;
-            cufftSetStream(v.plan_b, st);
+            cufftSetStream(v.plan_b, s);
             cufftExecC2R(v.plan_b, (cufftComplex*)v.cgrid, v.qgrid);
         });
         t.launch(k_gather, k_gather_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_CORR] : 0; }, GT, 0,
