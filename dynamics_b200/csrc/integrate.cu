@@ -490,6 +490,31 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (
     // one warp per region, all regions' partials in flight at once; each
     // region's sum has a fixed order
     __shared__ double rs[NREGION][4];
+    // the thermostat's and barostat's random numbers depend only on the
+    // step and the seed: two otherwise idle warps draw them while the
+    // others reduce the partials
+    __shared__ double rnd[4];  // CSVR normal, CSVR chi^2, exp(-dt/tau_t), barostat normal
+    const bool csvr_on = thermo && v.integrator == DYN_INTEGRATOR_VERLET_VELOCITY &&
+                         v.thermostat == DYN_THERMO_CSVR && v.tau_t > 0.f;
+    const bool baro_on = thermo && v.barostat == DYN_BARO_CRESCALE && v.tau_p > 0.f;
+    {
+        const uint32_t wr = threadIdx.x >> 5;
+        const uint32_t w_csvr = NREGION % (blockDim.x >> 5), w_baro = (NREGION + 1) % (blockDim.x >> 5);
+        const uint64_t step = v.sc->step;
+        if (csvr_on && wr == w_csvr && (threadIdx.x & 31) == 0) {
+            const double dof = (double)(v.thermo_dof > 2 ? v.thermo_dof : 2);
+            const Philox4 r = philox4x32(0u, (uint32_t)step, DYN_STREAM_CSVR, (uint32_t)(step >> 32),
+                                         (uint32_t)v.seed, (uint32_t)(v.seed >> 32));
+            rnd[0] = sqrt(-2.0 * log(uniform24d(r.x[0]))) * cos(2.0 * M_PI * uniform24d(r.x[1]));
+            rnd[1] = 2.0 * gamma_mt(0.5 * (dof - 1.0), step, v.seed);
+            rnd[2] = exp(-(double)dt / (double)v.tau_t);
+        }
+        if (baro_on && wr == w_baro && (threadIdx.x & 31) == 0) {
+            const Philox4 r = philox4x32(0u, (uint32_t)step, DYN_STREAM_BARO, (uint32_t)(step >> 32),
+                                         (uint32_t)v.seed, (uint32_t)(v.seed >> 32));
+            rnd[3] = sqrt(-2.0 * log(uniform24d(r.x[0]))) * cos(2.0 * M_PI * uniform24d(r.x[1]));
+        }
+    }
     {
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
         for (int reg = w; reg < NREGION; reg += (int)(blockDim.x >> 5)) {
@@ -558,15 +583,9 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (
     const double w_intra = x[14];
     // CSVR (src/thermostat.rs:258-304) after the final kick of velocity Verlet
     sc->csvr_lambda = 1.0;
-    if (thermo && v.integrator == DYN_INTEGRATOR_VERLET_VELOCITY && v.thermostat == DYN_THERMO_CSVR &&
-        v.tau_t > 0.f && ker > 1e-20) {
+    if (csvr_on && ker > 1e-20) {
         const double dof = (double)(v.thermo_dof > 2 ? v.thermo_dof : 2);
-        const double cc = exp(-(double)dt / (double)v.tau_t);
-        const uint64_t step = sc->step;
-        const Philox4 r = philox4x32(0u, (uint32_t)step, DYN_STREAM_CSVR, (uint32_t)(step >> 32),
-                                     (uint32_t)v.seed, (uint32_t)(v.seed >> 32));
-        const double rn = sqrt(-2.0 * log(uniform24d(r.x[0]))) * cos(2.0 * M_PI * uniform24d(r.x[1]));
-        const double chi = 2.0 * gamma_mt(0.5 * (dof - 1.0), step, v.seed);
+        const double rn = rnd[0], chi = rnd[1], cc = rnd[2];
         const double ket_target = 0.5 * dof * GAS_CONST_R * (double)v.temperature;
         // the thermostat acts on the rigid-body KE (the degrees of freedom
         // that survive the next rigid drift), not the kicked site velocities
@@ -593,11 +612,8 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (
     sc->temperature = v.thermo_dof ? 2.0 * ker / ((double)v.thermo_dof * GAS_CONST_R) : 0.0;
     // C-rescale (Bernetti & Bussi, J. Chem. Phys. 153, 114107 (2020))
     sc->baro_mu = 1.0;
-    if (thermo && v.barostat == DYN_BARO_CRESCALE && v.tau_p > 0.f) {
-        const uint64_t step = sc->step;
-        const Philox4 r = philox4x32(0u, (uint32_t)step, DYN_STREAM_BARO, (uint32_t)(step >> 32),
-                                     (uint32_t)v.seed, (uint32_t)(v.seed >> 32));
-        const double xi = sqrt(-2.0 * log(uniform24d(r.x[0]))) * cos(2.0 * M_PI * uniform24d(r.x[1]));
+    if (baro_on) {
+        const double xi = rnd[3];
         const double kap = v.kappa, tau = v.tau_p;
         const double det = kap / tau * (sc->pressure - (double)v.p_target) * dt;
         const double sig = sqrt(2.0 * kap * KB_BAR_A3 * (double)v.temperature * dt / (tau * vol));
