@@ -220,6 +220,21 @@ def test_overrides_disable_terms(gpu_lib):
     fp.close()
 
 
+def test_empty_pair_list(gpu_lib):
+    """No installed pairs: every force, the virial and the energy are zero."""
+    sysd = mixed()
+    na, nw = len(sysd["atom_pos"]), len(sysd["water_pos"])
+    fp = gi.ForcesPositsGpu(na, nw, CUTOFF, ALPHA)
+    pn = gi.PerNeighborGpu(fp)
+    pos_dyn, pw = _positions(sysd)
+    ext = (sysd["box_hi"] - sysd["box_lo"]).astype(np.float32)
+    fd, fw, vir, en, dh = gi.force_nonbonded_gpu(fp, pn, pos_dyn, pw, ext, lambda_alch=0.5)
+    assert np.all(fd == 0) and all(np.all(fw[k] == 0) for k in (1, 2, 3, 4))
+    assert vir == 0.0 and en == 0.0 and dh == 0.0
+    assert pn.mark_alchemical(0, na) == 0
+    fp.close()
+
+
 def test_invalid_arguments_raise(gpu_lib):
     from dynamics_b200 import DynError
     with pytest.raises(DynError):
