@@ -171,12 +171,7 @@ DYN_KERNEL(, k_convolve, (), ()) {
     }
 }
 
-// Force on charge q at p from the real-space potential grid, x-planes a of
-// the 4 x 4 x 4 stencil split over the 4 lanes of an aligned lane group
-// (lane & 3 = a) and summed with two butterfly shuffles, so every lane of
-// the group returns the same value.  All 4 lanes must call it.
-__device__ __forceinline__ float3 gather_one4(const SysView& v, float3 p, float q, const BoxDev& b, int a,
-                                              unsigned gmask) {
+__device__ __forceinline__ float3 gather_one(const SysView& v, float3 p, float q, const BoxDev& b) {
     int base[3];
     double wd[3];
     grid_coord(p, b, v.K, base, wd);
@@ -188,31 +183,25 @@ __device__ __forceinline__ float3 gather_one4(const SysView& v, float3 p, float 
     int iz[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) { int z = base[2] - 3 + c; iz[c] = z < 0 ? z + K2 : z; }
-    float txa = tx[0], dxa = dx[0];
-#pragma unroll
-    for (int k = 1; k < 4; ++k) if (a == k) { txa = tx[k]; dxa = dx[k]; }
-    int x = base[0] - 3 + a; x = x < 0 ? x + K0 : x;
     float gx = 0.f, gy = 0.f, gz = 0.f;
 #pragma unroll
-    for (int bb = 0; bb < 4; ++bb) {
-        int y = base[1] - 3 + bb; y = y < 0 ? y + K1 : y;
-        const float* row = v.qgrid + ((size_t)x * K1 + y) * K2;
-        float sz = 0.f, sdz = 0.f;
+    for (int a = 0; a < 4; ++a) {
+        int x = base[0] - 3 + a; x = x < 0 ? x + K0 : x;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const float ph = __ldg(row + iz[c]);
-            sz = fmaf(tz[c], ph, sz);
-            sdz = fmaf(dz[c], ph, sdz);
+        for (int bb = 0; bb < 4; ++bb) {
+            int y = base[1] - 3 + bb; y = y < 0 ? y + K1 : y;
+            const float* row = v.qgrid + ((size_t)x * K1 + y) * K2;
+            float sz = 0.f, sdz = 0.f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float ph = __ldg(row + iz[c]);
+                sz = fmaf(tz[c], ph, sz);
+                sdz = fmaf(dz[c], ph, sdz);
+            }
+            gx = fmaf(dx[a] * ty[bb], sz, gx);
+            gy = fmaf(tx[a] * dy[bb], sz, gy);
+            gz = fmaf(tx[a] * ty[bb], sdz, gz);
         }
-        gx = fmaf(dxa * ty[bb], sz, gx);
-        gy = fmaf(txa * dy[bb], sz, gy);
-        gz = fmaf(txa * ty[bb], sdz, gz);
-    }
-#pragma unroll
-    for (int o = 1; o < 4; o <<= 1) {
-        gx += __shfl_xor_sync(gmask, gx, o);
-        gy += __shfl_xor_sync(gmask, gy, o);
-        gz += __shfl_xor_sync(gmask, gz, o);
     }
     return f3(-q * K0 * b.inv_ext[0] * gx, -q * K1 * b.inv_ext[1] * gy, -q * K2 * b.inv_ext[2] * gz);
 }
@@ -231,28 +220,22 @@ __device__ __forceinline__ double excl_corr(double dx, double dy, double dz, dou
     return -qq * er / r;
 }
 
-// Gather: four lanes per charged site (an atom, or a water's H0, H1 or M),
-// one x-plane of the stencil each, writing the reciprocal cache.  With
-// Ewald corrections on, the intra-water exclusion corrections (H0-H1, H0-M,
-// H1-M) are added here in float64, each site adding its side of its two
-// pairs in pair order and the pair's energy counted by its first site.
+// Gather: one thread per atom, or per water (its H0, H1, M), writing the
+// reciprocal cache.  With Ewald corrections on, the intra-water exclusion
+// corrections (H0-H1, H0-M, H1-M) are added here in float64.
 // Pass 0 stores its (weighted) forces, later passes add theirs.
 DYN_KERNEL(, k_gather, (, int pass), (, pass)) {
     const BoxDev b = *v.box;
     const bool corr = pass == 0 && (v.flags & DYN_FLAG_EWALD_CORRECTIONS);
     const float wt = pass_weight(v, pass);
-    const int lane = threadIdx.x & 31, a = lane & 3;
-    const unsigned gmask = 0xFu << (lane & ~3);
     double e_c = 0.0, w_c = 0.0;
-    const uint32_t total = v.na + (pass == 2 ? 0u : 3u * v.nw_cap);
-    const uint32_t stride = (bk.cnt * blockDim.x) >> 2;
-    for (uint32_t t = (bk.idx * blockDim.x + threadIdx.x) >> 2; t < total; t += stride) {
+    const uint32_t total = v.na + (pass == 2 ? 0u : v.nw_cap);
+    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
         if (t < v.na) {
             if (!pass_has_atom(v, pass, t)) continue;
             const float4 p = v.apos[t];
             float3 f = f3(0.f, 0.f, 0.f);
-            if (p.w != 0.f) f = gather_one4(v, xyz(p), p.w, b, a, gmask) * wt;
-            if (a != 0) continue;
+            if (p.w != 0.f) f = gather_one(v, xyz(p), p.w, b) * wt;
             long long* c = v.arecip + 3 * (size_t)t;
             if (pass == 0) {
                 c[0] = fix_from_float(f.x); c[1] = fix_from_float(f.y); c[2] = fix_from_float(f.z);
@@ -260,39 +243,38 @@ DYN_KERNEL(, k_gather, (, int pass), (, pass)) {
                 c[0] += fix_from_float(f.x); c[1] += fix_from_float(f.y); c[2] += fix_from_float(f.z);
             }
         } else {
-            const uint32_t u = t - v.na;
-            const uint32_t s = u / 3, k = u % 3;
+            const uint32_t s = t - v.na;
             const uint32_t id = v.wid[s];
             if (id == INVALID_ID) continue;
-            const float4 pk = v.wpos[4 * s + 1 + k];
-            const float3 f = gather_one4(v, xyz(pk), pk.w, b, a, gmask) * wt;
-            if (a != 0) continue;
-            double3 fs = make_double3(f.x, f.y, f.z);
+            double3 fs[3];
+            float3 ps[3];
+            for (int k = 0; k < 3; ++k) {
+                const float4 p = v.wpos[4 * s + 1 + k];
+                ps[k] = xyz(p);
+                const float3 f = gather_one(v, ps[k], p.w, b) * wt;
+                fs[k] = make_double3(f.x, f.y, f.z);
+            }
             if (corr) {
-                float3 ps[3];
-                for (int m = 0; m < 3; ++m) ps[m] = xyz(v.wpos[4 * s + 1 + m]);
                 const double q[3] = {OPC_Q_H, OPC_Q_H, OPC_Q_EP};
                 const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
-                for (int j = 0; j < 3; ++j) {
-                    if (pa[j] != (int)k && pb[j] != (int)k) continue;
-                    double3 fc;
-                    const double dx = (double)ps[pa[j]].x - (double)ps[pb[j]].x;
-                    const double dy = (double)ps[pa[j]].y - (double)ps[pb[j]].y;
-                    const double dz = (double)ps[pa[j]].z - (double)ps[pb[j]].z;
-                    const double e = excl_corr(dx, dy, dz, q[pa[j]] * q[pb[j]], (double)v.alpha, &fc);
-                    if (pa[j] == (int)k) {
-                        e_c += e;
-                        w_c += fc.x * dx + fc.y * dy + fc.z * dz;
-                        fs.x += fc.x; fs.y += fc.y; fs.z += fc.z;
-                    } else {
-                        fs.x -= fc.x; fs.y -= fc.y; fs.z -= fc.z;
-                    }
+                for (int k = 0; k < 3; ++k) {
+                    double3 f;
+                    const double dx = (double)ps[pa[k]].x - (double)ps[pb[k]].x;
+                    const double dy = (double)ps[pa[k]].y - (double)ps[pb[k]].y;
+                    const double dz = (double)ps[pa[k]].z - (double)ps[pb[k]].z;
+                    e_c += excl_corr(dx, dy, dz, q[pa[k]] * q[pb[k]], (double)v.alpha, &f);
+                    w_c += f.x * dx + f.y * dy + f.z * dz;
+                    fs[pa[k]].x += f.x; fs[pa[k]].y += f.y; fs[pa[k]].z += f.z;
+                    fs[pb[k]].x -= f.x; fs[pb[k]].y -= f.y; fs[pb[k]].z -= f.z;
                 }
             }
-            long long* c = v.wrecip + 9 * (size_t)id + 3 * k;
-            const long long fx = fix_from_double(fs.x), fy = fix_from_double(fs.y), fz = fix_from_double(fs.z);
-            if (pass == 0) { c[0] = fx; c[1] = fy; c[2] = fz; }
-            else { c[0] += fx; c[1] += fy; c[2] += fz; }
+            long long* c = v.wrecip + 9 * (size_t)id;
+            for (int k = 0; k < 3; ++k) {
+                const long long fx = fix_from_double(fs[k].x), fy = fix_from_double(fs[k].y),
+                                fz = fix_from_double(fs[k].z);
+                if (pass == 0) { c[3 * k + 0] = fx; c[3 * k + 1] = fy; c[3 * k + 2] = fz; }
+                else { c[3 * k + 0] += fx; c[3 * k + 1] += fy; c[3 * k + 2] += fz; }
+            }
         }
     }
     if (pass != 0) return;  // the intra-water corrections belong to pass 0
@@ -427,7 +409,7 @@ namespace dyn {
 int pme_blocks(const SysView& v) {
     return gblocks(v, (uint64_t)v.K[0] * v.K[1] * (v.K[2] / 2 + 1));
 }
-int gather_blocks(const SysView& v) { return gblocks(v, 4 * ((uint64_t)v.na + 3ull * v.nw_cap)); }
+int gather_blocks(const SysView& v) { return gblocks(v, (uint64_t)v.na + v.nw_cap); }
 int corr_blocks(const SysView& v) { return gblocks(v, (uint64_t)v.n14 + v.nexcl); }
 
 int pme_init(SysView& v, cufftHandle* plan_f, cufftHandle* plan_b, cudaStream_t st) {
