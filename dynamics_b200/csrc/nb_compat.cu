@@ -848,13 +848,13 @@ extern "C" int dyn_nb_mark_alch(dyn_nb_t h, uint32_t atom_begin, uint32_t atom_e
     cudaStream_t st = h->stream;
     unsigned long long* d_cnt = nullptr;
     DYN_CUDA(cudaMalloc(&d_cnt, sizeof(unsigned long long)));
-    cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st);
-    if (h->n_pairs) {
+    cudaError_t e = cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st);
+    if (e == cudaSuccess && h->n_pairs) {
         const int blocks = (int)std::min<uint64_t>((h->n_pairs + 255) / 256, 148 * 8);
         mark_alch_kernel<<<blocks, 256, 0, st>>>(h->n_pairs, atom_begin, atom_end, h->d_pidx, d_cnt);
+        e = cudaGetLastError();
     }
     unsigned long long c = 0;
-    cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(&c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(d_cnt);
