@@ -26,6 +26,13 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def clock_csv(rank):
+    """Where the nvidia-smi clock samples of the timed region go: the
+    directory named by DYNB200_OUT, else /tmp."""
+    out = os.environ.get("DYNB200_OUT") or "/tmp"
+    return os.path.join(out, f"clocks_rank{rank}.csv")
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
@@ -160,8 +167,7 @@ def run_batch(args):
     r0 = sum(m.energies()["list_rebuilds"] for m in batch.members)
     ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-                          if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_rank{rank}.csv")
+    clocks = ClockSampler(clock_csv(rank))
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -286,8 +292,7 @@ def run_serve(args):
         done = max(done, r.arrival) + t * r.n_steps
         lat_plain.append(done - r.arrival)
     plain_ns_day = sum(r.n_steps for r in reqs) * DT * 1e-3 / done * 86400.0
-    clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-                          if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_rank{rank}.csv")
+    clocks = ClockSampler(clock_csv(rank))
     srv = serve.Server(budget_bytes=w["budget"], round_steps=100, dt=DT, stream=stream.cuda_stream,
                        keep_states=False)
     if dist:
@@ -473,8 +478,7 @@ def run_ours(args):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
     ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    clocks = ClockSampler(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-                          if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_rank{rank}.csv")
+    clocks = ClockSampler(clock_csv(rank))
     e_before = st.energies()
     if dist:
         dist.barrier()

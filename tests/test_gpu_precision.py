@@ -16,7 +16,8 @@ from .test_gpu_native import FORCE_RTOL, PE_RTOL, _compare, _oracle
 
 pytestmark = pytest.mark.gpu
 
-OUT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpurun_out")
+# records of the precision runs go to the directory named by DYNB200_OUT
+OUT = os.environ.get("DYNB200_OUT", "")
 
 
 def _cfg(**kw):
@@ -26,7 +27,7 @@ def _cfg(**kw):
 
 def _report(name, rec):
     print(name, json.dumps(rec))
-    if os.path.isdir(OUT):
+    if OUT and os.path.isdir(OUT):
         with open(os.path.join(OUT, f"precision_{name}.json"), "w") as f:
             json.dump(rec, f)
 
