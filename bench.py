@@ -179,16 +179,12 @@ def run_batch(args):
             ev1[k].record(stream)
         torch.cuda.synchronize(dev)
     batch.sync()
-    ms = float(np.sum([ev0[k].elapsed_time(ev1[k]) for k in range(args.steps)]))
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(float(np.sum([ev0[k].elapsed_time(ev1[k]) for k in range(args.steps)])), dist, dev)
     rebuilds = sum(m.energies()["list_rebuilds"] for m in batch.members) - r0
     fixed_s, reb_k, per_k = batch.launches(True)
     fixed_n, _, _ = batch.launches(False)
     launches = (fixed_s + fixed_n) / 2.0 * args.steps + reb_k * min(rebuilds, args.steps)
-    value = args.steps * DT * 1e-3 * n_sys * world / (ms * 1e-3) * 86400.0
+    value = aggregate_ns_per_day(args.steps, n_sys, world, ms)
     plain_value = DT * 1e-3 * n_sys / (plain_ms * 1e-3) * 86400.0
     # ---- end to end: every member's positions/velocities in and out per step ----
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory().numpy()
@@ -432,7 +428,11 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
+    """Rank, world size, local rank and the torch.distributed module (None
+    for one process) of a run launched one process per GPU; every rank runs
+    an independent replica, so the only collectives are the barriers and
+    the max over ranks of the timed duration."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -440,9 +440,25 @@ def dist_setup(n_gpus):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return rank, world, local, pg
+
+
+def max_over_ranks(ms, dist, device):
+    """The job's timed duration: the largest of the ranks' durations."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_ns_per_day(steps, systems_per_rank, world, ms):
+    """Simulated ns per day of the whole job: every rank advances
+    systems_per_rank systems by steps steps of DT in the job's ms."""
+    return steps * DT * 1e-3 * systems_per_rank * world / (ms * 1e-3) * 86400.0
 
 
 def plain_config(name, cfg, n_water, n_atoms, world):
@@ -496,14 +512,9 @@ def run_ours(args):
         dist.barrier()
     st.sync()
     ms_steps = [ev0[k].elapsed_time(ev1[k]) for k in range(args.steps)]
-    ms = float(np.sum(ms_steps))
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(float(np.sum(ms_steps)), dist, dev)
     en = st.energies()
-    ns_sim = args.steps * DT * 1e-3 * world
-    value = ns_sim / (ms * 1e-3) * 86400.0
+    value = aggregate_ns_per_day(args.steps, 1, world, ms)
     # ---- stage timing and roofline of the dominant kernel ----
     stages = st.stage_times(DT, 40)
     n_lj, n_c = count_pairs({**sysd, "water_pos": st.state()["water_pos"]}, w["cutoff"])
