@@ -82,3 +82,28 @@ def test_flat_pair_list_agrees_with_site_pairs(lam):
         f0, e0, _, _ = opairs.pair_forces(ref, pos_dyn, pw, ext, cut, alpha, lj_cutoff=cut)
         np.testing.assert_allclose(f, f0, rtol=0, atol=1e-12)
         assert abs(e - e0) < 1e-10
+
+
+def test_coincident_alchemical_pair():
+    """A coincident alchemical pair: the CPU path keeps its soft-core contact
+    energy and dH/dlambda with no force (src/non_bonded.rs:1002-1020), the
+    GPU kernel skips it (r^2 < 1e-16, src/cuda/cuda.cu:448-450)."""
+    from oracle import pairs as opairs
+    pairs = {k: np.array(v) for k, v in {
+        "tgt": [0], "src": [1], "sigma": [3.2], "eps": [0.15], "q_tgt": [0.4], "q_src": [-0.4],
+        "atype_tgt": [0], "wtype_tgt": [0], "atype_src": [0], "wtype_src": [0], "scale_14": [0],
+        "calc_lj": [1], "calc_coulomb": [1], "symmetric": [1], "alch": [1]}.items()}
+    pos = np.array([[5.0, 5.0, 5.0], [5.0, 5.0, 5.0]], np.float32)
+    pw = {s: np.zeros((0, 3)) for s in (1, 2, 3, 4)}
+    lam = 0.8
+    # the pair kernels take lambda as float32 (src/alchemical.rs:83)
+    cs, dcs, ll, dll = method.decoupling_schedule(np.float32(lam))
+    _, e_ref, dv = method.soft_core_lj(np.array([0.0]), np.array([3.2]), np.array([0.15]), ll)
+    f, e, vir, _, dh = opairs.pair_forces(pairs, pos, pw, [20.0] * 3, 10.0, 0.3, lj_cutoff=10.0,
+                                          lambda_alch=lam)
+    assert np.all(f == 0.0) and vir == 0.0
+    assert abs(e - float(e_ref[0])) < 1e-12 and e != 0.0
+    assert abs(dh - float(dv[0]) * dll) < 1e-12
+    f, e, vir, _, dh = opairs.pair_forces(pairs, pos, pw, [20.0] * 3, 10.0, 0.3, gpu_semantics=True,
+                                          lambda_alch=lam)
+    assert np.all(f == 0.0) and e == 0.0 and dh == 0.0
