@@ -300,8 +300,10 @@ def pair_forces(pairs, pos_dyn, pos_w, ext, cutoff, alpha, lj_cutoff=None,
         # the CPU path evaluates a coincident alchemical pair at r = 0
         r_sc = np.where(skip, 0.0, r)
         fs, es, dv = _soft_core_at(r_sc, sig, eps, ll, soft_core_lj)
-        lj_sc = lj_on | (skip & ~np.bool_(gpu_semantics) & pairs["calc_lj"].astype(bool)
-                         & (not lj_disabled))
+        # pairs with LJ soft-core terms: the evaluated ones, plus (CPU path
+        # only) coincident pairs, which keep their contact energy
+        lj_sc = (lj_on & ~skip) | (skip & ~np.bool_(gpu_semantics) & pairs["calc_lj"].astype(bool)
+                                   & (not lj_disabled))
         w14 = np.where(sc, 0.5, 1.0)
         f_lj = np.where(alch, np.where(lj_on, fs * w14, 0.0), f_lj)
         e_lj = np.where(alch, np.where(lj_sc, es * w14, 0.0), e_lj)
