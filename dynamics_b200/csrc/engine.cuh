@@ -30,7 +30,9 @@
 #define UMAX 5            // atoms per constraint unit (a heavy atom and up to 4 H)
 #define LPW 8             // lanes per i-water in the water-water kernel
 #define ACL 8             // atoms per cluster
-#define CH_MIX 16         // list entries per work item of the atom pair kernels
+#ifndef CH_MIX
+#define CH_MIX 8          // list entries per work item of the atom pair kernels (at most 32)
+#endif
 #define INVALID_ID 0xFFFFFFFFu
 #define NACC 16           // accumulator slots
 
