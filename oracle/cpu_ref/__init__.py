@@ -80,6 +80,30 @@ def write_input(path, sysd, workload, steps, warmup, dt=0.002, skin=4.0, seed=0)
                     np.stack([np.asarray(sysd[q], np.float32) for q in par], axis=1).tofile(f)
 
 
+def forces_once(sysd, cutoff, grid):
+    """One force evaluation of the restatement (its first step's forces:
+    O(N^2) list, flat-pair forces, bonded terms, SPME with the 1-4 vacuum
+    correction), for checking it against the float64 oracle.  Returns
+    f_water (nw, 4, 3) [O, H0, H1, M], f_atoms (na, 3), e_recip (self
+    term included) and the pair virial."""
+    binp = build()
+    wl = {"integrator": "verlet", "cutoff": float(cutoff), "grid": list(grid)}
+    with tempfile.TemporaryDirectory() as td:
+        inp, out = os.path.join(td, "in.bin"), os.path.join(td, "f.bin")
+        write_input(inp, sysd, wl, 1, 0)
+        r = subprocess.run([binp, inp, "0", out], capture_output=True, text=True,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1)), timeout=600)
+        if r.returncode != 0:
+            raise RuntimeError(f"cpu_ref failed: {r.stderr[-500:]}")
+        raw = open(out, "rb").read()
+    nw, na = np.frombuffer(raw[:8], np.int32)
+    d = np.frombuffer(raw[8:], np.float64)
+    fw = d[:12 * nw].reshape(nw, 4, 3)
+    fa = d[12 * nw:12 * nw + 3 * na].reshape(na, 3)
+    e_recip, vir = d[12 * nw + 3 * na:]
+    return {"f_water": fw, "f_atoms": fa, "e_recip": float(e_recip), "virial_pairs": float(vir)}
+
+
 def run_sample(workload, name, seconds=20.0, steps=None, warmup=None, seed=1000, sysd=None):
     """Time the restated reference CPU step on this host for about
     ``seconds`` (bounded sample of the workload) with all host threads.

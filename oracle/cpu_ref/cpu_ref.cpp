@@ -27,7 +27,9 @@
 //   * KE (src/thermostat.rs:46-84), pressure (src/barostat.rs:419-431),
 //     linear COM removal every 100 steps (src/com_zero.rs:57-81).
 //
-// Input (binary, little endian): see main().  Output: one JSON line.
+// Input (binary, little endian): see main().  Output: one JSON line; with a
+// third argument, the forces of the first evaluation written to that file
+// instead (no steps are run).
 #include <omp.h>
 
 #include <chrono>
@@ -815,6 +817,31 @@ int main(int argc, char** argv) {
     auto t0 = std::chrono::steady_clock::now();
     build_neighbors(S);
     all_forces(S);
+    if (argc > 3) {
+        // one force evaluation written out, for checking this restatement
+        // against the float64 oracle: int32 n_water, n_atoms; float64 water
+        // site forces [n][4][3] (O, H0, H1, M), atom forces [n_atoms][3];
+        // float64 SPME energy (self term included), pair virial
+        FILE* o = std::fopen(argv[3], "wb");
+        if (!o) { std::fprintf(stderr, "cannot open %s\n", argv[3]); return 2; }
+        const int32_t dims[2] = {n, na};
+        std::fwrite(dims, 4, 2, o);
+        for (const Water& w : S.w) {
+            const V3 fs[4] = {w.fo, w.fh0, w.fh1, w.fm};
+            for (const V3& v : fs) {
+                const double d[3] = {v.x, v.y, v.z};
+                std::fwrite(d, 8, 3, o);
+            }
+        }
+        for (const Atom& a : S.at) {
+            const double d[3] = {a.f.x, a.f.y, a.f.z};
+            std::fwrite(d, 8, 3, o);
+        }
+        const double sc[2] = {S.spme_e, S.virial};
+        std::fwrite(sc, 8, 2, o);
+        std::fclose(o);
+        return 0;
+    }
     kick_calc_accel(S, 0.f);
     auto t_setup = std::chrono::steady_clock::now();
     const double budget = argc > 2 ? std::atof(argv[2]) : 1e30;
