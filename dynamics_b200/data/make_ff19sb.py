@@ -183,4 +183,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/param_data")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_ff19sb.py <reference param_data directory>")
+    main(sys.argv[1])

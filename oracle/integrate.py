@@ -11,7 +11,11 @@ Restates, vectorised over molecules:
   apply_thermostat_csvr   src/thermostat.rs:258-304
   apply_langevin_thermostat  src/thermostat.rs:308-362
   measure_pressure        src/barostat.rs:419-431
+  Barostat::scale_factor, apply_isotropic  src/barostat.rs:329-413
   zero_linear_momentum    src/com_zero.rs:57-81
+and the engine's deliberate deviations from them: the CSVR scale and the
+temperature from the rigid-body kinetic energy (rigid_kinetic_energy), the
+barostat driven by the molecular virial (intramolecular_virial).
 Noise comes from oracle.philox (the engine's stream) instead of the
 reference's unseeded ThreadRng.
 """
@@ -396,3 +400,153 @@ def drift(state, dt, lo, ext):
     if len(state["water_vel"]):
         p, v, m, _ = rigid_water_drift(state["water_pos"], state["water_vel"], dt, lo, ext)
         state["water_pos"], state["water_vel"], state["water_m"] = p, v, m
+
+
+def _rigid_frames(wpos, wvel, ext):
+    """COM position and velocity, angular momentum L, inertia tensor and
+    angular velocity omega = I^-1 L of each water (the quantities
+    integrate_rigid_water computes first, src/solvent/opc_settle.rs:107-150),
+    with the H sites min-imaged next to O."""
+    mo, mh = float(opc.O_MASS), float(opc.H_MASS)
+    mt = float(opc.MASS_WATER_MOL)
+    o = wpos[:, 0]
+    h0 = o + min_image(wpos[:, 1] - o, ext)
+    h1 = o + min_image(wpos[:, 2] - o, ext)
+    vo, vh0, vh1 = wvel[:, 0], wvel[:, 1], wvel[:, 2]
+    r_com = (o * mo + h0 * mh + h1 * mh) / mt
+    v_com = (vo * mo + vh0 * mh + vh1 * mh) / mt
+    rs = (o - r_com, h0 - r_com, h1 - r_com)
+    us = (vo - v_com, vh0 - v_com, vh1 - v_com)
+    ms = (mo, mh, mh)
+    L = sum(np.cross(r, u) * m for r, u, m in zip(rs, us, ms))
+    t = [0.0] * 6
+    for r, m in zip(rs, ms):
+        x, y, z = r[:, 0], r[:, 1], r[:, 2]
+        r2 = x * x + y * y + z * z
+        for k, val in enumerate((m * (r2 - x * x), m * (r2 - y * y), m * (r2 - z * z),
+                                 -m * x * y, -m * x * z, -m * y * z)):
+            t[k] = t[k] + val
+    omega = solve_sym3(*t, L)
+    return r_com, v_com, L, omega
+
+
+def rigid_kinetic_energy(state, ext):
+    """Kinetic energy that survives the next rigid drift, kcal/mol: per water
+    M v_com^2 / 2 + omega . L / 2, plus the solute atoms' KE.  The engine's
+    thermostat and temperature use it instead of the site KE of
+    measure_kinetic_energy (src/thermostat.rs:46-64), whose constrained
+    components the rigid drift removes."""
+    ke = 0.0
+    dyn = ~state["atom_static"]
+    if len(state["atom_vel"]):
+        v = state["atom_vel"][dyn]
+        ke += float(np.sum(state["atom_mass"][dyn] * np.sum(v * v, axis=1)))
+    if len(state["water_vel"]):
+        _, vc, L, w = _rigid_frames(state["water_pos"], state["water_vel"], ext)
+        ke += float(np.sum(float(opc.MASS_WATER_MOL) * np.sum(vc * vc, axis=1) + np.sum(w * L, axis=1)))
+    return ke * 0.5 / float(opc.KCAL_TO_NATIVE)
+
+
+def csvr_lambda(ke, dt, tau, temp, dof, step, seed):
+    """Velocity scale of the CSVR update (Bussi, Donadio, Parrinello, J. Chem.
+    Phys. 126, 014101 (2007); apply_thermostat_csvr, src/thermostat.rs:258-304)
+    for kinetic energy ``ke`` (kcal/mol), with the engine's Philox draws."""
+    dof = float(max(dof, 2))
+    if tau <= 0.0 or ke <= 1e-20:
+        return 1.0
+    c = np.exp(-dt / tau)
+    r = philox.csvr_normal(step, seed)
+    chi = 2.0 * philox.gamma_marsaglia_tsang(0.5 * (dof - 1.0), step, seed)
+    ke_t = 0.5 * dof * opc.GAS_CONST_R * temp
+    kp = ke * c + ke_t * (1.0 - c) * ((chi + r * r) / dof) + 2.0 * r * np.sqrt(c * (1.0 - c) * ke * ke_t / dof)
+    return float(np.sqrt(max(kp, 1e-20) / ke))
+
+
+def intramolecular_virial(state, f_water, ext):
+    """sum over waters and their sites of (r_site - R_com) . F_site (kcal/mol),
+    sites O, H0, H1, M; subtracted from the site virial it gives the
+    molecular virial of rigid molecules."""
+    if len(state["water_vel"]) == 0:
+        return 0.0
+    wp = state["water_pos"]
+    o = wp[:, 0]
+    r_com, _, _, _ = _rigid_frames(wp, state["water_vel"], ext)
+    sites = [o, o + min_image(wp[:, 1] - o, ext), o + min_image(wp[:, 2] - o, ext),
+             o + min_image(state["water_m"] - o, ext)]
+    return float(sum(np.sum((s - r_com) * f_water[:, k], axis=1).sum() for k, s in enumerate(sites)))
+
+
+def crescale_mu(pressure, dt, temp, p_target, tau, kappa, volume, step, seed):
+    """Linear scale factor of the stochastic cell rescaling barostat
+    (Bernetti & Bussi, J. Chem. Phys. 153, 114107 (2020); scale_factor,
+    src/barostat.rs:329-354): d ln V = kappa / tau (P - P0) dt +
+    sqrt(2 kappa kB T dt / (tau V)) xi, clamped to +-0.1, mu = e^{d ln V / 3}."""
+    xi = philox.csvr_normal(step, seed, stream=philox.STREAM_BARO)
+    det = kappa / tau * (pressure - p_target) * dt
+    sig = np.sqrt(2.0 * kappa * opc.KB_BAR_A3_PER_K * temp * dt / (tau * volume))
+    dl = min(max(det + sig * xi, -0.1), 0.1)
+    return float(np.exp(dl / 3.0))
+
+
+def crescale_apply(state, mu, lam, lo, ext):
+    """apply_isotropic (src/barostat.rs:357-413, which the reference leaves
+    disabled at :367-368) as the engine applies it together with the CSVR
+    scale: water molecules moved with their COM (geometry kept), solute
+    atoms scaled about the box centre, velocities scaled by lam / mu, the box
+    scaled about its centre.  Returns the new (lo, ext)."""
+    cen = lo + 0.5 * ext
+    vs = lam / mu
+    state["water_vel"] = state["water_vel"] * vs
+    dyn = ~state["atom_static"]
+    if len(state["atom_vel"]):
+        state["atom_vel"] = np.where(dyn[:, None], state["atom_vel"] * vs, state["atom_vel"])
+    if mu == 1.0:
+        return lo, ext
+    if len(state["water_vel"]):
+        r_com, _, _, _ = _rigid_frames(state["water_pos"], state["water_vel"], ext)
+        sh = (r_com - cen) * (mu - 1.0)
+        state["water_pos"] = state["water_pos"] + sh[:, None, :]
+        if "water_m" in state:
+            state["water_m"] = state["water_m"] + sh
+    if len(state["atom_vel"]):
+        state["atom_pos"] = np.where(dyn[:, None], cen + (state["atom_pos"] - cen) * mu, state["atom_pos"])
+    e = ext * mu
+    return cen - 0.5 * e, e
+
+
+def step_langevin_middle(state, forces_fn, dt, gamma, temp, step, seed, lo, ext):
+    """One LangevinMiddle step (src/integrate.rs:100-212): kick dt/2 and
+    drift dt/2, the OU step on every site velocity, drift dt/2, forces,
+    kick dt/2.  ``forces_fn(state)`` returns the oracle force dict."""
+    kick_and_drift(state, dt / 2, dt / 2, lo, ext)
+    langevin_ou(state, dt, gamma, temp, step, seed)
+    drift(state, dt / 2, lo, ext)
+    f = forces_fn(state)
+    kick_and_calc_accel(state, f, dt / 2)
+    return f
+
+
+def step_verlet_csvr(state, forces_fn, dt, tau, temp, dof, step, seed, lo, ext, baro=None):
+    """One VerletVelocity step with CSVR (src/integrate.rs:213-317): kick
+    dt/2 and drift dt, forces, kick dt/2, the CSVR scale from the rigid-body
+    KE, and with ``baro`` = dict(p_target, tau, kappa) the C-rescale step
+    driven by the molecular pressure.  Returns (forces, lam, mu, pressure,
+    lo, ext)."""
+    state["virial_constraints"] = 0.0
+    kick_and_drift(state, dt / 2, dt, lo, ext)
+    # bond-to-H constraint virial (native units); the rigid waters enter
+    # through the molecular virial instead
+    vir_c = state["virial_constraints"] / float(opc.KCAL_TO_NATIVE)
+    f = forces_fn(state)
+    kick_and_calc_accel(state, f, dt / 2)
+    ke_r = rigid_kinetic_energy(state, ext)
+    lam = csvr_lambda(ke_r, dt, tau, temp, dof, step, seed) if tau else 1.0
+    ket = kinetic_energy_translational(state) * lam * lam
+    vol = float(np.prod(ext))
+    w = f["virial"] + vir_c - intramolecular_virial(state, f["f_water"], ext)
+    p = pressure_bar(ket, w, vol)
+    mu = 1.0
+    if baro is not None:
+        mu = crescale_mu(p, dt, temp, baro["p_target"], baro["tau"], baro["kappa"], vol, step, seed)
+    lo, ext = crescale_apply(state, mu, lam, lo, ext)
+    return f, lam, mu, p, lo, ext

@@ -29,10 +29,10 @@ FORCE_RTOL = 1e-5   # per-atom force relative RMS vs float64
 SCALAR_RTOL = 1e-5  # virial / energy relative error vs float64
 
 
-def _build(sysd, lj_cutoff=0.0):
+def _build(sysd, lj_cutoff=0.0, cutoff=CUTOFF):
     na = len(sysd["atom_pos"])
     nw = len(sysd["water_pos"])
-    fp = gi.ForcesPositsGpu(na, nw, CUTOFF, ALPHA, lj_cutoff)
+    fp = gi.ForcesPositsGpu(na, nw, cutoff, synth.ewald_alpha(cutoff), lj_cutoff)
     pn = gi.PerNeighborGpu.build(
         fp, sysd["atom_pos"], sysd["water_pos"][:, 0] if nw else None, sysd["atom_q"],
         sysd["atom_sigma"], sysd["atom_eps"], sysd["box_lo"], sysd["box_hi"], SKIN,
@@ -40,8 +40,8 @@ def _build(sysd, lj_cutoff=0.0):
     return fp, pn
 
 
-def _oracle_pairs(sysd):
-    lists = opairs.build_all_neighbors(sysd, SKIN, CUTOFF)
+def _oracle_pairs(sysd, cutoff=CUTOFF):
+    lists = opairs.build_all_neighbors(sysd, SKIN, cutoff)
     return opairs.setup_pairs(sysd, lists)
 
 
@@ -50,12 +50,10 @@ def _positions(sysd):
     return pos_dyn, pw
 
 
-@pytest.mark.parametrize("make", [water_only, mixed])
-def test_pair_set_bit_exact(gpu_lib, make):
-    sysd = make()
-    fp, pn = _build(sysd)
+def _check_pair_set(sysd, cutoff=CUTOFF):
+    fp, pn = _build(sysd, cutoff=cutoff)
     got = pn.get_pairs()
-    ref = _oracle_pairs(sysd)
+    ref = _oracle_pairs(sysd, cutoff)
     assert pn.n_pairs == len(ref["tgt"])
     np.testing.assert_array_equal(got["tgt"], ref["tgt"])
     np.testing.assert_array_equal(got["src"], ref["src"])
@@ -71,6 +69,25 @@ def test_pair_set_bit_exact(gpu_lib, make):
     qq = np.where(ref["calc_coulomb"] == 1, ref["q_tgt"] * ref["q_src"], 0).astype(np.float32)
     np.testing.assert_array_equal(got["qq"], qq)
     fp.close()
+
+
+@pytest.mark.parametrize("make", [water_only, mixed])
+def test_pair_set_bit_exact(gpu_lib, make):
+    _check_pair_set(make())
+
+
+def _c2_water_box():
+    return synth.water_box(7800, 62.0, seed=2)
+
+
+@pytest.mark.parametrize("make,cutoff", [(synth.config1, 10.0), (_c2_water_box, 9.0)], ids=["config1", "c2_size"])
+def test_pair_set_bit_exact_baseline_sizes(gpu_lib, make, cutoff):
+    """The reference's own configurations.  Config 1's 24.8 A box breaks the
+    reference's L > 2 (cutoff + skin) advice (src/lib.rs:560-561): the 14 A
+    list radius exceeds half the box, so membership rests on the min-image
+    rounding alone (0.89 M flat pairs).  A config-2-size water box (7,800
+    waters, 62 A, cutoff 9) has 14.8 M flat pairs."""
+    _check_pair_set(make(), cutoff)
 
 
 def test_pair_set_boundary_cases(gpu_lib):
