@@ -63,7 +63,7 @@ class Config(C.Structure):
         ("recenter_interval", C.c_uint32), ("energy_interval", C.c_uint32),
         ("flags", C.c_uint32), ("thermo_dof", C.c_uint32), ("seed", C.c_uint64),
         ("ww_union_chunk", C.c_uint32), ("lincs_order", C.c_uint32), ("lincs_iter", C.c_uint32),
-        ("reserved0", C.c_uint32),
+        ("prune_buffer", C.c_float),
         ("alch_begin", C.c_uint32), ("alch_end", C.c_uint32), ("alch_lambda", C.c_float),
         ("reserved1", C.c_uint32),
     ]
@@ -94,7 +94,8 @@ class Energies(C.Structure):
         "virial_bonded", "virial_constraints", "pressure_bar", "temperature")] + [
         ("box", C.c_double * 3), ("step", C.c_uint64), ("list_rebuilds", C.c_uint64),
         ("pairs_in_list", C.c_uint64), ("kinetic_rigid", C.c_double),
-        ("pressure_atomic_bar", C.c_double), ("list_union_max", C.c_uint64), ("dh_dl", C.c_double)]
+        ("pressure_atomic_bar", C.c_double), ("list_union_max", C.c_uint64), ("dh_dl", C.c_double),
+        ("list_prunes", C.c_uint64)]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_ if n != "box"}
@@ -167,6 +168,7 @@ _SIGS = {
     "dyn_sys_set_static": ([_P, _P, C.c_uint32], C.c_int),
     "dyn_sys_set_lambda": ([_P, C.c_float], C.c_int),
     "dyn_sys_snapshots_read": ([_P, C.c_uint32, _P, _P, _P, _P, _P, _P], C.c_int),
+    "dyn_sys_list_pairs": ([_P, C.c_uint32, _P, C.c_uint64, _P], C.c_int),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libdynb200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["errors.cu", "nb_compat.cu", "nblist.cu", "pair.cu", "pme.cu", "integrate.cu",
-           "bonded.cu", "system.cu", "batch.cu", "nb_static.cu", "minimize.cu"]
+           "bonded.cu", "system.cu", "batch.cu", "nb_static.cu", "minimize.cu", "list_export.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -38,18 +38,31 @@ def _stale():
 
 
 def build(force=False, verbose=False):
-    """Compile every source into dynamics_b200/libdynb200.so."""
+    """Compile every source into dynamics_b200/libdynb200.so: one object per
+    source, compiled in parallel under _build/, then linked."""
     if not force and not _stale():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
     lib64 = os.path.join(cuda_home(), "lib64")
-    cmd = [nvcc(), "-shared", "-std=c++17", "-O3", "-lineinfo", "-fmad=false", *ARCH,
-           "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=default",
-           "-cudart", "static",
-           "-I" + INCLUDE,
-           *[os.path.join(CSRC, s) for s in SOURCES],
-           "-L" + lib64, "-lcufft",
-           "-Xlinker", "-rpath=" + lib64,
-           "-o", LIB + ".tmp"]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", *ARCH,
+             "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=default", "-I" + INCLUDE]
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc(), "-c", *flags, os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}{r.stderr}")
+        return obj
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    cmd = [nvcc(), "-shared", *ARCH, "-cudart", "static", *objs,
+           "-L" + lib64, "-lcufft", "-Xlinker", "-rpath=" + lib64, "-o", LIB + ".tmp"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True, cwd=CSRC)

@@ -78,6 +78,8 @@ struct dyn_batch_s {
     cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
     float graph_dt[4] = {0, 0, 0, 0};
     uint64_t host_step = 0;
+    cudaEvent_t window_ev = nullptr;  // bounds the steps one dyn_batch_step call queues
+    bool window_armed = false;
     uint32_t spme_interval = 1, energy_interval = 1;
     bool fixed_intervals = false;   // set by the first member
     uint32_t views_cap = 0;         // members the device view arrays hold
@@ -109,7 +111,8 @@ int upload_maps(dyn_batch_s* b) {
 // src/integrate.rs:100-473).  With cond, the rebuild and the periodic tasks
 // go under IF nodes of the capture in progress.
 int enqueue_batch_step(dyn_batch_s* b, float dt, bool spme, bool energy, bool cond,
-                       cudaGraphConditionalHandle c_rebuild, cudaGraphConditionalHandle c_periodic) {
+                       cudaGraphConditionalHandle c_rebuild, cudaGraphConditionalHandle c_prune,
+                       cudaGraphConditionalHandle c_periodic) {
     const Target T{nullptr, &b->ctx, b->stream}, TA{nullptr, &b->ctx, b->aux};
     const Target S0{nullptr, &b->ctx, b->br.side[0]}, S1{nullptr, &b->ctx, b->br.side[1]};
     cudaGraph_t body = nullptr;
@@ -119,6 +122,9 @@ int enqueue_batch_step(dyn_batch_s* b, float dt, bool spme, bool energy, bool co
     dyn::launch_displacement_check(T);
     if (cond && (rc = dyn::begin_if_body(b->stream, b->aux, c_rebuild, &body)) != DYN_OK) return rc;
     dyn::launch_rebuild(cond ? TA : T, false);
+    if (cond && (rc = dyn::end_if_body(b->aux)) != DYN_OK) return rc;
+    if (cond && (rc = dyn::begin_if_body(b->stream, b->aux, c_prune, &body)) != DYN_OK) return rc;
+    dyn::launch_prune(cond ? TA : T, false);
     if (cond && (rc = dyn::end_if_body(b->aux)) != DYN_OK) return rc;
     dyn::launch_gather_atoms(T);
     if ((rc = dyn::enqueue_forces(T, S0, S1, b->br, cond, spme, energy)) != DYN_OK) return rc;
@@ -133,7 +139,7 @@ int enqueue_batch_step(dyn_batch_s* b, float dt, bool spme, bool energy, bool co
 // Records the block maps of a step variant (no launches) and uploads them.
 int collect_maps(dyn_batch_s* b, float dt, bool spme, bool energy) {
     b->ctx.collecting = true;
-    const int rc = enqueue_batch_step(b, dt, spme, energy, false, 0, 0);
+    const int rc = enqueue_batch_step(b, dt, spme, energy, false, 0, 0, 0);
     b->ctx.collecting = false;
     if (rc) return rc;
     return upload_maps(b);
@@ -160,16 +166,17 @@ int capture_batch_step(dyn_batch_s* b, int g, float dt, bool spme, bool energy, 
     b->ctx.d_views = b->d_views[g];
     b->ctx.map_missing = false;
     DYN_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    cudaGraphConditionalHandle hr = 0, hp = 0;
+    cudaGraphConditionalHandle hr = 0, hq = 0, hp = 0;
     {
         cudaStreamCaptureStatus cs;
         cudaGraph_t cg = nullptr;
         cudaError_t e = cudaStreamGetCaptureInfo(b->stream, &cs, nullptr, &cg, nullptr, nullptr);
         if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hr, cg, 0, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hq, cg, 0, cudaGraphCondAssignDefault);
         if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hp, cg, 0, cudaGraphCondAssignDefault);
         if (e != cudaSuccess) rc = dyn::cuda_fail(e, "cudaGraphConditionalHandleCreate");
     }
-    if (rc == DYN_OK) rc = enqueue_batch_step(b, dt, spme, energy, true, hr, hp);
+    if (rc == DYN_OK) rc = enqueue_batch_step(b, dt, spme, energy, true, hr, hq, hp);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
     if (rc == DYN_OK && e != cudaSuccess) rc = dyn::cuda_fail(e, "cudaStreamEndCapture");
@@ -186,6 +193,7 @@ int capture_batch_step(dyn_batch_s* b, int g, float dt, bool spme, bool energy, 
     // graph's conditional handles
     for (SysView& v : b->ctx.views) {
         v.cond_rebuild = hr;
+        v.cond_prune = hq;
         v.cond_periodic = hp;
         v.use_cond = 1;
     }
@@ -211,6 +219,7 @@ extern "C" int dyn_batch_destroy(dyn_batch_t b) {
     for (void* p : b->map_allocs) cudaFree(p);
     for (dyn_sys_t m : b->members) dyn_sys_destroy(m);
     if (b->aux) cudaStreamDestroy(b->aux);
+    if (b->window_ev) cudaEventDestroy(b->window_ev);
     b->br.destroy();
     for (int i = 0; i < BatchCtx::N_FFT; ++i)
         if (b->ctx.fft_st[i]) cudaStreamDestroy(b->ctx.fft_st[i]);
@@ -294,7 +303,15 @@ extern "C" int dyn_batch_step(dyn_batch_t b, uint32_t n_steps, float dt) {
         DYN_CUDA(cudaGraphLaunch(b->graph[g], b->stream));
         b->host_step += 1;
         for (dyn_sys_t m : b->members) m->host_step += 1;
+        // at most about 2 x 512 steps queued at a time
+        if ((i + 1) % 512 == 0 && i + 1 < n_steps) {
+            if (!b->window_ev) DYN_CUDA(cudaEventCreateWithFlags(&b->window_ev, cudaEventDisableTiming));
+            if (b->window_armed) DYN_CUDA(cudaEventSynchronize(b->window_ev));
+            DYN_CUDA(cudaEventRecord(b->window_ev, b->stream));
+            b->window_armed = true;
+        }
     }
+    b->window_armed = false;
     return DYN_OK;
 }
 
@@ -337,7 +354,7 @@ extern "C" int dyn_batch_launches(dyn_batch_t b, int spme, uint32_t* fixed, uint
         b->ctx.collecting = false;
         return b->ctx.launches;
     };
-    const uint32_t all = count([&] { enqueue_batch_step(b, 0.002f, spme != 0, true, false, 0, 0); });
+    const uint32_t all = count([&] { enqueue_batch_step(b, 0.002f, spme != 0, true, false, 0, 0, 0); });
     *rebuild = count([&] { dyn::launch_rebuild(T, false); });
     *periodic = count([&] { dyn::launch_periodic(T); });
     *fixed = all - *rebuild - *periodic;

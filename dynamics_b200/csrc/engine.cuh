@@ -26,7 +26,7 @@
 
 #define WCL 8             // waters per cluster
 #define GRPW 32           // waters per i-group of the water-water kernel (4 clusters)
-#define NPOLY_G 12        // coefficients of the screened-Coulomb force polynomial
+#define NPOLY_G 14        // coefficients of the screened-Coulomb force polynomial (14: the virial within 1e-5 of float64)
 #define UMAX 5            // atoms per constraint unit (a heavy atom and up to 4 H)
 #define LPW 8             // lanes per i-water in the water-water kernel
 #define ACL 8             // atoms per cluster
@@ -34,6 +34,7 @@
 #define CH_MIX 8          // list entries per work item of the atom pair kernels (at most 32)
 #endif
 #define INVALID_ID 0xFFFFFFFFu
+#define WW_JFIX_SHIFT 16  // j-side water-water sums: int32 fixed point, 2^-16 kcal/mol/A
 #define NACC 16           // accumulator slots
 
 enum Acc {
@@ -67,7 +68,7 @@ struct Scalars {
     unsigned int ctr_scale;       // blocks done in k_scale (last one scales the box)
     unsigned int union_max;       // largest group union of the last rebuild
     unsigned int a_sparse_base;   // first slot of the single-atom clusters
-    unsigned int n_ws_items;      // work items of the water-atom pair kernel
+    unsigned int aun_max;         // largest water-group atom union of the last rebuild
     unsigned int n_ss_items;      // work items of the atom-atom pair kernel
     double time_ps;               // simulated time (sum of the steps' dt)
     unsigned long long snap_count;  // snapshot frames recorded
@@ -81,6 +82,11 @@ struct Scalars {
     float min_alpha, min_alpha_try, min_fmax, min_step;
     unsigned int min_fmax_bits, min_ctr;
     unsigned int min_accepted, min_trials, min_done, min_action;
+    // pruned water-water lists: set by the displacement check (or with a
+    // rebuild), cleared when the prune has run
+    unsigned int need_prune;
+    unsigned int max_dprune_bits;  // float bits, as max_disp2_bits
+    unsigned long long prunes;
 };
 
 // Partial-sum regions (each kernel family writes 4 doubles per block).
@@ -130,14 +136,22 @@ struct SysView {
     uint32_t* wcol; uint32_t* acol;             // column of each water / atom
     // cluster bounding boxes (center xyz, half extent xyz)
     float4* wbb_c; float4* wbb_h; float4* abb_c; float4* abb_h;
-    // cluster lists (fixed capacity per i cluster): water cluster -> atom
-    // clusters, atom cluster -> atom clusters (cj >= ci) with masks; work
-    // items {i cluster, first entry} of CH_MIX list entries, in i order
-    uint32_t cap_ws, cap_ss;
-    uint32_t* ws_n; uint32_t* ws_j;
+    // atom-atom cluster lists (fixed capacity per i cluster): atom cluster
+    // -> atom clusters (cj >= ci) with interaction masks; work items
+    // {i cluster, first entry} of CH_MIX list entries, in i order
+    uint32_t cap_ss;
     uint32_t* ss_n; uint32_t* ss_j; unsigned long long* ss_mask;
-    uint2* ws_item; uint2* ss_item;
-    uint32_t ws_item_cap, ss_item_cap;
+    uint2* ss_item;
+    uint32_t ss_item_cap;
+    // water-atom: per 32-water group the atom clusters near the group box
+    // (atile), the union of the atoms its waters reach (cluster-slot
+    // indices, staged in shared memory by the pair kernel, aun_chunk at a
+    // time), and per water a list of indices into that union
+    uint32_t cap_atile, cap_aun, cap_wal, aun_chunk;
+    uint32_t* atile_n; uint32_t* atile_j;    // [ngrp_cap], [ngrp_cap*cap_atile]
+    uint32_t* aun_n; uint32_t* aun_idx;      // [ngrp_cap], [ngrp_cap*cap_aun]
+    uint16_t* acand_loc;                     // [ngrp_cap*cap_atile*ACL] rebuild scratch
+    uint32_t* wal_n; uint16_t* wal;          // [nw_cap], [nw_cap*cap_wal]
     // water-water: per 32-water i-group the candidate j-clusters (tile_j),
     // the union of the waters its members need, stored as runs of
     // consecutive slots (staged in shared memory by bulk copies), and per
@@ -150,6 +164,23 @@ struct SysView {
     uint2* grp_run;                          // [ngrp_cap*cap_run] (slot, union offset)
     uint16_t* cand_loc;                      // [ngrp_cap*cap_tile*8] rebuild scratch
     uint32_t* wnb_n; uint16_t* wnb;          // [nw_cap], [nw_cap*cap_nb]
+    // the lists the water-water kernel walks: wnb pruned to molecule pairs
+    // within r_in (k_ww_prune), re-pruned when a water has moved half of
+    // r_in's buffer since the last prune (O positions then: wprune)
+    uint32_t* winb_n; uint16_t* winb;        // [nw_cap], [nw_cap*cap_nb]
+    float4* wprune;                          // [nw_cap]
+    uint32_t* grp_uslot;                     // [ngrp_cap*cap_union] union index -> slot
+    // The molecule lists are half lists (each water pair once, listed by
+    // the lower slot).  The j-side forces a group's CTA computes are summed
+    // in shared memory as int32 fixed point (2^-16 kcal/mol/A) per union
+    // water and written to jbuf entry g * cap_union + u; every water then
+    // gathers its entries through the reverse index rev (rev_n per slot,
+    // entries are jbuf entry numbers).  j-contributions too large for the
+    // int32 sums go to wjbig (int64, 2^-32) by atomics.
+    int* jbuf;                               // [ngrp_cap * cap_union * 12]
+    uint32_t* rev_n; uint32_t* rev;          // [nw_cap], [nw_cap * rev_cap]
+    uint32_t rev_cap;
+    long long* wjbig;                        // [nw_cap * 12]
     // 1-4 pairs, exclusions (pairs), bonded terms, constraints
     uint32_t n14; uint2* p14; float4* p14_par;     // sigma, eps, qq, unused
     uint32_t nexcl; uint2* excl; float* excl_qq;
@@ -176,6 +207,7 @@ struct SysView {
     // parameters
     float rc, rc2, ljc2, alpha, buffer;
     float r_ww, r_ws, r_ss;     // list radii
+    float r_in, prune_buf;      // pruned water-water radius and its buffer
     uint32_t flags;
     uint64_t seed;
     float temperature, gamma, tau_t, p_target, tau_p, kappa;
@@ -203,7 +235,7 @@ struct SysView {
     // IF-node handles of the captured step graph: the displacement check
     // sets cond_rebuild, the step finalisation sets cond_periodic; only
     // kernels captured for a graph (use_cond != 0) set them
-    cudaGraphConditionalHandle cond_rebuild, cond_periodic;
+    cudaGraphConditionalHandle cond_rebuild, cond_periodic, cond_prune;
     uint32_t use_cond;
     uint32_t nb[NREGION];   // blocks each region's kernel is launched with
     int plan_f, plan_b;     // cuFFT plans (host-side handles, used by launch code only)
@@ -354,6 +386,9 @@ namespace dyn {
 // nblist.cu
 void launch_displacement_check(const Target& t);
 void launch_rebuild(const Target& t, bool force);
+// prunes the water-water lists if the displacement check (or a rebuild) asked
+// for it, or with force
+void launch_prune(const Target& t, bool force);
 void launch_gather_atoms(const Target& t);
 
 // pair.cu
@@ -367,8 +402,11 @@ void launch_pairs_ws(const Target& t, bool energy);
 void launch_pair14(const Target& t, bool energy);
 int pair_ww_setup(const SysView& v);
 int ww_tile_blocks(const SysView& v);
+size_t ww_tile_smem(const SysView& v);
+int ww_gather_blocks(const SysView& v);
 int pair_blocks_ss(const SysView& v);
 int pair_blocks_ws(const SysView& v);
+size_t ws_smem(const SysView& v);
 int pair14_blocks(const SysView& v);
 
 // pme.cu

@@ -558,11 +558,11 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (
                           ws[2] + ss[2], p14[0], p14[2], bo[0], bo[2], kw[0] + ka[0],
                           kw[1] + ka[1], co[0], kw[2] + ka[2], kw[3], 0};
     Scalars* sc = v.sc;
-    // the water-water list counts every pair from both sides, the atom
-    // lists once
+    // every list (water-water half lists, atom cluster pairs) counts each
+    // pair once
     if (ENERGY) {
-        sc->acc[ACC_E_LJ_WW] = 0.5 * x[0];
-        sc->acc[ACC_E_COUL_WW] = 0.5 * x[1];
+        sc->acc[ACC_E_LJ_WW] = x[0];
+        sc->acc[ACC_E_COUL_WW] = x[1];
         sc->acc[ACC_E_LJ_S] = x[3];
         sc->acc[ACC_E_COUL_S] = x[4];
         sc->acc[ACC_E_14] = x[6];
@@ -570,7 +570,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_finalize, (, float dt, bool thermo), (
         // alchemical dH/dlambda: short-range cross pairs + SPME cross term
         sc->dh_dl = ws[3] + ss[3] + sc->recip_dh_cache;
     }
-    sc->acc[ACC_VIR_SHORT] = 0.5 * x[2] + x[5] + x[7];
+    sc->acc[ACC_VIR_SHORT] = x[2] + x[5] + x[7];
     sc->acc[ACC_VIR_14] = x[7];
     sc->acc[ACC_VIR_BONDED] = x[9];
     sc->acc[ACC_VIR_CONSTR] = x[12];

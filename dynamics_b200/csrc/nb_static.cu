@@ -19,9 +19,14 @@
 // keeps the last call's contents; each call clears the part it uses before
 // accumulating.  Calls whose kernels overlap on one device (different
 // streams with no ordering between them) race on the scratch and give wrong
-// results.  The first call on each device looks up the scratch's device
-// address (cudaGetSymbolAddress) with that device current; make that first
-// call before any stream capture on that device.
+// results.  The first call on each device sets that device up with it
+// current: it looks up the scratch's device address (cudaGetSymbolAddress)
+// and loads this entry point's kernels.  With the runtime's lazy module
+// loading that first call is when the driver places the scratch in device
+// memory, so make it before reserving the rest of the device for other
+// work, and before any stream capture on that device.  The address is kept
+// for the life of the process: after cudaDeviceReset the module is gone and
+// this entry point must not be called again in that process.
 #include <mutex>
 
 #include "common.cuh"
@@ -46,24 +51,6 @@ static __device__ __align__(256) long long g_nb_scratch[ST_WORDS];
 
 std::mutex g_mu;
 void* g_scratch_ptr[ST_MAX_DEVICES] = {};
-
-// Device address of the scratch on the current device, looked up once per
-// device.
-int scratch_for_current_device(long long** out) {
-    int dev = 0;
-    DYN_CUDA(cudaGetDevice(&dev));
-    DYN_CHECK(dev >= 0 && (uint32_t)dev < ST_MAX_DEVICES, DYN_ERR_UNSUPPORTED,
-              "dyn_nb_forces_static: device ordinal beyond 63");
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_nb_scratch);
-        if (e != cudaSuccess) return dyn::cuda_fail(e, "dyn_nb_forces_static: cudaGetSymbolAddress");
-        g_scratch_ptr[dev] = p;
-    }
-    *out = (long long*)g_scratch_ptr[dev];
-    return DYN_OK;
-}
 
 struct StPos { const float* p[5]; };
 struct StOut { double* f[5]; };
@@ -192,6 +179,36 @@ __global__ void st_scalars_out(int nblocks, const long long* __restrict__ scratc
         scalars[1] = v[1];
         scalars[2] = (double)*skipped;
     }
+}
+
+// Set-up of the current device, once per device: the scratch's device
+// address, and the device code of this entry point.  The CUDA runtime loads
+// a module's code and its __device__ arrays lazily (CUDA_MODULE_LOADING=LAZY
+// is the default since CUDA 12.2): the symbol lookup makes the driver load
+// the scratch (its one allocation, made by the driver, not by this call's
+// work), and querying each kernel's attributes loads the kernels, so that no
+// later call loads anything -- not inside a stream capture either.
+int scratch_for_current_device(long long** out) {
+    int dev = 0;
+    DYN_CUDA(cudaGetDevice(&dev));
+    DYN_CHECK(dev >= 0 && (uint32_t)dev < ST_MAX_DEVICES, DYN_ERR_UNSUPPORTED,
+              "dyn_nb_forces_static: device ordinal beyond 63");
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_nb_scratch);
+        if (e != cudaSuccess) return dyn::cuda_fail(e, "dyn_nb_forces_static: cudaGetSymbolAddress");
+        const void* ks[4] = {(const void*)st_pair_kernel<true>, (const void*)st_pair_kernel<false>,
+                             (const void*)st_forces_out, (const void*)st_scalars_out};
+        for (const void* k : ks) {
+            cudaFuncAttributes fa;
+            e = cudaFuncGetAttributes(&fa, k);
+            if (e != cudaSuccess) return dyn::cuda_fail(e, "dyn_nb_forces_static: loading its kernels");
+        }
+        g_scratch_ptr[dev] = p;
+    }
+    *out = (long long*)g_scratch_ptr[dev];
+    return DYN_OK;
 }
 
 }  // namespace

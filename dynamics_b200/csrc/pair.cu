@@ -31,8 +31,15 @@ namespace {
 constexpr int PT = 128;  // threads per block (4 warps)
 
 // e_lj, e_c accumulate per-pair energies in float64 (energy steps only);
-// w accumulates the virial in float32
-struct Acc3 { double e_lj, e_c; float w; };
+// w sums the virial of one list entry (a molecule pair, or an i-body
+// against a j-cluster's atoms) in float32, and wd the entries' sums in
+// float64, so no long float32 chain feeds the pressure
+struct Acc3 {
+    double e_lj, e_c;
+    float w;
+    double wd;
+    __device__ __forceinline__ void flush_w() { wd += (double)w; w = 0.f; }
+};
 
 // erfc-screened Coulomb between site pi and site pj shifted by sh
 // (d = pi - (pj - sh)), branch-free: force q q (r^-3 + g(r^2)) d with
@@ -218,8 +225,83 @@ __device__ __forceinline__ uint32_t stage_chunk(const SysView& v, uint32_t g, ui
     return hi - lo;
 }
 
+// Screened Coulomb of one site pair of a molecule pair, both sides: the
+// pair force fs d (d = pi - pj) is added to the i-site sum fi and to the
+// j-site sum gj (the j site receives -gj).
+template <bool ENERGY>
+__device__ __forceinline__ void coul2(float3 pi, float3 pj, float qq, double qqe, const SysView& v, float3& fi,
+                                      float3& gj, Acc3& a) {
+    const float3 d = pi - pj;
+    const float r2 = dot3(d, d);
+    const float rinv = rsqrtf(r2);
+    const float t = fmaf(r2, v.two_over_rc2, -1.0f);
+    float g = v.poly_g[NPOLY_G - 1];
+#pragma unroll
+    for (int k = NPOLY_G - 2; k >= 0; --k) g = fmaf(g, t, v.poly_g[k]);
+    float fs = qq * fmaf(rinv * rinv, rinv, g);
+    fs = r2 < v.rc2 ? fs : 0.0f;
+    fi.x = fmaf(fs, d.x, fi.x); fi.y = fmaf(fs, d.y, fi.y); fi.z = fmaf(fs, d.z, fi.z);
+    gj.x = fmaf(fs, d.x, gj.x); gj.y = fmaf(fs, d.y, gj.y); gj.z = fmaf(fs, d.z, gj.z);
+    a.w = fmaf(fs, r2, a.w);
+    if (ENERGY && r2 < v.rc2) {
+        const float re = r2 * rinv;
+        a.e_c += qqe * (double)(erfcf(v.alpha * re) * rinv);
+    }
+}
+
+// j-side forces of union water u are added to the CTA's int32 sums; a
+// molecule pair with a component too large for them (|f| >= JFIX_MAX: 32
+// such contributions stay below 2^15 kcal/mol/A, the int32 range at
+// 2^-16) goes to the slot's int64 overflow sums instead.  Which path a pair
+// takes depends only on its values, and both are integer sums, so the
+// result stays deterministic.
+constexpr float JFIX_SCALE = (float)(1 << WW_JFIX_SHIFT);
+constexpr float JFIX_MAX = 1000.0f;
+
+__device__ __noinline__ void jforce_big(const SysView& v, uint32_t g, uint32_t u, int c, float f) {
+    // the slot of union entry u from the group's runs (ascending offsets)
+    const uint2* runs = v.grp_run + (size_t)g * v.cap_run;
+    uint32_t lo = 0, hi = v.grp_nrun[g];
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (runs[m].y <= u) lo = m; else hi = m;
+    }
+    const uint32_t slot = runs[lo].x + (u - runs[lo].y);
+    fix_atomic_add(v.wjbig + (size_t)slot * 12 + c, fix_from_float(f));
+}
+
+// The 12 j-side components of one molecule pair (the forces on the j
+// water's O, H0, H1, M); one range check for all of them.
+__device__ __forceinline__ void jforce_add12(const SysView& v, int* jacc, uint32_t chunk, uint32_t g, uint32_t u,
+                                             uint32_t ul, const float (&f)[12]) {
+    float m = 0.f;
+#pragma unroll
+    for (int c = 0; c < 12; ++c) m = fmaxf(m, fabsf(f[c]));
+    if (m < JFIX_MAX) {
+#pragma unroll
+        for (int c = 0; c < 12; ++c) atomicAdd(jacc + (size_t)c * chunk + ul, __float2int_rn(f[c] * JFIX_SCALE));
+    } else {
+        for (int c = 0; c < 12; ++c) jforce_big(v, g, u, c, f[c]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// water(i) - water(j), tile form, half lists.  One CTA per 32-water
+// i-group.  The waters the group's lists reach (its union, stored as runs
+// of consecutive slots) are copied global -> shared with one cp.async.bulk
+// per run, completing on an mbarrier, union_chunk waters at a time (one
+// chunk for almost every group; sized so that two CTAs fit on an SM).  Each
+// i-water is handled by LPW lanes walking its list of union indices: every
+// water pair once (the list of the lower slot), all 10 site pairs with one
+// min-image shift.  The i-side forces stay in registers and are stored
+// (first writer) after the group; the j-side forces are summed per union
+// water in shared memory (int32 fixed point, 12 components, component-major
+// so that the lanes' adds spread over the banks), then written to the
+// group's entries of jbuf (g * cap_union + union index), which k_ww_gather
+// adds to each water.
+// ---------------------------------------------------------------------------
 DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, (), ()) {
-    extern __shared__ __align__(128) float4 tile[];  // union_chunk waters, 4 float4 each
+    extern __shared__ __align__(128) float4 tile[];  // union_chunk waters x 4 float4, then the j sums
     __shared__ __align__(8) uint64_t bar;
     const int tid = threadIdx.x;
     const int il = tid / LPW, l = tid % LPW;
@@ -227,6 +309,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
     const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
     const uint32_t nslots = nwc * WCL;
     const uint32_t chunk = v.union_chunk;
+    int* jacc = reinterpret_cast<int*>(tile + 4 * (size_t)chunk);  // [12][chunk]
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     const float sig2 = OPC_O_SIGMA * OPC_O_SIGMA;
@@ -240,18 +323,18 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
     bool alive = true;
     for (uint32_t g = bk.idx; g < ng && alive; g += bk.cnt) {
         const uint32_t nloc = v.grp_nloc[g];
-        if (tid < 32 && nloc > 0) stage_chunk(v, g, 0, min(nloc, chunk), tile, &bar, tid);
+        const uint32_t uoff = g * v.cap_union;  // the group's jbuf entries
         const uint32_t s = g * GRPW + il;
         const bool have = s < nslots;
-        const uint32_t n = have ? v.wnb_n[s] : 0u;
+        const uint32_t n = have ? v.winb_n[s] : 0u;
         float3 iO = f3(0, 0, 0), iH0 = iO, iH1 = iO, iM = iO;
         if (have) {
             iO = xyz(v.wpos[4 * s + 0]); iH0 = xyz(v.wpos[4 * s + 1]);
             iH1 = xyz(v.wpos[4 * s + 2]); iM = xyz(v.wpos[4 * s + 3]);
         }
         float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
-        Acc3 a{0.0, 0.0, 0.f};
-        const uint16_t* lst = v.wnb + (size_t)s * v.cap_nb;
+        Acc3 a{0.0, 0.0, 0.f, 0.0};
+        const uint16_t* lst = v.winb + (size_t)s * v.cap_nb;  // the pruned list
         uint32_t k = l;  // this lane's next list entry (entries l, l + LPW, ...)
         // the next entry's index is loaded one iteration ahead, so the
         // global-memory latency of the list overlaps the arithmetic
@@ -261,7 +344,8 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
         // stopped
         for (uint32_t lo = 0; lo < nloc; lo += chunk) {
             const uint32_t hi = min(nloc, lo + chunk);
-            if (lo > 0 && tid < 32) stage_chunk(v, g, lo, hi, tile, &bar, tid);
+            if (tid < 32) stage_chunk(v, g, lo, hi, tile, &bar, tid);
+            for (uint32_t t = tid; t < 12 * chunk; t += WT) jacc[t] = 0;
             const bool ok = mbar_wait(&bar, parity, &v.sc->timeout);
             if (!__syncthreads_and(ok)) {
                 // give the copies in flight one more bounded chance, then stop
@@ -277,22 +361,41 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
                 const float4* jw = tile + 4 * (idx - lo);
                 const float3 jO = xyz(jw[0]);
                 const float3 sh = shift_of(iO - jO, b);
-                // the j sites moved by the shift once (the same float values
-                // pj - sh that each site pair would form), then zero shift
+                // the j sites moved by the shift once, then zero shift
                 const float3 z0 = f3(0.f, 0.f, 0.f);
                 const float3 sO = jO - sh, sH0 = xyz(jw[1]) - sh, sH1 = xyz(jw[2]) - sh, sM = xyz(jw[3]) - sh;
-                lj<ENERGY>(iO, sO, z0, sig2, OPC_O_EPS, ljc2, 1.0f, fO, a);
-                coul<ENERGY>(iH0, sH0, z0, qhh, ehh, v, fH0, a);
-                coul<ENERGY>(iH0, sH1, z0, qhh, ehh, v, fH0, a);
-                coul<ENERGY>(iH0, sM, z0, qhm, ehm, v, fH0, a);
-                coul<ENERGY>(iH1, sH0, z0, qhh, ehh, v, fH1, a);
-                coul<ENERGY>(iH1, sH1, z0, qhh, ehh, v, fH1, a);
-                coul<ENERGY>(iH1, sM, z0, qhm, ehm, v, fH1, a);
-                coul<ENERGY>(iM, sH0, z0, qhm, ehm, v, fM, a);
-                coul<ENERGY>(iM, sH1, z0, qhm, ehm, v, fM, a);
-                coul<ENERGY>(iM, sM, z0, qmm, emm, v, fM, a);
+                float3 gO = z0, gH0 = z0, gH1 = z0, gM = z0;
+                {
+                    float3 t = z0;
+                    lj<ENERGY>(iO, sO, z0, sig2, OPC_O_EPS, ljc2, 1.0f, t, a);
+                    fO = fO + t;
+                    gO = t;
+                }
+                coul2<ENERGY>(iH0, sH0, qhh, ehh, v, fH0, gH0, a);
+                coul2<ENERGY>(iH0, sH1, qhh, ehh, v, fH0, gH1, a);
+                coul2<ENERGY>(iH0, sM, qhm, ehm, v, fH0, gM, a);
+                coul2<ENERGY>(iH1, sH0, qhh, ehh, v, fH1, gH0, a);
+                coul2<ENERGY>(iH1, sH1, qhh, ehh, v, fH1, gH1, a);
+                coul2<ENERGY>(iH1, sM, qhm, ehm, v, fH1, gM, a);
+                coul2<ENERGY>(iM, sH0, qhm, ehm, v, fM, gH0, a);
+                coul2<ENERGY>(iM, sH1, qhm, ehm, v, fM, gH1, a);
+                coul2<ENERGY>(iM, sM, qmm, emm, v, fM, gM, a);
+                a.flush_w();
+                // the j waters receive the opposite forces (sites O, H0, H1, M)
+                const float jf[12] = {-gO.x, -gO.y, -gO.z, -gH0.x, -gH0.y, -gH0.z,
+                                      -gH1.x, -gH1.y, -gH1.z, -gM.x, -gM.y, -gM.z};
+                jforce_add12(v, jacc, chunk, g, idx, idx - lo, jf);
             }
-            __syncthreads();  // the tile is refilled by the next chunk's or group's copies
+            __syncthreads();  // every j sum of the chunk is in
+            // the chunk's sums -> the group's jbuf entries (48 B per water)
+            for (uint32_t u = tid; u < hi - lo; u += WT) {
+                int4* dst = reinterpret_cast<int4*>(v.jbuf + 12 * ((size_t)uoff + lo + u));
+                dst[0] = make_int4(jacc[0 * chunk + u], jacc[1 * chunk + u], jacc[2 * chunk + u], jacc[3 * chunk + u]);
+                dst[1] = make_int4(jacc[4 * chunk + u], jacc[5 * chunk + u], jacc[6 * chunk + u], jacc[7 * chunk + u]);
+                dst[2] = make_int4(jacc[8 * chunk + u], jacc[9 * chunk + u], jacc[10 * chunk + u],
+                                   jacc[11 * chunk + u]);
+            }
+            __syncthreads();  // the tile and the sums are refilled by the next chunk or group
         }
         if (!alive) break;
 #pragma unroll
@@ -311,9 +414,44 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
             store_fix3(p + 0, fO); store_fix3(p + 3, fH0); store_fix3(p + 6, fH1); store_fix3(p + 9, fM);
         }
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
-        ew += a.w;
+        ew += a.wd;
     }
     write_partials<ENERGY>(v, bk, REG_WW, el, ec, ew);
+}
+
+// ---------------------------------------------------------------------------
+// The j-side water-water forces: every water adds the sums the group CTAs
+// wrote for it (its reverse-index entries) and its int64 overflow sums,
+// which are cleared for the next step.  12 threads per water, one force
+// component each, so the 48-byte entries are read whole.  Integer sums in
+// any order: deterministic.
+// ---------------------------------------------------------------------------
+constexpr int GT = 384;  // 32 waters x 12 components per block
+
+DYN_KERNEL(__launch_bounds__(GT), k_ww_gather, (), ()) {
+    const uint32_t total = v.sc->n_wclus * WCL * 12;
+    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
+        const uint32_t s = t / 12, c = t - 12 * s;
+        if (v.wid[s] == INVALID_ID) continue;
+        const uint32_t n = min(v.rev_n[s], v.rev_cap);
+        const uint32_t* e = v.rev + (size_t)s * v.rev_cap;
+        // entries are jbuf entry numbers g * cap_union + u; four loads in
+        // flight per thread
+        long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        uint32_t k = 0;
+        for (; k + 4 <= n; k += 4) {
+            const uint32_t x0 = e[k], x1 = e[k + 1], x2 = e[k + 2], x3 = e[k + 3];
+            a0 += (long long)v.jbuf[12 * (size_t)x0 + c];
+            a1 += (long long)v.jbuf[12 * (size_t)x1 + c];
+            a2 += (long long)v.jbuf[12 * (size_t)x2 + c];
+            a3 += (long long)v.jbuf[12 * (size_t)x3 + c];
+        }
+        for (; k < n; ++k) a0 += (long long)v.jbuf[12 * (size_t)e[k] + c];
+        const long long acc = (a0 + a1) + (a2 + a3);
+        long long big = v.wjbig[t];
+        if (big != 0) v.wjbig[t] = 0;
+        v.wforce[t] += acc * (1ll << (32 - WW_JFIX_SHIFT)) + big;
+    }
 }
 
 // Reduce-scatter over the 8 lanes that share jq (lane bits 0-2): N values
@@ -347,108 +485,138 @@ __device__ __forceinline__ JAtoms load_jatoms(const SysView& v, uint32_t cj, int
 }
 
 // ---------------------------------------------------------------------------
-// water(i) - atom(j), each pair once.  One warp per work item (a water
-// i-cluster and CH_MIX entries of its atom-cluster list); the list entries
-// are read once per item (one per lane) and the next entry's j-atoms are
-// loaded while the current one is evaluated.  The water forces stay in
-// registers over the item; the j-atom forces (the opposite of the pair
-// forces) are reduce-scattered over the 8 water lanes of a j-group and added
-// with integer atomics (24 per entry).
+// water(i) - atom(j), each pair once.  One CTA per 32-water group (the
+// water-water kernel's groups).  The atoms the group's waters reach (its
+// atom union, cluster-slot indices from the rebuild) are gathered into
+// shared memory, aun_chunk at a time; each water is handled by LPW lanes
+// walking its list of union indices (O-atom distance below cutoff + O-H
+// reach + buffer at the rebuild).  The water forces stay in registers and
+// are added once per water (each water belongs to one group and no other
+// kernel writes them meanwhile); the atom forces are summed per union atom in
+// shared memory (int32 fixed point, as the water-water j sums) and added to
+// the atoms' int64 accumulators with three atomics per union atom.
 // ---------------------------------------------------------------------------
-DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT, 4), k_pair_ws, (), ()) {
-    const int lane = threadIdx.x & 31;
-    const int ii = lane & 7, jq = lane >> 3;
-    const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
-    const uint32_t nit = v.sc->n_ws_items;
-    const uint32_t first_single = v.sc->a_sparse_base / ACL;  // first single-atom cluster
+constexpr int AT = GRPW * LPW;  // threads per CTA
+
+DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(AT, 2), k_pair_ws, (), ()) {
+    extern __shared__ __align__(16) float4 apos_s[];  // aun_chunk x (float4, float2, uint32, 3 int32)
+    const uint32_t chunk = v.aun_chunk;
+    float2* alj_s = reinterpret_cast<float2*>(apos_s + chunk);
+    uint32_t* aid_s = reinterpret_cast<uint32_t*>(alj_s + chunk);
+    int* aacc = reinterpret_cast<int*>(aid_s + chunk);  // [3][chunk]
+    const int tid = threadIdx.x;
+    const int il = tid / LPW, l = tid % LPW;
+    const uint32_t nwc = v.sc->n_wclus;
+    const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
+    const uint32_t nslots = nwc * WCL;
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0, dh = 0.0;
-    for (uint32_t it = ((bk.idx * blockDim.x + threadIdx.x) >> 5); it < nit; it += nwarps) {
-        const uint2 item = v.ws_item[it];
-        const uint32_t ci = item.x, k0 = item.y;
-        const uint32_t n = min(v.ws_n[ci], k0 + CH_MIX) - k0;
-        const uint32_t si = ci * WCL + ii;
-        const bool vi = v.wid[si] != INVALID_ID;
-        const float3 iO = xyz(v.wpos[4 * si + 0]), iH0 = xyz(v.wpos[4 * si + 1]);
-        const float3 iH1 = xyz(v.wpos[4 * si + 2]), iM = xyz(v.wpos[4 * si + 3]);
-        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
-        Acc3 a{0.0, 0.0, 0.f};
-        const uint32_t my_j = (uint32_t)lane < n ? v.ws_j[(size_t)ci * v.cap_ws + k0 + lane] : 0u;
-        // Single-atom clusters (ions) come last in every list.  Four of them
-        // are taken per iteration, one per lane group jq (its atom in the
-        // h = 0 slot), instead of one cluster with seven empty slots.
-        auto load_at = [&](uint32_t k) -> JAtoms {
-            const uint32_t c0 = __shfl_sync(0xffffffffu, my_j, k);
-            const uint32_t kk = k + (uint32_t)jq;
-            const uint32_t cq = __shfl_sync(0xffffffffu, my_j, kk < n ? kk : k);
-            if (c0 < first_single) return load_jatoms(v, c0, jq);
-            const uint32_t sq = cq * ACL;
-            return JAtoms{v.spos[sq], make_float4(0.f, 0.f, 0.f, 0.f), v.slj[sq], make_float2(0.f, 0.f),
-                          kk < n ? v.sidx[sq] : INVALID_ID, INVALID_ID};
-        };
-        auto advance = [&](uint32_t k) -> uint32_t {
-            return __shfl_sync(0xffffffffu, my_j, k) < first_single ? 1u : 4u;
-        };
-        JAtoms nx = load_at(0);
-        for (uint32_t k = 0; k < n;) {
-            const JAtoms cur = nx;
-            k += advance(k);
-            if (k < n) nx = load_at(k);
-            float jf[8];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const float4 pj = h ? cur.p1 : cur.p0;
-                const float2 lj_j = h ? cur.l1 : cur.l0;
-                const uint32_t aj = h ? cur.a1 : cur.a0;
-                float3 fo = f3(0, 0, 0), f0 = fo, f1 = fo, fm = fo;
-                if (vi && aj != INVALID_ID) {
-                    const float3 jp = xyz(pj);
-                    // the atom moved by the shift once, then zero shift
-                    const float3 js = jp - shift_of(iO - jp, b), z0 = f3(0.f, 0.f, 0.f);
-                    const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
-                    const float ep = sqrtf(OPC_O_EPS * lj_j.y);
-                    const double qe = (double)pj.w;
-                    if (ALCH && aj >= v.alch_lo && aj < v.alch_hi) {
-                        // a water and an atom of the alchemical molecule
-                        lj_soft<ENERGY>(iO, js, z0, sg, ep, ljc2, v.alch_ll, v.alch_dll, fo, a, dh);
-                        Acc3 t{0.0, 0.0, 0.f};
-                        coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, t);
-                        coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, t);
-                        coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, t);
-                        const float cs = v.alch_cs;
-                        f0 = f0 * cs; f1 = f1 * cs; fm = fm * cs;
-                        a.w = fmaf(cs, t.w, a.w);
-                        if (ENERGY) { a.e_c += (double)cs * t.e_c; dh += (double)v.alch_dcs * t.e_c; }
-                    } else {
-                        lj<ENERGY>(iO, js, z0, sg * sg, ep, ljc2, 1.0f, fo, a);
-                        coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
-                        coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
-                        coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
-                    }
-                }
-                fO = fO + fo; fH0 = fH0 + f0; fH1 = fH1 + f1; fM = fM + fm;
-                const float3 t = (fo + f0) + (f1 + fm);
-                jf[3 * h + 0] = -t.x; jf[3 * h + 1] = -t.y; jf[3 * h + 2] = -t.z;
-            }
-            jf[6] = 0.f; jf[7] = 0.f;
-            // lane ii < 6 now holds component ii % 3 of the group's j-atom a0 (ii < 3) or a1
-            reduce_scatter8(jf, ii);
-            if (ii < 6) {
-                const uint32_t aj = ii < 3 ? cur.a0 : cur.a1;
-                if (aj != INVALID_ID) add_fix(v.aforce + 3 * (size_t)aj + ii % 3, jf[0]);
-            }
+    for (uint32_t g = bk.idx; g < ng; g += bk.cnt) {
+        const uint32_t nun = v.aun_n[g];  // the same for the whole CTA
+        if (nun == 0) continue;
+        const uint32_t s = g * GRPW + il;
+        const bool have = s < nslots && v.wid[s] != INVALID_ID;
+        const uint32_t n = have ? v.wal_n[s] : 0u;
+        float3 iO = f3(0, 0, 0), iH0 = iO, iH1 = iO, iM = iO;
+        if (have) {
+            iO = xyz(v.wpos[4 * s + 0]); iH0 = xyz(v.wpos[4 * s + 1]);
+            iH1 = xyz(v.wpos[4 * s + 2]); iM = xyz(v.wpos[4 * s + 3]);
         }
-        fO = f3(red4(fO.x), red4(fO.y), red4(fO.z));
-        fH0 = f3(red4(fH0.x), red4(fH0.y), red4(fH0.z));
-        fH1 = f3(red4(fH1.x), red4(fH1.y), red4(fH1.z));
-        fM = f3(red4(fM.x), red4(fM.y), red4(fM.z));
-        if (jq == 0 && vi) {
-            long long* p = v.wforce + (size_t)si * 12;
-            add_fix3(p + 0, fO); add_fix3(p + 3, fH0); add_fix3(p + 6, fH1); add_fix3(p + 9, fM);
+        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
+        Acc3 a{0.0, 0.0, 0.f, 0.0};
+        const uint16_t* lst = v.wal + (size_t)s * v.cap_wal;
+        uint32_t k = l;
+        uint32_t idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
+        const uint32_t* un = v.aun_idx + (size_t)g * v.cap_aun;
+        for (uint32_t lo = 0; lo < nun; lo += chunk) {
+            const uint32_t hi = min(nun, lo + chunk);
+            for (uint32_t t = tid; t < hi - lo; t += AT) {
+                const uint32_t cs = un[lo + t];
+                apos_s[t] = v.spos[cs];
+                alj_s[t] = v.slj[cs];
+                aid_s[t] = v.sidx[cs];
+            }
+            for (uint32_t t = tid; t < 3 * chunk; t += AT) aacc[t] = 0;
+            __syncthreads();
+            while (idx_next < hi) {
+                const uint32_t idx = idx_next;
+                k += LPW;
+                idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
+                const uint32_t u = idx - lo;
+                const float4 pj = apos_s[u];
+                const float2 lj_j = alj_s[u];
+                const uint32_t aj = aid_s[u];
+                const float3 jp = xyz(pj);
+                // the atom moved by the shift once, then zero shift
+                const float3 js = jp - shift_of(iO - jp, b), z0 = f3(0.f, 0.f, 0.f);
+                const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
+                const float ep = sqrtf(OPC_O_EPS * lj_j.y);
+                const double qe = (double)pj.w;
+                float3 fo = z0, f0 = z0, f1 = z0, fm = z0;
+                if (ALCH && aj >= v.alch_lo && aj < v.alch_hi) {
+                    // a water and an atom of the alchemical molecule
+                    lj_soft<ENERGY>(iO, js, z0, sg, ep, ljc2, v.alch_ll, v.alch_dll, fo, a, dh);
+                    Acc3 t{0.0, 0.0, 0.f, 0.0};
+                    coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, t);
+                    coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, t);
+                    coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, t);
+                    const float cs = v.alch_cs;
+                    f0 = f0 * cs; f1 = f1 * cs; fm = fm * cs;
+                    a.w = fmaf(cs, t.w, a.w);
+                    if (ENERGY) { a.e_c += (double)cs * t.e_c; dh += (double)v.alch_dcs * t.e_c; }
+                } else {
+                    lj<ENERGY>(iO, js, z0, sg * sg, ep, ljc2, 1.0f, fo, a);
+                    coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
+                    coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
+                    coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
+                }
+                a.flush_w();
+                fO = fO + fo; fH0 = fH0 + f0; fH1 = fH1 + f1; fM = fM + fm;
+                // the atom receives the opposite of the water's force
+                const float3 t = (fo + f0) + (f1 + fm);
+                if (fmaxf(fabsf(t.x), fmaxf(fabsf(t.y), fabsf(t.z))) < JFIX_MAX) {
+                    atomicAdd(aacc + 0 * (size_t)chunk + u, __float2int_rn(-t.x * JFIX_SCALE));
+                    atomicAdd(aacc + 1 * (size_t)chunk + u, __float2int_rn(-t.y * JFIX_SCALE));
+                    atomicAdd(aacc + 2 * (size_t)chunk + u, __float2int_rn(-t.z * JFIX_SCALE));
+                } else {
+                    add_fix3(v.aforce + 3 * (size_t)aj, f3(-t.x, -t.y, -t.z));
+                }
+            }
+            __syncthreads();  // every atom sum of the chunk is in
+            for (uint32_t t = tid; t < hi - lo; t += AT) {
+                long long* fa = v.aforce + 3 * (size_t)aid_s[t];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int q = aacc[c * chunk + t];
+                    if (q != 0) fix_atomic_add(fa + c, (long long)q * (1ll << (32 - WW_JFIX_SHIFT)));
+                }
+            }
+            __syncthreads();  // the shared buffers are refilled by the next chunk or group
+        }
+#pragma unroll
+        for (int o = 1; o < LPW; o <<= 1) {
+            fO.x += __shfl_xor_sync(0xffffffffu, fO.x, o); fO.y += __shfl_xor_sync(0xffffffffu, fO.y, o);
+            fO.z += __shfl_xor_sync(0xffffffffu, fO.z, o);
+            fH0.x += __shfl_xor_sync(0xffffffffu, fH0.x, o); fH0.y += __shfl_xor_sync(0xffffffffu, fH0.y, o);
+            fH0.z += __shfl_xor_sync(0xffffffffu, fH0.z, o);
+            fH1.x += __shfl_xor_sync(0xffffffffu, fH1.x, o); fH1.y += __shfl_xor_sync(0xffffffffu, fH1.y, o);
+            fH1.z += __shfl_xor_sync(0xffffffffu, fH1.z, o);
+            fM.x += __shfl_xor_sync(0xffffffffu, fM.x, o); fM.y += __shfl_xor_sync(0xffffffffu, fM.y, o);
+            fM.z += __shfl_xor_sync(0xffffffffu, fM.z, o);
+        }
+        if (l == 0 && have && n > 0) {
+            long long* p = v.wforce + (size_t)s * 12;
+            const float3 fs[4] = {fO, fH0, fH1, fM};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                p[3 * q + 0] += fix_from_float(fs[q].x);
+                p[3 * q + 1] += fix_from_float(fs[q].y);
+                p[3 * q + 2] += fix_from_float(fs[q].z);
+            }
         }
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
-        ew += a.w;
+        ew += a.wd;
     }
     write_partials<ENERGY>(v, bk, REG_WS, el, ec, ew, dh);
 }
@@ -475,7 +643,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT), k_
         const float4 pi = v.spos[si];
         const float2 lji = v.slj[si];
         float3 f = f3(0, 0, 0);
-        Acc3 a{0.0, 0.0, 0.f};
+        Acc3 a{0.0, 0.0, 0.f, 0.0};
         const size_t row = (size_t)ci * v.cap_ss + k0;
         const uint32_t my_j = (uint32_t)lane < n ? v.ss_j[row + lane] : 0u;
         const unsigned long long my_m = (uint32_t)lane < n ? v.ss_mask[row + lane] : 0ull;
@@ -499,7 +667,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT), k_
                         // exactly one atom of the pair in the alchemical molecule
                         lj_soft<ENERGY>(xyz(pi), xyz(pj), s, sg, sqrtf(lji.y * ljj.y), ljc2, v.alch_ll, v.alch_dll,
                                         fp, a, dh);
-                        Acc3 t{0.0, 0.0, 0.f};
+                        Acc3 t{0.0, 0.0, 0.f, 0.0};
                         float3 fc = f3(0.f, 0.f, 0.f);
                         coul<ENERGY>(xyz(pi), xyz(pj), s, pi.w * pj.w, (double)pi.w * (double)pj.w, v, fc, t);
                         const float cs = v.alch_cs;
@@ -515,6 +683,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT), k_
                 jf[3 * h + 0] = -fp.x; jf[3 * h + 1] = -fp.y; jf[3 * h + 2] = -fp.z;
             }
             jf[6] = 0.f; jf[7] = 0.f;
+            a.flush_w();
             // lane ii < 6 now holds component ii % 3 of atom jq + 4 (ii / 3)
             reduce_scatter8(jf, ii);
             if (ii < 6) {
@@ -525,7 +694,8 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT), k_
         f = f3(red4(f.x), red4(f.y), red4(f.z));
         if (jq == 0 && ai != INVALID_ID) add_fix3(v.aforce + 3 * (size_t)ai, f);
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
-        ew += a.w;
+        a.flush_w();
+        ew += a.wd;
     }
     write_partials<ENERGY>(v, bk, REG_SS, el, ec, ew, dh);
 }
@@ -542,10 +712,10 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_pair14, (), ()) {
         const float4 pa = v.apos[p.x], pb = v.apos[p.y];
         const float3 sh = shift_of(xyz(pa) - xyz(pb), b);
         float3 f = f3(0, 0, 0);
-        Acc3 a{0.0, 0.0, 0.f};
+        Acc3 a{0.0, 0.0, 0.f, 0.0};
         lj<ENERGY>(xyz(pa), xyz(pb), sh, par.x * par.x, par.y, v.ljc2, 0.5f, f, a);
         float3 fc = f3(0, 0, 0);
-        Acc3 ac{0.0, 0.0, 0.f};
+        Acc3 ac{0.0, 0.0, 0.f, 0.0};
         coul<ENERGY>(xyz(pa), xyz(pb), sh, par.z, (double)pa.w * (double)pb.w, v, fc, ac);
         const float s = 0.833333333f;
         f = f + fc * s;
@@ -571,13 +741,26 @@ inline int pblocks(const SysView& v, uint64_t warps) {
 
 namespace dyn {
 
-int pair_blocks_ws(const SysView& v) { return pblocks(v, v.ws_item_cap); }
+int pair_blocks_ws(const SysView& v) {
+    return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
+}
+
+// per staged atom: position and charge, sigma / eps, index, 3 int32 sums
+size_t ws_smem(const SysView& v) {
+    return (size_t)v.aun_chunk * (sizeof(float4) + sizeof(float2) + sizeof(uint32_t) + 3 * sizeof(int));
+}
 
 int ww_tile_blocks(const SysView& v) {
     return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
 }
 
-size_t ww_tile_smem(const SysView& v) { return (size_t)v.union_chunk * 4 * sizeof(float4); }
+// per union water: 4 float4 positions and 12 int32 j sums
+size_t ww_tile_smem(const SysView& v) { return (size_t)v.union_chunk * (4 * sizeof(float4) + 12 * sizeof(int)); }
+
+int ww_gather_blocks(const SysView& v) {
+    const uint64_t b = ((uint64_t)v.nw_cap * 12 + GT - 1) / GT;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, 148u * 8u));
+}
 
 // The limit is a property of the kernel, shared by every system in the
 // process, so it is raised to the device maximum once rather than set to one
@@ -593,6 +776,17 @@ int pair_ww_setup(const SysView& v) {
         DYN_CUDA(cudaFuncGetAttributes(&fa, k));
         const int lim = optin - (int)fa.sharedSizeBytes;
         DYN_CHECK(ww_tile_smem(v) <= (size_t)lim, DYN_ERR_UNSUPPORTED, "water-water chunk exceeds shared memory");
+        DYN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    }
+    const void* ka[8] = {(const void*)k_pair_ws<true, true>, (const void*)k_pair_ws<true, false>,
+                         (const void*)k_pair_ws<false, true>, (const void*)k_pair_ws<false, false>,
+                         (const void*)k_pair_ws_batch<true, true>, (const void*)k_pair_ws_batch<true, false>,
+                         (const void*)k_pair_ws_batch<false, true>, (const void*)k_pair_ws_batch<false, false>};
+    for (const void* k : ka) {
+        cudaFuncAttributes fa;
+        DYN_CUDA(cudaFuncGetAttributes(&fa, k));
+        const int lim = optin - (int)fa.sharedSizeBytes;
+        DYN_CHECK(ws_smem(v) <= (size_t)lim, DYN_ERR_UNSUPPORTED, "water-atom chunk exceeds shared memory");
         DYN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     }
     return DYN_OK;
@@ -633,17 +827,20 @@ void launch_pairs_water(const Target& t, bool energy) {
              [&](const SysView& v) { return v.nw && eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
     t.launch(k_pair_ww_tile<false>, k_pair_ww_tile_batch<false>,
              [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
-    // the water-atom kernel adds to the water forces the water-water kernel stores
+    // the j-side sums and the water-atom forces are added to the water
+    // forces the water-water kernel stores
+    t.launch(k_ww_gather, k_ww_gather_batch, [](const SysView& v) { return v.nw ? ww_gather_blocks(v) : 0; }, GT, 0);
     launch_pairs_ws(t, energy);
 }
 
 void launch_pairs_ws(const Target& t, bool energy) {
     auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
+    const size_t sm = t.max_over([](const SysView& v) { return v.nw && v.na ? ws_smem(v) : (size_t)0; });
     const bool al = any_alch(t);
-    if (energy && al) t.launch(k_pair_ws<true, true>, k_pair_ws_batch<true, true>, ws, PT, 0);
-    else if (energy) t.launch(k_pair_ws<true, false>, k_pair_ws_batch<true, false>, ws, PT, 0);
-    else if (al) t.launch(k_pair_ws<false, true>, k_pair_ws_batch<false, true>, ws, PT, 0);
-    else t.launch(k_pair_ws<false, false>, k_pair_ws_batch<false, false>, ws, PT, 0);
+    if (energy && al) t.launch(k_pair_ws<true, true>, k_pair_ws_batch<true, true>, ws, AT, sm);
+    else if (energy) t.launch(k_pair_ws<true, false>, k_pair_ws_batch<true, false>, ws, AT, sm);
+    else if (al) t.launch(k_pair_ws<false, true>, k_pair_ws_batch<false, true>, ws, AT, sm);
+    else t.launch(k_pair_ws<false, false>, k_pair_ws_batch<false, false>, ws, AT, sm);
 }
 
 void launch_pair14(const Target& t, bool energy) {

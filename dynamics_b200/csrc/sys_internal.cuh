@@ -34,6 +34,8 @@ struct dyn_sys_s {
     void* snap_mem = nullptr;      // snapshot ring (dyn_sys_snapshots)
     size_t snap_bytes = 0;
     uint64_t snap_read = 0;        // frames handed to the host so far
+    cudaEvent_t window_ev = nullptr;  // bounds the steps one dyn_sys_step call queues
+    bool window_armed = false;
 };
 
 namespace dyn {

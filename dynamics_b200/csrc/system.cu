@@ -215,12 +215,18 @@ int capture_step(dyn_sys_s* h, float dt, bool spme, bool energy, cudaGraph_t* ou
             e = cudaGraphConditionalHandleCreate(&v.cond_rebuild, cg, 0, cudaGraphCondAssignDefault);
         if (e == cudaSuccess)
             e = cudaGraphConditionalHandleCreate(&v.cond_periodic, cg, 0, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess)
+            e = cudaGraphConditionalHandleCreate(&v.cond_prune, cg, 0, cudaGraphCondAssignDefault);
         if (e != cudaSuccess) { rc = dyn::cuda_fail(e, "cudaGraphConditionalHandleCreate"); break; }
         v.use_cond = 1;
         if ((rc = dyn::enqueue_first_half(T, S0, h->br, true, dt)) != DYN_OK) break;
         dyn::launch_displacement_check(T);
         if ((rc = begin_if_body(st, h->aux, v.cond_rebuild, &br)) != DYN_OK) break;
         dyn::launch_rebuild(TA, false);
+        if ((rc = end_if_body(h->aux)) != DYN_OK) break;
+        cudaGraph_t bpr = nullptr;
+        if ((rc = begin_if_body(st, h->aux, v.cond_prune, &bpr)) != DYN_OK) break;
+        dyn::launch_prune(TA, false);
         if ((rc = end_if_body(h->aux)) != DYN_OK) break;
         dyn::launch_gather_atoms(T);
         if ((rc = dyn::enqueue_forces(T, S0, S1, h->br, true, spme, energy)) != DYN_OK) break;
@@ -256,6 +262,7 @@ void enqueue_forces(dyn_sys_s* h, bool force_rebuild) {
     const Target T{&v, nullptr, st};
     if (!force_rebuild) dyn::launch_displacement_check(T);
     dyn::launch_rebuild(T, force_rebuild);
+    dyn::launch_prune(T, force_rebuild);
     dyn::launch_gather_atoms(T);
     dyn::launch_pairs(T, true);
     dyn::launch_pair14(T, true);
@@ -312,6 +319,7 @@ void fill_energies(dyn_sys_s* h, dyn_energies_t* e) {
     e->pressure_atomic_bar = s.pressure_atomic;
     e->list_union_max = s.union_max;
     e->dh_dl = s.dh_dl;
+    e->list_prunes = s.prunes;
 }
 
 // staged_decoupling_schedule (src/alchemical.rs:77-96): Coulomb scaled
@@ -341,6 +349,7 @@ extern "C" int dyn_sys_destroy(dyn_sys_t h) {
     if (h->h_sc) cudaFreeHost(h->h_sc);
     if (h->own_stream) cudaStreamDestroy(h->stream);
     if (h->aux) cudaStreamDestroy(h->aux);
+    if (h->window_ev) cudaEventDestroy(h->window_ev);
     h->br.destroy();
     delete h;
     return DYN_OK;
@@ -455,6 +464,9 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     v.r_ww = std::max(ljc, rc + 2.0f * OPC_SITE_REACH) + v.buffer;
     v.r_ws = std::max(ljc, rc + OPC_SITE_REACH) + v.buffer;
     v.r_ss = std::max(ljc, rc) + v.buffer;
+    // pruned water-water lists (an inner buffer at most the outer one)
+    v.prune_buf = std::min(cfg->prune_buffer > 0.f ? cfg->prune_buffer : 0.4f, v.buffer);
+    v.r_in = std::max(ljc, rc + 2.0f * OPC_SITE_REACH) + v.prune_buf;
     v.flags = cfg->flags; v.seed = cfg->seed;
     v.temperature = cfg->temperature; v.gamma = cfg->langevin_gamma; v.tau_t = cfg->tau_temp;
     v.p_target = cfg->pressure_bar; v.tau_p = cfg->tau_pressure; v.kappa = cfg->compressibility;
@@ -533,14 +545,23 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         size_t per_cta = smem_sm > 6144 ? (size_t)smem_sm / 2 - 3072 : 48 * 1024;
         per_cta = std::min<size_t>(per_cta, smem_blk > 0 ? (size_t)smem_blk : per_cta);
-        const uint32_t fit = (uint32_t)(per_cta / (4 * sizeof(float4))) / 32 * 32;
+        // per staged water: its 4 site positions and its 12 int32 j sums
+        const uint32_t fit = (uint32_t)(per_cta / (4 * sizeof(float4) + 12 * sizeof(int))) / 32 * 32;
         v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(fit, (v.cap_union + 31) / 32 * 32));
         if (cfg->ww_union_chunk)
             v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(v.union_chunk, cfg->ww_union_chunk / 32 * 32));
         v.cap_run = v.cap_union;  // a run per union water at worst
         const double nb = 4.0 / 3.0 * M_PI * r * r * r * dl;
+        // half lists: about nb / 2 partners above a water's slot on average,
+        // but the first waters of the slot order keep nearly all of theirs
+        // (their periodic neighbours sit at the end of the order)
         v.cap_nb = std::min<uint32_t>((uint32_t)(1.5 * nb) + 32, 65535u);
+        // per water, the unions that hold it (union entries per water, at the
+        // densest and most spread-out groups, with margin)
+        v.rev_cap = (uint32_t)(2.0 * mink(ag) * dl / GRPW) + 32;
     }
+    DYN_CHECK((uint64_t)v.ngrp_cap * v.cap_union < (1ull << 32), DYN_ERR_UNSUPPORTED,
+              "dyn_sys_create: too many waters in one system");
     // screened-Coulomb force: F = q q (r^-3 + g(r^2)) d for r < rc with
     // g(z) = 2 d/dz [erf(alpha sqrt z) / sqrt z], an entire function of z
     // fitted on [0, rc^2]; the r^-3 part is exact, so no cancellation-free
@@ -572,10 +593,32 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         if ((uint64_t)n_i * n_j <= (1ull << 24)) return std::max(1u, n_j);
         return est(r, vol_cl, n_j);
     };
-    v.cap_ws = (v.nw && v.na) ? cap_mixed(v.r_ws, acl_vol, v.nwclus_cap, v.naclus_cap) : 1;
     v.cap_ss = v.na ? cap_mixed(v.r_ss, acl_vol, v.naclus_cap, v.naclus_cap) : 1;
-    v.ws_item_cap = v.nwclus_cap * ((v.cap_ws + CH_MIX - 1) / CH_MIX);
     v.ss_item_cap = v.naclus_cap * ((v.cap_ss + CH_MIX - 1) / CH_MIX);
+    // water-atom: atom clusters near a water group's box (every cluster while
+    // that stays small), the atoms a group reaches and the atoms one water
+    // reaches, at a dense solute's density (0.12 atoms / A^3) with margin
+    if (v.nw && v.na) {
+        const double r = v.r_ws;
+        const double ag = 1.4 * std::cbrt(GRPW / std::max(1e-3, std::min(0.0334, v.nw / vol)));
+        const double mink_a = ag * ag * ag + 6.0 * ag * ag * r + 3.0 * M_PI * ag * r * r + 4.0 / 3.0 * M_PI * r * r * r;
+        v.cap_atile = cap_mixed(r, acl_vol, v.ngrp_cap, v.naclus_cap);
+        v.cap_aun = std::min<uint32_t>(std::min<uint32_t>(v.na_cap, v.cap_atile * ACL),
+                                       (uint32_t)(0.24 * mink_a) + 256);
+        v.cap_aun = std::min<uint32_t>(v.cap_aun, 65535u);
+        v.cap_wal = std::min<uint32_t>(v.cap_aun, (uint32_t)(0.15 * 4.0 / 3.0 * M_PI * r * r * r) + 64);
+        // shared-memory chunk of the water-atom kernel: two CTAs per SM
+        int dev = 0, smem_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        const size_t per_atom = sizeof(float4) + sizeof(float2) + sizeof(uint32_t) + 3 * sizeof(int);
+        const size_t per_cta = smem_sm > 6144 ? std::min<size_t>((size_t)smem_sm / 2 - 4096, 64 * 1024) : 32 * 1024;
+        const uint32_t fit = (uint32_t)(per_cta / per_atom) / 32 * 32;
+        v.aun_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(fit, (v.cap_aun + 31) / 32 * 32));
+    } else {
+        v.cap_atile = v.cap_aun = v.cap_wal = 1;
+        v.aun_chunk = 32;
+    }
 
     // ---- allocations ----
     TRY(dev_alloc(h, &v.wpos, 4 * (size_t)v.nw_cap));
@@ -632,9 +675,21 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dev_alloc(h, &v.cand_loc, (size_t)v.ngrp_cap * v.cap_tile * WCL));
     TRY(dev_alloc(h, &v.wnb_n, v.nw_cap));
     TRY(dev_alloc(h, &v.wnb, (size_t)v.nw_cap * v.cap_nb));
-    TRY(dev_alloc(h, &v.ws_n, v.nwclus_cap));
-    TRY(dev_alloc(h, &v.ws_j, (size_t)v.nwclus_cap * v.cap_ws));
-    TRY(dev_alloc(h, &v.ws_item, std::max(1u, v.ws_item_cap)));
+    TRY(dev_alloc(h, &v.winb_n, v.nw_cap));
+    TRY(dev_alloc(h, &v.winb, (size_t)v.nw_cap * v.cap_nb));
+    TRY(dev_alloc(h, &v.wprune, v.nw_cap));
+    TRY(dev_alloc(h, &v.grp_uslot, (size_t)v.ngrp_cap * v.cap_union));
+    TRY(dev_alloc(h, &v.jbuf, 12 * (size_t)v.ngrp_cap * v.cap_union));
+    TRY(dev_alloc(h, &v.rev_n, v.nw_cap));
+    TRY(dev_alloc(h, &v.rev, (size_t)v.nw_cap * v.rev_cap));
+    TRY(dev_alloc(h, &v.wjbig, 12 * (size_t)v.nw_cap));
+    TRY(dev_alloc(h, &v.atile_n, v.ngrp_cap));
+    TRY(dev_alloc(h, &v.atile_j, (size_t)v.ngrp_cap * v.cap_atile));
+    TRY(dev_alloc(h, &v.aun_n, v.ngrp_cap));
+    TRY(dev_alloc(h, &v.aun_idx, (size_t)v.ngrp_cap * v.cap_aun));
+    TRY(dev_alloc(h, &v.acand_loc, (size_t)v.ngrp_cap * v.cap_atile * ACL));
+    TRY(dev_alloc(h, &v.wal_n, v.nw_cap));
+    TRY(dev_alloc(h, &v.wal, (size_t)v.nw_cap * v.cap_wal));
     TRY(dev_alloc(h, &v.ss_item, std::max(1u, v.ss_item_cap)));
     TRY(dev_alloc(h, &v.ss_n, v.naclus_cap));
     TRY(dev_alloc(h, &v.ss_j, (size_t)v.naclus_cap * v.cap_ss));
@@ -838,6 +893,9 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     return DYN_OK;
 }
 
+// Launches a long dyn_sys_step call keeps in flight before it waits.
+constexpr uint32_t STEP_WINDOW = 512;
+
 extern "C" int dyn_sys_step(dyn_sys_t h, uint32_t n_steps, float dt) {
     DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_step: NULL handle");
     DYN_CHECK(dt > 0.f && std::isfinite(dt), DYN_ERR_INVALID, "dyn_sys_step: dt must be > 0");
@@ -859,7 +917,16 @@ extern "C" int dyn_sys_step(dyn_sys_t h, uint32_t n_steps, float dt) {
         }
         DYN_CUDA(cudaGraphLaunch(h->graph[g], h->stream));
         h->host_step += 1;
+        // at most about 2 x STEP_WINDOW steps queued at a time: every
+        // STEP_WINDOW launches wait for the mark set STEP_WINDOW launches ago
+        if ((i + 1) % STEP_WINDOW == 0 && i + 1 < n_steps) {
+            if (!h->window_ev) DYN_CUDA(cudaEventCreateWithFlags(&h->window_ev, cudaEventDisableTiming));
+            if (h->window_armed) DYN_CUDA(cudaEventSynchronize(h->window_ev));
+            DYN_CUDA(cudaEventRecord(h->window_ev, h->stream));
+            h->window_armed = true;
+        }
     }
+    h->window_armed = false;
     return DYN_OK;
 }
 
@@ -1173,6 +1240,7 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
         cudaEventRecord(ev[1], st);
         dyn::launch_displacement_check(T);
         dyn::launch_rebuild(T, false);
+        dyn::launch_prune(T, false);
         cudaEventRecord(ev[2], st);
         dyn::launch_gather_atoms(T);
         dyn::launch_pairs(T, energy);

@@ -104,6 +104,9 @@ class MdConfig:
     reset_angle: bool = True
     seed: int = 0
     ww_union_chunk: int = 0         # 0 = automatic (tuning knob only)
+    # inner buffer of the pruned water-water lists (A); 0 = automatic
+    # (tuning knob only, results do not depend on it)
+    prune_buffer: float = 0.0
     lincs_order: int = 4            # HydrogenConstraint::Linear { order, iter } (src/prep.rs:77)
     lincs_iter: int = 1
     # constraint position corrections also correct the velocities (RATTLE);
@@ -192,6 +195,7 @@ def _config_struct(system, cfg):
     c.thermo_dof = thermo_dof(system, cfg)
     c.seed = int(cfg.seed) & 0xFFFFFFFFFFFFFFFF
     c.ww_union_chunk = int(cfg.ww_union_chunk)
+    c.prune_buffer = float(cfg.prune_buffer)
     c.lincs_order = int(cfg.lincs_order)
     c.lincs_iter = int(cfg.lincs_iter)
     return c
@@ -479,6 +483,16 @@ class MdState:
         r, p = C.c_uint32(), C.c_uint32()
         check(lib().dyn_sys_launches_conditional(self.handle, C.byref(r), C.byref(p)))
         return r.value, p.value
+
+    def list_pairs(self, kind):
+        """The pairs the pair kernels evaluate now (dyn_sys_list_pairs):
+        kind 0 water-water (water, water), 1 water-atom (water, atom),
+        2 atom-atom; an (n, 2) uint32 array of original indices."""
+        n = C.c_uint64(0)
+        check(lib().dyn_sys_list_pairs(self.handle, int(kind), None, 0, C.byref(n)))
+        out = np.zeros((max(int(n.value), 1), 2), np.uint32)
+        check(lib().dyn_sys_list_pairs(self.handle, int(kind), ptr(out), int(n.value), C.byref(n)))
+        return out[:int(n.value)]
 
     def set_state(self, atom_pos=None, atom_vel=None, water_pos=None, water_vel=None):
         conv = [None if x is None else f32(x).reshape(-1) for x in (atom_pos, atom_vel, water_pos, water_vel)]

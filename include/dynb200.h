@@ -204,9 +204,13 @@ int dyn_nb_destroy(dyn_nb_t h);
  * larger system is rejected with DYN_ERR_INVALID.  Every call on a device
  * shares it: calls whose work overlaps on one device (unordered streams)
  * race and give wrong results.  Each call clears what it uses first.  The
- * call is asynchronous on `stream`; the first call on each device looks up
- * the scratch address with that device current, so make it before any
- * stream capture. */
+ * call is asynchronous on `stream`.  The first call on each device sets it
+ * up with that device current: it looks up the scratch's address and loads
+ * this entry point's kernels, which is when the CUDA driver (lazy module
+ * loading, the default since CUDA 12.2) places the scratch in device memory;
+ * so make that first call before reserving the rest of the device and
+ * before any stream capture.  Not valid after cudaDeviceReset in the same
+ * process (the cached address belongs to the destroyed context). */
 int dyn_nb_forces_static(void* stream, uint32_t n_dyn, uint32_t n_water, const float* pos_dyn,
                          const float* pos_w_o, const float* pos_w_m, const float* pos_w_h0,
                          const float* pos_w_h1, uint64_t n_pairs, const uint32_t* tgt,
@@ -293,7 +297,12 @@ typedef struct {
                              * HydrogenConstraint::Linear (src/prep.rs:55-78);
                              * 0 = 4 (the reference default)                */
     uint32_t lincs_iter;    /* SHAKE-style correction passes; 0 = 1         */
-    uint32_t reserved0;
+    float prune_buffer;     /* water-water lists are pruned to molecule pairs
+                             * within cutoff + 2 x O-H reach + this (A)
+                             * whenever a water has moved half of it since
+                             * the last prune; 0 = 0.4 A; >= list_buffer:
+                             * pruned only at list rebuilds (a tuning knob:
+                             * results do not depend on it)                 */
     /* Alchemical decoupling of the atoms [alch_begin, alch_end) (one
      * molecule, StateAlchemical, src/alchemical.rs:98-121): pairs between
      * them and the rest use soft-core LJ and scaled Coulomb, SPME is
@@ -365,6 +374,8 @@ typedef struct {
                                * needed at the last list build */
     double dh_dl;             /* alchemical dH/dlambda, kcal/mol (short-range
                                * cross pairs + SPME cross term), energy steps */
+    uint64_t list_prunes;     /* prunes of the water-water lists so far (every
+                               * rebuild is followed by one) */
 } dyn_energies_t;
 
 /* Creates a resident system (replaces MdState::new's device setup,
@@ -435,6 +446,16 @@ int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
  * periodic task is due (*periodic); in the captured step graph these sit
  * under conditional nodes that the device sets. */
 int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic);
+
+/* The pairs the resident engine's pair kernels evaluate at this moment, as
+ * written by the last list build or prune: kind 0 water-water molecule pairs
+ * (water i, water j; original water indices), kind 1 water-atom (water,
+ * atom), kind 2 atom-atom (atom i, atom j).  pairs[2k], pairs[2k+1] form one
+ * pair; *n_pairs receives the count (pairs = NULL: count only).  Replaces
+ * the reference's inspectable neighbour lists (NeighborsNb,
+ * src/neighbors.rs:25-53) for checking that every pair inside the cutoff is
+ * covered.  Synchronous; for tests and diagnostics, not the step loop. */
+int dyn_sys_list_pairs(dyn_sys_t h, uint32_t kind, uint32_t* pairs, uint64_t capacity, uint64_t* n_pairs);
 
 /* Moves an alchemical system to another lambda (a new window of the
  * thermodynamic integration, set_alchemical_window, src/alchemical.rs). */
