@@ -129,6 +129,7 @@ struct Sim {
     float max_disp2 = 0.f;
     // SPME cache (src/lib.rs:1296-1340)
     std::vector<V3> spme_f;
+    std::vector<V3> spme_df14;  // 1-4 vacuum correction of the last SPME step
     double spme_e = 0, spme_w = 0;
     double ke = 0, pe = 0, virial = 0;
     int rebuilds = 0;
@@ -493,16 +494,18 @@ void spme(Sim& S) {
     for (int i = 0; i < nq; ++i) qs += (double)q[i] * q[i];
     S.spme_e = e - S.alpha / std::sqrt(M_PI) * qs;
     S.spme_w = w;
-    // 1-4 vacuum Coulomb correction, cached with the SPME forces
-    // (src/non_bonded.rs:763-790)
+    // 1-4 vacuum Coulomb correction (src/non_bonded.rs:763-790): applied
+    // on the SPME steps only -- its forces are not part of the cached
+    // reciprocal forces (src/lib.rs:1296-1340), its virial is
+    S.spme_df14.assign(na, V3{0, 0, 0});
     for (const uint64_t k : S.p14) {
         const uint32_t i = (uint32_t)(k >> 32), j = (uint32_t)(k & 0xFFFFFFFFu);
         const V3 d = S.box.min_image(S.at[i].p - S.at[j].p);
         const float r = std::sqrt(dot(d, d));
         if (r < 1e-6f) continue;
         const V3 df = d * (S.at[i].q * S.at[j].q / (r * r * r) * (1.0f / 1.2f - 1.0f));
-        S.spme_f[3 * n + i] = S.spme_f[3 * n + i] + df;
-        S.spme_f[3 * n + j] = S.spme_f[3 * n + j] - df;
+        S.spme_df14[i] = S.spme_df14[i] + df;
+        S.spme_df14[j] = S.spme_df14[j] - df;
     }
 }
 
@@ -579,14 +582,18 @@ void all_forces(Sim& S) {
     for (Atom& a : S.at) a.f = V3{0, 0, 0};
     pair_forces(S);
     bonded_forces(S);
-    if (S.step % 2 == 0) spme(S);  // SPME_RATIO (src/lib.rs:208)
+    const bool spme_step = S.step % 2 == 0;  // SPME_RATIO (src/lib.rs:208)
+    if (spme_step) spme(S);
     const size_t n = S.w.size();
     for (size_t i = 0; i < n; ++i) {
         S.w[i].fm = S.w[i].fm + S.spme_f[3 * i];
         S.w[i].fh0 = S.w[i].fh0 + S.spme_f[3 * i + 1];
         S.w[i].fh1 = S.w[i].fh1 + S.spme_f[3 * i + 2];
     }
-    for (size_t i = 0; i < S.at.size(); ++i) S.at[i].f = S.at[i].f + S.spme_f[3 * n + i];
+    for (size_t i = 0; i < S.at.size(); ++i) {
+        S.at[i].f = S.at[i].f + S.spme_f[3 * n + i];
+        if (spme_step) S.at[i].f = S.at[i].f + S.spme_df14[i];
+    }
     S.pe = S.spme_e;
 }
 
