@@ -59,21 +59,16 @@ WORKLOADS = {
                 n_water=None),
     # serving form: Poisson arrivals (20 / s) of systems drawn from the c4w
     # size distribution, 5000 steps each, Langevin-middle 300 K, 150 GB budget
-    "c5w": dict(kind="serve", n_req=48, rate=20.0, steps_each=5000, cutoff=9.0, budget=150e9,
+    "c5w": dict(kind="serve", n_req=400, rate=20.0, steps_each=5000, cutoff=9.0, budget=150e9,
                 integrator="langevin", barostat=False, n_water=None),
     # as c4w / c5w with 0-3 ten-residue ff19SB peptides (and counter-ions,
     # bond-to-H constraints) in every member
     "c4": dict(kind="batch", n_sys=64, cutoff=9.0, integrator="langevin", barostat=False,
                n_water=None, peptides=3),
-    "c5": dict(kind="serve", n_req=48, rate=20.0, steps_each=5000, cutoff=9.0, budget=150e9,
+    "c5": dict(kind="serve", n_req=400, rate=20.0, steps_each=5000, cutoff=9.0, budget=150e9,
                integrator="langevin", barostat=False, n_water=None, peptides=3),
 }
 DEFAULT_WORKLOAD = "c3"
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one step's
-# short-range pair kernels (water-water, water-atom, atom-atom), from an
-# ncu --set full capture of the workload (cold L2, as in the timed loop,
-# which flushes L2 between steps)
-PAIR_DRAM_BYTES = {"c3w": 17306880, "c3": 17521920 + 4856576 + 905984}
 DT = 0.002
 
 
@@ -98,16 +93,32 @@ def build_system(name, seed):
     return sysd, cfg
 
 
-def member_system(w, n_water, seed, rng):
-    """One batched / served member: a water box, or with w["peptides"] a box
-    with 0..w["peptides"] ten-residue peptides (count drawn from rng)."""
+def _member_job(job):
+    """One batched / served member (run in a worker process): a water box,
+    or a box with n_pep ten-residue peptides."""
+    n_water, n_pep, seed = job
     from dynamics_b200 import synth
-    if w.get("peptides"):
+    if n_pep is not None:
         from dynamics_b200 import peptide
-        n_pep = int(rng.integers(0, w["peptides"] + 1))
-        sysd, grid, _ = peptide.batch_member(int(n_water), n_pep, seed=seed)
+        sysd, grid, _ = peptide.batch_member(int(n_water), int(n_pep), seed=seed)
         return sysd, grid
     return synth.batch_member(int(n_water), seed=seed)
+
+
+def build_members(w, sizes, seeds, rng):
+    """Members for the given sizes and seeds; with w["peptides"], each gets
+    0..w["peptides"] peptides (counts drawn from rng here, so the result does
+    not depend on the workers).  Built in parallel on the host cores by
+    spawned processes (no CUDA state is inherited)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    jobs = [(int(n), int(rng.integers(0, w["peptides"] + 1)) if w.get("peptides") else None, int(sd))
+            for n, sd in zip(sizes, seeds)]
+    workers = max(1, min(len(jobs), (os.cpu_count() or 1)))
+    if workers == 1 or len(jobs) < 4:
+        return [_member_job(j) for j in jobs]
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_member_job, jobs, chunksize=max(1, len(jobs) // (4 * workers))))
 
 
 def build_batch(name, seed):
@@ -117,8 +128,8 @@ def build_batch(name, seed):
     rng = np.random.default_rng(seed + 7919)
     systems, cfgs = [], []
     alpha = synth.ewald_alpha(w["cutoff"])
-    for i, n in enumerate(sizes):
-        sysd, grid = member_system(w, n, seed * 1000 + i, rng)
+    built = build_members(w, sizes, [seed * 1000 + i for i in range(len(sizes))], rng)
+    for i, (sysd, grid) in enumerate(built):
         cfg = md.MdConfig(coulomb_cutoff=w["cutoff"], lj_cutoff=w["cutoff"], spme_alpha=alpha,
                           spme_grid=grid, seed=seed * 1000 + i,
                           integrator=md.LangevinMiddle(gamma=1.0))
@@ -127,30 +138,28 @@ def build_batch(name, seed):
     return systems, cfgs
 
 
-def run_batch(args):
-    """Batched form: aggregate ns/day of all members advanced together,
-    against the same systems stepped one by one through the plain path."""
+def measure_batch(name, args, stream, dev, dist=None, rank=0, world=1):
+    """Batched form: aggregate ns/day of all members advanced together
+    (CUDA events around each batched step, 256 MiB L2 flush between steps),
+    against the same systems stepped one by one through the plain path, and
+    the end-to-end rate with every member's state in and out through host
+    memory each step.  Returns the fields of a JSON line."""
     import torch
 
     from dynamics_b200 import md
-    rank, world, local, dist = dist_setup(args.gpus)
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    stream = torch.cuda.Stream(dev)
-    torch.cuda.set_stream(stream)
-    name = args.workload
     w = WORKLOADS[name]
     systems, cfgs = build_batch(name, seed=1 + rank)
     systems = [md.equilibrate(s, c, n_steps=min(args.equil, 200), dt=0.001) for s, c in zip(systems, cfgs)]
     n_sys = len(systems)
     n_water = int(sum(len(s["water_pos"]) for s in systems))
     n_atoms = int(sum(len(s.get("atom_pos", ())) for s in systems))
+    steps = max(args.steps, 50)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     # ---- plain path, one system at a time (each its own graph per step) ----
-    k_plain = max(10, min(args.steps, 100))
+    k_plain = max(10, min(steps, 100))
     plain_ms = 0.0
-    for s, c in zip(systems, cfgs):
-        st = md.MdState(s, c, stream=stream.cuda_stream)
+    for sysd, c in zip(systems, cfgs):
+        st = md.MdState(sysd, c, stream=stream.cuda_stream)
         st.step(DT, args.warmup)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(dev)
@@ -165,26 +174,31 @@ def run_batch(args):
     batch.step(DT, args.warmup)
     torch.cuda.synchronize(dev)
     r0 = sum(m.energies()["list_rebuilds"] for m in batch.members)
-    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    clocks = ClockSampler(clock_csv(rank))
+    p0 = sum(m.energies()["list_prunes"] for m in batch.members)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    clocks = ClockSampler(clock_csv(rank) + ".batch")
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
     with clocks:
-        for k in range(args.steps):
+        for k in range(steps):
             flush.zero_()
             ev0[k].record(stream)
             batch.step(DT, 1)
             ev1[k].record(stream)
         torch.cuda.synchronize(dev)
     batch.sync()
-    ms = max_over_ranks(float(np.sum([ev0[k].elapsed_time(ev1[k]) for k in range(args.steps)])), dist, dev)
+    ms = max_over_ranks(float(np.sum([ev0[k].elapsed_time(ev1[k]) for k in range(steps)])), dist, dev)
     rebuilds = sum(m.energies()["list_rebuilds"] for m in batch.members) - r0
+    prunes = sum(m.energies()["list_prunes"] for m in batch.members) - p0
     fixed_s, reb_k, per_k = batch.launches(True)
     fixed_n, _, _ = batch.launches(False)
-    launches = (fixed_s + fixed_n) / 2.0 * args.steps + reb_k * min(rebuilds, args.steps)
-    value = aggregate_ns_per_day(args.steps, n_sys, world, ms)
+    # the batch's rebuild (and prune, 2 kernels) IF nodes fire on a step
+    # where any member needs them: at most one of each per step
+    launches = ((fixed_s + fixed_n) / 2.0 * steps + reb_k * min(rebuilds, steps)
+                + 2 * min(max(0, prunes - rebuilds), steps))
+    value = aggregate_ns_per_day(steps, n_sys, world, ms)
     plain_value = DT * 1e-3 * n_sys / (plain_ms * 1e-3) * 86400.0
     # ---- end to end: every member's positions/velocities in and out per step ----
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory().numpy()
@@ -193,7 +207,7 @@ def run_batch(args):
     for m in batch.members:
         s0 = m.state()
         host.append({k: pin(s0[k]) for k in keys if k in s0 and s0[k].size})
-    n_e2e = max(5, args.steps // 20)
+    n_e2e = max(5, steps // 10)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for _ in range(n_e2e):
@@ -207,128 +221,152 @@ def run_batch(args):
     t_e2e = time.perf_counter() - t0
     e2e_value = n_e2e * DT * 1e-3 * n_sys * world / t_e2e * 86400.0
     io_bytes = int(sum(a.nbytes for hb in host for a in hb.values()))
-    clk = clocks.summary(local)
     batch.close()
+    return {
+        "value": round(value, 2), "unit": "ns/day (aggregate over members)", "steps": steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / steps, 5),
+        "members": n_sys, "n_water_total": n_water, "n_atoms_total": n_atoms,
+        "member_steps_per_s": round(n_sys * steps / (ms * 1e-3), 1),
+        "plain_one_by_one": {"value": round(plain_value, 2), "unit": "ns/day (aggregate)",
+                             "ms_per_round": round(plain_ms, 4), "steps_each": k_plain},
+        "batch_over_plain": round(value / world / plain_value, 3),
+        "e2e": {"value": round(e2e_value, 2), "unit": "ns/day (aggregate)",
+                "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+        "gpu_launches": int(round(launches)),
+        "launches_per_step": {"spme": fixed_s, "no_spme": fixed_n, "rebuild_extra": reb_k, "periodic_extra": per_k},
+        "clocks": clocks.summary(0 if dev.index is None else dev.index),
+        "data": "synthetic (seeded OPC water boxes" + (", 0-3 ten-residue ff19SB peptides each"
+                                                        if w.get("peptides") else "")
+                + ", equilibrated on device)",
+        "config": {"workload": name, "sizes": "512-8000 waters, log-uniform", "cutoff_A": w["cutoff"],
+                   "grid": "FFT-friendly ~1 A", "integrator": "langevin_middle", "dt_fs": DT * 1e3,
+                   "l2": "256 MiB flush between timed steps"},
+    }
+
+
+def serve_requests(name, n_req, rate, steps_each, seed, pool_size, args):
+    """A Poisson(rate) stream of n_req requests, each a system drawn from a
+    pool of pool_size systems whose sizes follow the workload's size
+    distribution (built and equilibrated once), steps_each steps each."""
+    from dynamics_b200 import md, serve, synth
+    w = WORKLOADS[name]
+    sizes = synth.config4_sizes(pool_size, seed=seed)
+    rng = np.random.default_rng(seed + 7919)
+    built = build_members(w, sizes, [seed * 1000 + i for i in range(pool_size)], rng)
+    alpha = synth.ewald_alpha(w["cutoff"])
+    pool = []
+    for i, (sysd, grid) in enumerate(built):
+        cfg = md.MdConfig(coulomb_cutoff=w["cutoff"], lj_cutoff=w["cutoff"], spme_alpha=alpha, spme_grid=grid,
+                          seed=seed * 1000 + i, integrator=md.LangevinMiddle(gamma=1.0))
+        pool.append((md.equilibrate(sysd, cfg, n_steps=min(args.equil, 200), dt=0.001), cfg))
+    pick = np.random.default_rng(seed + 31).integers(0, pool_size, n_req)
+    arrivals = serve.poisson_arrivals(n_req, rate, seed=seed)
+    return pool, [(int(k), float(t)) for k, t in zip(pick, arrivals)]
+
+
+def serve_once(pool, stream_spec, steps_each, budget, max_members, stream):
+    from dynamics_b200 import md, serve
+    reqs = []
+    for rid, (k, t) in enumerate(stream_spec):
+        sysd, cfg = pool[k]
+        c = md.MdConfig(**{**cfg.__dict__, "seed": cfg.seed + 1000 * rid})
+        reqs.append(serve.Request(rid=rid, system=sysd, cfg=c, n_steps=steps_each, arrival=t))
+    srv = serve.Server(budget_bytes=budget, max_members=max_members, round_steps=100, dt=DT, stream=stream,
+                       keep_states=False)
+    rep = srv.run(reqs)
+    return {"value": round(rep.ns_per_day, 2), "unit": "ns/day (aggregate over requests)",
+            "latency_s": {k: round(v, 4) for k, v in rep.latency_s.items()},
+            "queue_wait_s": {k: round(v, 4) for k, v in rep.queue_wait_s.items()},
+            "wall_s": round(rep.wall_s, 3), "requests": len(reqs), "peak_members": rep.peak_members,
+            "peak_device_GB": round(rep.peak_bytes / 1e9, 3), "budget_waits": rep.budget_waits,
+            "member_steps": rep.steps_total}
+
+
+def measure_served(name, args, stream, capacity_req_per_s=None, n_req=400, steps_each=1000, pool_size=64,
+                   budget=3e9):
+    """Serving form: continuous batching of a Poisson stream at the workload's
+    rate (20 / s) and at a sustainable rate (half the measured batched
+    capacity), under a device-memory budget small enough to hold requests
+    back, against a real server run one request at a time."""
+    w = WORKLOADS[name]
+    rate = w["rate"]
+    pool, spec = serve_requests(name, n_req, rate, steps_each, 7, pool_size, args)
+    out = {"stream": {"requests": n_req, "steps_each": steps_each, "arrival_rate_per_s": rate,
+                      "pool": f"{pool_size} systems drawn from the c4 size distribution, equilibrated once; "
+                              "each request one of them with its own seed",
+                      "budget_GB": budget / 1e9, "round_steps": 100}}
+    out["at_rate"] = serve_once(pool, spec, steps_each, budget, 256, stream)
+    if capacity_req_per_s is None:
+        capacity_req_per_s = out["at_rate"]["member_steps"] / out["at_rate"]["wall_s"] / steps_each
+    sus = max(1.0, 0.5 * capacity_req_per_s)
+    from dynamics_b200 import serve
+    arr = serve.poisson_arrivals(n_req, sus, seed=8)
+    spec_s = [(k, float(t)) for (k, _), t in zip(spec, arr)]
+    out["sustainable"] = serve_once(pool, spec_s, steps_each, budget, 256, stream)
+    out["sustainable"]["arrival_rate_per_s"] = round(sus, 3)
+    out["one_at_a_time"] = serve_once(pool, spec, steps_each, budget, 1, stream)
+    out["one_at_a_time"]["note"] = "the same stream at the workload's rate, served by a server holding one member"
+    out["served_over_one_at_a_time"] = round(out["at_rate"]["value"] / out["one_at_a_time"]["value"], 3)
+    return out
+
+
+def run_batch(args):
+    """--workload c4 / c4w: the batched form's own JSON line."""
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    res = measure_batch(args.workload, args, stream, dev, dist, rank, world)
     if dist:
         dist.barrier()
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
-    out = {
-        "metric": "ns/day", "value": round(value, 2), "unit": "ns/day (aggregate over members)",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded OPC water boxes" + (", 0-3 ten-residue ff19SB peptides each"
-                                                        if w.get("peptides") else "")
-                + ", equilibrated on device)",
-        "config": {"workload": name, "members": n_sys, "n_water_total": n_water,
-                   "n_atoms_total": n_atoms, "sizes": "512-8000 waters, log-uniform", "cutoff_A": w["cutoff"],
-                   "grid": "FFT-friendly ~1 A", "integrator": "langevin_middle", "dt_fs": DT * 1e3,
-                   "l2": "256 MiB flush between timed steps", "parallelism": f"replicas x{world}"},
-        "plain_one_by_one": {"value": round(plain_value, 2), "unit": "ns/day (aggregate)",
-                             "ms_per_round": round(plain_ms, 4), "steps_each": k_plain,
-                             "batch_over_plain": round(value / world / plain_value, 3)},
-        "e2e": {"value": round(e2e_value, 2), "unit": "ns/day (aggregate)",
-                "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
-        "gpu_launches": int(round(launches)),
-        "launches_per_step": {"spme": fixed_s, "no_spme": fixed_n, "rebuild_extra": reb_k,
-                              "periodic_extra": per_k},
-        "clocks": clk, "cpu_baseline": None,
-    }
+    out = {"metric": "ns/day", "value": res["value"], "unit": res["unit"], "n_gpus": world, "steps": res["steps"],
+           "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": res["data"],
+           "config": {**res["config"], "members": res["members"], "parallelism": f"replicas x{world}"},
+           **{k: res[k] for k in ("plain_one_by_one", "batch_over_plain", "e2e", "gpu_launches",
+                                  "launches_per_step", "clocks", "n_water_total", "n_atoms_total")},
+           "cpu_baseline": None}
     print(json.dumps(out))
     if dist:
         dist.destroy_process_group()
 
 
 def run_serve(args):
-    """Serving form: p50/p99 completion latency, queue wait and aggregate
-    ns/day of a continuous-batching server, against the same requests served
-    one at a time through the plain path (first come, first served)."""
+    """--workload c5 / c5w: the serving form's own JSON line."""
     import torch
-
-    from dynamics_b200 import md, serve, synth
     rank, world, local, dist = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    name = args.workload
-    w = WORKLOADS[name]
-    seed = 7 + rank
-    sizes = synth.config4_sizes(w["n_req"], seed=seed)
-    arrivals = serve.poisson_arrivals(w["n_req"], w["rate"], seed=seed)
-    alpha = synth.ewald_alpha(w["cutoff"])
-    reqs = []
-    rng = np.random.default_rng(seed + 7919)
-    for i, (n, t) in enumerate(zip(sizes, arrivals)):
-        sysd, grid = member_system(w, n, seed * 1000 + i, rng)
-        cfg = md.MdConfig(coulomb_cutoff=w["cutoff"], lj_cutoff=w["cutoff"], spme_alpha=alpha, spme_grid=grid,
-                          seed=seed * 1000 + i, integrator=md.LangevinMiddle(gamma=1.0))
-        sysd = md.equilibrate(sysd, cfg, n_steps=min(args.equil, 200), dt=0.001)
-        reqs.append(serve.Request(rid=i, system=sysd, cfg=cfg, n_steps=w["steps_each"], arrival=float(t)))
-    # plain path, one request at a time: time each alone on a bounded sample
-    k_plain = max(20, min(args.steps, 500))
-    per_step = []
-    for r in reqs:
-        st = md.MdState(r.system, r.cfg, stream=stream.cuda_stream)
-        st.step(DT, args.warmup)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize(dev)
-        e0.record(stream)
-        st.step(DT, k_plain)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        per_step.append(e0.elapsed_time(e1) / k_plain * 1e-3)
-        st.close()
-    done = 0.0
-    lat_plain = []
-    for r, t in zip(reqs, per_step):
-        done = max(done, r.arrival) + t * r.n_steps
-        lat_plain.append(done - r.arrival)
-    plain_ns_day = sum(r.n_steps for r in reqs) * DT * 1e-3 / done * 86400.0
+    w = WORKLOADS[args.workload]
     clocks = ClockSampler(clock_csv(rank))
-    srv = serve.Server(budget_bytes=w["budget"], round_steps=100, dt=DT, stream=stream.cuda_stream,
-                       keep_states=False)
-    if dist:
-        dist.barrier()
     with clocks:
-        rep = srv.run(reqs)
-    clk = clocks.summary(local)
+        res = measure_served(args.workload, args, stream.cuda_stream, n_req=w["n_req"], steps_each=w["steps_each"],
+                             budget=w["budget"])
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
-    io = int(sum(r.system["water_pos"].nbytes + r.system["water_vel"].nbytes for r in reqs))
-    out = {
-        "metric": "ns/day", "value": round(rep.ns_per_day, 2), "unit": "ns/day (aggregate over requests)",
-        "n_gpus": world, "steps": rep.steps_total, "warmup": args.warmup,
-        "ms_per_step": round(rep.wall_s / rep.rounds / 100 * 1e3, 5), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded OPC water boxes" + (", 0-3 ten-residue ff19SB peptides each"
-                                                        if w.get("peptides") else "")
-                + ", equilibrated on device before arrival)",
-        "config": {"workload": name, "requests": len(reqs), "arrival_rate_per_s": w["rate"],
-                   "steps_each": w["steps_each"], "sizes": "512-8000 waters, log-uniform",
-                   "budget_GB": w["budget"] / 1e9, "round_steps": 100, "integrator": "langevin_middle",
-                   "dt_fs": DT * 1e3, "parallelism": f"replicas x{world}"},
-        "latency_s": {k: round(v, 4) for k, v in rep.latency_s.items()},
-        "queue_wait_s": {k: round(v, 4) for k, v in rep.queue_wait_s.items()},
-        "wall_s": round(rep.wall_s, 3), "peak_members": rep.peak_members,
-        "peak_device_GB": round(rep.peak_bytes / 1e9, 3),
-        "plain_one_at_a_time": {
-            "value": round(plain_ns_day, 2), "unit": "ns/day (aggregate)",
-            "latency_s": {"p50": round(float(np.percentile(lat_plain, 50)), 4),
-                          "p99": round(float(np.percentile(lat_plain, 99)), 4)},
-            "note": f"each request timed alone over {k_plain} steps and scaled to its step count, "
-                    "served first come first served"},
-        "e2e": {"value": round(rep.ns_per_day, 2), "unit": "ns/day (aggregate)", "h2d_bytes_per_step": None,
-                "d2h_bytes_per_step": None,
-                "note": f"inputs ({io} bytes in total) enter through the public API at admission and results "
-                        "leave at completion, inside the timed region"},
-        "clocks": clk, "cpu_baseline": None,
-    }
+    a = res["at_rate"]
+    out = {"metric": "ns/day", "value": a["value"], "unit": a["unit"], "n_gpus": world,
+           "steps": a["member_steps"], "warmup": args.warmup,
+           "ms_per_step": round(a["wall_s"] * 1e3 / max(1, a["member_steps"]), 6),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded OPC water boxes" + (", 0-3 ten-residue ff19SB peptides each"
+                                                           if w.get("peptides") else "") + ")",
+           "config": {"workload": args.workload, "parallelism": f"replicas x{world}", **res["stream"]},
+           "served": res, "e2e": {"value": a["value"], "unit": a["unit"], "h2d_bytes_per_step": None,
+                                  "d2h_bytes_per_step": None,
+                                  "note": "inputs enter through the public API at admission and results leave "
+                                          "at completion, inside the served wall time"},
+           "clocks": clocks.summary(local), "cpu_baseline": None}
     print(json.dumps(out))
     if dist:
         dist.destroy_process_group()
@@ -354,18 +392,20 @@ def count_pairs(sysd, cutoff):
         excl = set(map(tuple, np.sort(np.asarray(sysd["excl"], np.int64), axis=1).tolist()))
 
     def npairs(pts, mol, atom_id):
+        """(pairs, water-water pairs) within the cutoff."""
         t = cKDTree(np.mod(pts - lo, ext), boxsize=ext)
         p = t.query_pairs(cutoff, output_type="ndarray")
         keep = mol[p[:, 0]] != mol[p[:, 1]]
         p = p[keep]
+        n_ww = int(np.count_nonzero((mol[p[:, 0]] >= 0) & (mol[p[:, 1]] >= 0)))
         if excl:
             a, b = atom_id[p[:, 0]], atom_id[p[:, 1]]
             both = (a >= 0) & (b >= 0)
             if both.any():
                 pa = np.sort(np.stack([a[both], b[both]], 1), axis=1)
                 ex = np.array([tuple(x) in excl for x in pa.tolist()])
-                return int(len(p) - np.count_nonzero(ex))
-        return int(len(p))
+                return int(len(p) - np.count_nonzero(ex)), n_ww
+        return int(len(p)), n_ww
 
     ljm = np.asarray(sysd.get("atom_eps", np.zeros(na))) > 0
     qm = np.asarray(sysd.get("atom_q", np.zeros(na))) != 0
@@ -374,12 +414,12 @@ def count_pairs(sysd, cutoff):
     lj_pts = np.concatenate([o, ap[ljm]])
     lj_mol = np.concatenate([np.arange(nw), amol[ljm]])
     lj_id = np.concatenate([np.full(nw, -1), aid[ljm]])
-    n_lj = npairs(lj_pts, lj_mol, lj_id)
+    n_lj, n_lj_ww = npairs(lj_pts, lj_mol, lj_id)
     q_pts = np.concatenate([wp[:, 1], wp[:, 2], m, ap[qm]])
     q_mol = np.concatenate([np.tile(np.arange(nw), 3), amol[qm]])
     q_id = np.concatenate([np.full(3 * nw, -1), aid[qm]])
-    n_c = npairs(q_pts, q_mol, q_id)
-    return n_lj, n_c
+    n_c, n_c_ww = npairs(q_pts, q_mol, q_id)
+    return {"lj": n_lj, "coulomb": n_c, "lj_ww": n_lj_ww, "coulomb_ww": n_c_ww}
 
 
 class ClockSampler:
@@ -517,7 +557,11 @@ def run_ours(args):
     value = aggregate_ns_per_day(args.steps, 1, world, ms)
     # ---- stage timing and roofline of the dominant kernel ----
     stages = st.stage_times(DT, 40)
-    n_lj, n_c = count_pairs({**sysd, "water_pos": st.state()["water_pos"]}, w["cutoff"])
+    pc = count_pairs({**sysd, "water_pos": st.state()["water_pos"]}, w["cutoff"])
+    n_lj, n_c = pc["lj"], pc["coulomb"]
+    # the dominant kernel: water-water pairs only, per launch
+    ww_flops = pc["lj_ww"] * (19 + 15) + pc["coulomb_ww"] * (19 + 23)
+    ww_ms = stages["pairs_water_water"]
     flops = n_lj * (19 + 15) + n_c * (19 + 23)   # frozen per-pair convention
     pair_ms = stages["pairs"]
     achieved = flops / (pair_ms * 1e-3) / 1e12
@@ -529,6 +573,7 @@ def run_ours(args):
     K = np.prod(w["grid"])
     pme_bytes = nq * 16 + K * 4 + nq * 16 + K * 4 + nq * 12
     pme_ms = stages["spme"]
+    spread_bytes, gather_bytes = nq * 16 + K * 4, nq * 16 + K * 4 + nq * 12
     # ---- end-to-end through the host-buffer C-ABI step ----
     nw, na = st.n_water, st.n_atoms
     st_nw, st_na = nw, na
@@ -557,8 +602,10 @@ def run_ours(args):
               if (cfg.zero_com_drift and t % cfg.com_removal_interval == 0)
               or (cfg.reset_angle and t % 1000 == 0)
               or (cfg.recenter_sim_box and na and t % 30 == 0))
+    # a prune of the water-water lists without a rebuild adds its 2 kernels
+    prune_only = max(0, (en["list_prunes"] - e_before["list_prunes"]) - rebuilds)
     launches = ((st.launches_per_step(True) + st.launches_per_step(False)) / 2.0 * args.steps
-                + rebuilds * n_rebuild_k + due * n_periodic_k)
+                + rebuilds * n_rebuild_k + prune_only * 2 + due * n_periodic_k)
     clk = clocks.summary(local)
     st.close()
     if dist:
@@ -581,15 +628,17 @@ def run_ours(args):
         "data": "synthetic (seeded ff19SB peptide / ions / OPC water, equilibrated on device)"
                 if w.get("n_res") else "synthetic (seeded OPC water lattice, equilibrated on device)",
         "config": plain_config(name, cfg, st_nw, st_na, world),
-        "roofline": {"bound": "fp32", "kernel": "short-range pair kernels",
-                     "achieved": round(achieved, 3), "peak": round(peak.value, 2), "unit": "TFLOP/s",
-                     "frac": round(achieved / peak.value, 4), "traffic": PAIR_DRAM_BYTES.get(name),
-                     "peak_source": "measured FP32 FMA probe (dyn_probe_fp32_peak)",
-                     "algorithmic_flops": int(flops), "pairs_lj": n_lj, "pairs_coulomb": n_c},
-        "roofline_spme": {"bound": "hbm", "achieved": round(pme_bytes / (pme_ms * 1e-3) / 1e9, 1),
-                          "peak": hbm, "unit": "GB/s",
-                          "frac": round(pme_bytes / (pme_ms * 1e-3) / 1e9 / hbm, 4) if hbm else None,
-                          "note": "whole SPME stage incl. cuFFT; grid is L2-resident"},
+        "roofline": roofline_dominant(name, ww_flops, ww_ms, peak.value, pc),
+        "roofline_pair_stage": {"bound": "fp32", "kernel": "all short-range pair kernels",
+                                "achieved": round(achieved, 3), "peak": round(peak.value, 2), "unit": "TFLOP/s",
+                                "frac": round(achieved / peak.value, 4), "ms": round(pair_ms, 5),
+                                "algorithmic_flops": int(flops), "pairs_lj": n_lj, "pairs_coulomb": n_c},
+        "roofline_spme": {
+            "spread": hbm_roofline(spread_bytes, stages["spme_spread"], hbm, "k_spread + k_spread_w + k_fix2real"),
+            "gather": hbm_roofline(gather_bytes, stages["spme_gather"], hbm, "k_gather + k_gather_w + k_recip_pass"),
+            "stage": hbm_roofline(pme_bytes, pme_ms, hbm, "whole SPME stage incl. cuFFT"),
+            "note": "algorithmic bytes: spread N_q*16 + K^3*4, gather N_q*16 + K^3*4 + N_q*12; the grid stays "
+                    "in L2, so GB/s below HBM peak is expected"},
         "stage_ms": {k: round(v, 5) for k, v in stages.items()},
         "e2e": {"value": round(e2e_value, 2), "unit": "ns/day",
                 "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes + 256},
@@ -600,9 +649,54 @@ def run_ours(args):
                      "list_rebuilds": en["list_rebuilds"], "list_union_max": en["list_union_max"]},
         "wall_s": round(t_wall, 3),
     }
+    if world == 1 and not args.no_extras and name in ("c3", "c3w"):
+        # BASELINE's metric also asks for the batched and served forms beside
+        # the plain one: config 4 (64 members with peptides) and a config-5
+        # stream (400 requests of 1,000 steps; the c5 workload runs 5,000)
+        try:
+            b = measure_batch("c4", args, stream, dev)
+            out["batched"] = b
+            cap = b["member_steps_per_s"] / 1000.0
+            out["served"] = measure_served("c5", args, stream.cuda_stream, capacity_req_per_s=cap)
+        except Exception as e:  # reported, never fatal for the plain number
+            out["batched_or_served_error"] = f"{type(e).__name__}: {e}"[:300]
     print(json.dumps(out))
     if dist:
         dist.destroy_process_group()
+
+
+def profile_record(name):
+    """The ncu summary numbers committed under profiles/ for this workload:
+    {kernel: {dram_bytes_per_launch, ...}, "_source": file, "_captured": date}
+    (profiles/traffic_<workload>.json), or {}."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", f"traffic_{name}.json")))
+    except Exception:
+        return {}
+
+
+def roofline_dominant(name, flops, ms, peak, pc):
+    """FP32 roofline of the water-water pair kernel: algorithmic FLOPs of the
+    water-water site pairs inside the cutoff (19 + 15 per LJ pair, 19 + 23 per
+    Coulomb pair, each pair once) per launch over its event-timed duration;
+    traffic from the committed ncu capture of the same kernel."""
+    rec = profile_record(name)
+    k = rec.get("k_pair_ww_tile", {})
+    return {"bound": "fp32", "kernel": "k_pair_ww_tile (water-water pairs)",
+            "achieved": round(flops / (ms * 1e-3) / 1e12, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
+            "frac": round(flops / (ms * 1e-3) / 1e12 / peak, 4), "ms": round(ms, 5),
+            "traffic": k.get("dram_bytes_per_launch"),
+            "traffic_source": f"profiles/traffic_{name}.json ({rec.get('_captured', 'not captured')})",
+            "peak_source": "measured FP32 FMA probe (dyn_probe_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",
+            "algorithmic_flops": int(flops), "pairs_lj_ww": pc["lj_ww"], "pairs_coulomb_ww": pc["coulomb_ww"]}
+
+
+def hbm_roofline(nbytes, ms, peak, kernels):
+    if not ms or ms <= 0:
+        return None
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernels": kernels, "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(gbs / peak, 4) if peak else None, "ms": round(ms, 5), "algorithmic_bytes": int(nbytes)}
 
 
 def cpu_baseline(name, args, sysd=None):
@@ -691,6 +785,8 @@ def main():
     ap.add_argument("--equil", type=int, default=1000)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain line only (no batched / served sub-objects)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -21,6 +21,7 @@ DYN_ERR_TIMEOUT = -6
 DYN_ERR_UNSUPPORTED = -7
 
 DYN_NB_STATIC_MAX_SITES = 131072
+DYN_STAGES = 14
 DYN_OVR_COULOMB_DISABLED = 1
 DYN_OVR_LJ_DISABLED = 2
 DYN_PAIR_SCALE14 = 1

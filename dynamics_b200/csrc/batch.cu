@@ -355,7 +355,10 @@ extern "C" int dyn_batch_launches(dyn_batch_t b, int spme, uint32_t* fixed, uint
         return b->ctx.launches;
     };
     const uint32_t all = count([&] { enqueue_batch_step(b, 0.002f, spme != 0, true, false, 0, 0, 0); });
-    *rebuild = count([&] { dyn::launch_rebuild(T, false); });
+    *rebuild = count([&] {
+        dyn::launch_rebuild(T, false);
+        dyn::launch_prune(T, false);
+    });
     *periodic = count([&] { dyn::launch_periodic(T); });
     *fixed = all - *rebuild - *periodic;
     return upload_maps(b);

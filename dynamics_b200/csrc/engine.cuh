@@ -68,7 +68,7 @@ struct Scalars {
     unsigned int ctr_scale;       // blocks done in k_scale (last one scales the box)
     unsigned int union_max;       // largest group union of the last rebuild
     unsigned int a_sparse_base;   // first slot of the single-atom clusters
-    unsigned int aun_max;         // largest water-group atom union of the last rebuild
+    unsigned int n_ws_items;      // work items of the water-atom pair kernel
     unsigned int n_ss_items;      // work items of the atom-atom pair kernel
     double time_ps;               // simulated time (sum of the steps' dt)
     unsigned long long snap_count;  // snapshot frames recorded
@@ -136,22 +136,14 @@ struct SysView {
     uint32_t* wcol; uint32_t* acol;             // column of each water / atom
     // cluster bounding boxes (center xyz, half extent xyz)
     float4* wbb_c; float4* wbb_h; float4* abb_c; float4* abb_h;
-    // atom-atom cluster lists (fixed capacity per i cluster): atom cluster
-    // -> atom clusters (cj >= ci) with interaction masks; work items
-    // {i cluster, first entry} of CH_MIX list entries, in i order
-    uint32_t cap_ss;
+    // cluster lists (fixed capacity per i cluster): water cluster -> atom
+    // clusters, atom cluster -> atom clusters (cj >= ci) with masks; work
+    // items {i cluster, first entry} of CH_MIX list entries, in i order
+    uint32_t cap_ws, cap_ss;
+    uint32_t* ws_n; uint32_t* ws_j;
     uint32_t* ss_n; uint32_t* ss_j; unsigned long long* ss_mask;
-    uint2* ss_item;
-    uint32_t ss_item_cap;
-    // water-atom: per 32-water group the atom clusters near the group box
-    // (atile), the union of the atoms its waters reach (cluster-slot
-    // indices, staged in shared memory by the pair kernel, aun_chunk at a
-    // time), and per water a list of indices into that union
-    uint32_t cap_atile, cap_aun, cap_wal, aun_chunk;
-    uint32_t* atile_n; uint32_t* atile_j;    // [ngrp_cap], [ngrp_cap*cap_atile]
-    uint32_t* aun_n; uint32_t* aun_idx;      // [ngrp_cap], [ngrp_cap*cap_aun]
-    uint16_t* acand_loc;                     // [ngrp_cap*cap_atile*ACL] rebuild scratch
-    uint32_t* wal_n; uint16_t* wal;          // [nw_cap], [nw_cap*cap_wal]
+    uint2* ws_item; uint2* ss_item;
+    uint32_t ws_item_cap, ss_item_cap;
     // water-water: per 32-water i-group the candidate j-clusters (tile_j),
     // the union of the waters its members need, stored as runs of
     // consecutive slots (staged in shared memory by bulk copies), and per
@@ -207,6 +199,7 @@ struct SysView {
     // parameters
     float rc, rc2, ljc2, alpha, buffer;
     float r_ww, r_ws, r_ss;     // list radii
+    float r_ws_skip2;           // (cutoff + O-H reach)^2: water-atom entries beyond it are skipped
     float r_in, prune_buf;      // pruned water-water radius and its buffer
     uint32_t flags;
     uint64_t seed;
@@ -397,7 +390,10 @@ void launch_pairs(const Target& t, bool energy);
 // (the latter adds to the water forces the former stores), and atom-atom
 void launch_pairs_water(const Target& t, bool energy);
 void launch_pairs_atoms(const Target& t, bool energy);
-// the water-atom kernel alone (part of launch_pairs_water)
+// the parts of launch_pairs_water, in order: water-water, its j-side
+// gather, water-atom
+void launch_pairs_ww(const Target& t, bool energy);
+void launch_ww_gather(const Target& t);
 void launch_pairs_ws(const Target& t, bool energy);
 void launch_pair14(const Target& t, bool energy);
 int pair_ww_setup(const SysView& v);
@@ -406,13 +402,16 @@ size_t ww_tile_smem(const SysView& v);
 int ww_gather_blocks(const SysView& v);
 int pair_blocks_ss(const SysView& v);
 int pair_blocks_ws(const SysView& v);
-size_t ws_smem(const SysView& v);
 int pair14_blocks(const SysView& v);
 
 // pme.cu
 int pme_init(SysView& v, cufftHandle* plan_f, cufftHandle* plan_b, cudaStream_t st);
 void pme_free(SysView& v, cufftHandle plan_f, cufftHandle plan_b);
 void launch_pme(const Target& t);
+// the parts of one SPME pass (launch_pme runs them for every pass)
+void launch_pme_spread(const Target& t, int pass);
+void launch_pme_transform(const Target& t, int pass);
+void launch_pme_gather(const Target& t, int pass);
 void launch_corrections(const Target& t);
 int pme_blocks(const SysView& v);
 int gather_blocks(const SysView& v);

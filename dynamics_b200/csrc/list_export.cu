@@ -1,9 +1,9 @@
 // Read-out of the resident engine's neighbour lists (dyn_sys_list_pairs).
 //
-// The pair kernels never see a flat pair list: water-water and water-atom
-// pairs come from per-water lists of indices into a water group's union of
-// j-waters or atoms, atom-atom pairs from cluster-pair lists with 64-bit
-// interaction masks.  This expands the lists exactly as the kernels
+// The pair kernels never see a flat pair list: water-water pairs come from
+// per-water lists of indices into a water group's union of j-waters,
+// water-atom and atom-atom pairs from cluster-pair lists (the latter with
+// 64-bit interaction masks).  This expands the lists exactly as the kernels
 // walk them into pairs of original indices (water ids in the order the
 // system was created, atom indices), so that a test can check that every
 // pair inside the cutoff is covered (src/neighbors.rs:102-281 holds every
@@ -67,29 +67,25 @@ int ww_pairs(const SysView& v, const Scalars& sc, std::vector<uint32_t>& out) {
     return DYN_OK;
 }
 
-// water-atom: every (water, atom) pair of the per-water lists (indices into
-// the water group's atom union)
+// water-atom: every (water, atom) of the water-cluster x atom-cluster pairs
 int ws_pairs(const SysView& v, const Scalars& sc, std::vector<uint32_t>& out) {
-    const uint32_t ng = (sc.n_wclus + GRPW / WCL - 1) / (GRPW / WCL);
-    std::vector<uint32_t> wid, sidx, un_n, un, nl;
-    std::vector<uint16_t> l;
+    std::vector<uint32_t> wid, sidx, n, j;
     TRY_D2H(wid, v.wid, v.nw_cap);
     TRY_D2H(sidx, v.sidx, v.na_cap);
-    TRY_D2H(un_n, v.aun_n, ng);
-    TRY_D2H(un, v.aun_idx, (size_t)ng * v.cap_aun);
-    TRY_D2H(nl, v.wal_n, v.nw_cap);
-    TRY_D2H(l, v.wal, (size_t)v.nw_cap * v.cap_wal);
-    for (uint32_t g = 0; g < ng; ++g)
-        for (uint32_t il = 0; il < GRPW; ++il) {
-            const uint32_t s = g * GRPW + il;
-            if (s >= v.nw_cap || wid[s] == INVALID_ID) continue;
-            for (uint32_t k = 0; k < nl[s]; ++k) {
-                const uint32_t u = l[(size_t)s * v.cap_wal + k];
-                if (u >= un_n[g]) continue;
-                const uint32_t a = sidx[un[(size_t)g * v.cap_aun + u]];
-                if (a == INVALID_ID) continue;
-                out.push_back(wid[s]);
-                out.push_back(a);
+    TRY_D2H(n, v.ws_n, sc.n_wclus);
+    TRY_D2H(j, v.ws_j, (size_t)sc.n_wclus * v.cap_ws);
+    for (uint32_t ci = 0; ci < sc.n_wclus; ++ci)
+        for (uint32_t k = 0; k < n[ci]; ++k) {
+            const uint32_t cj = j[(size_t)ci * v.cap_ws + k];
+            for (uint32_t ii = 0; ii < WCL; ++ii) {
+                const uint32_t w = wid[ci * WCL + ii];
+                if (w == INVALID_ID) continue;
+                for (uint32_t jj = 0; jj < ACL; ++jj) {
+                    const uint32_t a = sidx[(size_t)cj * ACL + jj];
+                    if (a == INVALID_ID) continue;
+                    out.push_back(w);
+                    out.push_back(a);
+                }
             }
         }
     return DYN_OK;

@@ -111,7 +111,6 @@ DYN_KERNEL(, k_col_clear, (, bool force), (, force)) {
     if (bk.idx == 0 && threadIdx.x == 0) {
         v.sc->list_pairs = 0ull;
         v.sc->union_max = 0u;
-        v.sc->aun_max = 0u;
     }
     const uint32_t nc = v.ncol > v.ancol ? v.ncol : v.ancol;
     for (uint32_t c = bk.idx * blockDim.x + threadIdx.x; c < nc; c += bk.cnt * blockDim.x) {
@@ -328,27 +327,27 @@ __device__ __forceinline__ bool excluded(const SysView& v, uint32_t a, uint32_t 
     return lo < v.ex_off[a + 1] && v.ex_idx[lo] == b;
 }
 
-// One warp per i-cluster (MODE 3): atom i-clusters against atom j-clusters
-// with cj >= ci (each cluster pair once), with the interaction mask of the
-// cluster pair (jj > ii on the diagonal, exclusions removed).
+// One warp per i-cluster.  MODE 1: water i-clusters against atom
+// j-clusters; MODE 3: atom i-clusters against atom j-clusters with cj >= ci
+// (each cluster pair once), with the interaction mask of the cluster pair
+// (jj > ii on the diagonal, exclusions removed).
 DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
-    static_assert(MODE == 3, "atom-atom lists only");
     if (!rebuild_on(v, force)) return;
     const BoxDev b = *v.box;
     const int lane = threadIdx.x & 31;
     const uint32_t ci = (bk.idx * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t ni = v.sc->n_aclus;
+    const uint32_t ni = MODE == 1 ? v.sc->n_wclus : v.sc->n_aclus;
     const uint32_t nj = v.sc->n_aclus;
     if (ci >= ni) return;
     const float4* bcj = v.abb_c;
     const float4* bhj = v.abb_h;
-    const float r = v.r_ss;
+    const float r = MODE == 3 ? v.r_ss : v.r_ws;
     const float r2 = r * r;
-    const uint32_t cap = v.cap_ss;
-    uint32_t* out = v.ss_j;
-    uint32_t* outn = v.ss_n;
-    const float4 c0 = v.abb_c[ci];
-    const float4 h0 = v.abb_h[ci];
+    const uint32_t cap = MODE == 1 ? v.cap_ws : v.cap_ss;
+    uint32_t* out = MODE == 1 ? v.ws_j : v.ss_j;
+    uint32_t* outn = MODE == 1 ? v.ws_n : v.ss_n;
+    const float4 c0 = MODE == 1 ? v.wbb_c[ci] : v.abb_c[ci];
+    const float4 h0 = MODE == 1 ? v.wbb_h[ci] : v.abb_h[ci];
     uint32_t cnt = 0;
     for (uint32_t jb = MODE == 3 ? (ci & ~31u) : 0u; jb < nj; jb += 32) {
         const uint32_t cj = jb + lane;
@@ -397,12 +396,11 @@ DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
 // an exclusive scan of the per-cluster item counts, tile by tile.
 constexpr int IT_T = 1024;
 DYN_KERNEL_T((int MODE), (MODE), __launch_bounds__(IT_T), k_items, (, bool force), (, force)) {
-    static_assert(MODE == 3, "atom-atom work items only");
     if (!rebuild_on(v, force)) return;
-    const uint32_t ni = v.sc->n_aclus;
-    const uint32_t* cnt = v.ss_n;
-    uint2* items = v.ss_item;
-    const uint32_t icap = v.ss_item_cap;
+    const uint32_t ni = MODE == 1 ? v.sc->n_wclus : v.sc->n_aclus;
+    const uint32_t* cnt = MODE == 1 ? v.ws_n : v.ss_n;
+    uint2* items = MODE == 1 ? v.ws_item : v.ss_item;
+    const uint32_t icap = MODE == 1 ? v.ws_item_cap : v.ss_item_cap;
     __shared__ uint32_t wsum[IT_T / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t base = 0;
@@ -433,7 +431,10 @@ DYN_KERNEL_T((int MODE), (MODE), __launch_bounds__(IT_T), k_items, (, bool force
         base += wsum[IT_T / 32 - 1];
         __syncthreads();
     }
-    if (threadIdx.x == 0) v.sc->n_ss_items = min(base, icap);
+    if (threadIdx.x == 0) {
+        if (MODE == 1) v.sc->n_ws_items = min(base, icap);
+        else v.sc->n_ss_items = min(base, icap);
+    }
 }
 
 // Group bounding boxes over the O positions of the group's waters,
@@ -625,136 +626,6 @@ DYN_KERNEL(__launch_bounds__(UT), k_group_union, (, bool force), (, force)) {
 }
 
 // ---------------------------------------------------------------------------
-// Water-atom lists.  Per 32-water group (the water-water kernel's groups):
-// the atom clusters whose box lies within r_ws of the group box (one warp
-// per group, ballot compaction), then (one CTA per group) the union of the
-// atoms any member's O reaches within r_ws, numbered by a block-wide scan,
-// and for every member the ascending list of union indices of its atoms.
-// The union holds cluster-slot indices (into spos / slj / sidx).
-// ---------------------------------------------------------------------------
-DYN_KERNEL(, k_ws_tile, (, bool force), (, force)) {
-    if (!rebuild_on(v, force)) return;
-    const BoxDev b = *v.box;
-    const int lane = threadIdx.x & 31;
-    const uint32_t ng = (v.sc->n_wclus + GRPW / WCL - 1) / (GRPW / WCL);
-    const uint32_t nac = v.sc->n_aclus;
-    const uint32_t g = (bk.idx * blockDim.x + threadIdx.x) >> 5;
-    if (g >= ng) return;
-    const float4 c0 = v.gbb_c[g], h0 = v.gbb_h[g];
-    const float r2 = v.r_ws * v.r_ws;
-    uint32_t cnt = 0;
-    for (uint32_t jb = 0; jb < nac; jb += 32) {
-        const uint32_t cj = jb + lane;
-        const bool hit = cj < nac && bb_dist2(c0, h0, v.abb_c[cj], v.abb_h[cj], b) < r2;
-        const uint32_t m = __ballot_sync(0xffffffffu, hit);
-        if (hit) {
-            const uint32_t k = cnt + __popc(m & ((1u << lane) - 1u));
-            if (k < v.cap_atile) v.atile_j[(size_t)g * v.cap_atile + k] = cj;
-        }
-        cnt += __popc(m);
-    }
-    if (lane == 0) {
-        v.atile_n[g] = min(cnt, v.cap_atile);
-        if (cnt > v.cap_atile) atomicMax(&v.sc->overflow, cnt);
-    }
-}
-
-DYN_KERNEL(__launch_bounds__(UT), k_ws_union, (, bool force), (, force)) {
-    if (!rebuild_on(v, force)) return;
-    const BoxDev b = *v.box;
-    const float r2 = v.r_ws * v.r_ws;
-    const uint32_t ng = (v.sc->n_wclus + GRPW / WCL - 1) / (GRPW / WCL);
-    const int tid = threadIdx.x, lane = tid & 31, wid_ = tid >> 5;
-    __shared__ float4 io[GRPW];
-    __shared__ uint32_t wn[UT / 32];
-    __shared__ uint32_t base_cnt;
-    for (uint32_t g = bk.idx; g < ng; g += bk.cnt) {
-        if (tid < GRPW) {
-            const uint32_t s = g * GRPW + tid;
-            const bool ok = s < v.nw_cap && v.wid[s] != INVALID_ID;
-            const float4 p = ok ? v.wpos[4 * s] : make_float4(0.f, 0.f, 0.f, 0.f);
-            io[tid] = make_float4(p.x, p.y, p.z, ok ? 1.f : 0.f);
-        }
-        if (tid == 0) base_cnt = 0;
-        __syncthreads();
-        const uint32_t ncand = v.atile_n[g] * ACL;
-        const uint32_t* tl = v.atile_j + (size_t)g * v.cap_atile;
-        uint16_t* cl = v.acand_loc + (size_t)g * v.cap_atile * ACL;
-        uint32_t* un = v.aun_idx + (size_t)g * v.cap_aun;
-        // pass 1: atoms within r_ws of any member, numbered in candidate order
-        for (uint32_t c0 = 0; c0 < ncand; c0 += UT) {
-            const uint32_t k = c0 + tid;
-            bool need = false;
-            uint32_t cs = INVALID_ID;
-            if (k < ncand) {
-                cs = tl[k / ACL] * ACL + (k % ACL);
-                if (v.sidx[cs] != INVALID_ID) {
-                    const float3 pa = xyz(v.spos[cs]);
-                    for (int i = 0; i < GRPW && !need; ++i) {
-                        const float4 q = io[i];
-                        if (q.w == 0.f) continue;
-                        const float3 d = min_image_rint(pa - xyz(q), b);
-                        need = dot3(d, d) < r2;
-                    }
-                }
-            }
-            const uint32_t mn = __ballot_sync(0xffffffffu, need);
-            if (lane == 0) wn[wid_] = __popc(mn);
-            __syncthreads();
-            uint32_t on = 0;
-            for (int w = 0; w < wid_; ++w) on += wn[w];
-            const uint32_t loc = base_cnt + on + __popc(mn & ((1u << lane) - 1u));
-            if (k < ncand) cl[k] = need && loc < v.cap_aun ? (uint16_t)loc : (uint16_t)0xFFFFu;
-            if (need && loc < v.cap_aun) un[loc] = cs;
-            __syncthreads();
-            if (tid == 0) {
-                uint32_t tn = 0;
-                for (int w = 0; w < UT / 32; ++w) tn += wn[w];
-                base_cnt += tn;
-            }
-            __syncthreads();
-        }
-        if (tid == 0) {
-            v.aun_n[g] = min(base_cnt, v.cap_aun);
-            atomicMax(&v.sc->aun_max, base_cnt);
-            if (base_cnt > v.cap_aun) atomicMax(&v.sc->overflow, base_cnt);
-        }
-        __syncthreads();
-        // pass 2: per water, LPW lanes test LPW candidates at a time
-        const int il = tid / LPW, l = tid % LPW;
-        const uint32_t si = g * GRPW + il;
-        const float4 qi = io[il];
-        const unsigned gmask = ((1u << LPW) - 1u) << ((lane / LPW) * LPW);
-        uint32_t cnt = 0;
-        uint16_t* out = v.wal + (size_t)si * v.cap_wal;
-        for (uint32_t c0 = 0; c0 < ncand; c0 += LPW) {
-            const uint32_t k = c0 + l;
-            bool hit = false;
-            uint16_t loc = 0xFFFFu;
-            if (k < ncand && qi.w != 0.f) {
-                loc = cl[k];
-                if (loc != 0xFFFFu) {
-                    const uint32_t cs = tl[k / ACL] * ACL + (k % ACL);
-                    const float3 d = min_image_rint(xyz(v.spos[cs]) - xyz(qi), b);
-                    hit = dot3(d, d) < r2;
-                }
-            }
-            const uint32_t m = __ballot_sync(0xffffffffu, hit) & gmask;
-            if (hit) {
-                const uint32_t pos = cnt + __popc(m & ((1u << lane) - 1u));
-                if (pos < v.cap_wal) out[pos] = loc;
-            }
-            cnt += __popc(m);
-        }
-        if (l == 0 && si < v.nw_cap) {
-            v.wal_n[si] = qi.w != 0.f ? min(cnt, v.cap_wal) : 0u;
-            if (cnt > v.cap_wal) atomicMax(&v.sc->overflow, cnt);
-        }
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Pruning of the water-water lists (a dual pair list: Pall, Zhmurov,
 // Bauer, Abraham, Lundborg, Gray, Hess, Lindahl, J. Chem. Phys. 153, 134110
 // (2020)).  The rebuild's lists hold the molecule pairs with an O-O distance
@@ -879,15 +750,13 @@ void launch_rebuild(const Target& t, bool force) {
              force);
     t.launch(k_group_union, k_group_union_batch,
              [](const SysView& v) { return v.nw ? (int)std::min<uint32_t>(v.ngrp_cap, 148 * 8) : 0; }, UT, 0, force);
-    t.launch(k_ws_tile, k_ws_tile_batch,
-             [](const SysView& v) { return v.nw && v.na ? nblocks((uint64_t)v.ngrp_cap * 32, 128, 1 << 30) : 0; },
+    t.launch(k_list<1>, k_list_batch<1>,
+             [](const SysView& v) { return v.nw && v.na ? nblocks((uint64_t)v.nwclus_cap * 32, 128, 1 << 30) : 0; },
              LT, 0, force);
-    t.launch(k_ws_union, k_ws_union_batch,
-             [](const SysView& v) { return v.nw && v.na ? (int)std::min<uint32_t>(v.ngrp_cap, 148 * 8) : 0; }, UT, 0,
-             force);
     t.launch(k_list<3>, k_list_batch<3>,
              [](const SysView& v) { return v.na ? nblocks((uint64_t)v.naclus_cap * 32, 128, 1 << 30) : 0; }, LT, 0,
              force);
+    t.launch(k_items<1>, k_items_batch<1>, [](const SysView& v) { return v.nw && v.na ? 1 : 0; }, IT_T, 0, force);
     t.launch(k_items<3>, k_items_batch<3>, [](const SysView& v) { return v.na ? 1 : 0; }, IT_T, 0, force);
     t.launch(k_rebuild_done, k_rebuild_done_batch, [](const SysView&) { return 1; }, 1, 0, force);
 }

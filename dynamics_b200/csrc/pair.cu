@@ -485,137 +485,124 @@ __device__ __forceinline__ JAtoms load_jatoms(const SysView& v, uint32_t cj, int
 }
 
 // ---------------------------------------------------------------------------
-// water(i) - atom(j), each pair once.  One CTA per 32-water group (the
-// water-water kernel's groups).  The atoms the group's waters reach (its
-// atom union, cluster-slot indices from the rebuild) are gathered into
-// shared memory, aun_chunk at a time; each water is handled by LPW lanes
-// walking its list of union indices (O-atom distance below cutoff + O-H
-// reach + buffer at the rebuild).  The water forces stay in registers and
-// are added once per water (each water belongs to one group and no other
-// kernel writes them meanwhile); the atom forces are summed per union atom in
-// shared memory (int32 fixed point, as the water-water j sums) and added to
-// the atoms' int64 accumulators with three atomics per union atom.
+// water(i) - atom(j), each pair once.  One warp per work item (a water
+// i-cluster and CH_MIX entries of its atom-cluster list); the list entries
+// are read once per item (one per lane) and the next entry's j-atoms are
+// loaded while the current one is evaluated.  The water forces stay in
+// registers over the item; the j-atom forces (the opposite of the pair
+// forces) are reduce-scattered over the 8 water lanes of a j-group and added
+// with integer atomics (24 per entry).
 // ---------------------------------------------------------------------------
-constexpr int AT = GRPW * LPW;  // threads per CTA
-
-DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(AT, 2), k_pair_ws, (), ()) {
-    extern __shared__ __align__(16) float4 apos_s[];  // aun_chunk x (float4, float2, uint32, 3 int32)
-    const uint32_t chunk = v.aun_chunk;
-    float2* alj_s = reinterpret_cast<float2*>(apos_s + chunk);
-    uint32_t* aid_s = reinterpret_cast<uint32_t*>(alj_s + chunk);
-    int* aacc = reinterpret_cast<int*>(aid_s + chunk);  // [3][chunk]
-    const int tid = threadIdx.x;
-    const int il = tid / LPW, l = tid % LPW;
-    const uint32_t nwc = v.sc->n_wclus;
-    const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
-    const uint32_t nslots = nwc * WCL;
+DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT, 4), k_pair_ws, (), ()) {
+    const int lane = threadIdx.x & 31;
+    const int ii = lane & 7, jq = lane >> 3;
+    const uint32_t nwarps = (bk.cnt * blockDim.x) >> 5;
+    const uint32_t nit = v.sc->n_ws_items;
+    const uint32_t first_single = v.sc->a_sparse_base / ACL;  // first single-atom cluster
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     double el = 0.0, ec = 0.0, ew = 0.0, dh = 0.0;
-    for (uint32_t g = bk.idx; g < ng; g += bk.cnt) {
-        const uint32_t nun = v.aun_n[g];  // the same for the whole CTA
-        if (nun == 0) continue;
-        const uint32_t s = g * GRPW + il;
-        const bool have = s < nslots && v.wid[s] != INVALID_ID;
-        const uint32_t n = have ? v.wal_n[s] : 0u;
-        float3 iO = f3(0, 0, 0), iH0 = iO, iH1 = iO, iM = iO;
-        if (have) {
-            iO = xyz(v.wpos[4 * s + 0]); iH0 = xyz(v.wpos[4 * s + 1]);
-            iH1 = xyz(v.wpos[4 * s + 2]); iM = xyz(v.wpos[4 * s + 3]);
-        }
+    for (uint32_t it = ((bk.idx * blockDim.x + threadIdx.x) >> 5); it < nit; it += nwarps) {
+        const uint2 item = v.ws_item[it];
+        const uint32_t ci = item.x, k0 = item.y;
+        const uint32_t n = min(v.ws_n[ci], k0 + CH_MIX) - k0;
+        const uint32_t si = ci * WCL + ii;
+        const bool vi = v.wid[si] != INVALID_ID;
+        const float3 iO = xyz(v.wpos[4 * si + 0]), iH0 = xyz(v.wpos[4 * si + 1]);
+        const float3 iH1 = xyz(v.wpos[4 * si + 2]), iM = xyz(v.wpos[4 * si + 3]);
         float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
         Acc3 a{0.0, 0.0, 0.f, 0.0};
-        const uint16_t* lst = v.wal + (size_t)s * v.cap_wal;
-        uint32_t k = l;
-        uint32_t idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
-        const uint32_t* un = v.aun_idx + (size_t)g * v.cap_aun;
-        for (uint32_t lo = 0; lo < nun; lo += chunk) {
-            const uint32_t hi = min(nun, lo + chunk);
-            for (uint32_t t = tid; t < hi - lo; t += AT) {
-                const uint32_t cs = un[lo + t];
-                apos_s[t] = v.spos[cs];
-                alj_s[t] = v.slj[cs];
-                aid_s[t] = v.sidx[cs];
-            }
-            for (uint32_t t = tid; t < 3 * chunk; t += AT) aacc[t] = 0;
-            __syncthreads();
-            while (idx_next < hi) {
-                const uint32_t idx = idx_next;
-                k += LPW;
-                idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
-                const uint32_t u = idx - lo;
-                const float4 pj = apos_s[u];
-                const float2 lj_j = alj_s[u];
-                const uint32_t aj = aid_s[u];
-                const float3 jp = xyz(pj);
-                // the atom moved by the shift once, then zero shift
-                const float3 js = jp - shift_of(iO - jp, b), z0 = f3(0.f, 0.f, 0.f);
-                const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
-                const float ep = sqrtf(OPC_O_EPS * lj_j.y);
-                const double qe = (double)pj.w;
-                float3 fo = z0, f0 = z0, f1 = z0, fm = z0;
-                if (ALCH && aj >= v.alch_lo && aj < v.alch_hi) {
-                    // a water and an atom of the alchemical molecule
-                    lj_soft<ENERGY>(iO, js, z0, sg, ep, ljc2, v.alch_ll, v.alch_dll, fo, a, dh);
-                    Acc3 t{0.0, 0.0, 0.f, 0.0};
-                    coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, t);
-                    coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, t);
-                    coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, t);
-                    const float cs = v.alch_cs;
-                    f0 = f0 * cs; f1 = f1 * cs; fm = fm * cs;
-                    a.w = fmaf(cs, t.w, a.w);
-                    if (ENERGY) { a.e_c += (double)cs * t.e_c; dh += (double)v.alch_dcs * t.e_c; }
-                } else {
-                    lj<ENERGY>(iO, js, z0, sg * sg, ep, ljc2, 1.0f, fo, a);
-                    coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
-                    coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
-                    coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
+        const uint32_t my_j = (uint32_t)lane < n ? v.ws_j[(size_t)ci * v.cap_ws + k0 + lane] : 0u;
+        // Single-atom clusters (ions) come last in every list.  Four of them
+        // are taken per iteration, one per lane group jq (its atom in the
+        // h = 0 slot), instead of one cluster with seven empty slots.
+        auto load_at = [&](uint32_t k) -> JAtoms {
+            const uint32_t c0 = __shfl_sync(0xffffffffu, my_j, k);
+            const uint32_t kk = k + (uint32_t)jq;
+            const uint32_t cq = __shfl_sync(0xffffffffu, my_j, kk < n ? kk : k);
+            if (c0 < first_single) return load_jatoms(v, c0, jq);
+            const uint32_t sq = cq * ACL;
+            return JAtoms{v.spos[sq], make_float4(0.f, 0.f, 0.f, 0.f), v.slj[sq], make_float2(0.f, 0.f),
+                          kk < n ? v.sidx[sq] : INVALID_ID, INVALID_ID};
+        };
+        auto advance = [&](uint32_t k) -> uint32_t {
+            return __shfl_sync(0xffffffffu, my_j, k) < first_single ? 1u : 4u;
+        };
+        JAtoms nx = load_at(0);
+        for (uint32_t k = 0; k < n;) {
+            const JAtoms cur = nx;
+            k += advance(k);
+            if (k < n) nx = load_at(k);
+            // the cluster boxes met within r_ws; skip the entry when no lane's
+            // water O lies within cutoff + O-H reach of its atoms
+            {
+                const float r2 = v.r_ws_skip2;
+                bool near = false;
+                if (vi && cur.a0 != INVALID_ID) {
+                    const float3 d = min_image_rint(iO - xyz(cur.p0), b);
+                    near = dot3(d, d) < r2;
                 }
-                a.flush_w();
+                if (vi && cur.a1 != INVALID_ID) {
+                    const float3 d = min_image_rint(iO - xyz(cur.p1), b);
+                    near = near || dot3(d, d) < r2;
+                }
+                if (!__any_sync(0xffffffffu, near)) continue;
+            }
+            float jf[8];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const float4 pj = h ? cur.p1 : cur.p0;
+                const float2 lj_j = h ? cur.l1 : cur.l0;
+                const uint32_t aj = h ? cur.a1 : cur.a0;
+                float3 fo = f3(0, 0, 0), f0 = fo, f1 = fo, fm = fo;
+                if (vi && aj != INVALID_ID) {
+                    const float3 jp = xyz(pj);
+                    // the atom moved by the shift once, then zero shift
+                    const float3 js = jp - shift_of(iO - jp, b), z0 = f3(0.f, 0.f, 0.f);
+                    const float sg = 0.5f * (OPC_O_SIGMA + lj_j.x);
+                    const float ep = sqrtf(OPC_O_EPS * lj_j.y);
+                    const double qe = (double)pj.w;
+                    if (ALCH && aj >= v.alch_lo && aj < v.alch_hi) {
+                        // a water and an atom of the alchemical molecule
+                        lj_soft<ENERGY>(iO, js, z0, sg, ep, ljc2, v.alch_ll, v.alch_dll, fo, a, dh);
+                        Acc3 t{0.0, 0.0, 0.f, 0.0};
+                        coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, t);
+                        coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, t);
+                        coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, t);
+                        const float cs = v.alch_cs;
+                        f0 = f0 * cs; f1 = f1 * cs; fm = fm * cs;
+                        a.w = fmaf(cs, t.w, a.w);
+                        if (ENERGY) { a.e_c += (double)cs * t.e_c; dh += (double)v.alch_dcs * t.e_c; }
+                    } else {
+                        lj<ENERGY>(iO, js, z0, sg * sg, ep, ljc2, 1.0f, fo, a);
+                        coul<ENERGY>(iH0, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f0, a);
+                        coul<ENERGY>(iH1, js, z0, OPC_Q_H * pj.w, (double)OPC_Q_H * qe, v, f1, a);
+                        coul<ENERGY>(iM, js, z0, OPC_Q_EP * pj.w, (double)OPC_Q_EP * qe, v, fm, a);
+                    }
+                }
                 fO = fO + fo; fH0 = fH0 + f0; fH1 = fH1 + f1; fM = fM + fm;
-                // the atom receives the opposite of the water's force
                 const float3 t = (fo + f0) + (f1 + fm);
-                if (fmaxf(fabsf(t.x), fmaxf(fabsf(t.y), fabsf(t.z))) < JFIX_MAX) {
-                    atomicAdd(aacc + 0 * (size_t)chunk + u, __float2int_rn(-t.x * JFIX_SCALE));
-                    atomicAdd(aacc + 1 * (size_t)chunk + u, __float2int_rn(-t.y * JFIX_SCALE));
-                    atomicAdd(aacc + 2 * (size_t)chunk + u, __float2int_rn(-t.z * JFIX_SCALE));
-                } else {
-                    add_fix3(v.aforce + 3 * (size_t)aj, f3(-t.x, -t.y, -t.z));
-                }
+                jf[3 * h + 0] = -t.x; jf[3 * h + 1] = -t.y; jf[3 * h + 2] = -t.z;
             }
-            __syncthreads();  // every atom sum of the chunk is in
-            for (uint32_t t = tid; t < hi - lo; t += AT) {
-                long long* fa = v.aforce + 3 * (size_t)aid_s[t];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const int q = aacc[c * chunk + t];
-                    if (q != 0) fix_atomic_add(fa + c, (long long)q * (1ll << (32 - WW_JFIX_SHIFT)));
-                }
+            jf[6] = 0.f; jf[7] = 0.f;
+            a.flush_w();
+            // lane ii < 6 now holds component ii % 3 of the group's j-atom a0 (ii < 3) or a1
+            reduce_scatter8(jf, ii);
+            if (ii < 6) {
+                const uint32_t aj = ii < 3 ? cur.a0 : cur.a1;
+                if (aj != INVALID_ID) add_fix(v.aforce + 3 * (size_t)aj + ii % 3, jf[0]);
             }
-            __syncthreads();  // the shared buffers are refilled by the next chunk or group
         }
-#pragma unroll
-        for (int o = 1; o < LPW; o <<= 1) {
-            fO.x += __shfl_xor_sync(0xffffffffu, fO.x, o); fO.y += __shfl_xor_sync(0xffffffffu, fO.y, o);
-            fO.z += __shfl_xor_sync(0xffffffffu, fO.z, o);
-            fH0.x += __shfl_xor_sync(0xffffffffu, fH0.x, o); fH0.y += __shfl_xor_sync(0xffffffffu, fH0.y, o);
-            fH0.z += __shfl_xor_sync(0xffffffffu, fH0.z, o);
-            fH1.x += __shfl_xor_sync(0xffffffffu, fH1.x, o); fH1.y += __shfl_xor_sync(0xffffffffu, fH1.y, o);
-            fH1.z += __shfl_xor_sync(0xffffffffu, fH1.z, o);
-            fM.x += __shfl_xor_sync(0xffffffffu, fM.x, o); fM.y += __shfl_xor_sync(0xffffffffu, fM.y, o);
-            fM.z += __shfl_xor_sync(0xffffffffu, fM.z, o);
-        }
-        if (l == 0 && have && n > 0) {
-            long long* p = v.wforce + (size_t)s * 12;
-            const float3 fs[4] = {fO, fH0, fH1, fM};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                p[3 * q + 0] += fix_from_float(fs[q].x);
-                p[3 * q + 1] += fix_from_float(fs[q].y);
-                p[3 * q + 2] += fix_from_float(fs[q].z);
-            }
+        fO = f3(red4(fO.x), red4(fO.y), red4(fO.z));
+        fH0 = f3(red4(fH0.x), red4(fH0.y), red4(fH0.z));
+        fH1 = f3(red4(fH1.x), red4(fH1.y), red4(fH1.z));
+        fM = f3(red4(fM.x), red4(fM.y), red4(fM.z));
+        if (jq == 0 && vi) {
+            long long* p = v.wforce + (size_t)si * 12;
+            add_fix3(p + 0, fO); add_fix3(p + 3, fH0); add_fix3(p + 6, fH1); add_fix3(p + 9, fM);
         }
         if (ENERGY) { el += a.e_lj; ec += a.e_c; }
+        a.flush_w();
         ew += a.wd;
     }
     write_partials<ENERGY>(v, bk, REG_WS, el, ec, ew, dh);
@@ -741,14 +728,7 @@ inline int pblocks(const SysView& v, uint64_t warps) {
 
 namespace dyn {
 
-int pair_blocks_ws(const SysView& v) {
-    return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
-}
-
-// per staged atom: position and charge, sigma / eps, index, 3 int32 sums
-size_t ws_smem(const SysView& v) {
-    return (size_t)v.aun_chunk * (sizeof(float4) + sizeof(float2) + sizeof(uint32_t) + 3 * sizeof(int));
-}
+int pair_blocks_ws(const SysView& v) { return pblocks(v, v.ws_item_cap); }
 
 int ww_tile_blocks(const SysView& v) {
     return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
@@ -776,17 +756,6 @@ int pair_ww_setup(const SysView& v) {
         DYN_CUDA(cudaFuncGetAttributes(&fa, k));
         const int lim = optin - (int)fa.sharedSizeBytes;
         DYN_CHECK(ww_tile_smem(v) <= (size_t)lim, DYN_ERR_UNSUPPORTED, "water-water chunk exceeds shared memory");
-        DYN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    }
-    const void* ka[8] = {(const void*)k_pair_ws<true, true>, (const void*)k_pair_ws<true, false>,
-                         (const void*)k_pair_ws<false, true>, (const void*)k_pair_ws<false, false>,
-                         (const void*)k_pair_ws_batch<true, true>, (const void*)k_pair_ws_batch<true, false>,
-                         (const void*)k_pair_ws_batch<false, true>, (const void*)k_pair_ws_batch<false, false>};
-    for (const void* k : ka) {
-        cudaFuncAttributes fa;
-        DYN_CUDA(cudaFuncGetAttributes(&fa, k));
-        const int lim = optin - (int)fa.sharedSizeBytes;
-        DYN_CHECK(ws_smem(v) <= (size_t)lim, DYN_ERR_UNSUPPORTED, "water-atom chunk exceeds shared memory");
         DYN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     }
     return DYN_OK;
@@ -817,7 +786,7 @@ void launch_pairs_atoms(const Target& t, bool energy) {
     else t.launch(k_pair_ss<false, false>, k_pair_ss_batch<false, false>, ss, PT, 0);
 }
 
-void launch_pairs_water(const Target& t, bool energy) {
+void launch_pairs_ww(const Target& t, bool energy) {
     const size_t sm = t.max_over([](const SysView& v) { return v.nw ? ww_tile_smem(v) : (size_t)0; });
     // water-water short-range energy is part of the potential only with
     // DYN_FLAG_FULL_ENERGY (the reference leaves it out,
@@ -827,20 +796,27 @@ void launch_pairs_water(const Target& t, bool energy) {
              [&](const SysView& v) { return v.nw && eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
     t.launch(k_pair_ww_tile<false>, k_pair_ww_tile_batch<false>,
              [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
+}
+
+void launch_ww_gather(const Target& t) {
+    t.launch(k_ww_gather, k_ww_gather_batch, [](const SysView& v) { return v.nw ? ww_gather_blocks(v) : 0; }, GT, 0);
+}
+
+void launch_pairs_water(const Target& t, bool energy) {
+    launch_pairs_ww(t, energy);
     // the j-side sums and the water-atom forces are added to the water
     // forces the water-water kernel stores
-    t.launch(k_ww_gather, k_ww_gather_batch, [](const SysView& v) { return v.nw ? ww_gather_blocks(v) : 0; }, GT, 0);
+    launch_ww_gather(t);
     launch_pairs_ws(t, energy);
 }
 
 void launch_pairs_ws(const Target& t, bool energy) {
     auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
-    const size_t sm = t.max_over([](const SysView& v) { return v.nw && v.na ? ws_smem(v) : (size_t)0; });
     const bool al = any_alch(t);
-    if (energy && al) t.launch(k_pair_ws<true, true>, k_pair_ws_batch<true, true>, ws, AT, sm);
-    else if (energy) t.launch(k_pair_ws<true, false>, k_pair_ws_batch<true, false>, ws, AT, sm);
-    else if (al) t.launch(k_pair_ws<false, true>, k_pair_ws_batch<false, true>, ws, AT, sm);
-    else t.launch(k_pair_ws<false, false>, k_pair_ws_batch<false, false>, ws, AT, sm);
+    if (energy && al) t.launch(k_pair_ws<true, true>, k_pair_ws_batch<true, true>, ws, PT, 0);
+    else if (energy) t.launch(k_pair_ws<true, false>, k_pair_ws_batch<true, false>, ws, PT, 0);
+    else if (al) t.launch(k_pair_ws<false, true>, k_pair_ws_batch<false, true>, ws, PT, 0);
+    else t.launch(k_pair_ws<false, false>, k_pair_ws_batch<false, false>, ws, PT, 0);
 }
 
 void launch_pair14(const Target& t, bool energy) {

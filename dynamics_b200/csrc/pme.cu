@@ -106,21 +106,153 @@ __device__ __forceinline__ float pass_weight(const SysView& v, int pass) {
     return pass == 0 ? v.alch_cs : 1.0f - v.alch_cs;
 }
 
-// one thread per charged site: atoms (q != 0), then water H0, H1, M
+// one thread per charged atom (the water sites go by group, below)
 DYN_KERNEL(, k_spread, (, int pass), (, pass)) {
     const BoxDev b = *v.box;
-    const uint32_t total = v.na + (pass == 2 ? 0u : 3 * v.nw_cap);
-    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
-        if (t < v.na) {
-            const float4 p = v.apos[t];
-            if (p.w != 0.f && pass_has_atom(v, pass, t)) spread_one(v, xyz(p), p.w, b);
-        } else {
-            const uint32_t k = t - v.na;
-            const uint32_t s = k / 3, site = 1 + k % 3;
-            if (v.wid[s] == INVALID_ID) continue;
-            const float4 p = v.wpos[4 * s + site];
-            spread_one(v, xyz(p), p.w, b);
+    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < v.na; t += bk.cnt * blockDim.x) {
+        const float4 p = v.apos[t];
+        if (p.w != 0.f && pass_has_atom(v, pass, t)) spread_one(v, xyz(p), p.w, b);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Water sites by water group.  A CTA takes a 32-water group of the pair
+// kernels (spatially compact): the order-4 stencils of its 96 charged sites
+// fall in a small box of grid points, held in shared memory.  The spread
+// adds every contribution there (the same int64 fixed-point values as one
+// global atomic per contribution would add: integer sums in any order, so
+// the grid is bit-identical) and then adds the box's nonzero points to the
+// global grid, about half as many global atomics; the gather stages the
+// box once with coalesced loads and reads the stencils from shared memory
+// (the same float arithmetic in the same order as per site).  A group whose
+// box exceeds the tile (scattered waters in a dilute system) takes the
+// per-site path.
+// ---------------------------------------------------------------------------
+constexpr int SG_T = 128;               // threads per CTA
+constexpr int SG_SITES = 3 * GRPW;      // charged sites of a group
+constexpr int TILE_PTS = 4096;          // shared tile capacity (grid points)
+
+struct GroupSites {
+    int base[SG_SITES][3];              // stencil base of each site
+    double w[SG_SITES][3];              // fractional grid coordinate
+    float3 pos[SG_SITES];
+    float q[SG_SITES];                  // 0: no site (padding slot)
+    int lo[3], n[3];                    // tile origin (relative to ref) and size
+    int ref[3];                         // base of the first site
+    int use_tile;
+};
+
+// Fills the group's sites and its tile box (whole CTA; ends synchronised).
+__device__ __forceinline__ void group_sites(const SysView& v, uint32_t g, const BoxDev& b, GroupSites& gs) {
+    const int tid = threadIdx.x;
+    if (tid < 3) { gs.lo[tid] = 1 << 30; gs.n[tid] = -(1 << 30); }
+    for (int t = tid; t < SG_SITES; t += SG_T) {
+        const uint32_t s = g * GRPW + t / 3;
+        const bool ok = s < v.nw_cap && v.wid[s] != INVALID_ID;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ok) p = v.wpos[4 * s + 1 + t % 3];
+        gs.pos[t] = xyz(p);
+        gs.q[t] = ok ? p.w : 0.f;
+        int bs[3];
+        double ww[3];
+        grid_coord(xyz(p), b, v.K, bs, ww);
+        for (int a = 0; a < 3; ++a) { gs.base[t][a] = bs[a]; gs.w[t][a] = ww[a]; }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int f = 0;
+        while (f < SG_SITES && gs.q[f] == 0.f) ++f;
+        for (int a = 0; a < 3; ++a) gs.ref[a] = f < SG_SITES ? gs.base[f][a] : 0;
+    }
+    __syncthreads();
+    for (int t = tid; t < SG_SITES; t += SG_T) {
+        if (gs.q[t] == 0.f) continue;
+        for (int a = 0; a < 3; ++a) {
+            const int K = (int)v.K[a];
+            int r = gs.base[t][a] - gs.ref[a];
+            r -= K * (int)floorf((float)r / (float)K + 0.5f);  // nearest image, |r| <= K/2
+            atomicMin(&gs.lo[a], r - 3);
+            atomicMax(&gs.n[a], r);
         }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        long long pts = 1;
+        bool fits = true;
+        for (int a = 0; a < 3; ++a) {
+            gs.n[a] = gs.n[a] - gs.lo[a] + 1;
+            fits = fits && gs.n[a] > 0 && gs.n[a] <= (int)v.K[a];
+            pts *= gs.n[a] > 0 ? gs.n[a] : 0;
+        }
+        gs.use_tile = fits && pts > 0 && pts <= TILE_PTS;
+    }
+    __syncthreads();
+}
+
+// tile offset of a site's stencil point (a, bb, c) and the grid index of a tile point
+__device__ __forceinline__ int rel_base(const SysView& v, const GroupSites& gs, int t, int a) {
+    const int K = (int)v.K[a];
+    int r = gs.base[t][a] - gs.ref[a];
+    r -= K * (int)floorf((float)r / (float)K + 0.5f);
+    return r - gs.lo[a];
+}
+__device__ __forceinline__ size_t tile_to_grid(const SysView& v, const GroupSites& gs, int idx) {
+    const int z = idx % gs.n[2], y = (idx / gs.n[2]) % gs.n[1], x = idx / (gs.n[2] * gs.n[1]);
+    int gi[3] = {x, y, z};
+    for (int a = 0; a < 3; ++a) {
+        const int K = (int)v.K[a];
+        int u = gs.ref[a] + gs.lo[a] + gi[a];
+        u %= K;
+        if (u < 0) u += K;
+        gi[a] = u;
+    }
+    return ((size_t)gi[0] * v.K[1] + gi[1]) * v.K[2] + gi[2];
+}
+
+DYN_KERNEL(__launch_bounds__(SG_T), k_spread_w, (, int pass), (, pass)) {
+    if (pass == 2) return;  // the alchemical molecule's own pass holds no water
+    __shared__ GroupSites gs;
+    __shared__ unsigned long long tile[TILE_PTS];
+    const BoxDev b = *v.box;
+    const uint32_t ng = (v.sc->n_wclus + GRPW / WCL - 1) / (GRPW / WCL);
+    const int tid = threadIdx.x;
+    for (uint32_t g = bk.idx; g < ng; g += bk.cnt) {
+        group_sites(v, g, b, gs);
+        if (!gs.use_tile) {
+            for (int t = tid; t < SG_SITES; t += SG_T)
+                if (gs.q[t] != 0.f) spread_one(v, gs.pos[t], gs.q[t], b);
+            __syncthreads();
+            continue;
+        }
+        const int npts = gs.n[0] * gs.n[1] * gs.n[2];
+        for (int i = tid; i < npts; i += SG_T) tile[i] = 0ull;
+        __syncthreads();
+        // one (site, x plane) per thread and round: 16 contributions each
+        for (int u = tid; u < SG_SITES * 4; u += SG_T) {
+            const int t = u >> 2, a = u & 3;
+            if (gs.q[t] == 0.f) continue;
+            double tx[4], ty[4], tz[4];
+            bspline4d(gs.w[t][0], tx);
+            bspline4d(gs.w[t][1], ty);
+            bspline4d(gs.w[t][2], tz);
+            const int x = rel_base(v, gs, t, 0) - 3 + a;
+            const int y0 = rel_base(v, gs, t, 1) - 3, z0 = rel_base(v, gs, t, 2) - 3;
+            const double qa = (double)gs.q[t] * tx[a];
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb) {
+                const double qab = qa * ty[bb];
+                const int row = (x * gs.n[1] + (y0 + bb)) * gs.n[2] + z0;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    atomicAdd(&tile[row + c], (unsigned long long)fix_from_double(qab * tz[c]));
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < npts; i += SG_T) {
+            const long long q = (long long)tile[i];
+            if (q != 0) fix_atomic_add(v.qgrid_fix + tile_to_grid(v, gs, i), q);
+        }
+        __syncthreads();
     }
 }
 
@@ -220,38 +352,94 @@ __device__ __forceinline__ double excl_corr(double dx, double dy, double dz, dou
     return -qq * er / r;
 }
 
-// Gather: one thread per atom, or per water (its H0, H1, M), writing the
-// reciprocal cache.  With Ewald corrections on, the intra-water exclusion
-// corrections (H0-H1, H0-M, H1-M) are added here in float64.
+// Gather for the atoms: one thread per atom, writing the reciprocal cache.
 // Pass 0 stores its (weighted) forces, later passes add theirs.
 DYN_KERNEL(, k_gather, (, int pass), (, pass)) {
     const BoxDev b = *v.box;
+    const float wt = pass_weight(v, pass);
+    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < v.na; t += bk.cnt * blockDim.x) {
+        if (!pass_has_atom(v, pass, t)) continue;
+        const float4 p = v.apos[t];
+        float3 f = f3(0.f, 0.f, 0.f);
+        if (p.w != 0.f) f = gather_one(v, xyz(p), p.w, b) * wt;
+        long long* c = v.arecip + 3 * (size_t)t;
+        if (pass == 0) {
+            c[0] = fix_from_float(f.x); c[1] = fix_from_float(f.y); c[2] = fix_from_float(f.z);
+        } else {
+            c[0] += fix_from_float(f.x); c[1] += fix_from_float(f.y); c[2] += fix_from_float(f.z);
+        }
+    }
+}
+
+// The gather of one site from a staged tile: gather_one's arithmetic, in its
+// order, with the grid values read from shared memory.
+__device__ __forceinline__ float3 gather_tile(const SysView& v, const GroupSites& gs, const float* tile, int t,
+                                              const BoxDev& b) {
+    float tx[4], ty[4], tz[4], dx[4], dy[4], dz[4];
+    bspline4((float)gs.w[t][0], tx, dx);
+    bspline4((float)gs.w[t][1], ty, dy);
+    bspline4((float)gs.w[t][2], tz, dz);
+    const int x0 = rel_base(v, gs, t, 0) - 3, y0 = rel_base(v, gs, t, 1) - 3, z0 = rel_base(v, gs, t, 2) - 3;
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            const float* row = tile + ((x0 + a) * gs.n[1] + (y0 + bb)) * gs.n[2] + z0;
+            float sz = 0.f, sdz = 0.f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float ph = row[c];
+                sz = fmaf(tz[c], ph, sz);
+                sdz = fmaf(dz[c], ph, sdz);
+            }
+            gx = fmaf(dx[a] * ty[bb], sz, gx);
+            gy = fmaf(tx[a] * dy[bb], sz, gy);
+            gz = fmaf(tx[a] * ty[bb], sdz, gz);
+        }
+    }
+    const float q = gs.q[t];
+    return f3(-q * v.K[0] * b.inv_ext[0] * gx, -q * v.K[1] * b.inv_ext[1] * gy, -q * v.K[2] * b.inv_ext[2] * gz);
+}
+
+// Gather for the water sites by group (tile as for the spread), writing the
+// reciprocal cache by original water id.  With Ewald corrections on, the
+// intra-water exclusion corrections (H0-H1, H0-M, H1-M) are added here in
+// float64.  Pass 0 stores its (weighted) forces, later passes add theirs.
+DYN_KERNEL(__launch_bounds__(SG_T), k_gather_w, (, int pass), (, pass)) {
+    __shared__ GroupSites gs;
+    __shared__ float tile[TILE_PTS];
+    __shared__ float3 fsite[SG_SITES];
+    const BoxDev b = *v.box;
     const bool corr = pass == 0 && (v.flags & DYN_FLAG_EWALD_CORRECTIONS);
     const float wt = pass_weight(v, pass);
+    const uint32_t ng = (v.sc->n_wclus + GRPW / WCL - 1) / (GRPW / WCL);
+    const int tid = threadIdx.x;
     double e_c = 0.0, w_c = 0.0;
-    const uint32_t total = v.na + (pass == 2 ? 0u : v.nw_cap);
-    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
-        if (t < v.na) {
-            if (!pass_has_atom(v, pass, t)) continue;
-            const float4 p = v.apos[t];
+    for (uint32_t g = bk.idx; g < ng && pass != 2; g += bk.cnt) {
+        group_sites(v, g, b, gs);
+        if (gs.use_tile) {
+            const int npts = gs.n[0] * gs.n[1] * gs.n[2];
+            for (int i = tid; i < npts; i += SG_T) tile[i] = __ldg(v.qgrid + tile_to_grid(v, gs, i));
+            __syncthreads();
+        }
+        for (int t = tid; t < SG_SITES; t += SG_T) {
             float3 f = f3(0.f, 0.f, 0.f);
-            if (p.w != 0.f) f = gather_one(v, xyz(p), p.w, b) * wt;
-            long long* c = v.arecip + 3 * (size_t)t;
-            if (pass == 0) {
-                c[0] = fix_from_float(f.x); c[1] = fix_from_float(f.y); c[2] = fix_from_float(f.z);
-            } else {
-                c[0] += fix_from_float(f.x); c[1] += fix_from_float(f.y); c[2] += fix_from_float(f.z);
-            }
-        } else {
-            const uint32_t s = t - v.na;
+            if (gs.q[t] != 0.f)
+                f = (gs.use_tile ? gather_tile(v, gs, tile, t, b) : gather_one(v, gs.pos[t], gs.q[t], b)) * wt;
+            fsite[t] = f;
+        }
+        __syncthreads();
+        for (int w = tid; w < GRPW; w += SG_T) {
+            const uint32_t s = g * GRPW + w;
+            if (s >= v.nw_cap) continue;
             const uint32_t id = v.wid[s];
             if (id == INVALID_ID) continue;
             double3 fs[3];
             float3 ps[3];
             for (int k = 0; k < 3; ++k) {
-                const float4 p = v.wpos[4 * s + 1 + k];
-                ps[k] = xyz(p);
-                const float3 f = gather_one(v, ps[k], p.w, b) * wt;
+                ps[k] = gs.pos[3 * w + k];
+                const float3 f = fsite[3 * w + k];
                 fs[k] = make_double3(f.x, f.y, f.z);
             }
             if (corr) {
@@ -276,6 +464,7 @@ DYN_KERNEL(, k_gather, (, int pass), (, pass)) {
                 else { c[3 * k + 0] += fx; c[3 * k + 1] += fy; c[3 * k + 2] += fz; }
             }
         }
+        __syncthreads();  // gs, the tile and fsite are refilled by the next group
     }
     if (pass != 0) return;  // the intra-water corrections belong to pass 0
     double x[2] = {e_c, w_c};
@@ -409,7 +598,10 @@ namespace dyn {
 int pme_blocks(const SysView& v) {
     return gblocks(v, (uint64_t)v.K[0] * v.K[1] * (v.K[2] / 2 + 1));
 }
-int gather_blocks(const SysView& v) { return gblocks(v, (uint64_t)v.na + v.nw_cap); }
+// blocks of the water-group SPME kernels (k_gather_w writes REG_CORR partials)
+int gather_blocks(const SysView& v) {
+    return v.nw ? (int)std::min<uint32_t>(v.ngrp_cap, v.max_blocks) : 0;
+}
 int corr_blocks(const SysView& v) { return gblocks(v, (uint64_t)v.n14 + v.nexcl); }
 
 int pme_init(SysView& v, cufftHandle* plan_f, cufftHandle* plan_b, cudaStream_t st) {
@@ -477,34 +669,49 @@ void each_fft(const Target& t, F f) {
     }
 }
 
+// one SPME pass in three parts (the stage timer times them apart)
+void launch_pme_spread(const Target& t, int pass) {
+    auto on = [pass](const SysView& v) { return pass == 0 || v.alch_on != 0u; };
+    t.launch(k_spread, k_spread_batch, [&](const SysView& v) { return on(v) && v.na ? gblocks(v, v.na) : 0; },
+             GT, 0, pass);
+    t.launch(k_spread_w, k_spread_w_batch, [&](const SysView& v) { return on(v) ? gather_blocks(v) : 0; }, SG_T, 0,
+             pass);
+    t.launch(k_fix2real, k_fix2real_batch,
+             [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]) : 0; }, GT, 0);
+}
+
+void launch_pme_transform(const Target& t, int pass) {
+    auto on = [pass](const SysView& v) { return pass == 0 || v.alch_on != 0u; };
+    each_fft(t, [on](const SysView& v, cudaStream_t s) {
+        if (!on(v)) return;
+        cufftSetStream(v.plan_f, s);
+        cufftExecR2C(v.plan_f, v.qgrid, (cufftComplex*)v.cgrid);
+    });
+    t.launch(k_convolve, k_convolve_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_PME] : 0; }, GT, 0);
+    each_fft(t, [on](const SysView& v, cudaStream_t s) {
+        if (!on(v)) return;
+        cufftSetStream(v.plan_b, s);
+        cufftExecC2R(v.plan_b, (cufftComplex*)v.cgrid, v.qgrid);
+    });
+}
+
+void launch_pme_gather(const Target& t, int pass) {
+    auto on = [pass](const SysView& v) { return pass == 0 || v.alch_on != 0u; };
+    t.launch(k_gather, k_gather_batch, [&](const SysView& v) { return on(v) && v.na ? gblocks(v, v.na) : 0; }, GT, 0,
+             pass);
+    t.launch(k_gather_w, k_gather_w_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_CORR] : 0; }, SG_T,
+             0, pass);
+    t.launch(k_recip_pass, k_recip_pass_batch, [&](const SysView& v) { return on(v) ? 1 : 0; }, 256, 0, pass);
+}
+
 void launch_pme(const Target& t) {
     // one pass, or three with an alchemical molecule in any system (systems
     // without one skip passes 1 and 2)
     const int npass = t.any([](const SysView& v) { return v.alch_on != 0u; }) ? 3 : 1;
     for (int pass = 0; pass < npass; ++pass) {
-        auto on = [pass](const SysView& v) { return pass == 0 || v.alch_on != 0u; };
-        t.launch(k_spread, k_spread_batch,
-                 [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.na + 3ull * v.nw_cap) : 0; }, GT, 0,
-                 pass);
-        t.launch(k_fix2real, k_fix2real_batch,
-                 [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]) : 0; }, GT, 0);
-        // the plans run on the target's stream or a batch's FFT streams (a
-        // graph branch may differ from the stream the plans were made on)
-        each_fft(t, [on](const SysView& v, cudaStream_t s) {
-            if (!on(v)) return;
-            cufftSetStream(v.plan_f, s);
-            cufftExecR2C(v.plan_f, v.qgrid, (cufftComplex*)v.cgrid);
-        });
-        t.launch(k_convolve, k_convolve_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_PME] : 0; }, GT,
-                 0);
-        each_fft(t, [on](const SysView& v, cudaStream_t s) {
-            if (!on(v)) return;
-            cufftSetStream(v.plan_b, s);
-            cufftExecC2R(v.plan_b, (cufftComplex*)v.cgrid, v.qgrid);
-        });
-        t.launch(k_gather, k_gather_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_CORR] : 0; }, GT, 0,
-                 pass);
-        t.launch(k_recip_pass, k_recip_pass_batch, [&](const SysView& v) { return on(v) ? 1 : 0; }, 256, 0, pass);
+        launch_pme_spread(t, pass);
+        launch_pme_transform(t, pass);
+        launch_pme_gather(t, pass);
     }
 }
 

@@ -464,6 +464,10 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     v.r_ww = std::max(ljc, rc + 2.0f * OPC_SITE_REACH) + v.buffer;
     v.r_ws = std::max(ljc, rc + OPC_SITE_REACH) + v.buffer;
     v.r_ss = std::max(ljc, rc) + v.buffer;
+    {
+        const float rs = std::max(ljc, rc + OPC_SITE_REACH);
+        v.r_ws_skip2 = rs * rs;
+    }
     // pruned water-water lists (an inner buffer at most the outer one)
     v.prune_buf = std::min(cfg->prune_buffer > 0.f ? cfg->prune_buffer : 0.4f, v.buffer);
     v.r_in = std::max(ljc, rc + 2.0f * OPC_SITE_REACH) + v.prune_buf;
@@ -593,32 +597,10 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         if ((uint64_t)n_i * n_j <= (1ull << 24)) return std::max(1u, n_j);
         return est(r, vol_cl, n_j);
     };
+    v.cap_ws = (v.nw && v.na) ? cap_mixed(v.r_ws, acl_vol, v.nwclus_cap, v.naclus_cap) : 1;
     v.cap_ss = v.na ? cap_mixed(v.r_ss, acl_vol, v.naclus_cap, v.naclus_cap) : 1;
+    v.ws_item_cap = v.nwclus_cap * ((v.cap_ws + CH_MIX - 1) / CH_MIX);
     v.ss_item_cap = v.naclus_cap * ((v.cap_ss + CH_MIX - 1) / CH_MIX);
-    // water-atom: atom clusters near a water group's box (every cluster while
-    // that stays small), the atoms a group reaches and the atoms one water
-    // reaches, at a dense solute's density (0.12 atoms / A^3) with margin
-    if (v.nw && v.na) {
-        const double r = v.r_ws;
-        const double ag = 1.4 * std::cbrt(GRPW / std::max(1e-3, std::min(0.0334, v.nw / vol)));
-        const double mink_a = ag * ag * ag + 6.0 * ag * ag * r + 3.0 * M_PI * ag * r * r + 4.0 / 3.0 * M_PI * r * r * r;
-        v.cap_atile = cap_mixed(r, acl_vol, v.ngrp_cap, v.naclus_cap);
-        v.cap_aun = std::min<uint32_t>(std::min<uint32_t>(v.na_cap, v.cap_atile * ACL),
-                                       (uint32_t)(0.24 * mink_a) + 256);
-        v.cap_aun = std::min<uint32_t>(v.cap_aun, 65535u);
-        v.cap_wal = std::min<uint32_t>(v.cap_aun, (uint32_t)(0.15 * 4.0 / 3.0 * M_PI * r * r * r) + 64);
-        // shared-memory chunk of the water-atom kernel: two CTAs per SM
-        int dev = 0, smem_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-        const size_t per_atom = sizeof(float4) + sizeof(float2) + sizeof(uint32_t) + 3 * sizeof(int);
-        const size_t per_cta = smem_sm > 6144 ? std::min<size_t>((size_t)smem_sm / 2 - 4096, 64 * 1024) : 32 * 1024;
-        const uint32_t fit = (uint32_t)(per_cta / per_atom) / 32 * 32;
-        v.aun_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(fit, (v.cap_aun + 31) / 32 * 32));
-    } else {
-        v.cap_atile = v.cap_aun = v.cap_wal = 1;
-        v.aun_chunk = 32;
-    }
 
     // ---- allocations ----
     TRY(dev_alloc(h, &v.wpos, 4 * (size_t)v.nw_cap));
@@ -683,13 +665,9 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dev_alloc(h, &v.rev_n, v.nw_cap));
     TRY(dev_alloc(h, &v.rev, (size_t)v.nw_cap * v.rev_cap));
     TRY(dev_alloc(h, &v.wjbig, 12 * (size_t)v.nw_cap));
-    TRY(dev_alloc(h, &v.atile_n, v.ngrp_cap));
-    TRY(dev_alloc(h, &v.atile_j, (size_t)v.ngrp_cap * v.cap_atile));
-    TRY(dev_alloc(h, &v.aun_n, v.ngrp_cap));
-    TRY(dev_alloc(h, &v.aun_idx, (size_t)v.ngrp_cap * v.cap_aun));
-    TRY(dev_alloc(h, &v.acand_loc, (size_t)v.ngrp_cap * v.cap_atile * ACL));
-    TRY(dev_alloc(h, &v.wal_n, v.nw_cap));
-    TRY(dev_alloc(h, &v.wal, (size_t)v.nw_cap * v.cap_wal));
+    TRY(dev_alloc(h, &v.ws_n, v.nwclus_cap));
+    TRY(dev_alloc(h, &v.ws_j, (size_t)v.nwclus_cap * v.cap_ws));
+    TRY(dev_alloc(h, &v.ws_item, std::max(1u, v.ws_item_cap)));
     TRY(dev_alloc(h, &v.ss_item, std::max(1u, v.ss_item_cap)));
     TRY(dev_alloc(h, &v.ss_n, v.naclus_cap));
     TRY(dev_alloc(h, &v.ss_j, (size_t)v.naclus_cap * v.cap_ss));
@@ -1226,11 +1204,20 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
     const SysView& v = h->v;
     cudaStream_t st = h->stream;
     const Target T{&v, nullptr, st};
-    cudaEvent_t ev[7];
-    for (int i = 0; i < 7; ++i) DYN_CUDA(cudaEventCreate(&ev[i]));
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    // events: 0..6 bound the six stages; 7..10 split the pair stage,
+    // 11..13 the SPME stage
+    constexpr int NE = 14;
+    cudaEvent_t ev[NE];
+    for (int i = 0; i < NE; ++i) DYN_CUDA(cudaEventCreate(&ev[i]));
+    double acc[DYN_STAGES] = {};
     uint32_t n_spme = 0;
     const uint32_t e_int = std::max(1u, h->cfg.energy_interval);
+    const bool alch = v.alch_on != 0u;
+    auto el = [&](int a, int b) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[a], ev[b]);
+        return (double)t;
+    };
     for (uint32_t i = 0; i < n_steps; ++i) {
         const uint64_t s = h->host_step;
         const bool spme = (s % v.spme_interval) == 0;
@@ -1243,13 +1230,28 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
         dyn::launch_prune(T, false);
         cudaEventRecord(ev[2], st);
         dyn::launch_gather_atoms(T);
-        dyn::launch_pairs(T, energy);
+        dyn::launch_pairs_ww(T, energy);
+        cudaEventRecord(ev[7], st);
+        dyn::launch_ww_gather(T);
+        cudaEventRecord(ev[8], st);
+        dyn::launch_pairs_ws(T, energy);
+        cudaEventRecord(ev[9], st);
+        dyn::launch_pairs_atoms(T, energy);
         cudaEventRecord(ev[3], st);
         dyn::launch_pair14(T, energy);
         dyn::launch_bonded(T, energy);
         cudaEventRecord(ev[4], st);
         if (spme) {
-            dyn::launch_pme(T);
+            if (alch) {
+                dyn::launch_pme(T);
+            } else {
+                dyn::launch_pme_spread(T, 0);
+                cudaEventRecord(ev[10], st);
+                dyn::launch_pme_transform(T, 0);
+                cudaEventRecord(ev[11], st);
+                dyn::launch_pme_gather(T, 0);
+                cudaEventRecord(ev[12], st);
+            }
             dyn::launch_corrections(T);
         }
         cudaEventRecord(ev[5], st);
@@ -1259,17 +1261,23 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
         cudaEventRecord(ev[6], st);
         DYN_CUDA(cudaGetLastError());
         DYN_CUDA(cudaEventSynchronize(ev[6]));
-        for (int k = 0; k < 6; ++k) {
-            float t = 0.f;
-            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
-            acc[k] += t;
+        for (int k = 0; k < 6; ++k) acc[k] += el(k, k + 1);
+        acc[6] += el(2, 7);   // includes the atoms' cluster-order copy before it
+        acc[7] += el(7, 8);
+        acc[8] += el(8, 9);
+        acc[9] += el(9, 3);
+        if (spme && !alch) {
+            acc[10] += el(4, 10);
+            acc[11] += el(10, 11);
+            acc[12] += el(11, 12);
+            acc[13] += el(12, 5);
         }
         n_spme += spme ? 1u : 0u;
         h->host_step += 1;
     }
-    for (int i = 0; i < 7; ++i) cudaEventDestroy(ev[i]);
-    for (int k = 0; k < 6; ++k) ms[k] = n_steps ? acc[k] / n_steps : 0.0;
-    ms[4] = n_spme ? acc[4] / n_spme : 0.0;
+    for (int i = 0; i < NE; ++i) cudaEventDestroy(ev[i]);
+    for (int k = 0; k < DYN_STAGES; ++k) ms[k] = n_steps ? acc[k] / n_steps : 0.0;
+    for (int k : {4, 10, 11, 12, 13}) ms[k] = n_spme ? acc[k] / n_spme : 0.0;
     return read_scalars(h);
 }
 
@@ -1321,7 +1329,12 @@ int count_step_kernels(dyn_sys_s* h, bool spme, uint32_t* fixed, uint32_t* rebui
         }
         *fixed = total - fft;
     }
-    if (rebuild && (rc = count([&] { dyn::launch_rebuild(T, false); }, rebuild))) return rc;
+    // a rebuild is always followed by a prune of the water-water lists (which
+    // also runs alone, 2 kernels, when only the prune buffer is used up)
+    if (rebuild && (rc = count([&] {
+            dyn::launch_rebuild(T, false);
+            dyn::launch_prune(T, false);
+        }, rebuild))) return rc;
     if (periodic && (rc = count([&] { dyn::launch_periodic(T); }, periodic))) return rc;
     return DYN_OK;
 }

@@ -347,11 +347,13 @@ class MdState:
                                       *[ptr(outputs.get(k)) for k in keys], C.byref(e)))
         return e.as_dict()
 
-    STAGES = ("first_half", "list", "pairs", "bonded", "spme", "kick_finalize")
+    STAGES = ("first_half", "list", "pairs", "bonded", "spme", "kick_finalize",
+              "pairs_water_water", "pairs_ww_gather", "pairs_water_atom", "pairs_atom_atom",
+              "spme_spread", "spme_fft_convolve", "spme_gather", "spme_corrections")
 
     def stage_times(self, dt, n_steps):
         """Mean ms per step of each stage, timed with CUDA events."""
-        ms = np.zeros(6)
+        ms = np.zeros(_lib.DYN_STAGES)
         check(lib().dyn_sys_stage_times(self.handle, int(n_steps), float(dt), ptr(ms)))
         return dict(zip(self.STAGES, ms.tolist()))
 
@@ -515,13 +517,20 @@ class MdBatch:
     """Independent systems advanced together (dyn_batch_*): every stage of a
     step is one kernel launch over all members with per-member block ranges,
     and a step is one CUDA graph.  ``members[i]`` is an MdState view of
-    system i (state, energies, forces); results equal running it alone."""
+    system i (state, energies, forces); results equal running it alone.
+    With ``tune``, each member takes the autotuner's choice for its size
+    class (dynamics_b200.tune; classes not yet in the cache are tuned
+    first, one representative member each)."""
 
-    def __init__(self, systems=(), cfgs=(), stream=None):
+    def __init__(self, systems=(), cfgs=(), stream=None, tune=False):
         systems = list(systems)
         if isinstance(cfgs, MdConfig):
             cfgs = [cfgs] * len(systems)
         cfgs = list(cfgs)
+        if tune:
+            from . import tune as _tune
+            cfgs = [_tune.apply_tuned(s, c, tune_missing=True, stream=stream) for s, c in zip(systems, cfgs)]
+        self.cfgs = cfgs
         n = len(systems)
         descs = (_lib.SystemDesc * max(n, 1))()
         confs = (_lib.Config * max(n, 1))()

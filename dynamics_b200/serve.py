@@ -48,6 +48,7 @@ class Report:
     peak_members: int
     peak_bytes: int
     rounds: int
+    budget_waits: int = 0             # admission points where the budget held a request back
     latency_s: dict = field(default_factory=dict)
     queue_wait_s: dict = field(default_factory=dict)
 
@@ -103,6 +104,7 @@ class Server:
         peak_bytes = 0
         rounds = 0
         steps_total = 0
+        budget_waits = 0
         t0 = self.clock()
         try:
             while pending or active:
@@ -111,6 +113,7 @@ class Server:
                     req = pending[0]
                     est = self._estimate(req)
                     if active and used + est > self.budget:
+                        budget_waits += 1
                         break
                     pending.pop(0)
                     m = batch.add(req.system, req.cfg)
@@ -152,7 +155,7 @@ class Server:
         lat = [r.completed - r.arrival for r in requests]
         wait = [r.admitted - r.arrival for r in requests]
         rep = Report(requests=list(requests), wall_s=wall, steps_total=steps_total, dt_ps=self.dt,
-                     peak_members=peak_members, peak_bytes=peak_bytes, rounds=rounds)
+                     peak_members=peak_members, peak_bytes=peak_bytes, rounds=rounds, budget_waits=budget_waits)
         rep.latency_s = {"p50": _pct(lat, 50), "p99": _pct(lat, 99), "mean": float(np.mean(lat))}
         rep.queue_wait_s = {"p50": _pct(wait, 50), "p99": _pct(wait, 99), "mean": float(np.mean(wait))}
         return rep

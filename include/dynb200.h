@@ -429,11 +429,16 @@ int dyn_sys_step_host(dyn_sys_t h, uint32_t n_steps, float dt, const float* atom
 /* Stage timing, the device counterpart of the reference's per-component
  * timers (ComputationTimeSums, src/util.rs:111-180): runs n_steps steps
  * without graphs, with CUDA events between stages on the handle's stream,
- * and writes the mean milliseconds per step of each stage into ms[6]:
- * [0] first half (kick/drift/thermostat), [1] displacement check and list
- * rebuild, [2] short-range pair kernels, [3] 1-4 and bonded terms,
- * [4] SPME (mean over the steps that ran it), [5] kick, reductions,
- * thermostat/barostat and periodic tasks. */
+ * and writes the mean milliseconds per step of each stage into
+ * ms[DYN_STAGES]: [0] first half (kick/drift/thermostat), [1] displacement
+ * check, list rebuild and prune, [2] short-range pair kernels, [3] 1-4 and
+ * bonded terms, [4] SPME (mean over the steps that ran it), [5] kick,
+ * reductions, thermostat/barostat and periodic tasks; the pair stage split
+ * into [6] water-water (with the atoms' cluster-order copy before it),
+ * [7] its j-side gather, [8] water-atom, [9] atom-atom; the SPME stage (per
+ * SPME step, without an alchemical molecule) into [10] spread, [11] FFTs
+ * and convolution, [12] gather, [13] corrections. */
+#define DYN_STAGES 14
 int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, double* ms);
 
 /* Number of this library's kernels one step launches (library kernels such
@@ -442,9 +447,11 @@ int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, double* ms);
  * (COM removal, recentering, reset_angle). */
 int dyn_sys_launches_per_step(dyn_sys_t h, int spme, uint32_t* out);
 
-/* Kernels a step adds when it rebuilds the lists (*rebuild) and when a
- * periodic task is due (*periodic); in the captured step graph these sit
- * under conditional nodes that the device sets. */
+/* Kernels a step adds when it rebuilds the lists (*rebuild, including the
+ * prune of the water-water lists that follows every rebuild; a step that
+ * only prunes adds 2) and when a periodic task is due (*periodic); in the
+ * captured step graph these sit under conditional nodes that the device
+ * sets. */
 int dyn_sys_launches_conditional(dyn_sys_t h, uint32_t* rebuild, uint32_t* periodic);
 
 /* The pairs the resident engine's pair kernels evaluate at this moment, as
