@@ -200,27 +200,18 @@ def measure_batch(name, args, stream, dev, dist=None, rank=0, world=1):
                 + 2 * min(max(0, prunes - rebuilds), steps))
     value = aggregate_ns_per_day(steps, n_sys, world, ms)
     plain_value = DT * 1e-3 * n_sys / (plain_ms * 1e-3) * 86400.0
-    # ---- end to end: every member's positions/velocities in and out per step ----
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory().numpy()
-    keys = ("water_pos", "water_vel", "atom_pos", "atom_vel")
-    host = []
-    for m in batch.members:
-        s0 = m.state()
-        host.append({k: pin(s0[k]) for k in keys if k in s0 and s0[k].size})
+    # ---- end to end: every member's positions/velocities in and out per step,
+    # one copy each way for the whole batch through its page-locked area ----
+    host = batch.host_buffer()
+    batch.step_host(DT, 1, None, host)
     n_e2e = max(5, steps // 10)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for _ in range(n_e2e):
-        for m, hb in zip(batch.members, host):
-            m.set_state(**hb)
-        batch.step(DT, 1)
-        for m, hb in zip(batch.members, host):
-            s1 = m.state()
-            for k in hb:
-                hb[k][:] = s1[k]
+        batch.step_host(DT, 1, host, host)
     t_e2e = time.perf_counter() - t0
     e2e_value = n_e2e * DT * 1e-3 * n_sys * world / t_e2e * 86400.0
-    io_bytes = int(sum(a.nbytes for hb in host for a in hb.values()))
+    io_bytes = int(host.nbytes)
     batch.close()
     return {
         "value": round(value, 2), "unit": "ns/day (aggregate over members)", "steps": steps,
@@ -231,7 +222,8 @@ def measure_batch(name, args, stream, dev, dist=None, rank=0, world=1):
                              "ms_per_round": round(plain_ms, 4), "steps_each": k_plain},
         "batch_over_plain": round(value / world / plain_value, 3),
         "e2e": {"value": round(e2e_value, 2), "unit": "ns/day (aggregate)",
-                "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+                "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
+                "of_device": round(e2e_value / value, 3), "path": "dyn_batch_step_host"},
         "gpu_launches": int(round(launches)),
         "launches_per_step": {"spme": fixed_s, "no_spme": fixed_n, "rebuild_extra": reb_k, "periodic_extra": per_k},
         "clocks": clocks.summary(0 if dev.index is None else dev.index),

@@ -163,6 +163,9 @@ _SIGS = {
     "dyn_batch_add": ([_P, _P, _P, _P], C.c_int),
     "dyn_batch_remove": ([_P, C.c_uint32], C.c_int),
     "dyn_batch_memory": ([_P, _P], C.c_int),
+    "dyn_batch_state_layout": ([_P, _P], C.c_int),
+    "dyn_batch_host_buffer": ([_P, _P, _P], C.c_int),
+    "dyn_batch_step_host": ([_P, C.c_uint32, C.c_float, _P, _P, _P], C.c_int),
     "dyn_sys_memory": ([_P, _P], C.c_int),
     "dyn_sys_snapshots": ([_P, C.c_uint32, C.c_uint32, C.c_uint32], C.c_int),
     "dyn_sys_minimize": ([_P, C.c_uint32, C.c_float, _P, _P], C.c_int),

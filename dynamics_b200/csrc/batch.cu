@@ -83,6 +83,21 @@ struct dyn_batch_s {
     uint32_t spme_interval = 1, energy_interval = 1;
     bool fixed_intervals = false;   // set by the first member
     uint32_t views_cap = 0;         // members the device view arrays hold
+    // batch-wide host step (dyn_batch_step_host): the members' packed
+    // states in one device area, their scalars gathered beside it
+    struct HostIo {
+        std::vector<unsigned long long> off;  // member offsets into the packed state (floats), n + 1
+        std::vector<SysView> views;           // the views d_views holds
+        float* d_state = nullptr;
+        size_t cap_floats = 0;
+        Scalars* d_sc = nullptr;
+        Scalars* h_sc = nullptr;              // pinned
+        SysView* d_views = nullptr;
+        unsigned long long* d_off = nullptr;
+        size_t cap_members = 0;
+        float* h_buf = nullptr;               // pinned packed state (dyn_batch_host_buffer)
+        size_t h_buf_floats = 0;
+    } io;
 };
 
 namespace {
@@ -218,6 +233,12 @@ extern "C" int dyn_batch_destroy(dyn_batch_t b) {
     }
     for (void* p : b->map_allocs) cudaFree(p);
     for (dyn_sys_t m : b->members) dyn_sys_destroy(m);
+    if (b->io.d_state) cudaFree(b->io.d_state);
+    if (b->io.d_sc) cudaFree(b->io.d_sc);
+    if (b->io.d_views) cudaFree(b->io.d_views);
+    if (b->io.d_off) cudaFree(b->io.d_off);
+    if (b->io.h_sc) cudaFreeHost(b->io.h_sc);
+    if (b->io.h_buf) cudaFreeHost(b->io.h_buf);
     if (b->aux) cudaStreamDestroy(b->aux);
     if (b->window_ev) cudaEventDestroy(b->window_ev);
     b->br.destroy();
@@ -424,5 +445,173 @@ extern "C" int dyn_batch_memory(dyn_batch_t b, uint64_t* bytes) {
     for (dyn_sys_t m : b->members) t += m->bytes;
     for (auto& kv : b->ctx.maps) t += (uint64_t)kv.second.total * sizeof(uint2);
     *bytes = t;
+    return DYN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batch-wide host step.  The packed host state holds, per member in order,
+// atom_pos [na][3], atom_vel [na][3], water_pos [nw][3][3], water_vel
+// [nw][3][3] (home order, as dyn_sys_step_host takes them); one copy moves
+// all members' states each way and one launch scatters / gathers them
+// (blockIdx.y = member).
+// ---------------------------------------------------------------------------
+namespace {
+
+static_assert(sizeof(Scalars) % 8 == 0, "Scalars is copied as 8-byte words");
+
+__global__ void k_batch_state_in(const SysView* __restrict__ vs, const unsigned long long* __restrict__ off,
+                                 const float* __restrict__ stage) {
+    const SysView& v = vs[blockIdx.y];
+    const float* ap = stage + off[blockIdx.y];
+    const float* av = ap + 3 * (size_t)v.na;
+    const float* wp = av + 3 * (size_t)v.na;
+    const float* wv = wp + 9 * (size_t)v.nw;
+    const uint32_t n = v.nw_cap + v.na;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        if (t < v.nw_cap) water_in(v, t, wp, wv);
+        else atom_in(v, t - v.nw_cap, ap, av);
+    }
+}
+
+// stage == nullptr: the scalars only
+__global__ void k_batch_state_out(const SysView* __restrict__ vs, const unsigned long long* __restrict__ off,
+                                  float* __restrict__ stage, Scalars* __restrict__ sc) {
+    const SysView& v = vs[blockIdx.y];
+    if (blockIdx.x == 0) {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(v.sc);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(sc + blockIdx.y);
+        for (uint32_t k = threadIdx.x; k < sizeof(Scalars) / 8; k += blockDim.x) dst[k] = src[k];
+    }
+    if (!stage) return;
+    float* ap = stage + off[blockIdx.y];
+    float* av = ap + 3 * (size_t)v.na;
+    float* wp = av + 3 * (size_t)v.na;
+    float* wv = wp + 9 * (size_t)v.nw;
+    const uint32_t n = v.nw_cap + v.na;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        if (t < v.nw_cap) water_out(v, t, wp, wv);
+        else atom_out(v, t - v.nw_cap, ap, av);
+    }
+}
+
+void host_layout(const dyn_batch_s* b, std::vector<unsigned long long>& off) {
+    off.assign(b->members.size() + 1, 0ull);
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        const SysView& v = b->members[i]->v;
+        off[i + 1] = off[i] + 6ull * v.na + 18ull * v.nw;
+    }
+}
+
+// Sizes the device areas for the current members and uploads their views
+// and offsets when they changed (membership, or a member's arrays).
+int ensure_io(dyn_batch_s* b) {
+    auto& io = b->io;
+    const size_t n = b->members.size();
+    std::vector<unsigned long long> off;
+    host_layout(b, off);
+    if (off.back() > io.cap_floats) {
+        if (io.d_state) cudaFree(io.d_state);
+        io.d_state = nullptr;
+        io.cap_floats = 0;
+        DYN_CUDA(cudaMalloc(&io.d_state, off.back() * sizeof(float)));
+        io.cap_floats = off.back();
+    }
+    if (n > io.cap_members) {
+        if (io.d_sc) cudaFree(io.d_sc);
+        if (io.d_views) cudaFree(io.d_views);
+        if (io.d_off) cudaFree(io.d_off);
+        if (io.h_sc) cudaFreeHost(io.h_sc);
+        io.d_sc = nullptr; io.d_views = nullptr; io.d_off = nullptr; io.h_sc = nullptr;
+        io.cap_members = 0;
+        io.views.clear();
+        const size_t cap = std::max<size_t>(8, 2 * n);
+        DYN_CUDA(cudaMalloc(&io.d_sc, cap * sizeof(Scalars)));
+        DYN_CUDA(cudaMalloc(&io.d_views, cap * sizeof(SysView)));
+        DYN_CUDA(cudaMalloc(&io.d_off, (cap + 1) * sizeof(unsigned long long)));
+        DYN_CUDA(cudaHostAlloc(&io.h_sc, cap * sizeof(Scalars), cudaHostAllocDefault));
+        io.cap_members = cap;
+    }
+    bool same = io.views.size() == n && io.off == off;
+    for (size_t i = 0; same && i < n; ++i)
+        same = std::memcmp(&io.views[i], &b->members[i]->v, sizeof(SysView)) == 0;
+    if (!same) {
+        io.views.resize(n);
+        for (size_t i = 0; i < n; ++i) io.views[i] = b->members[i]->v;
+        io.off = off;
+        DYN_CUDA(cudaMemcpyAsync(io.d_views, io.views.data(), n * sizeof(SysView), cudaMemcpyHostToDevice,
+                                 b->stream));
+        DYN_CUDA(cudaMemcpyAsync(io.d_off, io.off.data(), (n + 1) * sizeof(unsigned long long),
+                                 cudaMemcpyHostToDevice, b->stream));
+        DYN_CUDA(cudaStreamSynchronize(b->stream));  // the host vectors may change before the next call
+    }
+    return DYN_OK;
+}
+
+}  // namespace
+
+extern "C" int dyn_batch_state_layout(dyn_batch_t b, uint64_t* offsets) {
+    DYN_CHECK(b && offsets, DYN_ERR_INVALID, "dyn_batch_state_layout: NULL argument");
+    std::vector<unsigned long long> off;
+    host_layout(b, off);
+    for (size_t i = 0; i < off.size(); ++i) offsets[i] = off[i];
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_host_buffer(dyn_batch_t b, float** buf, uint64_t* n_floats) {
+    DYN_CHECK(b && buf && n_floats, DYN_ERR_INVALID, "dyn_batch_host_buffer: NULL argument");
+    std::vector<unsigned long long> off;
+    host_layout(b, off);
+    auto& io = b->io;
+    if (off.back() > io.h_buf_floats || !io.h_buf) {
+        DYN_CUDA(cudaStreamSynchronize(b->stream));
+        if (io.h_buf) cudaFreeHost(io.h_buf);
+        io.h_buf = nullptr;
+        io.h_buf_floats = 0;
+        const size_t nf = std::max<size_t>(off.back(), 1);
+        const cudaError_t e = cudaHostAlloc(&io.h_buf, nf * sizeof(float), cudaHostAllocDefault);
+        if (e != cudaSuccess) return dyn::fail(DYN_ERR_OOM, "dyn_batch_host_buffer: cudaHostAlloc failed");
+        io.h_buf_floats = nf;
+    }
+    *buf = io.h_buf;
+    *n_floats = off.back();
+    return DYN_OK;
+}
+
+extern "C" int dyn_batch_step_host(dyn_batch_t b, uint32_t n_steps, float dt, const float* state_in,
+                                   float* state_out, dyn_energies_t* energies) {
+    DYN_CHECK(b, DYN_ERR_INVALID, "dyn_batch_step_host: NULL handle");
+    DYN_CHECK(dt > 0.f && std::isfinite(dt), DYN_ERR_INVALID, "dyn_batch_step_host: dt must be > 0");
+    if (b->members.empty()) return DYN_OK;
+    int rc = ensure_io(b);
+    if (rc != DYN_OK) return rc;
+    auto& io = b->io;
+    const uint32_t n = (uint32_t)b->members.size();
+    DYN_CHECK(n <= 65535u, DYN_ERR_UNSUPPORTED, "dyn_batch_step_host: at most 65535 members");
+    uint32_t most = 1;
+    for (dyn_sys_t m : b->members) most = std::max(most, m->v.nw_cap + m->v.na);
+    const dim3 grid(std::min(64u, (most + 255) / 256), n);
+    const size_t bytes = io.off.back() * sizeof(float);
+    if (state_in) {
+        if (bytes) DYN_CUDA(cudaMemcpyAsync(io.d_state, state_in, bytes, cudaMemcpyHostToDevice, b->stream));
+        k_batch_state_in<<<grid, 256, 0, b->stream>>>(io.d_views, io.d_off, io.d_state);
+        DYN_CUDA(cudaGetLastError());
+    }
+    rc = dyn_batch_step(b, n_steps, dt);
+    if (rc != DYN_OK) return rc;
+    k_batch_state_out<<<grid, 256, 0, b->stream>>>(io.d_views, io.d_off, state_out ? io.d_state : nullptr, io.d_sc);
+    DYN_CUDA(cudaGetLastError());
+    if (state_out && bytes)
+        DYN_CUDA(cudaMemcpyAsync(state_out, io.d_state, bytes, cudaMemcpyDeviceToHost, b->stream));
+    DYN_CUDA(cudaMemcpyAsync(io.h_sc, io.d_sc, n * sizeof(Scalars), cudaMemcpyDeviceToHost, b->stream));
+    DYN_CUDA(cudaStreamSynchronize(b->stream));
+    for (uint32_t i = 0; i < n; ++i) {
+        dyn_sys_t m = b->members[i];
+        std::memcpy(m->h_sc, &io.h_sc[i], sizeof(Scalars));
+        if (energies) dyn::energies_of(m, &energies[i]);
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const int e = dyn::check_scalars(b->members[i]);
+        if (e != DYN_OK) return dyn::fail(e, "member " + std::to_string(i) + ": " + dyn_last_error());
+    }
     return DYN_OK;
 }

@@ -36,9 +36,71 @@ struct dyn_sys_s {
     uint64_t snap_read = 0;        // frames handed to the host so far
     cudaEvent_t window_ev = nullptr;  // bounds the steps one dyn_sys_step call queues
     bool window_armed = false;
+    float* host_stage = nullptr;   // device staging of dyn_sys_step_host (in allocs)
+    size_t host_stage_n = 0;       // floats
 };
 
+// Home-order host layout <-> the resident arrays.  Waters: (pos, vel) as
+// [nw][3][3] floats (O, H0, H1) by original id; the virtual site M is
+// placed from O, H0, H1.  Atoms: [na][3] floats by atom index.  One water
+// slot (cluster order) or one atom per call.
+__device__ __forceinline__ void water_in(const SysView& v, uint32_t s, const float* __restrict__ wp,
+                                         const float* __restrict__ wv) {
+    const uint32_t id = v.wid[s];
+    if (id == INVALID_ID) return;
+    if (wp) {
+        const float* x = wp + 9 * (size_t)id;
+        const float3 o = f3(x[0], x[1], x[2]), h0 = f3(x[3], x[4], x[5]), h1 = f3(x[6], x[7], x[8]);
+        const float3 bis = (h0 - o) + (h1 - o);
+        const float3 m = o + bis * (OPC_O_EP_R * rsqrtf(dot3(bis, bis)));
+        v.wpos[4 * s + 0] = make_float4(o.x, o.y, o.z, 0.f);
+        v.wpos[4 * s + 1] = make_float4(h0.x, h0.y, h0.z, OPC_Q_H);
+        v.wpos[4 * s + 2] = make_float4(h1.x, h1.y, h1.z, OPC_Q_H);
+        v.wpos[4 * s + 3] = make_float4(m.x, m.y, m.z, OPC_Q_EP);
+    }
+    if (wv) {
+        const float* x = wv + 9 * (size_t)id;
+        for (int k = 0; k < 3; ++k) v.wvel[3 * s + k] = make_float4(x[3 * k], x[3 * k + 1], x[3 * k + 2], 0.f);
+    }
+}
+
+__device__ __forceinline__ void water_out(const SysView& v, uint32_t s, float* __restrict__ wp,
+                                          float* __restrict__ wv) {
+    const uint32_t id = v.wid[s];
+    if (id == INVALID_ID) return;
+    for (int k = 0; k < 3; ++k) {
+        if (wp) {
+            const float4 a = v.wpos[4 * s + k];
+            float* o = wp + 9 * (size_t)id + 3 * k;
+            o[0] = a.x; o[1] = a.y; o[2] = a.z;
+        }
+        if (wv) {
+            const float4 b = v.wvel[3 * s + k];
+            float* o = wv + 9 * (size_t)id + 3 * k;
+            o[0] = b.x; o[1] = b.y; o[2] = b.z;
+        }
+    }
+}
+
+__device__ __forceinline__ void atom_in(const SysView& v, uint32_t a, const float* __restrict__ ap,
+                                        const float* __restrict__ av) {
+    if (ap) { float4 p = v.apos[a]; p.x = ap[3 * a]; p.y = ap[3 * a + 1]; p.z = ap[3 * a + 2]; v.apos[a] = p; }
+    if (av) v.avel[a] = make_float4(av[3 * a], av[3 * a + 1], av[3 * a + 2], 0.f);
+}
+
+__device__ __forceinline__ void atom_out(const SysView& v, uint32_t a, float* __restrict__ ap,
+                                         float* __restrict__ av) {
+    const float4 p = v.apos[a], w = v.avel[a];
+    if (ap) { ap[3 * a] = p.x; ap[3 * a + 1] = p.y; ap[3 * a + 2] = p.z; }
+    if (av) { av[3 * a] = w.x; av[3 * a + 1] = w.y; av[3 * a + 2] = w.z; }
+}
+
 namespace dyn {
+
+// Turns the device-side flags of h->h_sc (already on the host) into errors.
+int check_scalars(dyn_sys_s* h);
+// The energies of the last step from h->h_sc (already on the host).
+void energies_of(dyn_sys_s* h, dyn_energies_t* e);
 
 // Inside an active capture on st: appends an IF node on hc after everything
 // captured so far and starts capturing its body on aux.

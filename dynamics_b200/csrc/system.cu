@@ -283,6 +283,10 @@ namespace dyn {
 int read_scalars(dyn_sys_s* h) {
     DYN_CUDA(cudaMemcpyAsync(h->h_sc, h->v.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
     DYN_CUDA(cudaStreamSynchronize(h->stream));
+    return check_scalars(h);
+}
+
+int check_scalars(dyn_sys_s* h) {
     if (h->h_sc->overflow)
         return dyn::fail(DYN_ERR_UNSUPPORTED, "cluster list capacity exceeded (list length " +
                                                   std::to_string(h->h_sc->overflow) + ")");
@@ -1050,81 +1054,38 @@ extern "C" int dyn_sys_set_state(dyn_sys_t h, const float* atom_pos, const float
 // Home-order staging for the host-step path: water (pos, vel) as [nw*9]
 // floats each; kernels scatter into / gather from the cluster-ordered slots.
 __global__ void k_stage_in(SysView v, const float* __restrict__ wp, const float* __restrict__ wv) {
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
-        const uint32_t id = v.wid[s];
-        if (id == INVALID_ID) continue;
-        if (wp) {
-            const float* x = wp + 9 * (size_t)id;
-            const float3 o = f3(x[0], x[1], x[2]), h0 = f3(x[3], x[4], x[5]), h1 = f3(x[6], x[7], x[8]);
-            const float3 bis = (h0 - o) + (h1 - o);
-            const float3 m = o + bis * (OPC_O_EP_R * rsqrtf(dot3(bis, bis)));
-            v.wpos[4 * s + 0] = make_float4(o.x, o.y, o.z, 0.f);
-            v.wpos[4 * s + 1] = make_float4(h0.x, h0.y, h0.z, OPC_Q_H);
-            v.wpos[4 * s + 2] = make_float4(h1.x, h1.y, h1.z, OPC_Q_H);
-            v.wpos[4 * s + 3] = make_float4(m.x, m.y, m.z, OPC_Q_EP);
-        }
-        if (wv) {
-            const float* x = wv + 9 * (size_t)id;
-            for (int k = 0; k < 3; ++k) v.wvel[3 * s + k] = make_float4(x[3 * k], x[3 * k + 1], x[3 * k + 2], 0.f);
-        }
-    }
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x)
+        water_in(v, s, wp, wv);
 }
 
 __global__ void k_stage_out(SysView v, float* __restrict__ wp, float* __restrict__ wv) {
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x) {
-        const uint32_t id = v.wid[s];
-        if (id == INVALID_ID) continue;
-        for (int k = 0; k < 3; ++k) {
-            if (wp) {
-                const float4 a = v.wpos[4 * s + k];
-                wp[9 * (size_t)id + 3 * k] = a.x; wp[9 * (size_t)id + 3 * k + 1] = a.y; wp[9 * (size_t)id + 3 * k + 2] = a.z;
-            }
-            if (wv) {
-                const float4 b = v.wvel[3 * s + k];
-                wv[9 * (size_t)id + 3 * k] = b.x; wv[9 * (size_t)id + 3 * k + 1] = b.y; wv[9 * (size_t)id + 3 * k + 2] = b.z;
-            }
-        }
-    }
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nw_cap; s += gridDim.x * blockDim.x)
+        water_out(v, s, wp, wv);
 }
 
 __global__ void k_atoms_in(SysView v, const float* __restrict__ ap, const float* __restrict__ av) {
-    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
-        if (ap) { float4 p = v.apos[a]; p.x = ap[3 * a]; p.y = ap[3 * a + 1]; p.z = ap[3 * a + 2]; v.apos[a] = p; }
-        if (av) v.avel[a] = make_float4(av[3 * a], av[3 * a + 1], av[3 * a + 2], 0.f);
-    }
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x)
+        atom_in(v, a, ap, av);
 }
 
 __global__ void k_atoms_out(SysView v, float* __restrict__ ap, float* __restrict__ av) {
-    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x) {
-        const float4 p = v.apos[a], w = v.avel[a];
-        if (ap) { ap[3 * a] = p.x; ap[3 * a + 1] = p.y; ap[3 * a + 2] = p.z; }
-        if (av) { av[3 * a] = w.x; av[3 * a + 1] = w.y; av[3 * a + 2] = w.z; }
-    }
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < v.na; a += gridDim.x * blockDim.x)
+        atom_out(v, a, ap, av);
 }
 
 namespace {
 
-struct HostStage {
-    float* d = nullptr;   // [4 * (na*3 + nw*9)] device staging
-    size_t n = 0;
-};
-
-int ensure_stage(dyn_sys_s* h, HostStage& hs) {
+// The staging area of dyn_sys_step_host: [2 * (na*3 + nw*9)] floats,
+// owned by the handle (freed with its other allocations).
+int ensure_stage(dyn_sys_s* h) {
     const size_t need = 2 * (3 * (size_t)h->v.na) + 2 * (9 * (size_t)h->v.nw);
-    if (hs.d && hs.n >= need) return DYN_OK;
-    if (hs.d) cudaFree(hs.d);
-    DYN_CUDA(cudaMalloc(&hs.d, std::max<size_t>(need, 1) * sizeof(float)));
-    h->allocs.push_back(hs.d);
-    hs.n = need;
+    if (h->host_stage && h->host_stage_n >= need) return DYN_OK;
+    float* d = nullptr;
+    DYN_CUDA(cudaMalloc(&d, std::max<size_t>(need, 1) * sizeof(float)));
+    h->allocs.push_back(d);  // a smaller earlier area stays in allocs until destroy
+    h->host_stage = d;
+    h->host_stage_n = need;
     return DYN_OK;
-}
-
-HostStage& stage_of(dyn_sys_s* h) {
-    static thread_local std::vector<std::pair<dyn_sys_s*, HostStage>> tbl;
-    for (auto& e : tbl)
-        if (e.first == h) return e.second;
-    tbl.push_back({h, HostStage{}});
-    return tbl.back().second;
 }
 
 }  // namespace
@@ -1154,10 +1115,9 @@ extern "C" int dyn_sys_step_host(dyn_sys_t h, uint32_t n_steps, float dt, const 
                                  float* water_pos_out, float* water_vel_out, dyn_energies_t* energies) {
     DYN_CHECK(h, DYN_ERR_INVALID, "dyn_sys_step_host: NULL handle");
     SysView& v = h->v;
-    HostStage& hs = stage_of(h);
-    int rc = ensure_stage(h, hs);
+    int rc = ensure_stage(h);
     if (rc) return rc;
-    float* d_ap = hs.d;
+    float* d_ap = h->host_stage;
     float* d_av = d_ap + 3 * (size_t)v.na;
     float* d_wp = d_av + 3 * (size_t)v.na;
     float* d_wv = d_wp + 9 * (size_t)v.nw;
@@ -1492,4 +1452,8 @@ extern "C" int dyn_sys_snapshots_read(dyn_sys_t h, uint32_t max_frames, float* p
 
 namespace dyn {
 int evaluate_forces(dyn_sys_s* h) { return evaluate_forces_now(h); }
+}  // namespace dyn
+
+namespace dyn {
+void energies_of(dyn_sys_s* h, dyn_energies_t* e) { fill_energies(h, e); }
 }  // namespace dyn

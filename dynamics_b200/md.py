@@ -580,6 +580,45 @@ class MdBatch:
         check(lib().dyn_batch_memory(self._h, C.byref(b)))
         return b.value
 
+    def state_layout(self):
+        """Member offsets (floats) into the packed host state, n + 1 entries."""
+        off = np.zeros(len(self.members) + 1, np.uint64)
+        check(lib().dyn_batch_state_layout(self._h, ptr(off)))
+        return off
+
+    def host_buffer(self):
+        """The batch's page-locked packed-state area as a float32 array (valid
+        until the batch grows or closes)."""
+        buf, n = C.POINTER(C.c_float)(), C.c_uint64()
+        check(lib().dyn_batch_host_buffer(self._h, C.byref(buf), C.byref(n)))
+        return np.ctypeslib.as_array(buf, shape=(max(n.value, 1),))[:n.value]
+
+    def unpack(self, packed, i):
+        """Views of member i's atom_pos, atom_vel, water_pos, water_vel in a
+        packed state array."""
+        off = self.state_layout()
+        m = self.members[i]
+        na, nw = m.n_atoms, m.n_water
+        a = packed[int(off[i]):int(off[i + 1])]
+        return {"atom_pos": a[:3 * na].reshape(na, 3), "atom_vel": a[3 * na:6 * na].reshape(na, 3),
+                "water_pos": a[6 * na:6 * na + 9 * nw].reshape(nw, 3, 3),
+                "water_vel": a[6 * na + 9 * nw:].reshape(nw, 3, 3)}
+
+    def step_host(self, dt, n_steps=1, state_in=None, state_out=None, energies=False):
+        """dyn_batch_step_host: every member's packed state in (state_in,
+        None keeps the resident states), n steps, packed state out
+        (state_out, None skips it); one copy each way for the whole batch.
+        Returns the members' energies dicts with energies, else None."""
+        n = len(self.members)
+        total = int(self.state_layout()[-1])
+        for a in (state_in, state_out):
+            if a is not None and (a.dtype != np.float32 or a.size < total or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError(f"packed state: contiguous float32 with at least {total} values")
+        e = (_lib.Energies * max(n, 1))() if energies else None
+        check(lib().dyn_batch_step_host(self._h, int(n_steps), float(dt), ptr(state_in), ptr(state_out),
+                                        e if energies else None))
+        return [e[i].as_dict() for i in range(n)] if energies else None
+
     def launches(self, spme=True):
         """(fixed, rebuild, periodic) batched launches of one step."""
         f, r, p = C.c_uint32(), C.c_uint32(), C.c_uint32()

@@ -587,6 +587,32 @@ int dyn_batch_add(dyn_batch_t b, const dyn_config_t* cfg, const dyn_system_desc_
  * one index. */
 int dyn_batch_remove(dyn_batch_t b, uint32_t i);
 
+/* Layout of a batch's packed host state: member i's block starts at
+ * offsets[i] floats and holds atom_pos [na][3], atom_vel [na][3],
+ * water_pos [nw][3][3] and water_vel [nw][3][3] (home order, the arrays
+ * dyn_sys_step_host takes); offsets[n] is the total.  offsets holds n + 1
+ * entries.  The layout changes with dyn_batch_add / dyn_batch_remove. */
+int dyn_batch_state_layout(dyn_batch_t b, uint64_t* offsets);
+
+/* A page-locked host area of the packed size, owned by the batch (freed by
+ * dyn_batch_destroy; reallocated, and the old pointer invalid, when a later
+ * call finds the batch has grown).  *n_floats receives the packed size. */
+int dyn_batch_host_buffer(dyn_batch_t b, float** buf, uint64_t* n_floats);
+
+/* Batch-wide drop-in step with the states on the host (dyn_sys_step_host
+ * for every member at once): one host->device copy of the packed state
+ * (state_in; NULL keeps the resident states), one launch that scatters it
+ * to the members, n_steps batch steps, one launch that gathers positions,
+ * velocities and every member's scalars, one device->host copy into
+ * state_out (NULL skips it) and one of the scalars; energies[i] receives
+ * member i's energies (NULL skips them).  state_in may equal state_out.
+ * Synchronous; returns the first member's device-side error, if any.
+ * Host buffers should be page-locked (dyn_batch_host_buffer) for full copy
+ * bandwidth.  No counterpart in the reference (src/integrate.rs:72 steps
+ * one MdState whose state lives on the host). */
+int dyn_batch_step_host(dyn_batch_t b, uint32_t n_steps, float dt, const float* state_in,
+                        float* state_out, dyn_energies_t* energies);
+
 /* Device memory the batch holds (members, block maps, views), in bytes. */
 int dyn_batch_memory(dyn_batch_t b, uint64_t* bytes);
 

@@ -82,3 +82,38 @@ def test_batch_rejects_mixed_intervals(gpu_lib):
     cfgs[1] = _cfg(systems[1], spme_interval=1)
     with pytest.raises(Exception):
         md.MdBatch(systems[:2], cfgs[:2])
+
+
+def test_batch_host_step_matches_members_host_step(gpu_lib):
+    """dyn_batch_step_host (one copy each way for the whole batch) gives
+    each member exactly what dyn_sys_step_host gives it alone on the same
+    host state, and reads back the states dyn_sys_get_state reads."""
+    systems, cfgs = _members()
+    batch = md.MdBatch(systems, cfgs)
+    buf = batch.host_buffer()
+    off = batch.state_layout()
+    assert len(buf) == off[-1] and len(off) == len(systems) + 1
+    # the resident states, read back through the packed path
+    batch.step_host(0.002, 3, None, buf)
+    for i, m in enumerate(batch.members):
+        s, v = m.state(), batch.unpack(buf, i)
+        for k in v:
+            np.testing.assert_array_equal(np.asarray(s[k], np.float32).reshape(v[k].shape), v[k],
+                                          err_msg=f"member {i} {k}")
+    host_in = buf.copy()
+    alone = []
+    for i, (s, c) in enumerate(zip(systems, cfgs)):
+        st = md.MdState(s, c)
+        st.step(0.002, 3)
+        io = {k: np.ascontiguousarray(a) for k, a in batch.unpack(host_in.copy(), i).items()}
+        e = st.step_host(0.002, 20, io, io)
+        alone.append((io, e))
+        st.close()
+    en = batch.step_host(0.002, 20, buf, buf, energies=True)
+    for i, (io, e) in enumerate(alone):
+        v = batch.unpack(buf, i)
+        for k in v:
+            np.testing.assert_array_equal(io[k], v[k], err_msg=f"member {i} {k}")
+        for k in ("potential", "kinetic", "virial", "temperature", "step", "list_rebuilds"):
+            assert e[k] == en[i][k], (i, k, e[k], en[i][k])
+    batch.close()
