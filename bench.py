@@ -626,8 +626,8 @@ def run_ours(args):
                                 "frac": round(achieved / peak.value, 4), "ms": round(pair_ms, 5),
                                 "algorithmic_flops": int(flops), "pairs_lj": n_lj, "pairs_coulomb": n_c},
         "roofline_spme": {
-            "spread": hbm_roofline(spread_bytes, stages["spme_spread"], hbm, "k_spread + k_spread_w + k_fix2real"),
-            "gather": hbm_roofline(gather_bytes, stages["spme_gather"], hbm, "k_gather + k_gather_w + k_recip_pass"),
+            "spread": hbm_roofline(spread_bytes, stages["spme_spread"], hbm, "k_bin_sites + k_spread_brick"),
+            "gather": hbm_roofline(gather_bytes, stages["spme_gather"], hbm, "k_gather_brick + k_gather_wfin + k_recip_pass"),
             "stage": hbm_roofline(pme_bytes, pme_ms, hbm, "whole SPME stage incl. cuFFT"),
             "note": "algorithmic bytes: spread N_q*16 + K^3*4, gather N_q*16 + K^3*4 + N_q*12; the grid stays "
                     "in L2, so GB/s below HBM peak is expected"},

@@ -34,6 +34,8 @@
 #define CH_MIX 8          // list entries per work item of the atom pair kernels (at most 32)
 #endif
 #define INVALID_ID 0xFFFFFFFFu
+#define PME_BRICK 8       // edge of the SPME grid bricks (grid points)
+#define DYN_SITE_WATER 0x80000000u  // site code flag: a water site (3 * id + site) rather than an atom
 #define WW_JFIX_SHIFT 16  // j-side water-water sums: int32 fixed point, 2^-16 kcal/mol/A
 #define NACC 16           // accumulator slots
 
@@ -87,6 +89,16 @@ struct Scalars {
     unsigned int need_prune;
     unsigned int max_dprune_bits;  // float bits, as max_disp2_bits
     unsigned long long prunes;
+    unsigned int spme_ovf;        // sites of this SPME pass beyond their brick's capacity
+    unsigned int spme_ovf_max;    // largest spme_ovf seen
+};
+
+// One charged site of an SPME pass, binned by the grid brick of its stencil
+// base: fractional grid coordinates, charge and base (x | y << 10 | z << 20).
+struct SiteRec {
+    double w[3];
+    float q;
+    uint32_t base;
 };
 
 // Partial-sum regions (each kernel family writes 4 doubles per block).
@@ -187,10 +199,22 @@ struct SysView {
     uint32_t lincs_order, lincs_iter;
     // PME
     uint32_t K[3];
-    long long* qgrid_fix;   // [K0*K1*K2]
+    long long* qgrid_fix;   // [K0*K1*K2] overflow charge (zero between passes)
     float* qgrid;           // real grid (cuFFT in/out)
     float2* cgrid;          // complex grid [K0*K1*(K2/2+1)]
     float* bmod[3];         // |b(m)|^2 per dimension
+    // grid bricks of the spread and gather (PME_BRICK^3 points each): the
+    // charged sites binned by their stencil base's brick, brick_cap per
+    // brick, the rest in the overflow list
+    uint32_t nbrick[3], n_bricks, brick_cap, n_sites_max;
+    uint32_t* brick_n;      // [n_bricks] sites binned this pass (the gather zeroes it)
+    uint32_t* brick_ovf;    // [n_bricks] 1: overflow charge for this brick waits in qgrid_fix
+    uint32_t* brick_nbr;    // [n_bricks][27] bricks whose sites reach the brick (INVALID_ID-padded)
+    SiteRec* brick_site;    // [n_bricks * brick_cap]
+    uint32_t* brick_sid;    // site codes (atom index, or DYN_SITE_WATER | 3 * water id + site)
+    SiteRec* ovf_site;      // [n_sites_max]
+    uint32_t* ovf_sid;
+    float* wsite_f;         // [nw*9] reciprocal force on H0, H1, M by water id, before corrections
     // box and scalars
     BoxDev* box;
     Scalars* sc;
@@ -415,6 +439,9 @@ void launch_pme_gather(const Target& t, int pass);
 void launch_corrections(const Target& t);
 int pme_blocks(const SysView& v);
 int gather_blocks(const SysView& v);
+// brick layout and capacity of the spread / gather (nbrick, n_bricks, brick_cap, n_sites_max)
+void pme_bricks(SysView& v, uint32_t cap);
+void pme_brick_sources(const SysView& v, std::vector<uint32_t>& out);
 int corr_blocks(const SysView& v);
 
 // integrate.cu

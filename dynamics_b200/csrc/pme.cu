@@ -10,6 +10,7 @@
 // indexed by original particle id and added by the kick kernels on every
 // step, which implements the reference's SPME-every-n-steps reuse
 // (src/lib.rs:1282-1341).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -62,35 +63,6 @@ __device__ __forceinline__ void bspline4d(double w, double* th) {
     th[3] = w3 * (1.0 / 6.0);
 }
 
-// Charge spreading with float64 weights and products, accumulated as 64-bit
-// fixed point (exact, order-independent sums).
-__device__ __forceinline__ void spread_one(const SysView& v, float3 p, float q, const BoxDev& b) {
-    int base[3];
-    double w[3];
-    grid_coord(p, b, v.K, base, w);
-    double tx[4], ty[4], tz[4];
-    bspline4d(w[0], tx);
-    bspline4d(w[1], ty);
-    bspline4d(w[2], tz);
-    const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
-    int iz[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) { int z = base[2] - 3 + c; iz[c] = z < 0 ? z + K2 : z; }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        int x = base[0] - 3 + a; x = x < 0 ? x + K0 : x;
-        const double qa = (double)q * tx[a];
-#pragma unroll
-        for (int bb = 0; bb < 4; ++bb) {
-            int y = base[1] - 3 + bb; y = y < 0 ? y + K1 : y;
-            const double qab = qa * ty[bb];
-            long long* row = v.qgrid_fix + ((size_t)x * K1 + y) * K2;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) fix_atomic_add(row + iz[c], fix_from_double(qab * tz[c]));
-        }
-    }
-}
-
 // Which charges an SPME pass spreads and gathers: pass 0 all of them;
 // with an alchemical molecule, pass 1 all but the molecule's (the
 // environment) and pass 2 the molecule's only (src/non_bonded.rs:709-743).
@@ -106,162 +78,253 @@ __device__ __forceinline__ float pass_weight(const SysView& v, int pass) {
     return pass == 0 ? v.alch_cs : 1.0f - v.alch_cs;
 }
 
-// one thread per charged atom (the water sites go by group, below)
-DYN_KERNEL(, k_spread, (, int pass), (, pass)) {
-    const BoxDev b = *v.box;
-    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < v.na; t += bk.cnt * blockDim.x) {
-        const float4 p = v.apos[t];
-        if (p.w != 0.f && pass_has_atom(v, pass, t)) spread_one(v, xyz(p), p.w, b);
-    }
-}
-
 // ---------------------------------------------------------------------------
-// Water sites by water group.  A CTA takes a 32-water group of the pair
-// kernels (spatially compact): the order-4 stencils of its 96 charged sites
-// fall in a small box of grid points, held in shared memory.  The spread
-// adds every contribution there (the same int64 fixed-point values as one
-// global atomic per contribution would add: integer sums in any order, so
-// the grid is bit-identical) and then adds the box's nonzero points to the
-// global grid, about half as many global atomics; the gather stages the
-// box once with coalesced loads and reads the stencils from shared memory
-// (the same float arithmetic in the same order as per site).  A group whose
-// box exceeds the tile (scattered waters in a dilute system) takes the
-// per-site path.
+// Spread and gather by grid bricks.
+//
+// Every SPME pass first bins the charged sites (water H0, H1, M and the
+// charged atoms) by the PME_BRICK^3 brick that holds their stencil base,
+// one record each (fractional grid coordinates, charge, base).  A site with
+// base b covers grid points b-3 .. b in each dimension, so the points of a
+// brick receive charge only from sites based in it or in the next bricks
+// up (up to 3 points on).  The spread gives each brick to one CTA, which
+// adds those sites' stencils in shared memory, exactly, and writes its
+// points once, converted to float: no global atomics and no separate
+// conversion pass.  The gather stages a brick with its 3-point halo and
+// evaluates its own sites' stencils from shared memory.  Sites beyond a
+// brick's capacity (rare: a capacity of about twice the mean) go to an
+// overflow list, spread with global fixed-point atomics that the brick's
+// CTA folds in, and gathered from the global grid, with the same values.
 // ---------------------------------------------------------------------------
-constexpr int SG_T = 128;               // threads per CTA
-constexpr int SG_SITES = 3 * GRPW;      // charged sites of a group
-constexpr int TILE_PTS = 4096;          // shared tile capacity (grid points)
+constexpr int SB_T = 256;                               // spread: threads per CTA
+constexpr int GB_T = 128;                               // gather: threads per CTA
+constexpr int BR3 = PME_BRICK * PME_BRICK * PME_BRICK;
+constexpr int HB = PME_BRICK + 3;                       // gather tile edge (brick + halo)
+constexpr int OVF_BLOCKS = 8;                           // gather CTAs for the overflow list
+constexpr int MAX_NBR = 27;                             // bricks whose sites can reach a brick
 
-struct GroupSites {
-    int base[SG_SITES][3];              // stencil base of each site
-    double w[SG_SITES][3];              // fractional grid coordinate
-    float3 pos[SG_SITES];
-    float q[SG_SITES];                  // 0: no site (padding slot)
-    int lo[3], n[3];                    // tile origin (relative to ref) and size
-    int ref[3];                         // base of the first site
-    int use_tile;
-};
-
-// Fills the group's sites and its tile box (whole CTA; ends synchronised).
-__device__ __forceinline__ void group_sites(const SysView& v, uint32_t g, const BoxDev& b, GroupSites& gs) {
-    const int tid = threadIdx.x;
-    if (tid < 3) { gs.lo[tid] = 1 << 30; gs.n[tid] = -(1 << 30); }
-    for (int t = tid; t < SG_SITES; t += SG_T) {
-        const uint32_t s = g * GRPW + t / 3;
-        const bool ok = s < v.nw_cap && v.wid[s] != INVALID_ID;
-        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (ok) p = v.wpos[4 * s + 1 + t % 3];
-        gs.pos[t] = xyz(p);
-        gs.q[t] = ok ? p.w : 0.f;
-        int bs[3];
-        double ww[3];
-        grid_coord(xyz(p), b, v.K, bs, ww);
-        for (int a = 0; a < 3; ++a) { gs.base[t][a] = bs[a]; gs.w[t][a] = ww[a]; }
-    }
-    __syncthreads();
-    if (tid == 0) {
-        int f = 0;
-        while (f < SG_SITES && gs.q[f] == 0.f) ++f;
-        for (int a = 0; a < 3; ++a) gs.ref[a] = f < SG_SITES ? gs.base[f][a] : 0;
-    }
-    __syncthreads();
-    for (int t = tid; t < SG_SITES; t += SG_T) {
-        if (gs.q[t] == 0.f) continue;
-        for (int a = 0; a < 3; ++a) {
-            const int K = (int)v.K[a];
-            int r = gs.base[t][a] - gs.ref[a];
-            r -= K * (int)floorf((float)r / (float)K + 0.5f);  // nearest image, |r| <= K/2
-            atomicMin(&gs.lo[a], r - 3);
-            atomicMax(&gs.n[a], r);
-        }
-    }
-    __syncthreads();
-    if (tid == 0) {
-        long long pts = 1;
-        bool fits = true;
-        for (int a = 0; a < 3; ++a) {
-            gs.n[a] = gs.n[a] - gs.lo[a] + 1;
-            fits = fits && gs.n[a] > 0 && gs.n[a] <= (int)v.K[a];
-            pts *= gs.n[a] > 0 ? gs.n[a] : 0;
-        }
-        gs.use_tile = fits && pts > 0 && pts <= TILE_PTS;
-    }
-    __syncthreads();
+__device__ __forceinline__ void rec_base(uint32_t b, int* base) {
+    base[0] = (int)(b & 1023u);
+    base[1] = (int)((b >> 10) & 1023u);
+    base[2] = (int)(b >> 20);
 }
 
-// tile offset of a site's stencil point (a, bb, c) and the grid index of a tile point
-__device__ __forceinline__ int rel_base(const SysView& v, const GroupSites& gs, int t, int a) {
-    const int K = (int)v.K[a];
-    int r = gs.base[t][a] - gs.ref[a];
-    r -= K * (int)floorf((float)r / (float)K + 0.5f);
-    return r - gs.lo[a];
+__device__ __forceinline__ SiteRec make_rec(float3 p, float q, const BoxDev& b, const uint32_t* K) {
+    int base[3];
+    double w[3];
+    grid_coord(p, b, K, base, w);
+    SiteRec r;
+    r.w[0] = w[0]; r.w[1] = w[1]; r.w[2] = w[2];
+    r.q = q;
+    r.base = (uint32_t)base[0] | ((uint32_t)base[1] << 10) | ((uint32_t)base[2] << 20);
+    return r;
 }
-__device__ __forceinline__ size_t tile_to_grid(const SysView& v, const GroupSites& gs, int idx) {
-    const int z = idx % gs.n[2], y = (idx / gs.n[2]) % gs.n[1], x = idx / (gs.n[2] * gs.n[1]);
-    int gi[3] = {x, y, z};
+
+__device__ __forceinline__ uint32_t brick_index(const SysView& v, int x, int y, int z) {
+    return ((uint32_t)(x / PME_BRICK) * v.nbrick[1] + (uint32_t)(y / PME_BRICK)) * v.nbrick[2] +
+           (uint32_t)(z / PME_BRICK);
+}
+
+__device__ __forceinline__ void brick_origin(const SysView& v, uint32_t P, int* o, int* ext) {
+    const uint32_t nb1 = v.nbrick[1], nb2 = v.nbrick[2];
+    const uint32_t p[3] = {P / (nb1 * nb2), (P / nb2) % nb1, P % nb2};
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const int K = (int)v.K[a];
-        int u = gs.ref[a] + gs.lo[a] + gi[a];
-        u %= K;
-        if (u < 0) u += K;
-        gi[a] = u;
+        o[a] = (int)p[a] * PME_BRICK;
+        ext[a] = min(PME_BRICK, (int)v.K[a] - o[a]);
     }
-    return ((size_t)gi[0] * v.K[1] + gi[1]) * v.K[2] + gi[2];
 }
 
-DYN_KERNEL(__launch_bounds__(SG_T), k_spread_w, (, int pass), (, pass)) {
-    if (pass == 2) return;  // the alchemical molecule's own pass holds no water
-    __shared__ GroupSites gs;
-    __shared__ unsigned long long tile[TILE_PTS];
-    const BoxDev b = *v.box;
-    const uint32_t ng = (v.sc->n_wclus + GRPW / WCL - 1) / (GRPW / WCL);
-    const int tid = threadIdx.x;
-    for (uint32_t g = bk.idx; g < ng; g += bk.cnt) {
-        group_sites(v, g, b, gs);
-        if (!gs.use_tile) {
-            for (int t = tid; t < SG_SITES; t += SG_T)
-                if (gs.q[t] != 0.f) spread_one(v, gs.pos[t], gs.q[t], b);
-            __syncthreads();
-            continue;
+// An overflow site: its contributions go to the global fixed-point grid
+// (float64 weights and products, the values the brick path adds), and the
+// bricks they land in are flagged for their spread CTAs to fold in.
+__device__ void spread_global(const SysView& v, const SiteRec& r) {
+    int base[3];
+    rec_base(r.base, base);
+    double tx[4], ty[4], tz[4];
+    bspline4d(r.w[0], tx);
+    bspline4d(r.w[1], ty);
+    bspline4d(r.w[2], tz);
+    const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
+    int iz[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) { int z = base[2] - 3 + c; iz[c] = z < 0 ? z + K2 : z; }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        int x = base[0] - 3 + a; x = x < 0 ? x + K0 : x;
+        const double qa = (double)r.q * tx[a];
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            int y = base[1] - 3 + bb; y = y < 0 ? y + K1 : y;
+            const double qab = qa * ty[bb];
+            long long* row = v.qgrid_fix + ((size_t)x * K1 + y) * K2;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) fix_atomic_add(row + iz[c], fix_from_double(qab * tz[c]));
         }
-        const int npts = gs.n[0] * gs.n[1] * gs.n[2];
-        for (int i = tid; i < npts; i += SG_T) tile[i] = 0ull;
+    }
+    // per dimension the stencil spans the bricks of base - 3 (wrapped) and base
+    int lo[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { lo[a] = base[a] - 3; if (lo[a] < 0) lo[a] += (int)v.K[a]; }
+    for (int m = 0; m < 8; ++m)
+        v.brick_ovf[brick_index(v, (m & 1) ? base[0] : lo[0], (m & 2) ? base[1] : lo[1], (m & 4) ? base[2] : lo[2])] = 1u;
+}
+
+// Bins the pass's charged sites by brick (records and site codes).  Atoms
+// without charge get a zero reciprocal force on pass 0, as they have none.
+DYN_KERNEL(, k_bin_sites, (, int pass), (, pass)) {
+    const BoxDev b = *v.box;
+    const uint32_t nws = pass == 2 ? 0u : 3u * v.nw_cap;  // the molecule's own pass holds no water
+    const uint32_t total = nws + v.na;
+    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
+        float4 p;
+        uint32_t sid;
+        if (t < nws) {
+            const uint32_t s = t / 3u, k = t % 3u;
+            const uint32_t id = v.wid[s];
+            if (id == INVALID_ID) continue;
+            p = v.wpos[4 * s + 1 + k];
+            sid = DYN_SITE_WATER | (3u * id + k);
+        } else {
+            const uint32_t a = t - nws;
+            if (!pass_has_atom(v, pass, a)) continue;
+            p = v.apos[a];
+            if (p.w == 0.f) {
+                if (pass == 0) {
+                    long long* c = v.arecip + 3 * (size_t)a;
+                    c[0] = 0; c[1] = 0; c[2] = 0;
+                }
+                continue;
+            }
+            sid = a;
+        }
+        const SiteRec r = make_rec(xyz(p), p.w, b, v.K);
+        int base[3];
+        rec_base(r.base, base);
+        const uint32_t P = brick_index(v, base[0], base[1], base[2]);
+        const uint32_t slot = atomicAdd(&v.brick_n[P], 1u);
+        if (slot < v.brick_cap) {
+            v.brick_site[(size_t)P * v.brick_cap + slot] = r;
+            v.brick_sid[(size_t)P * v.brick_cap + slot] = sid;
+        } else {
+            const uint32_t o = atomicAdd(&v.sc->spme_ovf, 1u);  // < n_sites_max: one entry per site
+            v.ovf_site[o] = r;
+            v.ovf_sid[o] = sid;
+            spread_global(v, r);
+        }
+    }
+}
+
+// One CTA per brick: the charge of every site whose stencil reaches the
+// brick, summed in shared memory, written once as the float grid.  Each
+// int64 contribution f is added as two native 32-bit atomics, f >> 18 and
+// its low 18 bits, whose sums give the int64 sum exactly (a grid point gets
+// at most 8 x brick_cap <= 4096 contributions of magnitude below 2^37: no
+// int32 sum overflows).
+constexpr int SPLIT = 18;
+
+DYN_KERNEL(__launch_bounds__(SB_T), k_spread_brick, (, int pass), (, pass)) {
+    __shared__ int acc_hi[BR3], acc_lo[BR3];
+    __shared__ uint32_t nbr[MAX_NBR];
+    __shared__ uint32_t cnt[MAX_NBR + 1];
+    __shared__ int fold_s;
+    const int tid = threadIdx.x;
+    const int K[3] = {(int)v.K[0], (int)v.K[1], (int)v.K[2]};
+    for (uint32_t P = bk.idx; P < v.n_bricks; P += bk.cnt) {
+        int o[3], ext[3];
+        brick_origin(v, P, o, ext);
+        if (tid < 32) {
+            // the bricks whose sites reach this one (host-made list) and
+            // their task counts, scanned across the warp
+            const uint32_t q = tid < MAX_NBR ? v.brick_nbr[(size_t)P * MAX_NBR + tid] : INVALID_ID;
+            uint32_t c = q != INVALID_ID ? 4u * min(v.brick_n[q], v.brick_cap) : 0u;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xffffffffu, c, d);
+                if (tid >= d) c += x;
+            }
+            if (tid < MAX_NBR) { nbr[tid] = q; cnt[tid + 1] = c; }
+            if (tid == 0) { cnt[0] = 0u; fold_s = v.brick_ovf[P] != 0u; }
+        }
+        for (int i = tid; i < BR3; i += SB_T) { acc_hi[i] = 0; acc_lo[i] = 0; }
         __syncthreads();
-        // one (site, x plane) per thread and round: 16 contributions each
-        for (int u = tid; u < SG_SITES * 4; u += SG_T) {
-            const int t = u >> 2, a = u & 3;
-            if (gs.q[t] == 0.f) continue;
+        // one (site, x plane) per thread and round: up to 16 contributions
+        const uint32_t total = cnt[MAX_NBR];
+        for (uint32_t u = tid; u < total; u += SB_T) {
+            int j = 0;
+            while (u >= cnt[j + 1]) ++j;
+            const uint32_t e = (u - cnt[j]) >> 2;
+            const int a = (int)((u - cnt[j]) & 3u);
+            const SiteRec r = v.brick_site[(size_t)nbr[j] * v.brick_cap + e];
+            int base[3];
+            rec_base(r.base, base);
+            int x = base[0] - 3 + a;
+            if (x < 0) x += K[0];
+            const int lx = x - o[0];
+            if (lx < 0 || lx >= ext[0]) continue;
+            int ly[4], lz[4];
+            bool any_y = false, any_z = false;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                int y = base[1] - 3 + c, z = base[2] - 3 + c;
+                if (y < 0) y += K[1];
+                if (z < 0) z += K[2];
+                ly[c] = y - o[1];
+                lz[c] = z - o[2];
+                if (ly[c] < 0 || ly[c] >= ext[1]) ly[c] = -1; else any_y = true;
+                if (lz[c] < 0 || lz[c] >= ext[2]) lz[c] = -1; else any_z = true;
+            }
+            if (!any_y || !any_z) continue;
             double tx[4], ty[4], tz[4];
-            bspline4d(gs.w[t][0], tx);
-            bspline4d(gs.w[t][1], ty);
-            bspline4d(gs.w[t][2], tz);
-            const int x = rel_base(v, gs, t, 0) - 3 + a;
-            const int y0 = rel_base(v, gs, t, 1) - 3, z0 = rel_base(v, gs, t, 2) - 3;
-            const double qa = (double)gs.q[t] * tx[a];
+            bspline4d(r.w[0], tx);
+            bspline4d(r.w[1], ty);
+            bspline4d(r.w[2], tz);
+            const double qa = (double)r.q * tx[a];
 #pragma unroll
             for (int bb = 0; bb < 4; ++bb) {
+                if (ly[bb] < 0) continue;
                 const double qab = qa * ty[bb];
-                const int row = (x * gs.n[1] + (y0 + bb)) * gs.n[2] + z0;
+                const int row = (lx * PME_BRICK + ly[bb]) * PME_BRICK;
 #pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    atomicAdd(&tile[row + c], (unsigned long long)fix_from_double(qab * tz[c]));
+                for (int c = 0; c < 4; ++c) {
+                    if (lz[c] < 0) continue;
+                    const long long f = fix_from_double(qab * tz[c]);
+                    atomicAdd(&acc_hi[row + lz[c]], (int)(f >> SPLIT));
+                    atomicAdd(&acc_lo[row + lz[c]], (int)(f & ((1ll << SPLIT) - 1)));
+                }
             }
         }
         __syncthreads();
-        for (int i = tid; i < npts; i += SG_T) {
-            const long long q = (long long)tile[i];
-            if (q != 0) fix_atomic_add(v.qgrid_fix + tile_to_grid(v, gs, i), q);
+        const bool fold = fold_s != 0;
+        for (int i = tid; i < BR3; i += SB_T) {
+            const int lx = i / (PME_BRICK * PME_BRICK), ly = (i / PME_BRICK) % PME_BRICK, lz = i % PME_BRICK;
+            if (lx < ext[0] && ly < ext[1] && lz < ext[2]) {
+                const size_t gi = ((size_t)(o[0] + lx) * K[1] + (o[1] + ly)) * K[2] + (o[2] + lz);
+                long long q = (long long)acc_hi[i] * (1ll << SPLIT) + (long long)acc_lo[i];
+                if (fold) {
+                    // overflow sites' charge from the global fixed-point grid
+                    q += v.qgrid_fix[gi];
+                    v.qgrid_fix[gi] = 0;
+                }
+                v.qgrid[gi] = (float)((double)q * DYN_FIX_INV);
+            }
         }
-        __syncthreads();
+        if (tid == 0 && fold) v.brick_ovf[P] = 0u;
+        __syncthreads();  // the sums and the brick list are refilled by the next brick
     }
 }
 
-DYN_KERNEL(, k_fix2real, (), ()) {
-    const uint32_t n = v.K[0] * v.K[1] * v.K[2];
-    for (uint32_t i = bk.idx * blockDim.x + threadIdx.x; i < n; i += bk.cnt * blockDim.x) {
-        v.qgrid[i] = (float)((double)v.qgrid_fix[i] * DYN_FIX_INV);
-        v.qgrid_fix[i] = 0;
-    }
+// -q q erf(alpha r)/r between two sites, float64 from the exact float64
+// displacement (dx, dy, dz); returns the energy and the force on the first
+__device__ __forceinline__ double excl_corr(double dx, double dy, double dz, double qq, double alpha,
+                                           double3* f) {
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double r = sqrt(r2);
+    const double ar = alpha * r;
+    const double er = erf(ar);
+    const double du = qq * (er / r2 - 2.0 * alpha * 0.5641895835477563 * exp(-ar * ar) / r);
+    const double s = -du / r;
+    f->x = s * dx; f->y = s * dy; f->z = s * dz;
+    return -qq * er / r;
 }
 
 // Influence function B(m) C(m) applied in place; energy and virial of the
@@ -303,30 +366,26 @@ DYN_KERNEL(, k_convolve, (), ()) {
     }
 }
 
-__device__ __forceinline__ float3 gather_one(const SysView& v, float3 p, float q, const BoxDev& b) {
-    int base[3];
-    double wd[3];
-    grid_coord(p, b, v.K, base, wd);
+
+// The gather of one site, grid values from at(a, bb, c) (stencil point
+// base - 3 + (a, bb, c)): float B-splines of the float64 fractional
+// coordinates and this order of fused multiply-adds, from shared memory or
+// from the global grid alike.
+template <typename G>
+__device__ __forceinline__ float3 gather_rec(const SysView& v, const SiteRec& r, const BoxDev& b, G at) {
     float tx[4], ty[4], tz[4], dx[4], dy[4], dz[4];
-    bspline4((float)wd[0], tx, dx);
-    bspline4((float)wd[1], ty, dy);
-    bspline4((float)wd[2], tz, dz);
-    const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
-    int iz[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) { int z = base[2] - 3 + c; iz[c] = z < 0 ? z + K2 : z; }
+    bspline4((float)r.w[0], tx, dx);
+    bspline4((float)r.w[1], ty, dy);
+    bspline4((float)r.w[2], tz, dz);
     float gx = 0.f, gy = 0.f, gz = 0.f;
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-        int x = base[0] - 3 + a; x = x < 0 ? x + K0 : x;
 #pragma unroll
         for (int bb = 0; bb < 4; ++bb) {
-            int y = base[1] - 3 + bb; y = y < 0 ? y + K1 : y;
-            const float* row = v.qgrid + ((size_t)x * K1 + y) * K2;
             float sz = 0.f, sdz = 0.f;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                const float ph = __ldg(row + iz[c]);
+                const float ph = at(a, bb, c);
                 sz = fmaf(tz[c], ph, sz);
                 sdz = fmaf(dz[c], ph, sdz);
             }
@@ -335,136 +394,125 @@ __device__ __forceinline__ float3 gather_one(const SysView& v, float3 p, float q
             gz = fmaf(tx[a] * ty[bb], sdz, gz);
         }
     }
-    return f3(-q * K0 * b.inv_ext[0] * gx, -q * K1 * b.inv_ext[1] * gy, -q * K2 * b.inv_ext[2] * gz);
-}
-
-// -q q erf(alpha r)/r between two sites, float64 from the exact float64
-// displacement (dx, dy, dz); returns the energy and the force on the first
-__device__ __forceinline__ double excl_corr(double dx, double dy, double dz, double qq, double alpha,
-                                           double3* f) {
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const double r = sqrt(r2);
-    const double ar = alpha * r;
-    const double er = erf(ar);
-    const double du = qq * (er / r2 - 2.0 * alpha * 0.5641895835477563 * exp(-ar * ar) / r);
-    const double s = -du / r;
-    f->x = s * dx; f->y = s * dy; f->z = s * dz;
-    return -qq * er / r;
-}
-
-// Gather for the atoms: one thread per atom, writing the reciprocal cache.
-// Pass 0 stores its (weighted) forces, later passes add theirs.
-DYN_KERNEL(, k_gather, (, int pass), (, pass)) {
-    const BoxDev b = *v.box;
-    const float wt = pass_weight(v, pass);
-    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < v.na; t += bk.cnt * blockDim.x) {
-        if (!pass_has_atom(v, pass, t)) continue;
-        const float4 p = v.apos[t];
-        float3 f = f3(0.f, 0.f, 0.f);
-        if (p.w != 0.f) f = gather_one(v, xyz(p), p.w, b) * wt;
-        long long* c = v.arecip + 3 * (size_t)t;
-        if (pass == 0) {
-            c[0] = fix_from_float(f.x); c[1] = fix_from_float(f.y); c[2] = fix_from_float(f.z);
-        } else {
-            c[0] += fix_from_float(f.x); c[1] += fix_from_float(f.y); c[2] += fix_from_float(f.z);
-        }
-    }
-}
-
-// The gather of one site from a staged tile: gather_one's arithmetic, in its
-// order, with the grid values read from shared memory.
-__device__ __forceinline__ float3 gather_tile(const SysView& v, const GroupSites& gs, const float* tile, int t,
-                                              const BoxDev& b) {
-    float tx[4], ty[4], tz[4], dx[4], dy[4], dz[4];
-    bspline4((float)gs.w[t][0], tx, dx);
-    bspline4((float)gs.w[t][1], ty, dy);
-    bspline4((float)gs.w[t][2], tz, dz);
-    const int x0 = rel_base(v, gs, t, 0) - 3, y0 = rel_base(v, gs, t, 1) - 3, z0 = rel_base(v, gs, t, 2) - 3;
-    float gx = 0.f, gy = 0.f, gz = 0.f;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-#pragma unroll
-        for (int bb = 0; bb < 4; ++bb) {
-            const float* row = tile + ((x0 + a) * gs.n[1] + (y0 + bb)) * gs.n[2] + z0;
-            float sz = 0.f, sdz = 0.f;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const float ph = row[c];
-                sz = fmaf(tz[c], ph, sz);
-                sdz = fmaf(dz[c], ph, sdz);
-            }
-            gx = fmaf(dx[a] * ty[bb], sz, gx);
-            gy = fmaf(tx[a] * dy[bb], sz, gy);
-            gz = fmaf(tx[a] * ty[bb], sdz, gz);
-        }
-    }
-    const float q = gs.q[t];
+    const float q = r.q;
     return f3(-q * v.K[0] * b.inv_ext[0] * gx, -q * v.K[1] * b.inv_ext[1] * gy, -q * v.K[2] * b.inv_ext[2] * gz);
 }
 
-// Gather for the water sites by group (tile as for the spread), writing the
-// reciprocal cache by original water id.  With Ewald corrections on, the
-// intra-water exclusion corrections (H0-H1, H0-M, H1-M) are added here in
-// float64.  Pass 0 stores its (weighted) forces, later passes add theirs.
-DYN_KERNEL(__launch_bounds__(SG_T), k_gather_w, (, int pass), (, pass)) {
-    __shared__ GroupSites gs;
-    __shared__ float tile[TILE_PTS];
-    __shared__ float3 fsite[SG_SITES];
+// A site's reciprocal force: atoms into the reciprocal cache (pass 0 stores,
+// later passes add), water sites into the per-site scratch for
+// k_gather_wfin.
+__device__ __forceinline__ void gather_out(const SysView& v, uint32_t sid, float3 f, int pass) {
+    if (sid & DYN_SITE_WATER) {
+        float* o = v.wsite_f + 3 * (size_t)(sid & ~DYN_SITE_WATER);
+        o[0] = f.x; o[1] = f.y; o[2] = f.z;
+        return;
+    }
+    long long* c = v.arecip + 3 * (size_t)sid;
+    if (pass == 0) {
+        c[0] = fix_from_float(f.x); c[1] = fix_from_float(f.y); c[2] = fix_from_float(f.z);
+    } else {
+        c[0] += fix_from_float(f.x); c[1] += fix_from_float(f.y); c[2] += fix_from_float(f.z);
+    }
+}
+
+// One CTA per brick: the brick and its 3-point halo staged once, its sites'
+// stencils read from shared memory; the last OVF_BLOCKS CTAs take the
+// overflow list from the global grid.  Each brick's count is cleared for
+// the next pass.
+DYN_KERNEL(__launch_bounds__(GB_T), k_gather_brick, (, int pass), (, pass)) {
+    __shared__ float tile[HB * HB * HB];
     const BoxDev b = *v.box;
-    const bool corr = pass == 0 && (v.flags & DYN_FLAG_EWALD_CORRECTIONS);
     const float wt = pass_weight(v, pass);
-    const uint32_t ng = (v.sc->n_wclus + GRPW / WCL - 1) / (GRPW / WCL);
     const int tid = threadIdx.x;
-    double e_c = 0.0, w_c = 0.0;
-    for (uint32_t g = bk.idx; g < ng && pass != 2; g += bk.cnt) {
-        group_sites(v, g, b, gs);
-        if (gs.use_tile) {
-            const int npts = gs.n[0] * gs.n[1] * gs.n[2];
-            for (int i = tid; i < npts; i += SG_T) tile[i] = __ldg(v.qgrid + tile_to_grid(v, gs, i));
-            __syncthreads();
+    const int K[3] = {(int)v.K[0], (int)v.K[1], (int)v.K[2]};
+    for (uint32_t P = bk.idx; P < v.n_bricks + OVF_BLOCKS; P += bk.cnt) {
+        if (P >= v.n_bricks) {
+            const uint32_t n = v.sc->spme_ovf;
+            for (uint32_t t = (P - v.n_bricks) * GB_T + tid; t < n; t += OVF_BLOCKS * GB_T) {
+                const SiteRec r = v.ovf_site[t];
+                int base[3];
+                rec_base(r.base, base);
+                int ix[4], iy[4], iz[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    ix[c] = base[0] - 3 + c; if (ix[c] < 0) ix[c] += K[0];
+                    iy[c] = base[1] - 3 + c; if (iy[c] < 0) iy[c] += K[1];
+                    iz[c] = base[2] - 3 + c; if (iz[c] < 0) iz[c] += K[2];
+                }
+                const float3 f = gather_rec(v, r, b, [&](int a, int bb, int c) {
+                    return __ldg(v.qgrid + ((size_t)ix[a] * K[1] + iy[bb]) * K[2] + iz[c]);
+                }) * wt;
+                gather_out(v, v.ovf_sid[t], f, pass);
+            }
+            continue;
         }
-        for (int t = tid; t < SG_SITES; t += SG_T) {
-            float3 f = f3(0.f, 0.f, 0.f);
-            if (gs.q[t] != 0.f)
-                f = (gs.use_tile ? gather_tile(v, gs, tile, t, b) : gather_one(v, gs.pos[t], gs.q[t], b)) * wt;
-            fsite[t] = f;
+        int o[3], ext[3];
+        brick_origin(v, P, o, ext);
+#pragma unroll 4
+        for (int i = tid; i < HB * HB * HB; i += GB_T) {
+            int x = o[0] - 3 + i / (HB * HB), y = o[1] - 3 + (i / HB) % HB, z = o[2] - 3 + i % HB;
+            x = x < 0 ? x + K[0] : (x >= K[0] ? x - K[0] : x);
+            y = y < 0 ? y + K[1] : (y >= K[1] ? y - K[1] : y);
+            z = z < 0 ? z + K[2] : (z >= K[2] ? z - K[2] : z);
+            tile[i] = __ldg(v.qgrid + ((size_t)x * K[1] + y) * K[2] + z);
         }
         __syncthreads();
-        for (int w = tid; w < GRPW; w += SG_T) {
-            const uint32_t s = g * GRPW + w;
-            if (s >= v.nw_cap) continue;
-            const uint32_t id = v.wid[s];
-            if (id == INVALID_ID) continue;
-            double3 fs[3];
-            float3 ps[3];
+        const uint32_t n = min(v.brick_n[P], v.brick_cap);
+        for (uint32_t t = tid; t < n; t += GB_T) {
+            const size_t e = (size_t)P * v.brick_cap + t;
+            const SiteRec r = v.brick_site[e];
+            int base[3];
+            rec_base(r.base, base);
+            // stencil point a of the site is tile row (base - o) + a
+            const int x0 = base[0] - o[0], y0 = base[1] - o[1], z0 = base[2] - o[2];
+            const float3 f = gather_rec(v, r, b, [&](int a, int bb, int c) {
+                return tile[((x0 + a) * HB + (y0 + bb)) * HB + z0 + c];
+            }) * wt;
+            gather_out(v, v.brick_sid[e], f, pass);
+        }
+        __syncthreads();  // every thread has read the count; the tile is refilled next
+        if (tid == 0) v.brick_n[P] = 0u;
+    }
+}
+
+// Water reciprocal forces by molecule, into the cache by original id: the
+// sites' gathered forces in float64 plus, with Ewald corrections on, the
+// intra-water exclusion corrections (H0-H1, H0-M, H1-M).  Pass 0 stores,
+// later passes add.
+DYN_KERNEL(, k_gather_wfin, (, int pass), (, pass)) {
+    const bool corr = pass == 0 && (v.flags & DYN_FLAG_EWALD_CORRECTIONS);
+    double e_c = 0.0, w_c = 0.0;
+    for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.nw_cap; s += bk.cnt * blockDim.x) {
+        const uint32_t id = v.wid[s];
+        if (id == INVALID_ID) continue;
+        double3 fs[3];
+        float3 ps[3];
+        for (int k = 0; k < 3; ++k) {
+            ps[k] = xyz(v.wpos[4 * s + 1 + k]);
+            const float* f = v.wsite_f + 9 * (size_t)id + 3 * k;
+            fs[k] = make_double3(f[0], f[1], f[2]);
+        }
+        if (corr) {
+            const double q[3] = {OPC_Q_H, OPC_Q_H, OPC_Q_EP};
+            const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
             for (int k = 0; k < 3; ++k) {
-                ps[k] = gs.pos[3 * w + k];
-                const float3 f = fsite[3 * w + k];
-                fs[k] = make_double3(f.x, f.y, f.z);
-            }
-            if (corr) {
-                const double q[3] = {OPC_Q_H, OPC_Q_H, OPC_Q_EP};
-                const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
-                for (int k = 0; k < 3; ++k) {
-                    double3 f;
-                    const double dx = (double)ps[pa[k]].x - (double)ps[pb[k]].x;
-                    const double dy = (double)ps[pa[k]].y - (double)ps[pb[k]].y;
-                    const double dz = (double)ps[pa[k]].z - (double)ps[pb[k]].z;
-                    e_c += excl_corr(dx, dy, dz, q[pa[k]] * q[pb[k]], (double)v.alpha, &f);
-                    w_c += f.x * dx + f.y * dy + f.z * dz;
-                    fs[pa[k]].x += f.x; fs[pa[k]].y += f.y; fs[pa[k]].z += f.z;
-                    fs[pb[k]].x -= f.x; fs[pb[k]].y -= f.y; fs[pb[k]].z -= f.z;
-                }
-            }
-            long long* c = v.wrecip + 9 * (size_t)id;
-            for (int k = 0; k < 3; ++k) {
-                const long long fx = fix_from_double(fs[k].x), fy = fix_from_double(fs[k].y),
-                                fz = fix_from_double(fs[k].z);
-                if (pass == 0) { c[3 * k + 0] = fx; c[3 * k + 1] = fy; c[3 * k + 2] = fz; }
-                else { c[3 * k + 0] += fx; c[3 * k + 1] += fy; c[3 * k + 2] += fz; }
+                double3 f;
+                const double dx = (double)ps[pa[k]].x - (double)ps[pb[k]].x;
+                const double dy = (double)ps[pa[k]].y - (double)ps[pb[k]].y;
+                const double dz = (double)ps[pa[k]].z - (double)ps[pb[k]].z;
+                e_c += excl_corr(dx, dy, dz, q[pa[k]] * q[pb[k]], (double)v.alpha, &f);
+                w_c += f.x * dx + f.y * dy + f.z * dz;
+                fs[pa[k]].x += f.x; fs[pa[k]].y += f.y; fs[pa[k]].z += f.z;
+                fs[pb[k]].x -= f.x; fs[pb[k]].y -= f.y; fs[pb[k]].z -= f.z;
             }
         }
-        __syncthreads();  // gs, the tile and fsite are refilled by the next group
+        long long* c = v.wrecip + 9 * (size_t)id;
+        for (int k = 0; k < 3; ++k) {
+            const long long fx = fix_from_double(fs[k].x), fy = fix_from_double(fs[k].y),
+                            fz = fix_from_double(fs[k].z);
+            if (pass == 0) { c[3 * k + 0] = fx; c[3 * k + 1] = fy; c[3 * k + 2] = fz; }
+            else { c[3 * k + 0] += fx; c[3 * k + 1] += fy; c[3 * k + 2] += fz; }
+        }
     }
     if (pass != 0) return;  // the intra-water corrections belong to pass 0
     double x[2] = {e_c, w_c};
@@ -549,6 +597,9 @@ DYN_KERNEL(, k_recip_pass, (, int pass), (, pass)) {
     block_sum_d<2>(x);
     if (threadIdx.x != 0) return;
     Scalars* sc = v.sc;
+    // the pass's overflow list is done with (k_bin_sites fills the next)
+    sc->spme_ovf_max = max(sc->spme_ovf_max, sc->spme_ovf);
+    sc->spme_ovf = 0u;
     const double w = (double)pass_weight(v, pass);
     const double dc = v.alch_on ? (double)v.alch_dcs : 0.0;
     if (pass == 0) {
@@ -598,9 +649,45 @@ namespace dyn {
 int pme_blocks(const SysView& v) {
     return gblocks(v, (uint64_t)v.K[0] * v.K[1] * (v.K[2] / 2 + 1));
 }
-// blocks of the water-group SPME kernels (k_gather_w writes REG_CORR partials)
-int gather_blocks(const SysView& v) {
-    return v.nw ? (int)std::min<uint32_t>(v.ngrp_cap, v.max_blocks) : 0;
+// blocks of k_gather_wfin (which writes the REG_CORR partials)
+int gather_blocks(const SysView& v) { return v.nw ? gblocks(v, v.nw_cap) : 0; }
+
+// The brick layout of the grid and the per-brick capacity (cap, or by
+// default about twice the mean charged sites per brick plus 32, a multiple
+// of 32: liquid densities vary far less), at most 512; the overflow list
+// takes the rest.
+void pme_bricks(SysView& v, uint32_t cap) {
+    uint32_t n = 1;
+    for (int a = 0; a < 3; ++a) {
+        v.nbrick[a] = (v.K[a] + PME_BRICK - 1) / PME_BRICK;
+        n *= v.nbrick[a];
+    }
+    v.n_bricks = n;
+    v.n_sites_max = 3u * v.nw + v.na;
+    const uint32_t mean = (v.n_sites_max + n - 1) / n;
+    v.brick_cap = std::min(512u, cap ? cap : (2u * mean + 32u + 31u) / 32u * 32u);
+}
+
+// Per brick, the distinct bricks holding the stencil bases that reach it:
+// in each dimension those of grid points o .. o + ext + 2 (a base b covers
+// b - 3 .. b); MAX_NBR entries per brick, INVALID_ID after the last.
+void pme_brick_sources(const SysView& v, std::vector<uint32_t>& out) {
+    out.assign((size_t)v.n_bricks * MAX_NBR, INVALID_ID);
+    for (uint32_t P = 0; P < v.n_bricks; ++P) {
+        const uint32_t p[3] = {P / (v.nbrick[1] * v.nbrick[2]), (P / v.nbrick[2]) % v.nbrick[1], P % v.nbrick[2]};
+        std::vector<uint32_t> lst[3];
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t o = p[a] * PME_BRICK, ext = std::min<uint32_t>(PME_BRICK, v.K[a] - o);
+            for (uint32_t d = 0; d <= ext + 2; ++d) {
+                const uint32_t q = ((o + d) % v.K[a]) / PME_BRICK;
+                if (std::find(lst[a].begin(), lst[a].end(), q) == lst[a].end()) lst[a].push_back(q);
+            }
+        }
+        size_t n = 0;
+        for (uint32_t i : lst[0])
+            for (uint32_t j : lst[1])
+                for (uint32_t k : lst[2]) out[(size_t)P * MAX_NBR + n++] = (i * v.nbrick[1] + j) * v.nbrick[2] + k;
+    }
 }
 int corr_blocks(const SysView& v) { return gblocks(v, (uint64_t)v.n14 + v.nexcl); }
 
@@ -672,12 +759,10 @@ void each_fft(const Target& t, F f) {
 // one SPME pass in three parts (the stage timer times them apart)
 void launch_pme_spread(const Target& t, int pass) {
     auto on = [pass](const SysView& v) { return pass == 0 || v.alch_on != 0u; };
-    t.launch(k_spread, k_spread_batch, [&](const SysView& v) { return on(v) && v.na ? gblocks(v, v.na) : 0; },
-             GT, 0, pass);
-    t.launch(k_spread_w, k_spread_w_batch, [&](const SysView& v) { return on(v) ? gather_blocks(v) : 0; }, SG_T, 0,
-             pass);
-    t.launch(k_fix2real, k_fix2real_batch,
-             [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]) : 0; }, GT, 0);
+    t.launch(k_bin_sites, k_bin_sites_batch,
+             [&](const SysView& v) { return on(v) ? gblocks(v, 3ull * v.nw_cap + v.na) : 0; }, GT, 0, pass);
+    t.launch(k_spread_brick, k_spread_brick_batch,
+             [&](const SysView& v) { return on(v) ? (int)std::min(v.n_bricks, v.max_blocks) : 0; }, SB_T, 0, pass);
 }
 
 void launch_pme_transform(const Target& t, int pass) {
@@ -697,10 +782,12 @@ void launch_pme_transform(const Target& t, int pass) {
 
 void launch_pme_gather(const Target& t, int pass) {
     auto on = [pass](const SysView& v) { return pass == 0 || v.alch_on != 0u; };
-    t.launch(k_gather, k_gather_batch, [&](const SysView& v) { return on(v) && v.na ? gblocks(v, v.na) : 0; }, GT, 0,
-             pass);
-    t.launch(k_gather_w, k_gather_w_batch, [&](const SysView& v) { return on(v) ? (int)v.nb[REG_CORR] : 0; }, SG_T,
-             0, pass);
+    t.launch(k_gather_brick, k_gather_brick_batch,
+             [&](const SysView& v) { return on(v) ? (int)std::min(v.n_bricks + OVF_BLOCKS, v.max_blocks) : 0; },
+             GB_T, 0, pass);
+    // the molecule's own pass (2) holds no water
+    t.launch(k_gather_wfin, k_gather_wfin_batch,
+             [&](const SysView& v) { return on(v) && pass != 2 ? (int)v.nb[REG_CORR] : 0; }, GT, 0, pass);
     t.launch(k_recip_pass, k_recip_pass_batch, [&](const SysView& v) { return on(v) ? 1 : 0; }, 256, 0, pass);
 }
 

@@ -107,6 +107,9 @@ class MdConfig:
     # inner buffer of the pruned water-water lists (A); 0 = automatic
     # (tuning knob only, results do not depend on it)
     prune_buffer: float = 0.0
+    # charged sites per SPME grid brick before the overflow path; 0 =
+    # automatic (results do not depend on it)
+    spme_brick_cap: int = 0
     lincs_order: int = 4            # HydrogenConstraint::Linear { order, iter } (src/prep.rs:77)
     lincs_iter: int = 1
     # constraint position corrections also correct the velocities (RATTLE);
@@ -196,6 +199,7 @@ def _config_struct(system, cfg):
     c.seed = int(cfg.seed) & 0xFFFFFFFFFFFFFFFF
     c.ww_union_chunk = int(cfg.ww_union_chunk)
     c.prune_buffer = float(cfg.prune_buffer)
+    c.spme_brick_cap = int(cfg.spme_brick_cap)
     c.lincs_order = int(cfg.lincs_order)
     c.lincs_iter = int(cfg.lincs_iter)
     return c

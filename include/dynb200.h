@@ -313,7 +313,10 @@ typedef struct {
     uint32_t alch_begin;
     uint32_t alch_end;
     float alch_lambda;      /* 0 = fully coupled, 1 = decoupled             */
-    uint32_t reserved1;
+    uint32_t spme_brick_cap; /* charged sites per 8^3 SPME grid brick before
+                             * the overflow path (global atomics, per-site
+                             * gather) takes them; 0 = about twice the mean.
+                             * Results do not depend on it.                 */
 } dyn_config_t;
 
 typedef struct {
