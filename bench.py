@@ -200,6 +200,28 @@ def measure_batch(name, args, stream, dev, dist=None, rank=0, world=1):
                 + 2 * min(max(0, prunes - rebuilds), steps))
     value = aggregate_ns_per_day(steps, n_sys, world, ms)
     plain_value = DT * 1e-3 * n_sys / (plain_ms * 1e-3) * 86400.0
+    # ---- the same members with the autotuner's choices (--tune) ----
+    tuned = None
+    if getattr(args, "tune", False):
+        from dynamics_b200 import tune as _tune
+        t0 = time.perf_counter()
+        tb = md.MdBatch(systems, cfgs, stream=stream.cuda_stream, tune=True)
+        tune_s = time.perf_counter() - t0
+        tb.step(DT, args.warmup)
+        torch.cuda.synchronize(dev)
+        for k in range(steps):
+            flush.zero_()
+            ev0[k].record(stream)
+            tb.step(DT, 1)
+            ev1[k].record(stream)
+        torch.cuda.synchronize(dev)
+        tb.sync()
+        tms = max_over_ranks(float(np.sum([ev0[k].elapsed_time(ev1[k]) for k in range(steps)])), dist, dev)
+        keys = sorted({_tune.size_class(sd, c) for sd, c in zip(systems, cfgs)})
+        tuned = {"value": round(aggregate_ns_per_day(steps, n_sys, world, tms), 2),
+                 "ms_per_step": round(tms / steps, 5), "over_untuned": round(ms / tms, 3),
+                 "tune_s": round(tune_s, 1), "classes": {k: _tune.lookup(k) for k in keys}}
+        tb.close()
     # ---- end to end: every member's positions/velocities in and out per step,
     # one copy each way for the whole batch through its page-locked area ----
     host = batch.host_buffer()
@@ -221,6 +243,7 @@ def measure_batch(name, args, stream, dev, dist=None, rank=0, world=1):
         "plain_one_by_one": {"value": round(plain_value, 2), "unit": "ns/day (aggregate)",
                              "ms_per_round": round(plain_ms, 4), "steps_each": k_plain},
         "batch_over_plain": round(value / world / plain_value, 3),
+        "tuned": tuned,
         "e2e": {"value": round(e2e_value, 2), "unit": "ns/day (aggregate)",
                 "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes,
                 "of_device": round(e2e_value / value, 3), "path": "dyn_batch_step_host"},
@@ -321,7 +344,7 @@ def run_batch(args):
            "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": res["data"],
            "config": {**res["config"], "members": res["members"], "parallelism": f"replicas x{world}"},
-           **{k: res[k] for k in ("plain_one_by_one", "batch_over_plain", "e2e", "gpu_launches",
+           **{k: res[k] for k in ("plain_one_by_one", "batch_over_plain", "tuned", "e2e", "gpu_launches",
                                   "launches_per_step", "clocks", "n_water_total", "n_atoms_total")},
            "cpu_baseline": None}
     print(json.dumps(out))
@@ -777,6 +800,8 @@ def main():
     ap.add_argument("--equil", type=int, default=1000)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tune", action="store_true",
+                    help="batched workloads: also time the members with the autotuner's choices")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain line only (no batched / served sub-objects)")
     args = ap.parse_args()

@@ -21,7 +21,7 @@ DYN_ERR_TIMEOUT = -6
 DYN_ERR_UNSUPPORTED = -7
 
 DYN_NB_STATIC_MAX_SITES = 131072
-DYN_STAGES = 14
+DYN_STAGES = 13
 DYN_OVR_COULOMB_DISABLED = 1
 DYN_OVR_LJ_DISABLED = 2
 DYN_PAIR_SCALE14 = 1
@@ -66,7 +66,7 @@ class Config(C.Structure):
         ("ww_union_chunk", C.c_uint32), ("lincs_order", C.c_uint32), ("lincs_iter", C.c_uint32),
         ("prune_buffer", C.c_float),
         ("alch_begin", C.c_uint32), ("alch_end", C.c_uint32), ("alch_lambda", C.c_float),
-        ("spme_brick_cap", C.c_uint32),
+        ("spme_brick_cap", C.c_uint32), ("pair_item_entries", C.c_uint32),
     ]
 
 

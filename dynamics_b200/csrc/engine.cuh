@@ -30,9 +30,6 @@
 #define UMAX 5            // atoms per constraint unit (a heavy atom and up to 4 H)
 #define LPW 8             // lanes per i-water in the water-water kernel
 #define ACL 8             // atoms per cluster
-#ifndef CH_MIX
-#define CH_MIX 8          // list entries per work item of the atom pair kernels (at most 32)
-#endif
 #define INVALID_ID 0xFFFFFFFFu
 #define PME_BRICK 8       // edge of the SPME grid bricks (grid points)
 #define DYN_SITE_WATER 0x80000000u  // site code flag: a water site (3 * id + site) rather than an atom
@@ -150,8 +147,8 @@ struct SysView {
     float4* wbb_c; float4* wbb_h; float4* abb_c; float4* abb_h;
     // cluster lists (fixed capacity per i cluster): water cluster -> atom
     // clusters, atom cluster -> atom clusters (cj >= ci) with masks; work
-    // items {i cluster, first entry} of CH_MIX list entries, in i order
-    uint32_t cap_ws, cap_ss;
+    // items {i cluster, first entry} of ch_mix (1..32) list entries, in i order
+    uint32_t cap_ws, cap_ss, ch_mix;
     uint32_t* ws_n; uint32_t* ws_j;
     uint32_t* ss_n; uint32_t* ss_j; unsigned long long* ss_mask;
     uint2* ws_item; uint2* ss_item;
@@ -177,14 +174,8 @@ struct SysView {
     // The molecule lists are half lists (each water pair once, listed by
     // the lower slot).  The j-side forces a group's CTA computes are summed
     // in shared memory as int32 fixed point (2^-16 kcal/mol/A) per union
-    // water and written to jbuf entry g * cap_union + u; every water then
-    // gathers its entries through the reverse index rev (rev_n per slot,
-    // entries are jbuf entry numbers).  j-contributions too large for the
-    // int32 sums go to wjbig (int64, 2^-32) by atomics.
-    int* jbuf;                               // [ngrp_cap * cap_union * 12]
-    uint32_t* rev_n; uint32_t* rev;          // [nw_cap], [nw_cap * rev_cap]
-    uint32_t rev_cap;
-    long long* wjbig;                        // [nw_cap * 12]
+    // water and added to wforce with int64 atomics; contributions too large
+    // for the int32 sums go to wforce directly.
     // 1-4 pairs, exclusions (pairs), bonded terms, constraints
     uint32_t n14; uint2* p14; float4* p14_par;     // sigma, eps, qq, unused
     uint32_t nexcl; uint2* excl; float* excl_qq;
@@ -417,13 +408,11 @@ void launch_pairs_atoms(const Target& t, bool energy);
 // the parts of launch_pairs_water, in order: water-water, its j-side
 // gather, water-atom
 void launch_pairs_ww(const Target& t, bool energy);
-void launch_ww_gather(const Target& t);
 void launch_pairs_ws(const Target& t, bool energy);
 void launch_pair14(const Target& t, bool energy);
 int pair_ww_setup(const SysView& v);
 int ww_tile_blocks(const SysView& v);
 size_t ww_tile_smem(const SysView& v);
-int ww_gather_blocks(const SysView& v);
 int pair_blocks_ss(const SysView& v);
 int pair_blocks_ws(const SysView& v);
 int pair14_blocks(const SysView& v);

@@ -117,7 +117,6 @@ DYN_KERNEL(, k_col_clear, (, bool force), (, force)) {
         if (c < v.ncol) { v.col_count[c] = 0; v.col_fill[c] = 0; }
         if (c < v.ancol) { v.acol_count[c] = 0; v.acol_fill[c] = 0; }
     }
-    for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.nw_cap; s += bk.cnt * blockDim.x) v.rev_n[s] = 0;
 }
 
 DYN_KERNEL(, k_col_assign, (, bool force), (, force)) {
@@ -392,7 +391,7 @@ DYN_KERNEL_T((int MODE), (MODE), , k_list, (, bool force), (, force)) {
 }
 
 // Work items of the atom pair kernels: for every i-cluster (in order) one
-// item per CH_MIX entries of its list, {cluster, first entry}.  One block;
+// item per ch_mix entries of its list, {cluster, first entry}.  One block;
 // an exclusive scan of the per-cluster item counts, tile by tile.
 constexpr int IT_T = 1024;
 DYN_KERNEL_T((int MODE), (MODE), __launch_bounds__(IT_T), k_items, (, bool force), (, force)) {
@@ -406,7 +405,7 @@ DYN_KERNEL_T((int MODE), (MODE), __launch_bounds__(IT_T), k_items, (, bool force
     uint32_t base = 0;
     for (uint32_t c0 = 0; c0 < ni; c0 += IT_T) {
         const uint32_t c = c0 + threadIdx.x;
-        const uint32_t k = c < ni ? (cnt[c] + CH_MIX - 1) / CH_MIX : 0u;
+        const uint32_t k = c < ni ? (cnt[c] + v.ch_mix - 1) / v.ch_mix : 0u;
         uint32_t x = k;  // inclusive scan inside the warp
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -427,7 +426,7 @@ DYN_KERNEL_T((int MODE), (MODE), __launch_bounds__(IT_T), k_items, (, bool force
         __syncthreads();
         const uint32_t off = base + (w ? wsum[w - 1] : 0u) + x - k;
         for (uint32_t t = 0; t < k; ++t)
-            if (off + t < icap) items[off + t] = make_uint2(c, t * CH_MIX);
+            if (off + t < icap) items[off + t] = make_uint2(c, t * v.ch_mix);
         base += wsum[IT_T / 32 - 1];
         __syncthreads();
     }
@@ -567,11 +566,6 @@ DYN_KERNEL(__launch_bounds__(UT), k_group_union, (, bool force), (, force)) {
             if (k < ncand) cl[k] = need && loc < v.cap_union ? (uint16_t)loc : (uint16_t)0xFFFFu;
             if (need && loc < v.cap_union) {
                 v.grp_uslot[(size_t)g * v.cap_union + loc] = slot;
-                // reverse index: the water gathers this group's j sums
-                // (jbuf entry g * cap_union + loc)
-                const uint32_t r = atomicAdd(&v.rev_n[slot], 1u);
-                if (r < v.rev_cap) v.rev[(size_t)slot * v.rev_cap + r] = g * v.cap_union + loc;
-                else atomicMax(&v.sc->overflow, r + 1);
             }
             if (start && rid < v.cap_run) v.grp_run[(size_t)g * v.cap_run + rid] = make_uint2(slot, loc);
             __syncthreads();
@@ -699,16 +693,19 @@ DYN_KERNEL(, k_rebuild_done, (, bool force), (, force)) {
     v.sc->rebuilds += 1ull;
 }
 
-// Copies positions into cluster order and zeroes the atoms' short-range
-// force accumulators (every pair kernel adds to them).
+// Copies positions into cluster order and zeroes the atoms' and the
+// waters' short-range force accumulators (every pair kernel adds to them).
 DYN_KERNEL(, k_gather_atoms, (), ()) {
-    for (uint32_t s = bk.idx * blockDim.x + threadIdx.x; s < v.na_cap; s += bk.cnt * blockDim.x) {
+    const uint32_t t0 = bk.idx * blockDim.x + threadIdx.x, stride = bk.cnt * blockDim.x;
+    for (uint32_t s = t0; s < v.na_cap; s += stride) {
         const uint32_t a = v.sidx[s];
         if (a != INVALID_ID) {
             v.spos[s] = v.apos[a];
             v.aforce[3 * (size_t)a + 0] = 0; v.aforce[3 * (size_t)a + 1] = 0; v.aforce[3 * (size_t)a + 2] = 0;
         }
     }
+    int4* wf = reinterpret_cast<int4*>(v.wforce);  // 12 int64 = 6 int4 per slot
+    for (uint32_t t = t0; t < 6 * v.nw_cap; t += stride) wf[t] = make_int4(0, 0, 0, 0);
 }
 
 inline int nblocks(uint64_t n, int threads, int cap = 148 * 8) {
@@ -769,7 +766,7 @@ void launch_prune(const Target& t, bool force) {
 
 void launch_gather_atoms(const Target& t) {
     t.launch(k_gather_atoms, k_gather_atoms_batch,
-             [](const SysView& v) { return v.na ? nblocks(v.na_cap, 256) : 0; }, 256, 0);
+             [](const SysView& v) { return nblocks(std::max<uint64_t>(v.na_cap, 6ull * v.nw_cap), 256); }, 256, 0);
 }
 
 }  // namespace dyn

@@ -11,7 +11,7 @@
 // 32-water i-group, j sites staged in shared memory, LPW lanes per i-water
 // over its compact molecule list (k_pair_ww_tile).  Atom-water and atom-atom
 // (half lists: every pair once): one warp per work item (an 8-body
-// i-cluster and up to CH_MIX entries of its list); lane = (ii, jq) with
+// i-cluster and up to ch_mix entries of its list); lane = (ii, jq) with
 // ii = lane & 7 and jq = lane >> 3 evaluates i-body ii against j-atoms jq and
 // jq + 4 of every j-cluster in the item.  Water pairs are
 // handled as molecule pairs: one min-image shift from the O-O vector serves
@@ -138,9 +138,6 @@ __device__ __forceinline__ float red4(float x) {
     return x;
 }
 
-__device__ __forceinline__ void store_fix3(long long* p, float3 f) {
-    p[0] = fix_from_float(f.x); p[1] = fix_from_float(f.y); p[2] = fix_from_float(f.z);
-}
 __device__ __forceinline__ void add_fix3(long long* p, float3 f) {
     fix_atomic_add(p + 0, fix_from_float(f.x));
     fix_atomic_add(p + 1, fix_from_float(f.y));
@@ -259,27 +256,20 @@ constexpr float JFIX_SCALE = (float)(1 << WW_JFIX_SHIFT);
 constexpr float JFIX_MAX = 1000.0f;
 
 __device__ __noinline__ void jforce_big(const SysView& v, uint32_t g, uint32_t u, int c, float f) {
-    // the slot of union entry u from the group's runs (ascending offsets)
-    const uint2* runs = v.grp_run + (size_t)g * v.cap_run;
-    uint32_t lo = 0, hi = v.grp_nrun[g];
-    while (hi - lo > 1) {
-        const uint32_t m = (lo + hi) >> 1;
-        if (runs[m].y <= u) lo = m; else hi = m;
-    }
-    const uint32_t slot = runs[lo].x + (u - runs[lo].y);
-    fix_atomic_add(v.wjbig + (size_t)slot * 12 + c, fix_from_float(f));
+    const uint32_t slot = v.grp_uslot[(size_t)g * v.cap_union + u];
+    fix_atomic_add(v.wforce + (size_t)slot * 12 + c, fix_from_float(f));
 }
 
 // The 12 j-side components of one molecule pair (the forces on the j
 // water's O, H0, H1, M); one range check for all of them.
-__device__ __forceinline__ void jforce_add12(const SysView& v, int* jacc, uint32_t chunk, uint32_t g, uint32_t u,
+__device__ __forceinline__ void jforce_add12(const SysView& v, int* jacc, uint32_t cs, uint32_t g, uint32_t u,
                                              uint32_t ul, const float (&f)[12]) {
     float m = 0.f;
 #pragma unroll
     for (int c = 0; c < 12; ++c) m = fmaxf(m, fabsf(f[c]));
     if (m < JFIX_MAX) {
 #pragma unroll
-        for (int c = 0; c < 12; ++c) atomicAdd(jacc + (size_t)c * chunk + ul, __float2int_rn(f[c] * JFIX_SCALE));
+        for (int c = 0; c < 12; ++c) atomicAdd(jacc + (size_t)c * cs + ul, __float2int_rn(f[c] * JFIX_SCALE));
     } else {
         for (int c = 0; c < 12; ++c) jforce_big(v, g, u, c, f[c]);
     }
@@ -290,26 +280,36 @@ __device__ __forceinline__ void jforce_add12(const SysView& v, int* jacc, uint32
 // i-group.  The waters the group's lists reach (its union, stored as runs
 // of consecutive slots) are copied global -> shared with one cp.async.bulk
 // per run, completing on an mbarrier, union_chunk waters at a time (one
-// chunk for almost every group; sized so that two CTAs fit on an SM).  Each
-// i-water is handled by LPW lanes walking its list of union indices: every
-// water pair once (the list of the lower slot), all 10 site pairs with one
-// min-image shift.  The i-side forces stay in registers and are stored
-// (first writer) after the group; the j-side forces are summed per union
-// water in shared memory (int32 fixed point, 12 components, component-major
-// so that the lanes' adds spread over the banks), then written to the
-// group's entries of jbuf (g * cap_union + union index), which k_ww_gather
-// adds to each water.
+// chunk for almost every group; sized so that two CTAs fit on an SM).  The
+// lists hold every water pair once (in the list of the lower slot), so
+// their lengths vary several-fold across a group; the chunk's entries of
+// all 32 lists are therefore dealt out as one sequence, an equal
+// contiguous share per thread, whatever list they come from.  A thread
+// keeps the i-water's forces in registers while its share stays in one
+// list and adds them to the water forces (int64 reductions) when it moves
+// to the next list.  All 10 site pairs of a molecule pair use one
+// min-image shift.  The j-side forces are summed per union water in shared
+// memory (int32 fixed point, 12 components, component-major with a stride
+// of chunk + 1 words, so that both the threads' adds and the flush's reads
+// spread over the banks), then added to the union waters' forces with one
+// coalesced run of int64 reductions per chunk.  The shares depend only on
+// the lists, and every sum across threads is an integer sum: the forces are
+// the same bits run to run.
 // ---------------------------------------------------------------------------
 DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, (), ()) {
     extern __shared__ __align__(128) float4 tile[];  // union_chunk waters x 4 float4, then the j sums
     __shared__ __align__(8) uint64_t bar;
+    __shared__ float4 ipos[GRPW * 4];   // the group's i-water sites
+    __shared__ uint32_t woff[GRPW + 1]; // first share position of each list's chunk entries
+    __shared__ uint32_t wbeg[GRPW];     // each list's first entry in the chunk
+    __shared__ uint32_t wend[GRPW];     // ... and one past its last
     const int tid = threadIdx.x;
-    const int il = tid / LPW, l = tid % LPW;
     const uint32_t nwc = v.sc->n_wclus;
     const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
     const uint32_t nslots = nwc * WCL;
     const uint32_t chunk = v.union_chunk;
-    int* jacc = reinterpret_cast<int*>(tile + 4 * (size_t)chunk);  // [12][chunk]
+    const uint32_t cs = chunk + 1;  // component stride of the j sums
+    int* jacc = reinterpret_cast<int*>(tile + 4 * (size_t)chunk);  // [12][chunk + 1]
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     const float sig2 = OPC_O_SIGMA * OPC_O_SIGMA;
@@ -319,33 +319,45 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
     if (tid == 0) mbar_init(&bar, 1);
     __syncthreads();
     uint32_t parity = 0;
-    double el = 0.0, ec = 0.0, ew = 0.0;
+    Acc3 a{0.0, 0.0, 0.f, 0.0};
     bool alive = true;
     for (uint32_t g = bk.idx; g < ng && alive; g += bk.cnt) {
         const uint32_t nloc = v.grp_nloc[g];
-        const uint32_t uoff = g * v.cap_union;  // the group's jbuf entries
-        const uint32_t s = g * GRPW + il;
-        const bool have = s < nslots;
-        const uint32_t n = have ? v.winb_n[s] : 0u;
-        float3 iO = f3(0, 0, 0), iH0 = iO, iH1 = iO, iM = iO;
-        if (have) {
-            iO = xyz(v.wpos[4 * s + 0]); iH0 = xyz(v.wpos[4 * s + 1]);
-            iH1 = xyz(v.wpos[4 * s + 2]); iM = xyz(v.wpos[4 * s + 3]);
+        const uint32_t uoff = g * v.cap_union;  // the group's union entries
+        if (tid < GRPW * 4) {
+            const uint32_t s = g * GRPW + tid / 4;
+            ipos[tid] = s < nslots ? v.wpos[(size_t)4 * g * GRPW + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        float3 fO = f3(0, 0, 0), fH0 = fO, fH1 = fO, fM = fO;
-        Acc3 a{0.0, 0.0, 0.f, 0.0};
-        const uint16_t* lst = v.winb + (size_t)s * v.cap_nb;  // the pruned list
-        uint32_t k = l;  // this lane's next list entry (entries l, l + LPW, ...)
-        // the next entry's index is loaded one iteration ahead, so the
-        // global-memory latency of the list overlaps the arithmetic
-        uint32_t idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
-        // a union larger than the shared buffer is processed in chunks; the
-        // lists hold ascending union indices, so each lane resumes where it
-        // stopped
+        if (tid < GRPW) wend[tid] = 0u;
         for (uint32_t lo = 0; lo < nloc; lo += chunk) {
             const uint32_t hi = min(nloc, lo + chunk);
             if (tid < 32) stage_chunk(v, g, lo, hi, tile, &bar, tid);
-            for (uint32_t t = tid; t < 12 * chunk; t += WT) jacc[t] = 0;
+            for (uint32_t t = tid; t < 12 * cs; t += WT) jacc[t] = 0;
+            __syncthreads();  // wend of the previous chunk (or group start) is visible
+            if (tid >= 32 && tid < 32 + GRPW) {
+                // the list entries of this chunk: from where the previous
+                // chunk stopped to the first union index >= hi (lists ascend)
+                const int w = tid - 32;
+                const uint32_t s = g * GRPW + w;
+                const uint32_t n = s < nslots ? v.winb_n[s] : 0u;
+                const uint16_t* lst = v.winb + (size_t)s * v.cap_nb;
+                const uint32_t b0 = wend[w];
+                uint32_t l0 = b0, l1 = n;
+                while (l0 < l1) {
+                    const uint32_t m = (l0 + l1) >> 1;
+                    if ((uint32_t)lst[m] < hi) l0 = m + 1; else l1 = m;
+                }
+                uint32_t x = l0 - b0;  // inclusive scan of the counts over the 32 lists
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (w >= o) x += y;
+                }
+                wbeg[w] = b0;
+                woff[w + 1] = x;
+                if (w == 0) woff[0] = 0u;
+                wend[w] = l0;
+            }
             const bool ok = mbar_wait(&bar, parity, &v.sc->timeout);
             if (!__syncthreads_and(ok)) {
                 // give the copies in flight one more bounded chance, then stop
@@ -354,10 +366,43 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
                 break;
             }
             parity ^= 1u;
-            while (idx_next < hi) {
+            // this thread's share [e0, e1) of the chunk's entries
+            const uint32_t total = woff[GRPW];
+            const uint32_t e0 = (uint32_t)(((uint64_t)tid * total) / WT);
+            const uint32_t e1 = (uint32_t)(((uint64_t)(tid + 1) * total) / WT);
+            int w = 0;
+            while (w < GRPW - 1 && woff[w + 1] <= e0) ++w;
+            float3 iO = f3(0, 0, 0), iH0 = iO, iH1 = iO, iM = iO;
+            float3 fO = iO, fH0 = iO, fH1 = iO, fM = iO;
+            const uint16_t* lst = v.winb;
+            uint32_t wstop = 0;  // share position where list w ends
+            auto enter = [&](int wn) {
+                w = wn;
+                iO = xyz(ipos[4 * w + 0]); iH0 = xyz(ipos[4 * w + 1]);
+                iH1 = xyz(ipos[4 * w + 2]); iM = xyz(ipos[4 * w + 3]);
+                // lst[e] is the entry at list position wbeg[w] + (e - woff[w])
+                lst = v.winb + ((size_t)(g * GRPW + w) * v.cap_nb + wbeg[w]) - woff[w];
+                wstop = woff[w + 1];
+            };
+            auto leave = [&]() {
+                long long* p = v.wforce + (size_t)(g * GRPW + w) * 12;
+                add_fix3(p + 0, fO); add_fix3(p + 3, fH0); add_fix3(p + 6, fH1); add_fix3(p + 9, fM);
+                fO = f3(0, 0, 0); fH0 = fO; fH1 = fO; fM = fO;
+            };
+            if (e0 < e1) enter(w);
+            // the next entry's index is loaded one iteration ahead, so the
+            // global-memory latency of the list overlaps the arithmetic
+            uint32_t idx_next = e0 < e1 ? (uint32_t)lst[e0] : 0u;
+            for (uint32_t e = e0; e < e1; ++e) {
+                if (e >= wstop) {
+                    leave();
+                    int wn = w + 1;
+                    while (woff[wn + 1] <= e) ++wn;
+                    enter(wn);
+                    idx_next = (uint32_t)lst[e];
+                }
                 const uint32_t idx = idx_next;
-                k += LPW;
-                idx_next = k < n ? (uint32_t)lst[k] : 0xFFFFFFFFu;
+                if (e + 1 < e1 && e + 1 < wstop) idx_next = (uint32_t)lst[e + 1];
                 const float4* jw = tile + 4 * (idx - lo);
                 const float3 jO = xyz(jw[0]);
                 const float3 sh = shift_of(iO - jO, b);
@@ -384,75 +429,26 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
                 // the j waters receive the opposite forces (sites O, H0, H1, M)
                 const float jf[12] = {-gO.x, -gO.y, -gO.z, -gH0.x, -gH0.y, -gH0.z,
                                       -gH1.x, -gH1.y, -gH1.z, -gM.x, -gM.y, -gM.z};
-                jforce_add12(v, jacc, chunk, g, idx, idx - lo, jf);
+                jforce_add12(v, jacc, cs, g, idx, idx - lo, jf);
             }
+            if (e0 < e1) leave();
             __syncthreads();  // every j sum of the chunk is in
-            // the chunk's sums -> the group's jbuf entries (48 B per water)
-            for (uint32_t u = tid; u < hi - lo; u += WT) {
-                int4* dst = reinterpret_cast<int4*>(v.jbuf + 12 * ((size_t)uoff + lo + u));
-                dst[0] = make_int4(jacc[0 * chunk + u], jacc[1 * chunk + u], jacc[2 * chunk + u], jacc[3 * chunk + u]);
-                dst[1] = make_int4(jacc[4 * chunk + u], jacc[5 * chunk + u], jacc[6 * chunk + u], jacc[7 * chunk + u]);
-                dst[2] = make_int4(jacc[8 * chunk + u], jacc[9 * chunk + u], jacc[10 * chunk + u],
-                                   jacc[11 * chunk + u]);
+            // the chunk's sums -> the union waters' forces (2^-16 -> 2^-32
+            // fixed point); consecutive union entries of a run are
+            // consecutive slots, so the reductions are coalesced
+            for (uint32_t t = tid; t < 12 * (hi - lo); t += WT) {
+                const uint32_t u = t / 12, c = t - 12 * u;
+                const int val = jacc[c * cs + u];
+                if (val != 0)
+                    fix_atomic_add(v.wforce + 12 * (size_t)v.grp_uslot[(size_t)uoff + lo + u] + c,
+                                   (long long)val * (1ll << (32 - WW_JFIX_SHIFT)));
             }
             __syncthreads();  // the tile and the sums are refilled by the next chunk or group
         }
-        if (!alive) break;
-#pragma unroll
-        for (int o = 1; o < LPW; o <<= 1) {
-            fO.x += __shfl_xor_sync(0xffffffffu, fO.x, o); fO.y += __shfl_xor_sync(0xffffffffu, fO.y, o);
-            fO.z += __shfl_xor_sync(0xffffffffu, fO.z, o);
-            fH0.x += __shfl_xor_sync(0xffffffffu, fH0.x, o); fH0.y += __shfl_xor_sync(0xffffffffu, fH0.y, o);
-            fH0.z += __shfl_xor_sync(0xffffffffu, fH0.z, o);
-            fH1.x += __shfl_xor_sync(0xffffffffu, fH1.x, o); fH1.y += __shfl_xor_sync(0xffffffffu, fH1.y, o);
-            fH1.z += __shfl_xor_sync(0xffffffffu, fH1.z, o);
-            fM.x += __shfl_xor_sync(0xffffffffu, fM.x, o); fM.y += __shfl_xor_sync(0xffffffffu, fM.y, o);
-            fM.z += __shfl_xor_sync(0xffffffffu, fM.z, o);
-        }
-        if (l == 0 && have) {
-            long long* p = v.wforce + (size_t)s * 12;
-            store_fix3(p + 0, fO); store_fix3(p + 3, fH0); store_fix3(p + 6, fH1); store_fix3(p + 9, fM);
-        }
-        if (ENERGY) { el += a.e_lj; ec += a.e_c; }
-        ew += a.wd;
     }
-    write_partials<ENERGY>(v, bk, REG_WW, el, ec, ew);
+    write_partials<ENERGY>(v, bk, REG_WW, ENERGY ? a.e_lj : 0.0, ENERGY ? a.e_c : 0.0, a.wd);
 }
 
-// ---------------------------------------------------------------------------
-// The j-side water-water forces: every water adds the sums the group CTAs
-// wrote for it (its reverse-index entries) and its int64 overflow sums,
-// which are cleared for the next step.  12 threads per water, one force
-// component each, so the 48-byte entries are read whole.  Integer sums in
-// any order: deterministic.
-// ---------------------------------------------------------------------------
-constexpr int GT = 384;  // 32 waters x 12 components per block
-
-DYN_KERNEL(__launch_bounds__(GT), k_ww_gather, (), ()) {
-    const uint32_t total = v.sc->n_wclus * WCL * 12;
-    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
-        const uint32_t s = t / 12, c = t - 12 * s;
-        if (v.wid[s] == INVALID_ID) continue;
-        const uint32_t n = min(v.rev_n[s], v.rev_cap);
-        const uint32_t* e = v.rev + (size_t)s * v.rev_cap;
-        // entries are jbuf entry numbers g * cap_union + u; four loads in
-        // flight per thread
-        long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-        uint32_t k = 0;
-        for (; k + 4 <= n; k += 4) {
-            const uint32_t x0 = e[k], x1 = e[k + 1], x2 = e[k + 2], x3 = e[k + 3];
-            a0 += (long long)v.jbuf[12 * (size_t)x0 + c];
-            a1 += (long long)v.jbuf[12 * (size_t)x1 + c];
-            a2 += (long long)v.jbuf[12 * (size_t)x2 + c];
-            a3 += (long long)v.jbuf[12 * (size_t)x3 + c];
-        }
-        for (; k < n; ++k) a0 += (long long)v.jbuf[12 * (size_t)e[k] + c];
-        const long long acc = (a0 + a1) + (a2 + a3);
-        long long big = v.wjbig[t];
-        if (big != 0) v.wjbig[t] = 0;
-        v.wforce[t] += acc * (1ll << (32 - WW_JFIX_SHIFT)) + big;
-    }
-}
 
 // Reduce-scatter over the 8 lanes that share jq (lane bits 0-2): N values
 // per lane in, N/8 out; lane ii ends with the sums of values
@@ -486,7 +482,7 @@ __device__ __forceinline__ JAtoms load_jatoms(const SysView& v, uint32_t cj, int
 
 // ---------------------------------------------------------------------------
 // water(i) - atom(j), each pair once.  One warp per work item (a water
-// i-cluster and CH_MIX entries of its atom-cluster list); the list entries
+// i-cluster and ch_mix entries of its atom-cluster list); the list entries
 // are read once per item (one per lane) and the next entry's j-atoms are
 // loaded while the current one is evaluated.  The water forces stay in
 // registers over the item; the j-atom forces (the opposite of the pair
@@ -505,7 +501,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT, 4),
     for (uint32_t it = ((bk.idx * blockDim.x + threadIdx.x) >> 5); it < nit; it += nwarps) {
         const uint2 item = v.ws_item[it];
         const uint32_t ci = item.x, k0 = item.y;
-        const uint32_t n = min(v.ws_n[ci], k0 + CH_MIX) - k0;
+        const uint32_t n = min(v.ws_n[ci], k0 + v.ch_mix) - k0;
         const uint32_t si = ci * WCL + ii;
         const bool vi = v.wid[si] != INVALID_ID;
         const float3 iO = xyz(v.wpos[4 * si + 0]), iH0 = xyz(v.wpos[4 * si + 1]);
@@ -624,7 +620,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT), k_
     for (uint32_t it = ((bk.idx * blockDim.x + threadIdx.x) >> 5); it < nit; it += nwarps) {
         const uint2 item = v.ss_item[it];
         const uint32_t ci = item.x, k0 = item.y;
-        const uint32_t n = min(v.ss_n[ci], k0 + CH_MIX) - k0;
+        const uint32_t n = min(v.ss_n[ci], k0 + v.ch_mix) - k0;
         const uint32_t si = ci * ACL + ii;
         const uint32_t ai = v.sidx[si];
         const float4 pi = v.spos[si];
@@ -734,12 +730,9 @@ int ww_tile_blocks(const SysView& v) {
     return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
 }
 
-// per union water: 4 float4 positions and 12 int32 j sums
-size_t ww_tile_smem(const SysView& v) { return (size_t)v.union_chunk * (4 * sizeof(float4) + 12 * sizeof(int)); }
-
-int ww_gather_blocks(const SysView& v) {
-    const uint64_t b = ((uint64_t)v.nw_cap * 12 + GT - 1) / GT;
-    return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, 148u * 8u));
+// per union water: 4 float4 positions and 12 int32 j sums (+ the stride pad)
+size_t ww_tile_smem(const SysView& v) {
+    return (size_t)v.union_chunk * (4 * sizeof(float4) + 12 * sizeof(int)) + 12 * sizeof(int);
 }
 
 // The limit is a property of the kernel, shared by every system in the
@@ -798,15 +791,8 @@ void launch_pairs_ww(const Target& t, bool energy) {
              [&](const SysView& v) { return v.nw && !eww(v) ? ww_tile_blocks(v) : 0; }, WT, sm);
 }
 
-void launch_ww_gather(const Target& t) {
-    t.launch(k_ww_gather, k_ww_gather_batch, [](const SysView& v) { return v.nw ? ww_gather_blocks(v) : 0; }, GT, 0);
-}
-
 void launch_pairs_water(const Target& t, bool energy) {
     launch_pairs_ww(t, energy);
-    // the j-side sums and the water-atom forces are added to the water
-    // forces the water-water kernel stores
-    launch_ww_gather(t);
     launch_pairs_ws(t, energy);
 }
 

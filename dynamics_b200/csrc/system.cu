@@ -564,9 +564,6 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         // but the first waters of the slot order keep nearly all of theirs
         // (their periodic neighbours sit at the end of the order)
         v.cap_nb = std::min<uint32_t>((uint32_t)(1.5 * nb) + 32, 65535u);
-        // per water, the unions that hold it (union entries per water, at the
-        // densest and most spread-out groups, with margin)
-        v.rev_cap = (uint32_t)(2.0 * mink(ag) * dl / GRPW) + 32;
     }
     DYN_CHECK((uint64_t)v.ngrp_cap * v.cap_union < (1ull << 32), DYN_ERR_UNSUPPORTED,
               "dyn_sys_create: too many waters in one system");
@@ -603,8 +600,9 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     };
     v.cap_ws = (v.nw && v.na) ? cap_mixed(v.r_ws, acl_vol, v.nwclus_cap, v.naclus_cap) : 1;
     v.cap_ss = v.na ? cap_mixed(v.r_ss, acl_vol, v.naclus_cap, v.naclus_cap) : 1;
-    v.ws_item_cap = v.nwclus_cap * ((v.cap_ws + CH_MIX - 1) / CH_MIX);
-    v.ss_item_cap = v.naclus_cap * ((v.cap_ss + CH_MIX - 1) / CH_MIX);
+    v.ch_mix = cfg->pair_item_entries ? std::min(32u, cfg->pair_item_entries) : 8u;
+    v.ws_item_cap = v.nwclus_cap * ((v.cap_ws + v.ch_mix - 1) / v.ch_mix);
+    v.ss_item_cap = v.naclus_cap * ((v.cap_ss + v.ch_mix - 1) / v.ch_mix);
 
     // ---- allocations ----
     TRY(dev_alloc(h, &v.wpos, 4 * (size_t)v.nw_cap));
@@ -665,10 +663,6 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     TRY(dev_alloc(h, &v.winb, (size_t)v.nw_cap * v.cap_nb));
     TRY(dev_alloc(h, &v.wprune, v.nw_cap));
     TRY(dev_alloc(h, &v.grp_uslot, (size_t)v.ngrp_cap * v.cap_union));
-    TRY(dev_alloc(h, &v.jbuf, 12 * (size_t)v.ngrp_cap * v.cap_union));
-    TRY(dev_alloc(h, &v.rev_n, v.nw_cap));
-    TRY(dev_alloc(h, &v.rev, (size_t)v.nw_cap * v.rev_cap));
-    TRY(dev_alloc(h, &v.wjbig, 12 * (size_t)v.nw_cap));
     TRY(dev_alloc(h, &v.ws_n, v.nwclus_cap));
     TRY(dev_alloc(h, &v.ws_j, (size_t)v.nwclus_cap * v.cap_ws));
     TRY(dev_alloc(h, &v.ws_item, std::max(1u, v.ws_item_cap)));
@@ -1179,9 +1173,9 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
     const SysView& v = h->v;
     cudaStream_t st = h->stream;
     const Target T{&v, nullptr, st};
-    // events: 0..6 bound the six stages; 7..10 split the pair stage,
-    // 11..13 the SPME stage
-    constexpr int NE = 14;
+    // events: 0..6 bound the six stages; 7, 8 split the pair stage,
+    // 9..11 the SPME stage
+    constexpr int NE = 12;
     cudaEvent_t ev[NE];
     for (int i = 0; i < NE; ++i) DYN_CUDA(cudaEventCreate(&ev[i]));
     double acc[DYN_STAGES] = {};
@@ -1207,10 +1201,8 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
         dyn::launch_gather_atoms(T);
         dyn::launch_pairs_ww(T, energy);
         cudaEventRecord(ev[7], st);
-        dyn::launch_ww_gather(T);
-        cudaEventRecord(ev[8], st);
         dyn::launch_pairs_ws(T, energy);
-        cudaEventRecord(ev[9], st);
+        cudaEventRecord(ev[8], st);
         dyn::launch_pairs_atoms(T, energy);
         cudaEventRecord(ev[3], st);
         dyn::launch_pair14(T, energy);
@@ -1221,11 +1213,11 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
                 dyn::launch_pme(T);
             } else {
                 dyn::launch_pme_spread(T, 0);
-                cudaEventRecord(ev[10], st);
+                cudaEventRecord(ev[9], st);
                 dyn::launch_pme_transform(T, 0);
-                cudaEventRecord(ev[11], st);
+                cudaEventRecord(ev[10], st);
                 dyn::launch_pme_gather(T, 0);
-                cudaEventRecord(ev[12], st);
+                cudaEventRecord(ev[11], st);
             }
             dyn::launch_corrections(T);
         }
@@ -1237,22 +1229,21 @@ extern "C" int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, doub
         DYN_CUDA(cudaGetLastError());
         DYN_CUDA(cudaEventSynchronize(ev[6]));
         for (int k = 0; k < 6; ++k) acc[k] += el(k, k + 1);
-        acc[6] += el(2, 7);   // includes the atoms' cluster-order copy before it
+        acc[6] += el(2, 7);   // includes the force zeroing and the atoms' cluster-order copy before it
         acc[7] += el(7, 8);
-        acc[8] += el(8, 9);
-        acc[9] += el(9, 3);
+        acc[8] += el(8, 3);
         if (spme && !alch) {
-            acc[10] += el(4, 10);
+            acc[9] += el(4, 9);
+            acc[10] += el(9, 10);
             acc[11] += el(10, 11);
-            acc[12] += el(11, 12);
-            acc[13] += el(12, 5);
+            acc[12] += el(11, 5);
         }
         n_spme += spme ? 1u : 0u;
         h->host_step += 1;
     }
     for (int i = 0; i < NE; ++i) cudaEventDestroy(ev[i]);
     for (int k = 0; k < DYN_STAGES; ++k) ms[k] = n_steps ? acc[k] / n_steps : 0.0;
-    for (int k : {4, 10, 11, 12, 13}) ms[k] = n_spme ? acc[k] / n_spme : 0.0;
+    for (int k : {4, 9, 10, 11, 12}) ms[k] = n_spme ? acc[k] / n_spme : 0.0;
     return read_scalars(h);
 }
 

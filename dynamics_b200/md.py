@@ -110,6 +110,9 @@ class MdConfig:
     # charged sites per SPME grid brick before the overflow path; 0 =
     # automatic (results do not depend on it)
     spme_brick_cap: int = 0
+    # list entries per work item of the water-atom and atom-atom pair
+    # kernels (1..32); 0 = 8 (tuning knob only)
+    pair_item_entries: int = 0
     lincs_order: int = 4            # HydrogenConstraint::Linear { order, iter } (src/prep.rs:77)
     lincs_iter: int = 1
     # constraint position corrections also correct the velocities (RATTLE);
@@ -200,6 +203,7 @@ def _config_struct(system, cfg):
     c.ww_union_chunk = int(cfg.ww_union_chunk)
     c.prune_buffer = float(cfg.prune_buffer)
     c.spme_brick_cap = int(cfg.spme_brick_cap)
+    c.pair_item_entries = int(cfg.pair_item_entries)
     c.lincs_order = int(cfg.lincs_order)
     c.lincs_iter = int(cfg.lincs_iter)
     return c
@@ -352,7 +356,7 @@ class MdState:
         return e.as_dict()
 
     STAGES = ("first_half", "list", "pairs", "bonded", "spme", "kick_finalize",
-              "pairs_water_water", "pairs_ww_gather", "pairs_water_atom", "pairs_atom_atom",
+              "pairs_water_water", "pairs_water_atom", "pairs_atom_atom",
               "spme_spread", "spme_fft_convolve", "spme_gather", "spme_corrections")
 
     def stage_times(self, dt, n_steps):

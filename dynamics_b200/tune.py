@@ -10,6 +10,9 @@ measurement, per size class of system, and cached:
   (shorter lists against more prunes);
 * ``ww_union_chunk``: the water-water kernel's shared-memory chunk (waters
   staged at a time; two CTAs per SM at the largest);
+* ``pair_item_entries``: list entries per work item of the water-atom and
+  atom-atom pair kernels (more items balance better, fewer amortise the
+  per-item loads);
 * ``spme_grid``: the SPME grid among FFT-friendly sizes whose spacing is at
   most the configured grid's (the accuracy rule: a finer grid is never less
   accurate, so every candidate holds the force tolerance), at the
@@ -24,8 +27,11 @@ defaults: one knob at a time, each candidate timed over whole captured steps
 (the step graph as MdState.step runs it), the fastest kept unless the
 incumbent is within ``tie`` of it, so small timing noise does not flip a
 choice.  Results are cached by size class in a JSON file
-(``DYNB200_TUNE_CACHE``, default ~/.cache/dynb200/tune.json); the batched
-form (md.MdBatch(..., tune=True)) applies each member's class's choice.
+(``DYNB200_TUNE_CACHE``, default ~/.cache/dynb200/tune.json); classes
+missing there are looked up in the table measured on B200 that ships with
+the package (``data/tune_b200.json``) before anything is timed.  The
+batched form (md.MdBatch(..., tune=True)) applies each member's class's
+choice.
 
 The reference has no tuner (its parameters are constants, src/config.rs);
 this module is new.
@@ -40,11 +46,15 @@ import numpy as np
 
 from . import md, synth
 
-KNOBS = ("neighbor_skin", "prune_buffer", "ww_union_chunk", "spme_grid_step")
+KNOBS = ("neighbor_skin", "prune_buffer", "ww_union_chunk", "pair_item_entries", "spme_grid_step")
 SKINS = (1.0, 1.25, 1.5, 1.75, 2.0)
 PRUNES = (0.2, 0.3, 0.4, 0.6, 0.8)
 CHUNKS = (0, 256, 512)          # 0: the largest that lets two CTAs share an SM
+ITEMS = (4, 8, 16, 32)
 GRID_SPAN = 1.15                # grid candidates up to 15 % above the finest needed
+
+
+SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "tune_b200.json")
 
 
 def cache_path():
@@ -130,14 +140,18 @@ def tune(system, cfg, steps=100, warmup=20, tie=0.02, cache=True, stream=None, l
     """Chooses the knobs for this system (or its size class's cached choice).
     Returns {knob: value} and, with cache, stores it."""
     key = size_class(system, cfg)
-    store = load_cache() if cache else {}
-    if key in store:
-        return dict(store[key]["knobs"])
+    if cache:
+        hit = lookup(key)
+        if hit is not None:
+            return dict(hit)
     cur = {"neighbor_skin": float(cfg.neighbor_skin), "prune_buffer": float(cfg.prune_buffer or 0.4),
-           "ww_union_chunk": int(cfg.ww_union_chunk), "spme_grid_step": 0}
+           "ww_union_chunk": int(cfg.ww_union_chunk), "pair_item_entries": int(cfg.pair_item_entries or 8),
+           "spme_grid_step": 0}
     has_water = len(np.asarray(system.get("water_pos", np.zeros((0, 3, 3))))) > 0
+    has_atoms = len(np.asarray(system.get("atom_pos", np.zeros((0, 3))))) > 0
     space = [("neighbor_skin", SKINS), ("prune_buffer", PRUNES if has_water else ()),
              ("ww_union_chunk", CHUNKS if has_water else ()),
+             ("pair_item_entries", ITEMS if has_atoms else ()),
              ("spme_grid_step", tuple(range(len(grid_candidates(system, cfg)))))]
     measured = {}
     for knob, values in space:
@@ -160,12 +174,26 @@ def tune(system, cfg, steps=100, warmup=20, tie=0.02, cache=True, stream=None, l
     return cur
 
 
-def load_cache():
+def _load(path):
     try:
-        with open(cache_path()) as f:
+        with open(path) as f:
             return json.load(f)
     except (OSError, ValueError):
         return {}
+
+
+def load_cache():
+    """The user's cache (the classes tuned on this machine)."""
+    return _load(cache_path())
+
+
+def lookup(key):
+    """The knobs of a size class: the user's cache first, then the shipped
+    table; None when neither has it."""
+    for store in (load_cache(), _load(SHIPPED)):
+        if key in store:
+            return store[key]["knobs"]
+    return None
 
 
 def save_cache(store):
@@ -180,10 +208,9 @@ def save_cache(store):
 def apply_tuned(system, cfg, tune_missing=False, **kw):
     """cfg with the cached choice of its size class applied (tuned now with
     tune_missing, else the cfg unchanged when the class is not cached)."""
-    key = size_class(system, cfg)
-    store = load_cache()
-    if key in store:
-        return _apply(cfg, store[key]["knobs"], system)
+    hit = lookup(size_class(system, cfg))
+    if hit is not None:
+        return _apply(cfg, hit, system)
     if tune_missing:
         return _apply(cfg, tune(system, cfg, **kw), system)
     return cfg

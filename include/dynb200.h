@@ -317,6 +317,10 @@ typedef struct {
                              * the overflow path (global atomics, per-site
                              * gather) takes them; 0 = about twice the mean.
                              * Results do not depend on it.                 */
+    uint32_t pair_item_entries; /* list entries per work item of the
+                             * water-atom and atom-atom pair kernels (1..32);
+                             * 0 = 8.  A tuning knob: results do not depend
+                             * on it.                                       */
 } dyn_config_t;
 
 typedef struct {
@@ -437,11 +441,11 @@ int dyn_sys_step_host(dyn_sys_t h, uint32_t n_steps, float dt, const float* atom
  * check, list rebuild and prune, [2] short-range pair kernels, [3] 1-4 and
  * bonded terms, [4] SPME (mean over the steps that ran it), [5] kick,
  * reductions, thermostat/barostat and periodic tasks; the pair stage split
- * into [6] water-water (with the atoms' cluster-order copy before it),
- * [7] its j-side gather, [8] water-atom, [9] atom-atom; the SPME stage (per
- * SPME step, without an alchemical molecule) into [10] spread, [11] FFTs
- * and convolution, [12] gather, [13] corrections. */
-#define DYN_STAGES 14
+ * into [6] water-water (with the force zeroing and the atoms'
+ * cluster-order copy before it), [7] water-atom, [8] atom-atom; the SPME
+ * stage (per SPME step, without an alchemical molecule) into [9] spread,
+ * [10] FFTs and convolution, [11] gather, [12] corrections. */
+#define DYN_STAGES 13
 int dyn_sys_stage_times(dyn_sys_t h, uint32_t n_steps, float dt, double* ms);
 
 /* Number of this library's kernels one step launches (library kernels such

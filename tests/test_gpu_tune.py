@@ -24,6 +24,7 @@ def _sys(n, seed):
 
 def test_tune_caches_and_keeps_accuracy(gpu_lib, tmp_path, monkeypatch):
     monkeypatch.setenv("DYNB200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    monkeypatch.setattr(tune, "SHIPPED", str(tmp_path / "none.json"))
     sysd, cfg = _sys(700, 3)
     knobs = tune.tune(sysd, cfg, steps=20, warmup=5)
     assert set(knobs) == set(tune.KNOBS)
@@ -43,6 +44,7 @@ def test_tune_caches_and_keeps_accuracy(gpu_lib, tmp_path, monkeypatch):
 
 def test_tuned_batch_members_equal_alone(gpu_lib, tmp_path, monkeypatch):
     monkeypatch.setenv("DYNB200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    monkeypatch.setattr(tune, "SHIPPED", str(tmp_path / "none.json"))
     systems, cfgs = zip(*[_sys(n, 10 + i) for i, n in enumerate((600, 1500))])
     monkeypatch.setattr(tune, "time_steps", lambda system, cfg, *a, **k: 1.0 + 0.1 * cfg.neighbor_skin)
     b = md.MdBatch(systems, cfgs, tune=True)

@@ -40,6 +40,7 @@ def test_pick_is_stable_under_noise():
 
 def test_cache_round_trip(tmp_path, monkeypatch):
     monkeypatch.setenv("DYNB200_TUNE_CACHE", str(tmp_path / "t.json"))
+    monkeypatch.setattr(tune, "SHIPPED", str(tmp_path / "none.json"))
     sysd = synth.water_box(1000, 31.0, seed=1)
     cfg = _cfg((32, 32, 32))
     key = tune.size_class(sysd, cfg)
@@ -56,3 +57,23 @@ def test_cache_round_trip(tmp_path, monkeypatch):
     assert all(31.5 / k <= 31.5 / 36 + 1e-9 for k in g)
     other = synth.water_box(4000, 49.2, seed=3)
     assert tune.apply_tuned(other, _cfg((50, 50, 50))).spme_grid == (50, 50, 50)
+
+
+def test_shipped_table_behind_user_cache(tmp_path, monkeypatch):
+    """A class missing from the user's cache comes from the shipped table;
+    the user's cache wins where both have it."""
+    import json
+    monkeypatch.setenv("DYNB200_TUNE_CACHE", str(tmp_path / "t.json"))
+    shipped = tmp_path / "shipped.json"
+    monkeypatch.setattr(tune, "SHIPPED", str(shipped))
+    sysd = synth.water_box(1000, 31.0, seed=1)
+    cfg = _cfg((32, 32, 32))
+    key = tune.size_class(sysd, cfg)
+    assert tune.lookup(key) is None
+    ship = {"neighbor_skin": 1.75, "prune_buffer": 0.6, "ww_union_chunk": 0, "spme_grid_step": 0}
+    shipped.write_text(json.dumps({key: {"knobs": ship}}))
+    assert tune.lookup(key) == ship
+    assert tune.apply_tuned(sysd, cfg).neighbor_skin == 1.75
+    mine = dict(ship, neighbor_skin=1.25)
+    tune.save_cache({key: {"knobs": mine}})
+    assert tune.lookup(key) == mine and tune.tune(sysd, cfg) == mine
