@@ -206,7 +206,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
 // its runs of consecutive slots) into buf; one lane per run.  Called by one
 // whole warp; lane 0 arms the barrier with the byte count.
 __device__ __forceinline__ uint32_t stage_chunk(const SysView& v, uint32_t g, uint32_t lo, uint32_t hi,
-                                                float4* buf, uint64_t* bar, int lane) {
+                                                float4* buf, uint64_t* bar, int lane, uint32_t* uslot = nullptr) {
     const uint32_t nloc = v.grp_nloc[g], nrun = v.grp_nrun[g];
     const uint2* runs = v.grp_run + (size_t)g * v.cap_run;
     if (lane == 0) mbar_expect_tx(bar, (hi - lo) * (uint32_t)(4 * sizeof(float4)));
@@ -215,9 +215,12 @@ __device__ __forceinline__ uint32_t stage_chunk(const SysView& v, uint32_t g, ui
         const uint2 r = runs[t];
         const uint32_t end = t + 1 < nrun ? runs[t + 1].y : nloc;
         const uint32_t a = max(r.y, lo), e = min(end, hi);
-        if (a < e)
+        if (a < e) {
             bulk_g2s(buf + (size_t)(a - lo) * 4, v.wpos + (size_t)(r.x + (a - r.y)) * 4,
                      (e - a) * (uint32_t)(4 * sizeof(float4)), bar);
+            if (uslot)
+                for (uint32_t u = a; u < e; ++u) uslot[u - lo] = r.x + (u - r.y);
+        }
     }
     return hi - lo;
 }
@@ -292,9 +295,12 @@ __device__ __forceinline__ void jforce_add12(const SysView& v, int* jacc, uint32
 // memory (int32 fixed point, 12 components, component-major with a stride
 // of chunk + 1 words, so that both the threads' adds and the flush's reads
 // spread over the banks), then added to the union waters' forces with one
-// coalesced run of int64 reductions per chunk.  The shares depend only on
-// the lists, and every sum across threads is an integer sum: the forces are
-// the same bits run to run.
+// coalesced run of int64 reductions per chunk (the union's slots are noted
+// in shared memory while the copies are issued).  The shares depend only on
+// the lists and the chunk size, and every sum across threads is an integer
+// sum: the forces are the same bits run to run.  The list lengths of a group
+// whose union fits one chunk (almost every group) are read while its copies
+// are in flight; larger unions find each chunk's entries by binary search.
 // ---------------------------------------------------------------------------
 DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, (), ()) {
     extern __shared__ __align__(128) float4 tile[];  // union_chunk waters x 4 float4, then the j sums
@@ -303,6 +309,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
     __shared__ uint32_t woff[GRPW + 1]; // first share position of each list's chunk entries
     __shared__ uint32_t wbeg[GRPW];     // each list's first entry in the chunk
     __shared__ uint32_t wend[GRPW];     // ... and one past its last
+    __shared__ uint32_t wlen[GRPW];     // list lengths
     const int tid = threadIdx.x;
     const uint32_t nwc = v.sc->n_wclus;
     const uint32_t ng = (nwc + GRPW / WCL - 1) / (GRPW / WCL);
@@ -310,6 +317,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
     const uint32_t chunk = v.union_chunk;
     const uint32_t cs = chunk + 1;  // component stride of the j sums
     int* jacc = reinterpret_cast<int*>(tile + 4 * (size_t)chunk);  // [12][chunk + 1]
+    uint32_t* uslot = reinterpret_cast<uint32_t*>(jacc + 12 * (size_t)cs);  // [chunk] union entry -> slot
     const BoxDev b = *v.box;
     const float ljc2 = v.ljc2;
     const float sig2 = OPC_O_SIGMA * OPC_O_SIGMA;
@@ -321,38 +329,53 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
     uint32_t parity = 0;
     Acc3 a{0.0, 0.0, 0.f, 0.0};
     bool alive = true;
+    // inclusive scan of a count over the 32 lanes of a warp
+    auto scan32 = [](uint32_t x, int l) {
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (l >= o) x += y;
+        }
+        return x;
+    };
     for (uint32_t g = bk.idx; g < ng && alive; g += bk.cnt) {
         const uint32_t nloc = v.grp_nloc[g];
-        const uint32_t uoff = g * v.cap_union;  // the group's union entries
         if (tid < GRPW * 4) {
             const uint32_t s = g * GRPW + tid / 4;
             ipos[tid] = s < nslots ? v.wpos[(size_t)4 * g * GRPW + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        if (tid < GRPW) wend[tid] = 0u;
+        const bool single = nloc <= chunk;
+        if (tid >= 32 && tid < 32 + GRPW) {
+            const int w = tid - 32;
+            const uint32_t s = g * GRPW + w;
+            const uint32_t n = s < nslots ? v.winb_n[s] : 0u;
+            wlen[w] = n;
+            wend[w] = 0u;
+            if (single) {
+                // one chunk: every entry of every list
+                const uint32_t x = scan32(n, w);
+                wbeg[w] = 0u;
+                woff[w + 1] = x;
+                if (w == 0) woff[0] = 0u;
+            }
+        }
         for (uint32_t lo = 0; lo < nloc; lo += chunk) {
             const uint32_t hi = min(nloc, lo + chunk);
-            if (tid < 32) stage_chunk(v, g, lo, hi, tile, &bar, tid);
+            if (tid < 32) stage_chunk(v, g, lo, hi, tile, &bar, tid, uslot);
             for (uint32_t t = tid; t < 12 * cs; t += WT) jacc[t] = 0;
-            __syncthreads();  // wend of the previous chunk (or group start) is visible
-            if (tid >= 32 && tid < 32 + GRPW) {
+            __syncthreads();  // the lengths and wend of the previous chunk are visible
+            if (!single && tid >= 32 && tid < 32 + GRPW) {
                 // the list entries of this chunk: from where the previous
                 // chunk stopped to the first union index >= hi (lists ascend)
                 const int w = tid - 32;
-                const uint32_t s = g * GRPW + w;
-                const uint32_t n = s < nslots ? v.winb_n[s] : 0u;
-                const uint16_t* lst = v.winb + (size_t)s * v.cap_nb;
+                const uint16_t* lst = v.winb + (size_t)(g * GRPW + w) * v.cap_nb;
                 const uint32_t b0 = wend[w];
-                uint32_t l0 = b0, l1 = n;
+                uint32_t l0 = b0, l1 = wlen[w];
                 while (l0 < l1) {
                     const uint32_t m = (l0 + l1) >> 1;
                     if ((uint32_t)lst[m] < hi) l0 = m + 1; else l1 = m;
                 }
-                uint32_t x = l0 - b0;  // inclusive scan of the counts over the 32 lists
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                    if (w >= o) x += y;
-                }
+                const uint32_t x = scan32(l0 - b0, w);
                 wbeg[w] = b0;
                 woff[w + 1] = x;
                 if (w == 0) woff[0] = 0u;
@@ -440,7 +463,7 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
                 const uint32_t u = t / 12, c = t - 12 * u;
                 const int val = jacc[c * cs + u];
                 if (val != 0)
-                    fix_atomic_add(v.wforce + 12 * (size_t)v.grp_uslot[(size_t)uoff + lo + u] + c,
+                    fix_atomic_add(v.wforce + 12 * (size_t)uslot[u] + c,
                                    (long long)val * (1ll << (32 - WW_JFIX_SHIFT)));
             }
             __syncthreads();  // the tile and the sums are refilled by the next chunk or group
@@ -730,9 +753,9 @@ int ww_tile_blocks(const SysView& v) {
     return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
 }
 
-// per union water: 4 float4 positions and 12 int32 j sums (+ the stride pad)
+// per union water: 4 float4 positions, 12 int32 j sums (+ the stride pad) and its slot
 size_t ww_tile_smem(const SysView& v) {
-    return (size_t)v.union_chunk * (4 * sizeof(float4) + 12 * sizeof(int)) + 12 * sizeof(int);
+    return (size_t)v.union_chunk * (4 * sizeof(float4) + 13 * sizeof(int)) + 12 * sizeof(int);
 }
 
 // The limit is a property of the kernel, shared by every system in the

@@ -171,37 +171,57 @@ __device__ void spread_global(const SysView& v, const SiteRec& r) {
 
 // Bins the pass's charged sites by brick (records and site codes).  Atoms
 // without charge get a zero reciprocal force on pass 0, as they have none.
+// Neighbouring sites (cluster order) mostly share a brick: the lanes of a
+// warp with the same brick take their slots with one atomic.
 DYN_KERNEL(, k_bin_sites, (, int pass), (, pass)) {
     const BoxDev b = *v.box;
     const uint32_t nws = pass == 2 ? 0u : 3u * v.nw_cap;  // the molecule's own pass holds no water
     const uint32_t total = nws + v.na;
-    for (uint32_t t = bk.idx * blockDim.x + threadIdx.x; t < total; t += bk.cnt * blockDim.x) {
-        float4 p;
-        uint32_t sid;
-        if (t < nws) {
-            const uint32_t s = t / 3u, k = t % 3u;
-            const uint32_t id = v.wid[s];
-            if (id == INVALID_ID) continue;
-            p = v.wpos[4 * s + 1 + k];
-            sid = DYN_SITE_WATER | (3u * id + k);
-        } else {
-            const uint32_t a = t - nws;
-            if (!pass_has_atom(v, pass, a)) continue;
-            p = v.apos[a];
-            if (p.w == 0.f) {
-                if (pass == 0) {
-                    long long* c = v.arecip + 3 * (size_t)a;
-                    c[0] = 0; c[1] = 0; c[2] = 0;
+    const int lane = threadIdx.x & 31;
+    const uint32_t wstride = bk.cnt * blockDim.x;
+    for (uint32_t t0 = bk.idx * blockDim.x + (threadIdx.x & ~31u); t0 < total; t0 += wstride) {
+        const uint32_t t = t0 + lane;
+        bool has = false;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t sid = 0;
+        if (t < total) {
+            if (t < nws) {
+                const uint32_t s = t / 3u, k = t % 3u;
+                const uint32_t id = v.wid[s];
+                if (id != INVALID_ID) {
+                    p = v.wpos[4 * s + 1 + k];
+                    sid = DYN_SITE_WATER | (3u * id + k);
+                    has = true;
                 }
-                continue;
+            } else {
+                const uint32_t a = t - nws;
+                if (pass_has_atom(v, pass, a)) {
+                    p = v.apos[a];
+                    if (p.w != 0.f) {
+                        sid = a;
+                        has = true;
+                    } else if (pass == 0) {
+                        long long* c = v.arecip + 3 * (size_t)a;
+                        c[0] = 0; c[1] = 0; c[2] = 0;
+                    }
+                }
             }
-            sid = a;
         }
-        const SiteRec r = make_rec(xyz(p), p.w, b, v.K);
-        int base[3];
-        rec_base(r.base, base);
-        const uint32_t P = brick_index(v, base[0], base[1], base[2]);
-        const uint32_t slot = atomicAdd(&v.brick_n[P], 1u);
+        SiteRec r;
+        uint32_t P = INVALID_ID;
+        if (has) {
+            r = make_rec(xyz(p), p.w, b, v.K);
+            int base[3];
+            rec_base(r.base, base);
+            P = brick_index(v, base[0], base[1], base[2]);
+        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, P);
+        const int leader = __ffs(peers) - 1;
+        uint32_t first = 0;
+        if (has && lane == leader) first = atomicAdd(&v.brick_n[P], (uint32_t)__popc(peers));
+        first = __shfl_sync(0xffffffffu, first, leader);
+        if (!has) continue;
+        const uint32_t slot = first + __popc(peers & ((1u << lane) - 1u));
         if (slot < v.brick_cap) {
             v.brick_site[(size_t)P * v.brick_cap + slot] = r;
             v.brick_sid[(size_t)P * v.brick_cap + slot] = sid;
@@ -214,29 +234,43 @@ DYN_KERNEL(, k_bin_sites, (, int pass), (, pass)) {
     }
 }
 
+// Does a stencil with base b (points b-3 .. b, periodic in K) reach the
+// brick range [o, o + ext) of one dimension?
+__device__ __forceinline__ bool stencil_reaches(int b, int o, int ext, int K) {
+    const int lo = b - 3;
+    if (lo >= 0) return lo < o + ext && b >= o;
+    return (b >= o && 0 < o + ext) || (lo + K < o + ext && K - 1 >= o);
+}
+
 // One CTA per brick: the charge of every site whose stencil reaches the
-// brick, summed in shared memory, written once as the float grid.  Each
-// int64 contribution f is added as two native 32-bit atomics, f >> 18 and
-// its low 18 bits, whose sums give the int64 sum exactly (a grid point gets
-// at most 8 x brick_cap <= 4096 contributions of magnitude below 2^37: no
-// int32 sum overflows).
+// brick, summed in shared memory, written once as the float grid.  The
+// candidate sites (those binned in the bricks that can reach this one, a
+// host-made list) are staged SB_T records at a time with one load per
+// thread, keeping only those whose stencil does reach the brick (compacted
+// with ballots); then each kept (site, x plane) adds up to 16
+// contributions.  Each int64 contribution f is added as two native 32-bit
+// atomics, f >> 18 and its low 18 bits, whose sums give the int64 sum
+// exactly (a grid point gets at most 8 x brick_cap <= 4096 contributions of
+// magnitude below 2^37: no int32 sum overflows).
 constexpr int SPLIT = 18;
 
 DYN_KERNEL(__launch_bounds__(SB_T), k_spread_brick, (, int pass), (, pass)) {
     __shared__ int acc_hi[BR3], acc_lo[BR3];
+    __shared__ SiteRec recs[SB_T];
     __shared__ uint32_t nbr[MAX_NBR];
     __shared__ uint32_t cnt[MAX_NBR + 1];
+    __shared__ uint32_t wcnt[SB_T / 32];
     __shared__ int fold_s;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     const int K[3] = {(int)v.K[0], (int)v.K[1], (int)v.K[2]};
     for (uint32_t P = bk.idx; P < v.n_bricks; P += bk.cnt) {
         int o[3], ext[3];
         brick_origin(v, P, o, ext);
         if (tid < 32) {
-            // the bricks whose sites reach this one (host-made list) and
-            // their task counts, scanned across the warp
+            // the bricks whose sites can reach this one and their site
+            // counts, scanned across the warp
             const uint32_t q = tid < MAX_NBR ? v.brick_nbr[(size_t)P * MAX_NBR + tid] : INVALID_ID;
-            uint32_t c = q != INVALID_ID ? 4u * min(v.brick_n[q], v.brick_cap) : 0u;
+            uint32_t c = q != INVALID_ID ? min(v.brick_n[q], v.brick_cap) : 0u;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 const uint32_t x = __shfl_up_sync(0xffffffffu, c, d);
@@ -247,53 +281,73 @@ DYN_KERNEL(__launch_bounds__(SB_T), k_spread_brick, (, int pass), (, pass)) {
         }
         for (int i = tid; i < BR3; i += SB_T) { acc_hi[i] = 0; acc_lo[i] = 0; }
         __syncthreads();
-        // one (site, x plane) per thread and round: up to 16 contributions
         const uint32_t total = cnt[MAX_NBR];
-        for (uint32_t u = tid; u < total; u += SB_T) {
-            int j = 0;
-            while (u >= cnt[j + 1]) ++j;
-            const uint32_t e = (u - cnt[j]) >> 2;
-            const int a = (int)((u - cnt[j]) & 3u);
-            const SiteRec r = v.brick_site[(size_t)nbr[j] * v.brick_cap + e];
-            int base[3];
-            rec_base(r.base, base);
-            int x = base[0] - 3 + a;
-            if (x < 0) x += K[0];
-            const int lx = x - o[0];
-            if (lx < 0 || lx >= ext[0]) continue;
-            int ly[4], lz[4];
-            bool any_y = false, any_z = false;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                int y = base[1] - 3 + c, z = base[2] - 3 + c;
-                if (y < 0) y += K[1];
-                if (z < 0) z += K[2];
-                ly[c] = y - o[1];
-                lz[c] = z - o[2];
-                if (ly[c] < 0 || ly[c] >= ext[1]) ly[c] = -1; else any_y = true;
-                if (lz[c] < 0 || lz[c] >= ext[2]) lz[c] = -1; else any_z = true;
+        for (uint32_t u0 = 0; u0 < total; u0 += SB_T) {
+            // stage this round's records that reach the brick
+            const uint32_t u = u0 + tid;
+            bool keep = false;
+            SiteRec r;
+            if (u < total) {
+                int j = 0;
+                while (u >= cnt[j + 1]) ++j;
+                r = v.brick_site[(size_t)nbr[j] * v.brick_cap + (u - cnt[j])];
+                int base[3];
+                rec_base(r.base, base);
+                keep = stencil_reaches(base[0], o[0], ext[0], K[0]) && stencil_reaches(base[1], o[1], ext[1], K[1]) &&
+                       stencil_reaches(base[2], o[2], ext[2], K[2]);
             }
-            if (!any_y || !any_z) continue;
-            double tx[4], ty[4], tz[4];
-            bspline4d(r.w[0], tx);
-            bspline4d(r.w[1], ty);
-            bspline4d(r.w[2], tz);
-            const double qa = (double)r.q * tx[a];
-#pragma unroll
-            for (int bb = 0; bb < 4; ++bb) {
-                if (ly[bb] < 0) continue;
-                const double qab = qa * ty[bb];
-                const int row = (lx * PME_BRICK + ly[bb]) * PME_BRICK;
+            const uint32_t m = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) wcnt[wp] = __popc(m);
+            __syncthreads();
+            uint32_t off = 0, nk = 0;
+            for (int w = 0; w < SB_T / 32; ++w) {
+                off += w < wp ? wcnt[w] : 0u;
+                nk += wcnt[w];
+            }
+            if (keep) recs[off + __popc(m & ((1u << lane) - 1u))] = r;
+            __syncthreads();
+            // one (site, x plane) per thread and task: up to 16 contributions
+            for (uint32_t t = tid; t < 4 * nk; t += SB_T) {
+                const SiteRec& rr = recs[t >> 2];
+                const int a = (int)(t & 3u);
+                int base[3];
+                rec_base(rr.base, base);
+                int x = base[0] - 3 + a;
+                if (x < 0) x += K[0];
+                const int lx = x - o[0];
+                if (lx < 0 || lx >= ext[0]) continue;
+                int ly[4], lz[4];
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
-                    if (lz[c] < 0) continue;
-                    const long long f = fix_from_double(qab * tz[c]);
-                    atomicAdd(&acc_hi[row + lz[c]], (int)(f >> SPLIT));
-                    atomicAdd(&acc_lo[row + lz[c]], (int)(f & ((1ll << SPLIT) - 1)));
+                    int y = base[1] - 3 + c, z = base[2] - 3 + c;
+                    if (y < 0) y += K[1];
+                    if (z < 0) z += K[2];
+                    ly[c] = y - o[1];
+                    lz[c] = z - o[2];
+                    if (ly[c] < 0 || ly[c] >= ext[1]) ly[c] = -1;
+                    if (lz[c] < 0 || lz[c] >= ext[2]) lz[c] = -1;
+                }
+                double tx[4], ty[4], tz[4];
+                bspline4d(rr.w[0], tx);
+                bspline4d(rr.w[1], ty);
+                bspline4d(rr.w[2], tz);
+                const double qa = (double)rr.q * tx[a];
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    if (ly[bb] < 0) continue;
+                    const double qab = qa * ty[bb];
+                    const int row = (lx * PME_BRICK + ly[bb]) * PME_BRICK;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        if (lz[c] < 0) continue;
+                        const long long f = fix_from_double(qab * tz[c]);
+                        atomicAdd(&acc_hi[row + lz[c]], (int)(f >> SPLIT));
+                        atomicAdd(&acc_lo[row + lz[c]], (int)(f & ((1ll << SPLIT) - 1)));
+                    }
                 }
             }
+            __syncthreads();  // recs and wcnt are refilled by the next round
         }
-        __syncthreads();
         const bool fold = fold_s != 0;
         for (int i = tid; i < BR3; i += SB_T) {
             const int lx = i / (PME_BRICK * PME_BRICK), ly = (i / PME_BRICK) % PME_BRICK, lz = i % PME_BRICK;
@@ -448,19 +502,35 @@ DYN_KERNEL(__launch_bounds__(GB_T), k_gather_brick, (, int pass), (, pass)) {
         }
         int o[3], ext[3];
         brick_origin(v, P, o, ext);
-#pragma unroll 4
-        for (int i = tid; i < HB * HB * HB; i += GB_T) {
-            int x = o[0] - 3 + i / (HB * HB), y = o[1] - 3 + (i / HB) % HB, z = o[2] - 3 + i % HB;
-            x = x < 0 ? x + K[0] : (x >= K[0] ? x - K[0] : x);
-            y = y < 0 ? y + K[1] : (y >= K[1] ? y - K[1] : y);
-            z = z < 0 ? z + K[2] : (z >= K[2] ? z - K[2] : z);
-            tile[i] = __ldg(v.qgrid + ((size_t)x * K[1] + y) * K[2] + z);
-        }
-        __syncthreads();
+        // this thread's first site, loaded while the tile comes in
         const uint32_t n = min(v.brick_n[P], v.brick_cap);
+        SiteRec r0;
+        uint32_t sid0 = 0;
+        if ((uint32_t)tid < n) {
+            r0 = v.brick_site[(size_t)P * v.brick_cap + tid];
+            sid0 = v.brick_sid[(size_t)P * v.brick_cap + tid];
+        }
+        constexpr int NT = (HB * HB * HB + GB_T - 1) / GB_T;
+        float vals[NT];
+#pragma unroll
+        for (int k = 0; k < NT; ++k) {
+            const int i = tid + k * GB_T;
+            vals[k] = 0.f;
+            if (i < HB * HB * HB) {
+                int x = o[0] - 3 + i / (HB * HB), y = o[1] - 3 + (i / HB) % HB, z = o[2] - 3 + i % HB;
+                x = x < 0 ? x + K[0] : (x >= K[0] ? x - K[0] : x);
+                y = y < 0 ? y + K[1] : (y >= K[1] ? y - K[1] : y);
+                z = z < 0 ? z + K[2] : (z >= K[2] ? z - K[2] : z);
+                vals[k] = __ldg(v.qgrid + ((size_t)x * K[1] + y) * K[2] + z);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NT; ++k)
+            if (tid + k * GB_T < HB * HB * HB) tile[tid + k * GB_T] = vals[k];
+        __syncthreads();
         for (uint32_t t = tid; t < n; t += GB_T) {
             const size_t e = (size_t)P * v.brick_cap + t;
-            const SiteRec r = v.brick_site[e];
+            const SiteRec r = t == (uint32_t)tid ? r0 : v.brick_site[e];
             int base[3];
             rec_base(r.base, base);
             // stencil point a of the site is tile row (base - o) + a
@@ -468,7 +538,7 @@ DYN_KERNEL(__launch_bounds__(GB_T), k_gather_brick, (, int pass), (, pass)) {
             const float3 f = gather_rec(v, r, b, [&](int a, int bb, int c) {
                 return tile[((x0 + a) * HB + (y0 + bb)) * HB + z0 + c];
             }) * wt;
-            gather_out(v, v.brick_sid[e], f, pass);
+            gather_out(v, t == (uint32_t)tid ? sid0 : v.brick_sid[e], f, pass);
         }
         __syncthreads();  // every thread has read the count; the tile is refilled next
         if (tid == 0) v.brick_n[P] = 0u;

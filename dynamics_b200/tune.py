@@ -21,8 +21,10 @@ measurement, per size class of system, and cached:
   class member never gets a grid coarser than its configuration asks.
 
 None of them changes the physics beyond the grid's (finer grids only
-reduce the reciprocal-space error); results are the same method within the
-engine's force tolerance.  The search is coordinate descent from the
+reduce the reciprocal-space error); the others change how float sums are
+grouped, so results move only at rounding level: the same method within
+the engine's force tolerance, and bit-identical run to run for a given
+choice.  The search is coordinate descent from the
 defaults: one knob at a time, each candidate timed over whole captured steps
 (the step graph as MdState.step runs it), the fastest kept unless the
 incumbent is within ``tie`` of it, so small timing noise does not flip a

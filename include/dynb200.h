@@ -291,8 +291,9 @@ typedef struct {
     uint64_t seed;          /* Philox key for all stochastic terms          */
     uint32_t ww_union_chunk;/* waters per shared-memory chunk of the
                              * water-water kernel; 0 = the largest that lets
-                             * two CTAs share an SM (a tuning knob: results
-                             * do not depend on it)                         */
+                             * two CTAs share an SM (a tuning knob: it changes
+                             * how float sums are grouped, so results only
+                             * at rounding level)                           */
     uint32_t lincs_order;   /* bond-to-H constraints: projection passes of
                              * HydrogenConstraint::Linear (src/prep.rs:55-78);
                              * 0 = 4 (the reference default)                */
@@ -302,7 +303,7 @@ typedef struct {
                              * whenever a water has moved half of it since
                              * the last prune; 0 = 0.4 A; >= list_buffer:
                              * pruned only at list rebuilds (a tuning knob:
-                             * results do not depend on it)                 */
+                             * results change only at rounding level)       */
     /* Alchemical decoupling of the atoms [alch_begin, alch_end) (one
      * molecule, StateAlchemical, src/alchemical.rs:98-121): pairs between
      * them and the rest use soft-core LJ and scaled Coulomb, SPME is
@@ -316,11 +317,11 @@ typedef struct {
     uint32_t spme_brick_cap; /* charged sites per 8^3 SPME grid brick before
                              * the overflow path (global atomics, per-site
                              * gather) takes them; 0 = about twice the mean.
-                             * Results do not depend on it.                 */
+                             * Results do not depend on it (integer sums). */
     uint32_t pair_item_entries; /* list entries per work item of the
                              * water-atom and atom-atom pair kernels (1..32);
-                             * 0 = 8.  A tuning knob: results do not depend
-                             * on it.                                       */
+                             * 0 = 8.  A tuning knob: results change only at
+                             * rounding level.                              */
 } dyn_config_t;
 
 typedef struct {

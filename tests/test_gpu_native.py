@@ -215,21 +215,29 @@ def test_invalid_config_raises(gpu_lib):
         md.MdState(sysd, md.MdConfig(coulomb_cutoff=10.0))  # box too small for the cutoff
 
 
-def test_union_chunking_bit_identical(gpu_lib):
+def test_union_chunking(gpu_lib):
     """The water-water kernel stages a group's j-waters in shared-memory
-    chunks; forces and trajectories must not depend on the chunk size."""
+    chunks, and its threads' shares of the list entries follow the chunks,
+    so a different chunk size groups the float i-force sums differently:
+    forces agree to rounding, and every chunk size is bit-identical run to
+    run."""
     sysd = water_only()
     a = md.MdState(sysd, _cfg(sysd))
     b = md.MdState(sysd, _cfg(sysd, ww_union_chunk=64))
-    fa, fb = a.forces(), b.forces()
-    np.testing.assert_array_equal(fa["f_water"], fb["f_water"])
-    assert fa["virial"] == fb["virial"]
+    b2 = md.MdState(sysd, _cfg(sysd, ww_union_chunk=64))
+    fa, fb, fb2 = a.forces(), b.forces(), b2.forces()
+    assert rel_rms(fb["f_water"].reshape(-1), fa["f_water"].reshape(-1)) < 1e-6
+    assert abs(fa["virial"] - fb["virial"]) <= 1e-6 * abs(fa["virial"])
+    np.testing.assert_array_equal(fb["f_water"], fb2["f_water"])
     a.step(0.002, 30)
     b.step(0.002, 30)
-    np.testing.assert_array_equal(a.state()["water_pos"], b.state()["water_pos"])
+    b2.step(0.002, 30)
+    sb = b.state()
+    np.testing.assert_array_equal(sb["water_pos"], b2.state()["water_pos"])
+    assert np.max(np.abs(sb["water_pos"] - a.state()["water_pos"])) < 1e-3
     assert a.energies()["list_union_max"] > 64
-    a.close()
-    b.close()
+    for st in (a, b, b2):
+        st.close()
 
 
 @pytest.mark.parametrize("mode", ["reference", "corrected"])
