@@ -543,6 +543,12 @@ def run_ours(args):
     w = WORKLOADS[name]
     sysd, cfg = build_system(name, seed=1000 + rank)
     sysd = md.equilibrate(sysd, cfg, n_steps=args.equil, dt=0.001)
+    # the autotuner's choice for this size class (the shipped B200 table or
+    # the user's cache), if there is one
+    from dynamics_b200 import tune
+    tuned_knobs = tune.lookup(tune.size_class(sysd, cfg))
+    if tuned_knobs is not None:
+        cfg = tune.apply_tuned(sysd, cfg)
     st = md.MdState(sysd, cfg, stream=stream.cuda_stream)
     st.step(DT, args.warmup)
     torch.cuda.synchronize(dev)
@@ -585,7 +591,7 @@ def run_ours(args):
     _lib.check(_lib.lib().dyn_probe_fp32_peak(stream.cuda_stream, C.byref(peak)))
     # PME: algorithmic bytes of spread + gather per SPME step
     nq = 3 * st.n_water + st.n_atoms
-    K = np.prod(w["grid"])
+    K = np.prod(cfg.spme_grid)
     pme_bytes = nq * 16 + K * 4 + nq * 16 + K * 4 + nq * 12
     pme_ms = stages["spme"]
     spread_bytes, gather_bytes = nq * 16 + K * 4, nq * 16 + K * 4 + nq * 12
@@ -643,6 +649,8 @@ def run_ours(args):
         "data": "synthetic (seeded ff19SB peptide / ions / OPC water, equilibrated on device)"
                 if w.get("n_res") else "synthetic (seeded OPC water lattice, equilibrated on device)",
         "config": plain_config(name, cfg, st_nw, st_na, world),
+        "tuned": None if tuned_knobs is None else {"knobs": tuned_knobs, "spme_grid_used": list(cfg.spme_grid),
+                                                  "source": "dynamics_b200/data/tune_b200.json or the user cache"},
         "roofline": roofline_dominant(name, ww_flops, ww_ms, peak.value, pc),
         "roofline_pair_stage": {"bound": "fp32", "kernel": "all short-range pair kernels",
                                 "achieved": round(achieved, 3), "peak": round(peak.value, 2), "unit": "TFLOP/s",
@@ -790,6 +798,35 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def write_tune_table(path, names, steps=100, warmup=20):
+    """Tunes every size class of the given workloads on this GPU (the
+    autotuner timing whole captured steps, dynamics_b200.tune) and writes
+    the table that dynamics_b200 ships as data/tune_b200.json: per class the
+    chosen knobs and the milliseconds per step of every candidate."""
+    import torch
+    from dynamics_b200 import md, tune
+    torch.cuda.set_device(0)
+    os.environ["DYNB200_TUNE_CACHE"] = os.path.abspath(path)
+    tune.SHIPPED = os.path.abspath(path) + ".none"  # tune everything here
+    seen = set()
+    for name in names:
+        if WORKLOADS[name].get("kind") in ("batch", "serve"):
+            systems, cfgs = build_batch(name, seed=1)
+        else:
+            s, c = build_system(name, 1)
+            systems, cfgs = [s], [c]
+        for sd, c in zip(systems, cfgs):
+            key = tune.size_class(sd, c)
+            if key in seen:
+                continue
+            seen.add(key)
+            sd = md.equilibrate(sd, c, n_steps=200, dt=0.001)
+            t0 = time.perf_counter()
+            knobs = tune.tune(sd, c, steps=steps, warmup=warmup)
+            print(json.dumps({"workload": name, "class": key, "knobs": knobs,
+                              "s": round(time.perf_counter() - t0, 1)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -804,7 +841,13 @@ def main():
                     help="batched workloads: also time the members with the autotuner's choices")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain line only (no batched / served sub-objects)")
+    ap.add_argument("--write-tune-table", metavar="PATH",
+                    help="tune every size class of --tune-workloads and write the table to PATH")
+    ap.add_argument("--tune-workloads", default="c1,c2,c3,c4")
     args = ap.parse_args()
+    if args.write_tune_table:
+        write_tune_table(args.write_tune_table, args.tune_workloads.split(","))
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -159,6 +159,7 @@ struct SysView {
     // i-water a list of indices into that union
     uint32_t ngrp_cap, cap_tile, cap_nb, cap_union, cap_run;
     uint32_t union_chunk;         // waters staged in shared memory at a time
+    uint32_t ww_split;            // CTAs sharing one group's list entries (small systems)
     float4* gbb_c; float4* gbb_h;
     uint32_t* tile_n; uint32_t* tile_j;      // [ngrp_cap], [ngrp_cap*cap_tile]
     uint32_t* grp_nrun; uint32_t* grp_nloc;  // [ngrp_cap]

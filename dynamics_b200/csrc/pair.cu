@@ -301,6 +301,8 @@ __device__ __forceinline__ void jforce_add12(const SysView& v, int* jacc, uint32
 // sum: the forces are the same bits run to run.  The list lengths of a group
 // whose union fits one chunk (almost every group) are read while its copies
 // are in flight; larger unions find each chunk's entries by binary search.
+// A system with fewer groups than the GPU has SMs gives each group ww_split
+// CTAs, each staging the union and taking an equal slice of the entries.
 // ---------------------------------------------------------------------------
 DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, (), ()) {
     extern __shared__ __align__(128) float4 tile[];  // union_chunk waters x 4 float4, then the j sums
@@ -338,7 +340,9 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
         }
         return x;
     };
-    for (uint32_t g = bk.idx; g < ng && alive; g += bk.cnt) {
+    const uint32_t split = v.ww_split;
+    for (uint32_t q = bk.idx; q < ng * split && alive; q += bk.cnt) {
+        const uint32_t g = q / split, part = q - g * split;
         const uint32_t nloc = v.grp_nloc[g];
         if (tid < GRPW * 4) {
             const uint32_t s = g * GRPW + tid / 4;
@@ -389,10 +393,13 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
                 break;
             }
             parity ^= 1u;
-            // this thread's share [e0, e1) of the chunk's entries
+            // this CTA's slice of the chunk's entries, and this thread's
+            // share [e0, e1) of the slice
             const uint32_t total = woff[GRPW];
-            const uint32_t e0 = (uint32_t)(((uint64_t)tid * total) / WT);
-            const uint32_t e1 = (uint32_t)(((uint64_t)(tid + 1) * total) / WT);
+            const uint32_t s0 = (uint32_t)(((uint64_t)part * total) / split);
+            const uint32_t slen = (uint32_t)(((uint64_t)(part + 1) * total) / split) - s0;
+            const uint32_t e0 = s0 + (uint32_t)(((uint64_t)tid * slen) / WT);
+            const uint32_t e1 = s0 + (uint32_t)(((uint64_t)(tid + 1) * slen) / WT);
             int w = 0;
             while (w < GRPW - 1 && woff[w + 1] <= e0) ++w;
             float3 iO = f3(0, 0, 0), iH0 = iO, iH1 = iO, iM = iO;
@@ -750,7 +757,8 @@ namespace dyn {
 int pair_blocks_ws(const SysView& v) { return pblocks(v, v.ws_item_cap); }
 
 int ww_tile_blocks(const SysView& v) {
-    return (int)(v.ngrp_cap < v.max_blocks ? v.ngrp_cap : v.max_blocks);
+    const uint64_t n = (uint64_t)v.ngrp_cap * v.ww_split;
+    return (int)(n < v.max_blocks ? n : v.max_blocks);
 }
 
 // per union water: 4 float4 positions, 12 int32 j sums (+ the stride pad) and its slot

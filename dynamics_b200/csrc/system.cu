@@ -559,6 +559,12 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         if (cfg->ww_union_chunk)
             v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(v.union_chunk, cfg->ww_union_chunk / 32 * 32));
         v.cap_run = v.cap_union;  // a run per union water at worst
+        // fewer water groups than SMs: several CTAs share each group's entries
+        int n_sm = 0;
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        v.ww_split = v.ngrp_cap ? std::max<uint32_t>(1u, std::min<uint32_t>(8u, ((uint32_t)std::max(n_sm, 1) +
+                                                                               v.ngrp_cap - 1) / v.ngrp_cap))
+                                : 1u;
         const double nb = 4.0 / 3.0 * M_PI * r * r * r * dl;
         // half lists: about nb / 2 partners above a water's slot on average,
         // but the first waters of the slot order keep nearly all of theirs
