@@ -438,11 +438,65 @@ def count_pairs(sysd, cutoff):
 
 
 class ClockSampler:
-    def __init__(self, path):
+    """SM clocks and clock-event reasons sampled DURING a timed region: an
+    in-process thread reads NVML every 10 ms (read-only queries), so even a
+    region of a few milliseconds gets samples; nvidia-smi -lms 200 is the
+    fallback when NVML is unavailable.  Rows go to ``path`` as CSV."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, path, device_index=None):
         self.path = path
         self.proc = None
+        self.thread = None
+        self.rows = []
+        self.device_index = device_index
+
+    def _nvml_loop(self, nv, h, index):
+        import threading
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.rows.append([str(index), str(sm), str(mx), f"{pw:.1f}", hex(rs)] +
+                                 ["Active" if rs & getattr(nv, c) else "Not Active" for _, c in self.REASONS])
+            except Exception:
+                pass
+            self.stop.wait(0.01)
 
     def __enter__(self):
+        import threading
+        index = self.device_index
+        if index is None:
+            try:
+                import torch
+                index = torch.cuda.current_device()
+            except Exception:
+                index = 0
+        self.index = index
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            # the physical GPU behind this process's device index
+            vis = [x.strip() for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+            ident = vis[index] if index < len(vis) else str(index)
+            if ident.startswith("GPU-"):
+                h = nv.nvmlDeviceGetHandleByUUID(ident)
+            else:
+                h = nv.nvmlDeviceGetHandleByIndex(int(ident) if ident.isdigit() else index)
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h, index), daemon=True)
+            self.thread.start()
+            while not self.rows and self.thread.is_alive():
+                time.sleep(0.002)  # the first sample precedes the timed region
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
@@ -456,6 +510,12 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=2)
+            with open(self.path, "w") as f:
+                for r in self.rows:
+                    f.write(", ".join(r) + "\n")
         if self.proc is not None:
             self.proc.terminate()
             try:

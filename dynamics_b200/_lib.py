@@ -66,7 +66,7 @@ class Config(C.Structure):
         ("ww_union_chunk", C.c_uint32), ("lincs_order", C.c_uint32), ("lincs_iter", C.c_uint32),
         ("prune_buffer", C.c_float),
         ("alch_begin", C.c_uint32), ("alch_end", C.c_uint32), ("alch_lambda", C.c_float),
-        ("spme_brick_cap", C.c_uint32), ("pair_item_entries", C.c_uint32),
+        ("spme_brick_cap", C.c_uint32), ("pair_item_entries", C.c_uint32), ("ww_split", C.c_uint32),
     ]
 
 

@@ -565,6 +565,7 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         v.ww_split = v.ngrp_cap ? std::max<uint32_t>(1u, std::min<uint32_t>(8u, ((uint32_t)std::max(n_sm, 1) +
                                                                                v.ngrp_cap - 1) / v.ngrp_cap))
                                 : 1u;
+        if (cfg->ww_split) v.ww_split = std::min(8u, cfg->ww_split);
         const double nb = 4.0 / 3.0 * M_PI * r * r * r * dl;
         // half lists: about nb / 2 partners above a water's slot on average,
         // but the first waters of the slot order keep nearly all of theirs

@@ -113,6 +113,9 @@ class MdConfig:
     # list entries per work item of the water-atom and atom-atom pair
     # kernels (1..32); 0 = 8 (tuning knob only)
     pair_item_entries: int = 0
+    # CTAs sharing one water group's list entries (1..8); 0 = automatic
+    # (tuning knob only)
+    ww_split: int = 0
     lincs_order: int = 4            # HydrogenConstraint::Linear { order, iter } (src/prep.rs:77)
     lincs_iter: int = 1
     # constraint position corrections also correct the velocities (RATTLE);
@@ -204,6 +207,7 @@ def _config_struct(system, cfg):
     c.prune_buffer = float(cfg.prune_buffer)
     c.spme_brick_cap = int(cfg.spme_brick_cap)
     c.pair_item_entries = int(cfg.pair_item_entries)
+    c.ww_split = int(cfg.ww_split)
     c.lincs_order = int(cfg.lincs_order)
     c.lincs_iter = int(cfg.lincs_iter)
     return c

@@ -13,6 +13,8 @@ measurement, per size class of system, and cached:
 * ``pair_item_entries``: list entries per work item of the water-atom and
   atom-atom pair kernels (more items balance better, fewer amortise the
   per-item loads);
+* ``ww_split``: CTAs sharing one water group's list entries (more CTAs
+  shorten the last wave, each stages the group's union again);
 * ``spme_grid``: the SPME grid among FFT-friendly sizes whose spacing is at
   most the configured grid's (the accuracy rule: a finer grid is never less
   accurate, so every candidate holds the force tolerance), at the
@@ -48,11 +50,12 @@ import numpy as np
 
 from . import md, synth
 
-KNOBS = ("neighbor_skin", "prune_buffer", "ww_union_chunk", "pair_item_entries", "spme_grid_step")
+KNOBS = ("neighbor_skin", "prune_buffer", "ww_union_chunk", "ww_split", "pair_item_entries", "spme_grid_step")
 SKINS = (1.0, 1.25, 1.5, 1.75, 2.0)
 PRUNES = (0.2, 0.3, 0.4, 0.6, 0.8)
 CHUNKS = (0, 256, 512)          # 0: the largest that lets two CTAs share an SM
 ITEMS = (4, 8, 16, 32)
+SPLITS = (0, 1, 2, 4)           # 0: automatic
 GRID_SPAN = 1.15                # grid candidates up to 15 % above the finest needed
 
 
@@ -147,12 +150,14 @@ def tune(system, cfg, steps=100, warmup=20, tie=0.02, cache=True, stream=None, l
         if hit is not None:
             return dict(hit)
     cur = {"neighbor_skin": float(cfg.neighbor_skin), "prune_buffer": float(cfg.prune_buffer or 0.4),
-           "ww_union_chunk": int(cfg.ww_union_chunk), "pair_item_entries": int(cfg.pair_item_entries or 8),
+           "ww_union_chunk": int(cfg.ww_union_chunk), "ww_split": int(cfg.ww_split),
+           "pair_item_entries": int(cfg.pair_item_entries or 8),
            "spme_grid_step": 0}
     has_water = len(np.asarray(system.get("water_pos", np.zeros((0, 3, 3))))) > 0
     has_atoms = len(np.asarray(system.get("atom_pos", np.zeros((0, 3))))) > 0
     space = [("neighbor_skin", SKINS), ("prune_buffer", PRUNES if has_water else ()),
              ("ww_union_chunk", CHUNKS if has_water else ()),
+             ("ww_split", SPLITS if has_water else ()),
              ("pair_item_entries", ITEMS if has_atoms else ()),
              ("spme_grid_step", tuple(range(len(grid_candidates(system, cfg)))))]
     measured = {}

@@ -322,6 +322,12 @@ typedef struct {
                              * water-atom and atom-atom pair kernels (1..32);
                              * 0 = 8.  A tuning knob: results change only at
                              * rounding level.                              */
+    uint32_t ww_split;      /* CTAs that share one 32-water group's list
+                             * entries in the water-water kernel (1..8);
+                             * 0 = automatic (more than 1 only when the
+                             * system has fewer groups than the GPU has
+                             * SMs).  A tuning knob: results change only at
+                             * rounding level.                              */
 } dyn_config_t;
 
 typedef struct {
