@@ -243,17 +243,23 @@ __device__ __forceinline__ bool stencil_reaches(int b, int o, int ext, int K) {
 }
 
 // One CTA per brick: the charge of every site whose stencil reaches the
-// brick, written once as the float grid, without atomics.  The candidate
-// sites (those binned in the bricks that can reach this one, a host-made
-// list) are staged SB_T records at a time with one load per thread, keeping
-// only those whose stencil does reach the brick (compacted with ballots),
-// each with its FP64 B-spline weights.  Each of the brick's 8 x 8 (x, y)
-// columns belongs to 4 threads, each walking a quarter of the kept sites
-// and summing the contributions to its column's 8 points in int64
-// registers; the quarters are then added with shuffles.  The contributions
-// are the per-site path's values (q tx, times ty, times tz, in FP64, to
-// fixed point), and integer sums do not depend on their order.
+// brick, summed in shared memory, written once as the float grid.  The
+// candidate sites (those binned in the bricks that can reach this one, a
+// host-made list) are staged SB_T records at a time with one load per
+// thread, keeping only those whose stencil does reach the brick (compacted
+// with ballots), each with its FP64 B-spline weights.  Then each half-warp
+// takes one kept site, a lane per (x, y) column of its 4 x 4 x 4 stencil
+// adding the column's 4 contributions: the lanes of a site touch distinct
+// points, and the two halves of a warp take sites half the list apart, so
+// the shared-memory adds rarely collide.  Each int64 contribution f (the
+// per-site path's value: q tx, times ty, times tz, in FP64, to fixed point)
+// is added as two native 32-bit atomics, f >> 18 and its low 18 bits, whose
+// sums give the int64 sum exactly (a grid point gets at most 8 x brick_cap
+// <= 4096 contributions of magnitude below 2^37: no int32 sum overflows).
+constexpr int SPLIT = 18;
+
 DYN_KERNEL(__launch_bounds__(SB_T), k_spread_brick, (, int pass), (, pass)) {
+    __shared__ int acc_hi[BR3], acc_lo[BR3];
     __shared__ SiteRec recs[SB_T];
     __shared__ double wts[SB_T][12];   // tx[4], ty[4], tz[4] of each kept site
     __shared__ uint32_t nbr[MAX_NBR];
@@ -261,8 +267,7 @@ DYN_KERNEL(__launch_bounds__(SB_T), k_spread_brick, (, int pass), (, pass)) {
     __shared__ uint32_t wcnt[SB_T / 32];
     __shared__ int fold_s;
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    const int col = tid >> 2, quarter = tid & 3;
-    const int cx = col >> 3, cy = col & 7;
+    const int half = lane >> 4, a = (lane >> 2) & 3, bb = lane & 3;
     const int K[3] = {(int)v.K[0], (int)v.K[1], (int)v.K[2]};
     for (uint32_t P = bk.idx; P < v.n_bricks; P += bk.cnt) {
         int o[3], ext[3];
@@ -280,13 +285,8 @@ DYN_KERNEL(__launch_bounds__(SB_T), k_spread_brick, (, int pass), (, pass)) {
             if (tid < MAX_NBR) { nbr[tid] = q; cnt[tid + 1] = c; }
             if (tid == 0) { cnt[0] = 0u; fold_s = v.brick_ovf[P] != 0u; }
         }
+        for (int i = tid; i < BR3; i += SB_T) { acc_hi[i] = 0; acc_lo[i] = 0; }
         __syncthreads();
-        // this column's point (X, Y) and its 8 sums
-        const bool col_in = cx < ext[0] && cy < ext[1];
-        const int X = o[0] + cx, Y = o[1] + cy;
-        long long acc[PME_BRICK];
-#pragma unroll
-        for (int z = 0; z < PME_BRICK; ++z) acc[z] = 0;
         const uint32_t total = cnt[MAX_NBR];
         for (uint32_t u0 = 0; u0 < total; u0 += SB_T) {
             // stage this round's records that reach the brick, with weights
@@ -318,53 +318,50 @@ DYN_KERNEL(__launch_bounds__(SB_T), k_spread_brick, (, int pass), (, pass)) {
                 bspline4d(r.w[2], &wts[k][8]);
             }
             __syncthreads();
-            if (col_in) {
-                for (uint32_t k = quarter; k < nk; k += 4) {
-                    int base[3];
-                    rec_base(recs[k].base, base);
-                    // stencil offsets of this column: point = base - 3 + offset (periodic)
-                    int a = X - base[0] + 3, bb = Y - base[1] + 3;
-                    if (a < 0) a += K[0]; else if (a >= K[0]) a -= K[0];
-                    if (bb < 0) bb += K[1]; else if (bb >= K[1]) bb -= K[1];
-                    if (a > 3 || bb > 3) continue;
-                    const double qab = ((double)recs[k].q * wts[k][a]) * wts[k][4 + bb];
-                    int c0 = o[2] - base[2] + 3;  // offset of the column's first point
-                    if (c0 < 0) c0 += K[2]; else if (c0 >= K[2]) c0 -= K[2];
+            // half-warp h of warp w: sites w + 8 i (first half) and the same
+            // half the list further on (second half)
+            const uint32_t hn = (nk + 1) / 2;
+            for (uint32_t k0 = (uint32_t)wp; k0 < hn; k0 += SB_T / 32) {
+                const uint32_t k = k0 + (half ? hn : 0u);
+                if (k >= nk) continue;
+                int base[3];
+                rec_base(recs[k].base, base);
+                int x = base[0] - 3 + a, y = base[1] - 3 + bb;
+                if (x < 0) x += K[0];
+                if (y < 0) y += K[1];
+                const int lx = x - o[0], ly = y - o[1];
+                if (lx < 0 || lx >= ext[0] || ly < 0 || ly >= ext[1]) continue;
+                const double qab = ((double)recs[k].q * wts[k][a]) * wts[k][4 + bb];
+                const int row = (lx * PME_BRICK + ly) * PME_BRICK;
 #pragma unroll
-                    for (int z = 0; z < PME_BRICK; ++z) {
-                        int c = c0 + z;
-                        if (c >= K[2]) c -= K[2];
-                        if (c <= 3 && z < ext[2]) acc[z] += fix_from_double(qab * wts[k][8 + c]);
-                    }
+                for (int c = 0; c < 4; ++c) {
+                    int z = base[2] - 3 + c;
+                    if (z < 0) z += K[2];
+                    const int lz = z - o[2];
+                    if (lz < 0 || lz >= ext[2]) continue;
+                    const long long f = fix_from_double(qab * wts[k][8 + c]);
+                    atomicAdd(&acc_hi[row + lz], (int)(f >> SPLIT));
+                    atomicAdd(&acc_lo[row + lz], (int)(f & ((1ll << SPLIT) - 1)));
                 }
             }
             __syncthreads();  // recs, wts and wcnt are refilled by the next round
         }
-        // the column's 4 quarters -> one sum per point (lanes 4 col .. 4 col + 3)
-#pragma unroll
-        for (int z = 0; z < PME_BRICK; ++z) {
-            acc[z] += __shfl_xor_sync(0xffffffffu, acc[z], 1);
-            acc[z] += __shfl_xor_sync(0xffffffffu, acc[z], 2);
-        }
         const bool fold = fold_s != 0;
-        if (col_in) {
-            // lane quarter writes points 2 quarter and 2 quarter + 1
-#pragma unroll
-            for (int z = 0; z < PME_BRICK; ++z) {
-                if ((z >> 1) == quarter && z < ext[2]) {
-                    const size_t gi = ((size_t)X * K[1] + Y) * K[2] + (o[2] + z);
-                    long long q = acc[z];
-                    if (fold) {
-                        // overflow sites' charge from the global fixed-point grid
-                        q += v.qgrid_fix[gi];
-                        v.qgrid_fix[gi] = 0;
-                    }
-                    v.qgrid[gi] = (float)((double)q * DYN_FIX_INV);
+        for (int i = tid; i < BR3; i += SB_T) {
+            const int lx = i / (PME_BRICK * PME_BRICK), ly = (i / PME_BRICK) % PME_BRICK, lz = i % PME_BRICK;
+            if (lx < ext[0] && ly < ext[1] && lz < ext[2]) {
+                const size_t gi = ((size_t)(o[0] + lx) * K[1] + (o[1] + ly)) * K[2] + (o[2] + lz);
+                long long q = (long long)acc_hi[i] * (1ll << SPLIT) + (long long)acc_lo[i];
+                if (fold) {
+                    // overflow sites' charge from the global fixed-point grid
+                    q += v.qgrid_fix[gi];
+                    v.qgrid_fix[gi] = 0;
                 }
+                v.qgrid[gi] = (float)((double)q * DYN_FIX_INV);
             }
         }
         if (tid == 0 && fold) v.brick_ovf[P] = 0u;
-        __syncthreads();  // the brick list is refilled by the next brick
+        __syncthreads();  // the sums and the brick list are refilled by the next brick
     }
 }
 
