@@ -278,6 +278,20 @@ __device__ __forceinline__ void jforce_add12(const SysView& v, int* jacc, uint32
     }
 }
 
+// Per-warp partials (the atom pair kernels' warps run independent work
+// items: no block barrier at the end); fixed shuffle order, so the sums are
+// deterministic.  The region holds blocks x PT/32 entries.
+template <bool ENERGY>
+__device__ __forceinline__ void write_partials_warp(const SysView& v, Blk bk, int region, double el, double ec,
+                                                    double w, double dh) {
+    el = warp_sum_d(el); ec = warp_sum_d(ec); w = warp_sum_d(w); dh = warp_sum_d(dh);
+    if ((threadIdx.x & 31) == 0) {
+        const size_t e = (size_t)bk.idx * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        double* p = v.partials + ((size_t)region * v.max_blocks + e) * 4;
+        p[0] = el; p[1] = ec; p[2] = w; p[3] = dh;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // water(i) - water(j), tile form, half lists.  One CTA per 32-water
 // i-group.  The waters the group's lists reach (its union, stored as runs
@@ -631,7 +645,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT, 4),
         a.flush_w();
         ew += a.wd;
     }
-    write_partials<ENERGY>(v, bk, REG_WS, el, ec, ew, dh);
+    write_partials_warp<ENERGY>(v, bk, REG_WS, el, ec, ew, dh);
 }
 
 // ---------------------------------------------------------------------------
@@ -710,7 +724,7 @@ DYN_KERNEL_T((bool ENERGY, bool ALCH), (ENERGY, ALCH), __launch_bounds__(PT), k_
         a.flush_w();
         ew += a.wd;
     }
-    write_partials<ENERGY>(v, bk, REG_SS, el, ec, ew, dh);
+    write_partials_warp<ENERGY>(v, bk, REG_SS, el, ec, ew, dh);
 }
 
 // ---------------------------------------------------------------------------
@@ -746,7 +760,8 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), , k_pair14, (), ()) {
 inline int pblocks(const SysView& v, uint64_t warps) {
     uint64_t bl = (warps * 32 + PT - 1) / PT;
     if (bl < 1) bl = 1;
-    const uint64_t cap = std::min<uint64_t>(v.max_blocks, 148u * 4u);
+    // at most max_blocks / 4: the kernels write one partial per warp
+    const uint64_t cap = std::min<uint64_t>(v.max_blocks / (PT / 32), 148u * 4u);
     return (int)(bl < cap ? bl : cap);
 }
 
@@ -802,7 +817,7 @@ inline bool any_alch(const Target& t) {
 }
 
 void launch_pairs_atoms(const Target& t, bool energy) {
-    auto ss = [](const SysView& v) { return v.na ? (int)v.nb[REG_SS] : 0; };
+    auto ss = [](const SysView& v) { return v.na ? pair_blocks_ss(v) : 0; };
     const bool al = any_alch(t);
     if (energy && al) t.launch(k_pair_ss<true, true>, k_pair_ss_batch<true, true>, ss, PT, 0);
     else if (energy) t.launch(k_pair_ss<true, false>, k_pair_ss_batch<true, false>, ss, PT, 0);
@@ -828,7 +843,7 @@ void launch_pairs_water(const Target& t, bool energy) {
 }
 
 void launch_pairs_ws(const Target& t, bool energy) {
-    auto ws = [](const SysView& v) { return v.nw && v.na ? (int)v.nb[REG_WS] : 0; };
+    auto ws = [](const SysView& v) { return v.nw && v.na ? pair_blocks_ws(v) : 0; };
     const bool al = any_alch(t);
     if (energy && al) t.launch(k_pair_ws<true, true>, k_pair_ws_batch<true, true>, ws, PT, 0);
     else if (energy) t.launch(k_pair_ws<true, false>, k_pair_ws_batch<true, false>, ws, PT, 0);

@@ -81,9 +81,10 @@ void host_m_site(const float* o, const float* h0, const float* h1, float* m) {
 void set_block_counts(SysView& v) {
     for (int r = 0; r < NREGION; ++r) v.nb[r] = 0;
     v.nb[REG_WW] = v.nw ? dyn::ww_tile_blocks(v) : 0;
-    v.nb[REG_WS] = (v.nw && v.na) ? dyn::pair_blocks_ws(v) : 0;
+    // the atom pair kernels write one partial per warp (4 per block)
+    v.nb[REG_WS] = (v.nw && v.na) ? 4u * dyn::pair_blocks_ws(v) : 0;
     v.nb[REG_SW] = 0;
-    v.nb[REG_SS] = v.na ? dyn::pair_blocks_ss(v) : 0;
+    v.nb[REG_SS] = v.na ? 4u * dyn::pair_blocks_ss(v) : 0;
     v.nb[REG_14] = v.n14 ? dyn::pair14_blocks(v) : 0;
     v.nb[REG_BOND] = (v.nbond + v.nangle + v.ndih) ? dyn::bond_blocks(v) : 0;
     v.nb[REG_KICK_W] = v.nw ? dyn::kick_blocks_w(v) : 0;
