@@ -90,7 +90,7 @@ def build_system(name, seed):
         cfg.integrator = md.VerletVelocity(thermostat=0.1)
     if w["barostat"]:
         cfg.barostat_cfg = md.BarostatCfg(pressure_target=1.0, tau=5.0, solvent_compressibility=4.5e-5)
-    return sysd, cfg
+    return sysd, _override(cfg)
 
 
 def _member_job(job):
@@ -121,6 +121,19 @@ def build_members(w, sizes, seeds, rng):
         return list(ex.map(_member_job, jobs, chunksize=max(1, len(jobs) // (4 * workers))))
 
 
+# MdConfig fields set from the command line (--set field=value), applied to
+# every system a workload builds
+CFG_OVERRIDES = {}
+
+
+def _override(cfg):
+    for k, val in CFG_OVERRIDES.items():
+        if not hasattr(cfg, k):
+            raise SystemExit(f"--set: MdConfig has no field {k!r}")
+        setattr(cfg, k, type(getattr(cfg, k))(val))
+    return cfg
+
+
 def build_batch(name, seed):
     from dynamics_b200 import md, synth
     w = WORKLOADS[name]
@@ -134,7 +147,7 @@ def build_batch(name, seed):
                           spme_grid=grid, seed=seed * 1000 + i,
                           integrator=md.LangevinMiddle(gamma=1.0))
         systems.append(sysd)
-        cfgs.append(cfg)
+        cfgs.append(_override(cfg))
     return systems, cfgs
 
 
@@ -904,7 +917,12 @@ def main():
     ap.add_argument("--write-tune-table", metavar="PATH",
                     help="tune every size class of --tune-workloads and write the table to PATH")
     ap.add_argument("--tune-workloads", default="c1,c2,c3,c4")
+    ap.add_argument("--set", action="append", default=[], metavar="FIELD=VALUE",
+                    help="set an MdConfig field (numeric) for every system of the workload")
     args = ap.parse_args()
+    for kv in args.set:
+        k, _, val = kv.partition("=")
+        CFG_OVERRIDES[k.strip()] = float(val) if "." in val else int(val)
     if args.write_tune_table:
         write_tune_table(args.write_tune_table, args.tune_workloads.split(","))
         return
