@@ -101,6 +101,8 @@ namespace dyn {
 int check_scalars(dyn_sys_s* h);
 // The energies of the last step from h->h_sc (already on the host).
 void energies_of(dyn_sys_s* h, dyn_energies_t* e);
+// The water-water kernel's CTAs per group (before any step graph exists).
+void set_ww_split(dyn_sys_s* h, uint32_t split);
 
 // Inside an active capture on st: appends an IF node on hc after everything
 // captured so far and starts capturing its body on aux.

@@ -1470,4 +1470,9 @@ int evaluate_forces(dyn_sys_s* h) { return evaluate_forces_now(h); }
 
 namespace dyn {
 void energies_of(dyn_sys_s* h, dyn_energies_t* e) { fill_energies(h, e); }
+
+void set_ww_split(dyn_sys_s* h, uint32_t split) {
+    h->v.ww_split = std::max(1u, std::min(8u, split));
+    set_block_counts(h->v);
+}
 }  // namespace dyn

@@ -541,7 +541,11 @@ class MdBatch:
         cfgs = list(cfgs)
         if tune:
             from . import tune as _tune
-            cfgs = [_tune.apply_tuned(s, c, tune_missing=True, stream=stream) for s, c in zip(systems, cfgs)]
+            import dataclasses as _dc
+            # the tuner times systems alone; in a batch the members keep their
+            # own ww_split (0: none, as the batch fills the GPU)
+            cfgs = [_dc.replace(_tune.apply_tuned(s, c, tune_missing=True, stream=stream), ww_split=c.ww_split)
+                    for s, c in zip(systems, cfgs)]
         self.cfgs = cfgs
         n = len(systems)
         descs = (_lib.SystemDesc * max(n, 1))()

@@ -324,10 +324,10 @@ typedef struct {
                              * rounding level.                              */
     uint32_t ww_split;      /* CTAs that share one 32-water group's list
                              * entries in the water-water kernel (1..8);
-                             * 0 = automatic (more than 1 only when the
-                             * system has fewer groups than the GPU has
-                             * SMs).  A tuning knob: results change only at
-                             * rounding level.                              */
+                             * 0 = automatic: more than 1 only for a system
+                             * stepped alone with fewer groups than the GPU
+                             * has SMs; batch members get 1.  A tuning knob:
+                             * results change only at rounding level.       */
 } dyn_config_t;
 
 typedef struct {

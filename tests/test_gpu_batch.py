@@ -18,6 +18,9 @@ pytestmark = pytest.mark.gpu
 def _cfg(sysd, integ=None, **kw):
     box = float(sysd["box_hi"][0] - sysd["box_lo"][0])
     k = synth.fft_size(int(np.ceil(box)))
+    # ww_split 1: what a batch member gets by default, so the same system
+    # alone runs the same water-water partition
+    kw.setdefault("ww_split", 1)
     c = md.MdConfig(coulomb_cutoff=8.0, lj_cutoff=8.0, spme_alpha=synth.ewald_alpha(8.0),
                     spme_grid=(k, k, k), **kw)
     if integ is not None:

@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 def _sys(n, seed):
     sysd, grid = synth.batch_member(n, seed=seed)
-    cfg = md.MdConfig(coulomb_cutoff=9.0, lj_cutoff=9.0, spme_alpha=synth.ewald_alpha(9.0), spme_grid=grid,
+    cfg = md.MdConfig(coulomb_cutoff=9.0, lj_cutoff=9.0, spme_alpha=synth.ewald_alpha(9.0), spme_grid=grid, ww_split=1,
                       integrator=md.LangevinMiddle(gamma=1.0), seed=seed)
     return sysd, cfg
 
