@@ -311,11 +311,12 @@ def serve_once(pool, stream_spec, steps_each, budget, max_members, stream):
 
 
 def measure_served(name, args, stream, capacity_req_per_s=None, n_req=400, steps_each=1000, pool_size=64,
-                   budget=3e9):
+                   budget=0.7e9):
     """Serving form: continuous batching of a Poisson stream at the workload's
     rate (20 / s) and at a sustainable rate (half the measured batched
     capacity), under a device-memory budget small enough to hold requests
-    back, against a real server run one request at a time."""
+    back (0.7 GB: unconstrained, the 20 / s stream peaks near 1.2 GB), against
+    a real server run one request at a time."""
     w = WORKLOADS[name]
     rate = w["rate"]
     pool, spec = serve_requests(name, n_req, rate, steps_each, 7, pool_size, args)
