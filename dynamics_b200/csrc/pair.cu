@@ -341,6 +341,8 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
     const double ehh = (double)OPC_Q_H * (double)OPC_Q_H, ehm = (double)OPC_Q_H * (double)OPC_Q_EP,
                  emm = (double)OPC_Q_EP * (double)OPC_Q_EP;
     if (tid == 0) mbar_init(&bar, 1);
+    // the j sums start at zero; each chunk's flush zeroes what it read
+    for (uint32_t t = tid; t < 12 * cs; t += WT) jacc[t] = 0;
     __syncthreads();
     uint32_t parity = 0;
     Acc3 a{0.0, 0.0, 0.f, 0.0};
@@ -380,7 +382,6 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
         for (uint32_t lo = 0; lo < nloc; lo += chunk) {
             const uint32_t hi = min(nloc, lo + chunk);
             if (tid < 32) stage_chunk(v, g, lo, hi, tile, &bar, tid, uslot);
-            for (uint32_t t = tid; t < 12 * cs; t += WT) jacc[t] = 0;
             __syncthreads();  // the lengths and wend of the previous chunk are visible
             if (!single && tid >= 32 && tid < 32 + GRPW) {
                 // the list entries of this chunk: from where the previous
@@ -483,9 +484,11 @@ DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, 
             for (uint32_t t = tid; t < 12 * (hi - lo); t += WT) {
                 const uint32_t u = t / 12, c = t - 12 * u;
                 const int val = jacc[c * cs + u];
-                if (val != 0)
+                if (val != 0) {
+                    jacc[c * cs + u] = 0;
                     fix_atomic_add(v.wforce + 12 * (size_t)uslot[u] + c,
                                    (long long)val * (1ll << (32 - WW_JFIX_SHIFT)));
+                }
             }
             __syncthreads();  // the tile and the sums are refilled by the next chunk or group
         }
