@@ -201,7 +201,7 @@ struct SysView {
     uint32_t nbrick[3], n_bricks, brick_cap, n_sites_max;
     uint32_t* brick_n;      // [n_bricks] sites binned this pass (the gather zeroes it)
     uint32_t* brick_ovf;    // [n_bricks] 1: overflow charge for this brick waits in qgrid_fix
-    uint32_t* brick_nbr;    // [n_bricks][27] bricks whose sites reach the brick (INVALID_ID-padded)
+    long long* brick_tile;  // [n_bricks][11^3] each brick's spread tile (the brick and 3 points below)
     SiteRec* brick_site;    // [n_bricks * brick_cap]
     uint32_t* brick_sid;    // site codes (atom index, or DYN_SITE_WATER | 3 * water id + site)
     SiteRec* ovf_site;      // [n_sites_max]
@@ -431,7 +431,6 @@ int pme_blocks(const SysView& v);
 int gather_blocks(const SysView& v);
 // brick layout and capacity of the spread / gather (nbrick, n_bricks, brick_cap, n_sites_max)
 void pme_bricks(SysView& v, uint32_t cap);
-void pme_brick_sources(const SysView& v, std::vector<uint32_t>& out);
 int corr_blocks(const SysView& v);
 
 // integrate.cu

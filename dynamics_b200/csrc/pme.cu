@@ -100,7 +100,6 @@ constexpr int GB_T = 128;                               // gather: threads per C
 constexpr int BR3 = PME_BRICK * PME_BRICK * PME_BRICK;
 constexpr int HB = PME_BRICK + 3;                       // gather tile edge (brick + halo)
 constexpr int OVF_BLOCKS = 8;                           // gather CTAs for the overflow list
-constexpr int MAX_NBR = 27;                             // bricks whose sites can reach a brick
 
 __device__ __forceinline__ void rec_base(uint32_t b, int* base) {
     base[0] = (int)(b & 1023u);
@@ -234,134 +233,122 @@ DYN_KERNEL(, k_bin_sites, (, int pass), (, pass)) {
     }
 }
 
-// Does a stencil with base b (points b-3 .. b, periodic in K) reach the
-// brick range [o, o + ext) of one dimension?
-__device__ __forceinline__ bool stencil_reaches(int b, int o, int ext, int K) {
-    const int lo = b - 3;
-    if (lo >= 0) return lo < o + ext && b >= o;
-    return (b >= o && 0 < o + ext) || (lo + K < o + ext && K - 1 >= o);
-}
-
-// One CTA per brick: the charge of every site whose stencil reaches the
-// brick, summed in shared memory, written once as the float grid.  The
-// candidate sites (those binned in the bricks that can reach this one, a
-// host-made list) are staged SB_T records at a time with one load per
-// thread, keeping only those whose stencil does reach the brick (compacted
-// with ballots), each with its FP64 B-spline weights.  Then each half-warp
-// takes one kept site, a lane per (x, y) column of its 4 x 4 x 4 stencil
-// adding the column's 4 contributions: the lanes of a site touch distinct
-// points, and the two halves of a warp take sites half the list apart, so
-// the shared-memory adds rarely collide.  Each int64 contribution f (the
-// per-site path's value: q tx, times ty, times tz, in FP64, to fixed point)
-// is added as two native 32-bit atomics, f >> 18 and its low 18 bits, whose
-// sums give the int64 sum exactly (a grid point gets at most 8 x brick_cap
-// <= 4096 contributions of magnitude below 2^37: no int32 sum overflows).
+// Phase 1 of the spread: one CTA per brick, its own sites' whole stencils
+// into an 11^3 tile (the brick and the 3 grid points below it in each
+// dimension: a site with base b covers b-3 .. b, so every contribution
+// lands in its own brick's tile, with no bounds checks and no neighbour
+// reads).  A half-warp takes a site, a lane per (x, y) column of its
+// stencil adding the column's 4 contributions (the per-site path's values:
+// q tx, times ty, times tz, in FP64, to fixed point); the two halves of a
+// warp take sites half the list apart.  Each int64 contribution f is added
+// in shared memory as two native 32-bit atomics, f >> 18 and its low 18
+// bits, whose sums give the int64 sum exactly (a tile point gets at most
+// brick_cap <= 512 contributions of magnitude below 2^37); the tile is
+// written out as int64.
 constexpr int SPLIT = 18;
+constexpr int HB3 = HB * HB * HB;
 
 DYN_KERNEL(__launch_bounds__(SB_T), k_spread_brick, (, int pass), (, pass)) {
-    __shared__ int acc_hi[BR3], acc_lo[BR3];
-    __shared__ SiteRec recs[SB_T];
-    __shared__ double wts[SB_T][12];   // tx[4], ty[4], tz[4] of each kept site
-    __shared__ uint32_t nbr[MAX_NBR];
-    __shared__ uint32_t cnt[MAX_NBR + 1];
-    __shared__ uint32_t wcnt[SB_T / 32];
-    __shared__ int fold_s;
+    __shared__ int acc_hi[HB3], acc_lo[HB3];
+    __shared__ double wts[SB_T][12];   // tx[4], ty[4], tz[4] of each staged site
+    __shared__ int4 sloc[SB_T];        // tile position of each staged site's stencil, (base - o) per axis
+    __shared__ float sq[SB_T];
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     const int half = lane >> 4, a = (lane >> 2) & 3, bb = lane & 3;
-    const int K[3] = {(int)v.K[0], (int)v.K[1], (int)v.K[2]};
     for (uint32_t P = bk.idx; P < v.n_bricks; P += bk.cnt) {
         int o[3], ext[3];
         brick_origin(v, P, o, ext);
-        if (tid < 32) {
-            // the bricks whose sites can reach this one and their site
-            // counts, scanned across the warp
-            const uint32_t q = tid < MAX_NBR ? v.brick_nbr[(size_t)P * MAX_NBR + tid] : INVALID_ID;
-            uint32_t c = q != INVALID_ID ? min(v.brick_n[q], v.brick_cap) : 0u;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t x = __shfl_up_sync(0xffffffffu, c, d);
-                if (tid >= d) c += x;
-            }
-            if (tid < MAX_NBR) { nbr[tid] = q; cnt[tid + 1] = c; }
-            if (tid == 0) { cnt[0] = 0u; fold_s = v.brick_ovf[P] != 0u; }
-        }
-        for (int i = tid; i < BR3; i += SB_T) { acc_hi[i] = 0; acc_lo[i] = 0; }
-        __syncthreads();
-        const uint32_t total = cnt[MAX_NBR];
-        for (uint32_t u0 = 0; u0 < total; u0 += SB_T) {
-            // stage this round's records that reach the brick, with weights
-            const uint32_t u = u0 + tid;
-            bool keep = false;
-            SiteRec r;
-            if (u < total) {
-                int j = 0;
-                while (u >= cnt[j + 1]) ++j;
-                r = v.brick_site[(size_t)nbr[j] * v.brick_cap + (u - cnt[j])];
+        for (int i = tid; i < HB3; i += SB_T) { acc_hi[i] = 0; acc_lo[i] = 0; }
+        const uint32_t n = min(v.brick_n[P], v.brick_cap);
+        for (uint32_t u0 = 0; u0 < n; u0 += SB_T) {
+            if (u0 + tid < n) {
+                const SiteRec r = v.brick_site[(size_t)P * v.brick_cap + u0 + tid];
                 int base[3];
                 rec_base(r.base, base);
-                keep = stencil_reaches(base[0], o[0], ext[0], K[0]) && stencil_reaches(base[1], o[1], ext[1], K[1]) &&
-                       stencil_reaches(base[2], o[2], ext[2], K[2]);
+                sloc[tid] = make_int4(base[0] - o[0], base[1] - o[1], base[2] - o[2], 0);
+                sq[tid] = r.q;
+                bspline4d(r.w[0], &wts[tid][0]);
+                bspline4d(r.w[1], &wts[tid][4]);
+                bspline4d(r.w[2], &wts[tid][8]);
             }
-            const uint32_t m = __ballot_sync(0xffffffffu, keep);
-            if (lane == 0) wcnt[wp] = __popc(m);
-            __syncthreads();
-            uint32_t off = 0, nk = 0;
-            for (int w = 0; w < SB_T / 32; ++w) {
-                off += w < wp ? wcnt[w] : 0u;
-                nk += wcnt[w];
-            }
-            if (keep) {
-                const uint32_t k = off + __popc(m & ((1u << lane) - 1u));
-                recs[k] = r;
-                bspline4d(r.w[0], &wts[k][0]);
-                bspline4d(r.w[1], &wts[k][4]);
-                bspline4d(r.w[2], &wts[k][8]);
-            }
-            __syncthreads();
-            // half-warp h of warp w: sites w + 8 i (first half) and the same
-            // half the list further on (second half)
-            const uint32_t hn = (nk + 1) / 2;
+            __syncthreads();  // the staged sites (and, first, the zeroed tile)
+            const uint32_t m = min((uint32_t)SB_T, n - u0), hn = (m + 1) / 2;
             for (uint32_t k0 = (uint32_t)wp; k0 < hn; k0 += SB_T / 32) {
                 const uint32_t k = k0 + (half ? hn : 0u);
-                if (k >= nk) continue;
-                int base[3];
-                rec_base(recs[k].base, base);
-                int x = base[0] - 3 + a, y = base[1] - 3 + bb;
-                if (x < 0) x += K[0];
-                if (y < 0) y += K[1];
-                const int lx = x - o[0], ly = y - o[1];
-                if (lx < 0 || lx >= ext[0] || ly < 0 || ly >= ext[1]) continue;
-                const double qab = ((double)recs[k].q * wts[k][a]) * wts[k][4 + bb];
-                const int row = (lx * PME_BRICK + ly) * PME_BRICK;
+                if (k >= m) continue;
+                const int4 lb = sloc[k];
+                const double qab = ((double)sq[k] * wts[k][a]) * wts[k][4 + bb];
+                const int row = ((lb.x + a) * HB + (lb.y + bb)) * HB + lb.z;
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
-                    int z = base[2] - 3 + c;
-                    if (z < 0) z += K[2];
-                    const int lz = z - o[2];
-                    if (lz < 0 || lz >= ext[2]) continue;
                     const long long f = fix_from_double(qab * wts[k][8 + c]);
-                    atomicAdd(&acc_hi[row + lz], (int)(f >> SPLIT));
-                    atomicAdd(&acc_lo[row + lz], (int)(f & ((1ll << SPLIT) - 1)));
+                    atomicAdd(&acc_hi[row + c], (int)(f >> SPLIT));
+                    atomicAdd(&acc_lo[row + c], (int)(f & ((1ll << SPLIT) - 1)));
                 }
             }
-            __syncthreads();  // recs, wts and wcnt are refilled by the next round
+            __syncthreads();  // the staged sites are refilled by the next round
         }
-        const bool fold = fold_s != 0;
-        for (int i = tid; i < BR3; i += SB_T) {
-            const int lx = i / (PME_BRICK * PME_BRICK), ly = (i / PME_BRICK) % PME_BRICK, lz = i % PME_BRICK;
-            if (lx < ext[0] && ly < ext[1] && lz < ext[2]) {
-                const size_t gi = ((size_t)(o[0] + lx) * K[1] + (o[1] + ly)) * K[2] + (o[2] + lz);
-                long long q = (long long)acc_hi[i] * (1ll << SPLIT) + (long long)acc_lo[i];
-                if (fold) {
-                    // overflow sites' charge from the global fixed-point grid
-                    q += v.qgrid_fix[gi];
-                    v.qgrid_fix[gi] = 0;
-                }
-                v.qgrid[gi] = (float)((double)q * DYN_FIX_INV);
+        long long* tile = v.brick_tile + (size_t)P * HB3;
+        for (int i = tid; i < HB3; i += SB_T) tile[i] = (long long)acc_hi[i] * (1ll << SPLIT) + (long long)acc_lo[i];
+        __syncthreads();  // the tile is zeroed for the next brick
+    }
+}
+
+// The (brick, tile offset) pairs whose tiles hold grid coordinate x of one
+// axis: its own brick and the 1 or 2 bricks that start at most 3 points on
+// (tile offset t of brick b is point o_b - 3 + t, periodic); with K < 11 a
+// tile can hold a point twice.  Six fixed slots, (brick b0 + k, offset
+// d + r K) for k < 3, r < 2; d[] = HB marks an empty slot.  Static indices
+// only, so the slots stay in registers.
+__device__ __forceinline__ void tile_holders(int x, int K, uint32_t nb, int (&hb)[6], int (&hd)[6]) {
+    const int b0 = x / PME_BRICK;
+    int bs[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) bs[k] = (int)(((uint32_t)b0 + (uint32_t)k) % nb);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const bool dup = (k >= 1 && bs[k] == bs[0]) || (k == 2 && bs[2] == bs[1]);
+        const int d = ((x - bs[k] * PME_BRICK + 3) % K + K) % K;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            hb[2 * k + r] = bs[k];
+            hd[2 * k + r] = (!dup && d + r * K < HB) ? d + r * K : HB;
+        }
+    }
+}
+
+// Phase 2: one thread per grid point, the sum of the tile entries that hold
+// it (plus the overflow sites' charge where its brick is flagged), as float.
+DYN_KERNEL(, k_spread_merge, (, int pass), (, pass)) {
+    const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
+    const uint32_t npts = (uint32_t)K0 * K1 * K2;
+    for (uint32_t p = bk.idx * blockDim.x + threadIdx.x; p < npts; p += bk.cnt * blockDim.x) {
+        const int z = (int)(p % (uint32_t)K2), y = (int)((p / (uint32_t)K2) % (uint32_t)K1),
+                  x = (int)(p / ((uint32_t)K1 * K2));
+        int bx[6], dx[6], by[6], dy[6], bz[6], dz[6];
+        tile_holders(x, K0, v.nbrick[0], bx, dx);
+        tile_holders(y, K1, v.nbrick[1], by, dy);
+        tile_holders(z, K2, v.nbrick[2], bz, dz);
+        long long sum = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            if (dx[i] >= HB) continue;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                if (dy[j] >= HB) continue;
+                const size_t bxy = ((size_t)bx[i] * v.nbrick[1] + by[j]) * v.nbrick[2];
+                const int dxy = (dx[i] * HB + dy[j]) * HB;
+#pragma unroll
+                for (int k = 0; k < 6; ++k)
+                    if (dz[k] < HB) sum += v.brick_tile[(bxy + bz[k]) * HB3 + dxy + dz[k]];
             }
         }
-        if (tid == 0 && fold) v.brick_ovf[P] = 0u;
-        __syncthreads();  // the sums and the brick list are refilled by the next brick
+        if (v.brick_ovf[brick_index(v, x, y, z)]) {
+            // overflow sites' charge from the global fixed-point grid
+            sum += v.qgrid_fix[p];
+            v.qgrid_fix[p] = 0;
+        }
+        v.qgrid[p] = (float)((double)sum * DYN_FIX_INV);
     }
 }
 
@@ -539,7 +526,7 @@ DYN_KERNEL(__launch_bounds__(GB_T), k_gather_brick, (, int pass), (, pass)) {
             gather_out(v, t == (uint32_t)tid ? sid0 : v.brick_sid[e], f, pass);
         }
         __syncthreads();  // every thread has read the count; the tile is refilled next
-        if (tid == 0) v.brick_n[P] = 0u;
+        if (tid == 0) { v.brick_n[P] = 0u; v.brick_ovf[P] = 0u; }
     }
 }
 
@@ -736,27 +723,6 @@ void pme_bricks(SysView& v, uint32_t cap) {
     v.brick_cap = std::min(512u, cap ? cap : (2u * mean + 32u + 31u) / 32u * 32u);
 }
 
-// Per brick, the distinct bricks holding the stencil bases that reach it:
-// in each dimension those of grid points o .. o + ext + 2 (a base b covers
-// b - 3 .. b); MAX_NBR entries per brick, INVALID_ID after the last.
-void pme_brick_sources(const SysView& v, std::vector<uint32_t>& out) {
-    out.assign((size_t)v.n_bricks * MAX_NBR, INVALID_ID);
-    for (uint32_t P = 0; P < v.n_bricks; ++P) {
-        const uint32_t p[3] = {P / (v.nbrick[1] * v.nbrick[2]), (P / v.nbrick[2]) % v.nbrick[1], P % v.nbrick[2]};
-        std::vector<uint32_t> lst[3];
-        for (int a = 0; a < 3; ++a) {
-            const uint32_t o = p[a] * PME_BRICK, ext = std::min<uint32_t>(PME_BRICK, v.K[a] - o);
-            for (uint32_t d = 0; d <= ext + 2; ++d) {
-                const uint32_t q = ((o + d) % v.K[a]) / PME_BRICK;
-                if (std::find(lst[a].begin(), lst[a].end(), q) == lst[a].end()) lst[a].push_back(q);
-            }
-        }
-        size_t n = 0;
-        for (uint32_t i : lst[0])
-            for (uint32_t j : lst[1])
-                for (uint32_t k : lst[2]) out[(size_t)P * MAX_NBR + n++] = (i * v.nbrick[1] + j) * v.nbrick[2] + k;
-    }
-}
 int corr_blocks(const SysView& v) { return gblocks(v, (uint64_t)v.n14 + v.nexcl); }
 
 int pme_init(SysView& v, cufftHandle* plan_f, cufftHandle* plan_b, cudaStream_t st) {
@@ -831,6 +797,9 @@ void launch_pme_spread(const Target& t, int pass) {
              [&](const SysView& v) { return on(v) ? gblocks(v, 3ull * v.nw_cap + v.na) : 0; }, GT, 0, pass);
     t.launch(k_spread_brick, k_spread_brick_batch,
              [&](const SysView& v) { return on(v) ? (int)std::min(v.n_bricks, v.max_blocks) : 0; }, SB_T, 0, pass);
+    t.launch(k_spread_merge, k_spread_merge_batch,
+             [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]) : 0; }, GT, 0,
+             pass);
 }
 
 void launch_pme_transform(const Target& t, int pass) {

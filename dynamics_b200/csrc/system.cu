@@ -826,13 +826,7 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
     dyn::pme_bricks(v, cfg->spme_brick_cap);
     TRY(dev_alloc(h, &v.brick_n, v.n_bricks));
     TRY(dev_alloc(h, &v.brick_ovf, v.n_bricks));
-    {
-        std::vector<uint32_t> src;
-        dyn::pme_brick_sources(v, src);
-        TRY(dev_alloc(h, &v.brick_nbr, src.size(), false));
-        TRY(upload(h, v.brick_nbr, src.data(), src.size()));
-        TRYC(cudaStreamSynchronize(h->stream));  // src is freed at the end of this block
-    }
+    TRY(dev_alloc(h, &v.brick_tile, (size_t)v.n_bricks * 1331, false));  // 11^3 points per brick
     TRY(dev_alloc(h, &v.brick_site, (size_t)v.n_bricks * v.brick_cap, false));
     TRY(dev_alloc(h, &v.brick_sid, (size_t)v.n_bricks * v.brick_cap, false));
     TRY(dev_alloc(h, &v.ovf_site, v.n_sites_max, false));
