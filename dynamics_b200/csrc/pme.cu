@@ -317,14 +317,55 @@ __device__ __forceinline__ void tile_holders(int x, int K, uint32_t nb, int (&hb
     }
 }
 
+// The common case of tile_holders (every axis with K >= 11 and K mod 8 not
+// 1 or 2, so no brick is narrower than 3 points and no tile wraps onto
+// itself): the own brick (offset in [3, 11)) and the next brick, whose
+// halo holds x when its offset d1 = x - (next origin) + 3 is >= 0.
+__device__ __forceinline__ void tile_holders2(int x, int K, uint32_t nb, int& b0, int& d0, int& b1, int& d1) {
+    b0 = x / PME_BRICK;
+    d0 = x - b0 * PME_BRICK + 3;
+    const bool last = b0 + 1 == (int)nb;
+    b1 = last ? 0 : b0 + 1;
+    d1 = x - (last ? K : (b0 + 1) * PME_BRICK) + 3;
+}
+
+__device__ __forceinline__ bool axis_simple(int K) { return K >= HB && (K % PME_BRICK == 0 || K % PME_BRICK >= 3); }
+
 // Phase 2: one thread per grid point, the sum of the tile entries that hold
 // it (plus the overflow sites' charge where its brick is flagged), as float.
 DYN_KERNEL(, k_spread_merge, (, int pass), (, pass)) {
     const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
     const uint32_t npts = (uint32_t)K0 * K1 * K2;
+    const bool simple = axis_simple(K0) && axis_simple(K1) && axis_simple(K2);
     for (uint32_t p = bk.idx * blockDim.x + threadIdx.x; p < npts; p += bk.cnt * blockDim.x) {
         const int z = (int)(p % (uint32_t)K2), y = (int)((p / (uint32_t)K2) % (uint32_t)K1),
                   x = (int)(p / ((uint32_t)K1 * K2));
+        if (simple) {
+            int bx[2], dx[2], by[2], dy[2], bz[2], dz[2];
+            tile_holders2(x, K0, v.nbrick[0], bx[0], dx[0], bx[1], dx[1]);
+            tile_holders2(y, K1, v.nbrick[1], by[0], dy[0], by[1], dy[1]);
+            tile_holders2(z, K2, v.nbrick[2], bz[0], dz[0], bz[1], dz[1]);
+            long long sum = 0;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                if (dx[i] < 0) continue;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    if (dy[j] < 0) continue;
+                    const size_t bxy = ((size_t)bx[i] * v.nbrick[1] + by[j]) * v.nbrick[2];
+                    const int dxy = (dx[i] * HB + dy[j]) * HB;
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+                        if (dz[k] >= 0) sum += v.brick_tile[(bxy + bz[k]) * HB3 + dxy + dz[k]];
+                }
+            }
+            if (v.brick_ovf[brick_index(v, x, y, z)]) {
+                sum += v.qgrid_fix[p];
+                v.qgrid_fix[p] = 0;
+            }
+            v.qgrid[p] = (float)((double)sum * DYN_FIX_INV);
+            continue;
+        }
         int bx[6], dx[6], by[6], dy[6], bz[6], dz[6];
         tile_holders(x, K0, v.nbrick[0], bx, dx);
         tile_holders(y, K1, v.nbrick[1], by, dy);
