@@ -331,8 +331,57 @@ __device__ __forceinline__ void tile_holders2(int x, int K, uint32_t nb, int& b0
 
 __device__ __forceinline__ bool axis_simple(int K) { return K >= HB && (K % PME_BRICK == 0 || K % PME_BRICK >= 3); }
 
-// Phase 2: one thread per grid point, the sum of the tile entries that hold
-// it (plus the overflow sites' charge where its brick is flagged), as float.
+// Phase 2 for grids where every axis is simple: one CTA per brick, a thread
+// per point; a point at local coordinate l of an axis is held by its own
+// tile (offset l + 3) and, in the top 3 layers (l >= ext - 3), by the next
+// brick's tile (offset l - ext + 3), exactly the entries phase 1 writes.
+DYN_KERNEL(__launch_bounds__(SB_T), k_spread_merge_brick, (, int pass), (, pass)) {
+    const int K[3] = {(int)v.K[0], (int)v.K[1], (int)v.K[2]};
+    for (uint32_t P = bk.idx; P < v.n_bricks; P += bk.cnt) {
+        int o[3], ext[3];
+        brick_origin(v, P, o, ext);
+        int bi[3][2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int pb = o[a] / PME_BRICK;
+            bi[a][0] = pb;
+            bi[a][1] = pb + 1 == (int)v.nbrick[a] ? 0 : pb + 1;
+        }
+        const bool fold = v.brick_ovf[P] != 0u;
+        for (int i = threadIdx.x; i < BR3; i += SB_T) {
+            const int l[3] = {i / (PME_BRICK * PME_BRICK), (i / PME_BRICK) % PME_BRICK, i % PME_BRICK};
+            if (l[0] >= ext[0] || l[1] >= ext[1] || l[2] >= ext[2]) continue;
+            int d[3][2];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) { d[a][0] = l[a] + 3; d[a][1] = l[a] - ext[a] + 3; }
+            long long sum = 0;
+#pragma unroll
+            for (int x = 0; x < 2; ++x) {
+                if (d[0][x] < 0) continue;
+#pragma unroll
+                for (int y = 0; y < 2; ++y) {
+                    if (d[1][y] < 0) continue;
+                    const size_t bxy = ((size_t)bi[0][x] * v.nbrick[1] + bi[1][y]) * v.nbrick[2];
+                    const int dxy = (d[0][x] * HB + d[1][y]) * HB;
+#pragma unroll
+                    for (int z = 0; z < 2; ++z)
+                        if (d[2][z] >= 0) sum += v.brick_tile[(bxy + bi[2][z]) * HB3 + dxy + d[2][z]];
+                }
+            }
+            const size_t gi = ((size_t)(o[0] + l[0]) * K[1] + (o[1] + l[1])) * K[2] + (o[2] + l[2]);
+            if (fold) {
+                // overflow sites' charge from the global fixed-point grid
+                sum += v.qgrid_fix[gi];
+                v.qgrid_fix[gi] = 0;
+            }
+            v.qgrid[gi] = (float)((double)sum * DYN_FIX_INV);
+        }
+    }
+}
+
+// Phase 2 for any grid: one thread per grid point, the sum of the tile
+// entries that hold it (plus the overflow sites' charge where its brick is
+// flagged), as float.
 DYN_KERNEL(, k_spread_merge, (, int pass), (, pass)) {
     const int K0 = v.K[0], K1 = v.K[1], K2 = v.K[2];
     const uint32_t npts = (uint32_t)K0 * K1 * K2;
@@ -838,9 +887,19 @@ void launch_pme_spread(const Target& t, int pass) {
              [&](const SysView& v) { return on(v) ? gblocks(v, 3ull * v.nw_cap + v.na) : 0; }, GT, 0, pass);
     t.launch(k_spread_brick, k_spread_brick_batch,
              [&](const SysView& v) { return on(v) ? (int)std::min(v.n_bricks, v.max_blocks) : 0; }, SB_T, 0, pass);
+    // phase 2: per brick where every axis is simple, per point otherwise
+    auto simple = [](const SysView& v) {
+        auto ax = [](uint32_t K) { return K >= (uint32_t)HB && (K % PME_BRICK == 0 || K % PME_BRICK >= 3); };
+        return ax(v.K[0]) && ax(v.K[1]) && ax(v.K[2]);
+    };
+    t.launch(k_spread_merge_brick, k_spread_merge_brick_batch,
+             [&](const SysView& v) { return on(v) && simple(v) ? (int)std::min(v.n_bricks, v.max_blocks) : 0; },
+             SB_T, 0, pass);
     t.launch(k_spread_merge, k_spread_merge_batch,
-             [&](const SysView& v) { return on(v) ? gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]) : 0; }, GT, 0,
-             pass);
+             [&](const SysView& v) {
+                 return on(v) && !simple(v) ? gblocks(v, (uint64_t)v.K[0] * v.K[1] * v.K[2]) : 0;
+             },
+             GT, 0, pass);
 }
 
 void launch_pme_transform(const Target& t, int pass) {

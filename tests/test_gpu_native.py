@@ -23,8 +23,8 @@ PE_RTOL = 1e-6
 
 
 def _cfg(sysd, mode="reference", integ=None, **kw):
-    grid = tuple(int(2 ** np.ceil(np.log2(x))) if x <= 32 else int(np.ceil(x / 8) * 8)
-                 for x in (sysd["box_hi"] - sysd["box_lo"]))
+    grid = kw.pop("spme_grid", None) or tuple(int(2 ** np.ceil(np.log2(x))) if x <= 32 else int(np.ceil(x / 8) * 8)
+                                             for x in (sysd["box_hi"] - sysd["box_lo"]))
     c = md.MdConfig(coulomb_cutoff=8.0, lj_cutoff=8.0, spme_alpha=synth.ewald_alpha(8.0),
                     spme_grid=grid, ewald_corrections=(mode == "corrected"),
                     full_energy=(mode == "corrected"), **kw)
@@ -240,17 +240,21 @@ def test_union_chunking(gpu_lib):
         st.close()
 
 
+@pytest.mark.parametrize("grid", [None, (25, 27, 33)])
 @pytest.mark.parametrize("mode", ["reference", "corrected"])
 @pytest.mark.parametrize("make", [water_only, mixed])
-def test_spme_bricks_bit_identical_to_per_site(gpu_lib, make, mode):
+def test_spme_bricks_bit_identical_to_per_site(gpu_lib, make, mode, grid):
     """SPME spreads and gathers by grid brick in shared memory; with a brick
     capacity of 1 nearly every charged site takes the overflow path (global
     fixed-point atomics, per-site gather from the global grid, the per-site
     arithmetic).  Forces, the reciprocal energy and the trajectory must be
-    the same bits either way."""
+    the same bits either way.  Grid 25 x 27 x 33 has axes whose last brick
+    is narrower than 3 points, where the spread's second phase takes its
+    per-point form."""
     sysd = make()
-    a = md.MdState(sysd, _cfg(sysd, mode))
-    b = md.MdState(sysd, _cfg(sysd, mode, spme_brick_cap=1))
+    kw = {"spme_grid": grid} if grid else {}
+    a = md.MdState(sysd, _cfg(sysd, mode, **kw))
+    b = md.MdState(sysd, _cfg(sysd, mode, spme_brick_cap=1, **kw))
     fa, fb = a.forces(), b.forces()
     np.testing.assert_array_equal(fa["f_water"], fb["f_water"])
     np.testing.assert_array_equal(fa["f_atoms"], fb["f_atoms"])
