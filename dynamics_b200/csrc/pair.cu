@@ -156,12 +156,10 @@ __device__ __forceinline__ void write_partials(const SysView& v, Blk bk, int reg
 }
 
 // ---------------------------------------------------------------------------
-// water(i) - water(j), tile form.  One CTA per 32-water i-group.  The waters
-// the group needs (its union, stored as runs of consecutive slots) are copied
-// global -> shared with one cp.async.bulk per run, completing on an mbarrier,
-// union_chunk waters at a time (one chunk for almost every group; the chunk
-// is sized so that two CTAs fit on an SM).  Each i-water is handled by LPW
-// lanes walking its list of union indices; j sites come from shared memory
+// Staging for the water-water kernel (k_pair_ww_tile, below): a group's
+// union of j-waters, stored as runs of consecutive slots, is copied global
+// -> shared with one cp.async.bulk per run, completing on an mbarrier, with
+// bounded waits; the kernel then reads the j sites from shared memory
 // (4 x 16-byte loads per molecule pair).
 // ---------------------------------------------------------------------------
 constexpr int WT = GRPW * LPW;  // threads per CTA
@@ -297,8 +295,8 @@ __device__ __forceinline__ void write_partials_warp(const SysView& v, Blk bk, in
 // i-group.  The waters the group's lists reach (its union, stored as runs
 // of consecutive slots) are copied global -> shared with one cp.async.bulk
 // per run, completing on an mbarrier, union_chunk waters at a time (one
-// chunk for almost every group; sized so that two CTAs fit on an SM).  The
-// lists hold every water pair once (in the list of the lower slot), so
+// chunk for most groups; sized so that three CTAs fit on an SM, with 80
+// registers per thread).  The lists hold every water pair once (in the list of the lower slot), so
 // their lengths vary several-fold across a group; the chunk's entries of
 // all 32 lists are therefore dealt out as one sequence, an equal
 // contiguous share per thread, whatever list they come from.  A thread
@@ -318,7 +316,7 @@ __device__ __forceinline__ void write_partials_warp(const SysView& v, Blk bk, in
 // A system with fewer groups than the GPU has SMs gives each group ww_split
 // CTAs, each staging the union and taking an equal slice of the entries.
 // ---------------------------------------------------------------------------
-DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 2), k_pair_ww_tile, (), ()) {
+DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 3), k_pair_ww_tile, (), ()) {
     extern __shared__ __align__(128) float4 tile[];  // union_chunk waters x 4 float4, then the j sums
     __shared__ __align__(8) uint64_t bar;
     __shared__ float4 ipos[GRPW * 4];   // the group's i-water sites

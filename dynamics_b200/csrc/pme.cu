@@ -160,12 +160,25 @@ __device__ void spread_global(const SysView& v, const SiteRec& r) {
             for (int c = 0; c < 4; ++c) fix_atomic_add(row + iz[c], fix_from_double(qab * tz[c]));
         }
     }
-    // per dimension the stencil spans the bricks of base - 3 (wrapped) and base
-    int lo[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) { lo[a] = base[a] - 3; if (lo[a] < 0) lo[a] += (int)v.K[a]; }
-    for (int m = 0; m < 8; ++m)
-        v.brick_ovf[brick_index(v, (m & 1) ? base[0] : lo[0], (m & 2) ? base[1] : lo[1], (m & 4) ? base[2] : lo[2])] = 1u;
+    // flag every brick that holds a stencil point: per axis the distinct
+    // bricks of the 4 points (3 where the last brick is 1 or 2 points wide)
+    int bl[3][4], nbl[3];
+    for (int a = 0; a < 3; ++a) {
+        nbl[a] = 0;
+        for (int c = 0; c < 4; ++c) {
+            int x = base[a] - 3 + c;
+            if (x < 0) x += (int)v.K[a];
+            const int q = x / PME_BRICK;
+            bool seen = false;
+            for (int t = 0; t < nbl[a]; ++t) seen = seen || bl[a][t] == q;
+            if (!seen) bl[a][nbl[a]++] = q;
+        }
+    }
+    for (int i = 0; i < nbl[0]; ++i)
+        for (int j = 0; j < nbl[1]; ++j)
+            for (int k = 0; k < nbl[2]; ++k)
+                v.brick_ovf[((uint32_t)bl[0][i] * v.nbrick[1] + (uint32_t)bl[1][j]) * v.nbrick[2] + (uint32_t)bl[2][k]] =
+                    1u;
 }
 
 // Bins the pass's charged sites by brick (records and site codes).  Atoms

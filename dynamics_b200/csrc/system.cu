@@ -546,13 +546,13 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         // several chunks, so this is only the list-build capacity
         v.cap_union = std::min<uint32_t>((uint32_t)(2.8 * mink(ag) * dl) + 64, 65534u);
         v.cap_union = std::min<uint32_t>(v.cap_union, v.nw_cap);
-        // shared-memory chunk of the water-water kernel: two CTAs per SM
+        // shared-memory chunk of the water-water kernel: three CTAs per SM
         // (each CTA also needs 1 KB reserved plus < 5 KB static shared)
         int dev = 0, smem_sm = 0, smem_blk = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
         cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        size_t per_cta = smem_sm > 12288 ? (size_t)smem_sm / 2 - 6144 : 48 * 1024;
+        size_t per_cta = smem_sm > 18432 ? (size_t)smem_sm / 3 - 6144 : 48 * 1024;
         per_cta = std::min<size_t>(per_cta, smem_blk > 0 ? (size_t)smem_blk : per_cta);
         // per staged water: its 4 site positions, its 12 int32 j sums and its slot
         const uint32_t fit = (uint32_t)((per_cta - 12 * sizeof(int)) / (4 * sizeof(float4) + 13 * sizeof(int))) / 32 * 32;

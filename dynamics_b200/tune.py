@@ -9,7 +9,7 @@ measurement, per size class of system, and cached:
 * ``prune_buffer``: the inner buffer of the pruned water-water lists
   (shorter lists against more prunes);
 * ``ww_union_chunk``: the water-water kernel's shared-memory chunk (waters
-  staged at a time; two CTAs per SM at the largest);
+  staged at a time; three CTAs per SM at the largest);
 * ``pair_item_entries``: list entries per work item of the water-atom and
   atom-atom pair kernels (more items balance better, fewer amortise the
   per-item loads);
@@ -53,7 +53,7 @@ from . import md, synth
 KNOBS = ("neighbor_skin", "prune_buffer", "ww_union_chunk", "ww_split", "pair_item_entries", "spme_grid_step")
 SKINS = (1.0, 1.25, 1.5, 1.75, 2.0)
 PRUNES = (0.2, 0.3, 0.4, 0.6, 0.8)
-CHUNKS = (0, 256, 512)          # 0: the largest that lets two CTAs share an SM
+CHUNKS = (0, 256, 512)          # 0: the largest that lets three CTAs share an SM
 ITEMS = (4, 8, 16, 32)
 SPLITS = (0, 1, 2, 4)           # 0: automatic
 GRID_SPAN = 1.15                # grid candidates up to 15 % above the finest needed

@@ -291,7 +291,7 @@ typedef struct {
     uint64_t seed;          /* Philox key for all stochastic terms          */
     uint32_t ww_union_chunk;/* waters per shared-memory chunk of the
                              * water-water kernel; 0 = the largest that lets
-                             * two CTAs share an SM (a tuning knob: it changes
+                             * three CTAs share an SM (a tuning knob: it changes
                              * how float sums are grouped, so results only
                              * at rounding level)                           */
     uint32_t lincs_order;   /* bond-to-H constraints: projection passes of
