@@ -290,9 +290,7 @@ extern "C" int dyn_batch_create(void* stream, uint32_t n, const dyn_config_t* cf
     for (uint32_t i = 0; i < n; ++i) {
         dyn_sys_t m = nullptr;
         const int rc = dyn_sys_create(b->stream, &cfgs[i], &systems[i], &m);
-        if (rc == DYN_OK) m->batch_member = true;
-        // the batch fills the GPU: no automatic group split
-        if (rc == DYN_OK && cfgs[i].ww_split == 0) dyn::set_ww_split(m, 1);
+        if (rc == DYN_OK) dyn::set_batch_member(m);
         if (rc != DYN_OK) {
             const std::string msg = "dyn_batch_create: member " + std::to_string(i) + ": " + dyn_last_error();
             dyn_batch_destroy(b);
@@ -417,8 +415,7 @@ extern "C" int dyn_batch_add(dyn_batch_t b, const dyn_config_t* cfg, const dyn_s
     DYN_CUDA(cudaStreamSynchronize(b->stream));
     dyn_sys_t m = nullptr;
     const int rc = dyn_sys_create(b->stream, cfg, system, &m);
-    if (rc == DYN_OK) m->batch_member = true;
-    if (rc == DYN_OK && cfg->ww_split == 0) dyn::set_ww_split(m, 1);  // the batch fills the GPU
+    if (rc == DYN_OK) dyn::set_batch_member(m);
     if (rc != DYN_OK) return rc;
     if (!b->fixed_intervals) {
         b->spme_interval = std::max(1u, cfg->spme_interval);

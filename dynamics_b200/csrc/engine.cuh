@@ -289,7 +289,11 @@ __device__ __forceinline__ void pdl_enter() {
     }                                                                                                \
     __device__ __forceinline__ void NAME##_B::run(const SysView& v, Blk bk DYN_UNPAREN PARAMS)
 
-#define DYN_KERNEL_T(TDECL, TARGS, LB, NAME, PARAMS, ARGS)                                          \
+// DYN_KERNEL for a template (TDECL its parameters, TARGS their names), with
+// launch bounds LBB of their own for NAME##_batch, which reads its SysView
+// from global memory and so holds more registers; DYN_KERNEL_T gives both
+// forms the same bounds.
+#define DYN_KERNEL_T2(TDECL, TARGS, LB, LBB, NAME, PARAMS, ARGS)                                    \
     template <DYN_UNPAREN TDECL>                                                                     \
     struct NAME##_B {                                                                                \
         static __device__ __forceinline__ void run(const SysView& v, Blk bk DYN_UNPAREN PARAMS);     \
@@ -300,8 +304,8 @@ __device__ __forceinline__ void pdl_enter() {
         NAME##_B<DYN_UNPAREN TARGS>::run(v, Blk{blockIdx.x, gridDim.x} DYN_UNPAREN ARGS);            \
     }                                                                                                \
     template <DYN_UNPAREN TDECL>                                                                     \
-    __global__ void LB NAME##_batch(const SysView* __restrict__ vs,                                  \
-                                    const uint2* __restrict__ bm DYN_UNPAREN PARAMS) {               \
+    __global__ void LBB NAME##_batch(const SysView* __restrict__ vs,                                 \
+                                     const uint2* __restrict__ bm DYN_UNPAREN PARAMS) {              \
         pdl_enter();                                                                                 \
         const uint2 m = bm[blockIdx.x];                                                              \
         NAME##_B<DYN_UNPAREN TARGS>::run(vs[m.x], Blk{m.y & 0xFFFFu, m.y >> 16} DYN_UNPAREN ARGS);   \
@@ -309,6 +313,8 @@ __device__ __forceinline__ void pdl_enter() {
     template <DYN_UNPAREN TDECL>                                                                     \
     __device__ __forceinline__ void NAME##_B<DYN_UNPAREN TARGS>::run(const SysView& v,               \
                                                                      Blk bk DYN_UNPAREN PARAMS)
+
+#define DYN_KERNEL_T(TDECL, TARGS, LB, NAME, PARAMS, ARGS) DYN_KERNEL_T2(TDECL, TARGS, LB, LB, NAME, PARAMS, ARGS)
 
 // ---------------------------------------------------------------------------
 // Launch target: one system, or every system of a batch.  The launch code

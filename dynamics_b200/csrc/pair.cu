@@ -296,7 +296,9 @@ __device__ __forceinline__ void write_partials_warp(const SysView& v, Blk bk, in
 // of consecutive slots) are copied global -> shared with one cp.async.bulk
 // per run, completing on an mbarrier, union_chunk waters at a time (one
 // chunk for most groups; sized so that three CTAs fit on an SM, with 80
-// registers per thread).  The lists hold every water pair once (in the list of the lower slot), so
+// registers per thread; the batch form, which reads its SysView from global
+// memory, spills at 80 and runs two CTAs per SM instead).  The lists hold
+// every water pair once (in the list of the lower slot), so
 // their lengths vary several-fold across a group; the chunk's entries of
 // all 32 lists are therefore dealt out as one sequence, an equal
 // contiguous share per thread, whatever list they come from.  A thread
@@ -316,7 +318,7 @@ __device__ __forceinline__ void write_partials_warp(const SysView& v, Blk bk, in
 // A system with fewer groups than the GPU has SMs gives each group ww_split
 // CTAs, each staging the union and taking an equal slice of the entries.
 // ---------------------------------------------------------------------------
-DYN_KERNEL_T((bool ENERGY), (ENERGY), __launch_bounds__(WT, 3), k_pair_ww_tile, (), ()) {
+DYN_KERNEL_T2((bool ENERGY), (ENERGY), __launch_bounds__(WT, 3), __launch_bounds__(WT, 2), k_pair_ww_tile, (), ()) {
     extern __shared__ __align__(128) float4 tile[];  // union_chunk waters x 4 float4, then the j sums
     __shared__ __align__(8) uint64_t bar;
     __shared__ float4 ipos[GRPW * 4];   // the group's i-water sites

@@ -103,6 +103,12 @@ int check_scalars(dyn_sys_s* h);
 void energies_of(dyn_sys_s* h, dyn_energies_t* e);
 // The water-water kernel's CTAs per group (before any step graph exists).
 void set_ww_split(dyn_sys_s* h, uint32_t split);
+// Marks h as a batch member (before any step graph exists): no automatic
+// water-water group split.  The chunk stays the one sized for three CTAs per
+// SM although the kernel's batch form runs two (a chunk sized for two was
+// slower on the batched workloads), so a member computes exactly what it
+// computes alone.
+void set_batch_member(dyn_sys_s* h);
 
 // Inside an active capture on st: appends an IF node on hc after everything
 // captured so far and starts capturing its body on aux.

@@ -78,6 +78,25 @@ void host_m_site(const float* o, const float* h0, const float* h1, float* m) {
     for (int k = 0; k < 3; ++k) m[k] = (float)(o[k] + b[k] / n * (double)OPC_O_EP_R);
 }
 
+// Waters per shared-memory chunk of the water-water kernel with ctas CTAs
+// per SM (each CTA also needs 1 KB reserved plus < 5 KB static shared):
+// per staged water its 4 site positions, its 12 int32 j sums and its slot,
+// no more than the union capacity, and no more than cfg->ww_union_chunk
+// when that is set.
+uint32_t ww_chunk_for(const SysView& v, const dyn_config_t* cfg, int ctas) {
+    int dev = 0, smem_sm = 0, smem_blk = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    size_t per_cta = smem_sm > 6144 * ctas ? (size_t)smem_sm / ctas - 6144 : 48 * 1024;
+    per_cta = std::min<size_t>(per_cta, smem_blk > 0 ? (size_t)smem_blk : per_cta);
+    const uint32_t fit =
+        (uint32_t)((per_cta - 12 * sizeof(int)) / (4 * sizeof(float4) + 13 * sizeof(int))) / 32 * 32;
+    uint32_t chunk = std::max<uint32_t>(32u, std::min<uint32_t>(fit, (v.cap_union + 31) / 32 * 32));
+    if (cfg->ww_union_chunk) chunk = std::max<uint32_t>(32u, std::min<uint32_t>(chunk, cfg->ww_union_chunk / 32 * 32));
+    return chunk;
+}
+
 void set_block_counts(SysView& v) {
     for (int r = 0; r < NREGION; ++r) v.nb[r] = 0;
     v.nb[REG_WW] = v.nw ? dyn::ww_tile_blocks(v) : 0;
@@ -547,21 +566,11 @@ extern "C" int dyn_sys_create(void* stream, const dyn_config_t* cfg, const dyn_s
         v.cap_union = std::min<uint32_t>((uint32_t)(2.8 * mink(ag) * dl) + 64, 65534u);
         v.cap_union = std::min<uint32_t>(v.cap_union, v.nw_cap);
         // shared-memory chunk of the water-water kernel: three CTAs per SM
-        // (each CTA also needs 1 KB reserved plus < 5 KB static shared)
-        int dev = 0, smem_sm = 0, smem_blk = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-        cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        size_t per_cta = smem_sm > 18432 ? (size_t)smem_sm / 3 - 6144 : 48 * 1024;
-        per_cta = std::min<size_t>(per_cta, smem_blk > 0 ? (size_t)smem_blk : per_cta);
-        // per staged water: its 4 site positions, its 12 int32 j sums and its slot
-        const uint32_t fit = (uint32_t)((per_cta - 12 * sizeof(int)) / (4 * sizeof(float4) + 13 * sizeof(int))) / 32 * 32;
-        v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(fit, (v.cap_union + 31) / 32 * 32));
-        if (cfg->ww_union_chunk)
-            v.union_chunk = std::max<uint32_t>(32u, std::min<uint32_t>(v.union_chunk, cfg->ww_union_chunk / 32 * 32));
+        v.union_chunk = ww_chunk_for(v, cfg, 3);
         v.cap_run = v.cap_union;  // a run per union water at worst
         // fewer water groups than SMs: several CTAs share each group's entries
-        int n_sm = 0;
+        int dev = 0, n_sm = 0;
+        cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
         v.ww_split = v.ngrp_cap ? std::max<uint32_t>(1u, std::min<uint32_t>(8u, ((uint32_t)std::max(n_sm, 1) +
                                                                                v.ngrp_cap - 1) / v.ngrp_cap))
@@ -1467,6 +1476,13 @@ void energies_of(dyn_sys_s* h, dyn_energies_t* e) { fill_energies(h, e); }
 
 void set_ww_split(dyn_sys_s* h, uint32_t split) {
     h->v.ww_split = std::max(1u, std::min(8u, split));
+    set_block_counts(h->v);
+}
+
+void set_batch_member(dyn_sys_s* h) {
+    h->batch_member = true;
+    // the batch fills the GPU: no automatic group split
+    if (h->cfg.ww_split == 0) h->v.ww_split = 1;
     set_block_counts(h->v);
 }
 }  // namespace dyn
