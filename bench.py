@@ -747,8 +747,8 @@ def run_ours(args):
         "wall_s": round(t_wall, 3),
     }
     if world == 1 and not args.no_extras and name in ("c3", "c3w"):
-        # BASELINE's metric also asks for the batched and served forms beside
-        # the plain one: config 4 (64 members with peptides) and a config-5
+        # the headline metric covers the batched and served forms beside the
+        # plain one: the c4 batch (64 members with peptides) and a c5-style
         # stream (400 requests of 1,000 steps; the c5 workload runs 5,000)
         try:
             b = measure_batch("c4", args, stream, dev)

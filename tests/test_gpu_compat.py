@@ -82,10 +82,10 @@ def _c2_water_box():
 
 @pytest.mark.parametrize("make,cutoff", [(synth.config1, 10.0), (_c2_water_box, 9.0)], ids=["config1", "c2_size"])
 def test_pair_set_bit_exact_baseline_sizes(gpu_lib, make, cutoff):
-    """The reference's own configurations.  Config 1's 24.8 A box breaks the
+    """The reference's own system sizes.  The 512-water 24.8 A box breaks the
     reference's L > 2 (cutoff + skin) advice (src/lib.rs:560-561): the 14 A
     list radius exceeds half the box, so membership rests on the min-image
-    rounding alone (0.89 M flat pairs).  A config-2-size water box (7,800
+    rounding alone (0.89 M flat pairs).  A 62 A water box (7,800
     waters, 62 A, cutoff 9) has 14.8 M flat pairs."""
     _check_pair_set(make(), cutoff)
 

@@ -10,10 +10,10 @@ periodic k-d trees on the same coordinates, must be in them:
 
 * at the list build, and at the last step before the next rebuild (where
   the molecules have moved the most since the build);
-* on config 1's box (512 waters, 24.8 A, cutoff 10: the list radius exceeds
+* on the c1 box (512 waters, 24.8 A, cutoff 10: the list radius exceeds
   half the box) at every step until the first rebuild, and on a box of
   waters with chain molecules (water-atom and atom-atom lists, exclusions,
-  1-4 pairs); the config-3 box is checked in test_gpu_precision.py.
+  1-4 pairs); the 100k-atom c3 box is checked in test_gpu_precision.py.
 """
 import numpy as np
 import pytest

@@ -5,7 +5,7 @@ Config 3: a 300-residue ff19SB peptide with 0.15 M NaCl and counter-ions in
 40-residue peptide with counter-ions in 7,800 OPC waters (about 32k sites,
 62 A box, rc 9, SPME 64^3).  Forces and potential energy are compared with
 the float64 oracle in both Ewald modes (per-site force relative RMS <= 1e-5,
-potential energy relative error <= 1e-6); at config 3 the neighbour lists
+potential energy relative error <= 1e-6); on the 100k-atom c3 system (300-residue peptide, 24,000 waters) the neighbour lists
 are checked for completeness, and the total energy of a 100 ps
 constant-energy run after 100 ps of CSVR equilibration is fitted for its
 drift per ns and per atom."""
